@@ -1,0 +1,183 @@
+/* caps_gpu.h — C ABI of the B200 engine for CAPS's MD force-and-integrate step.
+ *
+ * This is the drop-in boundary between CAPS's C++ core and the device. Only plain C types cross it: pointers, sizes,
+ * doubles and POD structs. Every entry point returns 0 on success or a negative status; caps_gpu_error() gives the text,
+ * which is the text the CPU path would have thrown (FieldError messages) so the caller can rethrow it unchanged.
+ *
+ * What each entry point replaces in the reference (paths inside MuhammadUzairRiaz/CAPS):
+ *   caps_gpu_create     Evaluator::Evaluator(const ForceField&, const EnergyOptions&)   core/include/caps/field.hpp:332
+ *   caps_gpu_set_options Evaluator::set_options(const EnergyOptions&)                    core/include/caps/field.hpp:337
+ *   caps_gpu_energies   Evaluator::energies(bool)                                       core/include/caps/field.hpp:344
+ *   caps_gpu_compute    Evaluator::compute(x, cell, f) -> EnergyTerms                    core/include/caps/field.hpp:340
+ *   caps_gpu_list_builds Evaluator::list_builds()                                       core/include/caps/field.hpp:341
+ *   caps_gpu_run        run_dynamics(System&, const DynamicsOptions&, DynamicsReport*)   core/include/caps/dynamics.hpp:180
+ *   caps_gpu_destroy    Evaluator::~Evaluator()                                          core/include/caps/field.hpp:333
+ *   caps_gpu_error      FieldError text / caps_last_error()                              capi/include/caps_c.h:63
+ *
+ * Units are the reference's (LAMMPS "real"): Å, fs, kcal/mol, e, g/mol, K, atm.
+ */
+#ifndef CAPS_GPU_H
+#define CAPS_GPU_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CAPS_GPU_ABI_VERSION 1
+
+/* Status codes (negative). The text is in caps_gpu_error(). */
+#define CAPS_GPU_OK 0
+#define CAPS_GPU_EINVAL (-1)      /* bad argument: sizes, options the engine does not take */
+#define CAPS_GPU_ECUDA (-2)       /* a CUDA call failed */
+#define CAPS_GPU_EFIELD (-3)      /* FieldError: FENE overstretch, cell too small, non-finite coordinates */
+#define CAPS_GPU_ECONSTRAINT (-4) /* SHAKE/RATTLE did not converge or a bond turned past 90 degrees */
+#define CAPS_GPU_ECANCEL (-5)     /* the progress callback asked to stop (DynamicsCancelled) */
+#define CAPS_GPU_ENODEV (-6)      /* no CUDA device: there is no CPU fallback */
+
+/* The force field as the device path consumes it: the subset of caps::ForceField (core/include/caps/field.hpp:154-249)
+ * that the MD hot path reads, flattened to arrays. Pair coefficients are given per type pair after mixing
+ * (caps::mixed_pair, field.cpp:2588), so the mixing rule stays on the host. Term lists keep the reference's order;
+ * dihedral and improper Fourier terms of one quadruple stay adjacent, as the reference groups them
+ * (field.cpp:1875-1920). Arrays are read during caps_gpu_create and not kept. */
+typedef struct {
+  int32_t natoms;
+  int32_t ntypes;
+  const int32_t* type_index; /* [natoms] */
+  const double* charge;      /* [natoms] e (already divided by sqrt(dielectric) if the model has one) */
+  const double* mass;        /* [natoms] g/mol */
+  const double* pair_eps;    /* [ntypes*ntypes] kcal/mol, after mixing; <= 0: the pair does not interact */
+  const double* pair_sigma;  /* [ntypes*ntypes] Å */
+  int32_t nbonds;            /* harmonic bonds k (r - r0)^2 */
+  const uint32_t* bond_ij;   /* [2*nbonds] */
+  const double* bond_k_r0;   /* [2*nbonds] */
+  int32_t nangles;           /* harmonic angles kt (theta - theta0)^2, j the vertex, theta0 in radians */
+  const uint32_t* angle_ijk; /* [3*nangles] */
+  const double* angle_kt_theta0;
+  int32_t ndihedrals;        /* v [1 + cos(n phi - delta)], IUPAC phi */
+  const uint32_t* dihedral_ijkl; /* [4*ndihedrals] */
+  const double* dihedral_v_delta; /* [2*ndihedrals] */
+  const int32_t* dihedral_n;      /* [ndihedrals] */
+  int32_t nimpropers;             /* same form as the dihedrals (AMBER/OPLS order) */
+  const uint32_t* improper_ijkl;
+  const double* improper_v_delta;
+  const int32_t* improper_n;
+  int32_t npairs14;               /* 1-4 pairs: LJ scaled by lj14 (or per pair), Coulomb handled with the exclusions */
+  const uint32_t* pair14_ij;      /* [2*npairs14] */
+  const double* pair14_lj;        /* [npairs14] per-pair LJ scale, or NULL for lj14 */
+  const double* pair14_coul;      /* [npairs14] per-pair Coulomb scale, or NULL for coul14 */
+  double lj14, coul14;
+  const uint32_t* excl_offset;    /* [natoms+1] CSR of ForceField::excluded (1-2, 1-3, 1-4 partners, sorted) */
+  const uint32_t* excl_list;
+  int32_t nfene;                  /* BondX form 3: -0.5 K R0^2 ln(1-(r/R0)^2) + WCA(eps, sigma) below 2^(1/6) sigma */
+  const uint32_t* fene_ij;        /* [2*nfene] */
+  const double* fene_k_r0_eps_sigma; /* [4*nfene] */
+  int32_t lj_shift;               /* ForceField::lj_shift: LJ shifted to zero at the cut-off, no tail correction */
+  double model_cutoff;            /* ForceField::cutoff: > 0 replaces the options' cut-off */
+} caps_gpu_ff;
+
+/* caps::EnergyOptions (field.hpp:274-308), the fields the device path takes. */
+typedef struct {
+  double cutoff;        /* Å, LJ and Coulomb (default 10) */
+  double skin;          /* Å, Verlet buffer (default 2) */
+  int32_t coulomb;      /* electrostatics on */
+  int32_t electrostatics; /* 0 damped shifted force, 1 PME */
+  double dsf_alpha;     /* 1/Å (0.2) */
+  double ewald_rtol;    /* erfc(beta rc) = rtol (1e-5) */
+  double pme_spacing;   /* Å (1.0) */
+  int32_t pme_order;    /* B-spline order, 3..8 (reference default 5; the configs use 4) */
+  int32_t tail;         /* LJ tail correction */
+  int32_t precision;    /* 0 mixed: FP32 arithmetic, int64 fixed-point forces; 1 double: FP64 throughout */
+  double force_cap;     /* > 0: LJ continued linearly inside the radius where |F| reaches this (push-off); FP64 only */
+  int32_t parts;        /* 1 bonded, 2 non-bonded, 3 both (r-RESPA splits) */
+} caps_gpu_opts;
+
+/* caps::EnergyTerms (field.hpp:310-320). */
+typedef struct {
+  double bond, angle, dihedral, improper, vdw, coulomb;
+  double virial;        /* sum r.f, kcal/mol */
+  double w[6];          /* virial tensor xx yy zz xy xz yz */
+  double tail_energy, tail_virial;
+} caps_gpu_terms;
+
+/* caps::DynamicsOptions (dynamics.hpp:60-154), the fields the device step takes. */
+typedef struct {
+  double dt;                /* fs */
+  int64_t steps;
+  double temperature;       /* K */
+  double temperature_end;   /* K; >= 0 ramps the target linearly over the run */
+  int32_t thermostat;       /* 0 none (NVE), 1 Bussi, 2 Langevin (BAOAB), 3 Nose-Hoover chain of 3 */
+  double tau_t;             /* fs */
+  int32_t barostat;         /* 0 none, 1 stochastic cell rescaling */
+  double pressure;          /* atm */
+  double tau_p;             /* fs */
+  double compressibility;   /* 1/atm */
+  int32_t barostat_every;
+  int32_t constraints;      /* 0 none, 1 bonds to hydrogen and rigid water (SHAKE/RATTLE; SETTLE for waters) */
+  int32_t new_velocities;   /* draw Maxwell-Boltzmann velocities even when given some */
+  uint64_t seed;
+  int32_t thermo_every;
+  int32_t frame_every;      /* 0 none */
+  int64_t step_offset;
+  int32_t respa;            /* r-RESPA inner steps (1 off) */
+  const int8_t* is_hydrogen; /* [natoms] element == 1, for the constraint set; NULL: mass < 1.6 */
+  const int8_t* is_oxygen;   /* [natoms] element == 8, for rigid waters; NULL: none */
+} caps_gpu_md_opts;
+
+/* caps::ThermoRow (dynamics.hpp:28-43), the fields the device step fills. */
+typedef struct {
+  int64_t step;
+  double time_ps, temperature, potential, kinetic, total, conserved, pressure, volume, density;
+  double target_temperature;
+  double p[6];
+  caps_gpu_terms terms;
+} caps_gpu_thermo;
+
+/* Called with each thermo row; non-zero cancels the run (DynamicsCancelled). */
+typedef int32_t (*caps_gpu_progress_fn)(const caps_gpu_thermo* row, void* user);
+/* Called with each recorded frame: positions (3N, unwrapped), cell[12] (origin, a, b, c) and step. */
+typedef void (*caps_gpu_frame_fn)(const double* x, const double* cell, int64_t step, void* user);
+
+/* The state a run works on, in place: positions (3N unwrapped), velocities (3N, Å/fs; may be NULL to draw them),
+ * cell[12] (origin, a, b, c). On return they hold the end state. */
+typedef struct {
+  double* x;
+  double* v;
+  double* cell;
+  int32_t has_velocities;
+} caps_gpu_state;
+
+typedef struct caps_gpu_engine caps_gpu_engine;
+
+int32_t caps_gpu_abi_version(void);
+/* Number of CUDA devices visible (0: none). Needs no engine. */
+int32_t caps_gpu_device_count(void);
+
+/* Builds the engine on the current CUDA device: uploads the force field, sizes the buffers. NULL on error, with the
+ * text in caps_gpu_error(NULL). Replaces Evaluator::Evaluator (core/include/caps/field.hpp:332). */
+caps_gpu_engine* caps_gpu_create(const caps_gpu_ff* ff, const caps_gpu_opts* opts);
+/* Replaces Evaluator::set_options (field.hpp:337): a new cut-off or skin rebuilds the list at the next call. */
+int32_t caps_gpu_set_options(caps_gpu_engine* e, const caps_gpu_opts* opts);
+/* Replaces Evaluator::energies(bool) (field.hpp:344): 0 lets later calls skip the pair energies (forces unchanged). */
+int32_t caps_gpu_energies(caps_gpu_engine* e, int32_t on);
+/* Energy, forces and virial at x (3N, Å, host memory) in cell[12]; f (3N host) is overwritten. Replaces
+ * Evaluator::compute (field.hpp:340, field.cpp:1249-2539). */
+int32_t caps_gpu_compute(caps_gpu_engine* e, const double* x, const double* cell, double* f, caps_gpu_terms* out);
+/* The same with x and f already in device memory (3N doubles each): no host copies. */
+int32_t caps_gpu_compute_device(caps_gpu_engine* e, const double* d_x, const double* cell, double* d_f, caps_gpu_terms* out);
+/* Replaces Evaluator::list_builds (field.hpp:341). */
+int32_t caps_gpu_list_builds(const caps_gpu_engine* e);
+/* Molecular dynamics in place on `state` (host memory). Replaces run_dynamics (dynamics.hpp:180; dynamics.cpp:71-815)
+ * for the options above. progress and frame may be NULL. report (may be NULL) receives a short text summary. */
+int32_t caps_gpu_run(caps_gpu_engine* e, caps_gpu_state* state, const caps_gpu_md_opts* md, caps_gpu_progress_fn progress,
+                     caps_gpu_frame_fn frame, void* user, char* report, int32_t report_cap);
+/* The last run's throughput: steps per second over the step loop (first force excluded, as dynamics.cpp:601,776). */
+double caps_gpu_last_steps_per_second(const caps_gpu_engine* e);
+void caps_gpu_destroy(caps_gpu_engine* e);
+/* Text of the last error on this engine (or of the last failed caps_gpu_create when e is NULL). */
+const char* caps_gpu_error(const caps_gpu_engine* e);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CAPS_GPU_H */

@@ -1,0 +1,421 @@
+// ORACLE / TEST INFRASTRUCTURE — not part of the product path.
+//
+// A C entry layer over the reference CAPS C++ core (compiled from its sources by oracle/Makefile), so that the parity
+// tests and the CPU baseline can drive the reference from plain arrays through ctypes. It takes the same POD force
+// field (caps_gpu_ff, include/caps_gpu.h) the device engine takes and rebuilds a caps::ForceField from it:
+//   ref_compute  -> caps::Evaluator::compute      (core/src/field.cpp:1249)
+//   ref_run      -> caps::run_dynamics            (core/src/dynamics.cpp:71)
+//   ref_pme      -> caps::pme_reciprocal (threaded, core/src/kspace.cpp:80)
+//   ref_build_*  -> the reference builders (grow + relax + assign_gaff as tests/test_nbnxm.cpp:19-34; kremer_grest),
+//                   written to a flat binary file the Python side reads (tests/golden fixtures are made from these).
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "caps/dynamics.hpp"
+#include "caps/field.hpp"
+#include "caps/grow.hpp"
+#include "caps/kremer_grest.hpp"
+#include "caps/kspace.hpp"
+#include "caps/relax.hpp"
+#include "kspace_pool.hpp"
+#include "parallel.hpp"
+#include "caps_gpu.h"
+
+using namespace caps;
+
+namespace {
+
+thread_local std::string g_err;
+
+Cell to_cell(const double* c) {
+  Cell cell;
+  for (int k = 0; k < 3; ++k) {
+    cell.origin[k] = c[k];
+    cell.a[k] = c[3 + k];
+    cell.b[k] = c[6 + k];
+    cell.c[k] = c[9 + k];
+  }
+  return cell;
+}
+
+void from_cell(const Cell& cell, double* c) {
+  for (int k = 0; k < 3; ++k) {
+    c[k] = cell.origin[k];
+    c[3 + k] = cell.a[k];
+    c[6 + k] = cell.b[k];
+    c[9 + k] = cell.c[k];
+  }
+}
+
+std::shared_ptr<ForceField> to_ff(const caps_gpu_ff* p) {
+  auto ff = std::make_shared<ForceField>();
+  const int n = p->natoms, nt = p->ntypes;
+  ff->name = "from caps_gpu_ff";
+  ff->type_index.assign(p->type_index, p->type_index + n);
+  ff->atom_type.resize(size_t(n));
+  ff->type_names.resize(size_t(nt));
+  ff->lj.assign(size_t(nt), PairType{0.0, 1.0});
+  for (int t = 0; t < nt; ++t) {
+    ff->type_names[size_t(t)] = "t" + std::to_string(t);
+    ff->lj[size_t(t)] = {p->pair_eps[t * nt + t], p->pair_sigma[t * nt + t]};
+  }
+  for (int i = 0; i < n; ++i) ff->atom_type[size_t(i)] = ff->type_names[size_t(p->type_index[i])];
+  for (int a = 0; a < nt; ++a)
+    for (int b = a; b < nt; ++b) ff->pair_override[{a, b}] = PairType{p->pair_eps[a * nt + b], p->pair_sigma[a * nt + b]};
+  ff->mixing = "geometric";
+  ff->pair_form = "lj12-6";
+  ff->charge.assign(p->charge, p->charge + n);
+  ff->mass.assign(p->mass, p->mass + n);
+  for (int k = 0; k < p->nbonds; ++k) ff->bonds.push_back({p->bond_ij[2 * k], p->bond_ij[2 * k + 1], p->bond_k_r0[2 * k], p->bond_k_r0[2 * k + 1]});
+  for (int k = 0; k < p->nangles; ++k)
+    ff->angles.push_back({p->angle_ijk[3 * k], p->angle_ijk[3 * k + 1], p->angle_ijk[3 * k + 2], p->angle_kt_theta0[2 * k], p->angle_kt_theta0[2 * k + 1]});
+  for (int k = 0; k < p->ndihedrals; ++k)
+    ff->dihedrals.push_back({p->dihedral_ijkl[4 * k], p->dihedral_ijkl[4 * k + 1], p->dihedral_ijkl[4 * k + 2], p->dihedral_ijkl[4 * k + 3],
+                             p->dihedral_v_delta[2 * k], p->dihedral_n[k], p->dihedral_v_delta[2 * k + 1]});
+  for (int k = 0; k < p->nimpropers; ++k)
+    ff->impropers.push_back({p->improper_ijkl[4 * k], p->improper_ijkl[4 * k + 1], p->improper_ijkl[4 * k + 2], p->improper_ijkl[4 * k + 3],
+                             p->improper_v_delta[2 * k], p->improper_n[k], p->improper_v_delta[2 * k + 1]});
+  for (int k = 0; k < p->npairs14; ++k) {
+    ff->pairs14.push_back({p->pair14_ij[2 * k], p->pair14_ij[2 * k + 1]});
+    if (p->pair14_lj) ff->pairs14_lj.push_back(p->pair14_lj[k]);
+    if (p->pair14_coul) ff->pairs14_coul.push_back(p->pair14_coul[k]);
+  }
+  if (p->pair14_lj && !p->pair14_coul) ff->pairs14_coul.assign(size_t(p->npairs14), p->coul14);
+  if (p->pair14_coul && !p->pair14_lj) ff->pairs14_lj.assign(size_t(p->npairs14), p->lj14);
+  ff->lj14 = p->lj14;
+  ff->coul14 = p->coul14;
+  ff->excluded.assign(size_t(n), {});
+  if (p->excl_offset)
+    for (int i = 0; i < n; ++i) ff->excluded[size_t(i)].assign(p->excl_list + p->excl_offset[i], p->excl_list + p->excl_offset[i + 1]);
+  for (int k = 0; k < p->nfene; ++k) {
+    const double* q = p->fene_k_r0_eps_sigma + 4 * k;
+    ff->bonds_x.push_back({p->fene_ij[2 * k], p->fene_ij[2 * k + 1], 3, q[0], q[1], q[2], q[3]});
+  }
+  ff->lj_shift = p->lj_shift != 0;
+  ff->cutoff = p->model_cutoff;
+  return ff;
+}
+
+EnergyOptions to_eo(const caps_gpu_opts* o, int threads) {
+  EnergyOptions e;
+  e.cutoff = o->cutoff;
+  e.skin = o->skin;
+  e.coulomb = o->coulomb != 0;
+  e.electrostatics = o->electrostatics ? EnergyOptions::Electrostatics::PME : EnergyOptions::Electrostatics::DSF;
+  e.dsf_alpha = o->dsf_alpha;
+  e.ewald_rtol = o->ewald_rtol;
+  e.pme_spacing = o->pme_spacing;
+  e.pme_order = o->pme_order;
+  e.tail = o->tail != 0;
+  e.mixed = o->precision == 0;
+  e.force_cap = o->force_cap;
+  e.parts = o->parts ? o->parts : 3;
+  e.threads = threads;
+  return e;
+}
+
+void to_terms(const EnergyTerms& t, caps_gpu_terms* o) {
+  o->bond = t.bond;
+  o->angle = t.angle;
+  o->dihedral = t.dihedral;
+  o->improper = t.improper;
+  o->vdw = t.vdw;
+  o->coulomb = t.coulomb;
+  o->virial = t.virial;
+  for (int c = 0; c < 6; ++c) o->w[c] = t.w[c];
+  o->tail_energy = t.tail_energy;
+  o->tail_virial = t.tail_virial;
+}
+
+// --- a flat binary export: records of (name[32], kind char, 7 pad bytes, int64 count, data) ---------------------
+struct Writer {
+  FILE* f;
+  explicit Writer(const char* path) : f(std::fopen(path, "wb")) {
+    if (!f) throw std::runtime_error(std::string("cannot write ") + path);
+    std::fwrite("CAPSFF1\n", 1, 8, f);
+  }
+  ~Writer() { if (f) std::fclose(f); }
+  void rec(const char* name, char kind, const void* data, int64_t count, size_t size) {
+    char head[40] = {0};
+    std::strncpy(head, name, 31);
+    head[32] = kind;
+    std::fwrite(head, 1, 40, f);
+    std::fwrite(&count, sizeof count, 1, f);
+    if (count) std::fwrite(data, size, size_t(count), f);
+  }
+  void d(const char* name, const std::vector<double>& v) { rec(name, 'd', v.data(), int64_t(v.size()), 8); }
+  void i(const char* name, const std::vector<int32_t>& v) { rec(name, 'i', v.data(), int64_t(v.size()), 4); }
+  void u(const char* name, const std::vector<uint32_t>& v) { rec(name, 'u', v.data(), int64_t(v.size()), 4); }
+  void s(const char* name, const std::string& v) { rec(name, 's', v.data(), int64_t(v.size()), 1); }
+};
+
+void export_system(const System& s, const ForceField& ff, const char* path) {
+  Writer w(path);
+  const size_t n = s.atoms.size(), nt = ff.lj.size();
+  std::vector<double> x, cell(12);
+  for (const auto& a : s.atoms) x.insert(x.end(), a.pos.begin(), a.pos.end());
+  from_cell(s.cell, cell.data());
+  w.d("x", x);
+  w.d("cell", cell);
+  std::vector<int32_t> el, ti(ff.type_index.begin(), ff.type_index.end());
+  for (const auto& a : s.atoms) el.push_back(a.element);
+  w.i("element", el);
+  w.i("type_index", ti);
+  w.d("charge", ff.charge);
+  w.d("mass", ff.mass);
+  std::vector<double> pe(nt * nt), ps(nt * nt);
+  for (size_t a = 0; a < nt; ++a)
+    for (size_t b = 0; b < nt; ++b) {
+      const PairType pt = mixed_pair(ff, int(a), int(b));
+      pe[a * nt + b] = pt.eps;
+      ps[a * nt + b] = pt.sigma;
+    }
+  w.d("pair_eps", pe);
+  w.d("pair_sigma", ps);
+  std::vector<uint32_t> bij;
+  std::vector<double> bkr;
+  for (const auto& b : ff.bonds) bij.insert(bij.end(), {b.i, b.j}), bkr.insert(bkr.end(), {b.k, b.r0});
+  w.u("bond_ij", bij);
+  w.d("bond_k_r0", bkr);
+  std::vector<uint32_t> aijk;
+  std::vector<double> akt;
+  for (const auto& a : ff.angles) aijk.insert(aijk.end(), {a.i, a.j, a.k}), akt.insert(akt.end(), {a.kt, a.theta0});
+  w.u("angle_ijk", aijk);
+  w.d("angle_kt_theta0", akt);
+  auto tors = [&](const std::vector<TorsionTerm>& T, const char* a, const char* b, const char* c) {
+    std::vector<uint32_t> ijkl;
+    std::vector<double> vd;
+    std::vector<int32_t> nn;
+    for (const auto& t : T) ijkl.insert(ijkl.end(), {t.i, t.j, t.k, t.l}), vd.insert(vd.end(), {t.v, t.delta}), nn.push_back(t.n);
+    w.u(a, ijkl);
+    w.d(b, vd);
+    w.i(c, nn);
+  };
+  tors(ff.dihedrals, "dihedral_ijkl", "dihedral_v_delta", "dihedral_n");
+  tors(ff.impropers, "improper_ijkl", "improper_v_delta", "improper_n");
+  std::vector<uint32_t> p14;
+  for (const auto& p : ff.pairs14) p14.insert(p14.end(), {p[0], p[1]});
+  w.u("pair14_ij", p14);
+  w.d("pair14_lj", ff.pairs14_lj);
+  w.d("pair14_coul", ff.pairs14_coul);
+  w.d("lj14_coul14", {ff.lj14, ff.coul14});
+  std::vector<uint32_t> eo{0}, el2;
+  for (size_t i = 0; i < n; ++i) {
+    const auto& e = i < ff.excluded.size() ? ff.excluded[i] : std::vector<uint32_t>{};
+    el2.insert(el2.end(), e.begin(), e.end());
+    eo.push_back(uint32_t(el2.size()));
+  }
+  w.u("excl_offset", eo);
+  w.u("excl_list", el2);
+  std::vector<uint32_t> fij;
+  std::vector<double> fp;
+  int other_bx = 0;
+  for (const auto& b : ff.bonds_x) {
+    if (b.form != 3) { ++other_bx; continue; }
+    fij.insert(fij.end(), {b.i, b.j});
+    fp.insert(fp.end(), {b.a, b.b, b.c, b.d});
+  }
+  w.u("fene_ij", fij);
+  w.d("fene_k_r0_eps_sigma", fp);
+  w.i("flags", {ff.lj_shift ? 1 : 0, ff.keep13 ? 1 : 0});
+  w.d("model_cutoff", {ff.cutoff});
+  // terms the device path does not take: the exporter counts them so a test can refuse such a cell
+  const size_t unsupported = ff.impropers_harmonic.size() + ff.inversions.size() + size_t(other_bx) + ff.angles_x.size() + ff.urey_bradley.size() +
+                             ff.cbt.size() + ff.lj_pairs.size() + ff.pair_func.size() + ff.bonds2.size() + ff.angles2.size() + ff.dihedrals2.size() +
+                             ff.impropers2.size() + ff.vsites.size() + (ff.pair_form != "lj12-6") + ff.lj14_types.size();
+  w.i("unsupported", {int32_t(unsupported)});
+  w.s("name", ff.name);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ref_error() { return g_err.c_str(); }
+
+int ref_compute(const caps_gpu_ff* p, const caps_gpu_opts* o, const double* x, const double* cell, double* f, caps_gpu_terms* out, int threads) {
+  try {
+    auto ff = to_ff(p);
+    Evaluator ev(*ff, to_eo(o, threads));
+    std::vector<double> xv(x, x + 3 * size_t(p->natoms)), fv;
+    const EnergyTerms t = ev.compute(xv, to_cell(cell), fv);
+    std::memcpy(f, fv.data(), fv.size() * sizeof(double));
+    to_terms(t, out);
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+// Times `reps` evaluations on one evaluator (the list built on the first), for the CPU baseline: seconds per call.
+int ref_time_compute(const caps_gpu_ff* p, const caps_gpu_opts* o, const double* x, const double* cell, int reps, int threads, double* seconds) {
+  try {
+    auto ff = to_ff(p);
+    Evaluator ev(*ff, to_eo(o, threads));
+    std::vector<double> xv(x, x + 3 * size_t(p->natoms)), fv;
+    const Cell c = to_cell(cell);
+    ev.compute(xv, c, fv);
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int r = 0; r < reps; ++r) ev.compute(xv, c, fv);
+    *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() / std::max(1, reps);
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+// run_dynamics on a System rebuilt from the arrays. element: [natoms] atomic numbers (for SHAKE's hydrogens and rigid
+// waters). rows: up to max_rows thermo rows out. seconds and ns_per_day from the reference's own report.
+int ref_run(const caps_gpu_ff* p, const caps_gpu_opts* eo, caps_gpu_state* st, const caps_gpu_md_opts* md, const int32_t* element, int threads,
+            caps_gpu_thermo* rows, int max_rows, int* nrows, double* seconds, double* ns_per_day) {
+  try {
+    auto ff = to_ff(p);
+    System s;
+    const int n = p->natoms;
+    s.atoms.resize(size_t(n));
+    for (int i = 0; i < n; ++i) {
+      for (int k = 0; k < 3; ++k) s.atoms[size_t(i)].pos[k] = st->x[3 * i + k];
+      s.atoms[size_t(i)].element = element ? element[i] : 6;
+      s.atoms[size_t(i)].charge = p->charge[i];
+      s.atoms[size_t(i)].type = p->type_index[i] + 1;
+    }
+    for (const auto& b : ff->bonds) s.bonds.push_back({b.i, b.j, 1});
+    for (const auto& b : ff->bonds_x) s.bonds.push_back({b.i, b.j, 1});
+    s.cell = to_cell(st->cell);
+    if (st->has_velocities && st->v) {
+      s.velocities.resize(size_t(n));
+      for (int i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) s.velocities[size_t(i)][k] = st->v[3 * i + k];
+    }
+    DynamicsOptions o;
+    o.field = ff;
+    o.dt = md->dt;
+    o.steps = md->steps;
+    o.temperature = md->temperature;
+    o.temperature_end = md->temperature_end;
+    const Thermostat th[4] = {Thermostat::None, Thermostat::Bussi, Thermostat::Langevin, Thermostat::NoseHoover};
+    o.thermostat = th[md->thermostat & 3];
+    o.tau_t = md->tau_t;
+    o.barostat = md->barostat == 1 ? Barostat::CRescale : Barostat::None;
+    o.pressure = md->pressure;
+    o.tau_p = md->tau_p;
+    o.compressibility = md->compressibility;
+    o.barostat_every = md->barostat_every;
+    o.constraints = md->constraints ? ConstraintMode::HBonds : ConstraintMode::None;
+    o.new_velocities = md->new_velocities != 0;
+    o.seed = md->seed;
+    o.thermo_every = md->thermo_every;
+    o.frame_every = 0;
+    o.step_offset = md->step_offset;
+    o.respa = md->respa > 1 ? md->respa : 1;
+    o.energy = to_eo(eo, threads);
+    int k = 0;
+    o.progress = [&](const ThermoRow& r) {
+      if (k < max_rows) {
+        caps_gpu_thermo& t = rows[k];
+        std::memset(&t, 0, sizeof t);
+        t.step = r.step;
+        t.time_ps = r.time_ps;
+        t.temperature = r.temperature;
+        t.potential = r.potential;
+        t.kinetic = r.kinetic;
+        t.total = r.total;
+        t.conserved = r.conserved;
+        t.pressure = r.pressure;
+        t.volume = r.volume;
+        t.density = r.density;
+        t.target_temperature = r.target_temperature;
+        for (int c = 0; c < 6; ++c) t.p[c] = r.p[c];
+      }
+      ++k;
+      return true;
+    };
+    DynamicsReport rep;
+    run_dynamics(s, o, &rep);
+    *nrows = k;
+    *seconds = rep.seconds;
+    *ns_per_day = rep.ns_per_day;
+    for (int i = 0; i < n; ++i)
+      for (int c = 0; c < 3; ++c) {
+        st->x[3 * i + c] = s.atoms[size_t(i)].pos[c];
+        if (st->v) st->v[3 * i + c] = s.velocities[size_t(i)][c];
+      }
+    from_cell(s.cell, st->cell);
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+double ref_ewald_beta(double rc, double rtol) { return ewald_beta(rc, rtol); }
+
+void ref_pme_grid(const double* cell, double beta, double spacing, int order, int* k) {
+  const PmeGrid g = pme_grid(to_cell(cell), beta, spacing, order);
+  for (int d = 0; d < 3; ++d) k[d] = g.k[d];
+}
+
+// The threaded half-spectrum PME of the evaluator (kspace.cpp:80) on given arrays; forces added to f.
+double ref_pme(int n, const double* x, const double* q, const double* cell, const int* k, int order, double beta, double* f, double* vir, int threads) {
+  std::vector<double> xv(x, x + 3 * size_t(n)), qv(q, q + n), fv(f, f + 3 * size_t(n));
+  PmeGrid g;
+  for (int d = 0; d < 3; ++d) g.k[d] = k[d];
+  g.order = order;
+  g.beta = beta;
+  ThreadPool pool(threads > 0 ? threads : 1);
+  const double e = pme_reciprocal(xv, qv, to_cell(cell), g, fv, vir, pool);
+  std::memcpy(f, fv.data(), fv.size() * sizeof(double));
+  return e;
+}
+
+// Builders: a grown and relaxed atactic polystyrene cell with GAFF (tests/test_nbnxm.cpp:19-34 builds the same kind).
+int ref_build_ps_gaff(int chains, int dp, double grow_density, double target_density, uint64_t seed, const char* path) {
+  try {
+    GrowOptions g;
+    g.chains = chains;
+    g.dp = dp;
+    g.density = grow_density;
+    g.seed = seed;
+    System c = grow(g);
+    RelaxOptions r;
+    r.target_density = target_density;
+    r.ftol = 1.0;
+    relax(c, r);
+    const ForceField ff = assign_gaff(c);
+    export_system(c, ff, path);
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+// A Kremer-Grest melt (random-walk chains, not pushed off) with its FENE-WCA force field, in reduced units mapped as
+// sigma = 1 Å, eps = kB T at T = 1/kB... the caller picks; here the unmapped reduced model (1 Å, 1 kcal/mol, 1 g/mol).
+int ref_build_kg(int chains, int beads, double density, uint64_t seed, const char* path) {
+  try {
+    KgOptions o;
+    o.chains = chains;
+    o.beads = beads;
+    o.density = density;
+    o.seed = seed;
+    System s = kremer_grest(o);
+    const ForceField ff = kremer_grest_forcefield(s, o);
+    export_system(s, ff, path);
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+}  // extern "C"
