@@ -1,0 +1,340 @@
+// K-BOND: bonded terms, 1-4 pairs, the Coulomb corrections of excluded pairs and FENE bonds, one thread per term.
+// Reference: Evaluator::compute's bonded phase (core/src/field.cpp:1863-2283): harmonic bonds (:1986-1995), harmonic
+// angles (:1996-2010), Fourier torsion groups for dihedrals and impropers (:1875-1920, 2011-2018), 1-4 pairs (:2019-2043),
+// excluded-pair electrostatics (:2206-2266), FENE + WCA (:2152-2166). The FP32 path computes each term in single
+// precision from double separations and adds forces as 64-bit fixed point; the FP64 path is double throughout.
+#pragma once
+#include "common.cuh"
+
+namespace capsb {
+
+struct BondedArgs {
+  const double* x;
+  DevCell cell;
+  EnergySink en;
+  int fixed;   // 1: mixed path (fixed-point sinks)
+};
+
+// Per-thread energy and virial, summed over the block and added once.
+template <bool VIR>
+struct Tally {
+  double e = 0;
+  double w[6] = {0, 0, 0, 0, 0, 0};
+  template <class R>
+  __device__ __forceinline__ void vir(R dx, R dy, R dz, R fx, R fy, R fz) {
+    if (!VIR) return;
+    w[0] += double(dx * fx);
+    w[1] += double(dy * fy);
+    w[2] += double(dz * fz);
+    w[3] += 0.5 * double(dx * fy + dy * fx);
+    w[4] += 0.5 * double(dx * fz + dz * fx);
+    w[5] += 0.5 * double(dy * fz + dz * fy);
+  }
+  __device__ void flush(const BondedArgs& A, int slot, bool ener) {
+    __shared__ double scratch[32];
+    if (ener) {
+      const double s = block_sum(e, scratch);
+      if (threadIdx.x == 0 && s != 0) A.en.add(slot, s, A.fixed);
+    }
+    if (VIR)
+      for (int k = 0; k < 6; ++k) {
+        const double s = block_sum(w[k], scratch);
+        if (threadIdx.x == 0 && s != 0) A.en.add(kEW0 + k, s, A.fixed);
+      }
+  }
+};
+
+template <class R>
+__device__ __forceinline__ void sep(const BondedArgs& A, int i, int j, R& dx, R& dy, R& dz) {
+  double ex = A.x[3 * j] - A.x[3 * i], ey = A.x[3 * j + 1] - A.x[3 * i + 1], ez = A.x[3 * j + 2] - A.x[3 * i + 2];
+  min_image(A.cell, ex, ey, ez);
+  dx = R(ex), dy = R(ey), dz = R(ez);
+}
+
+template <class R> __device__ __forceinline__ R rsq(R v) { return sqrt(v); }
+template <> __device__ __forceinline__ float rsq<float>(float v) { return sqrtf(v); }
+
+// harmonic bonds: k (r - r0)^2
+template <class R, bool ENER, bool VIR>
+static __global__ void k_bonds(int nb, const uint32_t* __restrict__ ij, const double* __restrict__ kr, BondedArgs A, ForceSink<R> F) {
+  Tally<VIR> T;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nb; t += gridDim.x * blockDim.x) {
+    const int i = int(ij[2 * t]), j = int(ij[2 * t + 1]);
+    R dx, dy, dz;
+    sep(A, i, j, dx, dy, dz);
+    const R k = R(kr[2 * t]), r0 = R(kr[2 * t + 1]);
+    const R r = rsq(dx * dx + dy * dy + dz * dz), dr = r - r0;
+    if (ENER) T.e += double(k * dr * dr);
+    const R s = r > R(1e-12) ? -2 * k * dr / r : R(0);
+    const R fx = dx * s, fy = dy * s, fz = dz * s;
+    F.add(j, fx, fy, fz);
+    F.add(i, -fx, -fy, -fz);
+    T.vir(dx, dy, dz, fx, fy, fz);
+  }
+  T.flush(A, kEBond, ENER);
+}
+
+// harmonic angles: kt (theta - theta0)^2, j the vertex
+template <class R, bool ENER, bool VIR>
+static __global__ void k_angles(int na, const uint32_t* __restrict__ ijk, const double* __restrict__ kt0, BondedArgs A, ForceSink<R> F) {
+  Tally<VIR> T;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < na; t += gridDim.x * blockDim.x) {
+    const int i = int(ijk[3 * t]), j = int(ijk[3 * t + 1]), k = int(ijk[3 * t + 2]);
+    R ux, uy, uz, vx, vy, vz;
+    sep(A, j, i, ux, uy, uz);   // u = x_i - x_j
+    sep(A, j, k, vx, vy, vz);   // v = x_k - x_j
+    const R lu = rsq(ux * ux + uy * uy + uz * uz), lv = rsq(vx * vx + vy * vy + vz * vz);
+    R c = (ux * vx + uy * vy + uz * vz) / (lu * lv);
+    c = c > R(1) ? R(1) : (c < R(-1) ? R(-1) : c);
+    const R th = acos(c);
+    R sn = rsq(R(1) - c * c);
+    sn = sn > R(1e-8) ? sn : R(1e-8);
+    const R dth = th - R(kt0[2 * t + 1]);
+    const R kk = R(kt0[2 * t]);
+    if (ENER) T.e += double(kk * dth * dth);
+    const R g = 2 * kk * dth / sn;
+    const R iuv = R(1) / (lu * lv), cu = c / (lu * lu), cv = c / (lv * lv);
+    const R fix = (vx * iuv - ux * cu) * g, fiy = (vy * iuv - uy * cu) * g, fiz = (vz * iuv - uz * cu) * g;
+    const R fkx = (ux * iuv - vx * cv) * g, fky = (uy * iuv - vy * cv) * g, fkz = (uz * iuv - vz * cv) * g;
+    F.add(i, fix, fiy, fiz);
+    F.add(k, fkx, fky, fkz);
+    F.add(j, -(fix + fkx), -(fiy + fky), -(fiz + fkz));
+    T.vir(ux, uy, uz, fix, fiy, fiz);
+    T.vir(vx, vy, vz, fkx, fky, fkz);
+  }
+  T.flush(A, kEAngle, ENER);
+}
+
+// Fourier torsion groups: terms [gs[g], gs[g+1]) share one quadruple; v [1 + cos(n phi - delta)], phi IUPAC, cos/sin of
+// n phi by recurrence (field.cpp:1875-1920).
+template <class R, bool ENER, bool VIR>
+static __global__ void k_torsions(int ngroups, const int* __restrict__ gs, const uint32_t* __restrict__ ijkl, const double* __restrict__ vd,
+                           const int* __restrict__ nn, BondedArgs A, ForceSink<R> F, int slot) {
+  Tally<VIR> T;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ngroups; g += gridDim.x * blockDim.x) {
+    const int t0 = gs[g], t1 = gs[g + 1];
+    const int i = int(ijkl[4 * t0]), j = int(ijkl[4 * t0 + 1]), k = int(ijkl[4 * t0 + 2]), l = int(ijkl[4 * t0 + 3]);
+    R b1x, b1y, b1z, b2x, b2y, b2z, b3x, b3y, b3z;
+    sep(A, i, j, b1x, b1y, b1z);
+    sep(A, j, k, b2x, b2y, b2z);
+    sep(A, k, l, b3x, b3y, b3z);
+    const R mx = b1y * b2z - b1z * b2y, my = b1z * b2x - b1x * b2z, mz = b1x * b2y - b1y * b2x;
+    const R nx = b2y * b3z - b2z * b3y, ny = b2z * b3x - b2x * b3z, nz = b2x * b3y - b2y * b3x;
+    const R m2 = mx * mx + my * my + mz * mz, n2 = nx * nx + ny * ny + nz * nz;
+    const R lb2 = rsq(b2x * b2x + b2y * b2y + b2z * b2z);
+    if (m2 < R(1e-12) || n2 < R(1e-12) || lb2 < R(1e-9)) continue;
+    const R xc = mx * nx + my * ny + mz * nz, yc = lb2 * (b1x * nx + b1y * ny + b1z * nz);
+    const R rc_ = rsq(xc * xc + yc * yc);
+    const R c1 = xc / rc_, s1 = yc / rc_;
+    R dEdphi = 0, e = 0;
+    for (int t = t0; t < t1; ++t) {
+      const int n = nn[t];
+      R cn = 1, sn = 0;
+      if (n >= 0 && n <= 12) {
+        for (int r = 0; r < n; ++r) {
+          const R c = cn * c1 - sn * s1;
+          sn = sn * c1 + cn * s1;
+          cn = c;
+        }
+      } else {
+        const R phi = atan2(yc, xc);
+        cn = cos(R(n) * phi), sn = sin(R(n) * phi);
+      }
+      const double delta = vd[2 * t + 1];
+      R cd = 1, sd = 0;
+      if (delta != 0) {
+        if (fabs(delta - kPi) < 1e-12) cd = -1;
+        else cd = R(cos(delta)), sd = R(sin(delta));
+      }
+      const R v = R(vd[2 * t]);
+      e += v * (1 + cn * cd + sn * sd);
+      dEdphi -= v * R(n) * (sn * cd - cn * sd);
+    }
+    if (ENER) T.e += double(e);
+    const R g1x = mx * (-lb2 / m2), g1y = my * (-lb2 / m2), g1z = mz * (-lb2 / m2);
+    const R g4x = nx * (lb2 / n2), g4y = ny * (lb2 / n2), g4z = nz * (lb2 / n2);
+    const R p = (b1x * b2x + b1y * b2y + b1z * b2z) / (lb2 * lb2), qd = (b3x * b2x + b3y * b2y + b3z * b2z) / (lb2 * lb2);
+    const R g2x = g4x * qd - g1x * (1 + p), g2y = g4y * qd - g1y * (1 + p), g2z = g4z * qd - g1z * (1 + p);
+    const R g3x = g1x * p - g4x * (1 + qd), g3y = g1y * p - g4y * (1 + qd), g3z = g1z * p - g4z * (1 + qd);
+    const R s = -dEdphi;
+    F.add(i, g1x * s, g1y * s, g1z * s);
+    F.add(j, g2x * s, g2y * s, g2z * s);
+    F.add(k, g3x * s, g3y * s, g3z * s);
+    F.add(l, g4x * s, g4y * s, g4z * s);
+    T.vir(b1x, b1y, b1z, g2x * s, g2y * s, g2z * s);
+    T.vir(b1x + b2x, b1y + b2y, b1z + b2z, g3x * s, g3y * s, g3z * s);
+    T.vir(b1x + b2x + b3x, b1y + b2y + b3y, b1z + b2z + b3z, g4x * s, g4y * s, g4z * s);
+  }
+  T.flush(A, slot, ENER);
+}
+
+// 1-4 pairs: LJ times the 1-4 scale (and the same cut-off shift as the pairs), at the nearest image (field.cpp:2019-2043).
+// lj: per type pair (eps, sigma^6, energy shift of 4 eps (q_c^2 - q_c) or 0, 0); capped: (rcap^2, ecap, fcap, 0).
+template <class R, bool ENER, bool VIR>
+static __global__ void k_pairs14(int np, const uint32_t* __restrict__ ij, const double* __restrict__ scale, double lj14, const int* __restrict__ type, int nt,
+                          const double4* __restrict__ lj, const double4* __restrict__ cap, BondedArgs A, ForceSink<R> F) {
+  Tally<VIR> T;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < np; t += gridDim.x * blockDim.x) {
+    const int i = int(ij[2 * t]), j = int(ij[2 * t + 1]);
+    R dx, dy, dz;
+    sep(A, i, j, dx, dy, dz);
+    const double4 c = lj[type[i] * nt + type[j]];
+    if (c.x <= 0) continue;
+    const R sc = R(scale ? scale[t] : lj14);
+    const R r2 = dx * dx + dy * dy + dz * dz;
+    R fr, ev;
+    if (cap && r2 < R(cap[type[i] * nt + type[j]].x)) {
+      const double4 cp = cap[type[i] * nt + type[j]];
+      const R r = rsq(r2), rcp = rsq(R(cp.x));
+      ev = sc * (R(cp.y) + R(cp.z) * (rcp - r));
+      fr = sc * R(cp.z) / r;
+    } else {
+      const R q = R(c.y) / (r2 * r2 * r2);
+      ev = sc * 4 * R(c.x) * (q * q - q);
+      fr = sc * 24 * R(c.x) * (2 * q * q - q) / r2;
+    }
+    if (ENER) T.e += double(ev - sc * R(c.z));
+    const R fx = dx * fr, fy = dy * fr, fz = dz * fr;
+    F.add(j, fx, fy, fz);
+    F.add(i, -fx, -fy, -fz);
+    T.vir(dx, dy, dz, fx, fy, fz);
+  }
+  T.flush(A, kEVdw, ENER);
+}
+
+// Coulomb of excluded pairs (1-2, 1-3 factor 0; 1-4 the Coulomb fraction they keep): the damped / Ewald real-space sum
+// includes them and the bare 1/r is removed in proportion (1 - factor) (field.cpp:2206-2266). FP64: the reference's
+// branches (the Hermite table inside the cut-off, its erf form below 0.5 Å, Abramowitz-Stegun erfc beyond the cut-off
+// under PME). FP32: E = qq (f/r - erf(kr)/r) in closed form (no cancellation), the same terms beyond.
+struct ExclArgs {
+  const uint32_t* ij;
+  const float* factor;
+  const double* q;
+  const double* gtab;
+  double ghi, rc, rc2, kappa, dsf_e0, dsf_f0;
+  int pme;
+};
+
+__device__ __forceinline__ double erfc_as(double x, double& ex2) {   // Abramowitz & Stegun 7.1.26, as field.cpp:585-591
+  const double P = 0.3275911, A1 = 0.254829592, A2 = -0.284496736, A3 = 1.421413741, A4 = -1.453152027, A5 = 1.061405429;
+  ex2 = exp(-x * x);
+  const double t = 1.0 / (1.0 + P * x);
+  return t * (A1 + t * (A2 + t * (A3 + t * (A4 + t * A5)))) * ex2;
+}
+
+template <bool ENER, bool VIR>
+static __global__ void k_excl_f64(int nx, ExclArgs E, BondedArgs A, ForceSink<double> F) {
+  Tally<VIR> T;
+  const double sp = 2 / sqrt(kPi), kap = E.kappa;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nx; t += gridDim.x * blockDim.x) {
+    const int i = int(E.ij[2 * t]), j = int(E.ij[2 * t + 1]);
+    if (E.q[i] == 0 || E.q[j] == 0) continue;
+    double dx, dy, dz;
+    sep(A, i, j, dx, dy, dz);
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    if (r2 >= E.rc2 && !E.pme) continue;
+    const double r = sqrt(r2), qq = kCoulomb * E.q[i] * E.q[j], f = double(E.factor[t]);
+    double e, fr;
+    if (r < 0.5) {
+      const double xk = kap * r;
+      const double g = r > 1e-8 ? erf(xk) / r : sp * kap;
+      const double gr = r > 1e-4 ? (sp * kap * exp(-xk * xk) * r - erf(xk)) / (r2 * r) : -2 * sp * kap * kap * kap / 3;
+      const double shift = E.pme ? 0.0 : -E.dsf_e0 + E.dsf_f0 * (r - E.rc);
+      const double inv = r > 1e-8 ? 1 / r : 0.0;
+      e = qq * (-g + f * inv + shift);
+      fr = qq * (gr + f * inv * inv * inv - (E.pme ? 0.0 : E.dsf_f0) * inv);
+    } else if (r2 < E.rc2) {
+      const double u = r2 * E.ghi;
+      const int k = int(u);
+      const double tt = u - k, t2 = tt * tt;
+      const double* g = E.gtab + 2 * k;
+      const double G = g[0] + t2 * (3 - 2 * tt) * (g[2] - g[0]) + tt * (1 - tt) * ((1 - tt) * g[1] - tt * g[3]);
+      const double dG = (6 * tt * (1 - tt) * (g[2] - g[0]) * E.ghi) + (1 - tt) * (1 - 3 * tt) * g[1] * E.ghi + tt * (3 * tt - 2) * g[3] * E.ghi;
+      const double rinv = 1 / r, Ee = rinv - G, Fc = rinv * rinv * rinv + 2 * dG;
+      if (E.pme) {
+        e = qq * Ee - (1 - f) * qq / r;
+        fr = qq * (Fc - (1 - f) / (r2 * r));
+      } else {
+        e = qq * (Ee - E.dsf_e0 + E.dsf_f0 * (r - E.rc)) - (1 - f) * qq / r;
+        fr = qq * (Fc - E.dsf_f0 / r - (1 - f) / (r2 * r));
+      }
+    } else {
+      double ex2;
+      const double er = erfc_as(kap * r, ex2);
+      e = qq * er / r - (1 - f) * qq / r;
+      fr = qq * ((er / r2 + sp * kap * ex2 / r) - (1 - f) / r2) / r;
+    }
+    if (ENER) T.e += e;
+    const double fx = dx * fr, fy = dy * fr, fz = dz * fr;
+    F.add(j, fx, fy, fz);
+    F.add(i, -fx, -fy, -fz);
+    T.vir(dx, dy, dz, fx, fy, fz);
+  }
+  T.flush(A, kECoul, ENER);
+}
+
+template <bool ENER, bool VIR>
+static __global__ void k_excl_f32(int nx, ExclArgs E, BondedArgs A, ForceSink<float> F) {
+  Tally<VIR> T;
+  const float kap = float(E.kappa), kc = float(2 * E.kappa / sqrt(kPi)), rcf = float(E.rc), e0 = float(E.dsf_e0), f0 = float(E.dsf_f0);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nx; t += gridDim.x * blockDim.x) {
+    const int i = int(E.ij[2 * t]), j = int(E.ij[2 * t + 1]);
+    if (E.q[i] == 0 || E.q[j] == 0) continue;
+    float dx, dy, dz;
+    sep(A, i, j, dx, dy, dz);
+    const float r2 = dx * dx + dy * dy + dz * dz;
+    if (r2 >= float(E.rc2) && !E.pme) continue;
+    if (r2 <= 0.f) continue;
+    const float qq = float(kCoulomb * E.q[i] * E.q[j]), f = E.factor[t];
+    const float rinv = rsqrtf(r2), r = r2 * rinv, r2i = rinv * rinv;
+    // erf(kr)/r and its derivative term, direct: E = qq (f/r - erf/r), -(dE/dr)/r = qq (f/r^3 + kc e^-k2r2 / r^2 - erf / r^3)
+    const float erfv = erff(kap * r), ex = __expf(-kap * kap * r2);
+    float e = qq * (f * rinv - erfv * rinv);
+    float fr = qq * (f * rinv * r2i + kc * ex * r2i - erfv * rinv * r2i);
+    if (!E.pme) {
+      e += qq * (f0 * (r - rcf) - e0);
+      fr -= qq * f0 * rinv;
+    }
+    if (ENER) T.e += double(e);
+    const float fx = dx * fr, fy = dy * fr, fz = dz * fr;
+    F.add(j, fx, fy, fz);
+    F.add(i, -fx, -fy, -fz);
+    T.vir(dx, dy, dz, fx, fy, fz);
+  }
+  T.flush(A, kECoul, ENER);
+}
+
+// FENE (-1/2 K R0^2 ln(1 - (r/R0)^2)) plus WCA below 2^(1/6) sigma (LAMMPS bond fene; field.cpp:2152-2166). A bond
+// stretched to R0 or past raises kErrFene (the reference throws FieldError there).
+template <class R, bool ENER, bool VIR>
+static __global__ void k_fene(int nf, const uint32_t* __restrict__ ij, const double* __restrict__ p, BondedArgs A, ForceSink<R> F, int* counters) {
+  Tally<VIR> T;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nf; t += gridDim.x * blockDim.x) {
+    const int i = int(ij[2 * t]), j = int(ij[2 * t + 1]);
+    R dx, dy, dz;
+    sep(A, i, j, dx, dy, dz);
+    const R K = R(p[4 * t]), R0 = R(p[4 * t + 1]), eps = R(p[4 * t + 2]), sg = R(p[4 * t + 3]);
+    const R r = rsq(dx * dx + dy * dy + dz * dz);
+    const R q = r / R0;
+    if (!(q < R(1))) {
+      atomicOr(reinterpret_cast<unsigned*>(counters + 3), kErrFene);
+      continue;
+    }
+    R e = -R(0.5) * K * R0 * R0 * log(R(1) - q * q);
+    R dEdr = K * r / (R(1) - q * q);
+    if (eps > 0 && r < R(1.122462048309373) * sg) {
+      const R s2 = sg * sg / (r * r), s6 = s2 * s2 * s2;
+      e += 4 * eps * (s6 * s6 - s6) + eps;
+      dEdr += -24 * eps * (2 * s6 * s6 - s6) / r;
+    }
+    if (ENER) T.e += double(e);
+    const R s = r > R(1e-12) ? -dEdr / r : R(0);
+    const R fx = dx * s, fy = dy * s, fz = dz * s;
+    F.add(j, fx, fy, fz);
+    F.add(i, -fx, -fy, -fz);
+    T.vir(dx, dy, dz, fx, fy, fz);
+  }
+  T.flush(A, kEBond, ENER);
+}
+
+}  // namespace capsb

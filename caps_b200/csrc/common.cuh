@@ -1,0 +1,171 @@
+// Shared device helpers for the B200 MD engine: cell algebra, fixed-point accumulation, warp reductions, error words.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace capsb {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kCoulomb = 332.06371;   // kcal*Å/(mol*e^2), as the reference (core/src/field.cpp:29)
+
+// Fixed-point scales. Forces and energies: 2^32 units per kcal/mol/Å (or per kcal/mol): resolution 2.3e-10, range
+// +-2.1e9. PME grid charges: 2^40 per e (resolution 9e-13 e). Integer sums are exact, so every reduction that goes
+// through these is independent of the order the GPU runs it in: bit-reproducible forces and energies.
+constexpr double kFixF = 4294967296.0;
+constexpr double kInvFixF = 1.0 / 4294967296.0;
+constexpr double kFixQ = 1099511627776.0;
+constexpr double kInvFixQ = 1.0 / 1099511627776.0;
+
+// Error bits raised by kernels (never a trap): the host reads the word and throws the reference's message.
+enum ErrorBits : unsigned {
+  kErrListOverflow = 1u << 0,     // cluster-pair entries past capacity
+  kErrExclOverflow = 1u << 1,     // exclusion records of a super-cluster past the per-warp table
+  kErrColumnTooBig = 1u << 2,     // a grid column holds more atoms than the column sort takes
+  kErrScOverflow = 1u << 3,       // more super-clusters than allocated
+  kErrFene = 1u << 4,             // a FENE bond stretched past R0
+  kErrShake = 1u << 5,            // SHAKE / RATTLE did not converge
+  kErrShakeTurn = 1u << 6,        // a constrained bond turned past 90 degrees
+  kErrNonFinite = 1u << 7,        // a coordinate became NaN / inf
+  kErrMaskOverflow = 1u << 8,     // exclusion masks past capacity
+  kErrImageRange = 1u << 9,       // an image shift outside +-63 cells
+};
+
+// Periodic cell: origin o, edge vectors a, b, c (columns of h) and h^-1 (rows: reciprocal vectors without 2 pi).
+struct DevCell {
+  double o[3];
+  double h[3][3];    // h[r][c]: component r of edge vector c
+  double hi[3][3];   // inverse
+  double vol;
+};
+
+__host__ __device__ inline void frac_of(const DevCell& c, const double x[3], double f[3]) {
+  const double d0 = x[0] - c.o[0], d1 = x[1] - c.o[1], d2 = x[2] - c.o[2];
+  for (int r = 0; r < 3; ++r) f[r] = c.hi[r][0] * d0 + c.hi[r][1] * d1 + c.hi[r][2] * d2;
+}
+
+// Separation d brought to its nearest periodic image (fractional rounding; bonded partners sit well inside half a cell).
+template <class R>
+__device__ __forceinline__ void min_image(const DevCell& c, R& dx, R& dy, R& dz) {
+  double f[3];
+  for (int r = 0; r < 3; ++r) {
+    f[r] = c.hi[r][0] * double(dx) + c.hi[r][1] * double(dy) + c.hi[r][2] * double(dz);
+    f[r] -= rint(f[r]);
+  }
+  dx = R(c.h[0][0] * f[0] + c.h[0][1] * f[1] + c.h[0][2] * f[2]);
+  dy = R(c.h[1][0] * f[0] + c.h[1][1] * f[1] + c.h[1][2] * f[2]);
+  dz = R(c.h[2][0] * f[0] + c.h[2][1] * f[1] + c.h[2][2] * f[2]);
+}
+
+__device__ __forceinline__ long long to_fix(double v, double scale) { return __double2ll_rn(v * scale); }
+__device__ __forceinline__ long long to_fixf(float v) { return __float2ll_rn(v * 4294967296.0f); }
+
+__device__ __forceinline__ void atomic_add_fix(long long* p, long long v) {
+  atomicAdd(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(v));
+}
+
+// Force accumulation into either fixed-point (mixed precision) or double (FP64) SoA arrays.
+template <class R> struct ForceSink;
+template <> struct ForceSink<float> {
+  long long* fx;
+  long long* fy;
+  long long* fz;
+  __device__ __forceinline__ void add(int i, float x, float y, float z) const {
+    atomic_add_fix(fx + i, to_fixf(x));
+    atomic_add_fix(fy + i, to_fixf(y));
+    atomic_add_fix(fz + i, to_fixf(z));
+  }
+  __device__ __forceinline__ void add1(int comp, int i, float v) const {
+    long long* p = comp == 0 ? fx : comp == 1 ? fy : fz;
+    atomic_add_fix(p + i, to_fixf(v));
+  }
+};
+template <> struct ForceSink<double> {
+  double* fx;
+  double* fy;
+  double* fz;
+  __device__ __forceinline__ void add(int i, double x, double y, double z) const {
+    atomicAdd(fx + i, x);
+    atomicAdd(fy + i, y);
+    atomicAdd(fz + i, z);
+  }
+  __device__ __forceinline__ void add1(int comp, int i, double v) const {
+    double* p = comp == 0 ? fx : comp == 1 ? fy : fz;
+    atomicAdd(p + i, v);
+  }
+};
+
+// Energy / virial accumulators: index into a small array; fixed point for the mixed path (deterministic), double for
+// the FP64 path.
+enum EnergySlot { kEBond = 0, kEAngle, kEDihedral, kEImproper, kEVdw, kECoul, kEW0, kEW1, kEW2, kEW3, kEW4, kEW5, kEPmeRecip, kEKin,
+                  kENumSlots = 16 };
+
+struct EnergySink {
+  long long* fix;    // [kENumSlots] mixed path
+  double* dbl;       // [kENumSlots] FP64 path
+  __device__ __forceinline__ void add(int slot, double v, bool fixed) const {
+    if (fixed) atomic_add_fix(fix + slot, to_fix(v, kFixF));
+    else atomicAdd(dbl + slot, v);
+  }
+};
+
+template <class T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-wide sum (any blockDim that is a multiple of 32, up to 1024); result valid in thread 0.
+template <class T>
+__device__ T block_sum(T v, T* scratch /* >= 32 */) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) scratch[w] = v;
+  __syncthreads();
+  T s = 0;
+  if (w == 0) {
+    s = lane < int(blockDim.x >> 5) ? scratch[lane] : T(0);
+    s = warp_sum(s);
+  }
+  return s;
+}
+
+// Philox4x32-10 (Salmon, Moraes, Dror & Shaw, SC'11): counter-based random numbers, so every atom's noise at every
+// step is a pure function of (seed, step, atom) whatever the launch shape.
+struct Philox {
+  __device__ __forceinline__ static void round(uint32_t& c0, uint32_t& c1, uint32_t& c2, uint32_t& c3, uint32_t k0, uint32_t k1) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+    const uint32_t hi0 = __umulhi(M0, c0), lo0 = M0 * c0;
+    const uint32_t hi1 = __umulhi(M1, c2), lo1 = M1 * c2;
+    const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+    c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+  }
+  __device__ static uint4 gen(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1) {
+    const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+      round(c0, c1, c2, c3, k0, k1);
+      k0 += W0;
+      k1 += W1;
+    }
+    return make_uint4(c0, c1, c2, c3);
+  }
+};
+
+// Four standard normals from one Philox block (Box-Muller on 24-bit uniforms in (0, 1]).
+__device__ inline void normals4(uint64_t seed, uint64_t step, uint32_t idx, uint32_t stream, double out[4]) {
+  const uint4 r = Philox::gen(idx, stream, uint32_t(step), uint32_t(step >> 32), uint32_t(seed), uint32_t(seed >> 32));
+  const double s = 1.0 / 4294967296.0;
+  const double u0 = (double(r.x) + 1.0) * s, u1 = (double(r.y) + 0.5) * s, u2 = (double(r.z) + 1.0) * s, u3 = (double(r.w) + 0.5) * s;
+  const double ra = sqrt(-2.0 * log(u0)), rb = sqrt(-2.0 * log(u2));
+  double sa, ca, sb, cb;
+  sincospi(2.0 * u1, &sa, &ca);
+  sincospi(2.0 * u3, &sb, &cb);
+  out[0] = ra * ca;
+  out[1] = ra * sa;
+  out[2] = rb * cb;
+  out[3] = rb * sb;
+}
+
+}  // namespace capsb

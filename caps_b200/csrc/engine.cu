@@ -1,0 +1,996 @@
+// Host side of the device engine: the C ABI of include/caps_gpu.h, force-field upload, cell and list geometry, and the
+// kernel sequence of one force evaluation (Evaluator::compute, core/src/field.cpp:1249-2539).
+#include "engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "bonded.cuh"
+#include "pair.cuh"
+
+namespace capsb {
+
+// ---------------------------------------------------------------------------------------------------------------
+#define CK(call)                                                                                         \
+  do {                                                                                                   \
+    cudaError_t e_ = (call);                                                                             \
+    if (e_ != cudaSuccess) throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_));          \
+  } while (0)
+
+namespace {
+
+// Ewald coefficient by bisection of erfc(beta rc) = rtol (core/src/kspace.cpp:35-43).
+double ewald_beta(double cutoff, double rtol) {
+  double lo = 0, hi = 20.0 / cutoff;
+  for (int it = 0; it < 100; ++it) {
+    const double mid = 0.5 * (lo + hi);
+    (std::erfc(mid * cutoff) > rtol ? lo : hi) = mid;
+  }
+  return 0.5 * (lo + hi);
+}
+
+// smallest n' >= n with prime factors 2, 3, 5, 7 (caps_kspace.f90:23-36)
+int good_size(int n) {
+  int m = std::max(n, 1);
+  for (;;) {
+    int k = m;
+    while (k % 2 == 0) k /= 2;
+    while (k % 3 == 0) k /= 3;
+    while (k % 5 == 0) k /= 5;
+    while (k % 7 == 0) k /= 7;
+    if (k == 1) return m;
+    ++m;
+  }
+}
+
+double erfc_as_host(double x, double& ex2) {   // Abramowitz & Stegun 7.1.26 (field.cpp:585-591), used for the DSF constants
+  const double P = 0.3275911, A1 = 0.254829592, A2 = -0.284496736, A3 = 1.421413741, A4 = -1.453152027, A5 = 1.061405429;
+  ex2 = std::exp(-x * x);
+  const double t = 1.0 / (1.0 + P * x);
+  return t * (A1 + t * (A2 + t * (A3 + t * (A4 + t * A5)))) * ex2;
+}
+
+// |b(m)|^2 of the Euler exponential spline (caps_kspace.f90:601-620), from the order-p weights at w = 0
+void bspline_moduli(int k, int p, std::vector<double>& bsp) {
+  std::vector<double> th(size_t(p), 0.0);
+  // bspline(0, p): the recursion of caps_kspace.f90:568-598 at w = 0
+  const double w = 0;
+  th[1] = w;
+  th[0] = 1 - w;
+  for (int kk = 3; kk <= p - 1; ++kk) {
+    const double div = 1.0 / (kk - 1);
+    th[size_t(kk - 1)] = div * w * th[size_t(kk - 2)];
+    for (int j = 1; j <= kk - 2; ++j) th[size_t(kk - j - 1)] = div * ((w + j) * th[size_t(kk - j - 2)] + (kk - j - w) * th[size_t(kk - j - 1)]);
+    th[0] = div * (1 - w) * th[0];
+  }
+  {
+    const double div = 1.0 / (p - 1);
+    th[size_t(p - 1)] = div * w * th[size_t(p - 2)];
+    for (int j = 1; j <= p - 2; ++j) th[size_t(p - j - 1)] = div * ((w + j) * th[size_t(p - j - 2)] + (p - j - w) * th[size_t(p - j - 1)]);
+    th[0] = div * (1 - w) * th[0];
+  }
+  bsp.assign(size_t(k), 0.0);
+  for (int m = 0; m < k; ++m) {
+    double sr = 0, si = 0;
+    for (int j = 0; j <= p - 2; ++j) {
+      const double arg = 2 * kPi * m * j / double(k);
+      sr += th[size_t(j)] * std::cos(arg);
+      si += th[size_t(j)] * std::sin(arg);
+    }
+    bsp[size_t(m)] = sr * sr + si * si;
+  }
+  for (int m = 0; m < k; ++m)
+    if (bsp[size_t(m)] < 1e-7) bsp[size_t(m)] = 0.5 * (bsp[size_t(((m - 1) % k + k) % k)] + bsp[size_t((m + 1) % k)]);
+}
+
+__global__ void k_set_flag(int* counters, int slot, int v) { counters[slot] = v; }
+
+// Forces to the caller's AoS doubles: atom-order sums plus the pair kernel's slot-order sums.
+__global__ void k_reduce_f32(int n, const long long* __restrict__ F, const long long* __restrict__ Fs, int nslots, const int* __restrict__ iperm,
+                             double* __restrict__ f, int with_pairs) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int s = with_pairs ? iperm[i] : -1;
+  const bool ok = s >= 0 && s < nslots;   // a build that overflowed can leave iperm stale: the host reports it
+  for (int k = 0; k < 3; ++k) {
+    long long v = F[size_t(k) * n + i];
+    if (ok) v += Fs[size_t(k) * nslots + s];
+    f[3 * i + k] = double(v) * kInvFixF;
+  }
+}
+__global__ void k_reduce_f64(int n, const double* __restrict__ F, const double* __restrict__ Fs, int nslots, const int* __restrict__ iperm,
+                             double* __restrict__ f, int with_pairs) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int s = with_pairs ? iperm[i] : -1;
+  const bool ok = s >= 0 && s < nslots;
+  for (int k = 0; k < 3; ++k) {
+    double v = F[size_t(k) * n + i];
+    if (ok) v += Fs[size_t(k) * nslots + s];
+    f[3 * i + k] = v;
+  }
+}
+
+int blocks_for(size_t n, int threads) { return int(std::max<size_t>(1, (n + size_t(threads) - 1) / size_t(threads))); }
+
+void cell_matrices(const double* c, DevCell& d) {
+  for (int k = 0; k < 3; ++k) d.o[k] = c[k];
+  for (int r = 0; r < 3; ++r)
+    for (int col = 0; col < 3; ++col) d.h[r][col] = c[3 + 3 * col + r];
+  const auto& h = d.h;
+  // the inverse as caps_kspace.f90:495-511 (cell_inverse) writes it
+  const double vol = h[0][0] * (h[1][1] * h[2][2] - h[2][1] * h[1][2]) - h[0][1] * (h[1][0] * h[2][2] - h[2][0] * h[1][2]) +
+                     h[0][2] * (h[1][0] * h[2][1] - h[2][0] * h[1][1]);
+  d.hi[0][0] = (h[1][1] * h[2][2] - h[1][2] * h[2][1]) / vol;
+  d.hi[0][1] = (h[0][2] * h[2][1] - h[0][1] * h[2][2]) / vol;
+  d.hi[0][2] = (h[0][1] * h[1][2] - h[0][2] * h[1][1]) / vol;
+  d.hi[1][0] = (h[1][2] * h[2][0] - h[1][0] * h[2][2]) / vol;
+  d.hi[1][1] = (h[0][0] * h[2][2] - h[0][2] * h[2][0]) / vol;
+  d.hi[1][2] = (h[0][2] * h[1][0] - h[0][0] * h[1][2]) / vol;
+  d.hi[2][0] = (h[1][0] * h[2][1] - h[1][1] * h[2][0]) / vol;
+  d.hi[2][1] = (h[0][1] * h[2][0] - h[0][0] * h[2][1]) / vol;
+  d.hi[2][2] = (h[0][0] * h[1][1] - h[0][1] * h[1][0]) / vol;
+  d.vol = std::fabs(vol);
+}
+
+double norm3(const double* v) { return std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]); }
+void cross3(const double* a, const double* b, double* o) {
+  o[0] = a[1] * b[2] - a[2] * b[1];
+  o[1] = a[2] * b[0] - a[0] * b[2];
+  o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// radices of n for the line FFT: 4s first, then 2, 3, 5, 7 and any other prime
+void factor_radices(int n, int* rad, int& nst) {
+  nst = 0;
+  int r = n;
+  while (r % 4 == 0 && nst < kMaxRadices) rad[nst++] = 4, r /= 4;
+  for (int p : {2, 3, 5, 7}) while (r % p == 0 && nst < kMaxRadices) rad[nst++] = p, r /= p;
+  for (int p = 11; r > 1 && p <= kMaxRadices && nst < kMaxRadices; p += 2)
+    while (r % p == 0 && nst < kMaxRadices) rad[nst++] = p, r /= p;
+  if (r != 1) throw ModelError(CAPS_GPU_EINVAL, "PME grid length " + std::to_string(n) + " cannot be factored for the line FFT");
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------------------------
+Engine::Engine(const caps_gpu_ff* ff, const caps_gpu_opts* o) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    throw ModelError(CAPS_GPU_ENODEV, "no CUDA device: the B200 engine has no CPU fallback");
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&dev_sms_, cudaDevAttrMultiProcessorCount, dev));
+  CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  CK(cudaMallocHost(&h_counters_, sizeof(int) * kCntNum));
+  CK(cudaMallocHost(&h_efix_, sizeof(long long) * kENumSlots));
+  CK(cudaMallocHost(&h_edbl_, sizeof(double) * kENumSlots));
+  opt_ = *o;
+  setup_ff(ff);
+  setup_options();
+}
+
+Engine::~Engine() {
+  if (stream_) cudaStreamSynchronize(stream_);
+  if (h_counters_) cudaFreeHost(h_counters_);
+  if (h_efix_) cudaFreeHost(h_efix_);
+  if (h_edbl_) cudaFreeHost(h_edbl_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Engine::setup_ff(const caps_gpu_ff* ff) {
+  n_ = ff->natoms;
+  nt_ = ff->ntypes;
+  if (n_ < 1 || nt_ < 1) throw ModelError(CAPS_GPU_EINVAL, "the force field needs atoms and types");
+  if (nt_ > 63) throw ModelError(CAPS_GPU_EINVAL, "at most 63 atom types on the device path");
+  h_type_.assign(ff->type_index, ff->type_index + n_);
+  for (int t : h_type_)
+    if (t < 0 || t >= nt_) throw ModelError(CAPS_GPU_EINVAL, "type index out of range");
+  h_q_.assign(ff->charge, ff->charge + n_);
+  h_mass_.assign(ff->mass, ff->mass + n_);
+  h_eps_.assign(ff->pair_eps, ff->pair_eps + size_t(nt_) * nt_);
+  h_sig_.assign(ff->pair_sigma, ff->pair_sigma + size_t(nt_) * nt_);
+  type_count_.assign(size_t(nt_), 0.0);
+  for (int t : h_type_) type_count_[size_t(t)] += 1;
+  d_type_.upload(h_type_, stream_);
+  d_q_.upload(h_q_, stream_);
+  d_mass_.upload(h_mass_, stream_);
+  auto check_idx = [&](const uint32_t* v, size_t cnt, const char* what) {
+    for (size_t k = 0; k < cnt; ++k)
+      if (v[k] >= uint32_t(n_)) throw ModelError(CAPS_GPU_EINVAL, std::string(what) + ": atom index out of range");
+  };
+  hb_.clear();
+  hr0_.clear();
+  ha_.clear();
+  hth0_.clear();
+  for (int k = 0; k < ff->nbonds; ++k) hb_.push_back({ff->bond_ij[2 * k], ff->bond_ij[2 * k + 1]}), hr0_.push_back(ff->bond_k_r0[2 * k + 1]);
+  for (int k = 0; k < ff->nfene; ++k) hb_.push_back({ff->fene_ij[2 * k], ff->fene_ij[2 * k + 1]}), hr0_.push_back(0.0);
+  for (int k = 0; k < ff->nangles; ++k)
+    ha_.push_back({ff->angle_ijk[3 * k], ff->angle_ijk[3 * k + 1], ff->angle_ijk[3 * k + 2]}), hth0_.push_back(ff->angle_kt_theta0[2 * k + 1]);
+  nb_ = ff->nbonds;
+  if (nb_) {
+    check_idx(ff->bond_ij, size_t(2) * nb_, "bonds");
+    d_bond_ij_.upload(ff->bond_ij, size_t(2) * nb_, stream_);
+    d_bond_kr_.upload(ff->bond_k_r0, size_t(2) * nb_, stream_);
+  }
+  na_ = ff->nangles;
+  if (na_) {
+    check_idx(ff->angle_ijk, size_t(3) * na_, "angles");
+    d_angle_ijk_.upload(ff->angle_ijk, size_t(3) * na_, stream_);
+    d_angle_kt_.upload(ff->angle_kt_theta0, size_t(2) * na_, stream_);
+  }
+  // torsion groups: consecutive terms on one quadruple (field.cpp:1875-1920)
+  auto groups = [](int cnt, const uint32_t* q, std::vector<int>& g) {
+    g.clear();
+    for (int t = 0; t < cnt; ++t) {
+      if (t == 0 || q[4 * t] != q[4 * (t - 1)] || q[4 * t + 1] != q[4 * (t - 1) + 1] || q[4 * t + 2] != q[4 * (t - 1) + 2] ||
+          q[4 * t + 3] != q[4 * (t - 1) + 3])
+        g.push_back(t);
+    }
+    g.push_back(cnt);
+  };
+  std::vector<int> grp;
+  nd_ = ff->ndihedrals;
+  if (nd_) {
+    check_idx(ff->dihedral_ijkl, size_t(4) * nd_, "dihedrals");
+    d_dih_ijkl_.upload(ff->dihedral_ijkl, size_t(4) * nd_, stream_);
+    d_dih_vd_.upload(ff->dihedral_v_delta, size_t(2) * nd_, stream_);
+    d_dih_n_.upload(ff->dihedral_n, size_t(nd_), stream_);
+    groups(nd_, ff->dihedral_ijkl, grp);
+    ndg_ = int(grp.size()) - 1;
+    d_dih_grp_.upload(grp, stream_);
+    CK(cudaStreamSynchronize(stream_));
+  }
+  ni_ = ff->nimpropers;
+  if (ni_) {
+    check_idx(ff->improper_ijkl, size_t(4) * ni_, "impropers");
+    d_imp_ijkl_.upload(ff->improper_ijkl, size_t(4) * ni_, stream_);
+    d_imp_vd_.upload(ff->improper_v_delta, size_t(2) * ni_, stream_);
+    d_imp_n_.upload(ff->improper_n, size_t(ni_), stream_);
+    groups(ni_, ff->improper_ijkl, grp);
+    nig_ = int(grp.size()) - 1;
+    d_imp_grp_.upload(grp, stream_);
+    CK(cudaStreamSynchronize(stream_));
+  }
+  // 1-4 pairs and the Coulomb fraction each keeps (field.cpp:445-457)
+  np14_ = ff->npairs14;
+  lj14_ = ff->lj14;
+  std::map<std::pair<uint32_t, uint32_t>, double> p14;
+  if (np14_) {
+    check_idx(ff->pair14_ij, size_t(2) * np14_, "pairs14");
+    d_p14_ij_.upload(ff->pair14_ij, size_t(2) * np14_, stream_);
+    p14_scaled_ = ff->pair14_lj != nullptr;
+    if (p14_scaled_) d_p14_scale_.upload(ff->pair14_lj, size_t(np14_), stream_);
+    for (int k = 0; k < np14_; ++k) {
+      const uint32_t a = ff->pair14_ij[2 * k], b = ff->pair14_ij[2 * k + 1];
+      p14[{std::min(a, b), std::max(a, b)}] = ff->pair14_coul ? ff->pair14_coul[k] : ff->coul14;
+    }
+  }
+  // excluded partners: the CSR for the list, and (i < j, factor) pairs for the Coulomb corrections
+  std::vector<uint32_t> eoff(size_t(n_) + 1, 0), elist, xij;
+  std::vector<float> xf;
+  for (int i = 0; i < n_; ++i) {
+    const uint32_t b0 = ff->excl_offset ? ff->excl_offset[i] : 0, b1 = ff->excl_offset ? ff->excl_offset[i + 1] : 0;
+    for (uint32_t p = b0; p < b1; ++p) {
+      const uint32_t j = ff->excl_list[p];
+      if (j >= uint32_t(n_)) throw ModelError(CAPS_GPU_EINVAL, "excluded: atom index out of range");
+      if (j == uint32_t(i)) continue;
+      elist.push_back(j);
+      if (j > uint32_t(i)) {
+        const auto it = p14.find({uint32_t(i), j});
+        xij.push_back(uint32_t(i));
+        xij.push_back(j);
+        xf.push_back(float(it != p14.end() ? it->second : 0.0));
+      }
+    }
+    eoff[size_t(i) + 1] = uint32_t(elist.size());
+  }
+  d_excl_off_.upload(eoff, stream_);
+  d_excl_list_.upload(elist, stream_);
+  nx_ = int(xf.size());
+  if (nx_) {
+    d_excl_ij_.upload(xij, stream_);
+    d_excl_f_.upload(xf, stream_);
+  }
+  nfene_ = ff->nfene;
+  if (nfene_) {
+    check_idx(ff->fene_ij, size_t(2) * nfene_, "fene");
+    d_fene_ij_.upload(ff->fene_ij, size_t(2) * nfene_, stream_);
+    d_fene_p_.upload(ff->fene_k_r0_eps_sigma, size_t(4) * nfene_, stream_);
+  }
+  lj_shift_model_ = ff->lj_shift != 0;
+  model_cutoff_ = ff->model_cutoff;
+  CK(cudaStreamSynchronize(stream_));
+}
+
+void Engine::setup_options() {
+  rc_ = model_cutoff_ > 0 ? model_cutoff_ : opt_.cutoff;
+  skin_ = opt_.skin;
+  if (!(rc_ > 0) || skin_ < 0) throw ModelError(CAPS_GPU_EINVAL, "cut-off must be positive and skin non-negative");
+  mixed_ = opt_.precision == 0;
+  tail_ = opt_.tail != 0 && !lj_shift_model_;
+  shifted_ = !tail_;
+  coul_ = opt_.coulomb != 0;
+  pme_ = coul_ && opt_.electrostatics == 1;
+  order_ = opt_.pme_order;
+  if (pme_ && (order_ < 3 || order_ > kMaxOrder)) throw ModelError(CAPS_GPU_EINVAL, "PME order must be 3..8");
+  if (opt_.force_cap > 0 && mixed_) throw ModelError(CAPS_GPU_EINVAL, "a force cap runs on the FP64 path (as the reference's push-off)");
+  beta_ = pme_ ? ewald_beta(rc_, opt_.ewald_rtol) : 0.0;
+  const double a = opt_.dsf_alpha;
+  double ex;
+  erfc_rc_ = erfc_as_host(a * rc_, ex);
+  dsf_e0_ = erfc_rc_ / rc_;
+  dsf_f0_ = erfc_rc_ / (rc_ * rc_) + 2 * a / std::sqrt(kPi) * std::exp(-a * a * rc_ * rc_) / rc_;
+  kappa_ = pme_ ? beta_ : a;
+  // Ewald / DSF table G(s) = erf(kappa sqrt s)/sqrt s and h dG/ds (field.cpp:1126-1157)
+  if (coul_) {
+    const double smax = rc_ * rc_, kap = kappa_;
+    const size_t m = std::max<size_t>(1024, size_t(std::ceil(smax * kap * kap / 0.025)));
+    const double h = smax / double(m);
+    const double c = 2 * kap / std::sqrt(kPi), k2 = kap * kap;
+    std::vector<double> gt(2 * (m + 2), 0.0);
+    for (size_t k = 0; k <= m + 1; ++k) {
+      const double s = double(k) * h, x = k2 * s;
+      double G, dG;
+      if (x < 1) {
+        G = 0, dG = 0;
+        double term = 1;
+        for (int nn = 0; nn < 30; ++nn) {
+          G += term / (2 * nn + 1);
+          dG -= term / (2 * nn + 3);
+          term *= -x / (nn + 1);
+        }
+        G *= c;
+        dG *= c * k2;
+      } else {
+        const double r = std::sqrt(s), e = std::erf(kap * r);
+        G = e / r;
+        dG = (c * std::exp(-x) - G) / (2 * s);
+      }
+      gt[2 * k] = G;
+      gt[2 * k + 1] = h * dG;
+    }
+    d_gtab_.upload(gt, stream_);
+    gnodes_ = int(m + 2);
+    ghi_ = 1 / h;
+  }
+  // pair coefficient tables, the padding type last (all zero)
+  const int ntab = nt_ + 1;
+  std::vector<float4> tab(size_t(ntab) * ntab, make_float4(0, 0, 0, 0));
+  std::vector<double4> tabd(size_t(ntab) * ntab, make_double4(0, 0, 0, 0)), l14(size_t(nt_) * nt_);
+  const double rc2 = rc_ * rc_;
+  for (int a0 = 0; a0 < nt_; ++a0)
+    for (int b0 = 0; b0 < nt_; ++b0) {
+      const double eps = h_eps_[size_t(a0) * nt_ + b0], sg = h_sig_[size_t(a0) * nt_ + b0];
+      const double s6 = std::pow(sg, 6);
+      const double c6 = eps > 0 ? 4 * eps * s6 : 0.0, c12 = eps > 0 ? 4 * eps * s6 * s6 : 0.0;
+      const double qc = s6 / (rc2 * rc2 * rc2);
+      const double sh = shifted_ && eps > 0 ? 4 * eps * (qc * qc - qc) : 0.0;
+      tab[size_t(a0) * ntab + b0] = make_float4(float(c6), float(c12), float(sh), 0.f);
+      tabd[size_t(a0) * ntab + b0] = make_double4(c6, c12, sh, 0.0);
+      l14[size_t(a0) * nt_ + b0] = make_double4(eps, s6, sh, 0.0);
+    }
+  d_tab_.upload(tab, stream_);
+  d_tabd_.upload(tabd, stream_);
+  d_lj14_.upload(l14, stream_);
+  list_valid_ = false;
+  green_valid_ = false;
+  if (cell_set_) {
+    double c[12];
+    std::memcpy(c, cell_h_, sizeof c);
+    cell_set_ = false;
+    set_cell(c);
+  }
+  CK(cudaStreamSynchronize(stream_));
+}
+
+void Engine::set_options(const caps_gpu_opts* o) {
+  opt_ = *o;
+  setup_options();
+}
+
+// The cell: matrices, list geometry (columns about as wide as a cubic 64-atom super-cluster, reach in columns and
+// images as nbnxm.cpp:54-57, 154-161) and the PME grid (kspace.cpp:45-51).
+void Engine::set_cell(const double* cell) {
+  if (cell_set_ && std::memcmp(cell, cell_h_, sizeof cell_h_) == 0) return;
+  std::memcpy(cell_h_, cell, sizeof cell_h_);
+  cell_set_ = true;
+  cell_matrices(cell, dcell_);
+  if (!(dcell_.vol > 0) || !std::isfinite(dcell_.vol)) throw ModelError(CAPS_GPU_EINVAL, "the device path needs a periodic cell with a volume");
+  const double* a = cell + 3;
+  const double* b = cell + 6;
+  const double* c = cell + 9;
+  double bc[3], ca[3], ab[3];
+  cross3(b, c, bc);
+  cross3(c, a, ca);
+  cross3(a, b, ab);
+  ListGeom g{};
+  g.w[0] = dcell_.vol / norm3(bc);
+  g.w[1] = dcell_.vol / norm3(ca);
+  g.w[2] = dcell_.vol / norm3(ab);
+  const double side = std::cbrt(64.0 * dcell_.vol / std::max(1, n_));
+  g.nu = std::clamp(int(g.w[0] / side), 1, 1024);
+  g.nv = std::clamp(int(g.w[1] / side), 1, 1024);
+  g.ncol = g.nu * g.nv;
+  g.rlist = rc_ + skin_;
+  g.rlist2 = g.rlist * g.rlist;
+  g.ru = int(std::floor(g.rlist * g.nu / g.w[0])) + 1;
+  g.rv = int(std::floor(g.rlist * g.nv / g.w[1])) + 1;
+  g.rq = int(std::ceil(g.rlist / g.w[2])) + 1;
+  g.dw = g.rlist / g.w[2];
+  if (g.ru / g.nu > 60 || g.rv / g.nv > 60 || g.rq > 60)
+    throw ModelError(CAPS_GPU_EFIELD, "the cell is too small for the cut-off: more than 60 periodic images in range");
+  const bool geom_changed = g.nu != geom_.nu || g.nv != geom_.nv;
+  geom_ = g;
+  if (geom_changed) {
+    d_col_count_.alloc(size_t(g.ncol));
+    d_col_fill_.alloc(size_t(g.ncol));
+    d_col_start_.alloc(size_t(g.ncol) + 1);
+    d_col_sc_.alloc(size_t(g.ncol) + 1);
+  }
+  ensure_list_capacity();
+  list_valid_ = false;
+  green_valid_ = false;
+  if (pme_) {
+    int k[3];
+    const double* e[3] = {a, b, c};
+    for (int d = 0; d < 3; ++d) k[d] = good_size(std::max(order_ + 1, int(std::ceil(norm3(e[d]) / opt_.pme_spacing))));
+    if (k[0] != pk_[0] || k[1] != pk_[1] || k[2] != pk_[2]) {
+      for (int d = 0; d < 3; ++d) pk_[d] = k[d];
+      ph1_ = pk_[0] / 2 + 1;
+      for (int d = 0; d < 3; ++d) {
+        std::vector<double> bsp;
+        bspline_moduli(pk_[d], order_, bsp);
+        d_bsp_[d].upload(bsp, stream_);
+      }
+      if (mixed_) pme_setup(pf_);
+      else pme_setup(pd_);
+    }
+  }
+}
+
+void Engine::ensure_list_capacity() {
+  const int ncol = geom_.ncol;
+  const int nsc = n_ / kScAtoms + ncol + 16;
+  // entries: j clusters within the list radius of a super-cluster (its images included), half of them, with margin
+  const double dens_cl = double(nsc) * 8.0 / dcell_.vol;
+  const double side = std::cbrt(64.0 * dcell_.vol / std::max(1, n_));
+  const double R = geom_.rlist + 1.0 * side;
+  const double per_sc = 4.0 / 3.0 * kPi * R * R * R * dens_cl;
+  const size_t ent = size_t(double(nsc) * std::max(16.0, 0.75 * per_sc)) + 4096;
+  if (nsc > nsc_cap_ || ent > d_ent_.n) {
+    nsc_cap_ = std::max(nsc, nsc_cap_);
+    const size_t ns = size_t(nsc_cap_) * kScAtoms;
+    d_sc_col_.alloc(size_t(nsc_cap_));
+    d_sc_z_.alloc(size_t(2) * nsc_cap_);
+    d_sc_org_.alloc(size_t(3) * nsc_cap_);
+    d_cl_box_.alloc(size_t(6) * 8 * nsc_cap_);
+    d_cl_real_.alloc(size_t(8) * nsc_cap_);
+    d_perm_.alloc(ns);
+    d_xq_.alloc(ns);
+    if (!mixed_) d_xqd_.alloc(ns);
+    d_tslot_.alloc(ns);
+    d_Fs_.alloc(3 * ns);
+    if (!mixed_) d_Fsd_.alloc(3 * ns);
+    const size_t ecap = std::max(ent, d_ent_.n);
+    d_ent_.alloc(ecap);
+    d_ent_shift_.alloc(ecap);
+    d_work_.alloc(ecap / 4 + size_t(nsc_cap_) * 2 + 64);
+    d_masks_.alloc(size_t(8) * 64 * nsc_cap_ + 8 * 256);
+  }
+  d_col_.alloc(size_t(n_));
+  d_frac_.alloc(size_t(3) * n_);
+  d_ioff_.alloc(size_t(3) * n_);
+  d_order_.alloc(size_t(n_));
+  d_iperm_.alloc(size_t(n_));
+  d_x0_.alloc(size_t(3) * n_);
+  if (!d_counters_.p) {
+    d_counters_.alloc(kCntNum);
+    CK(cudaMemsetAsync(d_counters_.p, 0, sizeof(int) * kCntNum, stream_));
+  }
+  d_F_.alloc(size_t(3) * n_);
+  if (!mixed_) d_Fd_.alloc(size_t(3) * n_);
+  d_efix_.alloc(kENumSlots);
+  d_edbl_.alloc(kENumSlots);
+  d_x_.alloc(size_t(3) * n_);
+  d_f_.alloc(size_t(3) * n_);
+  ListBufs& b = lb_;
+  b.col = d_col_.p;
+  b.frac = d_frac_.p;
+  b.ioff = d_ioff_.p;
+  b.order = d_order_.p;
+  b.iperm = d_iperm_.p;
+  b.col_count = d_col_count_.p;
+  b.col_fill = d_col_fill_.p;
+  b.col_start = d_col_start_.p;
+  b.col_sc = d_col_sc_.p;
+  b.sc_col = d_sc_col_.p;
+  b.sc_z = d_sc_z_.p;
+  b.sc_org = d_sc_org_.p;
+  b.cl_box = d_cl_box_.p;
+  b.cl_real = d_cl_real_.p;
+  b.perm = d_perm_.p;
+  b.ent = d_ent_.p;
+  b.ent_shift = d_ent_shift_.p;
+  b.masks = d_masks_.p;
+  b.work = d_work_.p;
+  b.nsc_cap = nsc_cap_;
+  b.ent_cap = int(std::min<size_t>(d_ent_.n, size_t(INT32_MAX)));
+  b.mask_cap = int(d_masks_.n / 8);
+  b.work_cap = int(d_work_.n);
+  b.counters = d_counters_.p;
+}
+
+template <class R>
+void Engine::pme_setup(PmePath<R>& P) {
+  using T = typename Cpx<R>::T;
+  const size_t half = size_t(ph1_) * pk_[1] * pk_[2];
+  P.h.alloc(half);
+  P.gr.alloc(size_t(pk_[0]) * pk_[1] * pk_[2]);
+  P.gt.alloc(half);
+  P.wt.alloc(6 * half);
+  if (mixed_) d_gridq_.alloc(size_t(pk_[0]) * pk_[1] * pk_[2]);
+  else d_grid_.alloc(size_t(pk_[0]) * pk_[1] * pk_[2]);
+  for (int d = 0; d < 3; ++d)
+    for (int dir = 0; dir < 2; ++dir) {
+      const int nn = pk_[d];
+      const int sign = dir == 0 ? -1 : +1;   // forward e^{-i}, inverse e^{+i}: the convolution is the same either way
+      std::vector<T> tw(static_cast<size_t>(nn));
+      for (int k = 0; k < nn; ++k) {
+        const double ang = 2 * kPi * k / nn;
+        tw[size_t(k)] = T{R(std::cos(ang)), R(sign * std::sin(ang))};
+      }
+      P.tw[d][dir].upload(tw, stream_);
+      FftPlan<R>& pl = P.plan[d][dir];
+      pl.n = nn;
+      factor_radices(nn, pl.rad, pl.nst);
+      pl.tw = P.tw[d][dir].p;
+      pl.sign = sign;
+    }
+  // lines per block: two complex buffers within 48 KB of shared memory
+  const int cap = int(48 * 1024 / (2 * sizeof(T)));
+  lines_x_ = std::max(1, std::min(64, cap / pk_[0]));
+  lines_y_ = std::max(1, std::min({64, cap / pk_[1], ph1_}));
+  lines_z_ = std::max(1, std::min({64, cap / pk_[2], ph1_}));
+  green_valid_ = false;
+  CK(cudaStreamSynchronize(stream_));
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+void Engine::launch_build(const double* d_x) {
+  const ListGeom& g = geom_;
+  k_clear_columns<<<blocks_for(size_t(g.ncol), 256), 256, 0, stream_>>>(g, lb_);
+  k_bin<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_x, dcell_, g, lb_);
+  k_scan_columns<<<1, 1024, 0, stream_>>>(g, lb_);
+  k_scatter<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, lb_);
+  const size_t sort_smem = size_t(kSortMax) * (sizeof(double) + sizeof(int));
+  k_sort_columns<<<std::min(g.ncol, dev_sms_ * 8), 256, sort_smem, stream_>>>(g, lb_);
+  k_superclusters<<<std::max(1, std::min(blocks_for(size_t(nsc_cap_), 4), dev_sms_ * 16)), 128, 0, stream_>>>(dcell_, lb_);
+  k_search<<<std::max(1, std::min(nsc_cap_, dev_sms_ * 16)), 32, sizeof(SearchShared), stream_>>>(dcell_, g, d_excl_off_.p, d_excl_list_.p, lb_);
+  k_end_build<<<blocks_for(size_t(3) * n_, 256), 256, 0, stream_>>>(n_, d_x, d_x0_.p, lb_.counters);
+  CK(cudaGetLastError());
+}
+
+void Engine::pair_forces(bool ener, bool vir) {
+  PairArgs A{};
+  A.work = d_work_.p;
+  A.ent = d_ent_.p;
+  A.ent_shift = d_ent_shift_.p;
+  A.masks = d_masks_.p;
+  A.counters = d_counters_.p;
+  A.tslot = d_tslot_.p;
+  A.xq = d_xq_.p;
+  A.xqd = d_xqd_.p;
+  A.tab = d_tab_.p;
+  A.tabd = d_tabd_.p;
+  A.gtab = d_gtab_.p;
+  A.ntab = nt_ + 1;
+  A.gnodes = gnodes_;
+  A.ghi = ghi_;
+  A.cell = dcell_;
+  A.rc2 = rc_ * rc_;
+  A.rc = rc_;
+  A.beta = kappa_;
+  A.kc = 2 * kappa_ / std::sqrt(kPi);
+  A.kcoul = kCoulomb;
+  A.dsf_e0 = dsf_e0_;
+  A.dsf_f0 = dsf_f0_;
+  A.fsx = d_Fs_.p;
+  A.fsy = d_Fs_.p + d_Fs_.n / 3;
+  A.fsz = d_Fs_.p + 2 * (d_Fs_.n / 3);
+  if (!mixed_) {
+    A.fdx = d_Fsd_.p;
+    A.fdy = d_Fsd_.p + d_Fsd_.n / 3;
+    A.fdz = d_Fsd_.p + 2 * (d_Fsd_.n / 3);
+  }
+  A.en.fix = d_efix_.p;
+  A.en.dbl = d_edbl_.p;
+  A.work_cap = int(d_work_.n);
+  const int coul = coul_ ? (pme_ ? 1 : 2) : 0;
+  const int grid = dev_sms_ * 8;
+  const int ntab = nt_ + 1;
+  if (mixed_) {
+    const size_t smem = sizeof(float4) * (size_t(ntab) * ntab + 4 * 64) + sizeof(int) * 4 * 64;
+#define PAIR32(C, E, V)                                                                                              \
+  do {                                                                                                               \
+    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_pair_f32<C, E, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
+    k_pair_f32<C, E, V><<<grid, 128, smem, stream_>>>(A);                                                            \
+  } while (0)
+    if (coul == 1) { if (ener) { if (vir) PAIR32(1, true, true); else PAIR32(1, true, false); } else { if (vir) PAIR32(1, false, true); else PAIR32(1, false, false); } }
+    else if (coul == 2) { if (ener) { if (vir) PAIR32(2, true, true); else PAIR32(2, true, false); } else { if (vir) PAIR32(2, false, true); else PAIR32(2, false, false); } }
+    else { if (ener) { if (vir) PAIR32(0, true, true); else PAIR32(0, true, false); } else { if (vir) PAIR32(0, false, true); else PAIR32(0, false, false); } }
+#undef PAIR32
+  } else {
+    const size_t smem = sizeof(double4) * (size_t(ntab) * ntab + 4 * 64) + sizeof(double) * 2 * size_t(coul ? gnodes_ : 0) + sizeof(int) * 4 * 64;
+#define PAIR64(C, E, V)                                                                                              \
+  do {                                                                                                               \
+    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_pair_f64<C, E, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
+    k_pair_f64<C, E, V><<<grid, 128, smem, stream_>>>(A);                                                            \
+  } while (0)
+    if (coul == 1) { if (ener) { if (vir) PAIR64(1, true, true); else PAIR64(1, true, false); } else { if (vir) PAIR64(1, false, true); else PAIR64(1, false, false); } }
+    else if (coul == 2) { if (ener) { if (vir) PAIR64(2, true, true); else PAIR64(2, true, false); } else { if (vir) PAIR64(2, false, true); else PAIR64(2, false, false); } }
+    else { if (ener) { if (vir) PAIR64(0, true, true); else PAIR64(0, true, false); } else { if (vir) PAIR64(0, false, true); else PAIR64(0, false, false); } }
+#undef PAIR64
+  }
+  CK(cudaGetLastError());
+}
+
+void Engine::bonded_forces(const double* d_x, bool ener, bool vir) {
+  BondedArgs A{d_x, dcell_, EnergySink{d_efix_.p, d_edbl_.p}, mixed_ ? 1 : 0};
+  const int T = 256;
+  const bool bonded = (opt_.parts & 1) != 0, nonb = (opt_.parts & 2) != 0;
+  auto nblk = [&](int cnt) { return std::min(blocks_for(size_t(std::max(cnt, 1)), T), dev_sms_ * 4); };
+#define LAUNCH3(K, R, cnt, ...)                                                                                     \
+  do {                                                                                                              \
+    if (ener) { if (vir) K<R, true, true><<<nblk(cnt), T, 0, stream_>>>(__VA_ARGS__); else K<R, true, false><<<nblk(cnt), T, 0, stream_>>>(__VA_ARGS__); } \
+    else { if (vir) K<R, false, true><<<nblk(cnt), T, 0, stream_>>>(__VA_ARGS__); else K<R, false, false><<<nblk(cnt), T, 0, stream_>>>(__VA_ARGS__); } \
+  } while (0)
+  auto run = [&](auto tag) {
+    using R = decltype(tag);
+    ForceSink<R> F;
+    if constexpr (sizeof(R) == 4) F = ForceSink<R>{d_F_.p, d_F_.p + n_, d_F_.p + 2 * size_t(n_)};
+    else F = ForceSink<R>{d_Fd_.p, d_Fd_.p + n_, d_Fd_.p + 2 * size_t(n_)};
+    if (bonded) {
+      if (nb_) LAUNCH3(k_bonds, R, nb_, nb_, d_bond_ij_.p, d_bond_kr_.p, A, F);
+      if (na_) LAUNCH3(k_angles, R, na_, na_, d_angle_ijk_.p, d_angle_kt_.p, A, F);
+      if (ndg_) LAUNCH3(k_torsions, R, ndg_, ndg_, d_dih_grp_.p, d_dih_ijkl_.p, d_dih_vd_.p, d_dih_n_.p, A, F, int(kEDihedral));
+      if (nig_) LAUNCH3(k_torsions, R, nig_, nig_, d_imp_grp_.p, d_imp_ijkl_.p, d_imp_vd_.p, d_imp_n_.p, A, F, int(kEImproper));
+      if (nfene_) LAUNCH3(k_fene, R, nfene_, nfene_, d_fene_ij_.p, d_fene_p_.p, A, F, d_counters_.p);
+    }
+    if (nonb && np14_)
+      LAUNCH3(k_pairs14, R, np14_, np14_, d_p14_ij_.p, p14_scaled_ ? d_p14_scale_.p : nullptr, lj14_, d_type_.p, nt_, d_lj14_.p,
+              (const double4*)nullptr, A, F);
+    if (nonb && coul_ && nx_) {
+      ExclArgs E{d_excl_ij_.p, d_excl_f_.p, d_q_.p, d_gtab_.p, ghi_, rc_, rc_ * rc_, kappa_, dsf_e0_, dsf_f0_, pme_ ? 1 : 0};
+      if constexpr (sizeof(R) == 4) {
+        if (ener) { if (vir) k_excl_f32<true, true><<<nblk(nx_), T, 0, stream_>>>(nx_, E, A, F); else k_excl_f32<true, false><<<nblk(nx_), T, 0, stream_>>>(nx_, E, A, F); }
+        else { if (vir) k_excl_f32<false, true><<<nblk(nx_), T, 0, stream_>>>(nx_, E, A, F); else k_excl_f32<false, false><<<nblk(nx_), T, 0, stream_>>>(nx_, E, A, F); }
+      } else {
+        if (ener) { if (vir) k_excl_f64<true, true><<<nblk(nx_), T, 0, stream_>>>(nx_, E, A, F); else k_excl_f64<true, false><<<nblk(nx_), T, 0, stream_>>>(nx_, E, A, F); }
+        else { if (vir) k_excl_f64<false, true><<<nblk(nx_), T, 0, stream_>>>(nx_, E, A, F); else k_excl_f64<false, false><<<nblk(nx_), T, 0, stream_>>>(nx_, E, A, F); }
+      }
+    }
+  };
+  if (mixed_) run(float{});
+  else run(double{});
+#undef LAUNCH3
+  CK(cudaGetLastError());
+}
+
+template <class R>
+void Engine::pme_run(PmePath<R>& P, const double* d_x, bool ener, bool vir) {
+  using T = typename Cpx<R>::T;
+  PmeArgs A{pk_[0], pk_[1], pk_[2], ph1_, dcell_, d_x, d_q_.p, n_};
+  if (!green_valid_ || std::memcmp(green_cell_, cell_h_, sizeof cell_h_) != 0) {
+    const size_t half = size_t(ph1_) * pk_[1] * pk_[2];
+    k_pme_green<R><<<blocks_for(half, 256), 256, 0, stream_>>>(A, d_bsp_[0].p, d_bsp_[1].p, d_bsp_[2].p, beta_, kCoulomb, P.gt.p, P.wt.p);
+    std::memcpy(green_cell_, cell_h_, sizeof cell_h_);
+    green_valid_ = true;
+  }
+  const int nb = blocks_for(size_t(n_), 128);
+  if (mixed_) CK(cudaMemsetAsync(d_gridq_.p, 0, d_gridq_.n * sizeof(long long), stream_));
+  else CK(cudaMemsetAsync(d_grid_.p, 0, d_grid_.n * sizeof(double), stream_));
+#define SPREAD(P_) k_spread<R, P_><<<nb, 128, 0, stream_>>>(A, d_grid_.p, d_gridq_.p)
+  switch (order_) {
+    case 3: SPREAD(3); break;
+    case 4: SPREAD(4); break;
+    case 5: SPREAD(5); break;
+    case 6: SPREAD(6); break;
+    case 7: SPREAD(7); break;
+    default: SPREAD(8); break;
+  }
+#undef SPREAD
+  const size_t sx = size_t(lines_x_) * pk_[0] * 2 * sizeof(T), sy = size_t(lines_y_) * pk_[1] * 2 * sizeof(T), sz = size_t(lines_z_) * pk_[2] * 2 * sizeof(T);
+  const int nlx = pk_[1] * pk_[2];
+  k_fft_x_fwd<R><<<blocks_for(size_t(nlx), lines_x_), 256, sx, stream_>>>(A, mixed_ ? nullptr : d_grid_.p, mixed_ ? d_gridq_.p : nullptr, P.h.p,
+                                                                        P.plan[0][0], lines_x_);
+  const int gy = ((ph1_ + lines_y_ - 1) / lines_y_) * pk_[2];
+  k_fft_y<R><<<gy, 256, sy, stream_>>>(A, P.h.p, P.plan[1][0], lines_y_);
+  const int gz = ((ph1_ + lines_z_ - 1) / lines_z_) * pk_[1];
+  EnergySink en{d_efix_.p, d_edbl_.p};
+  if (ener) { if (vir) k_fft_z_solve<R, true, true><<<gz, 256, sz, stream_>>>(A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); else k_fft_z_solve<R, true, false><<<gz, 256, sz, stream_>>>(A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); }
+  else { if (vir) k_fft_z_solve<R, false, true><<<gz, 256, sz, stream_>>>(A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); else k_fft_z_solve<R, false, false><<<gz, 256, sz, stream_>>>(A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); }
+  k_fft_y<R><<<gy, 256, sy, stream_>>>(A, P.h.p, P.plan[1][1], lines_y_);
+  k_fft_x_inv<R><<<blocks_for(size_t(nlx), lines_x_), 256, sx, stream_>>>(A, P.h.p, P.gr.p, P.plan[0][1], lines_x_);
+  ForceSink<R> F;
+  if constexpr (sizeof(R) == 4) F = ForceSink<R>{d_F_.p, d_F_.p + n_, d_F_.p + 2 * size_t(n_)};
+  else F = ForceSink<R>{d_Fd_.p, d_Fd_.p + n_, d_Fd_.p + 2 * size_t(n_)};
+#define GATHER(P_) k_gather<R, P_><<<nb, 128, 0, stream_>>>(A, P.gr.p, F)
+  switch (order_) {
+    case 3: GATHER(3); break;
+    case 4: GATHER(4); break;
+    case 5: GATHER(5); break;
+    case 6: GATHER(6); break;
+    case 7: GATHER(7); break;
+    default: GATHER(8); break;
+  }
+#undef GATHER
+  CK(cudaGetLastError());
+}
+
+void Engine::pme_forces(const double* d_x, bool ener, bool vir) {
+  if (mixed_) pme_run(pf_, d_x, ener, vir);
+  else pme_run(pd_, d_x, ener, vir);
+}
+
+// One force evaluation on device positions d_x (AoS, 3 n): accumulators cleared, list checked / rebuilt, every term,
+// forces reduced into d_f_ (AoS doubles). Asynchronous on stream_.
+void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild) {
+  const bool nonb = (opt_.parts & 2) != 0;
+  if (nonb) {
+    if (!list_valid_) {
+      k_set_flag<<<1, 1, 0, stream_>>>(d_counters_.p, kCntRebuild, 1);
+      list_valid_ = true;
+      ++builds_;
+    } else if (check_rebuild) {
+      k_check_moved<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_x, d_x0_.p, 0.25 * skin_ * skin_, d_counters_.p);
+    }
+    launch_build(d_x);
+  }
+  if (mixed_) {
+    CK(cudaMemsetAsync(d_F_.p, 0, d_F_.n * sizeof(long long), stream_));
+    if (nonb) CK(cudaMemsetAsync(d_Fs_.p, 0, d_Fs_.n * sizeof(long long), stream_));
+  } else {
+    CK(cudaMemsetAsync(d_Fd_.p, 0, d_Fd_.n * sizeof(double), stream_));
+    if (nonb) CK(cudaMemsetAsync(d_Fsd_.p, 0, d_Fsd_.n * sizeof(double), stream_));
+  }
+  CK(cudaMemsetAsync(d_efix_.p, 0, d_efix_.n * sizeof(long long), stream_));
+  CK(cudaMemsetAsync(d_edbl_.p, 0, d_edbl_.n * sizeof(double), stream_));
+  if (nonb) {
+    const size_t ns = size_t(nsc_cap_) * kScAtoms;
+    if (mixed_)
+      k_pack_f32<<<blocks_for(ns, 256), 256, 0, stream_>>>(int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_sc_org_.p, d_q_.p, d_type_.p, nt_,
+                                                           d_xq_.p, d_tslot_.p, d_counters_.p);
+    else
+      k_pack_f64<<<blocks_for(ns, 256), 256, 0, stream_>>>(int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_q_.p, d_type_.p, nt_, d_xqd_.p, d_tslot_.p,
+                                                           d_counters_.p);
+    pair_forces(ener, vir);
+  }
+  bonded_forces(d_x, ener, vir);
+  if (nonb && pme_) pme_forces(d_x, ener, vir);
+  const size_t ns = size_t(nsc_cap_) * kScAtoms;
+  if (mixed_) k_reduce_f32<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_F_.p, d_Fs_.p, int(ns), d_iperm_.p, d_f_.p, nonb ? 1 : 0);
+  else k_reduce_f64<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_Fd_.p, d_Fsd_.p, int(ns), d_iperm_.p, d_f_.p, nonb ? 1 : 0);
+  if (nonb) k_lower_flag<<<1, 1, 0, stream_>>>(d_counters_.p);
+  CK(cudaGetLastError());
+}
+
+void Engine::check_errors() {
+  const unsigned e = unsigned(h_counters_[kCntErr]);
+  if (!e) return;
+  CK(cudaMemsetAsync(d_counters_.p + kCntErr, 0, sizeof(int), stream_));
+  if (e & kErrFene) throw ModelError(CAPS_GPU_EFIELD, "a FENE bond is stretched past R0; lower --dt or relax the structure first");
+  if (e & (kErrListOverflow | kErrMaskOverflow | kErrScOverflow)) throw ModelError(-100, "pair list capacity exceeded");
+  if (e & kErrColumnTooBig) throw ModelError(CAPS_GPU_EINVAL, "a grid column holds more atoms than the device sort takes (the cell is too dense or too thin)");
+  if (e & kErrExclOverflow) throw ModelError(CAPS_GPU_EINVAL, "too many excluded partners in one super-cluster for the device list");
+  if (e & kErrImageRange) throw ModelError(CAPS_GPU_EFIELD, "an excluded pair is more than 63 cells apart: unwrap the molecules first");
+  if (e & (kErrShake | kErrShakeTurn))
+    throw ModelError(CAPS_GPU_ECONSTRAINT, (e & kErrShakeTurn) ? "a constrained bond turned by more than 90° in one step; lower the time step or relax first"
+                                                                 : "the bond constraints did not converge (SHAKE); lower the time step or relax first");
+  if (e & kErrNonFinite) throw ModelError(CAPS_GPU_EFIELD, "the simulation became unstable; lower the time step or relax first");
+  throw ModelError(CAPS_GPU_EINVAL, "device error word " + std::to_string(e));
+}
+
+// Host-side constants: self energy, neutralising background, LJ tail (field.cpp:2455-2537).
+void Engine::host_constants(caps_gpu_terms* t, bool ener, bool vir) const {
+  (void)vir;
+  const bool nonb = (opt_.parts & 2) != 0;
+  if (!nonb) return;
+  double q2 = 0, qt = 0;
+  for (double c : h_q_) q2 += c * c, qt += c;
+  if (coul_) {
+    if (pme_) {
+      if (ener) t->coulomb -= kCoulomb * beta_ / std::sqrt(kPi) * q2;
+      if (std::fabs(qt) > 1e-10) {
+        const double eb = -kCoulomb * kPi * qt * qt / (2 * dcell_.vol * beta_ * beta_);
+        if (ener) t->coulomb += eb;
+        t->virial += 3 * eb;
+        for (int c = 0; c < 3; ++c) t->w[c] += eb;
+      }
+    } else if (ener) {
+      const double a = opt_.dsf_alpha;
+      t->coulomb -= (erfc_rc_ / (2 * rc_) + dsf_f0_ * rc_ / 2 + a / std::sqrt(kPi)) * q2 * kCoulomb;
+    }
+  }
+  if (tail_) {
+    const double vol = dcell_.vol, rc2 = rc_ * rc_, rc3 = rc2 * rc_, rc9 = rc3 * rc3 * rc3;
+    double et = 0, wt = 0;
+    for (int a0 = 0; a0 < nt_; ++a0)
+      for (int b0 = 0; b0 < nt_; ++b0) {
+        const double eps = h_eps_[size_t(a0) * nt_ + b0], s6 = std::pow(h_sig_[size_t(a0) * nt_ + b0], 6), s12 = s6 * s6;
+        const double nn = type_count_[size_t(a0)] * type_count_[size_t(b0)];
+        et += nn * 2 * kPi * 4 * eps * (s12 / (9 * rc9) - s6 / (3 * rc3));
+        wt += nn * 2 * kPi * 4 * eps * (4 * s12 / (3 * rc9) - 2 * s6 / rc3);
+      }
+    if (ener) t->vdw += et / vol;
+    t->virial += wt / vol;
+    t->tail_energy = et / vol;
+    t->tail_virial = wt / vol;
+    for (int c = 0; c < 3; ++c) t->w[c] += wt / vol / 3;
+  }
+}
+
+void Engine::read_terms(caps_gpu_terms* out, bool ener, bool vir) {
+  caps_gpu_terms t{};
+  double e[kENumSlots];
+  for (int k = 0; k < kENumSlots; ++k) e[k] = mixed_ ? double(h_efix_[k]) * kInvFixF : h_edbl_[k];
+  t.bond = e[kEBond];
+  t.angle = e[kEAngle];
+  t.dihedral = e[kEDihedral];
+  t.improper = e[kEImproper];
+  t.vdw = e[kEVdw];
+  t.coulomb = e[kECoul];
+  for (int c = 0; c < 6; ++c) t.w[c] = vir ? e[kEW0 + c] : 0.0;
+  t.virial = t.w[0] + t.w[1] + t.w[2];
+  host_constants(&t, ener, vir);
+  if (out) *out = t;
+}
+
+void Engine::compute_dev(const double* d_x, const double* cell, double* d_f, caps_gpu_terms* out) {
+  set_cell(cell);
+  for (int attempt = 0;; ++attempt) {
+    forces(d_x, true, true, true);
+    CK(cudaMemcpyAsync(h_counters_, d_counters_.p, sizeof(int) * kCntNum, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(h_efix_, d_efix_.p, sizeof(long long) * kENumSlots, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(h_edbl_, d_edbl_.p, sizeof(double) * kENumSlots, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    try {
+      check_errors();
+    } catch (const ModelError& m) {
+      if (m.code != -100 || attempt >= 3) throw;
+      // grow the list and build again
+      const size_t ent = d_ent_.n * 2;
+      d_ent_.release();
+      d_ent_shift_.release();
+      d_ent_.alloc(ent);
+      d_ent_shift_.alloc(ent);
+      d_work_.release();
+      d_work_.alloc(ent / 4 + size_t(nsc_cap_) * 2 + 64);
+      const size_t mk = d_masks_.n * 2;
+      d_masks_.release();
+      d_masks_.alloc(mk);
+      ensure_list_capacity();
+      list_valid_ = false;
+      continue;
+    }
+    break;
+  }
+  const bool ener_pairs = energies_ || !mixed_;
+  (void)ener_pairs;
+  read_terms(out, true, true);
+  if (d_f != d_f_.p) CK(cudaMemcpyAsync(d_f, d_f_.p, sizeof(double) * 3 * size_t(n_), cudaMemcpyDeviceToDevice, stream_));
+  CK(cudaStreamSynchronize(stream_));
+}
+
+void Engine::compute_host(const double* x, const double* cell, double* f, caps_gpu_terms* out) {
+  set_cell(cell);
+  CK(cudaMemcpyAsync(d_x_.p, x, sizeof(double) * 3 * size_t(n_), cudaMemcpyHostToDevice, stream_));
+  compute_dev(d_x_.p, cell, d_f_.p, out);
+  CK(cudaMemcpyAsync(f, d_f_.p, sizeof(double) * 3 * size_t(n_), cudaMemcpyDeviceToHost, stream_));
+  CK(cudaStreamSynchronize(stream_));
+}
+
+
+}  // namespace capsb
+
+// ---------------------------------------------------------------------------------------------------------------
+// C ABI
+using capsb::Engine;
+
+struct caps_gpu_engine {
+  std::unique_ptr<Engine> e;
+  std::string err;
+};
+
+namespace {
+thread_local std::string g_create_error;
+
+int32_t guard(caps_gpu_engine* h, const std::function<void()>& fn) {
+  try {
+    fn();
+    return CAPS_GPU_OK;
+  } catch (const capsb::ModelError& m) {
+    if (h) h->err = m.what();
+    else g_create_error = m.what();
+    return m.code < 0 && m.code > -100 ? m.code : CAPS_GPU_EINVAL;
+  } catch (const capsb::CudaError& c) {
+    if (h) h->err = c.what();
+    else g_create_error = c.what();
+    return CAPS_GPU_ECUDA;
+  } catch (const std::exception& x) {
+    if (h) h->err = x.what();
+    else g_create_error = x.what();
+    return CAPS_GPU_EINVAL;
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int32_t caps_gpu_abi_version(void) { return CAPS_GPU_ABI_VERSION; }
+
+int32_t caps_gpu_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+  return n;
+}
+
+caps_gpu_engine* caps_gpu_create(const caps_gpu_ff* ff, const caps_gpu_opts* opts) {
+  if (!ff || !opts) {
+    g_create_error = "caps_gpu_create: null argument";
+    return nullptr;
+  }
+  auto h = std::make_unique<caps_gpu_engine>();
+  const int32_t rc = guard(nullptr, [&] { h->e = std::make_unique<Engine>(ff, opts); });
+  if (rc != CAPS_GPU_OK) return nullptr;
+  return h.release();
+}
+
+int32_t caps_gpu_set_options(caps_gpu_engine* e, const caps_gpu_opts* opts) {
+  if (!e || !opts) return CAPS_GPU_EINVAL;
+  return guard(e, [&] { e->e->set_options(opts); });
+}
+
+int32_t caps_gpu_energies(caps_gpu_engine* e, int32_t on) {
+  if (!e) return CAPS_GPU_EINVAL;
+  e->e->energies(on != 0);
+  return CAPS_GPU_OK;
+}
+
+int32_t caps_gpu_compute(caps_gpu_engine* e, const double* x, const double* cell, double* f, caps_gpu_terms* out) {
+  if (!e || !x || !cell || !f) return CAPS_GPU_EINVAL;
+  return guard(e, [&] { e->e->compute_host(x, cell, f, out); });
+}
+
+int32_t caps_gpu_compute_device(caps_gpu_engine* e, const double* d_x, const double* cell, double* d_f, caps_gpu_terms* out) {
+  if (!e || !d_x || !cell || !d_f) return CAPS_GPU_EINVAL;
+  return guard(e, [&] { e->e->compute_dev(d_x, cell, d_f, out); });
+}
+
+int32_t caps_gpu_list_builds(const caps_gpu_engine* e) { return e ? e->e->list_builds() : 0; }
+
+int32_t caps_gpu_run(caps_gpu_engine* e, caps_gpu_state* state, const caps_gpu_md_opts* md, caps_gpu_progress_fn progress, caps_gpu_frame_fn frame,
+                     void* user, char* report, int32_t report_cap) {
+  if (!e || !state || !md || !state->x || !state->cell) return CAPS_GPU_EINVAL;
+  std::string rep;
+  const int32_t rc = guard(e, [&] { e->e->run(state, md, progress, frame, user, &rep); });
+  if (report && report_cap > 0) {
+    std::snprintf(report, size_t(report_cap), "%s", rc == CAPS_GPU_OK ? rep.c_str() : e->err.c_str());
+  }
+  return rc;
+}
+
+double caps_gpu_last_steps_per_second(const caps_gpu_engine* e) { return e ? e->e->last_steps_per_second() : 0.0; }
+
+void caps_gpu_destroy(caps_gpu_engine* e) { delete e; }
+
+const char* caps_gpu_error(const caps_gpu_engine* e) { return e ? e->err.c_str() : g_create_error.c_str(); }
+
+}  // extern "C"

@@ -1,0 +1,200 @@
+// The device engine behind include/caps_gpu.h: owns the force field on the device, the cluster pair list, the PME
+// grids and the MD state, and runs Evaluator::compute and run_dynamics for one system on one GPU.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <array>
+#include <cstdint>
+#include <functional>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "caps_gpu.h"
+#include "common.cuh"
+#include "nblist.cuh"
+#include "pme.cuh"
+
+namespace capsb {
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count);        // throws on failure; keeps the buffer when large enough
+  void upload(const T* h, size_t count, cudaStream_t s);
+  void upload(const std::vector<T>& h, cudaStream_t s) { upload(h.data(), h.size(), s); }
+  void zero(cudaStream_t s);
+};
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+template <class T>
+void DevBuf<T>::alloc(size_t count) {
+  if (count <= n && p) return;
+  release();
+  if (count == 0) count = 1;
+  const cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+  if (e != cudaSuccess) {
+    p = nullptr;
+    throw CudaError(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  n = count;
+}
+template <class T>
+void DevBuf<T>::upload(const T* h, size_t count, cudaStream_t s) {
+  alloc(count);
+  if (!count) return;
+  const cudaError_t e = cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) throw CudaError(std::string("cudaMemcpyAsync: ") + cudaGetErrorString(e));
+}
+template <class T>
+void DevBuf<T>::zero(cudaStream_t s) {
+  if (!p) return;
+  const cudaError_t e = cudaMemsetAsync(p, 0, n * sizeof(T), s);
+  if (e != cudaSuccess) throw CudaError(std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
+}
+struct ModelError : std::runtime_error {   // the reference's FieldError and argument errors
+  int code;
+  ModelError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+// PME plans and buffers of one precision.
+template <class R>
+struct PmePath {
+  using T = typename Cpx<R>::T;
+  DevBuf<T> h;          // half spectrum
+  DevBuf<R> gr;         // real grid after the inverse transform
+  DevBuf<R> gt, wt;     // influence function, virial weights
+  DevBuf<T> tw[3][2];   // twiddles per axis: forward, inverse
+  FftPlan<R> plan[3][2];
+};
+
+class Engine {
+ public:
+  Engine(const caps_gpu_ff* ff, const caps_gpu_opts* o);
+  ~Engine();
+  void set_options(const caps_gpu_opts* o);
+  void energies(bool on) { energies_ = on; }
+  // compute on host arrays (copies in and out) or on device arrays
+  void compute_host(const double* x, const double* cell, double* f, caps_gpu_terms* out);
+  void compute_dev(const double* d_x, const double* cell, double* d_f, caps_gpu_terms* out);
+  int list_builds() const { return builds_; }
+  void run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progress_fn progress, caps_gpu_frame_fn frame, void* user, std::string* report);
+  double last_steps_per_second() const { return last_sps_; }
+  std::string err;
+
+  // --- internals used by the step kernels' launcher (integrate.cu) ---
+  int n_ = 0, nt_ = 0;
+  bool mixed_ = true;
+  caps_gpu_opts opt_{};
+  cudaStream_t stream_ = nullptr;
+
+ private:
+  friend struct Stepper;
+  void setup_ff(const caps_gpu_ff* ff);
+  void setup_options();
+  void set_cell(const double* cell);
+  void ensure_list_capacity();
+  void forces(const double* d_x, bool ener, bool vir, bool check_rebuild);   // everything up to d_f_ (device), async
+  void read_terms(caps_gpu_terms* out, bool ener, bool vir);
+  void check_errors();
+  void launch_build(const double* d_x);
+  void pme_forces(const double* d_x, bool ener, bool vir);
+  template <class R> void pme_setup(PmePath<R>& P);
+  template <class R> void pme_run(PmePath<R>& P, const double* d_x, bool ener, bool vir);
+  void pair_forces(bool ener, bool vir);
+  void bonded_forces(const double* d_x, bool ener, bool vir);
+  void host_constants(caps_gpu_terms* t, bool ener, bool vir) const;
+
+  // force field (device)
+  DevBuf<int> d_type_;
+  DevBuf<double> d_q_, d_mass_;
+  std::vector<int> h_type_;
+  std::vector<double> h_q_, h_mass_, h_eps_, h_sig_;   // per type pair
+  std::vector<double> type_count_;
+  std::vector<std::array<uint32_t, 2>> hb_;   // bonds (harmonic, then FENE) and their r0 (0: none), for constraints
+  std::vector<double> hr0_;
+  std::vector<std::array<uint32_t, 3>> ha_;   // angles and theta0, for rigid waters
+  std::vector<double> hth0_;
+  DevBuf<float4> d_tab_;
+  DevBuf<double4> d_tabd_, d_lj14_;
+  DevBuf<double> d_gtab_;
+  int gnodes_ = 0;
+  double ghi_ = 0;
+  DevBuf<uint32_t> d_bond_ij_, d_angle_ijk_, d_dih_ijkl_, d_imp_ijkl_, d_p14_ij_, d_excl_ij_, d_fene_ij_;
+  DevBuf<double> d_bond_kr_, d_angle_kt_, d_dih_vd_, d_imp_vd_, d_p14_scale_, d_fene_p_;
+  DevBuf<int> d_dih_n_, d_imp_n_, d_dih_grp_, d_imp_grp_;
+  DevBuf<float> d_excl_f_;
+  DevBuf<uint32_t> d_excl_off_, d_excl_list_;
+  int nb_ = 0, na_ = 0, nd_ = 0, ndg_ = 0, ni_ = 0, nig_ = 0, np14_ = 0, nx_ = 0, nfene_ = 0;
+  double lj14_ = 0.5;
+  bool p14_scaled_ = false;
+  bool lj_shift_model_ = false;
+  double model_cutoff_ = 0;
+
+  // options derived
+  double rc_ = 10, skin_ = 2, beta_ = 0, kappa_ = 0, dsf_e0_ = 0, dsf_f0_ = 0, erfc_rc_ = 0;
+  bool pme_ = false, coul_ = true, tail_ = true, shifted_ = false;
+  int order_ = 4;
+  bool energies_ = true;
+
+  // cell and list
+  double cell_h_[12] = {0};
+  bool cell_set_ = false;
+  DevCell dcell_{};
+  ListGeom geom_{};
+  ListBufs lb_{};
+  DevBuf<int> d_col_, d_ioff_, d_order_, d_iperm_, d_col_count_, d_col_fill_, d_col_start_, d_col_sc_, d_sc_col_, d_perm_, d_counters_;
+  DevBuf<double> d_frac_, d_sc_z_, d_sc_org_, d_cl_box_, d_x0_;
+  DevBuf<unsigned char> d_cl_real_;
+  DevBuf<uint4> d_ent_;
+  DevBuf<float4> d_ent_shift_;
+  DevBuf<unsigned long long> d_masks_;
+  DevBuf<int4> d_work_;
+  bool list_valid_ = false;
+  int builds_ = 0;
+  int nsc_cap_ = 0;
+
+  // packed positions, forces
+  DevBuf<float4> d_xq_;
+  DevBuf<double4> d_xqd_;
+  DevBuf<int> d_tslot_;
+  DevBuf<long long> d_F_, d_Fs_;    // fixed point, SoA: atom order (3 n), slot order (3 nslots)
+  DevBuf<double> d_Fd_, d_Fsd_;     // FP64 path
+  DevBuf<long long> d_efix_;
+  DevBuf<double> d_edbl_;
+  DevBuf<double> d_x_, d_f_;        // host-call staging: positions in, forces out (3 n AoS)
+  int* h_counters_ = nullptr;       // pinned
+  long long* h_efix_ = nullptr;     // pinned
+  double* h_edbl_ = nullptr;        // pinned
+
+  // PME
+  int pk_[3] = {0, 0, 0}, ph1_ = 0;
+  DevBuf<double> d_bsp_[3];
+  DevBuf<double> d_grid_;           // FP64 spread grid
+  DevBuf<long long> d_gridq_;       // FP32 path: fixed-point spread grid
+  PmePath<float> pf_;
+  PmePath<double> pd_;
+  double green_cell_[12] = {0};
+  bool green_valid_ = false;
+  int lines_x_ = 1, lines_y_ = 1, lines_z_ = 1;
+
+  double last_sps_ = 0;
+  int dev_sms_ = 148;
+};
+
+}  // namespace capsb

@@ -1,0 +1,856 @@
+// run_dynamics on the device (core/src/dynamics.cpp:71-815): velocity Verlet with the Bussi, Langevin (BAOAB) and
+// Nose-Hoover-chain thermostats, stochastic cell rescaling, SHAKE / RATTLE for bonds to hydrogen and rigid waters.
+//
+// The state (x, v, forces, thermostat chain) stays in HBM for the whole run. One MD step is a fixed kernel sequence,
+// captured once as a CUDA graph and replayed: the list check and the gated list build, the force kernels, the kicks,
+// drifts, constraint solves and thermostat updates all read their scalars (target temperature, step number, chain
+// variables) from device memory, so the graph is the same every step. Steps that report a thermo row, record a frame or
+// scale the cell run the same sequence uncaptured with energies and virial on and synchronise with the host.
+//
+// Random numbers. Initial Maxwell-Boltzmann velocities and the Bussi thermostat's per-step draws come from a host
+// stream built exactly as the reference's (std::mt19937_64 seeded with DynamicsOptions::seed, 53-bit uniforms,
+// Marsaglia's polar normals, Marsaglia-Tsang gamma; core/include/caps/rng.hpp), uploaded ahead in chunks, so a Bussi or
+// NVE or Nose-Hoover run starts from the reference's velocities and draws the reference's numbers. Langevin noise, 3N
+// normals a step, comes from a counter-based Philox stream on the device (a pure function of seed, step and atom).
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+
+namespace capsb {
+
+#define CK(call)                                                                                         \
+  do {                                                                                                   \
+    cudaError_t e_ = (call);                                                                             \
+    if (e_ != cudaSuccess) throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_));          \
+  } while (0)
+
+namespace {
+
+constexpr double kB = 0.0019872041;    // kcal/(mol K), as core/src/dynamics.cpp:22
+constexpr double kAcc = 4.184e-4;      // (kcal/mol/Å)/(g/mol) -> Å/fs^2
+constexpr double kAtm = 68568.415;     // kcal/(mol Å^3) -> atm
+constexpr double kNA = 6.02214076e23;
+constexpr int kMaxClAtoms = 8, kMaxClCons = 8;
+constexpr int kShakeIter = 1000;
+constexpr double kShakeTol = 1e-8;
+
+// device scalars
+enum Sc { kScKE = 0, kScKE0, kScBath, kScFactor, kScTnow, kScKtarget, kScStep, kScCW0, kScKin0 = kScCW0 + 6, kScNum = kScKin0 + 6 };
+struct Chain {
+  double eta[3], eta_dot[4], eta_dotdot[3], eta_mass[3];
+};
+
+int blocks(size_t n, int t) { return int(std::max<size_t>(1, (n + size_t(t) - 1) / size_t(t))); }
+
+// --- the reference's random stream (core/include/caps/rng.hpp): 53-bit uniforms, polar normals, Marsaglia-Tsang ---
+struct HostRng {
+  std::mt19937_64 g;
+  bool have = false;
+  double spare = 0;
+  explicit HostRng(uint64_t seed) : g(seed) {}
+  double u01() { return double(uint64_t(g() - std::mt19937_64::min()) >> 11) * 0x1.0p-53; }
+  double normal(bool& hv, double& sp) {
+    if (hv) {
+      hv = false;
+      return sp;
+    }
+    double u, v, q;
+    do {
+      u = 2 * u01() - 1, v = 2 * u01() - 1, q = u * u + v * v;
+    } while (q >= 1 || q == 0);
+    const double f = std::sqrt(-2 * std::log(q) / q);
+    sp = v * f;
+    hv = true;
+    return u * f;
+  }
+  double gauss() { return normal(have, spare); }
+  double gamma(double k, double th) {   // shape k >= 1 (a fresh normal generator per call, as a fresh Gamma object)
+    bool hv = false;
+    double sp = 0;
+    if (k <= 0) return 0;
+    if (k < 1) {
+      double u;
+      do u = u01(); while (u == 0);
+      const double up = gamma(k + 1, th);
+      return up * std::pow(u, 1.0 / k);
+    }
+    const double d = k - 1.0 / 3.0, c = 1.0 / std::sqrt(9 * d);
+    for (;;) {
+      double x, v;
+      do {
+        x = normal(hv, sp);
+        v = 1 + c * x;
+      } while (v <= 0);
+      v = v * v * v;
+      double u;
+      do u = u01(); while (u == 0);
+      if (u < 1 - 0.0331 * x * x * x * x || std::log(u) < 0.5 * x * x + d * (1 - v + std::log(v))) return d * v * th;
+    }
+  }
+};
+
+// --- kernels --------------------------------------------------------------------------------------------------
+__global__ void k_kick(int n, double* __restrict__ v, const double* __restrict__ f, const double* __restrict__ invm, double h) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double a = h * kAcc * invm[i];
+  v[3 * i] += a * f[3 * i];
+  v[3 * i + 1] += a * f[3 * i + 1];
+  v[3 * i + 2] += a * f[3 * i + 2];
+}
+
+// drift: x0 = x (the constraint reference), x += h v; non-finite positions raise the error word
+__global__ void k_drift(int n, double* __restrict__ x, const double* __restrict__ v, double* __restrict__ x0, double h, int* counters) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 3 * n) return;
+  const double xo = x[i];
+  x0[i] = xo;
+  const double xn = xo + h * v[i];
+  x[i] = xn;
+  if (!isfinite(xn)) atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), kErrNonFinite);
+}
+
+struct ConsArgs {
+  int ncl;
+  const int* cl_start;     // ncl + 1: constraints of each cluster
+  const int* cl_atom0;     // ncl + 1: atoms of each cluster in cl_atoms
+  const int* cl_atoms;     // atom indices
+  const int4* cons;        // x, y: local atom indices, z: global i, w: global j
+  const double* d2;        // squared lengths
+  const double* invm;      // per atom
+  DevCell cell;
+};
+
+// SHAKE on each cluster (Gauss-Seidel along the reference vectors, tol 1e-8 relative; core/src/constraints.cpp:196-230),
+// then v += (x - x_before) / h when h > 0.
+__global__ void k_shake(ConsArgs C, double* __restrict__ x, const double* __restrict__ x0, double* __restrict__ v, double h, int* counters) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C.ncl) return;
+  const int k0 = C.cl_start[c], k1 = C.cl_start[c + 1], a0 = C.cl_atom0[c], a1 = C.cl_atom0[c + 1];
+  const int na = a1 - a0, nk = k1 - k0;
+  double px[kMaxClAtoms][3], ox[kMaxClAtoms][3], bx[kMaxClAtoms][3], im[kMaxClAtoms];
+  for (int a = 0; a < na; ++a) {
+    const int g = C.cl_atoms[a0 + a];
+    for (int r = 0; r < 3; ++r) px[a][r] = x[3 * g + r], ox[a][r] = x0[3 * g + r], bx[a][r] = px[a][r];
+    im[a] = C.invm[g];
+  }
+  double ref[kMaxClCons][3];
+  int li[kMaxClCons], lj[kMaxClCons];
+  double dd[kMaxClCons];
+  for (int k = 0; k < nk; ++k) {
+    const int4 q = C.cons[k0 + k];
+    li[k] = q.x, lj[k] = q.y;
+    dd[k] = C.d2[k0 + k];
+    double d0 = ox[q.x][0] - ox[q.y][0], d1 = ox[q.x][1] - ox[q.y][1], d2v = ox[q.x][2] - ox[q.y][2];
+    min_image(C.cell, d0, d1, d2v);
+    ref[k][0] = d0, ref[k][1] = d1, ref[k][2] = d2v;
+  }
+  bool done = false;
+  for (int it = 0; it < kShakeIter && !done; ++it) {
+    done = true;
+    for (int k = 0; k < nk; ++k) {
+      const int i = li[k], j = lj[k];
+      double s[3];
+      for (int r = 0; r < 3; ++r) s[r] = ref[k][r] + (px[i][r] - ox[i][r]) - (px[j][r] - ox[j][r]);
+      const double diff = dd[k] - (s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+      if (fabs(diff) <= 2 * kShakeTol * dd[k]) continue;
+      done = false;
+      const double sr = s[0] * ref[k][0] + s[1] * ref[k][1] + s[2] * ref[k][2];
+      if (sr < 1e-6 * dd[k]) {
+        atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), kErrShakeTurn);
+        return;
+      }
+      const double g = diff / (2 * (im[i] + im[j]) * sr);
+      for (int r = 0; r < 3; ++r) {
+        px[i][r] += g * im[i] * ref[k][r];
+        px[j][r] -= g * im[j] * ref[k][r];
+      }
+    }
+  }
+  if (!done) atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), kErrShake);
+  for (int a = 0; a < na; ++a) {
+    const int g = C.cl_atoms[a0 + a];
+    for (int r = 0; r < 3; ++r) {
+      x[3 * g + r] = px[a][r];
+      if (h > 0) v[3 * g + r] += (px[a][r] - bx[a][r]) / h;
+    }
+  }
+}
+
+// RATTLE: removes the relative velocity along each constraint (constraints.cpp:232-269); with h > 0 the impulses are
+// read as forces over a half kick and their virial (xx yy zz xy xz yz) is added to sc[kScCW0..].
+__global__ void k_rattle(ConsArgs C, const double* __restrict__ x, double* __restrict__ v, double h, double* sc, int* counters) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double w[6] = {0, 0, 0, 0, 0, 0};
+  if (c < C.ncl) {
+    const int k0 = C.cl_start[c], k1 = C.cl_start[c + 1], a0 = C.cl_atom0[c], a1 = C.cl_atom0[c + 1];
+    const int na = a1 - a0, nk = k1 - k0;
+    double pv[kMaxClAtoms][3], im[kMaxClAtoms];
+    for (int a = 0; a < na; ++a) {
+      const int g = C.cl_atoms[a0 + a];
+      for (int r = 0; r < 3; ++r) pv[a][r] = v[3 * g + r];
+      im[a] = C.invm[g];
+    }
+    double rr[kMaxClCons][3], lam[kMaxClCons], dd[kMaxClCons];
+    int li[kMaxClCons], lj[kMaxClCons];
+    for (int k = 0; k < nk; ++k) {
+      const int4 q = C.cons[k0 + k];
+      li[k] = q.x, lj[k] = q.y;
+      dd[k] = C.d2[k0 + k];
+      lam[k] = 0;
+      double d0 = x[3 * q.z] - x[3 * q.w], d1 = x[3 * q.z + 1] - x[3 * q.w + 1], d2v = x[3 * q.z + 2] - x[3 * q.w + 2];
+      min_image(C.cell, d0, d1, d2v);
+      rr[k][0] = d0, rr[k][1] = d1, rr[k][2] = d2v;
+    }
+    bool done = false;
+    for (int it = 0; it < kShakeIter && !done; ++it) {
+      done = true;
+      for (int k = 0; k < nk; ++k) {
+        const int i = li[k], j = lj[k];
+        const double rv = rr[k][0] * (pv[i][0] - pv[j][0]) + rr[k][1] * (pv[i][1] - pv[j][1]) + rr[k][2] * (pv[i][2] - pv[j][2]);
+        if (fabs(rv) <= kShakeTol * dd[k]) continue;
+        done = false;
+        const double g = -rv / ((im[i] + im[j]) * dd[k]);
+        lam[k] += g;
+        for (int r = 0; r < 3; ++r) {
+          pv[i][r] += g * im[i] * rr[k][r];
+          pv[j][r] -= g * im[j] * rr[k][r];
+        }
+      }
+    }
+    if (!done) atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), kErrShake);
+    for (int a = 0; a < na; ++a) {
+      const int g = C.cl_atoms[a0 + a];
+      for (int r = 0; r < 3; ++r) v[3 * g + r] = pv[a][r];
+    }
+    if (h > 0)
+      for (int k = 0; k < nk; ++k) {
+        const double s = 2 * lam[k] / (h * kAcc);
+        w[0] += s * rr[k][0] * rr[k][0];
+        w[1] += s * rr[k][1] * rr[k][1];
+        w[2] += s * rr[k][2] * rr[k][2];
+        w[3] += s * rr[k][0] * rr[k][1];
+        w[4] += s * rr[k][0] * rr[k][2];
+        w[5] += s * rr[k][1] * rr[k][2];
+      }
+  }
+  if (h > 0) {
+    __shared__ double scratch[32];
+    for (int q = 0; q < 6; ++q) {
+      const double s = block_sum(w[q], scratch);
+      if (threadIdx.x == 0 && s != 0) atomicAdd(sc + kScCW0 + q, s);
+    }
+  }
+}
+
+// Kinetic energy (and, when asked, the kinetic tensor sum m v_a v_b / kAcc) into partials per block.
+__global__ void k_ke_partial(int n, const double* __restrict__ v, const double* __restrict__ m, double* __restrict__ part, int tensor) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0, t[6] = {0, 0, 0, 0, 0, 0};
+  if (i < n) {
+    const double vx = v[3 * i], vy = v[3 * i + 1], vz = v[3 * i + 2], mi = m[i];
+    e = mi * (vx * vx + vy * vy + vz * vz);
+    if (tensor) t[0] = mi * vx * vx, t[1] = mi * vy * vy, t[2] = mi * vz * vz, t[3] = mi * vx * vy, t[4] = mi * vx * vz, t[5] = mi * vy * vz;
+  }
+  __shared__ double scratch[32];
+  const double s = block_sum(e, scratch);
+  if (threadIdx.x == 0) part[blockIdx.x * 7] = s;
+  if (tensor)
+    for (int q = 0; q < 6; ++q) {
+      const double st = block_sum(t[q], scratch);
+      if (threadIdx.x == 0) part[blockIdx.x * 7 + 1 + q] = st;
+    }
+}
+
+// Sums the partials in block order (deterministic) into sc[slot] = 0.5 sum / kAcc, and the tensor into kScKin0.
+__global__ void k_ke_final(int nparts, const double* __restrict__ part, double* sc, int slot, int tensor) {
+  double e = 0, t[6] = {0, 0, 0, 0, 0, 0};
+  for (int b = threadIdx.x; b < nparts; b += blockDim.x) {
+    e += part[7 * b];
+    if (tensor)
+      for (int q = 0; q < 6; ++q) t[q] += part[7 * b + 1 + q];
+  }
+  __shared__ double scratch[32];
+  const double s = block_sum(e, scratch);
+  if (threadIdx.x == 0) sc[slot] = 0.5 * s / kAcc;
+  if (tensor)
+    for (int q = 0; q < 6; ++q) {
+      const double st = block_sum(t[q], scratch);
+      if (threadIdx.x == 0) sc[kScKin0 + q] = st / kAcc;
+    }
+}
+
+__global__ void k_scale_v(int n, double* __restrict__ v, const double* __restrict__ sc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 3 * n) return;
+  v[i] *= sc[kScFactor];
+}
+
+// The step counter and the thermostat target: T ramps linearly from t0 to t1 over `steps` when t1 >= 0.
+__global__ void k_step_begin(double* sc, double t0, double t1, long long steps, double ndof) {
+  const double step = sc[kScStep] + 1;
+  sc[kScStep] = step;
+  const double t = (t1 >= 0 && steps > 0) ? t0 + (t1 - t0) * step / double(steps) : t0;
+  sc[kScTnow] = t;
+  sc[kScKtarget] = 0.5 * ndof * kB * t;
+}
+
+// Nose-Hoover chain over half a step (LAMMPS FixNH::nhc_temp_integrate, as dynamics.cpp:479-508): sets the velocity
+// factor in sc[kScFactor]; the caller scales v by it.
+__global__ void k_nhc(Chain* ch, double* sc, double ndof, double t_freq, double dt) {
+  const double dthalf = 0.5 * dt, dt4 = 0.25 * dt, dt8 = 0.125 * dt;
+  const double tt = sc[kScTnow], kt = kB * tt, ke_target = ndof * kt;
+  Chain& c = *ch;
+  c.eta_mass[0] = ndof * kt / (t_freq * t_freq);
+  for (int q = 1; q < 3; ++q) c.eta_mass[q] = kt / (t_freq * t_freq);
+  double kecur = 2 * sc[kScKE];
+  c.eta_dotdot[0] = (kecur - ke_target) / c.eta_mass[0];
+  for (int q = 2; q > 0; --q) {
+    const double ex = exp(-dt8 * c.eta_dot[q + 1]);
+    c.eta_dot[q] = (c.eta_dot[q] * ex + c.eta_dotdot[q] * dt4) * ex;
+  }
+  double ex = exp(-dt8 * c.eta_dot[1]);
+  c.eta_dot[0] = (c.eta_dot[0] * ex + c.eta_dotdot[0] * dt4) * ex;
+  const double factor = exp(-dthalf * c.eta_dot[0]);
+  kecur *= factor * factor;
+  c.eta_dotdot[0] = (kecur - ke_target) / c.eta_mass[0];
+  for (int q = 0; q < 3; ++q) c.eta[q] += dthalf * c.eta_dot[q];
+  c.eta_dot[0] = (c.eta_dot[0] * ex + c.eta_dotdot[0] * dt4) * ex;
+  for (int q = 1; q < 3; ++q) {
+    ex = exp(-dt8 * c.eta_dot[q + 1]);
+    c.eta_dot[q] *= ex;
+    c.eta_dotdot[q] = (c.eta_mass[q - 1] * c.eta_dot[q - 1] * c.eta_dot[q - 1] - kt) / c.eta_mass[q];
+    c.eta_dot[q] = (c.eta_dot[q] + c.eta_dotdot[q] * dt4) * ex;
+  }
+  sc[kScFactor] = factor;
+  sc[kScKE] = 0.5 * kecur;
+}
+
+// Bussi velocity rescaling (Bussi, Donadio & Parrinello 2007, appendix; dynamics.cpp:466-477) from this step's draws
+// (r1, sum of ndof - 1 squared normals) read from the host-made table.
+__global__ void k_bussi(double* sc, const double2* __restrict__ draws, long long first_step, double h, double tau, double ndof) {
+  const double k = sc[kScKE];
+  const long long step = (long long)sc[kScStep];
+  if (k <= 0) {
+    sc[kScFactor] = 1;
+    return;
+  }
+  const double2 d = draws[step - first_step];
+  const double c = exp(-h / tau), kt = sc[kScKtarget];
+  const double r1 = d.x, sum = d.y;
+  const double knew = k + (1 - c) * (kt * (r1 * r1 + sum) / ndof - k) + 2 * r1 * sqrt(c * (1 - c) * kt * k / ndof);
+  sc[kScFactor] = sqrt(fmax(knew, 0.0) / k);
+  sc[kScBath] -= knew - k;
+}
+
+// Langevin O step: v = c1 v + c2 sqrt(kB T kAcc / m) N(0, 1), Philox normals keyed by (seed, step, atom)
+__global__ void k_langevin_o(int n, double* __restrict__ v, const double* __restrict__ invm, const double* __restrict__ sc, double c1, double c2,
+                             uint64_t seed) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t step = (uint64_t)sc[kScStep];
+  double z[4];
+  normals4(seed, step, uint32_t(i), 0x4C414E47u, z);
+  const double sd = sqrt(kB * sc[kScTnow] * kAcc * invm[i]);
+  for (int r = 0; r < 3; ++r) v[3 * i + r] = c1 * v[3 * i + r] + c2 * sd * z[r];
+}
+
+// bath -= KE(after) - KE(before)
+__global__ void k_bath_update(double* sc) { sc[kScBath] -= sc[kScKE] - sc[kScKE0]; }
+__global__ void k_copy_slot(double* sc, int dst, int src) { sc[dst] = sc[src]; }
+__global__ void k_zero_cw(double* sc) {
+  for (int q = 0; q < 6; ++q) sc[kScCW0 + q] = 0;
+}
+__global__ void k_remove_com(int n, double* __restrict__ v, const double* __restrict__ p) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int r = 0; r < 3; ++r) v[3 * i + r] -= p[r];
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------------------------
+struct Stepper {
+  Engine& E;
+  const caps_gpu_md_opts& o;
+  int n;
+  DevBuf<double> x, v, x0, invm, m, sc, part;
+  DevBuf<Chain> chain;
+  DevBuf<int> cl_start, cl_atom0, cl_atoms;
+  DevBuf<int4> cons;
+  DevBuf<double> d2;
+  DevBuf<double2> draws;
+  long long draws_first = 0, draws_count = 0;
+  ConsArgs C{};
+  int ncons = 0;
+  double ndof = 0;
+  bool nhc = false, bussi = false, langevin = false;
+  double t_freq = 0;
+  std::unique_ptr<HostRng> rng;
+  double* h_sc = nullptr;
+  Chain* h_chain = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  int nparts = 0;
+
+  Stepper(Engine& e, const caps_gpu_md_opts& md) : E(e), o(md), n(e.n_) {}
+  ~Stepper() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (h_sc) cudaFreeHost(h_sc);
+    if (h_chain) cudaFreeHost(h_chain);
+  }
+
+  // The constraint set of ConstraintMode::HBonds (core/src/constraints.cpp:40-103): every bond to a hydrogen at its r0
+  // (or its present length without one), and rigid waters (an oxygen bonded to exactly two hydrogens: their H-H
+  // distance from r0 and theta0). Connected constraints form a cluster, solved by one thread.
+  void build_constraints(const double* hx) {
+    if (!o.constraints) return;
+    const auto& hm = E.h_mass_;
+    auto is_h = [&](int a) { return o.is_hydrogen ? o.is_hydrogen[a] != 0 : hm[size_t(a)] < 1.6; };
+    auto is_o = [&](int a) { return o.is_oxygen ? o.is_oxygen[a] != 0 : false; };
+    std::vector<std::array<uint32_t, 2>> bonds;
+    std::vector<double> r0;
+    for (size_t k = 0; k < E.hb_.size(); ++k) bonds.push_back(E.hb_[k]), r0.push_back(E.hr0_[k]);
+    std::vector<std::vector<int>> nb(static_cast<size_t>(n));
+    for (auto& b : bonds) nb[b[0]].push_back(int(b[1])), nb[b[1]].push_back(int(b[0]));
+    auto dist = [&](int i, int j) {
+      double d[3] = {hx[3 * j] - hx[3 * i], hx[3 * j + 1] - hx[3 * i + 1], hx[3 * j + 2] - hx[3 * i + 2]};
+      min_image_host(d);
+      return std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    };
+    auto length = [&](int i, int j) {
+      for (size_t k = 0; k < bonds.size(); ++k)
+        if ((int(bonds[k][0]) == i && int(bonds[k][1]) == j) || (int(bonds[k][0]) == j && int(bonds[k][1]) == i))
+          if (r0[k] > 0.3) return r0[k];
+      return dist(i, j);
+    };
+    struct Cn { int i, j; double d; };
+    std::vector<Cn> cs;
+    for (size_t k = 0; k < bonds.size(); ++k) {
+      const int i = int(bonds[k][0]), j = int(bonds[k][1]);
+      if (!(is_h(i) || is_h(j))) continue;
+      cs.push_back({i, j, r0[k] > 0.3 ? r0[k] : dist(i, j)});
+    }
+    for (int ox = 0; ox < n; ++ox) {
+      if (!is_o(ox) || nb[size_t(ox)].size() != 2) continue;
+      const int a = nb[size_t(ox)][0], b = nb[size_t(ox)][1];
+      if (!is_h(a) || !is_h(b)) continue;
+      const double da = length(ox, a), db = length(ox, b);
+      double th = -1;
+      for (size_t k = 0; k < E.ha_.size(); ++k) {
+        const auto& t = E.ha_[k];
+        if (int(t[1]) == ox && ((int(t[0]) == a && int(t[2]) == b) || (int(t[0]) == b && int(t[2]) == a))) th = E.hth0_[k];
+      }
+      if (th < 0) {
+        double u[3] = {hx[3 * a] - hx[3 * ox], hx[3 * a + 1] - hx[3 * ox + 1], hx[3 * a + 2] - hx[3 * ox + 2]};
+        double w[3] = {hx[3 * b] - hx[3 * ox], hx[3 * b + 1] - hx[3 * ox + 1], hx[3 * b + 2] - hx[3 * ox + 2]};
+        min_image_host(u);
+        min_image_host(w);
+        const double c = (u[0] * w[0] + u[1] * w[1] + u[2] * w[2]) /
+                         (std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]) * std::sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]));
+        th = std::acos(std::max(-1.0, std::min(1.0, c)));
+      }
+      cs.push_back({a, b, std::sqrt(da * da + db * db - 2 * da * db * std::cos(th))});
+    }
+    ncons = int(cs.size());
+    if (!ncons) return;
+    // clusters: connected components of the constraint graph
+    std::vector<int> root(static_cast<size_t>(n));
+    for (int i = 0; i < n; ++i) root[size_t(i)] = i;
+    std::function<int(int)> find = [&](int a) { return root[size_t(a)] == a ? a : root[size_t(a)] = find(root[size_t(a)]); };
+    for (auto& c : cs) root[size_t(find(c.i))] = find(c.j);
+    std::map<int, std::vector<int>> comp_cons;
+    for (int k = 0; k < ncons; ++k) comp_cons[find(cs[size_t(k)].i)].push_back(k);
+    std::vector<int> st{0}, a0{0}, atoms;
+    std::vector<int4> cv;
+    std::vector<double> dv;
+    for (auto& [r, ks] : comp_cons) {
+      std::vector<int> loc;
+      auto local = [&](int a) {
+        for (size_t q = 0; q < loc.size(); ++q)
+          if (loc[q] == a) return int(q);
+        loc.push_back(a);
+        return int(loc.size() - 1);
+      };
+      for (int k : ks) {
+        const Cn& c = cs[size_t(k)];
+        const int li = local(c.i), lj = local(c.j);
+        cv.push_back(make_int4(li, lj, c.i, c.j));
+        dv.push_back(c.d * c.d);
+      }
+      if (int(ks.size()) > kMaxClCons || int(loc.size()) > kMaxClAtoms)
+        throw ModelError(CAPS_GPU_EINVAL, "a constraint cluster has more than 8 atoms or constraints (the device SHAKE takes bonds to hydrogen and rigid waters)");
+      atoms.insert(atoms.end(), loc.begin(), loc.end());
+      st.push_back(int(cv.size()));
+      a0.push_back(int(atoms.size()));
+    }
+    cl_start.upload(st, E.stream_);
+    cl_atom0.upload(a0, E.stream_);
+    cl_atoms.upload(atoms, E.stream_);
+    cons.upload(cv, E.stream_);
+    d2.upload(dv, E.stream_);
+    C.ncl = int(st.size()) - 1;
+    C.cl_start = cl_start.p;
+    C.cl_atom0 = cl_atom0.p;
+    C.cl_atoms = cl_atoms.p;
+    C.cons = cons.p;
+    C.d2 = d2.p;
+    C.invm = invm.p;
+    CK(cudaStreamSynchronize(E.stream_));
+  }
+
+  void min_image_host(double* d) const {
+    const DevCell& c = E.dcell_;
+    double f[3];
+    for (int r = 0; r < 3; ++r) {
+      f[r] = c.hi[r][0] * d[0] + c.hi[r][1] * d[1] + c.hi[r][2] * d[2];
+      f[r] -= std::nearbyint(f[r]);
+    }
+    for (int r = 0; r < 3; ++r) d[r] = c.h[r][0] * f[0] + c.h[r][1] * f[1] + c.h[r][2] * f[2];
+  }
+
+  // --- step pieces (all asynchronous on E.stream_) ---
+  void ke(int slot, bool tensor) {
+    k_ke_partial<<<nparts, 256, 0, E.stream_>>>(n, v.p, m.p, part.p, tensor ? 1 : 0);
+    k_ke_final<<<1, 256, 0, E.stream_>>>(nparts, part.p, sc.p, slot, tensor ? 1 : 0);
+  }
+  void kick(double h) { k_kick<<<blocks(size_t(n), 256), 256, 0, E.stream_>>>(n, v.p, E.d_f_.p, invm.p, h); }
+  void drift(double h) {
+    k_drift<<<blocks(size_t(3) * n, 256), 256, 0, E.stream_>>>(n, x.p, v.p, x0.p, h, E.d_counters_.p);
+    if (ncons) k_shake<<<blocks(size_t(C.ncl), 128), 128, 0, E.stream_>>>(C, x.p, x0.p, v.p, h, E.d_counters_.p);
+  }
+  void rattle(double h) {
+    if (!ncons) return;
+    if (h > 0) k_zero_cw<<<1, 1, 0, E.stream_>>>(sc.p);
+    k_rattle<<<blocks(size_t(C.ncl), 128), 128, 0, E.stream_>>>(C, x.p, v.p, h, sc.p, E.d_counters_.p);
+  }
+  void scale_v() { k_scale_v<<<blocks(size_t(3) * n, 256), 256, 0, E.stream_>>>(n, v.p, sc.p); }
+  void nhc_half(double dt) {
+    ke(kScKE, false);
+    k_nhc<<<1, 1, 0, E.stream_>>>(chain.p, sc.p, ndof, t_freq, dt);
+    scale_v();
+  }
+  void forces(bool ener, bool vir) { E.forces(x.p, ener, vir, true); }
+
+  // One MD step (dynamics.cpp:606-666), energies and virial on request.
+  void step(bool ener, bool vir) {
+    const double dt = o.dt;
+    k_step_begin<<<1, 1, 0, E.stream_>>>(sc.p, o.temperature, o.temperature_end, (long long)o.steps, ndof);
+    if (langevin) {
+      const double c1 = std::exp(-dt / std::max(o.tau_t, 1e-9)), c2 = std::sqrt(1 - c1 * c1);
+      kick(0.5 * dt);
+      drift(0.5 * dt);
+      ke(kScKE0, false);
+      k_langevin_o<<<blocks(size_t(n), 256), 256, 0, E.stream_>>>(n, v.p, invm.p, sc.p, c1, c2, o.seed);
+      rattle(0);
+      ke(kScKE, false);
+      k_bath_update<<<1, 1, 0, E.stream_>>>(sc.p);
+      drift(0.5 * dt);
+      forces(ener, vir);
+      kick(0.5 * dt);
+      rattle(dt);
+    } else if (nhc) {
+      nhc_half(dt);
+      kick(0.5 * dt);
+      drift(dt);
+      forces(ener, vir);
+      kick(0.5 * dt);
+      rattle(dt);
+      nhc_half(dt);
+    } else {
+      kick(0.5 * dt);
+      drift(dt);
+      forces(ener, vir);
+      kick(0.5 * dt);
+      rattle(dt);
+      if (bussi) {
+        ke(kScKE, false);
+        k_bussi<<<1, 1, 0, E.stream_>>>(sc.p, draws.p, draws_first, dt, o.tau_t, ndof);
+        scale_v();
+      }
+    }
+  }
+
+  // Bussi draws for steps [first, first + count): r1 = gauss, then the chi-squared of ndof - 1 by a fresh Gamma
+  void make_draws(long long first, long long count) {
+    std::vector<double2> d(static_cast<size_t>(count));
+    for (long long s = 0; s < count; ++s) {
+      const double r1 = rng->gauss();
+      const double sum = ndof > 1 ? rng->gamma((ndof - 1) / 2, 2.0) : 0.0;
+      d[size_t(s)] = make_double2(r1, sum);
+    }
+    draws.upload(d, E.stream_);
+    draws_first = first;
+    draws_count = count;
+  }
+};
+
+void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progress_fn progress, caps_gpu_frame_fn frame, void* user, std::string* report) {
+  const caps_gpu_md_opts& o = *md;
+  if (n_ < 2) throw ModelError(CAPS_GPU_EFIELD, "dynamics needs at least two atoms");
+  if (o.dt <= 0 || o.dt > 50) throw ModelError(CAPS_GPU_EINVAL, "time step must be in (0, 50] fs");
+  if (o.steps < 0) throw ModelError(CAPS_GPU_EINVAL, "the number of steps must be 0 or more");
+  if (o.respa > 1) throw ModelError(CAPS_GPU_EINVAL, "r-RESPA is not on the device path yet");
+  if (o.thermostat < 0 || o.thermostat > 3) throw ModelError(CAPS_GPU_EINVAL, "unknown thermostat");
+  if (o.barostat != 0 && o.barostat != 1) throw ModelError(CAPS_GPU_EINVAL, "the device path takes stochastic cell rescaling or no barostat");
+  if (o.barostat == 1 && o.thermostat == 0) throw ModelError(CAPS_GPU_EINVAL, "stochastic cell rescaling needs a thermostat");
+  set_cell(st->cell);
+  Stepper S(*this, o);
+  const size_t n3 = size_t(3) * n_;
+  S.x.upload(st->x, n3, stream_);
+  S.x0.alloc(n3);
+  S.v.alloc(n3);
+  S.m.upload(h_mass_, stream_);
+  std::vector<double> im(static_cast<size_t>(n_));
+  for (int i = 0; i < n_; ++i) im[size_t(i)] = h_mass_[size_t(i)] > 0 ? 1.0 / h_mass_[size_t(i)] : 0.0;
+  S.invm.upload(im, stream_);
+  S.sc.alloc(kScNum);
+  S.sc.zero(stream_);
+  S.chain.alloc(1);
+  CK(cudaMemsetAsync(S.chain.p, 0, sizeof(Chain), stream_));
+  S.nparts = blocks(size_t(n_), 256);
+  S.part.alloc(size_t(7) * S.nparts);
+  CK(cudaMallocHost(&S.h_sc, sizeof(double) * kScNum));
+  CK(cudaMallocHost(&S.h_chain, sizeof(Chain)));
+  S.nhc = o.thermostat == 3;
+  S.bussi = o.thermostat == 1;
+  S.langevin = o.thermostat == 2;
+  S.t_freq = 1.0 / std::max(o.tau_t, 1e-9);
+  S.C.cell = dcell_;
+  S.build_constraints(st->x);
+  S.ndof = 3.0 * double(n_) - 3.0 - double(S.ncons);
+  if (S.ndof < 1) throw ModelError(CAPS_GPU_EINVAL, "the constraints leave no degree of freedom");
+  S.rng = std::make_unique<HostRng>(o.seed);
+  if (S.ncons) {   // the constrained lengths hold from the start (dynamics.cpp:198-203)
+    CK(cudaMemcpyAsync(S.x0.p, S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    k_shake<<<blocks(size_t(S.C.ncl), 128), 128, 0, stream_>>>(S.C, S.x.p, S.x0.p, S.v.p, 0.0, d_counters_.p);
+  }
+
+  // velocities: given, or Maxwell-Boltzmann from the reference's stream, no centre-of-mass motion, rescaled to T
+  std::vector<double> hv(n3, 0.0);
+  auto host_ke = [&](const std::vector<double>& vv) {
+    double k = 0;
+    for (int i = 0; i < n_; ++i) k += h_mass_[size_t(i)] * (vv[3 * i] * vv[3 * i] + vv[3 * i + 1] * vv[3 * i + 1] + vv[3 * i + 2] * vv[3 * i + 2]);
+    return 0.5 * k / kAcc;
+  };
+  const bool drawn = !(st->has_velocities && st->v && !o.new_velocities);
+  if (!drawn) {
+    std::memcpy(hv.data(), st->v, n3 * sizeof(double));
+  } else {
+    for (int i = 0; i < n_; ++i) {
+      const double sd = std::sqrt(kB * o.temperature * kAcc / h_mass_[size_t(i)]);
+      for (int k = 0; k < 3; ++k) hv[3 * size_t(i) + k] = sd * S.rng->gauss();
+    }
+    double p[3] = {0, 0, 0}, mf = 0;
+    for (int i = 0; i < n_; ++i) {
+      mf += h_mass_[size_t(i)];
+      for (int k = 0; k < 3; ++k) p[k] += h_mass_[size_t(i)] * hv[3 * size_t(i) + k];
+    }
+    for (int i = 0; i < n_; ++i)
+      for (int k = 0; k < 3; ++k) hv[3 * size_t(i) + k] -= p[k] / mf;
+  }
+  S.v.upload(hv, stream_);
+  if (drawn) {
+    if (S.ncons) S.rattle(0);
+    CK(cudaMemcpyAsync(hv.data(), S.v.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    const double t0 = 2 * host_ke(hv) / (S.ndof * kB);
+    if (t0 > 0)
+      for (auto& q : hv) q *= std::sqrt(o.temperature / t0);
+    S.v.upload(hv, stream_);
+  }
+  if (S.ncons) S.rattle(0);
+  if (S.bussi) S.make_draws(1, std::min<long long>(std::max<long long>(o.steps, 1), 4096));
+
+  // the first force, energies and virial
+  auto row = [&](long long step, caps_gpu_thermo& r) {
+    caps_gpu_terms t{};
+    read_terms(&t, true, true);
+    const double* sc = S.h_sc;
+    for (int c = 0; c < 6; ++c) t.w[c] += sc[kScCW0 + c];
+    t.virial = t.w[0] + t.w[1] + t.w[2];
+    std::memset(&r, 0, sizeof r);
+    r.step = step + o.step_offset;
+    r.time_ps = double(step + o.step_offset) * o.dt * 1e-3;
+    r.target_temperature = (o.temperature_end >= 0 && o.steps > 0) ? o.temperature + (o.temperature_end - o.temperature) * double(step) / double(o.steps)
+                                                                  : o.temperature;
+    r.kinetic = sc[kScKE];
+    r.temperature = 2 * r.kinetic / (S.ndof * kB);
+    r.potential = t.bond + t.angle + t.dihedral + t.improper + t.vdw + t.coulomb;
+    r.total = r.potential + r.kinetic;
+    r.volume = dcell_.vol;
+    double mtot = 0;
+    for (double mm : h_mass_) mtot += mm;
+    r.density = mtot / kNA / (r.volume * 1e-24);
+    r.pressure = (2 * r.kinetic + t.virial) / (3 * r.volume) * kAtm;
+    for (int c = 0; c < 6; ++c) r.p[c] = (sc[kScKin0 + c] + t.w[c]) / r.volume * kAtm;
+    if (S.nhc) {
+      const Chain& ch = *S.h_chain;
+      const double kt = kB * r.target_temperature;
+      double e = S.ndof * kt * ch.eta[0] + 0.5 * ch.eta_mass[0] * ch.eta_dot[0] * ch.eta_dot[0];
+      for (int c = 1; c < 3; ++c) e += kt * ch.eta[c] + 0.5 * ch.eta_mass[c] * ch.eta_dot[c] * ch.eta_dot[c];
+      r.conserved = r.total + e;
+    } else {
+      r.conserved = r.total + sc[kScBath] + (o.barostat ? o.pressure * r.volume / kAtm : 0.0);
+    }
+    r.terms = t;
+  };
+  auto sync_scalars = [&]() {
+    CK(cudaMemcpyAsync(S.h_sc, S.sc.p, sizeof(double) * kScNum, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(S.h_chain, S.chain.p, sizeof(Chain), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(h_counters_, d_counters_.p, sizeof(int) * kCntNum, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(h_efix_, d_efix_.p, sizeof(long long) * kENumSlots, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(h_edbl_, d_edbl_.p, sizeof(double) * kENumSlots, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    check_errors();
+  };
+  auto emit = [&](long long step) {
+    S.ke(kScKE, true);
+    sync_scalars();
+    caps_gpu_thermo r;
+    row(step, r);
+    if (progress && progress(&r, user) != 0) throw ModelError(CAPS_GPU_ECANCEL, "dynamics cancelled");
+  };
+  auto emit_frame = [&](long long step) {
+    if (!frame || o.frame_every <= 0) return;
+    std::vector<double> hx(n3);
+    CK(cudaMemcpyAsync(hx.data(), S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    frame(hx.data(), cell_h_, step + o.step_offset, user);
+  };
+
+  S.forces(true, true);
+  if (S.ncons) {
+    // step 0's constraint virial from one trial step on copies (dynamics.cpp:582-600)
+    DevBuf<double> xs, vs;
+    xs.alloc(n3);
+    vs.alloc(n3);
+    CK(cudaMemcpyAsync(xs.p, S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    CK(cudaMemcpyAsync(vs.p, S.v.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    S.kick(0.5 * o.dt);
+    S.drift(o.dt);
+    S.kick(0.5 * o.dt);
+    S.rattle(o.dt);
+    CK(cudaMemcpyAsync(S.x.p, xs.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    CK(cudaMemcpyAsync(S.v.p, vs.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    CK(cudaStreamSynchronize(stream_));
+  }
+  emit(0);
+  emit_frame(0);
+
+  // the step loop: plain steps replay a captured graph; thermo / frame / barostat steps run uncaptured
+  const int thermo_every = std::max(1, o.thermo_every);
+  const int baro_every = std::max(1, o.barostat_every);
+  auto special = [&](long long s) {
+    return s % thermo_every == 0 || s == o.steps || (o.frame_every > 0 && s % o.frame_every == 0) || (o.barostat && s % baro_every == 0) ||
+           (S.bussi && s - S.draws_first >= S.draws_count);
+  };
+  cudaEvent_t ev0, ev1;
+  CK(cudaEventCreate(&ev0));
+  CK(cudaEventCreate(&ev1));
+  const auto w0 = std::chrono::steady_clock::now();
+  CK(cudaEventRecord(ev0, stream_));
+  bool have_graph = false;
+  for (long long s = 1; s <= o.steps; ++s) {
+    if (S.bussi && s - S.draws_first >= S.draws_count) {
+      CK(cudaStreamSynchronize(stream_));
+      S.make_draws(s, std::min<long long>(o.steps - s + 1, 4096));
+      if (S.graph) {
+        cudaGraphExecDestroy(S.graph);
+        S.graph = nullptr;
+        have_graph = false;
+      }
+    }
+    if (!special(s)) {
+      if (!have_graph) {
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        S.step(false, false);
+        CK(cudaStreamEndCapture(stream_, &g));
+        CK(cudaGraphInstantiate(&S.graph, g, 0));
+        CK(cudaGraphDestroy(g));
+        have_graph = true;
+      }
+      CK(cudaGraphLaunch(S.graph, stream_));
+      continue;
+    }
+    const bool baro = o.barostat && s % baro_every == 0;
+    S.step(true, true);
+    if (baro) {
+      // stochastic cell rescaling (Bernetti & Bussi 2020, dynamics.cpp:684-723), isotropic
+      S.ke(kScKE, true);
+      sync_scalars();
+      caps_gpu_terms t{};
+      read_terms(&t, true, true);
+      for (int c = 0; c < 6; ++c) t.w[c] += S.h_sc[kScCW0 + c];
+      t.virial = t.w[0] + t.w[1] + t.w[2];
+      const double k = S.h_sc[kScKE], vol = dcell_.vol;
+      const double p = (2 * k + t.virial) / (3 * vol) * kAtm;
+      const double hp = o.dt * baro_every;
+      const double tnow = S.h_sc[kScTnow];
+      double deps = -o.compressibility / o.tau_p * (o.pressure - p) * hp;
+      const double ktv = kB * tnow / vol * kAtm;
+      deps += o.compressibility / o.tau_p * ktv * hp + std::sqrt(2 * ktv * o.compressibility * hp / o.tau_p) * S.rng->gauss();
+      deps = std::max(-0.01, std::min(0.01, deps));
+      const double mu = std::exp(deps / 3);
+      std::vector<double> hx(n3);
+      CK(cudaMemcpyAsync(hx.data(), S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+      CK(cudaMemcpyAsync(hv.data(), S.v.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+      CK(cudaStreamSynchronize(stream_));
+      double cell[12];
+      std::memcpy(cell, cell_h_, sizeof cell);
+      for (int i = 0; i < n_; ++i)
+        for (int c = 0; c < 3; ++c) hx[3 * size_t(i) + c] = cell[c] + mu * (hx[3 * size_t(i) + c] - cell[c]);
+      for (int q = 3; q < 12; ++q) cell[q] *= mu;
+      for (auto& q : hv) q /= mu;
+      const double k2 = host_ke(hv);
+      S.h_sc[kScBath] -= k2 - k;
+      CK(cudaMemcpyAsync(S.sc.p + kScBath, S.h_sc + kScBath, sizeof(double), cudaMemcpyHostToDevice, stream_));
+      S.x.upload(hx, stream_);
+      S.v.upload(hv, stream_);
+      set_cell(cell);
+      S.C.cell = dcell_;
+      if (S.ncons) {
+        CK(cudaMemcpyAsync(S.x0.p, S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+        k_shake<<<blocks(size_t(S.C.ncl), 128), 128, 0, stream_>>>(S.C, S.x.p, S.x0.p, S.v.p, 0.0, d_counters_.p);
+        S.rattle(0);
+      }
+      S.forces(true, true);
+      if (S.graph) {
+        cudaGraphExecDestroy(S.graph);
+        S.graph = nullptr;
+        have_graph = false;
+      }
+    }
+    if (s % thermo_every == 0 || s == o.steps) emit(s);
+    if (o.frame_every > 0 && (s % o.frame_every == 0 || s == o.steps)) emit_frame(s);
+  }
+  CK(cudaEventRecord(ev1, stream_));
+  CK(cudaEventSynchronize(ev1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, ev0, ev1));
+  const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  sync_scalars();
+  last_sps_ = o.steps > 0 && ms > 0 ? double(o.steps) / (ms * 1e-3) : 0.0;
+  // state back to the caller
+  CK(cudaMemcpyAsync(st->x, S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  if (st->v) CK(cudaMemcpyAsync(st->v, S.v.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  CK(cudaStreamSynchronize(stream_));
+  std::memcpy(st->cell, cell_h_, sizeof cell_h_);
+  if (report) {
+    char b[400];
+    const double nsday = wall > 0 ? double(o.steps) * o.dt * 1e-6 / wall * 86400 : 0.0;
+    std::snprintf(b, sizeof b, "%lld steps of %.2f fs in %.3f s (device %.3f s) · %.2f ns/day · %d constraints · %.0f degrees of freedom · %s",
+                  (long long)o.steps, o.dt, wall, ms * 1e-3, nsday, S.ncons, S.ndof, mixed_ ? "mixed FP32/fixed-point" : "FP64");
+    *report = b;
+  }
+}
+
+}  // namespace capsb

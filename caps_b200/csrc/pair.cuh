@@ -1,0 +1,414 @@
+// K-PACK and K-PAIR: the LJ 12-6 plus real-space Coulomb pair kernels over the cluster pair list.
+//
+// Reference: the FP64 atom-pair loop (core/src/field.cpp:1604-1686: 12-6 LJ with the cut-off shift, Ewald real space
+// from the cubic-Hermite table of erf(kappa sqrt s)/sqrt s, field.cpp:1126-1157 and 1593-1602, DSF) and the FP32
+// cluster kernel (core/src/nbnxm.cpp:408-567). Excluded pairs are left out of the list (their Ewald / DSF corrections
+// are the bonded-phase kernel's, as the reference's FP64 path does at field.cpp:2206-2266).
+//
+// One warp per work item: a super-cluster of 64 i atoms (8 clusters, kept in shared memory) against up to 32 j
+// clusters. Lane l takes i atom l & 7 of every i cluster and j atoms (l >> 3) and (l >> 3) + 4 of each j cluster, so a
+// j cluster costs one 128-byte line and its forces are reduced over 8 lanes once per entry, after all 8 i clusters.
+// FP32 path: float arithmetic, positions relative to super-cluster origins (the shift of an entry carries the origins'
+// difference, so single precision keeps its digits), forces and energies summed as 64-bit fixed point.
+// FP64 path: double arithmetic on wrapped absolute positions, the reference's Hermite table for the Ewald term.
+#pragma once
+#include "common.cuh"
+#include "nblist.cuh"
+
+namespace capsb {
+
+constexpr float kPadFar = 1.0e5f;   // padding slots sit this far from their super-cluster's origin (never within reach)
+
+// K-PACK (FP32): per slot, float4 (position relative to the super-cluster origin, charge) and the type index.
+static __global__ void k_pack_f32(int nslots, const int* __restrict__ perm, const double* __restrict__ x, const int* __restrict__ ioff, DevCell cell,
+                           const double* __restrict__ sc_org, const double* __restrict__ q, const int* __restrict__ type, int pad_type,
+                           float4* __restrict__ xq, int* __restrict__ tslot, const int* counters) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nsc = counters[kCntNsc];
+  if (s >= nslots || s >= 64 * nsc) return;
+  const int a = perm[s];
+  if (a < 0) {
+    xq[s] = make_float4(0.f, 0.f, kPadFar, 0.f);
+    tslot[s] = pad_type;
+    return;
+  }
+  const int sc = s >> 6;
+  const int o0 = ioff[3 * a], o1 = ioff[3 * a + 1], o2 = ioff[3 * a + 2];
+  float p[3];
+  for (int r = 0; r < 3; ++r)
+    p[r] = float(x[3 * a + r] + (cell.h[r][0] * o0 + cell.h[r][1] * o1 + cell.h[r][2] * o2) - sc_org[3 * sc + r]);
+  xq[s] = make_float4(p[0], p[1], p[2], float(q[a]));
+  tslot[s] = type[a];
+}
+
+// K-PACK (FP64): per slot, double4 (wrapped absolute position, charge) and the type index.
+static __global__ void k_pack_f64(int nslots, const int* __restrict__ perm, const double* __restrict__ x, const int* __restrict__ ioff, DevCell cell,
+                           const double* __restrict__ q, const int* __restrict__ type, int pad_type, double4* __restrict__ xq, int* __restrict__ tslot,
+                           const int* counters) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nsc = counters[kCntNsc];
+  if (s >= nslots || s >= 64 * nsc) return;
+  const int a = perm[s];
+  if (a < 0) {
+    xq[s] = make_double4(1e7, 1e7, 1e7 + 16.0 * (s & 63), 0.0);
+    tslot[s] = pad_type;
+    return;
+  }
+  const int o0 = ioff[3 * a], o1 = ioff[3 * a + 1], o2 = ioff[3 * a + 2];
+  double p[3];
+  for (int r = 0; r < 3; ++r) p[r] = x[3 * a + r] + (cell.h[r][0] * o0 + cell.h[r][1] * o1 + cell.h[r][2] * o2);
+  xq[s] = make_double4(p[0], p[1], p[2], q[a]);
+  tslot[s] = type[a];
+}
+
+struct PairArgs {
+  const int4* work;
+  const uint4* ent;
+  const float4* ent_shift;
+  const unsigned long long* masks;
+  const int* counters;
+  const int* tslot;
+  const float4* xq;      // FP32 path
+  const double4* xqd;    // FP64 path
+  const float4* tab;     // FP32: per type pair (c6, c12, energy shift, 0)
+  const double4* tabd;   // FP64: per type pair (c6, c12, energy shift, 0)
+  const double* gtab;    // FP64 Ewald table: 2 per node (G, h dG/ds)
+  int ntab;              // types incl. the padding type
+  int gnodes;            // table nodes
+  double ghi;            // 1 / node spacing
+  DevCell cell;
+  double rc2, rc, beta, kc, kcoul, dsf_e0, dsf_f0;
+  long long* fsx;        // slot-order force sums (FP32 path: fixed point)
+  long long* fsy;
+  long long* fsz;
+  double* fdx;           // slot-order force sums (FP64 path)
+  double* fdy;
+  double* fdz;
+  EnergySink en;
+  int work_cap;
+};
+
+// --- FP32 path ---------------------------------------------------------------------------------------------------
+// COUL: 0 none, 1 Ewald real space (PME), 2 damped shifted force.
+template <int COUL, bool ENER, bool VIR>
+static __global__ void __launch_bounds__(128, 4) k_pair_f32(PairArgs A) {
+  extern __shared__ float4 smem_f4[];
+  float4* tab = smem_f4;                                  // ntab * ntab
+  float4* s_xi = smem_f4 + A.ntab * A.ntab;               // 4 warps x 64
+  int* s_ti = reinterpret_cast<int*>(s_xi + 4 * 64);      // 4 warps x 64
+  for (int t = threadIdx.x; t < A.ntab * A.ntab; t += blockDim.x) tab[t] = A.tab[t];
+  __syncthreads();
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i8 = lane & 7, jq = lane >> 3;
+  float4* xi_s = s_xi + 64 * wib;
+  int* ti_s = s_ti + 64 * wib;
+  // a list build that ran out of room leaves stale work items: skip the pass, the host reports the error
+  if (A.counters[kCntErr] & (kErrListOverflow | kErrMaskOverflow | kErrScOverflow | kErrColumnTooBig | kErrExclOverflow)) return;
+  const int nwork = min(A.counters[kCntWork], A.work_cap);
+  const int pad = A.ntab - 1;
+  const float rc2 = float(A.rc2), beta = float(A.beta), kc = float(A.kc), kcoul = float(A.kcoul);
+  const float e0 = float(A.dsf_e0), f0 = float(A.dsf_f0), rcf = float(A.rc);
+  const int nwarps = gridDim.x * 4;
+  double acc_v = 0, acc_c = 0, acc_w[6] = {0, 0, 0, 0, 0, 0};
+  for (int w = blockIdx.x * 4 + wib; w < nwork; w += nwarps) {
+    const int4 wk = A.work[w];
+    const int sc = wk.x;
+    for (int t = lane; t < 64; t += 32) {
+      float4 v = A.xq[64 * sc + t];
+      v.w *= kcoul;
+      xi_s[t] = v;
+      ti_s[t] = A.tslot[64 * sc + t];
+    }
+    __syncwarp();
+    unsigned ireal = 0;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) ireal |= unsigned(ti_s[8 * c + i8] != pad) << c;
+    float fix[8], fiy[8], fiz[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) fix[c] = fiy[c] = fiz[c] = 0.f;
+    float ev = 0.f, ec = 0.f, vw[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int e = wk.y; e < wk.y + wk.z; ++e) {
+      const uint4 en = A.ent[e];
+      const float4 sh = A.ent_shift[e];
+      const int cj = int(en.x);
+      const unsigned imask = en.y & 255u;
+      const int j0 = 8 * cj + jq, j1 = j0 + 4;
+      const float4 a0 = A.xq[j0], a1 = A.xq[j1];
+      const int t0 = A.tslot[j0], t1 = A.tslot[j1];
+      const float xj0 = a0.x + sh.x, yj0 = a0.y + sh.y, zj0 = a0.z + sh.z;
+      const float xj1 = a1.x + sh.x, yj1 = a1.y + sh.y, zj1 = a1.z + sh.z;
+      float f0x = 0.f, f0y = 0.f, f0z = 0.f, f1x = 0.f, f1y = 0.f, f1z = 0.f;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        if (!((imask >> c) & 1u)) continue;
+        const unsigned long long mm = en.z ? A.masks[8 * size_t(en.z - 1) + c] : ~0ull;
+        const float4 xi = xi_s[8 * c + i8];
+        const int ti = ti_s[8 * c + i8];
+        const bool oki = (ireal >> c) & 1u;
+#pragma unroll
+        for (int jj = 0; jj < 2; ++jj) {
+          const float xj = jj ? xj1 : xj0, yj = jj ? yj1 : yj0, zj = jj ? zj1 : zj0;
+          const float qj = jj ? a1.w : a0.w;
+          const int tj = jj ? t1 : t0;
+          const int bit = 8 * i8 + jq + 4 * jj;
+          const float dx = xj - xi.x, dy = yj - xi.y, dz = zj - xi.z;
+          const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+          const bool ok = oki && ((mm >> bit) & 1ull) && (r2 < rc2);
+          const float r2s = ok ? r2 : 1.f;
+          const float rinv = rsqrtf(r2s);
+          const float r2i = rinv * rinv;
+          const float r6i = r2i * r2i * r2i;
+          const float4 cc = tab[ti * A.ntab + tj];
+          const float a12 = cc.y * r6i;
+          float fr = r6i * fmaf(12.f, a12, -6.f * cc.x) * r2i;
+          if (ENER) ev += ok ? fmaf(r6i, a12 - cc.x, -cc.z) : 0.f;
+          if (COUL != 0) {
+            const float qq = xi.w * qj;
+            const float r = r2s * rinv;
+            const float br = beta * r;
+            const float erfcv = erfcf(br);
+            const float ex = __expf(-br * br);
+            float fc = qq * fmaf(erfcv, rinv, kc * ex) * r2i;
+            if (COUL == 2) fc -= qq * f0 * rinv;
+            fr += fc;
+            if (ENER) {
+              float ecp = qq * erfcv * rinv;
+              if (COUL == 2) ecp += qq * (f0 * (r - rcf) - e0);
+              ec += ok ? ecp : 0.f;
+            }
+          }
+          fr = ok ? fr : 0.f;
+          const float fx = fr * dx, fy = fr * dy, fz = fr * dz;
+          if (jj) f1x += fx, f1y += fy, f1z += fz;
+          else f0x += fx, f0y += fy, f0z += fz;
+          fix[c] -= fx;
+          fiy[c] -= fy;
+          fiz[c] -= fz;
+          if (VIR) {
+            vw[0] = fmaf(fx, dx, vw[0]);
+            vw[1] = fmaf(fy, dy, vw[1]);
+            vw[2] = fmaf(fz, dz, vw[2]);
+            vw[3] = fmaf(fx, dy, vw[3]);
+            vw[4] = fmaf(fx, dz, vw[4]);
+            vw[5] = fmaf(fy, dz, vw[5]);
+          }
+        }
+      }
+      // j forces: sum over the 8 lanes holding the same j atoms, then one fixed-point add per component
+#pragma unroll
+      for (int o = 1; o < 8; o <<= 1) {
+        f0x += __shfl_xor_sync(0xffffffffu, f0x, o);
+        f0y += __shfl_xor_sync(0xffffffffu, f0y, o);
+        f0z += __shfl_xor_sync(0xffffffffu, f0z, o);
+        f1x += __shfl_xor_sync(0xffffffffu, f1x, o);
+        f1y += __shfl_xor_sync(0xffffffffu, f1y, o);
+        f1z += __shfl_xor_sync(0xffffffffu, f1z, o);
+      }
+      if (i8 < 6) {
+        const float v = i8 == 0 ? f0x : i8 == 1 ? f0y : i8 == 2 ? f0z : i8 == 3 ? f1x : i8 == 4 ? f1y : f1z;
+        const int js = i8 < 3 ? j0 : j1;
+        long long* dst = (i8 % 3 == 0) ? A.fsx : (i8 % 3 == 1) ? A.fsy : A.fsz;
+        if (v != 0.f) atomic_add_fix(dst + js, to_fixf(v));
+      }
+    }
+    // i forces: sum over the 4 lanes of each i atom, then lanes share the adds
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      fix[c] += __shfl_xor_sync(0xffffffffu, fix[c], 8);
+      fiy[c] += __shfl_xor_sync(0xffffffffu, fiy[c], 8);
+      fiz[c] += __shfl_xor_sync(0xffffffffu, fiz[c], 8);
+      fix[c] += __shfl_xor_sync(0xffffffffu, fix[c], 16);
+      fiy[c] += __shfl_xor_sync(0xffffffffu, fiy[c], 16);
+      fiz[c] += __shfl_xor_sync(0xffffffffu, fiz[c], 16);
+    }
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      if ((c & 3) != jq || !((ireal >> c) & 1u)) continue;
+      const int s = 64 * sc + 8 * c + i8;
+      if (fix[c] != 0.f) atomic_add_fix(A.fsx + s, to_fixf(fix[c]));
+      if (fiy[c] != 0.f) atomic_add_fix(A.fsy + s, to_fixf(fiy[c]));
+      if (fiz[c] != 0.f) atomic_add_fix(A.fsz + s, to_fixf(fiz[c]));
+    }
+    if (ENER) {
+      acc_v += double(warp_sum(ev));
+      acc_c += double(warp_sum(ec));
+    }
+    if (VIR)
+      for (int k = 0; k < 6; ++k) acc_w[k] += double(warp_sum(vw[k]));
+    __syncwarp();
+  }
+  if (lane == 0) {
+    if (ENER) {
+      A.en.add(kEVdw, acc_v, true);
+      A.en.add(kECoul, acc_c, true);
+    }
+    if (VIR)
+      for (int k = 0; k < 6; ++k) A.en.add(kEW0 + k, acc_w[k], true);
+  }
+}
+
+// --- FP64 path ---------------------------------------------------------------------------------------------------
+// The reference's ewald_ef (field.cpp:1593-1602): E = 1/r - G(s), F = 1/r^3 + 2 dG/ds by cubic Hermite interpolation.
+__device__ __forceinline__ void ewald_ef(const double* __restrict__ gt, double ghi, double s, double rinv, double& E, double& F) {
+  const double u = s * ghi;
+  const int k = int(u);
+  const double t = u - double(k), t2 = t * t;
+  const double g0 = gt[2 * k], g1 = gt[2 * k + 1], g2 = gt[2 * k + 2], g3 = gt[2 * k + 3];
+  const double G = g0 + t2 * (3 - 2 * t) * (g2 - g0) + t * (1 - t) * ((1 - t) * g1 - t * g3);
+  const double dG = (6 * t * (1 - t) * (g2 - g0) * ghi) + (1 - t) * (1 - 3 * t) * g1 * ghi + t * (3 * t - 2) * g3 * ghi;
+  E = rinv - G;
+  F = rinv * rinv * rinv + 2 * dG;
+}
+
+template <int COUL, bool ENER, bool VIR>
+static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
+  extern __shared__ double4 smem_d4[];
+  double4* tab = smem_d4;                                   // ntab * ntab
+  double* gt = reinterpret_cast<double*>(tab + A.ntab * A.ntab);   // 2 * gnodes
+  double4* s_xi = reinterpret_cast<double4*>(gt + 2 * A.gnodes);   // 4 x 64
+  int* s_ti = reinterpret_cast<int*>(s_xi + 4 * 64);
+  for (int t = threadIdx.x; t < A.ntab * A.ntab; t += blockDim.x) tab[t] = A.tabd[t];
+  if (COUL != 0)
+    for (int t = threadIdx.x; t < 2 * A.gnodes; t += blockDim.x) gt[t] = A.gtab[t];
+  __syncthreads();
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i8 = lane & 7, jq = lane >> 3;
+  double4* xi_s = s_xi + 64 * wib;
+  int* ti_s = s_ti + 64 * wib;
+  if (A.counters[kCntErr] & (kErrListOverflow | kErrMaskOverflow | kErrScOverflow | kErrColumnTooBig | kErrExclOverflow)) return;
+  const int nwork = min(A.counters[kCntWork], A.work_cap);
+  const int pad = A.ntab - 1;
+  const int nwarps = gridDim.x * 4;
+  double acc_v = 0, acc_c = 0, acc_w[6] = {0, 0, 0, 0, 0, 0};
+  for (int w = blockIdx.x * 4 + wib; w < nwork; w += nwarps) {
+    const int4 wk = A.work[w];
+    const int sc = wk.x;
+    for (int t = lane; t < 64; t += 32) {
+      double4 v = A.xqd[64 * sc + t];
+      v.w *= A.kcoul;
+      xi_s[t] = v;
+      ti_s[t] = A.tslot[64 * sc + t];
+    }
+    __syncwarp();
+    unsigned ireal = 0;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) ireal |= unsigned(ti_s[8 * c + i8] != pad) << c;
+    double fix[8], fiy[8], fiz[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) fix[c] = fiy[c] = fiz[c] = 0.0;
+    double ev = 0, ec = 0, vw[6] = {0, 0, 0, 0, 0, 0};
+    for (int e = wk.y; e < wk.y + wk.z; ++e) {
+      const uint4 en = A.ent[e];
+      const int cj = int(en.x);
+      const unsigned imask = en.y & 255u;
+      int qa, qb, qc;
+      unpack_image(en.y >> 8, qa, qb, qc);
+      const double Sx = A.cell.h[0][0] * qa + A.cell.h[0][1] * qb + A.cell.h[0][2] * qc;
+      const double Sy = A.cell.h[1][0] * qa + A.cell.h[1][1] * qb + A.cell.h[1][2] * qc;
+      const double Sz = A.cell.h[2][0] * qa + A.cell.h[2][1] * qb + A.cell.h[2][2] * qc;
+      const int j0 = 8 * cj + jq, j1 = j0 + 4;
+      const double4 a0 = A.xqd[j0], a1 = A.xqd[j1];
+      const int t0 = A.tslot[j0], t1 = A.tslot[j1];
+      double f0x = 0, f0y = 0, f0z = 0, f1x = 0, f1y = 0, f1z = 0;
+#pragma unroll 2
+      for (int c = 0; c < 8; ++c) {
+        if (!((imask >> c) & 1u)) continue;
+        const unsigned long long mm = en.z ? A.masks[8 * size_t(en.z - 1) + c] : ~0ull;
+        const double4 xi = xi_s[8 * c + i8];
+        const int ti = ti_s[8 * c + i8];
+        const bool oki = (ireal >> c) & 1u;
+        // d = xs_j - (xs_i - S), as field.cpp:1628-1636
+        const double xs = xi.x - Sx, ys = xi.y - Sy, zs = xi.z - Sz;
+#pragma unroll
+        for (int jj = 0; jj < 2; ++jj) {
+          const double4 aj = jj ? a1 : a0;
+          const int tj = jj ? t1 : t0;
+          const int bit = 8 * i8 + jq + 4 * jj;
+          const double dx = aj.x - xs, dy = aj.y - ys, dz = aj.z - zs;
+          const double r2 = dx * dx + dy * dy + dz * dz;
+          const bool ok = oki && ((mm >> bit) & 1ull) && (r2 < A.rc2);
+          if (!ok) continue;
+          const double r2i = 1 / r2, r6i = r2i * r2i * r2i, rinv = sqrt(r2i);
+          const double4 cc = tab[ti * A.ntab + tj];
+          double fr = r6i * (12 * cc.y * r6i - 6 * cc.x) * r2i;
+          if (ENER) ev += r6i * (cc.y * r6i - cc.x) - cc.z;
+          if (COUL != 0) {
+            const double qq = xi.w * aj.w;
+            double E, Fc;
+            ewald_ef(gt, A.ghi, r2, rinv, E, Fc);
+            if (COUL == 1) {
+              if (ENER) ec += qq * E;
+              fr += qq * Fc;
+            } else {
+              if (ENER) ec += qq * (E - A.dsf_e0 + A.dsf_f0 * (r2 * rinv - A.rc));
+              fr += qq * (Fc - A.dsf_f0 * rinv);
+            }
+          }
+          const double fx = fr * dx, fy = fr * dy, fz = fr * dz;
+          if (jj) f1x += fx, f1y += fy, f1z += fz;
+          else f0x += fx, f0y += fy, f0z += fz;
+          fix[c] -= fx;
+          fiy[c] -= fy;
+          fiz[c] -= fz;
+          if (VIR) {
+            vw[0] += fx * dx;
+            vw[1] += fy * dy;
+            vw[2] += fz * dz;
+            vw[3] += fx * dy;
+            vw[4] += fx * dz;
+            vw[5] += fy * dz;
+          }
+        }
+      }
+#pragma unroll
+      for (int o = 1; o < 8; o <<= 1) {
+        f0x += __shfl_xor_sync(0xffffffffu, f0x, o);
+        f0y += __shfl_xor_sync(0xffffffffu, f0y, o);
+        f0z += __shfl_xor_sync(0xffffffffu, f0z, o);
+        f1x += __shfl_xor_sync(0xffffffffu, f1x, o);
+        f1y += __shfl_xor_sync(0xffffffffu, f1y, o);
+        f1z += __shfl_xor_sync(0xffffffffu, f1z, o);
+      }
+      if (i8 < 6) {
+        const double v = i8 == 0 ? f0x : i8 == 1 ? f0y : i8 == 2 ? f0z : i8 == 3 ? f1x : i8 == 4 ? f1y : f1z;
+        const int js = i8 < 3 ? j0 : j1;
+        double* dst = (i8 % 3 == 0) ? A.fdx : (i8 % 3 == 1) ? A.fdy : A.fdz;
+        if (v != 0.0) atomicAdd(dst + js, v);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      fix[c] += __shfl_xor_sync(0xffffffffu, fix[c], 8);
+      fiy[c] += __shfl_xor_sync(0xffffffffu, fiy[c], 8);
+      fiz[c] += __shfl_xor_sync(0xffffffffu, fiz[c], 8);
+      fix[c] += __shfl_xor_sync(0xffffffffu, fix[c], 16);
+      fiy[c] += __shfl_xor_sync(0xffffffffu, fiy[c], 16);
+      fiz[c] += __shfl_xor_sync(0xffffffffu, fiz[c], 16);
+    }
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      if ((c & 3) != jq || !((ireal >> c) & 1u)) continue;
+      const int s = 64 * sc + 8 * c + i8;
+      if (fix[c] != 0.0) atomicAdd(A.fdx + s, fix[c]);
+      if (fiy[c] != 0.0) atomicAdd(A.fdy + s, fiy[c]);
+      if (fiz[c] != 0.0) atomicAdd(A.fdz + s, fiz[c]);
+    }
+    if (ENER) {
+      acc_v += warp_sum(ev);
+      acc_c += warp_sum(ec);
+    }
+    if (VIR)
+      for (int k = 0; k < 6; ++k) acc_w[k] += warp_sum(vw[k]);
+    __syncwarp();
+  }
+  if (lane == 0) {
+    if (ENER) {
+      A.en.add(kEVdw, acc_v, false);
+      A.en.add(kECoul, acc_c, false);
+    }
+    if (VIR)
+      for (int k = 0; k < 6; ++k) A.en.add(kEW0 + k, acc_w[k], false);
+  }
+}
+
+}  // namespace capsb

@@ -1,0 +1,215 @@
+"""The reference's Evaluator / run_dynamics interface over the device engine.
+
+Names and meanings follow caps::EnergyOptions, caps::Evaluator (core/include/caps/field.hpp:274-434) and
+caps::DynamicsOptions / run_dynamics (core/include/caps/dynamics.hpp:60-180). Every call goes through the C ABI of
+include/caps_gpu.h; errors come back as the reference's exception types (FieldError, ValueError for bad arguments,
+DynamicsCancelled).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi
+from .forcefield import ForceField
+
+
+class FieldError(RuntimeError):
+    """caps::FieldError (core/include/caps/field.hpp:17)."""
+
+
+class DynamicsCancelled(RuntimeError):
+    """caps::DynamicsCancelled (core/include/caps/dynamics.hpp:168)."""
+
+
+class DeviceError(RuntimeError):
+    """A CUDA call failed, or there is no device (the engine has no CPU fallback)."""
+
+
+def _raise(code: int, text: str):
+    if code == -3 or code == -4:
+        raise FieldError(text)
+    if code == -5:
+        raise DynamicsCancelled(text)
+    if code == -2 or code == -6:
+        raise DeviceError(text)
+    raise ValueError(text)
+
+
+@dataclass
+class EnergyOptions:
+    """caps::EnergyOptions (field.hpp:274-308), the fields the device path takes. precision "mixed" is
+    EnergyOptions::mixed = true; the device's mixed form adds bit-reproducible fixed-point force sums."""
+    cutoff: float = 10.0
+    skin: float = 2.0
+    coulomb: bool = True
+    electrostatics: str = "dsf"        # "dsf" | "pme"
+    dsf_alpha: float = 0.2
+    ewald_rtol: float = 1e-5
+    pme_spacing: float = 1.0
+    pme_order: int = 5
+    tail: bool = True
+    precision: str = "mixed"           # "mixed" | "double"
+    force_cap: float = 0.0
+    parts: int = 3
+
+    def to_struct(self) -> _abi.Opts:
+        o = _abi.Opts()
+        o.cutoff, o.skin, o.coulomb = self.cutoff, self.skin, int(bool(self.coulomb))
+        o.electrostatics = 1 if self.electrostatics.lower() == "pme" else 0
+        o.dsf_alpha, o.ewald_rtol, o.pme_spacing, o.pme_order = self.dsf_alpha, self.ewald_rtol, self.pme_spacing, self.pme_order
+        o.tail = int(bool(self.tail))
+        o.precision = 1 if self.precision == "double" else 0
+        o.force_cap, o.parts = self.force_cap, self.parts
+        return o
+
+
+THERMOSTATS = {"none": 0, "nve": 0, "bussi": 1, "csvr": 1, "langevin": 2, "baoab": 2, "nose-hoover": 3, "nhc": 3}
+BAROSTATS = {"none": 0, "crescale": 1, "c-rescale": 1}
+
+
+@dataclass
+class DynamicsOptions:
+    """caps::DynamicsOptions (dynamics.hpp:60-154), the fields the device step takes."""
+    dt: float = 1.0
+    steps: int = 10000
+    temperature: float = 300.0
+    temperature_end: float = -1.0
+    thermostat: str = "bussi"
+    tau_t: float = 100.0
+    barostat: str = "none"
+    pressure: float = 1.0
+    tau_p: float = 1000.0
+    compressibility: float = 4.5e-5
+    barostat_every: int = 10
+    constraints: str = "none"          # "none" | "h-bonds"
+    new_velocities: bool = False
+    seed: int = 1
+    thermo_every: int = 100
+    frame_every: int = 0
+    step_offset: int = 0
+    respa: int = 1
+    energy: EnergyOptions = field(default_factory=EnergyOptions)
+
+    def to_struct(self, ff: ForceField, keep: list) -> _abi.MdOpts:
+        m = _abi.MdOpts()
+        m.dt, m.steps, m.temperature, m.temperature_end = self.dt, self.steps, self.temperature, self.temperature_end
+        m.thermostat = THERMOSTATS[self.thermostat.lower()]
+        m.tau_t = self.tau_t
+        m.barostat = BAROSTATS[self.barostat.lower()]
+        m.pressure, m.tau_p, m.compressibility, m.barostat_every = self.pressure, self.tau_p, self.compressibility, self.barostat_every
+        m.constraints = 0 if self.constraints in ("none", "", None) else 1
+        m.new_velocities = int(bool(self.new_velocities))
+        m.seed, m.thermo_every, m.frame_every, m.step_offset, m.respa = self.seed, self.thermo_every, self.frame_every, self.step_offset, self.respa
+        if ff.element is not None:
+            h = np.ascontiguousarray((ff.element == 1).astype(np.int8))
+            o = np.ascontiguousarray((ff.element == 8).astype(np.int8))
+            keep += [h, o]
+            m.is_hydrogen = h.ctypes.data_as(C.c_void_p)
+            m.is_oxygen = o.ctypes.data_as(C.c_void_p)
+        return m
+
+
+def cell_array(cell) -> np.ndarray:
+    """cell[12] = origin, a, b, c (accepts a 3x3 of edge vectors, a 4x3, or 12 numbers)."""
+    c = np.asarray(cell, dtype=np.float64).reshape(-1)
+    if c.size == 9:
+        c = np.concatenate([np.zeros(3), c])
+    if c.size != 12:
+        raise ValueError("cell: 12 numbers (origin, a, b, c) or 9 (a, b, c)")
+    return np.ascontiguousarray(c)
+
+
+class Evaluator:
+    """caps::Evaluator on the device: Evaluator(ff, options); compute(x, cell) -> (terms, forces)."""
+
+    def __init__(self, ff: ForceField, options: EnergyOptions | None = None):
+        self.lib = _abi.load()
+        self.ff = ff
+        self.options = options or EnergyOptions()
+        s, keep = ff.to_struct()
+        o = self.options.to_struct()
+        h = self.lib.caps_gpu_create(C.byref(s), C.byref(o))
+        if not h:
+            text = self.lib.caps_gpu_error(None).decode()
+            if "no CUDA device" in text:
+                raise DeviceError(text)
+            raise ValueError(text)
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.caps_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int):
+        if rc != 0:
+            _raise(rc, self.lib.caps_gpu_error(self.h).decode())
+
+    def set_options(self, options: EnergyOptions):
+        self.options = options
+        o = options.to_struct()
+        self._check(self.lib.caps_gpu_set_options(self.h, C.byref(o)))
+
+    def energies(self, on: bool):
+        self._check(self.lib.caps_gpu_energies(self.h, int(bool(on))))
+
+    def compute(self, x, cell) -> tuple[dict, np.ndarray]:
+        x = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1))
+        c = cell_array(cell)
+        f = np.zeros_like(x)
+        t = _abi.Terms()
+        self._check(self.lib.caps_gpu_compute(self.h, x.ctypes.data_as(C.c_void_p), c.ctypes.data_as(C.c_void_p),
+                                              f.ctypes.data_as(C.c_void_p), C.byref(t)))
+        return t.as_dict(), f.reshape(-1, 3)
+
+    def list_builds(self) -> int:
+        return int(self.lib.caps_gpu_list_builds(self.h))
+
+    def run(self, x, cell, opts: DynamicsOptions, v=None, progress=None, frame=None) -> dict:
+        """run_dynamics on this evaluator's force field: returns {x, v, cell, thermo, report, steps_per_second}."""
+        x = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1)).copy()
+        vv = np.zeros_like(x) if v is None else np.ascontiguousarray(np.asarray(v, dtype=np.float64).reshape(-1)).copy()
+        c = cell_array(cell).copy()
+        st = _abi.State(x.ctypes.data_as(C.c_void_p), vv.ctypes.data_as(C.c_void_p), c.ctypes.data_as(C.c_void_p),
+                        0 if v is None else 1)
+        keep: list = []
+        m = opts.to_struct(self.ff, keep)
+        rows = []
+
+        def _prog(row, user):
+            d = row.contents.as_dict()
+            rows.append(d)
+            if progress is not None and progress(d) is False:
+                return 1
+            return 0
+
+        def _frame(xp, cp, step, user):
+            if frame is not None:
+                n = self.ff.natoms
+                frame(np.ctypeslib.as_array(xp, shape=(3 * n,)).copy().reshape(-1, 3),
+                      np.ctypeslib.as_array(cp, shape=(12,)).copy(), int(step))
+
+        pf, ff_ = _abi.PROGRESS_FN(_prog), _abi.FRAME_FN(_frame)
+        buf = C.create_string_buffer(4096)
+        rc = self.lib.caps_gpu_run(self.h, C.byref(st), C.byref(m), pf, ff_, None, buf, 4096)
+        self._check(rc)
+        return {"x": x.reshape(-1, 3), "v": vv.reshape(-1, 3), "cell": c, "thermo": rows, "report": buf.value.decode(),
+                "steps_per_second": float(self.lib.caps_gpu_last_steps_per_second(self.h))}
+
+
+def run_dynamics(ff: ForceField, x, cell, opts: DynamicsOptions, v=None, progress=None, frame=None) -> dict:
+    """caps::run_dynamics on the device (dynamics.hpp:180)."""
+    ev = Evaluator(ff, opts.energy)
+    try:
+        return ev.run(x, cell, opts, v=v, progress=progress, frame=frame)
+    finally:
+        ev.close()

