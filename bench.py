@@ -1,0 +1,290 @@
+#!/usr/bin/env python
+"""Benchmark: ns/day and atom-steps/s of CAPS's MD step on the 32,000-atom polystyrene PME melt, on one B200, in the mixed
+FP32/fixed-point form against the FP64 form at a stated force error.
+
+Workload (the reference's configuration "All-atom atactic polystyrene melt with PME"): 40 chains x 50 repeat units x 16
+atoms = 32,000 atoms, atactic, cubic box at 1.04 g/cm^3, OPLS-AA-style LJ 12-6 with geometric mixing, cut-off 12 Å with a
+2 Å Verlet buffer, partial charges (aromatic C -0.115 / H +0.115, backbone neutral), 1-2/1-3 excluded, 1-4 scaled 0.5, PME
+(rtol 1e-5, 1.0 Å spacing, order 4), SHAKE on C-H, Nose-Hoover chain NVT at 500 K, dt 1 fs. The cell is synthetic (seeded
+growth, device push-off and equilibration: caps_b200/data/make_ps32k.py); the starting positions and velocities are
+caps_b200/data/ps32k_start.npz.
+
+A step is one MD step. value: simulated ns/day summed over the replicas of the job (one per GPU, no collective: the
+path does not shard; replicas only), from CUDA events around every step on the engine's stream, with a 256 MB L2
+flush between steps outside the events. e2e: the same metric through the C ABI call caps_gpu_run with host buffers
+(wall clock around the call: setup, first force, host<->device copies included).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl caps_b200|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+FLOPS_PER_PAIR = 59          # FP32 flops of one interacting pair on a force-only step (FMA as 2)
+FLUSH_BYTES = 256 << 20      # > 126 MB L2
+START = ROOT / "caps_b200" / "data" / "ps32k_start.npz"
+WORKLOAD = {"workload": "polystyrene PME melt, 40 chains x 50 units x 16 atoms = 32,000 atoms", "box_A": None, "density_g_cm3": 1.04,
+            "cutoff_A": 12.0, "skin_A": 2.0, "pme": "rtol 1e-5, spacing 1.0 Å, order 4", "constraints": "SHAKE on C-H",
+            "thermostat": "Nose-Hoover chain 500 K", "dt_fs": 1.0, "l2": "256 MB flush between timed steps"}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+class Clocks:
+    """nvidia-smi sampled every 200 ms during the timed region: median SM clock under load and throttle reasons."""
+
+    def __init__(self, index: int):
+        self.index, self.rows, self.proc = index, [], None
+
+    def __enter__(self):
+        q = "index,clocks.sm,clocks.max.sm,power.draw,utilization.gpu,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+            "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        import statistics
+        rows = [r for r in self.rows if len(r) >= 9]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        load = [r for r in rows if r[4].isdigit() and int(r[4]) > 10] or rows
+        sm = [float(r[1]) for r in load if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in load for k in range(4) if r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(load)}
+
+
+def workload():
+    import numpy as np
+
+    from caps_b200.systems import polystyrene_melt
+    z = np.load(START)
+    ff, _, cell = polystyrene_melt(40, 50, 1.04, seed=1, grow=False)
+    return ff, z["x"].astype(np.float64), z["v"].astype(np.float64), z["cell"].astype(np.float64)
+
+
+def options(precision: str, steps: int, seed: int, thermostat: str = "nose-hoover", thermo_every: int | None = None):
+    from caps_b200 import DynamicsOptions, EnergyOptions
+    eo = EnergyOptions(cutoff=12.0, skin=2.0, electrostatics="pme", ewald_rtol=1e-5, pme_spacing=1.0, pme_order=4, tail=True, precision=precision)
+    return DynamicsOptions(dt=1.0, steps=steps, temperature=500.0, thermostat=thermostat, tau_t=100.0, constraints="h-bonds", seed=seed,
+                           thermo_every=thermo_every or max(steps, 1), energy=eo)
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    return json.loads(p.read_text()) if p.exists() else {}
+
+
+def run_reference(args, rank: int) -> dict:
+    """The reference's own CPU implementation (oracle/_ref: the reference core built from its sources) on this
+    workload: run_dynamics in its fastest form (EnergyOptions::mixed = true), all host threads."""
+    from oracle import ref
+    if not ref.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libcaps_ref.so is not built (make -C oracle where the reference sources are)"}
+    ff, x, v, cell = workload()
+    threads = os.cpu_count() or 1
+    if args.warmup > 0:
+        ref.run(ff, x, cell, options("mixed", min(args.warmup, 3), 1), v=v, threads=threads)
+    steps = max(1, args.steps)
+    t0 = time.perf_counter()
+    out = ref.run(ff, x, cell, options("mixed", steps, 1), v=v, threads=threads)
+    wall = time.perf_counter() - t0
+    nsd = out["ns_per_day"]
+    n = ff.natoms
+    sps = steps / out["seconds"] if out["seconds"] > 0 else 0.0
+    cfg = dict(WORKLOAD, box_A=round(float(cell[3]), 3), parallelism="1 CPU process", sample=f"{steps} MD steps")
+    return {"impl": "reference", "metric": "ns/day (32k-atom polystyrene PME melt, MD step)", "value": nsd, "unit": "ns/day", "n_gpus": args.gpus,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": 1000.0 / sps if sps else None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 pair kernel, f64 sums (reference mixed)", "data": "synthetic", "config": cfg,
+            "atom_steps_per_s": sps * n,
+            "cpu_baseline": {"value": nsd, "unit": "ns/day", "cores": threads, "kind": "reference",
+                             "sample": f"{steps} steps of run_dynamics on the same cell, EnergyOptions::mixed = true, {threads} threads, wall {wall:.1f} s"},
+            "e2e": {"value": nsd, "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=200)
+    ap.add_argument("--impl", default="caps_b200")
+    ap.add_argument("--fp64-steps", type=int, default=None)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    args = ap.parse_args()
+    rank, world, local = int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+    if args.warmup < 3:
+        args.warmup = 3
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args, rank)), flush=True)
+        return
+
+    # one process per GPU: this rank sees its own device only (the engine takes the current device)
+    if world > 1:
+        os.environ["CUDA_VISIBLE_DEVICES"] = str(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(0)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        pg = dist
+
+    import numpy as np
+
+    from caps_b200 import Evaluator
+    ff, x, v, cell = workload()
+    n = ff.natoms
+    seed = 1 + rank
+
+    def barrier():
+        if pg:
+            pg.barrier()
+
+    def max_over_ranks(val: float) -> float:
+        if not pg:
+            return val
+        import torch
+        t = torch.tensor([val], dtype=torch.float64, device="cuda" if pg.get_backend() == "nccl" else "cpu")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    # --- mixed FP32/fixed-point: warm-up, then K timed steps (events per step, L2 flushed between steps) ---
+    o = options("mixed", args.warmup, seed)
+    ev = Evaluator(ff, o.energy)
+    out = ev.run(x, cell, o, v=v)
+    x1, v1 = out["x"], out["v"]
+    ev.set_timing(FLUSH_BYTES)
+    barrier()
+    with Clocks(local) as clk:
+        out = ev.run(x1, cell, options("mixed", args.steps, seed), v=v1)
+    barrier()
+    ms_step = max_over_ranks(ev.last_step_ms())
+    launches = ev.step_kernels() * args.steps
+    ev.set_timing(-1)
+    x2, v2 = out["x"], out["v"]
+    sps = 1000.0 / ms_step
+    nsd = sps * 1.0 * 86400e-6            # dt = 1 fs
+    value = nsd * world                    # whole job: the replicas' simulated time per day
+    # --- e2e: the C ABI call with host buffers, wall clock around it ---
+    t0 = time.perf_counter()
+    eo_run = ev.run(x2, cell, options("mixed", args.steps, seed), v=v2)
+    e2e_wall = time.perf_counter() - t0
+    e2e_nsd = args.steps * 1.0 * 1e-6 / e2e_wall * 86400 * world
+    h2d = (2 * 3 * n * 8 + 12 * 8) / args.steps
+    d2h = (2 * 3 * n * 8 + 12 * 8 + 2 * 232) / args.steps
+    del eo_run
+    # --- the dominant kernel (the pair kernel) timed alone: roofline ---
+    pt = ev.pair_timing(x2, cell, launches=max(20, min(args.steps, 200)), flush_bytes=FLUSH_BYTES)
+    achieved = pt["pairs_in_cutoff"] * FLOPS_PER_PAIR / (pt["avg_ms"] * 1e-3) / 1e12
+    peaks = measured_peaks()
+    sm_max = peaks.get("sm_max_mhz", 1965.0)
+    fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12   # FP32 FMA issue peak at the measured max clock (not measured directly)
+    # --- forces at the end state: mixed vs FP64 ---
+    em = Evaluator(ff, options("mixed", 1, seed).energy)
+    tm, fm = em.compute(x2, cell)
+    ed = Evaluator(ff, options("double", 1, seed).energy)
+    td, fd = ed.compute(x2, cell)
+    df = fm - fd
+    rms_rel = float(np.sqrt((df ** 2).sum(1).mean() / (fd ** 2).sum(1).mean()))
+    per_atom = np.linalg.norm(df, axis=1) / np.maximum(np.linalg.norm(fd, axis=1), 1e-12)
+    e_err = abs(tm["total"] - td["total"]) / abs(td["total"])
+    em.close()
+    ed.close()
+    # --- the FP64 path on the same workload ---
+    k64 = args.fp64_steps or max(100, args.steps // 4)
+    ev64 = Evaluator(ff, options("double", args.warmup, seed).energy)
+    ev64.run(x2, cell, options("double", args.warmup, seed), v=v2)
+    ev64.set_timing(FLUSH_BYTES)
+    ev64.run(x2, cell, options("double", k64, seed), v=v2)
+    ms64 = max_over_ranks(ev64.last_step_ms())
+    nsd64 = 1000.0 / ms64 * 86400e-6
+    ev64.close()
+    # --- NVE drift of the mixed path (2 ps) ---
+    nve = options("mixed", 2000, seed, thermostat="none", thermo_every=100)
+    outn = ev.run(x2, cell, nve, v=v2)
+    cons = np.array([r["conserved"] for r in outn["thermo"]])
+    tps = np.array([r["time_ps"] for r in outn["thermo"]])
+    slope = float(np.polyfit(tps, cons, 1)[0]) if len(cons) > 2 else 0.0          # kcal/mol/ps
+    kT = 0.0019872041 * float(np.mean([r["temperature"] for r in outn["thermo"]]))
+    drift_kt_ns_atom = slope * 1000.0 / kT / n
+    ev.close()
+    # --- CPU baseline: the reference's own code on the host cores, bounded sample (rank 0, N = 1) ---
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            from oracle import ref
+            if ref.available():
+                threads = os.cpu_count() or 1
+                steps_cpu = 10
+                r = ref.run(ff, x2, cell, options("mixed", steps_cpu, seed), v=v2, threads=threads)
+                cpu = {"value": r["ns_per_day"], "unit": "ns/day", "cores": threads, "kind": "reference",
+                       "sample": f"{steps_cpu} MD steps of the same cell through the reference's run_dynamics (mixed, its fastest), "
+                                 f"{threads} threads, {r['seconds']:.1f} s"}
+        except Exception as e:   # the baseline is reported, not required
+            cpu = {"value": None, "unit": "ns/day", "cores": os.cpu_count(), "kind": "reference", "sample": f"failed: {e}"}
+    if rank == 0:
+        cfg = dict(WORKLOAD, box_A=round(float(cell[3]), 3), parallelism=f"{world} independent replica(s), one per GPU")
+        line = {
+            "metric": "ns/day (32k-atom polystyrene PME melt, MD step, mixed FP32/fixed-point)", "value": value, "unit": "ns/day", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 pair/PME spread-gather, int64 fixed-point sums, f64 FFT/bonded/integrator", "data": "synthetic", "config": cfg,
+            "atom_steps_per_s": sps * n * world,
+            "fp64": {"ns_per_day": nsd64 * world, "ms_per_step": ms64, "steps": k64, "mixed_speedup": ms64 / ms_step},
+            "force_error_vs_fp64": {"rms_relative": rms_rel, "per_atom_rms": float(np.sqrt(np.mean(per_atom ** 2))),
+                                    "per_atom_max": float(per_atom.max()), "energy_relative": e_err},
+            "nve_drift_kT_per_ns_per_atom": drift_kt_ns_atom,
+            "e2e": {"value": e2e_nsd, "unit": "ns/day", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "call": "caps_gpu_run (C ABI) on host buffers, wall clock"},
+            "roofline": {"bound": "fp32", "kernel": "k_pair_f32 (LJ + Ewald real space)", "achieved": achieved,
+                         "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                         "peak_note": "FP32 FMA issue rate, 148 SMs x 128 lanes x 2 at the measured max SM clock (nominal)",
+                         "work": f"{pt['pairs_in_cutoff']:.0f} pairs inside the cut-off x {FLOPS_PER_PAIR} flops per launch",
+                         "pair_ms": pt["avg_ms"], "pairs_listed": pt["pairs_listed"], "entries": pt["entries"], "traffic": None},
+            "gpu_launches": launches,
+            "gpu_launches_note": "kernel nodes of the captured step graph x timed steps (thermo steps launch the same kernels uncaptured)",
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -33,7 +33,7 @@ def up_to_date() -> bool:
     if not LIB.exists():
         return False
     t = LIB.stat().st_mtime
-    deps = list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [ROOT / "include" / "caps_gpu.h"]
+    deps = list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list((ROOT / "include").glob("*.h"))
     return all(p.stat().st_mtime <= t for p in deps)
 
 

@@ -1,8 +1,10 @@
 // K-BOND: bonded terms, 1-4 pairs, the Coulomb corrections of excluded pairs and FENE bonds, one thread per term.
 // Reference: Evaluator::compute's bonded phase (core/src/field.cpp:1863-2283): harmonic bonds (:1986-1995), harmonic
 // angles (:1996-2010), Fourier torsion groups for dihedrals and impropers (:1875-1920, 2011-2018), 1-4 pairs (:2019-2043),
-// excluded-pair electrostatics (:2206-2266), FENE + WCA (:2152-2166). The FP32 path computes each term in single
-// precision from double separations and adds forces as 64-bit fixed point; the FP64 path is double throughout.
+// excluded-pair electrostatics (:2206-2266), FENE + WCA (:2152-2166). These run in double arithmetic on both paths (the
+// reference keeps them double in its mixed mode too: r - r0 of a stiff bond loses most of a float's digits, which
+// measured 1.4e-4 RMS relative force error on a relaxed cell against the 5e-6 target); the mixed path adds the forces
+// as 64-bit fixed point (order-free, bit-reproducible), the FP64 path as doubles. The sink type S picks which.
 #pragma once
 #include "common.cuh"
 
@@ -55,8 +57,8 @@ template <class R> __device__ __forceinline__ R rsq(R v) { return sqrt(v); }
 template <> __device__ __forceinline__ float rsq<float>(float v) { return sqrtf(v); }
 
 // harmonic bonds: k (r - r0)^2
-template <class R, bool ENER, bool VIR>
-static __global__ void k_bonds(int nb, const uint32_t* __restrict__ ij, const double* __restrict__ kr, BondedArgs A, ForceSink<R> F) {
+template <class R, class S, bool ENER, bool VIR>
+static __global__ void k_bonds(int nb, const uint32_t* __restrict__ ij, const double* __restrict__ kr, BondedArgs A, S F) {
   Tally<VIR> T;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nb; t += gridDim.x * blockDim.x) {
     const int i = int(ij[2 * t]), j = int(ij[2 * t + 1]);
@@ -75,8 +77,8 @@ static __global__ void k_bonds(int nb, const uint32_t* __restrict__ ij, const do
 }
 
 // harmonic angles: kt (theta - theta0)^2, j the vertex
-template <class R, bool ENER, bool VIR>
-static __global__ void k_angles(int na, const uint32_t* __restrict__ ijk, const double* __restrict__ kt0, BondedArgs A, ForceSink<R> F) {
+template <class R, class S, bool ENER, bool VIR>
+static __global__ void k_angles(int na, const uint32_t* __restrict__ ijk, const double* __restrict__ kt0, BondedArgs A, S F) {
   Tally<VIR> T;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < na; t += gridDim.x * blockDim.x) {
     const int i = int(ijk[3 * t]), j = int(ijk[3 * t + 1]), k = int(ijk[3 * t + 2]);
@@ -107,9 +109,9 @@ static __global__ void k_angles(int na, const uint32_t* __restrict__ ijk, const 
 
 // Fourier torsion groups: terms [gs[g], gs[g+1]) share one quadruple; v [1 + cos(n phi - delta)], phi IUPAC, cos/sin of
 // n phi by recurrence (field.cpp:1875-1920).
-template <class R, bool ENER, bool VIR>
+template <class R, class S, bool ENER, bool VIR>
 static __global__ void k_torsions(int ngroups, const int* __restrict__ gs, const uint32_t* __restrict__ ijkl, const double* __restrict__ vd,
-                           const int* __restrict__ nn, BondedArgs A, ForceSink<R> F, int slot) {
+                           const int* __restrict__ nn, BondedArgs A, S F, int slot) {
   Tally<VIR> T;
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ngroups; g += gridDim.x * blockDim.x) {
     const int t0 = gs[g], t1 = gs[g + 1];
@@ -170,9 +172,9 @@ static __global__ void k_torsions(int ngroups, const int* __restrict__ gs, const
 
 // 1-4 pairs: LJ times the 1-4 scale (and the same cut-off shift as the pairs), at the nearest image (field.cpp:2019-2043).
 // lj: per type pair (eps, sigma^6, energy shift of 4 eps (q_c^2 - q_c) or 0, 0); capped: (rcap^2, ecap, fcap, 0).
-template <class R, bool ENER, bool VIR>
+template <class R, class S, bool ENER, bool VIR>
 static __global__ void k_pairs14(int np, const uint32_t* __restrict__ ij, const double* __restrict__ scale, double lj14, const int* __restrict__ type, int nt,
-                          const double4* __restrict__ lj, const double4* __restrict__ cap, BondedArgs A, ForceSink<R> F) {
+                          const double4* __restrict__ lj, const double4* __restrict__ cap, BondedArgs A, S F) {
   Tally<VIR> T;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < np; t += gridDim.x * blockDim.x) {
     const int i = int(ij[2 * t]), j = int(ij[2 * t + 1]);
@@ -208,7 +210,7 @@ static __global__ void k_pairs14(int np, const uint32_t* __restrict__ ij, const 
 // under PME). FP32: E = qq (f/r - erf(kr)/r) in closed form (no cancellation), the same terms beyond.
 struct ExclArgs {
   const uint32_t* ij;
-  const float* factor;
+  const double* factor;
   const double* q;
   const double* gtab;
   double ghi, rc, rc2, kappa, dsf_e0, dsf_f0;
@@ -222,8 +224,8 @@ __device__ __forceinline__ double erfc_as(double x, double& ex2) {   // Abramowi
   return t * (A1 + t * (A2 + t * (A3 + t * (A4 + t * A5)))) * ex2;
 }
 
-template <bool ENER, bool VIR>
-static __global__ void k_excl_f64(int nx, ExclArgs E, BondedArgs A, ForceSink<double> F) {
+template <class S, bool ENER, bool VIR>
+static __global__ void k_excl_f64(int nx, ExclArgs E, BondedArgs A, S F) {
   Tally<VIR> T;
   const double sp = 2 / sqrt(kPi), kap = E.kappa;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nx; t += gridDim.x * blockDim.x) {
@@ -233,7 +235,7 @@ static __global__ void k_excl_f64(int nx, ExclArgs E, BondedArgs A, ForceSink<do
     sep(A, i, j, dx, dy, dz);
     const double r2 = dx * dx + dy * dy + dz * dz;
     if (r2 >= E.rc2 && !E.pme) continue;
-    const double r = sqrt(r2), qq = kCoulomb * E.q[i] * E.q[j], f = double(E.factor[t]);
+    const double r = sqrt(r2), qq = kCoulomb * E.q[i] * E.q[j], f = E.factor[t];
     double e, fr;
     if (r < 0.5) {
       const double xk = kap * r;
@@ -273,41 +275,10 @@ static __global__ void k_excl_f64(int nx, ExclArgs E, BondedArgs A, ForceSink<do
   T.flush(A, kECoul, ENER);
 }
 
-template <bool ENER, bool VIR>
-static __global__ void k_excl_f32(int nx, ExclArgs E, BondedArgs A, ForceSink<float> F) {
-  Tally<VIR> T;
-  const float kap = float(E.kappa), kc = float(2 * E.kappa / sqrt(kPi)), rcf = float(E.rc), e0 = float(E.dsf_e0), f0 = float(E.dsf_f0);
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nx; t += gridDim.x * blockDim.x) {
-    const int i = int(E.ij[2 * t]), j = int(E.ij[2 * t + 1]);
-    if (E.q[i] == 0 || E.q[j] == 0) continue;
-    float dx, dy, dz;
-    sep(A, i, j, dx, dy, dz);
-    const float r2 = dx * dx + dy * dy + dz * dz;
-    if (r2 >= float(E.rc2) && !E.pme) continue;
-    if (r2 <= 0.f) continue;
-    const float qq = float(kCoulomb * E.q[i] * E.q[j]), f = E.factor[t];
-    const float rinv = rsqrtf(r2), r = r2 * rinv, r2i = rinv * rinv;
-    // erf(kr)/r and its derivative term, direct: E = qq (f/r - erf/r), -(dE/dr)/r = qq (f/r^3 + kc e^-k2r2 / r^2 - erf / r^3)
-    const float erfv = erff(kap * r), ex = __expf(-kap * kap * r2);
-    float e = qq * (f * rinv - erfv * rinv);
-    float fr = qq * (f * rinv * r2i + kc * ex * r2i - erfv * rinv * r2i);
-    if (!E.pme) {
-      e += qq * (f0 * (r - rcf) - e0);
-      fr -= qq * f0 * rinv;
-    }
-    if (ENER) T.e += double(e);
-    const float fx = dx * fr, fy = dy * fr, fz = dz * fr;
-    F.add(j, fx, fy, fz);
-    F.add(i, -fx, -fy, -fz);
-    T.vir(dx, dy, dz, fx, fy, fz);
-  }
-  T.flush(A, kECoul, ENER);
-}
-
 // FENE (-1/2 K R0^2 ln(1 - (r/R0)^2)) plus WCA below 2^(1/6) sigma (LAMMPS bond fene; field.cpp:2152-2166). A bond
 // stretched to R0 or past raises kErrFene (the reference throws FieldError there).
-template <class R, bool ENER, bool VIR>
-static __global__ void k_fene(int nf, const uint32_t* __restrict__ ij, const double* __restrict__ p, BondedArgs A, ForceSink<R> F, int* counters) {
+template <class R, class S, bool ENER, bool VIR>
+static __global__ void k_fene(int nf, const uint32_t* __restrict__ ij, const double* __restrict__ p, BondedArgs A, S F, int* counters) {
   Tally<VIR> T;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nf; t += gridDim.x * blockDim.x) {
     const int i = int(ij[2 * t]), j = int(ij[2 * t + 1]);

@@ -8,11 +8,15 @@ namespace capsb {
 constexpr double kPi = 3.14159265358979323846;
 constexpr double kCoulomb = 332.06371;   // kcal*Å/(mol*e^2), as the reference (core/src/field.cpp:29)
 
-// Fixed-point scales. Forces and energies: 2^32 units per kcal/mol/Å (or per kcal/mol): resolution 2.3e-10, range
-// +-2.1e9. PME grid charges: 2^40 per e (resolution 9e-13 e). Integer sums are exact, so every reduction that goes
+// Fixed-point scales. Forces: 2^32 units per kcal/mol/Å: resolution 2.3e-10, range +-2.1e9. PME grid charges: 2^40 per e (resolution 9e-13 e). Integer sums are exact, so every reduction that goes
 // through these is independent of the order the GPU runs it in: bit-reproducible forces and energies.
 constexpr double kFixF = 4294967296.0;
 constexpr double kInvFixF = 1.0 / 4294967296.0;
+// Energies and virials: 2^24 per kcal/mol (resolution 6e-8, range +-5.5e11).
+constexpr double kFixE = 16777216.0;
+constexpr double kInvFixE = 1.0 / 16777216.0;
+// A force component past this cannot be held in the fixed-point sums: the kernel raises kErrFixRange instead.
+constexpr float kFixFMax = 2.0e9f;
 constexpr double kFixQ = 1099511627776.0;
 constexpr double kInvFixQ = 1.0 / 1099511627776.0;
 
@@ -28,6 +32,7 @@ enum ErrorBits : unsigned {
   kErrNonFinite = 1u << 7,        // a coordinate became NaN / inf
   kErrMaskOverflow = 1u << 8,     // exclusion masks past capacity
   kErrImageRange = 1u << 9,       // an image shift outside +-63 cells
+  kErrFixRange = 1u << 10,        // a force or energy outside the fixed-point range (overlapping atoms: push off first)
 };
 
 // Periodic cell: origin o, edge vectors a, b, c (columns of h) and h^-1 (rows: reciprocal vectors without 2 pi).
@@ -63,21 +68,29 @@ __device__ __forceinline__ void atomic_add_fix(long long* p, long long v) {
   atomicAdd(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(v));
 }
 
+// A float force component into fixed point, or the range error (bit 10 of the error word) when it cannot be held.
+__device__ __forceinline__ void fix_add_f(long long* p, float v, int* err) {
+  if (fabsf(v) < kFixFMax) atomic_add_fix(p, to_fixf(v));
+  else atomicOr(reinterpret_cast<unsigned*>(err), 1u << 10);
+}
+
 // Force accumulation into either fixed-point (mixed precision) or double (FP64) SoA arrays.
 template <class R> struct ForceSink;
 template <> struct ForceSink<float> {
   long long* fx;
   long long* fy;
   long long* fz;
-  __device__ __forceinline__ void add(int i, float x, float y, float z) const {
-    atomic_add_fix(fx + i, to_fixf(x));
-    atomic_add_fix(fy + i, to_fixf(y));
-    atomic_add_fix(fz + i, to_fixf(z));
+  int* err;
+  __device__ __forceinline__ void one(long long* p, double v) const {
+    if (fabs(v) < double(kFixFMax)) atomic_add_fix(p, to_fix(v, kFixF));
+    else atomicOr(reinterpret_cast<unsigned*>(err), 1u << 10);
   }
-  __device__ __forceinline__ void add1(int comp, int i, float v) const {
-    long long* p = comp == 0 ? fx : comp == 1 ? fy : fz;
-    atomic_add_fix(p + i, to_fixf(v));
+  __device__ __forceinline__ void add(int i, double x, double y, double z) const {
+    one(fx + i, x);
+    one(fy + i, y);
+    one(fz + i, z);
   }
+  __device__ __forceinline__ void add1(int comp, int i, double v) const { one(comp == 0 ? fx : comp == 1 ? fy : fz, v); }
 };
 template <> struct ForceSink<double> {
   double* fx;
@@ -96,14 +109,14 @@ template <> struct ForceSink<double> {
 
 // Energy / virial accumulators: index into a small array; fixed point for the mixed path (deterministic), double for
 // the FP64 path.
-enum EnergySlot { kEBond = 0, kEAngle, kEDihedral, kEImproper, kEVdw, kECoul, kEW0, kEW1, kEW2, kEW3, kEW4, kEW5, kEPmeRecip, kEKin,
+enum EnergySlot { kEBond = 0, kEAngle, kEDihedral, kEImproper, kEVdw, kECoul, kEW0, kEW1, kEW2, kEW3, kEW4, kEW5, kEPmeRecip, kEPairs, kEListed,
                   kENumSlots = 16 };
 
 struct EnergySink {
   long long* fix;    // [kENumSlots] mixed path
   double* dbl;       // [kENumSlots] FP64 path
   __device__ __forceinline__ void add(int slot, double v, bool fixed) const {
-    if (fixed) atomic_add_fix(fix + slot, to_fix(v, kFixF));
+    if (fixed) atomic_add_fix(fix + slot, to_fix(v, kFixE));
     else atomicAdd(dbl + slot, v);
   }
 };

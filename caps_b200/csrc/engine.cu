@@ -1,6 +1,7 @@
 // Host side of the device engine: the C ABI of include/caps_gpu.h, force-field upload, cell and list geometry, and the
 // kernel sequence of one force evaluation (Evaluator::compute, core/src/field.cpp:1249-2539).
 #include "engine.h"
+#include "caps_gpu_diag.h"
 
 #include <algorithm>
 #include <cmath>
@@ -275,7 +276,7 @@ void Engine::setup_ff(const caps_gpu_ff* ff) {
   }
   // excluded partners: the CSR for the list, and (i < j, factor) pairs for the Coulomb corrections
   std::vector<uint32_t> eoff(size_t(n_) + 1, 0), elist, xij;
-  std::vector<float> xf;
+  std::vector<double> xf;
   for (int i = 0; i < n_; ++i) {
     const uint32_t b0 = ff->excl_offset ? ff->excl_offset[i] : 0, b1 = ff->excl_offset ? ff->excl_offset[i + 1] : 0;
     for (uint32_t p = b0; p < b1; ++p) {
@@ -287,7 +288,7 @@ void Engine::setup_ff(const caps_gpu_ff* ff) {
         const auto it = p14.find({uint32_t(i), j});
         xij.push_back(uint32_t(i));
         xij.push_back(j);
-        xf.push_back(float(it != p14.end() ? it->second : 0.0));
+        xf.push_back(it != p14.end() ? it->second : 0.0);
       }
     }
     eoff[size_t(i) + 1] = uint32_t(elist.size());
@@ -380,6 +381,30 @@ void Engine::setup_options() {
   d_tab_.upload(tab, stream_);
   d_tabd_.upload(tabd, stream_);
   d_lj14_.upload(l14, stream_);
+  // force-cap radii (field.cpp:557-581): where |F_LJ| reaches the cap, by bisection; beyond it nothing changes
+  std::vector<double4> cap(size_t(ntab) * ntab, make_double4(0, 0, 0, 0)), cap14(size_t(nt_) * nt_, make_double4(0, 0, 0, 0));
+  if (opt_.force_cap > 0)
+    for (int a0 = 0; a0 < nt_; ++a0)
+      for (int b0 = 0; b0 < nt_; ++b0) {
+        const double e = h_eps_[size_t(a0) * nt_ + b0], s6 = std::pow(h_sig_[size_t(a0) * nt_ + b0], 6);
+        if (e <= 0) continue;
+        const double sg = std::pow(s6, 1.0 / 6);
+        auto force = [&](double r) {
+          const double q = s6 / std::pow(r, 6);
+          return 24 * e / r * (2 * q * q - q);
+        };
+        double lo = 0.3 * sg, hi = std::pow(2 * s6, 1.0 / 6);
+        if (force(lo) < opt_.force_cap) continue;
+        for (int it = 0; it < 80; ++it) {
+          const double m = 0.5 * (lo + hi);
+          (force(m) > opt_.force_cap ? lo : hi) = m;
+        }
+        const double r = hi, q = s6 / std::pow(r, 6);
+        cap[size_t(a0) * ntab + b0] = make_double4(r * r, 4 * e * (q * q - q), force(r), 0.0);
+        cap14[size_t(a0) * nt_ + b0] = cap[size_t(a0) * ntab + b0];
+      }
+  d_tabcap_.upload(cap, stream_);
+  d_cap14_.upload(cap14, stream_);
   list_valid_ = false;
   green_valid_ = false;
   if (cell_set_) {
@@ -450,8 +475,7 @@ void Engine::set_cell(const double* cell) {
         bspline_moduli(pk_[d], order_, bsp);
         d_bsp_[d].upload(bsp, stream_);
       }
-      if (mixed_) pme_setup(pf_);
-      else pme_setup(pd_);
+      pme_setup(pd_);
     }
   }
 }
@@ -537,7 +561,7 @@ void Engine::pme_setup(PmePath<R>& P) {
   P.gt.alloc(half);
   P.wt.alloc(6 * half);
   if (mixed_) d_gridq_.alloc(size_t(pk_[0]) * pk_[1] * pk_[2]);
-  else d_grid_.alloc(size_t(pk_[0]) * pk_[1] * pk_[2]);
+  d_grid_.alloc(size_t(pk_[0]) * pk_[1] * pk_[2]);
   for (int d = 0; d < 3; ++d)
     for (int dir = 0; dir < 2; ++dir) {
       const int nn = pk_[d];
@@ -590,6 +614,7 @@ void Engine::pair_forces(bool ener, bool vir) {
   A.xqd = d_xqd_.p;
   A.tab = d_tab_.p;
   A.tabd = d_tabd_.p;
+  A.tabcap = d_tabcap_.p;
   A.gtab = d_gtab_.p;
   A.ntab = nt_ + 1;
   A.gnodes = gnodes_;
@@ -613,6 +638,7 @@ void Engine::pair_forces(bool ener, bool vir) {
   A.en.fix = d_efix_.p;
   A.en.dbl = d_edbl_.p;
   A.work_cap = int(d_work_.n);
+  A.err = d_counters_.p + kCntErr;
   const int coul = coul_ ? (pme_ ? 1 : 2) : 0;
   const int grid = dev_sms_ * 8;
   const int ntab = nt_ + 1;
@@ -629,12 +655,17 @@ void Engine::pair_forces(bool ener, bool vir) {
 #undef PAIR32
   } else {
     const size_t smem = sizeof(double4) * (size_t(ntab) * ntab + 4 * 64) + sizeof(double) * 2 * size_t(coul ? gnodes_ : 0) + sizeof(int) * 4 * 64;
-#define PAIR64(C, E, V)                                                                                              \
+#define PAIR64(C, ...)                                                                                               \
   do {                                                                                                               \
-    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_pair_f64<C, E, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
-    k_pair_f64<C, E, V><<<grid, 128, smem, stream_>>>(A);                                                            \
+    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_pair_f64<C, __VA_ARGS__>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
+    k_pair_f64<C, __VA_ARGS__><<<grid, 128, smem, stream_>>>(A);                                                     \
   } while (0)
-    if (coul == 1) { if (ener) { if (vir) PAIR64(1, true, true); else PAIR64(1, true, false); } else { if (vir) PAIR64(1, false, true); else PAIR64(1, false, false); } }
+    if (opt_.force_cap > 0) {
+      // push-off: energies and virial always on (a rare path, kept to one instantiation per Coulomb form)
+      if (coul == 1) PAIR64(1, true, true, true);
+      else if (coul == 2) PAIR64(2, true, true, true);
+      else PAIR64(0, true, true, true);
+    } else if (coul == 1) { if (ener) { if (vir) PAIR64(1, true, true); else PAIR64(1, true, false); } else { if (vir) PAIR64(1, false, true); else PAIR64(1, false, false); } }
     else if (coul == 2) { if (ener) { if (vir) PAIR64(2, true, true); else PAIR64(2, true, false); } else { if (vir) PAIR64(2, false, true); else PAIR64(2, false, false); } }
     else { if (ener) { if (vir) PAIR64(0, true, true); else PAIR64(0, true, false); } else { if (vir) PAIR64(0, false, true); else PAIR64(0, false, false); } }
 #undef PAIR64
@@ -647,40 +678,38 @@ void Engine::bonded_forces(const double* d_x, bool ener, bool vir) {
   const int T = 256;
   const bool bonded = (opt_.parts & 1) != 0, nonb = (opt_.parts & 2) != 0;
   auto nblk = [&](int cnt) { return std::min(blocks_for(size_t(std::max(cnt, 1)), T), dev_sms_ * 4); };
-#define LAUNCH3(K, R, cnt, ...)                                                                                     \
+#define LAUNCH3(K, S, cnt, ...)                                                                                     \
   do {                                                                                                              \
-    if (ener) { if (vir) K<R, true, true><<<nblk(cnt), T, 0, stream_>>>(__VA_ARGS__); else K<R, true, false><<<nblk(cnt), T, 0, stream_>>>(__VA_ARGS__); } \
-    else { if (vir) K<R, false, true><<<nblk(cnt), T, 0, stream_>>>(__VA_ARGS__); else K<R, false, false><<<nblk(cnt), T, 0, stream_>>>(__VA_ARGS__); } \
+    if (ener) { if (vir) K<double, S, true, true><<<nblk(cnt), T, 0, stream_>>>(__VA_ARGS__); else K<double, S, true, false><<<nblk(cnt), T, 0, stream_>>>(__VA_ARGS__); } \
+    else { if (vir) K<double, S, false, true><<<nblk(cnt), T, 0, stream_>>>(__VA_ARGS__); else K<double, S, false, false><<<nblk(cnt), T, 0, stream_>>>(__VA_ARGS__); } \
   } while (0)
-  auto run = [&](auto tag) {
-    using R = decltype(tag);
-    ForceSink<R> F;
-    if constexpr (sizeof(R) == 4) F = ForceSink<R>{d_F_.p, d_F_.p + n_, d_F_.p + 2 * size_t(n_)};
-    else F = ForceSink<R>{d_Fd_.p, d_Fd_.p + n_, d_Fd_.p + 2 * size_t(n_)};
+#define LAUNCHX(S, ...)                                                                                             \
+  do {                                                                                                              \
+    if (ener) { if (vir) k_excl_f64<S, true, true><<<nblk(nx_), T, 0, stream_>>>(__VA_ARGS__); else k_excl_f64<S, true, false><<<nblk(nx_), T, 0, stream_>>>(__VA_ARGS__); } \
+    else { if (vir) k_excl_f64<S, false, true><<<nblk(nx_), T, 0, stream_>>>(__VA_ARGS__); else k_excl_f64<S, false, false><<<nblk(nx_), T, 0, stream_>>>(__VA_ARGS__); } \
+  } while (0)
+  auto run = [&](auto sink) {
+    using S = decltype(sink);
+    const S F = sink;
     if (bonded) {
-      if (nb_) LAUNCH3(k_bonds, R, nb_, nb_, d_bond_ij_.p, d_bond_kr_.p, A, F);
-      if (na_) LAUNCH3(k_angles, R, na_, na_, d_angle_ijk_.p, d_angle_kt_.p, A, F);
-      if (ndg_) LAUNCH3(k_torsions, R, ndg_, ndg_, d_dih_grp_.p, d_dih_ijkl_.p, d_dih_vd_.p, d_dih_n_.p, A, F, int(kEDihedral));
-      if (nig_) LAUNCH3(k_torsions, R, nig_, nig_, d_imp_grp_.p, d_imp_ijkl_.p, d_imp_vd_.p, d_imp_n_.p, A, F, int(kEImproper));
-      if (nfene_) LAUNCH3(k_fene, R, nfene_, nfene_, d_fene_ij_.p, d_fene_p_.p, A, F, d_counters_.p);
+      if (nb_) LAUNCH3(k_bonds, S, nb_, nb_, d_bond_ij_.p, d_bond_kr_.p, A, F);
+      if (na_) LAUNCH3(k_angles, S, na_, na_, d_angle_ijk_.p, d_angle_kt_.p, A, F);
+      if (ndg_) LAUNCH3(k_torsions, S, ndg_, ndg_, d_dih_grp_.p, d_dih_ijkl_.p, d_dih_vd_.p, d_dih_n_.p, A, F, int(kEDihedral));
+      if (nig_) LAUNCH3(k_torsions, S, nig_, nig_, d_imp_grp_.p, d_imp_ijkl_.p, d_imp_vd_.p, d_imp_n_.p, A, F, int(kEImproper));
+      if (nfene_) LAUNCH3(k_fene, S, nfene_, nfene_, d_fene_ij_.p, d_fene_p_.p, A, F, d_counters_.p);
     }
     if (nonb && np14_)
-      LAUNCH3(k_pairs14, R, np14_, np14_, d_p14_ij_.p, p14_scaled_ ? d_p14_scale_.p : nullptr, lj14_, d_type_.p, nt_, d_lj14_.p,
-              (const double4*)nullptr, A, F);
+      LAUNCH3(k_pairs14, S, np14_, np14_, d_p14_ij_.p, p14_scaled_ ? d_p14_scale_.p : nullptr, lj14_, d_type_.p, nt_, d_lj14_.p,
+              opt_.force_cap > 0 ? (const double4*)d_cap14_.p : (const double4*)nullptr, A, F);
     if (nonb && coul_ && nx_) {
       ExclArgs E{d_excl_ij_.p, d_excl_f_.p, d_q_.p, d_gtab_.p, ghi_, rc_, rc_ * rc_, kappa_, dsf_e0_, dsf_f0_, pme_ ? 1 : 0};
-      if constexpr (sizeof(R) == 4) {
-        if (ener) { if (vir) k_excl_f32<true, true><<<nblk(nx_), T, 0, stream_>>>(nx_, E, A, F); else k_excl_f32<true, false><<<nblk(nx_), T, 0, stream_>>>(nx_, E, A, F); }
-        else { if (vir) k_excl_f32<false, true><<<nblk(nx_), T, 0, stream_>>>(nx_, E, A, F); else k_excl_f32<false, false><<<nblk(nx_), T, 0, stream_>>>(nx_, E, A, F); }
-      } else {
-        if (ener) { if (vir) k_excl_f64<true, true><<<nblk(nx_), T, 0, stream_>>>(nx_, E, A, F); else k_excl_f64<true, false><<<nblk(nx_), T, 0, stream_>>>(nx_, E, A, F); }
-        else { if (vir) k_excl_f64<false, true><<<nblk(nx_), T, 0, stream_>>>(nx_, E, A, F); else k_excl_f64<false, false><<<nblk(nx_), T, 0, stream_>>>(nx_, E, A, F); }
-      }
+      LAUNCHX(S, nx_, E, A, F);
     }
   };
-  if (mixed_) run(float{});
-  else run(double{});
+  if (mixed_) run(ForceSink<float>{d_F_.p, d_F_.p + n_, d_F_.p + 2 * size_t(n_), d_counters_.p + kCntErr});
+  else run(ForceSink<double>{d_Fd_.p, d_Fd_.p + n_, d_Fd_.p + 2 * size_t(n_)});
 #undef LAUNCH3
+#undef LAUNCHX
   CK(cudaGetLastError());
 }
 
@@ -697,7 +726,11 @@ void Engine::pme_run(PmePath<R>& P, const double* d_x, bool ener, bool vir) {
   const int nb = blocks_for(size_t(n_), 128);
   if (mixed_) CK(cudaMemsetAsync(d_gridq_.p, 0, d_gridq_.n * sizeof(long long), stream_));
   else CK(cudaMemsetAsync(d_grid_.p, 0, d_grid_.n * sizeof(double), stream_));
-#define SPREAD(P_) k_spread<R, P_><<<nb, 128, 0, stream_>>>(A, d_grid_.p, d_gridq_.p)
+#define SPREAD(P_)                                                                            \
+  do {                                                                                        \
+    if (mixed_) k_spread<float, P_><<<nb, 128, 0, stream_>>>(A, d_grid_.p, d_gridq_.p);      \
+    else k_spread<double, P_><<<nb, 128, 0, stream_>>>(A, d_grid_.p, d_gridq_.p);            \
+  } while (0)
   switch (order_) {
     case 3: SPREAD(3); break;
     case 4: SPREAD(4); break;
@@ -719,10 +752,13 @@ void Engine::pme_run(PmePath<R>& P, const double* d_x, bool ener, bool vir) {
   else { if (vir) k_fft_z_solve<R, false, true><<<gz, 256, sz, stream_>>>(A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); else k_fft_z_solve<R, false, false><<<gz, 256, sz, stream_>>>(A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); }
   k_fft_y<R><<<gy, 256, sy, stream_>>>(A, P.h.p, P.plan[1][1], lines_y_);
   k_fft_x_inv<R><<<blocks_for(size_t(nlx), lines_x_), 256, sx, stream_>>>(A, P.h.p, P.gr.p, P.plan[0][1], lines_x_);
-  ForceSink<R> F;
-  if constexpr (sizeof(R) == 4) F = ForceSink<R>{d_F_.p, d_F_.p + n_, d_F_.p + 2 * size_t(n_)};
-  else F = ForceSink<R>{d_Fd_.p, d_Fd_.p + n_, d_Fd_.p + 2 * size_t(n_)};
-#define GATHER(P_) k_gather<R, P_><<<nb, 128, 0, stream_>>>(A, P.gr.p, F)
+  const ForceSink<float> Ff{d_F_.p, d_F_.p + n_, d_F_.p + 2 * size_t(n_), d_counters_.p + kCntErr};
+  const ForceSink<double> Fd{d_Fd_.p, d_Fd_.p + n_, d_Fd_.p + 2 * size_t(n_)};
+#define GATHER(P_)                                                                            \
+  do {                                                                                        \
+    if (mixed_) k_gather<float, R, P_><<<nb, 128, 0, stream_>>>(A, P.gr.p, Ff);              \
+    else k_gather<double, R, P_><<<nb, 128, 0, stream_>>>(A, P.gr.p, Fd);                     \
+  } while (0)
   switch (order_) {
     case 3: GATHER(3); break;
     case 4: GATHER(4); break;
@@ -735,10 +771,7 @@ void Engine::pme_run(PmePath<R>& P, const double* d_x, bool ener, bool vir) {
   CK(cudaGetLastError());
 }
 
-void Engine::pme_forces(const double* d_x, bool ener, bool vir) {
-  if (mixed_) pme_run(pf_, d_x, ener, vir);
-  else pme_run(pd_, d_x, ener, vir);
-}
+void Engine::pme_forces(const double* d_x, bool ener, bool vir) { pme_run(pd_, d_x, ener, vir); }
 
 // One force evaluation on device positions d_x (AoS, 3 n): accumulators cleared, list checked / rebuilt, every term,
 // forces reduced into d_f_ (AoS doubles). Asynchronous on stream_.
@@ -794,6 +827,8 @@ void Engine::check_errors() {
   if (e & (kErrShake | kErrShakeTurn))
     throw ModelError(CAPS_GPU_ECONSTRAINT, (e & kErrShakeTurn) ? "a constrained bond turned by more than 90° in one step; lower the time step or relax first"
                                                                  : "the bond constraints did not converge (SHAKE); lower the time step or relax first");
+  if (e & kErrFixRange)
+    throw ModelError(CAPS_GPU_EFIELD, "a force beyond the fixed-point range (2e9 kcal/mol/Å): overlapping atoms; push the structure off first (FP64 with a force cap)");
   if (e & kErrNonFinite) throw ModelError(CAPS_GPU_EFIELD, "the simulation became unstable; lower the time step or relax first");
   throw ModelError(CAPS_GPU_EINVAL, "device error word " + std::to_string(e));
 }
@@ -840,7 +875,7 @@ void Engine::host_constants(caps_gpu_terms* t, bool ener, bool vir) const {
 void Engine::read_terms(caps_gpu_terms* out, bool ener, bool vir) {
   caps_gpu_terms t{};
   double e[kENumSlots];
-  for (int k = 0; k < kENumSlots; ++k) e[k] = mixed_ ? double(h_efix_[k]) * kInvFixF : h_edbl_[k];
+  for (int k = 0; k < kENumSlots; ++k) e[k] = mixed_ ? double(h_efix_[k]) * kInvFixE : h_edbl_[k];
   t.bond = e[kEBond];
   t.angle = e[kEAngle];
   t.dihedral = e[kEDihedral];
@@ -990,6 +1025,22 @@ int32_t caps_gpu_run(caps_gpu_engine* e, caps_gpu_state* state, const caps_gpu_m
 double caps_gpu_last_steps_per_second(const caps_gpu_engine* e) { return e ? e->e->last_steps_per_second() : 0.0; }
 
 void caps_gpu_destroy(caps_gpu_engine* e) { delete e; }
+
+int32_t caps_gpu_diag_set_timing(caps_gpu_engine* e, int64_t flush_bytes) {
+  if (!e) return CAPS_GPU_EINVAL;
+  e->e->set_timing(flush_bytes);
+  return CAPS_GPU_OK;
+}
+
+double caps_gpu_diag_last_step_ms(const caps_gpu_engine* e) { return e ? e->e->last_step_ms_device() : 0.0; }
+
+int32_t caps_gpu_diag_step_kernels(const caps_gpu_engine* e) { return e ? e->e->graph_kernels() : 0; }
+
+int32_t caps_gpu_diag_pair_timing(caps_gpu_engine* e, const double* x, const double* cell, int32_t launches, int64_t flush_bytes, double* avg_ms,
+                                  double* pairs_in, double* pairs_listed, double* entries) {
+  if (!e || !x || !cell || launches < 1) return CAPS_GPU_EINVAL;
+  return guard(e, [&] { e->e->time_pair_kernel(x, cell, launches, flush_bytes, avg_ms, pairs_in, pairs_listed, entries); });
+}
 
 const char* caps_gpu_error(const caps_gpu_engine* e) { return e ? e->err.c_str() : g_create_error.c_str(); }
 

@@ -95,6 +95,12 @@ class Engine {
   int list_builds() const { return builds_; }
   void run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progress_fn progress, caps_gpu_frame_fn frame, void* user, std::string* report);
   double last_steps_per_second() const { return last_sps_; }
+  // measurement support (include/caps_gpu_diag.h)
+  void set_timing(int64_t flush_bytes) { timing_flush_ = flush_bytes; }
+  void time_pair_kernel(const double* x, const double* cell, int launches, int64_t flush_bytes, double* avg_ms, double* pairs_in,
+                        double* pairs_listed, double* entries);
+  double last_step_ms_device() const { return last_step_ms_; }
+  int graph_kernels() const { return graph_kernels_; }
   std::string err;
 
   // --- internals used by the step kernels' launcher (integrate.cu) ---
@@ -131,14 +137,14 @@ class Engine {
   std::vector<std::array<uint32_t, 3>> ha_;   // angles and theta0, for rigid waters
   std::vector<double> hth0_;
   DevBuf<float4> d_tab_;
-  DevBuf<double4> d_tabd_, d_lj14_;
+  DevBuf<double4> d_tabd_, d_lj14_, d_tabcap_, d_cap14_;
   DevBuf<double> d_gtab_;
   int gnodes_ = 0;
   double ghi_ = 0;
   DevBuf<uint32_t> d_bond_ij_, d_angle_ijk_, d_dih_ijkl_, d_imp_ijkl_, d_p14_ij_, d_excl_ij_, d_fene_ij_;
   DevBuf<double> d_bond_kr_, d_angle_kt_, d_dih_vd_, d_imp_vd_, d_p14_scale_, d_fene_p_;
   DevBuf<int> d_dih_n_, d_imp_n_, d_dih_grp_, d_imp_grp_;
-  DevBuf<float> d_excl_f_;
+  DevBuf<double> d_excl_f_;
   DevBuf<uint32_t> d_excl_off_, d_excl_list_;
   int nb_ = 0, na_ = 0, nd_ = 0, ndg_ = 0, ni_ = 0, nig_ = 0, np14_ = 0, nx_ = 0, nfene_ = 0;
   double lj14_ = 0.5;
@@ -187,13 +193,15 @@ class Engine {
   DevBuf<double> d_bsp_[3];
   DevBuf<double> d_grid_;           // FP64 spread grid
   DevBuf<long long> d_gridq_;       // FP32 path: fixed-point spread grid
-  PmePath<float> pf_;
   PmePath<double> pd_;
   double green_cell_[12] = {0};
   bool green_valid_ = false;
   int lines_x_ = 1, lines_y_ = 1, lines_z_ = 1;
 
-  double last_sps_ = 0;
+  double last_sps_ = 0, last_step_ms_ = 0;
+  int64_t timing_flush_ = -1;
+  int graph_kernels_ = 0;
+  DevBuf<unsigned char> d_flush_;
   int dev_sms_ = 148;
 };
 

@@ -753,10 +753,30 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
   cudaEvent_t ev0, ev1;
   CK(cudaEventCreate(&ev0));
   CK(cudaEventCreate(&ev1));
+  // measurement mode (include/caps_gpu_diag.h): an event pair around every step and an L2 flush between steps
+  const bool timed = timing_flush_ >= 0;
+  std::vector<cudaEvent_t> tev;
+  if (timed) {
+    tev.resize(size_t(2 * std::max<long long>(o.steps, 0)));
+    for (auto& e : tev) CK(cudaEventCreate(&e));
+    if (timing_flush_ > 0) d_flush_.alloc(size_t(timing_flush_));
+  }
   const auto w0 = std::chrono::steady_clock::now();
   CK(cudaEventRecord(ev0, stream_));
   bool have_graph = false;
   for (long long s = 1; s <= o.steps; ++s) {
+    if (timed) {
+      if (timing_flush_ > 0) CK(cudaMemsetAsync(d_flush_.p, int(s & 255), size_t(timing_flush_), stream_));
+      CK(cudaEventRecord(tev[size_t(2 * (s - 1))], stream_));
+    }
+    struct EndEvent {
+      bool on;
+      cudaEvent_t e;
+      cudaStream_t st;
+      ~EndEvent() {
+        if (on) cudaEventRecord(e, st);
+      }
+    } end_ev{timed, timed ? tev[size_t(2 * (s - 1) + 1)] : nullptr, stream_};
     if (S.bussi && s - S.draws_first >= S.draws_count) {
       CK(cudaStreamSynchronize(stream_));
       S.make_draws(s, std::min<long long>(o.steps - s + 1, 4096));
@@ -772,6 +792,17 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
         CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
         S.step(false, false);
         CK(cudaStreamEndCapture(stream_, &g));
+        size_t nn = 0;
+        CK(cudaGraphGetNodes(g, nullptr, &nn));
+        std::vector<cudaGraphNode_t> nodes(nn);
+        CK(cudaGraphGetNodes(g, nodes.data(), &nn));
+        int kernels = 0;
+        for (auto nd : nodes) {
+          cudaGraphNodeType ty;
+          CK(cudaGraphNodeGetType(nd, &ty));
+          kernels += ty == cudaGraphNodeTypeKernel;
+        }
+        graph_kernels_ = kernels;
         CK(cudaGraphInstantiate(&S.graph, g, 0));
         CK(cudaGraphDestroy(g));
         have_graph = true;
@@ -834,6 +865,17 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
   CK(cudaEventSynchronize(ev1));
   float ms = 0;
   CK(cudaEventElapsedTime(&ms, ev0, ev1));
+  if (timed && o.steps > 0) {
+    double sum = 0;
+    for (long long k = 0; k < o.steps; ++k) {
+      float t = 0;
+      CK(cudaEventElapsedTime(&t, tev[size_t(2 * k)], tev[size_t(2 * k + 1)]));
+      sum += t;
+    }
+    for (auto& e : tev) cudaEventDestroy(e);
+    ms = float(sum);
+  }
+  last_step_ms_ = o.steps > 0 ? double(ms) / double(o.steps) : 0.0;
   const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
   cudaEventDestroy(ev0);
   cudaEventDestroy(ev1);

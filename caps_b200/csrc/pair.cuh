@@ -72,6 +72,7 @@ struct PairArgs {
   const double4* xqd;    // FP64 path
   const float4* tab;     // FP32: per type pair (c6, c12, energy shift, 0)
   const double4* tabd;   // FP64: per type pair (c6, c12, energy shift, 0)
+  const double4* tabcap; // FP64 with a force cap: per type pair (r_cap^2, E at r_cap, |F| at r_cap, 0)
   const double* gtab;    // FP64 Ewald table: 2 per node (G, h dG/ds)
   int ntab;              // types incl. the padding type
   int gnodes;            // table nodes
@@ -86,6 +87,7 @@ struct PairArgs {
   double* fdz;
   EnergySink en;
   int work_cap;
+  int* err;              // the error word (range errors of the fixed-point sums)
 };
 
 // --- FP32 path ---------------------------------------------------------------------------------------------------
@@ -109,7 +111,7 @@ static __global__ void __launch_bounds__(128, 4) k_pair_f32(PairArgs A) {
   const float rc2 = float(A.rc2), beta = float(A.beta), kc = float(A.kc), kcoul = float(A.kcoul);
   const float e0 = float(A.dsf_e0), f0 = float(A.dsf_f0), rcf = float(A.rc);
   const int nwarps = gridDim.x * 4;
-  double acc_v = 0, acc_c = 0, acc_w[6] = {0, 0, 0, 0, 0, 0};
+  double acc_v = 0, acc_c = 0, acc_w[6] = {0, 0, 0, 0, 0, 0}, acc_np = 0, acc_nl = 0;
   for (int w = blockIdx.x * 4 + wib; w < nwork; w += nwarps) {
     const int4 wk = A.work[w];
     const int sc = wk.x;
@@ -126,7 +128,7 @@ static __global__ void __launch_bounds__(128, 4) k_pair_f32(PairArgs A) {
     float fix[8], fiy[8], fiz[8];
 #pragma unroll
     for (int c = 0; c < 8; ++c) fix[c] = fiy[c] = fiz[c] = 0.f;
-    float ev = 0.f, ec = 0.f, vw[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float ev = 0.f, ec = 0.f, vw[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, npair = 0.f, nlist = 0.f;
     for (int e = wk.y; e < wk.y + wk.z; ++e) {
       const uint4 en = A.ent[e];
       const float4 sh = A.ent_shift[e];
@@ -154,6 +156,10 @@ static __global__ void __launch_bounds__(128, 4) k_pair_f32(PairArgs A) {
           const float dx = xj - xi.x, dy = yj - xi.y, dz = zj - xi.z;
           const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
           const bool ok = oki && ((mm >> bit) & 1ull) && (r2 < rc2);
+          if (ENER) {
+            npair += ok ? 1.f : 0.f;
+            nlist += (oki && ((mm >> bit) & 1ull)) ? 1.f : 0.f;
+          }
           const float r2s = ok ? r2 : 1.f;
           const float rinv = rsqrtf(r2s);
           const float r2i = rinv * rinv;
@@ -208,7 +214,7 @@ static __global__ void __launch_bounds__(128, 4) k_pair_f32(PairArgs A) {
         const float v = i8 == 0 ? f0x : i8 == 1 ? f0y : i8 == 2 ? f0z : i8 == 3 ? f1x : i8 == 4 ? f1y : f1z;
         const int js = i8 < 3 ? j0 : j1;
         long long* dst = (i8 % 3 == 0) ? A.fsx : (i8 % 3 == 1) ? A.fsy : A.fsz;
-        if (v != 0.f) atomic_add_fix(dst + js, to_fixf(v));
+        if (v != 0.f) fix_add_f(dst + js, v, A.err);
       }
     }
     // i forces: sum over the 4 lanes of each i atom, then lanes share the adds
@@ -225,13 +231,15 @@ static __global__ void __launch_bounds__(128, 4) k_pair_f32(PairArgs A) {
     for (int c = 0; c < 8; ++c) {
       if ((c & 3) != jq || !((ireal >> c) & 1u)) continue;
       const int s = 64 * sc + 8 * c + i8;
-      if (fix[c] != 0.f) atomic_add_fix(A.fsx + s, to_fixf(fix[c]));
-      if (fiy[c] != 0.f) atomic_add_fix(A.fsy + s, to_fixf(fiy[c]));
-      if (fiz[c] != 0.f) atomic_add_fix(A.fsz + s, to_fixf(fiz[c]));
+      if (fix[c] != 0.f) fix_add_f(A.fsx + s, fix[c], A.err);
+      if (fiy[c] != 0.f) fix_add_f(A.fsy + s, fiy[c], A.err);
+      if (fiz[c] != 0.f) fix_add_f(A.fsz + s, fiz[c], A.err);
     }
     if (ENER) {
       acc_v += double(warp_sum(ev));
       acc_c += double(warp_sum(ec));
+      acc_np += double(warp_sum(npair));
+      acc_nl += double(warp_sum(nlist));
     }
     if (VIR)
       for (int k = 0; k < 6; ++k) acc_w[k] += double(warp_sum(vw[k]));
@@ -241,6 +249,8 @@ static __global__ void __launch_bounds__(128, 4) k_pair_f32(PairArgs A) {
     if (ENER) {
       A.en.add(kEVdw, acc_v, true);
       A.en.add(kECoul, acc_c, true);
+      A.en.add(kEPairs, acc_np, true);
+      A.en.add(kEListed, acc_nl, true);
     }
     if (VIR)
       for (int k = 0; k < 6; ++k) A.en.add(kEW0 + k, acc_w[k], true);
@@ -260,7 +270,7 @@ __device__ __forceinline__ void ewald_ef(const double* __restrict__ gt, double g
   F = rinv * rinv * rinv + 2 * dG;
 }
 
-template <int COUL, bool ENER, bool VIR>
+template <int COUL, bool ENER, bool VIR, bool CAP = false>
 static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
   extern __shared__ double4 smem_d4[];
   double4* tab = smem_d4;                                   // ntab * ntab
@@ -330,8 +340,17 @@ static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
           if (!ok) continue;
           const double r2i = 1 / r2, r6i = r2i * r2i * r2i, rinv = sqrt(r2i);
           const double4 cc = tab[ti * A.ntab + tj];
-          double fr = r6i * (12 * cc.y * r6i - 6 * cc.x) * r2i;
-          if (ENER) ev += r6i * (cc.y * r6i - cc.x) - cc.z;
+          double fr;
+          const double4 cp = CAP ? A.tabcap[ti * A.ntab + tj] : make_double4(0, 0, 0, 0);
+          if (CAP && r2 < cp.x) {
+            // the push-off cap (field.cpp:1534-1538): LJ continued linearly inside the radius where |F| reaches the cap
+            const double r = r2 * rinv, rcp = sqrt(cp.x);
+            fr = cp.z / r * rinv;
+            if (ENER) ev += cp.y + cp.z * (rcp - r) - cc.z;
+          } else {
+            fr = r6i * (12 * cc.y * r6i - 6 * cc.x) * r2i;
+            if (ENER) ev += r6i * (cc.y * r6i - cc.x) - cc.z;
+          }
           if (COUL != 0) {
             const double qq = xi.w * aj.w;
             double E, Fc;

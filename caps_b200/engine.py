@@ -171,6 +171,26 @@ class Evaluator:
                                               f.ctypes.data_as(C.c_void_p), C.byref(t)))
         return t.as_dict(), f.reshape(-1, 3)
 
+    def set_timing(self, flush_bytes: int):
+        """Measurement mode for run(): per-step CUDA events, an L2 flush of flush_bytes between steps (< 0: off)."""
+        self._check(self.lib.caps_gpu_diag_set_timing(self.h, int(flush_bytes)))
+
+    def last_step_ms(self) -> float:
+        return float(self.lib.caps_gpu_diag_last_step_ms(self.h))
+
+    def step_kernels(self) -> int:
+        """Kernel launches in one plain MD step of the last run (the captured graph's kernel nodes)."""
+        return int(self.lib.caps_gpu_diag_step_kernels(self.h))
+
+    def pair_timing(self, x, cell, launches: int = 50, flush_bytes: int = 0) -> dict:
+        """The pair kernel alone: mean launch time and the pairs it evaluates (include/caps_gpu_diag.h)."""
+        x = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1))
+        c = cell_array(cell)
+        ms, pin, pl, ne = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+        self._check(self.lib.caps_gpu_diag_pair_timing(self.h, x.ctypes.data_as(C.c_void_p), c.ctypes.data_as(C.c_void_p), launches,
+                                                       int(flush_bytes), C.byref(ms), C.byref(pin), C.byref(pl), C.byref(ne)))
+        return {"avg_ms": ms.value, "pairs_in_cutoff": pin.value, "pairs_listed": pl.value, "entries": ne.value}
+
     def list_builds(self) -> int:
         return int(self.lib.caps_gpu_list_builds(self.h))
 

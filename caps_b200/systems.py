@@ -1,0 +1,363 @@
+"""Synthetic cells of the benchmark shapes, built from seeds (no files, no network).
+
+polystyrene_melt: atactic polystyrene, 16 atoms per repeat unit, OPLS-AA-style parameters (geometric mixing, 1-4 at 0.5,
+aromatic C -0.115 / H +0.115, backbone CH2 and CH balanced to neutral), grown as random-walk chains in a cubic box at
+the target density. kg_melt: Kremer-Grest bead-spring chains (WCA + FENE). spce_water: rigid SPC/E water on a jittered
+lattice with random orientations. The geometry code is this package's own; the overlaps a dense growth leaves are
+removed by push_off (capped-force FP64 MD on the device) before a run.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .forcefield import ForceField
+
+KB = 0.0019872041   # kcal/(mol K)
+NA = 6.02214076e23
+M_C, M_H, M_O = 12.011, 1.008, 15.999
+
+
+# --- topology helpers -----------------------------------------------------------------------------------------
+def _graph(n: int, bonds: np.ndarray) -> list[list[int]]:
+    nb = [[] for _ in range(n)]
+    for i, j in bonds:
+        nb[int(i)].append(int(j))
+        nb[int(j)].append(int(i))
+    return nb
+
+
+def angles_from_bonds(nb: list[list[int]]) -> np.ndarray:
+    out = []
+    for j, ns in enumerate(nb):
+        for a in range(len(ns)):
+            for b in range(a + 1, len(ns)):
+                out.append((ns[a], j, ns[b]))
+    return np.array(out, dtype=np.uint32).reshape(-1, 3)
+
+
+def dihedrals_from_bonds(nb: list[list[int]], bonds: np.ndarray) -> np.ndarray:
+    out = []
+    for j, k in bonds:
+        j, k = int(j), int(k)
+        for i in nb[j]:
+            if i == k:
+                continue
+            for l in nb[k]:
+                if l == j or l == i:
+                    continue
+                out.append((i, j, k, l))
+    return np.array(out, dtype=np.uint32).reshape(-1, 4)
+
+
+def exclusions(n: int, nb: list[list[int]], depth: int = 3) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """CSR of partners within `depth` bonds, and the 1-4 pairs (exactly 3 bonds apart, not closer)."""
+    off = np.zeros(n + 1, np.uint32)
+    lst, p14 = [], []
+    for i in range(n):
+        dist = {i: 0}
+        frontier = [i]
+        for d in range(1, depth + 1):
+            nxt = []
+            for a in frontier:
+                for b in nb[a]:
+                    if b not in dist:
+                        dist[b] = d
+                        nxt.append(b)
+            frontier = nxt
+        part = sorted(j for j in dist if j != i)
+        lst += part
+        off[i + 1] = len(lst)
+        p14 += [(i, j) for j in part if dist[j] == 3 and j > i]
+    return off, np.array(lst, np.uint32), np.array(p14, np.uint32).reshape(-1, 2)
+
+
+def _unit(v):
+    return v / np.linalg.norm(v)
+
+
+def _nerf(a, b, c, bond, angle, torsion):
+    """Position of d with |cd| = bond, angle bcd, dihedral abcd (radians)."""
+    bc = _unit(c - b)
+    nrm = _unit(np.cross(b - a, bc))
+    m = np.array([bc, np.cross(nrm, bc), nrm]).T
+    d2 = np.array([-bond * math.cos(angle), bond * math.sin(angle) * math.cos(torsion), bond * math.sin(angle) * math.sin(torsion)])
+    return c + m @ d2
+
+
+class _Grid:
+    """A cell list over a periodic cubic box for overlap checks while growing."""
+
+    def __init__(self, L: float, cell: float = 3.2, cap: int = 24):
+        self.L = L
+        self.n = max(3, int(L / cell))
+        self.h = L / self.n
+        self.cap = cap
+        self.cnt = np.zeros((self.n,) * 3, np.int32)
+        self.idx = np.full((self.n,) * 3 + (cap,), -1, np.int64)
+        self.pos: list[np.ndarray] = []
+
+    def add(self, p: np.ndarray, owner: int):
+        c = tuple((np.floor(p / self.h).astype(int)) % self.n)
+        k = self.cnt[c]
+        if k < self.cap:
+            self.idx[c + (k,)] = len(self.pos)
+            self.cnt[c] += 1
+        self.pos.append(np.asarray(p, float))
+
+    def min_dist(self, pts: np.ndarray, skip_from: int) -> float:
+        """Smallest distance from pts to stored atoms with index < skip_from (minimum image)."""
+        if not self.pos or skip_from <= 0:
+            return 1e9
+        P = np.array(self.pos[:skip_from]) if False else None  # noqa: F841  (kept lazy below)
+        cells = np.floor(pts / self.h).astype(int)
+        lo, hi = cells.min(0) - 1, cells.max(0) + 2
+        ids = []
+        for a in range(lo[0], hi[0]):
+            for b in range(lo[1], hi[1]):
+                for c in range(lo[2], hi[2]):
+                    t = (a % self.n, b % self.n, c % self.n)
+                    k = self.cnt[t]
+                    if k:
+                        ids.append(self.idx[t][:k])
+        if not ids:
+            return 1e9
+        ids = np.concatenate(ids)
+        ids = ids[ids < skip_from]
+        if ids.size == 0:
+            return 1e9
+        Q = np.array([self.pos[i] for i in ids])
+        d = pts[:, None, :] - Q[None, :, :]
+        d -= self.L * np.round(d / self.L)
+        return float(np.sqrt((d * d).sum(-1)).min())
+
+
+# OPLS-AA-style parameters (kcal/mol, Å, degrees): classes CT (sp3 C), CA (aromatic C), HC, HA
+_LJ = {"CT": (0.066, 3.50), "CA": (0.070, 3.55), "HC": (0.030, 2.50), "HA": (0.030, 2.42)}
+_BOND = {("CT", "CT"): (268.0, 1.529), ("CT", "HC"): (340.0, 1.090), ("CA", "CA"): (469.0, 1.400), ("CA", "HA"): (367.0, 1.080),
+         ("CA", "CT"): (317.0, 1.510)}
+_ANGLE = {("CT", "CT", "CT"): (58.35, 112.7), ("CT", "CT", "HC"): (37.5, 110.7), ("HC", "CT", "HC"): (33.0, 107.8),
+          ("CA", "CT", "CT"): (63.0, 114.0), ("CA", "CT", "HC"): (35.0, 109.5), ("CA", "CA", "CT"): (70.0, 120.0),
+          ("CA", "CA", "CA"): (63.0, 120.0), ("CA", "CA", "HA"): (35.0, 120.0)}
+# OPLS Fourier V1, V2, V3 (E = V1/2 (1 + cos phi) + V2/2 (1 - cos 2 phi) + V3/2 (1 + cos 3 phi))
+_TORS = {("CT", "CT", "CT", "CT"): (1.740, -0.157, 0.279), ("CT", "CT", "CT", "HC"): (0.0, 0.0, 0.300),
+         ("HC", "CT", "CT", "HC"): (0.0, 0.0, 0.300), ("CA", "CA", "CA", "CA"): (0.0, 7.250, 0.0),
+         ("CA", "CA", "CA", "HA"): (0.0, 7.250, 0.0), ("HA", "CA", "CA", "HA"): (0.0, 7.250, 0.0),
+         ("CA", "CA", "CA", "CT"): (0.0, 7.250, 0.0), ("CT", "CA", "CA", "HA"): (0.0, 7.250, 0.0),
+         ("CA", "CA", "CT", "CT"): (0.0, 0.0, 0.0), ("CA", "CA", "CT", "HC"): (0.0, 0.0, 0.0),
+         ("CA", "CT", "CT", "CT"): (-2.4, 0.0, 0.0), ("CA", "CT", "CT", "HC"): (0.0, 0.0, 0.462),
+         ("CA", "CT", "CT", "CA"): (0.0, 0.0, 0.0)}
+_Q = {"CA": -0.115, "HA": 0.115}
+
+
+def _key_sym(d: dict, k: tuple):
+    if k in d:
+        return d[k]
+    return d.get(tuple(reversed(k)))
+
+
+def polystyrene_melt(chains: int = 40, dp: int = 50, density: float = 1.04, seed: int = 1, min_sep: float = 2.4,
+                     trials: int = 24, grow: bool = True) -> tuple[ForceField, np.ndarray, np.ndarray]:
+    """Atactic polystyrene, `chains` x `dp` repeat units of 16 atoms (CH2-CH(C6H5), chain ends left open so the count
+    is exactly 16 per unit), at `density` g/cm^3 in a cubic periodic box. Returns (force field, x [n,3], cell[12]).
+    grow=False skips the geometry (positions left zero; the topology and force field do not depend on it)."""
+    rng = np.random.default_rng(seed)
+    n_unit = 16
+    n = chains * dp * n_unit
+    mass_unit = 8 * M_C + 8 * M_H
+    L = (chains * dp * mass_unit / (density * NA) * 1e24) ** (1.0 / 3.0)
+    grid = _Grid(L)
+    x = np.zeros((n, 3))
+    cls = [""] * n
+    bonds = []
+    tet = math.radians(112.7)
+    for ch in range(chains):
+        base = ch * dp * n_unit
+        # backbone: CH2 (index 0 of a unit) and CH (index 1); three seed points for the NeRF frames
+        p0 = rng.uniform(0, L, 3)
+        d1 = _unit(rng.normal(size=3))
+        p1 = p0 + 1.529 * d1
+        perp = _unit(np.cross(d1, _unit(rng.normal(size=3))))
+        p_prev2 = p0 - 1.529 * (math.cos(math.pi - tet) * d1 + math.sin(math.pi - tet) * perp)
+        bb = [p_prev2, p0, p1]
+        chain_first_atom = len(grid.pos)
+        for u in range(dp):
+            a_ch2, a_ch = base + u * n_unit, base + u * n_unit + 1
+            best, best_d = None, -1.0
+            for _ in range(trials if grow else 1):
+                if u == 0:
+                    q_ch2, q_ch = bb[1], bb[2]
+                    q_prev = bb[0]
+                else:
+                    t1 = rng.choice([math.pi, math.pi / 3, -math.pi / 3], p=[0.6, 0.2, 0.2])
+                    t2 = rng.choice([math.pi, math.pi / 3, -math.pi / 3], p=[0.6, 0.2, 0.2])
+                    q_ch2 = _nerf(bb[-3], bb[-2], bb[-1], 1.529, tet, t1)
+                    q_ch = _nerf(bb[-2], bb[-1], q_ch2, 1.529, tet, t2)
+                    q_prev = bb[-1]
+                # the next backbone atom direction (for the CH's tetrahedral sites)
+                q_next = _nerf(q_prev, q_ch2, q_ch, 1.529, tet, math.pi)
+                u1, u2 = _unit(q_ch2 - q_ch), _unit(q_next - q_ch)
+                bis, nrm = _unit(-(u1 + u2)), _unit(np.cross(u1, u2))
+                side = 1.0 if rng.random() < 0.5 else -1.0     # tacticity: which site holds the ring
+                ang = math.radians(54.75)
+                d_ring = _unit(bis * math.cos(ang) + side * nrm * math.sin(ang))
+                d_h = _unit(bis * math.cos(ang) - side * nrm * math.sin(ang))
+                ipso = q_ch + 1.510 * d_ring
+                centre = ipso + 1.400 * d_ring
+                e2 = _unit(np.cross(d_ring, _unit(rng.normal(size=3))))
+                e3 = np.cross(d_ring, e2)
+                ring = [centre + 1.400 * (-d_ring * math.cos(math.radians(60 * k)) + e2 * math.sin(math.radians(60 * k))) for k in range(6)]
+                ring_h = [centre + 2.480 * _unit(r - centre) for r in ring[1:]]
+                # CH2 hydrogens: the two sites of a tetrahedral carbon between q_prev and q_ch
+                v1, v2 = _unit(q_prev - q_ch2), _unit(q_ch - q_ch2)
+                b2, n2 = _unit(-(v1 + v2)), _unit(np.cross(v1, v2))
+                h2a = q_ch2 + 1.090 * _unit(b2 * math.cos(ang) + n2 * math.sin(ang))
+                h2b = q_ch2 + 1.090 * _unit(b2 * math.cos(ang) - n2 * math.sin(ang))
+                h1 = q_ch + 1.090 * d_h
+                pts = np.array([q_ch2, q_ch, h2a, h2b, h1] + ring + ring_h)
+                del e3
+                dmin = grid.min_dist(np.mod(pts, L), max(chain_first_atom, len(grid.pos) - 2 * n_unit)) if grow else 1e9
+                if dmin > best_d:
+                    best, best_d = pts, dmin
+                if dmin >= min_sep:
+                    break
+            pts = best
+            bb.extend([pts[0], pts[1]]) if u > 0 else None
+            if u == 0:
+                bb = [bb[0], pts[0], pts[1]]
+            # atom order in the unit: CH2 C, CH C, 2 H on CH2, H on CH, ring C ipso..C6, ring H 2..6
+            order = [0, 1, 2, 3, 4] + list(range(5, 11)) + list(range(11, 16))
+            for k, idx in enumerate(order):
+                x[base + u * n_unit + k] = pts[idx]
+                if grow:
+                    grid.add(np.mod(pts[idx], L), base + u * n_unit + k)
+            o = base + u * n_unit
+            cls[o:o + 16] = ["CT", "CT", "HC", "HC", "HC"] + ["CA"] * 6 + ["HA"] * 5
+            bonds += [(o, o + 1), (o, o + 2), (o, o + 3), (o + 1, o + 4), (o + 1, o + 5)]
+            for k in range(6):
+                bonds.append((o + 5 + k, o + 5 + (k + 1) % 6))
+            for k in range(5):
+                bonds.append((o + 6 + k, o + 11 + k))
+            if u > 0:
+                bonds.append((o - n_unit + 1, o))   # CH of the previous unit to this CH2
+    bonds = np.array(bonds, np.uint32)
+    nb = _graph(n, bonds)
+    types = ["CT", "CA", "HC", "HA"]
+    tidx = np.array([types.index(c) for c in cls], np.int32)
+    eps = np.array([_LJ[t][0] for t in types])
+    sig = np.array([_LJ[t][1] for t in types])
+    q = np.array([_Q.get(c, 0.0) for c in cls])
+    # backbone balanced to neutral per unit: the ipso carbon carries nothing, the 6 aromatic CH pairs are neutral;
+    # the ring's C-H pairs (5) sum to 0, so the backbone stays at 0: CH2 C -0.12, its H +0.06 each; CH C -0.06, H +0.06
+    for u0 in range(0, n, n_unit):
+        q[u0 + 5] = 0.0          # ipso carbon
+        q[u0] = -0.12
+        q[u0 + 2] = q[u0 + 3] = 0.06
+        q[u0 + 1] = -0.06
+        q[u0 + 4] = 0.06
+    mass = np.array([M_C if c in ("CT", "CA") else M_H for c in cls])
+    bk = np.array([_key_sym(_BOND, (cls[i], cls[j])) for i, j in bonds])
+    ang = angles_from_bonds(nb)
+    ak = []
+    for i, j, k in ang:
+        kt, th = _key_sym(_ANGLE, (cls[i], cls[j], cls[k]))
+        ak.append((kt, math.radians(th)))
+    dih = dihedrals_from_bonds(nb, bonds)
+    d_ijkl, d_vd, d_n = [], [], []
+    for i, j, k, l in dih:
+        v = _key_sym(_TORS, (cls[i], cls[j], cls[k], cls[l]))
+        if v is None:
+            continue
+        for nn, (vv, delta) in enumerate(((v[0] / 2, 0.0), (v[1] / 2, math.pi), (v[2] / 2, 0.0)), start=1):
+            if vv != 0.0:
+                d_ijkl.append((i, j, k, l))
+                d_vd.append((vv, delta))
+                d_n.append(nn)
+    # impropers keeping the ring and its substituents planar: v [1 + cos(2 phi - pi)], v = 1.1 (OPLS aromatic)
+    imp_ijkl, imp_vd, imp_n = [], [], []
+    for u0 in range(0, n, n_unit):
+        for k in range(6):
+            c = u0 + 5 + k
+            sub = u0 + 1 if k == 0 else u0 + 11 + (k - 1)
+            a, b = u0 + 5 + (k - 1) % 6, u0 + 5 + (k + 1) % 6
+            imp_ijkl.append((a, b, c, sub))
+            imp_vd.append((1.1, math.pi))
+            imp_n.append(2)
+    off, lst, p14 = exclusions(n, nb)
+    pe = np.sqrt(np.outer(eps, eps))
+    ps = np.sqrt(np.outer(sig, sig))
+    el = np.array([6 if c in ("CT", "CA") else 1 for c in cls], np.int32)
+    ff = ForceField(type_index=tidx, charge=q, mass=mass, pair_eps=pe, pair_sigma=ps, bond_ij=bonds, bond_k_r0=bk,
+                    angle_ijk=ang, angle_kt_theta0=np.array(ak), dihedral_ijkl=np.array(d_ijkl, np.uint32).reshape(-1, 4),
+                    dihedral_v_delta=np.array(d_vd).reshape(-1, 2), dihedral_n=np.array(d_n, np.int32),
+                    improper_ijkl=np.array(imp_ijkl, np.uint32), improper_v_delta=np.array(imp_vd), improper_n=np.array(imp_n, np.int32),
+                    pair14_ij=p14, lj14=0.5, coul14=0.5, excl_offset=off, excl_list=lst, element=el)
+    cell = np.array([0, 0, 0, L, 0, 0, 0, L, 0, 0, 0, L], float)
+    return ff, x, cell
+
+
+def kg_melt(chains: int = 100, beads: int = 50, density: float = 0.85, seed: int = 1, bond: float = 0.97):
+    """Kremer-Grest chains in reduced units mapped as sigma = 1 Å, eps = 1 kcal/mol, m = 1 g/mol: WCA (cut-off
+    2^(1/6), shifted), FENE K = 30, R0 = 1.5 with the WCA core on bonded pairs, 1-2 pairs excluded from the WCA pairs."""
+    rng = np.random.default_rng(seed)
+    n = chains * beads
+    L = (n / density) ** (1.0 / 3.0)
+    x = np.zeros((n, 3))
+    for c in range(chains):
+        p = rng.uniform(0, L, 3)
+        prev = None
+        for k in range(beads):
+            if k:
+                for _ in range(1000):
+                    d = _unit(rng.normal(size=3))
+                    if prev is None or np.dot(d, prev) > -0.5:
+                        break
+                p = p + bond * d
+                prev = d
+            x[c * beads + k] = p
+    bonds = np.array([(c * beads + k, c * beads + k + 1) for c in range(chains) for k in range(beads - 1)], np.uint32)
+    nb = _graph(n, bonds)
+    off, lst, _ = exclusions(n, nb, depth=1)
+    ff = ForceField(type_index=np.zeros(n, np.int32), charge=np.zeros(n), mass=np.ones(n), pair_eps=[[1.0]], pair_sigma=[[1.0]],
+                    fene_ij=bonds, fene_k_r0_eps_sigma=np.tile([30.0, 1.5, 1.0, 1.0], (len(bonds), 1)), excl_offset=off,
+                    excl_list=lst, lj_shift=True, model_cutoff=2 ** (1 / 6), element=np.zeros(n, np.int32))
+    cell = np.array([0, 0, 0, L, 0, 0, 0, L, 0, 0, 0, L], float)
+    return ff, x, cell
+
+
+def spce_water(nmol: int = 100000, density: float = 0.997, seed: int = 1):
+    """Rigid SPC/E water (O-H 1.0 Å, H-O-H 109.47 degrees; O sigma 3.166 Å, eps 0.650 kJ/mol; q_O -0.8476, q_H
+    +0.4238) on a jittered cubic lattice with random orientations."""
+    rng = np.random.default_rng(seed)
+    mass_mol = M_O + 2 * M_H
+    L = (nmol * mass_mol / (density * NA) * 1e24) ** (1.0 / 3.0)
+    m = int(math.ceil(nmol ** (1.0 / 3.0)))
+    a = L / m
+    sites = np.array([(i, j, k) for i in range(m) for j in range(m) for k in range(m)], float)[:nmol]
+    o = (sites + 0.5 + rng.uniform(-0.1, 0.1, sites.shape)) * a
+    theta = math.radians(109.47)
+    x = np.zeros((3 * nmol, 3))
+    for w in range(nmol):
+        e1 = _unit(rng.normal(size=3))
+        e2 = _unit(np.cross(e1, _unit(rng.normal(size=3))))
+        h1 = o[w] + 1.0 * e1
+        h2 = o[w] + 1.0 * (math.cos(theta) * e1 + math.sin(theta) * e2)
+        x[3 * w], x[3 * w + 1], x[3 * w + 2] = o[w], h1, h2
+    n = 3 * nmol
+    tidx = np.tile([0, 1, 1], nmol).astype(np.int32)
+    q = np.tile([-0.8476, 0.4238, 0.4238], nmol)
+    mass = np.tile([M_O, M_H, M_H], nmol)
+    bonds = np.array([(3 * w, 3 * w + b) for w in range(nmol) for b in (1, 2)], np.uint32)
+    ang = np.array([(3 * w + 1, 3 * w, 3 * w + 2) for w in range(nmol)], np.uint32)
+    nb = _graph(n, bonds)
+    off, lst, _ = exclusions(n, nb, depth=2)
+    eps_o = 0.650 / 4.184
+    pe = np.array([[eps_o, 0.0], [0.0, 0.0]])
+    ps = np.array([[3.166, 1.0], [1.0, 1.0]])
+    ff = ForceField(type_index=tidx, charge=q, mass=mass, pair_eps=pe, pair_sigma=ps, bond_ij=bonds,
+                    bond_k_r0=np.tile([450.0, 1.0], (len(bonds), 1)), angle_ijk=ang,
+                    angle_kt_theta0=np.tile([55.0, theta], (len(ang), 1)), excl_offset=off, excl_list=lst,
+                    element=np.tile([8, 1, 1], nmol).astype(np.int32))
+    cell = np.array([0, 0, 0, L, 0, 0, 0, L, 0, 0, 0, L], float)
+    return ff, x, cell

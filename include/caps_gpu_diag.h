@@ -1,0 +1,31 @@
+/* caps_gpu_diag.h — measurement entry points of the B200 engine for the benchmark harness and profiling.
+ * These have no counterpart in the reference (it publishes its timings from std::chrono around the step loop,
+ * core/src/dynamics.cpp:776-778); they sit beside the drop-in boundary of caps_gpu.h and change no result. */
+#ifndef CAPS_GPU_DIAG_H
+#define CAPS_GPU_DIAG_H
+#include <stdint.h>
+#include "caps_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Measurement mode for caps_gpu_run: flush_bytes >= 0 brackets every MD step with a CUDA event pair on the engine's
+ * stream and, when > 0, writes flush_bytes (larger than the 126 MB L2) between steps, outside the events; < 0 turns it
+ * off. caps_gpu_last_steps_per_second then reports K / (sum of the per-step event times). */
+int32_t caps_gpu_diag_set_timing(caps_gpu_engine* e, int64_t flush_bytes);
+/* Device milliseconds per MD step of the last run (the per-step events in measurement mode). */
+double caps_gpu_diag_last_step_ms(const caps_gpu_engine* e);
+/* Kernel launches in one plain MD step of the last run (the kernel nodes of its captured CUDA graph). */
+int32_t caps_gpu_diag_step_kernels(const caps_gpu_engine* e);
+/* Times the non-bonded pair kernel alone: one force evaluation at x (host, 3N) builds the list, then `launches`
+ * launches of the pair kernel (forces only), each bracketed by CUDA events, an L2 flush of flush_bytes before each.
+ * avg_ms: mean launch time; pairs_in: atom pairs inside the cut-off per launch; pairs_listed: atom pairs the kernel
+ * evaluates (list pairs, masked lanes excluded); entries: cluster-pair entries (FP32 path only; 0 on FP64). */
+int32_t caps_gpu_diag_pair_timing(caps_gpu_engine* e, const double* x, const double* cell, int32_t launches, int64_t flush_bytes, double* avg_ms,
+                                  double* pairs_in, double* pairs_listed, double* entries);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CAPS_GPU_DIAG_H */

@@ -12,6 +12,7 @@ from caps_b200 import _abi, build
 
 ROOT = Path(__file__).resolve().parent.parent
 HEADER = ROOT / "include" / "caps_gpu.h"
+HEADERS = sorted((ROOT / "include").glob("*.h"))
 
 
 @pytest.fixture(scope="module")
@@ -21,7 +22,7 @@ def lib():
 
 
 def declared_functions():
-    text = HEADER.read_text()
+    text = "\n".join(h.read_text() for h in HEADERS)
     return sorted(set(re.findall(r"^\s*[A-Za-z_][A-Za-z0-9_ \*]*?\b(caps_gpu_[a-z_]+)\s*\(", text, re.M)))
 
 
@@ -34,7 +35,7 @@ def test_header_declares_the_boundary():
 def test_library_exports_every_declared_symbol(lib):
     for name in declared_functions():
         assert hasattr(lib, name), name
-    assert set(_abi.EXPORTS) <= set(declared_functions())
+    assert set(_abi.EXPORTS) | set(_abi.DIAG_EXPORTS) <= set(declared_functions())
     assert lib.caps_gpu_abi_version() == 1
 
 
