@@ -140,10 +140,21 @@ def main():
     ap.add_argument("--impl", default="caps_b200")
     ap.add_argument("--fp64-steps", type=int, default=None)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--profile-pair", type=int, default=0, metavar="LAUNCHES",
+                    help="only time the pair kernel LAUNCHES times on the start structure (a small case for ncu captures)")
     args = ap.parse_args()
     rank, world, local = int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
     if args.warmup < 3:
         args.warmup = 3
+
+    if args.profile_pair:
+        from caps_b200 import Evaluator
+        ff, x, v, cell = workload()
+        for prec in ("mixed", "double"):
+            ev = Evaluator(ff, options(prec, 1, 1).energy)
+            print(json.dumps({"precision": prec, **ev.pair_timing(x, cell, launches=args.profile_pair)}), flush=True)
+            ev.close()
+        return
 
     if args.impl == "reference":
         if rank == 0:

@@ -515,6 +515,7 @@ void Engine::ensure_list_capacity() {
   d_order_.alloc(size_t(n_));
   d_iperm_.alloc(size_t(n_));
   d_x0_.alloc(size_t(3) * n_);
+  d_xp_.alloc(size_t(3) * n_);
   if (!d_counters_.p) {
     d_counters_.alloc(kCntNum);
     CK(cudaMemsetAsync(d_counters_.p, 0, sizeof(int) * kCntNum, stream_));
@@ -602,7 +603,7 @@ void Engine::launch_build(const double* d_x) {
   CK(cudaGetLastError());
 }
 
-void Engine::pair_forces(bool ener, bool vir) {
+PairArgs Engine::pair_args() {
   PairArgs A{};
   A.work = d_work_.p;
   A.ent = d_ent_.p;
@@ -639,19 +640,45 @@ void Engine::pair_forces(bool ener, bool vir) {
   A.en.dbl = d_edbl_.p;
   A.work_cap = int(d_work_.n);
   A.err = d_counters_.p + kCntErr;
+  return A;
+}
+
+// Dynamic pruning: when an atom has moved b/2 since the last prune (b = min(0.8 Å, skin), as field.cpp:1306-1312), or a
+// build set the flag, every entry's i-cluster mask is rewritten for r_c + b.
+void Engine::prune(const double* d_x) {
+  const double b = std::min(0.8, skin_);
+  const PairArgs A = pair_args();
+  k_check_moved<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_x, d_xp_.p, 0.25 * b * b, d_counters_.p, kCntPrune);
+  const double rp = rc_ + b;
+  if (mixed_) k_prune<false><<<dev_sms_ * 8, 128, 0, stream_>>>(A, rp * rp, d_ent_.p);
+  else k_prune<true><<<dev_sms_ * 8, 128, 0, stream_>>>(A, rp * rp, d_ent_.p);
+  k_end_prune<<<blocks_for(size_t(3) * n_, 256), 256, 0, stream_>>>(n_, d_x, d_xp_.p, d_counters_.p);
+  k_lower_prune<<<1, 1, 0, stream_>>>(d_counters_.p);
+}
+
+void Engine::pair_forces(bool ener, bool vir) {
+  PairArgs A = pair_args();
   const int coul = coul_ ? (pme_ ? 1 : 2) : 0;
   const int grid = dev_sms_ * 8;
   const int ntab = nt_ + 1;
   if (mixed_) {
     const size_t smem = sizeof(float4) * (size_t(ntab) * ntab + 4 * 64) + sizeof(int) * 4 * 64;
+    // the rational fits hold for (kappa r_c)^2 <= 16; past that the library erfc form
+    const int c32 = coul == 0 ? 0 : (kappa_ * kappa_ * rc_ * rc_ <= double(kEwUMax) ? coul : coul + 2);
 #define PAIR32(C, E, V)                                                                                              \
   do {                                                                                                               \
     if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_pair_f32<C, E, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
     k_pair_f32<C, E, V><<<grid, 128, smem, stream_>>>(A);                                                            \
   } while (0)
-    if (coul == 1) { if (ener) { if (vir) PAIR32(1, true, true); else PAIR32(1, true, false); } else { if (vir) PAIR32(1, false, true); else PAIR32(1, false, false); } }
-    else if (coul == 2) { if (ener) { if (vir) PAIR32(2, true, true); else PAIR32(2, true, false); } else { if (vir) PAIR32(2, false, true); else PAIR32(2, false, false); } }
-    else { if (ener) { if (vir) PAIR32(0, true, true); else PAIR32(0, true, false); } else { if (vir) PAIR32(0, false, true); else PAIR32(0, false, false); } }
+#define PAIR32C(C) { if (ener) { if (vir) PAIR32(C, true, true); else PAIR32(C, true, false); } else { if (vir) PAIR32(C, false, true); else PAIR32(C, false, false); } }
+    switch (c32) {
+      case 1: PAIR32C(1) break;
+      case 2: PAIR32C(2) break;
+      case 3: PAIR32C(3) break;
+      case 4: PAIR32C(4) break;
+      default: PAIR32C(0) break;
+    }
+#undef PAIR32C
 #undef PAIR32
   } else {
     const size_t smem = sizeof(double4) * (size_t(ntab) * ntab + 4 * 64) + sizeof(double) * 2 * size_t(coul ? gnodes_ : 0) + sizeof(int) * 4 * 64;
@@ -804,6 +831,7 @@ void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild) 
     else
       k_pack_f64<<<blocks_for(ns, 256), 256, 0, stream_>>>(int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_q_.p, d_type_.p, nt_, d_xqd_.p, d_tslot_.p,
                                                            d_counters_.p);
+    prune(d_x);
     pair_forces(ener, vir);
   }
   bonded_forces(d_x, ener, vir);

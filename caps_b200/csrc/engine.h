@@ -16,6 +16,7 @@
 #include "common.cuh"
 #include "nblist.cuh"
 #include "pme.cuh"
+#include "pair.cuh"
 
 namespace capsb {
 
@@ -123,6 +124,8 @@ class Engine {
   template <class R> void pme_setup(PmePath<R>& P);
   template <class R> void pme_run(PmePath<R>& P, const double* d_x, bool ener, bool vir);
   void pair_forces(bool ener, bool vir);
+  PairArgs pair_args();
+  void prune(const double* d_x);
   void bonded_forces(const double* d_x, bool ener, bool vir);
   void host_constants(caps_gpu_terms* t, bool ener, bool vir) const;
 
@@ -165,7 +168,7 @@ class Engine {
   ListGeom geom_{};
   ListBufs lb_{};
   DevBuf<int> d_col_, d_ioff_, d_order_, d_iperm_, d_col_count_, d_col_fill_, d_col_start_, d_col_sc_, d_sc_col_, d_perm_, d_counters_;
-  DevBuf<double> d_frac_, d_sc_z_, d_sc_org_, d_cl_box_, d_x0_;
+  DevBuf<double> d_frac_, d_sc_z_, d_sc_org_, d_cl_box_, d_x0_, d_xp_;
   DevBuf<unsigned char> d_cl_real_;
   DevBuf<uint4> d_ent_;
   DevBuf<float4> d_ent_shift_;

@@ -52,7 +52,7 @@ struct ListBufs {
   // per slot
   int* perm;
   // list
-  uint4* ent;         // x cj, y imask | image << 8, z mask index + 1, w unused
+  uint4* ent;         // x cj, y imask | image << 8, z mask index + 1, w the pruned imask (the pair kernels read w)
   float4* ent_shift;  // org(sc_j) + S - org(sc_i), for the FP32 kernel
   unsigned long long* masks;   // 8 per masked entry
   int4* work;         // x sc, y first entry, z count
@@ -62,7 +62,7 @@ struct ListBufs {
   int* counters;
 };
 
-enum Counter { kCntEnt = 0, kCntWork, kCntMask, kCntErr, kCntRebuild, kCntNsc, kCntMaxCol, kCntNum = 8 };
+enum Counter { kCntEnt = 0, kCntWork, kCntMask, kCntErr, kCntRebuild, kCntNsc, kCntMaxCol, kCntPrune, kCntNum = 8 };
 
 __device__ __forceinline__ void raise_error(int* counters, unsigned bit) { atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), bit); }
 
@@ -79,7 +79,8 @@ __host__ __device__ __forceinline__ void unpack_image(unsigned p, int& qa, int& 
 // ---------------------------------------------------------------------------------------------------------------
 // K-CHECK: has any atom moved more than half the skin since the last build? (core/src/field.cpp:800-838, the
 // constant-cell branch). Sets counters[kCntRebuild].
-static __global__ void k_check_moved(int n, const double* __restrict__ x, const double* __restrict__ x0, double lim2, int* counters) {
+static __global__ void k_check_moved(int n, const double* __restrict__ x, const double* __restrict__ x0, double lim2, int* counters,
+                                     int flag = kCntRebuild) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   bool moved = false;
   if (i < n) {
@@ -87,7 +88,7 @@ static __global__ void k_check_moved(int n, const double* __restrict__ x, const 
     const double d2 = dx * dx + dy * dy + dz * dz;
     moved = !(d2 <= lim2);   // NaN counts as moved
   }
-  if (__any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) atomicOr(counters + kCntRebuild, 1);
+  if (__any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) atomicOr(counters + flag, 1);
 }
 
 // Gate for the build kernels in a captured step: they all return at once unless the rebuild flag is set.
@@ -99,11 +100,12 @@ static __global__ void k_clear_columns(ListGeom g, ListBufs b) {
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.ncol; c += gridDim.x * blockDim.x) b.col_count[c] = 0;
 }
 
-// Ends a build: keeps the positions the list was built at and lowers the flag.
+// Ends a build: keeps the positions the list was built at; a fresh list is pruned at once.
 static __global__ void k_end_build(int n, const double* __restrict__ x, double* __restrict__ x0, int* counters) {
   if (build_off(counters)) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < 3 * n) x0[i] = x[i];
+  if (i == 0) counters[kCntPrune] = 1;
 }
 static __global__ void k_lower_flag(int* counters) { counters[kCntRebuild] = 0; }
 
@@ -374,6 +376,7 @@ static __device__ void flush_batch(SearchShared& S, int sc, int cnt, int lane, c
   }
   for (int e = lane; e < cnt; e += 32) {
     uint4 en = S.ent[e];
+    en.w = en.y & 255u;   // unpruned until the first prune
     if (S.needs_mask[e]) {
       const int mi = atomicAdd(b.counters + kCntMask, 1);
       if (mi < b.mask_cap) {

@@ -14,6 +14,7 @@
 #pragma once
 #include "common.cuh"
 #include "nblist.cuh"
+#include "ewald_fit.cuh"
 
 namespace capsb {
 
@@ -91,7 +92,8 @@ struct PairArgs {
 };
 
 // --- FP32 path ---------------------------------------------------------------------------------------------------
-// COUL: 0 none, 1 Ewald real space (PME), 2 damped shifted force.
+// COUL: 0 none; 1 Ewald real space (PME) and 2 damped shifted force through the rational fits of ewald_fit.cuh
+// (kappa r_c <= 4); 3 and 4 the same through erfcf and expf (any kappa).
 template <int COUL, bool ENER, bool VIR>
 static __global__ void __launch_bounds__(128, 4) k_pair_f32(PairArgs A) {
   extern __shared__ float4 smem_f4[];
@@ -109,6 +111,7 @@ static __global__ void __launch_bounds__(128, 4) k_pair_f32(PairArgs A) {
   const int nwork = min(A.counters[kCntWork], A.work_cap);
   const int pad = A.ntab - 1;
   const float rc2 = float(A.rc2), beta = float(A.beta), kc = float(A.kc), kcoul = float(A.kcoul);
+  const float ku = float(A.beta * A.beta / kEwUMax), kap3 = float(A.beta * A.beta * A.beta);
   const float e0 = float(A.dsf_e0), f0 = float(A.dsf_f0), rcf = float(A.rc);
   const int nwarps = gridDim.x * 4;
   double acc_v = 0, acc_c = 0, acc_w[6] = {0, 0, 0, 0, 0, 0}, acc_np = 0, acc_nl = 0;
@@ -133,7 +136,8 @@ static __global__ void __launch_bounds__(128, 4) k_pair_f32(PairArgs A) {
       const uint4 en = A.ent[e];
       const float4 sh = A.ent_shift[e];
       const int cj = int(en.x);
-      const unsigned imask = en.y & 255u;
+      const unsigned imask = en.w & 255u;
+      if (!imask) continue;
       const int j0 = 8 * cj + jq, j1 = j0 + 4;
       const float4 a0 = A.xq[j0], a1 = A.xq[j1];
       const int t0 = A.tslot[j0], t1 = A.tslot[j1];
@@ -168,18 +172,31 @@ static __global__ void __launch_bounds__(128, 4) k_pair_f32(PairArgs A) {
           const float a12 = cc.y * r6i;
           float fr = r6i * fmaf(12.f, a12, -6.f * cc.x) * r2i;
           if (ENER) ev += ok ? fmaf(r6i, a12 - cc.x, -cc.z) : 0.f;
-          if (COUL != 0) {
+          if (COUL == 1 || COUL == 2) {
+            // E = qq (1/r - kappa g(u)), F = qq (1/r^3 - kappa^3 h(u)), u = (kappa r)^2: FMAs and one division
+            const float qq = xi.w * qj;
+            const float t = r2s * ku;
+            float fc = qq * fmaf(-kap3, ew_h(t), rinv * r2i);
+            if (COUL == 2) fc -= qq * f0 * rinv;
+            fr += fc;
+            if (ENER) {
+              float ecp = qq * fmaf(-beta, ew_g(t), rinv);
+              if (COUL == 2) ecp += qq * (f0 * (r2s * rinv - rcf) - e0);
+              ec += ok ? ecp : 0.f;
+            }
+          }
+          if (COUL == 3 || COUL == 4) {
             const float qq = xi.w * qj;
             const float r = r2s * rinv;
             const float br = beta * r;
             const float erfcv = erfcf(br);
             const float ex = __expf(-br * br);
             float fc = qq * fmaf(erfcv, rinv, kc * ex) * r2i;
-            if (COUL == 2) fc -= qq * f0 * rinv;
+            if (COUL == 4) fc -= qq * f0 * rinv;
             fr += fc;
             if (ENER) {
               float ecp = qq * erfcv * rinv;
-              if (COUL == 2) ecp += qq * (f0 * (r - rcf) - e0);
+              if (COUL == 4) ecp += qq * (f0 * (r - rcf) - e0);
               ec += ok ? ecp : 0.f;
             }
           }
@@ -310,7 +327,8 @@ static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
     for (int e = wk.y; e < wk.y + wk.z; ++e) {
       const uint4 en = A.ent[e];
       const int cj = int(en.x);
-      const unsigned imask = en.y & 255u;
+      const unsigned imask = en.w & 255u;
+      if (!imask) continue;
       int qa, qb, qc;
       unpack_image(en.y >> 8, qa, qb, qc);
       const double Sx = A.cell.h[0][0] * qa + A.cell.h[0][1] * qb + A.cell.h[0][2] * qc;
@@ -429,5 +447,90 @@ static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
       for (int k = 0; k < 6; ++k) A.en.add(kEW0 + k, acc_w[k], false);
   }
 }
+
+// K-PRUNE (dynamic pruning, as core/src/nbnxm.cpp:328-363 does on the CPU): each entry's i-cluster mask is rewritten
+// to the i clusters with at least one atom pair inside r_prune = r_c + b at the present positions; the pair kernels
+// read that mask. Pruned again once an atom has moved b/2 since the last prune, so no pair inside r_c is lost. Gated by
+// the prune flag, set by the displacement check and by every list build. FP32 path: packed float positions; FP64 path:
+// packed double positions.
+template <bool DBL>
+static __global__ void __launch_bounds__(128) k_prune(PairArgs A, double rprune2, uint4* __restrict__ ent) {
+  if (*(volatile const int*)(A.counters + kCntPrune) == 0) return;
+  if (A.counters[kCntErr] & (kErrListOverflow | kErrMaskOverflow | kErrScOverflow | kErrColumnTooBig | kErrExclOverflow)) return;
+  __shared__ float4 s_xi[4][64];
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i8 = lane & 7, jq = lane >> 3;
+  const int nwork = min(A.counters[kCntWork], A.work_cap);
+  const int pad = A.ntab - 1;
+  const float rp2 = float(rprune2);
+  for (int w = blockIdx.x * 4 + wib; w < nwork; w += gridDim.x * 4) {
+    const int4 wk = A.work[w];
+    const int sc = wk.x;
+    for (int t = lane; t < 64; t += 32) {
+      float4 v;
+      if (DBL) {
+        const double4 d = A.xqd[64 * sc + t];
+        v = make_float4(float(d.x), float(d.y), float(d.z), 0.f);
+      } else {
+        v = A.xq[64 * sc + t];
+      }
+      v.w = A.tslot[64 * sc + t] != pad ? 1.f : 0.f;
+      s_xi[wib][t] = v;
+    }
+    __syncwarp();
+    for (int e = wk.y; e < wk.y + wk.z; ++e) {
+      uint4 en = ent[e];
+      const unsigned built = en.y & 255u;
+      const int j0 = 8 * int(en.x) + jq, j1 = j0 + 4;
+      float xj[2], yj[2], zj[2];
+      bool rj[2];
+      if (DBL) {
+        int qa, qb, qc;
+        unpack_image(en.y >> 8, qa, qb, qc);
+        const double Sx = A.cell.h[0][0] * qa + A.cell.h[0][1] * qb + A.cell.h[0][2] * qc;
+        const double Sy = A.cell.h[1][0] * qa + A.cell.h[1][1] * qb + A.cell.h[1][2] * qc;
+        const double Sz = A.cell.h[2][0] * qa + A.cell.h[2][1] * qb + A.cell.h[2][2] * qc;
+        const double4 b0 = A.xqd[j0], b1 = A.xqd[j1];
+        xj[0] = float(b0.x + Sx), yj[0] = float(b0.y + Sy), zj[0] = float(b0.z + Sz);
+        xj[1] = float(b1.x + Sx), yj[1] = float(b1.y + Sy), zj[1] = float(b1.z + Sz);
+      } else {
+        const float4 sh = A.ent_shift[e];
+        const float4 b0 = A.xq[j0], b1 = A.xq[j1];
+        xj[0] = b0.x + sh.x, yj[0] = b0.y + sh.y, zj[0] = b0.z + sh.z;
+        xj[1] = b1.x + sh.x, yj[1] = b1.y + sh.y, zj[1] = b1.z + sh.z;
+      }
+      rj[0] = A.tslot[j0] != pad;
+      rj[1] = A.tslot[j1] != pad;
+      unsigned keep = 0;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        if (!((built >> c) & 1u)) continue;
+        const float4 xi = s_xi[wib][8 * c + i8];
+        bool in = false;
+#pragma unroll
+        for (int jj = 0; jj < 2; ++jj) {
+          // FP64 path: absolute positions rounded to float (1e-5 Å at 100 Å), far inside the 0.8 Å prune margin
+          const float dx = xj[jj] - xi.x, dy = yj[jj] - xi.y, dz = zj[jj] - xi.z;
+          const float r2 = dx * dx + dy * dy + dz * dz;
+          in |= xi.w != 0.f && rj[jj] && r2 < rp2;
+        }
+        if (__any_sync(0xffffffffu, in)) keep |= 1u << c;
+      }
+      if (lane == 0) {
+        en.w = keep;
+        ent[e] = en;
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// Ends a prune: keeps the positions it was done at and lowers the prune flag (one thread block per 256 coordinates).
+static __global__ void k_end_prune(int n, const double* __restrict__ x, double* __restrict__ xp, int* counters) {
+  if (*(volatile const int*)(counters + kCntPrune) == 0) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < 3 * n) xp[i] = x[i];
+}
+static __global__ void k_lower_prune(int* counters) { counters[kCntPrune] = 0; }
 
 }  // namespace capsb
