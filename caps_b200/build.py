@@ -8,15 +8,17 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
 CSRC = HERE / "csrc"
 LIB = HERE / "libcaps_b200.so"
+OBJ = HERE / "_build"
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
-    "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr",
+    "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
 ]
 
 
@@ -38,12 +40,22 @@ def up_to_date() -> bool:
 
 
 def build(force: bool = False, verbose: bool = True) -> Path:
+    """Compiles each translation unit in parallel into caps_b200/_build/, then links the shared library."""
     if not force and up_to_date():
         return LIB
-    cmd = [_nvcc(), *NVCC_FLAGS, "-I", str(ROOT / "include"), *map(str, sources()), "-o", str(LIB) + ".tmp", "-lcudart"]
+    OBJ.mkdir(exist_ok=True)
+    objs = [OBJ / (src.stem + ".o") for src in sources()]
+    cmds = [[_nvcc(), *NVCC_FLAGS, "-c", "-I", str(ROOT / "include"), str(src), "-o", str(obj)] for src, obj in zip(sources(), objs)]
     if verbose:
-        print("[caps_b200] " + " ".join(cmd), file=sys.stderr)
-    subprocess.run(cmd, check=True)
+        print("[caps_b200] " + " ".join(cmds[0][:-4]) + " -c <each csrc/*.cu>", file=sys.stderr)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as pool:
+        results = list(pool.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds))
+    for c, r in zip(cmds, results):
+        if r.stderr and verbose:
+            print(r.stderr, file=sys.stderr, end="")
+        if r.returncode != 0:
+            raise subprocess.CalledProcessError(r.returncode, c, r.stdout, r.stderr)
+    subprocess.run([_nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *map(str, objs), "-o", str(LIB) + ".tmp", "-lcudart"], check=True)
     os.replace(str(LIB) + ".tmp", LIB)
     return LIB
 

@@ -13,17 +13,10 @@
 #include <string>
 #include <vector>
 
-#include "bonded.cuh"
-#include "pair.cuh"
 
 namespace capsb {
 
 // ---------------------------------------------------------------------------------------------------------------
-#define CK(call)                                                                                         \
-  do {                                                                                                   \
-    cudaError_t e_ = (call);                                                                             \
-    if (e_ != cudaSuccess) throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_));          \
-  } while (0)
 
 namespace {
 
@@ -91,36 +84,6 @@ void bspline_moduli(int k, int p, std::vector<double>& bsp) {
     if (bsp[size_t(m)] < 1e-7) bsp[size_t(m)] = 0.5 * (bsp[size_t(((m - 1) % k + k) % k)] + bsp[size_t((m + 1) % k)]);
 }
 
-__global__ void k_set_flag(int* counters, int slot, int v) { counters[slot] = v; }
-
-// Forces to the caller's AoS doubles: atom-order sums plus the pair kernel's slot-order sums.
-__global__ void k_reduce_f32(int n, const long long* __restrict__ F, const long long* __restrict__ Fs, int nslots, const int* __restrict__ iperm,
-                             double* __restrict__ f, int with_pairs) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const int s = with_pairs ? iperm[i] : -1;
-  const bool ok = s >= 0 && s < nslots;   // a build that overflowed can leave iperm stale: the host reports it
-  for (int k = 0; k < 3; ++k) {
-    long long v = F[size_t(k) * n + i];
-    if (ok) v += Fs[size_t(k) * nslots + s];
-    f[3 * i + k] = double(v) * kInvFixF;
-  }
-}
-__global__ void k_reduce_f64(int n, const double* __restrict__ F, const double* __restrict__ Fs, int nslots, const int* __restrict__ iperm,
-                             double* __restrict__ f, int with_pairs) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const int s = with_pairs ? iperm[i] : -1;
-  const bool ok = s >= 0 && s < nslots;
-  for (int k = 0; k < 3; ++k) {
-    double v = F[size_t(k) * n + i];
-    if (ok) v += Fs[size_t(k) * nslots + s];
-    f[3 * i + k] = v;
-  }
-}
-
-int blocks_for(size_t n, int threads) { return int(std::max<size_t>(1, (n + size_t(threads) - 1) / size_t(threads))); }
-
 void cell_matrices(const double* c, DevCell& d) {
   for (int k = 0; k < 3; ++k) d.o[k] = c[k];
   for (int r = 0; r < 3; ++r)
@@ -149,16 +112,6 @@ void cross3(const double* a, const double* b, double* o) {
 }
 
 // radices of n for the line FFT: 4s first, then 2, 3, 5, 7 and any other prime
-void factor_radices(int n, int* rad, int& nst) {
-  nst = 0;
-  int r = n;
-  while (r % 4 == 0 && nst < kMaxRadices) rad[nst++] = 4, r /= 4;
-  for (int p : {2, 3, 5, 7}) while (r % p == 0 && nst < kMaxRadices) rad[nst++] = p, r /= p;
-  for (int p = 11; r > 1 && p <= kMaxRadices && nst < kMaxRadices; p += 2)
-    while (r % p == 0 && nst < kMaxRadices) rad[nst++] = p, r /= p;
-  if (r != 1) throw ModelError(CAPS_GPU_EINVAL, "PME grid length " + std::to_string(n) + " cannot be factored for the line FFT");
-}
-
 }  // namespace
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -551,296 +504,6 @@ void Engine::ensure_list_capacity() {
   b.mask_cap = int(d_masks_.n / 8);
   b.work_cap = int(d_work_.n);
   b.counters = d_counters_.p;
-}
-
-template <class R>
-void Engine::pme_setup(PmePath<R>& P) {
-  using T = typename Cpx<R>::T;
-  const size_t half = size_t(ph1_) * pk_[1] * pk_[2];
-  P.h.alloc(half);
-  P.gr.alloc(size_t(pk_[0]) * pk_[1] * pk_[2]);
-  P.gt.alloc(half);
-  P.wt.alloc(6 * half);
-  if (mixed_) d_gridq_.alloc(size_t(pk_[0]) * pk_[1] * pk_[2]);
-  d_grid_.alloc(size_t(pk_[0]) * pk_[1] * pk_[2]);
-  for (int d = 0; d < 3; ++d)
-    for (int dir = 0; dir < 2; ++dir) {
-      const int nn = pk_[d];
-      const int sign = dir == 0 ? -1 : +1;   // forward e^{-i}, inverse e^{+i}: the convolution is the same either way
-      std::vector<T> tw(static_cast<size_t>(nn));
-      for (int k = 0; k < nn; ++k) {
-        const double ang = 2 * kPi * k / nn;
-        tw[size_t(k)] = T{R(std::cos(ang)), R(sign * std::sin(ang))};
-      }
-      P.tw[d][dir].upload(tw, stream_);
-      FftPlan<R>& pl = P.plan[d][dir];
-      pl.n = nn;
-      factor_radices(nn, pl.rad, pl.nst);
-      pl.tw = P.tw[d][dir].p;
-      pl.sign = sign;
-    }
-  // lines per block: two complex buffers within 48 KB of shared memory
-  const int cap = int(48 * 1024 / (2 * sizeof(T)));
-  lines_x_ = std::max(1, std::min(64, cap / pk_[0]));
-  lines_y_ = std::max(1, std::min({64, cap / pk_[1], ph1_}));
-  lines_z_ = std::max(1, std::min({64, cap / pk_[2], ph1_}));
-  green_valid_ = false;
-  CK(cudaStreamSynchronize(stream_));
-}
-
-// ---------------------------------------------------------------------------------------------------------------
-void Engine::launch_build(const double* d_x) {
-  const ListGeom& g = geom_;
-  k_clear_columns<<<blocks_for(size_t(g.ncol), 256), 256, 0, stream_>>>(g, lb_);
-  k_bin<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_x, dcell_, g, lb_);
-  k_scan_columns<<<1, 1024, 0, stream_>>>(g, lb_);
-  k_scatter<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, lb_);
-  const size_t sort_smem = size_t(kSortMax) * (sizeof(double) + sizeof(int));
-  k_sort_columns<<<std::min(g.ncol, dev_sms_ * 8), 256, sort_smem, stream_>>>(g, lb_);
-  k_superclusters<<<std::max(1, std::min(blocks_for(size_t(nsc_cap_), 4), dev_sms_ * 16)), 128, 0, stream_>>>(dcell_, lb_);
-  k_search<<<std::max(1, std::min(nsc_cap_, dev_sms_ * 16)), 32, sizeof(SearchShared), stream_>>>(dcell_, g, d_excl_off_.p, d_excl_list_.p, lb_);
-  k_end_build<<<blocks_for(size_t(3) * n_, 256), 256, 0, stream_>>>(n_, d_x, d_x0_.p, lb_.counters);
-  CK(cudaGetLastError());
-}
-
-PairArgs Engine::pair_args() {
-  PairArgs A{};
-  A.work = d_work_.p;
-  A.ent = d_ent_.p;
-  A.ent_shift = d_ent_shift_.p;
-  A.masks = d_masks_.p;
-  A.counters = d_counters_.p;
-  A.tslot = d_tslot_.p;
-  A.xq = d_xq_.p;
-  A.xqd = d_xqd_.p;
-  A.tab = d_tab_.p;
-  A.tabd = d_tabd_.p;
-  A.tabcap = d_tabcap_.p;
-  A.gtab = d_gtab_.p;
-  A.ntab = nt_ + 1;
-  A.gnodes = gnodes_;
-  A.ghi = ghi_;
-  A.cell = dcell_;
-  A.rc2 = rc_ * rc_;
-  A.rc = rc_;
-  A.beta = kappa_;
-  A.kc = 2 * kappa_ / std::sqrt(kPi);
-  A.kcoul = kCoulomb;
-  A.dsf_e0 = dsf_e0_;
-  A.dsf_f0 = dsf_f0_;
-  A.fsx = d_Fs_.p;
-  A.fsy = d_Fs_.p + d_Fs_.n / 3;
-  A.fsz = d_Fs_.p + 2 * (d_Fs_.n / 3);
-  if (!mixed_) {
-    A.fdx = d_Fsd_.p;
-    A.fdy = d_Fsd_.p + d_Fsd_.n / 3;
-    A.fdz = d_Fsd_.p + 2 * (d_Fsd_.n / 3);
-  }
-  A.en.fix = d_efix_.p;
-  A.en.dbl = d_edbl_.p;
-  A.work_cap = int(d_work_.n);
-  A.err = d_counters_.p + kCntErr;
-  return A;
-}
-
-// Dynamic pruning: when an atom has moved b/2 since the last prune (b = min(0.8 Å, skin), as field.cpp:1306-1312), or a
-// build set the flag, every entry's i-cluster mask is rewritten for r_c + b.
-void Engine::prune(const double* d_x) {
-  const double b = std::min(0.8, skin_);
-  const PairArgs A = pair_args();
-  k_check_moved<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_x, d_xp_.p, 0.25 * b * b, d_counters_.p, kCntPrune);
-  const double rp = rc_ + b;
-  if (mixed_) k_prune<false><<<dev_sms_ * 8, 128, 0, stream_>>>(A, rp * rp, d_ent_.p);
-  else k_prune<true><<<dev_sms_ * 8, 128, 0, stream_>>>(A, rp * rp, d_ent_.p);
-  k_end_prune<<<blocks_for(size_t(3) * n_, 256), 256, 0, stream_>>>(n_, d_x, d_xp_.p, d_counters_.p);
-  k_lower_prune<<<1, 1, 0, stream_>>>(d_counters_.p);
-}
-
-void Engine::pair_forces(bool ener, bool vir) {
-  PairArgs A = pair_args();
-  const int coul = coul_ ? (pme_ ? 1 : 2) : 0;
-  const int grid = dev_sms_ * 8;
-  const int ntab = nt_ + 1;
-  if (mixed_) {
-    const size_t smem = sizeof(float4) * (size_t(ntab) * ntab + 4 * 64) + sizeof(int) * 4 * 64;
-    // the rational fits hold for (kappa r_c)^2 <= 16; past that the library erfc form
-    const int c32 = coul == 0 ? 0 : (kappa_ * kappa_ * rc_ * rc_ <= double(kEwUMax) ? coul : coul + 2);
-#define PAIR32(C, E, V)                                                                                              \
-  do {                                                                                                               \
-    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_pair_f32<C, E, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
-    k_pair_f32<C, E, V><<<grid, 128, smem, stream_>>>(A);                                                            \
-  } while (0)
-#define PAIR32C(C) { if (ener) { if (vir) PAIR32(C, true, true); else PAIR32(C, true, false); } else { if (vir) PAIR32(C, false, true); else PAIR32(C, false, false); } }
-    switch (c32) {
-      case 1: PAIR32C(1) break;
-      case 2: PAIR32C(2) break;
-      case 3: PAIR32C(3) break;
-      case 4: PAIR32C(4) break;
-      default: PAIR32C(0) break;
-    }
-#undef PAIR32C
-#undef PAIR32
-  } else {
-    const size_t smem = sizeof(double4) * (size_t(ntab) * ntab + 4 * 64) + sizeof(double) * 2 * size_t(coul ? gnodes_ : 0) + sizeof(int) * 4 * 64;
-#define PAIR64(C, ...)                                                                                               \
-  do {                                                                                                               \
-    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_pair_f64<C, __VA_ARGS__>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
-    k_pair_f64<C, __VA_ARGS__><<<grid, 128, smem, stream_>>>(A);                                                     \
-  } while (0)
-    if (opt_.force_cap > 0) {
-      // push-off: energies and virial always on (a rare path, kept to one instantiation per Coulomb form)
-      if (coul == 1) PAIR64(1, true, true, true);
-      else if (coul == 2) PAIR64(2, true, true, true);
-      else PAIR64(0, true, true, true);
-    } else if (coul == 1) { if (ener) { if (vir) PAIR64(1, true, true); else PAIR64(1, true, false); } else { if (vir) PAIR64(1, false, true); else PAIR64(1, false, false); } }
-    else if (coul == 2) { if (ener) { if (vir) PAIR64(2, true, true); else PAIR64(2, true, false); } else { if (vir) PAIR64(2, false, true); else PAIR64(2, false, false); } }
-    else { if (ener) { if (vir) PAIR64(0, true, true); else PAIR64(0, true, false); } else { if (vir) PAIR64(0, false, true); else PAIR64(0, false, false); } }
-#undef PAIR64
-  }
-  CK(cudaGetLastError());
-}
-
-void Engine::bonded_forces(const double* d_x, bool ener, bool vir) {
-  BondedArgs A{d_x, dcell_, EnergySink{d_efix_.p, d_edbl_.p}, mixed_ ? 1 : 0};
-  const int T = 256;
-  const bool bonded = (opt_.parts & 1) != 0, nonb = (opt_.parts & 2) != 0;
-  auto nblk = [&](int cnt) { return std::min(blocks_for(size_t(std::max(cnt, 1)), T), dev_sms_ * 4); };
-#define LAUNCH3(K, S, cnt, ...)                                                                                     \
-  do {                                                                                                              \
-    if (ener) { if (vir) K<double, S, true, true><<<nblk(cnt), T, 0, stream_>>>(__VA_ARGS__); else K<double, S, true, false><<<nblk(cnt), T, 0, stream_>>>(__VA_ARGS__); } \
-    else { if (vir) K<double, S, false, true><<<nblk(cnt), T, 0, stream_>>>(__VA_ARGS__); else K<double, S, false, false><<<nblk(cnt), T, 0, stream_>>>(__VA_ARGS__); } \
-  } while (0)
-#define LAUNCHX(S, ...)                                                                                             \
-  do {                                                                                                              \
-    if (ener) { if (vir) k_excl_f64<S, true, true><<<nblk(nx_), T, 0, stream_>>>(__VA_ARGS__); else k_excl_f64<S, true, false><<<nblk(nx_), T, 0, stream_>>>(__VA_ARGS__); } \
-    else { if (vir) k_excl_f64<S, false, true><<<nblk(nx_), T, 0, stream_>>>(__VA_ARGS__); else k_excl_f64<S, false, false><<<nblk(nx_), T, 0, stream_>>>(__VA_ARGS__); } \
-  } while (0)
-  auto run = [&](auto sink) {
-    using S = decltype(sink);
-    const S F = sink;
-    if (bonded) {
-      if (nb_) LAUNCH3(k_bonds, S, nb_, nb_, d_bond_ij_.p, d_bond_kr_.p, A, F);
-      if (na_) LAUNCH3(k_angles, S, na_, na_, d_angle_ijk_.p, d_angle_kt_.p, A, F);
-      if (ndg_) LAUNCH3(k_torsions, S, ndg_, ndg_, d_dih_grp_.p, d_dih_ijkl_.p, d_dih_vd_.p, d_dih_n_.p, A, F, int(kEDihedral));
-      if (nig_) LAUNCH3(k_torsions, S, nig_, nig_, d_imp_grp_.p, d_imp_ijkl_.p, d_imp_vd_.p, d_imp_n_.p, A, F, int(kEImproper));
-      if (nfene_) LAUNCH3(k_fene, S, nfene_, nfene_, d_fene_ij_.p, d_fene_p_.p, A, F, d_counters_.p);
-    }
-    if (nonb && np14_)
-      LAUNCH3(k_pairs14, S, np14_, np14_, d_p14_ij_.p, p14_scaled_ ? d_p14_scale_.p : nullptr, lj14_, d_type_.p, nt_, d_lj14_.p,
-              opt_.force_cap > 0 ? (const double4*)d_cap14_.p : (const double4*)nullptr, A, F);
-    if (nonb && coul_ && nx_) {
-      ExclArgs E{d_excl_ij_.p, d_excl_f_.p, d_q_.p, d_gtab_.p, ghi_, rc_, rc_ * rc_, kappa_, dsf_e0_, dsf_f0_, pme_ ? 1 : 0};
-      LAUNCHX(S, nx_, E, A, F);
-    }
-  };
-  if (mixed_) run(ForceSink<float>{d_F_.p, d_F_.p + n_, d_F_.p + 2 * size_t(n_), d_counters_.p + kCntErr});
-  else run(ForceSink<double>{d_Fd_.p, d_Fd_.p + n_, d_Fd_.p + 2 * size_t(n_)});
-#undef LAUNCH3
-#undef LAUNCHX
-  CK(cudaGetLastError());
-}
-
-template <class R>
-void Engine::pme_run(PmePath<R>& P, const double* d_x, bool ener, bool vir) {
-  using T = typename Cpx<R>::T;
-  PmeArgs A{pk_[0], pk_[1], pk_[2], ph1_, dcell_, d_x, d_q_.p, n_};
-  if (!green_valid_ || std::memcmp(green_cell_, cell_h_, sizeof cell_h_) != 0) {
-    const size_t half = size_t(ph1_) * pk_[1] * pk_[2];
-    k_pme_green<R><<<blocks_for(half, 256), 256, 0, stream_>>>(A, d_bsp_[0].p, d_bsp_[1].p, d_bsp_[2].p, beta_, kCoulomb, P.gt.p, P.wt.p);
-    std::memcpy(green_cell_, cell_h_, sizeof cell_h_);
-    green_valid_ = true;
-  }
-  const int nb = blocks_for(size_t(n_), 128);
-  if (mixed_) CK(cudaMemsetAsync(d_gridq_.p, 0, d_gridq_.n * sizeof(long long), stream_));
-  else CK(cudaMemsetAsync(d_grid_.p, 0, d_grid_.n * sizeof(double), stream_));
-#define SPREAD(P_)                                                                            \
-  do {                                                                                        \
-    if (mixed_) k_spread<float, P_><<<nb, 128, 0, stream_>>>(A, d_grid_.p, d_gridq_.p);      \
-    else k_spread<double, P_><<<nb, 128, 0, stream_>>>(A, d_grid_.p, d_gridq_.p);            \
-  } while (0)
-  switch (order_) {
-    case 3: SPREAD(3); break;
-    case 4: SPREAD(4); break;
-    case 5: SPREAD(5); break;
-    case 6: SPREAD(6); break;
-    case 7: SPREAD(7); break;
-    default: SPREAD(8); break;
-  }
-#undef SPREAD
-  const size_t sx = size_t(lines_x_) * pk_[0] * 2 * sizeof(T), sy = size_t(lines_y_) * pk_[1] * 2 * sizeof(T), sz = size_t(lines_z_) * pk_[2] * 2 * sizeof(T);
-  const int nlx = pk_[1] * pk_[2];
-  k_fft_x_fwd<R><<<blocks_for(size_t(nlx), lines_x_), 256, sx, stream_>>>(A, mixed_ ? nullptr : d_grid_.p, mixed_ ? d_gridq_.p : nullptr, P.h.p,
-                                                                        P.plan[0][0], lines_x_);
-  const int gy = ((ph1_ + lines_y_ - 1) / lines_y_) * pk_[2];
-  k_fft_y<R><<<gy, 256, sy, stream_>>>(A, P.h.p, P.plan[1][0], lines_y_);
-  const int gz = ((ph1_ + lines_z_ - 1) / lines_z_) * pk_[1];
-  EnergySink en{d_efix_.p, d_edbl_.p};
-  if (ener) { if (vir) k_fft_z_solve<R, true, true><<<gz, 256, sz, stream_>>>(A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); else k_fft_z_solve<R, true, false><<<gz, 256, sz, stream_>>>(A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); }
-  else { if (vir) k_fft_z_solve<R, false, true><<<gz, 256, sz, stream_>>>(A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); else k_fft_z_solve<R, false, false><<<gz, 256, sz, stream_>>>(A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); }
-  k_fft_y<R><<<gy, 256, sy, stream_>>>(A, P.h.p, P.plan[1][1], lines_y_);
-  k_fft_x_inv<R><<<blocks_for(size_t(nlx), lines_x_), 256, sx, stream_>>>(A, P.h.p, P.gr.p, P.plan[0][1], lines_x_);
-  const ForceSink<float> Ff{d_F_.p, d_F_.p + n_, d_F_.p + 2 * size_t(n_), d_counters_.p + kCntErr};
-  const ForceSink<double> Fd{d_Fd_.p, d_Fd_.p + n_, d_Fd_.p + 2 * size_t(n_)};
-#define GATHER(P_)                                                                            \
-  do {                                                                                        \
-    if (mixed_) k_gather<float, R, P_><<<nb, 128, 0, stream_>>>(A, P.gr.p, Ff);              \
-    else k_gather<double, R, P_><<<nb, 128, 0, stream_>>>(A, P.gr.p, Fd);                     \
-  } while (0)
-  switch (order_) {
-    case 3: GATHER(3); break;
-    case 4: GATHER(4); break;
-    case 5: GATHER(5); break;
-    case 6: GATHER(6); break;
-    case 7: GATHER(7); break;
-    default: GATHER(8); break;
-  }
-#undef GATHER
-  CK(cudaGetLastError());
-}
-
-void Engine::pme_forces(const double* d_x, bool ener, bool vir) { pme_run(pd_, d_x, ener, vir); }
-
-// One force evaluation on device positions d_x (AoS, 3 n): accumulators cleared, list checked / rebuilt, every term,
-// forces reduced into d_f_ (AoS doubles). Asynchronous on stream_.
-void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild) {
-  const bool nonb = (opt_.parts & 2) != 0;
-  if (nonb) {
-    if (!list_valid_) {
-      k_set_flag<<<1, 1, 0, stream_>>>(d_counters_.p, kCntRebuild, 1);
-      list_valid_ = true;
-      ++builds_;
-    } else if (check_rebuild) {
-      k_check_moved<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_x, d_x0_.p, 0.25 * skin_ * skin_, d_counters_.p);
-    }
-    launch_build(d_x);
-  }
-  if (mixed_) {
-    CK(cudaMemsetAsync(d_F_.p, 0, d_F_.n * sizeof(long long), stream_));
-    if (nonb) CK(cudaMemsetAsync(d_Fs_.p, 0, d_Fs_.n * sizeof(long long), stream_));
-  } else {
-    CK(cudaMemsetAsync(d_Fd_.p, 0, d_Fd_.n * sizeof(double), stream_));
-    if (nonb) CK(cudaMemsetAsync(d_Fsd_.p, 0, d_Fsd_.n * sizeof(double), stream_));
-  }
-  CK(cudaMemsetAsync(d_efix_.p, 0, d_efix_.n * sizeof(long long), stream_));
-  CK(cudaMemsetAsync(d_edbl_.p, 0, d_edbl_.n * sizeof(double), stream_));
-  if (nonb) {
-    const size_t ns = size_t(nsc_cap_) * kScAtoms;
-    if (mixed_)
-      k_pack_f32<<<blocks_for(ns, 256), 256, 0, stream_>>>(int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_sc_org_.p, d_q_.p, d_type_.p, nt_,
-                                                           d_xq_.p, d_tslot_.p, d_counters_.p);
-    else
-      k_pack_f64<<<blocks_for(ns, 256), 256, 0, stream_>>>(int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_q_.p, d_type_.p, nt_, d_xqd_.p, d_tslot_.p,
-                                                           d_counters_.p);
-    prune(d_x);
-    pair_forces(ener, vir);
-  }
-  bonded_forces(d_x, ener, vir);
-  if (nonb && pme_) pme_forces(d_x, ener, vir);
-  const size_t ns = size_t(nsc_cap_) * kScAtoms;
-  if (mixed_) k_reduce_f32<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_F_.p, d_Fs_.p, int(ns), d_iperm_.p, d_f_.p, nonb ? 1 : 0);
-  else k_reduce_f64<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_Fd_.p, d_Fsd_.p, int(ns), d_iperm_.p, d_f_.p, nonb ? 1 : 0);
-  if (nonb) k_lower_flag<<<1, 1, 0, stream_>>>(d_counters_.p);
-  CK(cudaGetLastError());
 }
 
 void Engine::check_errors() {

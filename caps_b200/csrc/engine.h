@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <array>
 #include <cstdint>
 #include <functional>
@@ -14,11 +15,14 @@
 
 #include "caps_gpu.h"
 #include "common.cuh"
-#include "nblist.cuh"
-#include "pme.cuh"
-#include "pair.cuh"
+#include "list_types.cuh"
+#include "pme_types.cuh"
 
 namespace capsb {
+
+struct PairArgs;
+
+inline int blocks_for(size_t n, int threads) { return int(std::max<size_t>(1, (n + size_t(threads) - 1) / size_t(threads))); }
 
 template <class T>
 struct DevBuf {
@@ -42,6 +46,13 @@ struct DevBuf {
 struct CudaError : std::runtime_error {
   using std::runtime_error::runtime_error;
 };
+
+// Every CUDA runtime call of the host engine goes through CK: a failure becomes a CudaError with the call's text.
+#define CK(call)                                                                                         \
+  do {                                                                                                   \
+    cudaError_t e_ = (call);                                                                             \
+    if (e_ != cudaSuccess) throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_));          \
+  } while (0)
 
 template <class T>
 void DevBuf<T>::alloc(size_t count) {

@@ -24,11 +24,6 @@
 
 namespace capsb {
 
-#define CK(call)                                                                                         \
-  do {                                                                                                   \
-    cudaError_t e_ = (call);                                                                             \
-    if (e_ != cudaSuccess) throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_));          \
-  } while (0)
 
 namespace {
 
@@ -363,14 +358,8 @@ __global__ void k_langevin_o(int n, double* __restrict__ v, const double* __rest
 
 // bath -= KE(after) - KE(before)
 __global__ void k_bath_update(double* sc) { sc[kScBath] -= sc[kScKE] - sc[kScKE0]; }
-__global__ void k_copy_slot(double* sc, int dst, int src) { sc[dst] = sc[src]; }
 __global__ void k_zero_cw(double* sc) {
   for (int q = 0; q < 6; ++q) sc[kScCW0 + q] = 0;
-}
-__global__ void k_remove_com(int n, double* __restrict__ v, const double* __restrict__ p) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  for (int r = 0; r < 3; ++r) v[3 * i + r] -= p[r];
 }
 
 }  // namespace

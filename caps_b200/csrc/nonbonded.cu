@@ -1,0 +1,201 @@
+// Host side of the non-bonded forces: the list build sequence, dynamic pruning, the pair-kernel launch, and the
+// per-evaluation orchestration of every force term into the caller's AoS doubles.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <vector>
+
+#include "engine.h"
+#include "pair.cuh"
+
+namespace capsb {
+
+namespace {
+
+__global__ void k_set_flag(int* counters, int slot, int v) { counters[slot] = v; }
+
+// Forces to the caller's AoS doubles: atom-order sums plus the pair kernel's slot-order sums.
+__global__ void k_reduce_f32(int n, const long long* __restrict__ F, const long long* __restrict__ Fs, int nslots, const int* __restrict__ iperm,
+                             double* __restrict__ f, int with_pairs) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int s = with_pairs ? iperm[i] : -1;
+  const bool ok = s >= 0 && s < nslots;   // a build that overflowed can leave iperm stale: the host reports it
+  for (int k = 0; k < 3; ++k) {
+    long long v = F[size_t(k) * n + i];
+    if (ok) v += Fs[size_t(k) * nslots + s];
+    f[3 * i + k] = double(v) * kInvFixF;
+  }
+}
+__global__ void k_reduce_f64(int n, const double* __restrict__ F, const double* __restrict__ Fs, int nslots, const int* __restrict__ iperm,
+                             double* __restrict__ f, int with_pairs) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int s = with_pairs ? iperm[i] : -1;
+  const bool ok = s >= 0 && s < nslots;
+  for (int k = 0; k < 3; ++k) {
+    double v = F[size_t(k) * n + i];
+    if (ok) v += Fs[size_t(k) * nslots + s];
+    f[3 * i + k] = v;
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------------------------
+void Engine::launch_build(const double* d_x) {
+  const ListGeom& g = geom_;
+  k_clear_columns<<<blocks_for(size_t(g.ncol), 256), 256, 0, stream_>>>(g, lb_);
+  k_bin<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_x, dcell_, g, lb_);
+  k_scan_columns<<<1, 1024, 0, stream_>>>(g, lb_);
+  k_scatter<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, lb_);
+  const size_t sort_smem = size_t(kSortMax) * (sizeof(double) + sizeof(int));
+  k_sort_columns<<<std::min(g.ncol, dev_sms_ * 8), 256, sort_smem, stream_>>>(g, lb_);
+  k_superclusters<<<std::max(1, std::min(blocks_for(size_t(nsc_cap_), 4), dev_sms_ * 16)), 128, 0, stream_>>>(dcell_, lb_);
+  k_search<<<std::max(1, std::min(nsc_cap_, dev_sms_ * 16)), 32, sizeof(SearchShared), stream_>>>(dcell_, g, d_excl_off_.p, d_excl_list_.p, lb_);
+  k_end_build<<<blocks_for(size_t(3) * n_, 256), 256, 0, stream_>>>(n_, d_x, d_x0_.p, lb_.counters);
+  CK(cudaGetLastError());
+}
+
+PairArgs Engine::pair_args() {
+  PairArgs A{};
+  A.work = d_work_.p;
+  A.ent = d_ent_.p;
+  A.ent_shift = d_ent_shift_.p;
+  A.masks = d_masks_.p;
+  A.counters = d_counters_.p;
+  A.tslot = d_tslot_.p;
+  A.xq = d_xq_.p;
+  A.xqd = d_xqd_.p;
+  A.tab = d_tab_.p;
+  A.tabd = d_tabd_.p;
+  A.tabcap = d_tabcap_.p;
+  A.gtab = d_gtab_.p;
+  A.ntab = nt_ + 1;
+  A.gnodes = gnodes_;
+  A.ghi = ghi_;
+  A.cell = dcell_;
+  A.rc2 = rc_ * rc_;
+  A.rc = rc_;
+  A.beta = kappa_;
+  A.kc = 2 * kappa_ / std::sqrt(kPi);
+  A.kcoul = kCoulomb;
+  A.dsf_e0 = dsf_e0_;
+  A.dsf_f0 = dsf_f0_;
+  A.fsx = d_Fs_.p;
+  A.fsy = d_Fs_.p + d_Fs_.n / 3;
+  A.fsz = d_Fs_.p + 2 * (d_Fs_.n / 3);
+  if (!mixed_) {
+    A.fdx = d_Fsd_.p;
+    A.fdy = d_Fsd_.p + d_Fsd_.n / 3;
+    A.fdz = d_Fsd_.p + 2 * (d_Fsd_.n / 3);
+  }
+  A.en.fix = d_efix_.p;
+  A.en.dbl = d_edbl_.p;
+  A.work_cap = int(d_work_.n);
+  A.err = d_counters_.p + kCntErr;
+  return A;
+}
+
+// Dynamic pruning: when an atom has moved b/2 since the last prune (b = min(0.8 Å, skin), as field.cpp:1306-1312), or a
+// build set the flag, every entry's i-cluster mask is rewritten for r_c + b.
+void Engine::prune(const double* d_x) {
+  const double b = std::min(0.8, skin_);
+  const PairArgs A = pair_args();
+  k_check_moved<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_x, d_xp_.p, 0.25 * b * b, d_counters_.p, kCntPrune);
+  const double rp = rc_ + b;
+  if (mixed_) k_prune<false><<<dev_sms_ * 8, 128, 0, stream_>>>(A, rp * rp, d_ent_.p);
+  else k_prune<true><<<dev_sms_ * 8, 128, 0, stream_>>>(A, rp * rp, d_ent_.p);
+  k_end_prune<<<blocks_for(size_t(3) * n_, 256), 256, 0, stream_>>>(n_, d_x, d_xp_.p, d_counters_.p);
+  k_lower_prune<<<1, 1, 0, stream_>>>(d_counters_.p);
+}
+
+void Engine::pair_forces(bool ener, bool vir) {
+  PairArgs A = pair_args();
+  const int coul = coul_ ? (pme_ ? 1 : 2) : 0;
+  const int grid = dev_sms_ * 8;
+  const int ntab = nt_ + 1;
+  if (mixed_) {
+    const size_t smem = sizeof(float4) * (size_t(ntab) * ntab + 4 * 64) + sizeof(int) * 4 * 64;
+    // the rational fits hold for (kappa r_c)^2 <= 16; past that the library erfc form
+    const int c32 = coul == 0 ? 0 : (kappa_ * kappa_ * rc_ * rc_ <= double(kEwUMax) ? coul : coul + 2);
+#define PAIR32(C, E, V)                                                                                              \
+  do {                                                                                                               \
+    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_pair_f32<C, E, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
+    k_pair_f32<C, E, V><<<grid, 128, smem, stream_>>>(A);                                                            \
+  } while (0)
+#define PAIR32C(C) { if (ener) { if (vir) PAIR32(C, true, true); else PAIR32(C, true, false); } else { if (vir) PAIR32(C, false, true); else PAIR32(C, false, false); } }
+    switch (c32) {
+      case 1: PAIR32C(1) break;
+      case 2: PAIR32C(2) break;
+      case 3: PAIR32C(3) break;
+      case 4: PAIR32C(4) break;
+      default: PAIR32C(0) break;
+    }
+#undef PAIR32C
+#undef PAIR32
+  } else {
+    const size_t smem = sizeof(double4) * (size_t(ntab) * ntab + 4 * 64) + sizeof(double) * 2 * size_t(coul ? gnodes_ : 0) + sizeof(int) * 4 * 64;
+#define PAIR64(C, ...)                                                                                               \
+  do {                                                                                                               \
+    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_pair_f64<C, __VA_ARGS__>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
+    k_pair_f64<C, __VA_ARGS__><<<grid, 128, smem, stream_>>>(A);                                                     \
+  } while (0)
+    if (opt_.force_cap > 0) {
+      // push-off: energies and virial always on (a rare path, kept to one instantiation per Coulomb form)
+      if (coul == 1) PAIR64(1, true, true, true);
+      else if (coul == 2) PAIR64(2, true, true, true);
+      else PAIR64(0, true, true, true);
+    } else if (coul == 1) { if (ener) { if (vir) PAIR64(1, true, true); else PAIR64(1, true, false); } else { if (vir) PAIR64(1, false, true); else PAIR64(1, false, false); } }
+    else if (coul == 2) { if (ener) { if (vir) PAIR64(2, true, true); else PAIR64(2, true, false); } else { if (vir) PAIR64(2, false, true); else PAIR64(2, false, false); } }
+    else { if (ener) { if (vir) PAIR64(0, true, true); else PAIR64(0, true, false); } else { if (vir) PAIR64(0, false, true); else PAIR64(0, false, false); } }
+#undef PAIR64
+  }
+  CK(cudaGetLastError());
+}
+
+// One force evaluation on device positions d_x (AoS, 3 n): accumulators cleared, list checked / rebuilt, every term,
+// forces reduced into d_f_ (AoS doubles). Asynchronous on stream_.
+void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild) {
+  const bool nonb = (opt_.parts & 2) != 0;
+  if (nonb) {
+    if (!list_valid_) {
+      k_set_flag<<<1, 1, 0, stream_>>>(d_counters_.p, kCntRebuild, 1);
+      list_valid_ = true;
+      ++builds_;
+    } else if (check_rebuild) {
+      k_check_moved<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_x, d_x0_.p, 0.25 * skin_ * skin_, d_counters_.p);
+    }
+    launch_build(d_x);
+  }
+  if (mixed_) {
+    CK(cudaMemsetAsync(d_F_.p, 0, d_F_.n * sizeof(long long), stream_));
+    if (nonb) CK(cudaMemsetAsync(d_Fs_.p, 0, d_Fs_.n * sizeof(long long), stream_));
+  } else {
+    CK(cudaMemsetAsync(d_Fd_.p, 0, d_Fd_.n * sizeof(double), stream_));
+    if (nonb) CK(cudaMemsetAsync(d_Fsd_.p, 0, d_Fsd_.n * sizeof(double), stream_));
+  }
+  CK(cudaMemsetAsync(d_efix_.p, 0, d_efix_.n * sizeof(long long), stream_));
+  CK(cudaMemsetAsync(d_edbl_.p, 0, d_edbl_.n * sizeof(double), stream_));
+  if (nonb) {
+    const size_t ns = size_t(nsc_cap_) * kScAtoms;
+    if (mixed_)
+      k_pack_f32<<<blocks_for(ns, 256), 256, 0, stream_>>>(int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_sc_org_.p, d_q_.p, d_type_.p, nt_,
+                                                           d_xq_.p, d_tslot_.p, d_counters_.p);
+    else
+      k_pack_f64<<<blocks_for(ns, 256), 256, 0, stream_>>>(int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_q_.p, d_type_.p, nt_, d_xqd_.p, d_tslot_.p,
+                                                           d_counters_.p);
+    prune(d_x);
+    pair_forces(ener, vir);
+  }
+  bonded_forces(d_x, ener, vir);
+  if (nonb && pme_) pme_forces(d_x, ener, vir);
+  const size_t ns = size_t(nsc_cap_) * kScAtoms;
+  if (mixed_) k_reduce_f32<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_F_.p, d_Fs_.p, int(ns), d_iperm_.p, d_f_.p, nonb ? 1 : 0);
+  else k_reduce_f64<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_Fd_.p, d_Fsd_.p, int(ns), d_iperm_.p, d_f_.p, nonb ? 1 : 0);
+  if (nonb) k_lower_flag<<<1, 1, 0, stream_>>>(d_counters_.p);
+  CK(cudaGetLastError());
+}
+
+}  // namespace capsb

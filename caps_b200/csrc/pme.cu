@@ -1,0 +1,130 @@
+// Host side of PME: plans, twiddle tables and line blocking per grid, and the spread / transform / solve / gather
+// launch sequence.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <vector>
+
+#include "engine.h"
+#include "pme.cuh"
+
+namespace capsb {
+
+namespace {
+
+void factor_radices(int n, int* rad, int& nst) {
+  nst = 0;
+  int r = n;
+  while (r % 4 == 0 && nst < kMaxRadices) rad[nst++] = 4, r /= 4;
+  for (int p : {2, 3, 5, 7}) while (r % p == 0 && nst < kMaxRadices) rad[nst++] = p, r /= p;
+  if (r != 1) throw ModelError(CAPS_GPU_EINVAL, "PME grid length " + std::to_string(n) + " cannot be factored for the line FFT");
+}
+
+}  // namespace
+
+template <class R>
+void Engine::pme_setup(PmePath<R>& P) {
+  using T = typename Cpx<R>::T;
+  const size_t half = size_t(ph1_) * pk_[1] * pk_[2];
+  P.h.alloc(half);
+  P.gr.alloc(size_t(pk_[0]) * pk_[1] * pk_[2]);
+  P.gt.alloc(half);
+  P.wt.alloc(6 * half);
+  if (mixed_) d_gridq_.alloc(size_t(pk_[0]) * pk_[1] * pk_[2]);
+  d_grid_.alloc(size_t(pk_[0]) * pk_[1] * pk_[2]);
+  for (int d = 0; d < 3; ++d)
+    for (int dir = 0; dir < 2; ++dir) {
+      const int nn = pk_[d];
+      const int sign = dir == 0 ? -1 : +1;   // forward e^{-i}, inverse e^{+i}: the convolution is the same either way
+      std::vector<T> tw(static_cast<size_t>(nn));
+      for (int k = 0; k < nn; ++k) {
+        const double ang = 2 * kPi * k / nn;
+        tw[size_t(k)] = T{R(std::cos(ang)), R(sign * std::sin(ang))};
+      }
+      P.tw[d][dir].upload(tw, stream_);
+      FftPlan<R>& pl = P.plan[d][dir];
+      pl.n = nn;
+      factor_radices(nn, pl.rad, pl.nst);
+      pl.tw = P.tw[d][dir].p;
+      pl.sign = sign;
+    }
+  // Lines per block. x: contiguous lines, enough blocks for four per SM, two buffers within 40 KB of shared memory.
+  // y, z: `la` consecutive a per block so that each row read is 128 bytes.
+  const int cap = int(40 * 1024 / (2 * sizeof(T)));
+  const int nlx = pk_[1] * pk_[2];
+  lines_x_ = std::max(1, std::min({cap / pk_[0], 16, (nlx + 4 * dev_sms_ - 1) / (4 * dev_sms_)}));
+  const int la = int(128 / sizeof(T));
+  lines_y_ = std::max(1, std::min({la, cap / pk_[1], ph1_}));
+  lines_z_ = std::max(1, std::min({la, cap / pk_[2], ph1_}));
+  green_valid_ = false;
+  CK(cudaStreamSynchronize(stream_));
+}
+
+template <class R>
+void Engine::pme_run(PmePath<R>& P, const double* d_x, bool ener, bool vir) {
+  using T = typename Cpx<R>::T;
+  PmeArgs A{pk_[0], pk_[1], pk_[2], ph1_, dcell_, d_x, d_q_.p, n_};
+  if (!green_valid_ || std::memcmp(green_cell_, cell_h_, sizeof cell_h_) != 0) {
+    const size_t half = size_t(ph1_) * pk_[1] * pk_[2];
+    k_pme_green<R><<<blocks_for(half, 256), 256, 0, stream_>>>(A, d_bsp_[0].p, d_bsp_[1].p, d_bsp_[2].p, beta_, kCoulomb, P.gt.p, P.wt.p);
+    std::memcpy(green_cell_, cell_h_, sizeof cell_h_);
+    green_valid_ = true;
+  }
+  const int nb = blocks_for(size_t(n_), 128);
+  if (mixed_) CK(cudaMemsetAsync(d_gridq_.p, 0, d_gridq_.n * sizeof(long long), stream_));
+  else CK(cudaMemsetAsync(d_grid_.p, 0, d_grid_.n * sizeof(double), stream_));
+#define SPREAD(P_)                                                                            \
+  do {                                                                                        \
+    if (mixed_) k_spread<float, P_><<<nb, 128, 0, stream_>>>(A, d_grid_.p, d_gridq_.p);      \
+    else k_spread<double, P_><<<nb, 128, 0, stream_>>>(A, d_grid_.p, d_gridq_.p);            \
+  } while (0)
+  switch (order_) {
+    case 3: SPREAD(3); break;
+    case 4: SPREAD(4); break;
+    case 5: SPREAD(5); break;
+    case 6: SPREAD(6); break;
+    case 7: SPREAD(7); break;
+    default: SPREAD(8); break;
+  }
+#undef SPREAD
+  // shared memory: twiddle table(s) + two line buffers
+  const size_t sx = (size_t(lines_x_) * 2 + 1) * pk_[0] * sizeof(T), sy = (size_t(lines_y_) * 2 + 1) * pk_[1] * sizeof(T),
+               sz = (size_t(lines_z_) + 1) * 2 * pk_[2] * sizeof(T);
+  const int nlx = pk_[1] * pk_[2];
+  k_fft_x_fwd<R><<<blocks_for(size_t(nlx), lines_x_), 128, sx, stream_>>>(A, mixed_ ? nullptr : d_grid_.p, mixed_ ? d_gridq_.p : nullptr, P.h.p,
+                                                                        P.plan[0][0], lines_x_);
+  const int gy = ((ph1_ + lines_y_ - 1) / lines_y_) * pk_[2];
+  k_fft_y<R><<<gy, 128, sy, stream_>>>(A, P.h.p, P.plan[1][0], lines_y_);
+  const int gz = ((ph1_ + lines_z_ - 1) / lines_z_) * pk_[1];
+  EnergySink en{d_efix_.p, d_edbl_.p};
+  if (ener) { if (vir) k_fft_z_solve<R, true, true><<<gz, 128, sz, stream_>>>(A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); else k_fft_z_solve<R, true, false><<<gz, 128, sz, stream_>>>(A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); }
+  else { if (vir) k_fft_z_solve<R, false, true><<<gz, 128, sz, stream_>>>(A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); else k_fft_z_solve<R, false, false><<<gz, 128, sz, stream_>>>(A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); }
+  k_fft_y<R><<<gy, 128, sy, stream_>>>(A, P.h.p, P.plan[1][1], lines_y_);
+  k_fft_x_inv<R><<<blocks_for(size_t(nlx), lines_x_), 128, sx, stream_>>>(A, P.h.p, P.gr.p, P.plan[0][1], lines_x_);
+  const ForceSink<float> Ff{d_F_.p, d_F_.p + n_, d_F_.p + 2 * size_t(n_), d_counters_.p + kCntErr};
+  const ForceSink<double> Fd{d_Fd_.p, d_Fd_.p + n_, d_Fd_.p + 2 * size_t(n_)};
+#define GATHER(P_)                                                                            \
+  do {                                                                                        \
+    if (mixed_) k_gather<float, R, P_><<<nb, 128, 0, stream_>>>(A, P.gr.p, Ff);              \
+    else k_gather<double, R, P_><<<nb, 128, 0, stream_>>>(A, P.gr.p, Fd);                     \
+  } while (0)
+  switch (order_) {
+    case 3: GATHER(3); break;
+    case 4: GATHER(4); break;
+    case 5: GATHER(5); break;
+    case 6: GATHER(6); break;
+    case 7: GATHER(7); break;
+    default: GATHER(8); break;
+  }
+#undef GATHER
+  CK(cudaGetLastError());
+}
+
+void Engine::pme_forces(const double* d_x, bool ener, bool vir) { pme_run(pd_, d_x, ener, vir); }
+
+
+template void Engine::pme_setup<double>(PmePath<double>&);
+template void Engine::pme_run<double>(PmePath<double>&, const double*, bool, bool);
+
+}  // namespace capsb

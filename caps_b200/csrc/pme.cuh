@@ -13,78 +13,75 @@
 // Kernels: K-SPREAD (thread per atom, fixed-point atomics on the FP32 path: deterministic), K-FFT-X (real lines to half
 // spectra), K-FFT-Y, K-FFT-Z+SOLVE (forward z transform, G multiply with energy/virial, inverse z transform, fused in one
 // pass over the grid), K-FFT-Y inverse, K-FFT-X inverse (half spectra to real lines), K-GATHER. Each line transform is a
-// Stockham autosort FFT in shared memory (radix 2, 3, 4, 5, 7 and a generic odd radix), twiddles from host tables.
+// Stockham autosort FFT in shared memory (radix 2, 3, 4, 5, 7 butterflies unrolled in registers), twiddles staged from
+// host-computed tables into shared memory.
 #pragma once
-#include "common.cuh"
+#include "pme_types.cuh"
 
 namespace capsb {
 
-constexpr int kMaxRadices = 16;
-constexpr int kMaxOrder = 8;
+// One radix-RAD Stockham pass over `nl` lines of length n, line-major, from `in` to `out`; Ns = product of the radices
+// before this pass. tw is the plan's twiddle table staged in shared memory. Every index stays below n: r k stride <=
+// (RAD-1)(Ns-1) n / (Ns RAD) < n. Butterflies are unrolled in registers; the small-radix DFT constants W_RAD^e = tw[e n/RAD].
+template <class T, int RAD>
+__device__ __forceinline__ void stockham_pass(const T* __restrict__ in, T* __restrict__ out, const T* __restrict__ tw, int n, int Ns, int nl,
+                                              int sign) {
+  using R = decltype(T::x);
+  const int nb = n / RAD, stride = n / (Ns * RAD);
+  T w[RAD];
+#pragma unroll
+  for (int e = 0; e < RAD; ++e) w[e] = tw[e * nb];
+  for (int t = threadIdx.x; t < nl * nb; t += blockDim.x) {
+    const int l = t / nb, j = t - l * nb;
+    const int k = j % Ns;
+    const T* src = in + l * n;
+    T v[RAD];
+    v[0] = src[j];
+#pragma unroll
+    for (int r = 1; r < RAD; ++r) v[r] = cmul(src[j + r * nb], tw[r * k * stride]);
+    T o[RAD];
+    if constexpr (RAD == 2) {
+      o[0] = cadd(v[0], v[1]);
+      o[1] = csub(v[0], v[1]);
+    } else if constexpr (RAD == 4) {
+      const T s0 = cadd(v[0], v[2]), s1 = csub(v[0], v[2]), s2 = cadd(v[1], v[3]), s3 = csub(v[1], v[3]);
+      const T is3 = {R(-sign) * s3.y, R(sign) * s3.x};   // sign * i * s3
+      o[0] = cadd(s0, s2);
+      o[2] = csub(s0, s2);
+      o[1] = cadd(s1, is3);
+      o[3] = csub(s1, is3);
+    } else {
+#pragma unroll
+      for (int m = 0; m < RAD; ++m) {
+        T acc = v[0];
+#pragma unroll
+        for (int r = 1; r < RAD; ++r) acc = cadd(acc, cmul(v[r], w[(m * r) % RAD]));
+        o[m] = acc;
+      }
+    }
+    T* dst = out + l * n + (j - k) * RAD + k;   // (j / Ns) Ns RAD + k
+#pragma unroll
+    for (int r = 0; r < RAD; ++r) dst[r * Ns] = o[r];
+  }
+}
 
-template <class R> struct Cpx;
-template <> struct Cpx<float> { using T = float2; };
-template <> struct Cpx<double> { using T = double2; };
-
-template <class T> __device__ __forceinline__ T cmul(T a, T b) { return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x}; }
-template <class T> __device__ __forceinline__ T cadd(T a, T b) { return {a.x + b.x, a.y + b.y}; }
-template <class T> __device__ __forceinline__ T csub(T a, T b) { return {a.x - b.x, a.y - b.y}; }
-
+// All passes of a plan over `nl` lines held line-major in a (scratch b; tw in shared memory). Returns the buffer holding
+// the result (a or b). The plans hold radices 2, 3, 4, 5 and 7 only (grid lengths are 2^a 3^b 5^c 7^d).
 template <class R>
-struct FftPlan {
-  int n, nst;
-  int rad[kMaxRadices];
-  const typename Cpx<R>::T* tw;   // exp(sign 2 pi i k / n), k < n
-  int sign;                        // +1 / -1 (the sign of tw)
-};
-
-// One Stockham pass set over `nl` lines of length n held line-major in a (scratch b). Returns the buffer holding the
-// result (a or b).
-template <class R>
-__device__ typename Cpx<R>::T* fft_lines_smem(typename Cpx<R>::T* a, typename Cpx<R>::T* b, int nl, const FftPlan<R>& P) {
+__device__ typename Cpx<R>::T* fft_lines_smem(typename Cpx<R>::T* a, typename Cpx<R>::T* b, const typename Cpx<R>::T* tw, int nl,
+                                              const FftPlan<R>& P) {
   using T = typename Cpx<R>::T;
-  const int n = P.n;
   int Ns = 1;
   T* in = a;
   T* out = b;
   for (int s = 0; s < P.nst; ++s) {
     const int Rr = P.rad[s];
-    const int nb = n / Rr;               // butterflies per line
-    const int stride = n / (Ns * Rr);    // twiddle stride
-    for (int t = threadIdx.x; t < nl * nb; t += blockDim.x) {
-      const int l = t / nb, j = t - l * nb;
-      const int k = j % Ns;
-      T v[kMaxRadices];
-      const T* src = in + l * n;
-      v[0] = src[j];
-      for (int r = 1; r < Rr; ++r) v[r] = cmul(src[j + r * nb], P.tw[(r * k * stride) % n]);
-      T o[kMaxRadices];
-      if (Rr == 2) {
-        o[0] = cadd(v[0], v[1]);
-        o[1] = csub(v[0], v[1]);
-      } else if (Rr == 4) {
-        const T s0 = cadd(v[0], v[2]), s1 = csub(v[0], v[2]), s2 = cadd(v[1], v[3]), s3 = csub(v[1], v[3]);
-        const T is3 = {R(-P.sign) * s3.y, R(P.sign) * s3.x};   // sign * i * s3
-        o[0] = cadd(s0, s2);
-        o[2] = csub(s0, s2);
-        o[1] = cadd(s1, is3);
-        o[3] = csub(s1, is3);
-      } else {
-        const int step = n / Rr;   // W_R^m = tw[m * n / R]
-        for (int m = 0; m < Rr; ++m) {
-          T acc = v[0];
-          int e = 0;
-          for (int r = 1; r < Rr; ++r) {
-            e += m;
-            if (e >= Rr) e -= Rr;
-            acc = cadd(acc, cmul(v[r], P.tw[e * step]));
-          }
-          o[m] = acc;
-        }
-      }
-      const int d = (j / Ns) * Ns * Rr + k;
-      T* dst = out + l * n;
-      for (int r = 0; r < Rr; ++r) dst[d + r * Ns] = o[r];
+    switch (Rr) {
+      case 2: stockham_pass<T, 2>(in, out, tw, P.n, Ns, nl, P.sign); break;
+      case 3: stockham_pass<T, 3>(in, out, tw, P.n, Ns, nl, P.sign); break;
+      case 4: stockham_pass<T, 4>(in, out, tw, P.n, Ns, nl, P.sign); break;
+      case 5: stockham_pass<T, 5>(in, out, tw, P.n, Ns, nl, P.sign); break;
+      default: stockham_pass<T, 7>(in, out, tw, P.n, Ns, nl, P.sign); break;
     }
     __syncthreads();
     T* tmp = in;
@@ -93,6 +90,11 @@ __device__ typename Cpx<R>::T* fft_lines_smem(typename Cpx<R>::T* a, typename Cp
     Ns *= Rr;
   }
   return in;
+}
+
+template <class T>
+__device__ __forceinline__ void stage_twiddles(T* dst, const T* __restrict__ src, int n) {
+  for (int t = threadIdx.x; t < n; t += blockDim.x) dst[t] = src[t];
 }
 
 // Cardinal B-spline weights of order P at fractional offset w (caps_kspace.f90:568-598), 0-based: th[j] weighs grid
@@ -178,24 +180,27 @@ static __global__ void k_spread(PmeArgs A, double* __restrict__ g, long long* __
   }
 }
 
+// Shared memory of the line-transform kernels: the twiddle table(s), then two buffers of `lines` lines of length n.
 // K-FFT-X forward: real lines (b, c) of length K1 to half spectra h(a, b, c), a <= K1/2. Input: g (double) or gq (fixed).
 template <class R>
-static __global__ void k_fft_x_fwd(PmeArgs A, const double* __restrict__ g, const long long* __restrict__ gq, typename Cpx<R>::T* __restrict__ h,
-                            FftPlan<R> P, int lines_per_block) {
+static __global__ void __launch_bounds__(128) k_fft_x_fwd(PmeArgs A, const double* __restrict__ g, const long long* __restrict__ gq,
+                                                          typename Cpx<R>::T* __restrict__ h, FftPlan<R> P, int lines_per_block) {
   using T = typename Cpx<R>::T;
   extern __shared__ unsigned char smem_raw[];
-  T* s0 = reinterpret_cast<T*>(smem_raw);
+  T* tw = reinterpret_cast<T*>(smem_raw);
+  T* s0 = tw + A.k1;
   T* s1 = s0 + lines_per_block * A.k1;
   const int nlines = A.k2 * A.k3;
   const int l0 = blockIdx.x * lines_per_block;
   const int nl = min(lines_per_block, nlines - l0);
+  stage_twiddles(tw, P.tw, A.k1);
   for (int t = threadIdx.x; t < nl * A.k1; t += blockDim.x) {
     const size_t gidx = size_t(l0) * A.k1 + t;   // lines are contiguous in the real grid
     const R v = gq ? R(double(gq[gidx]) * kInvFixQ) : R(g[gidx]);
     s0[t] = {v, R(0)};
   }
   __syncthreads();
-  const T* res = fft_lines_smem<R>(s0, s1, nl, P);
+  const T* res = fft_lines_smem<R>(s0, s1, tw, nl, P);
   for (int t = threadIdx.x; t < nl * A.h1; t += blockDim.x) {
     const int l = t / A.h1, a = t - l * A.h1;
     h[size_t(l0 + l) * A.h1 + a] = res[l * A.k1 + a];
@@ -204,14 +209,17 @@ static __global__ void k_fft_x_fwd(PmeArgs A, const double* __restrict__ g, cons
 
 // K-FFT-X inverse: half spectra back to real lines (the missing half by Hermitian symmetry), real part kept.
 template <class R>
-static __global__ void k_fft_x_inv(PmeArgs A, const typename Cpx<R>::T* __restrict__ h, R* __restrict__ gr, FftPlan<R> P, int lines_per_block) {
+static __global__ void __launch_bounds__(128) k_fft_x_inv(PmeArgs A, const typename Cpx<R>::T* __restrict__ h, R* __restrict__ gr, FftPlan<R> P,
+                                                          int lines_per_block) {
   using T = typename Cpx<R>::T;
   extern __shared__ unsigned char smem_raw[];
-  T* s0 = reinterpret_cast<T*>(smem_raw);
+  T* tw = reinterpret_cast<T*>(smem_raw);
+  T* s0 = tw + A.k1;
   T* s1 = s0 + lines_per_block * A.k1;
   const int nlines = A.k2 * A.k3;
   const int l0 = blockIdx.x * lines_per_block;
   const int nl = min(lines_per_block, nlines - l0);
+  stage_twiddles(tw, P.tw, A.k1);
   for (int t = threadIdx.x; t < nl * A.k1; t += blockDim.x) {
     const int l = t / A.k1, m = t - l * A.k1;
     const size_t lb = size_t(l0 + l) * A.h1;
@@ -224,26 +232,28 @@ static __global__ void k_fft_x_inv(PmeArgs A, const typename Cpx<R>::T* __restri
     s0[t] = v;
   }
   __syncthreads();
-  const T* res = fft_lines_smem<R>(s0, s1, nl, P);
+  const T* res = fft_lines_smem<R>(s0, s1, tw, nl, P);
   for (int t = threadIdx.x; t < nl * A.k1; t += blockDim.x) gr[size_t(l0) * A.k1 + t] = res[t].x;
 }
 
-// K-FFT-Y: lines along b for fixed (a, c); a block takes `la` consecutive a (coalesced) of one c.
+// K-FFT-Y: lines along b for fixed (a, c); a block takes `la` consecutive a (coalesced rows) of one c.
 template <class R>
-static __global__ void k_fft_y(PmeArgs A, typename Cpx<R>::T* __restrict__ h, FftPlan<R> P, int la) {
+static __global__ void __launch_bounds__(128) k_fft_y(PmeArgs A, typename Cpx<R>::T* __restrict__ h, FftPlan<R> P, int la) {
   using T = typename Cpx<R>::T;
   extern __shared__ unsigned char smem_raw[];
-  T* s0 = reinterpret_cast<T*>(smem_raw);
+  T* tw = reinterpret_cast<T*>(smem_raw);
+  T* s0 = tw + A.k2;
   T* s1 = s0 + la * A.k2;
   const int ngrp = (A.h1 + la - 1) / la;
   const int c = blockIdx.x / ngrp, a0 = (blockIdx.x % ngrp) * la;
   const int nl = min(la, A.h1 - a0);
+  stage_twiddles(tw, P.tw, A.k2);
   for (int t = threadIdx.x; t < nl * A.k2; t += blockDim.x) {
     const int b = t / nl, al = t - b * nl;
     s0[al * A.k2 + b] = h[size_t(a0 + al) + size_t(A.h1) * (size_t(b) + size_t(A.k2) * c)];
   }
   __syncthreads();
-  const T* res = fft_lines_smem<R>(s0, s1, nl, P);
+  const T* res = fft_lines_smem<R>(s0, s1, tw, nl, P);
   for (int t = threadIdx.x; t < nl * A.k2; t += blockDim.x) {
     const int b = t / nl, al = t - b * nl;
     h[size_t(a0 + al) + size_t(A.h1) * (size_t(b) + size_t(A.k2) * c)] = res[al * A.k2 + b];
@@ -253,22 +263,27 @@ static __global__ void k_fft_y(PmeArgs A, typename Cpx<R>::T* __restrict__ h, Ff
 // K-FFT-Z+SOLVE: lines along c for fixed (a, b): forward transform, energy and virial of the half spectrum (e_m doubled
 // for 0 < a < K1/2), multiply by G, inverse transform, in one pass.
 template <class R, bool ENER, bool VIR>
-static __global__ void k_fft_z_solve(PmeArgs A, typename Cpx<R>::T* __restrict__ h, const R* __restrict__ gt, const R* __restrict__ wt, FftPlan<R> Pf,
-                              FftPlan<R> Pi, int la, EnergySink en, int fixed) {
+static __global__ void __launch_bounds__(128) k_fft_z_solve(PmeArgs A, typename Cpx<R>::T* __restrict__ h, const R* __restrict__ gt,
+                                                            const R* __restrict__ wt, FftPlan<R> Pf, FftPlan<R> Pi, int la, EnergySink en,
+                                                            int fixed) {
   using T = typename Cpx<R>::T;
   extern __shared__ unsigned char smem_raw[];
-  T* s0 = reinterpret_cast<T*>(smem_raw);
+  T* twf = reinterpret_cast<T*>(smem_raw);
+  T* twi = twf + A.k3;
+  T* s0 = twi + A.k3;
   T* s1 = s0 + la * A.k3;
   const int ngrp = (A.h1 + la - 1) / la;
   const int b = blockIdx.x / ngrp, a0 = (blockIdx.x % ngrp) * la;
   const int nl = min(la, A.h1 - a0);
   const size_t plane = size_t(A.h1) * A.k2;
+  stage_twiddles(twf, Pf.tw, A.k3);
+  stage_twiddles(twi, Pi.tw, A.k3);
   for (int t = threadIdx.x; t < nl * A.k3; t += blockDim.x) {
     const int c = t / nl, al = t - c * nl;
     s0[al * A.k3 + c] = h[size_t(a0 + al) + size_t(A.h1) * b + plane * c];
   }
   __syncthreads();
-  T* res = fft_lines_smem<R>(s0, s1, nl, Pf);
+  T* res = fft_lines_smem<R>(s0, s1, twf, nl, Pf);
   T* other = res == s0 ? s1 : s0;
   double e = 0, w[6] = {0, 0, 0, 0, 0, 0};
   for (int t = threadIdx.x; t < nl * A.k3; t += blockDim.x) {
@@ -289,7 +304,7 @@ static __global__ void k_fft_z_solve(PmeArgs A, typename Cpx<R>::T* __restrict__
     res[t] = v;
   }
   __syncthreads();
-  const T* back = fft_lines_smem<R>(res, other, nl, Pi);
+  const T* back = fft_lines_smem<R>(res, other, twi, nl, Pi);
   for (int t = threadIdx.x; t < nl * A.k3; t += blockDim.x) {
     const int c = t / nl, al = t - c * nl;
     h[size_t(a0 + al) + size_t(A.h1) * b + plane * c] = back[al * A.k3 + c];
