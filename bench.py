@@ -142,6 +142,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--profile-pair", type=int, default=0, metavar="LAUNCHES",
                     help="only time the pair kernel LAUNCHES times on the start structure (a small case for ncu captures)")
+    ap.add_argument("--profile-md", type=int, default=0, metavar="STEPS",
+                    help="only run the mixed MD: --warmup steps, then STEPS steps (the command for ncu launch lists)")
     args = ap.parse_args()
     rank, world, local = int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
     if args.warmup < 3:
@@ -154,6 +156,17 @@ def main():
             ev = Evaluator(ff, options(prec, 1, 1).energy)
             print(json.dumps({"precision": prec, **ev.pair_timing(x, cell, launches=args.profile_pair)}), flush=True)
             ev.close()
+        return
+
+    if args.profile_md:
+        from caps_b200 import Evaluator
+        ff, x, v, cell = workload()
+        o = options("mixed", args.warmup, 7)
+        ev = Evaluator(ff, o.energy)
+        out = ev.run(x, cell, o, v=v)
+        out = ev.run(out["x"], cell, options("mixed", args.profile_md, 7), v=out["v"])
+        print(json.dumps({"profile_md": args.profile_md, "report": out["report"], "kernels_run": ev.kernels_run()}), flush=True)
+        ev.close()
         return
 
     if args.impl == "reference":
@@ -202,11 +215,14 @@ def main():
     x1, v1 = out["x"], out["v"]
     ev.set_timing(FLUSH_BYTES)
     barrier()
+    b0 = ev.list_builds()
     with Clocks(local) as clk:
         out = ev.run(x1, cell, options("mixed", args.steps, seed), v=v1)
     barrier()
+    builds = ev.list_builds() - b0
     ms_step = max_over_ranks(ev.last_step_ms())
-    launches = ev.step_kernels() * args.steps
+    launches = ev.kernels_run()
+    print(f"[bench] timed run: {out['report']} · {ev.step_kernels()} kernel nodes per plain step, {launches} kernels run", file=sys.stderr, flush=True)
     ev.set_timing(-1)
     x2, v2 = out["x"], out["v"]
     sps = 1000.0 / ms_step
@@ -216,6 +232,7 @@ def main():
     t0 = time.perf_counter()
     eo_run = ev.run(x2, cell, options("mixed", args.steps, seed), v=v2)
     e2e_wall = time.perf_counter() - t0
+    print(f"[bench] e2e run: {eo_run['report']}", file=sys.stderr, flush=True)
     e2e_nsd = args.steps * 1.0 * 1e-6 / e2e_wall * 86400 * world
     h2d = (2 * 3 * n * 8 + 12 * 8) / args.steps
     d2h = (2 * 3 * n * 8 + 12 * 8 + 2 * 232) / args.steps
@@ -276,6 +293,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 pair/PME spread-gather, int64 fixed-point sums, f64 FFT/bonded/integrator", "data": "synthetic", "config": cfg,
             "atom_steps_per_s": sps * n * world,
+            "list_builds": builds,
             "fp64": {"ns_per_day": nsd64 * world, "ms_per_step": ms64, "steps": k64, "mixed_speedup": ms64 / ms_step},
             "force_error_vs_fp64": {"rms_relative": rms_rel, "per_atom_rms": float(np.sqrt(np.mean(per_atom ** 2))),
                                     "per_atom_max": float(per_atom.max()), "energy_relative": e_err},
@@ -288,7 +306,7 @@ def main():
                          "work": f"{pt['pairs_in_cutoff']:.0f} pairs inside the cut-off x {FLOPS_PER_PAIR} flops per launch",
                          "pair_ms": pt["avg_ms"], "pairs_listed": pt["pairs_listed"], "entries": pt["entries"], "traffic": None},
             "gpu_launches": launches,
-            "gpu_launches_note": "kernel nodes of the captured step graph x timed steps (thermo steps launch the same kernels uncaptured)",
+            "gpu_launches_note": "kernels launched in the timed step loop, counted by the engine: the step graphs' kernel nodes per replayed step (list-build and prune kernels included; they return at once on steps without a build or prune), plus one kinetic-energy kernel per thermo row",
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
         }

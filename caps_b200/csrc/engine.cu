@@ -123,6 +123,13 @@ Engine::Engine(const caps_gpu_ff* ff, const caps_gpu_opts* o) {
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&dev_sms_, cudaDevAttrMultiProcessorCount, dev));
   CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  // the side streams (bonded terms, PME) run at the highest priority: their short kernels take SM slots as the long
+  // pair kernel frees them
+  int prio_lo = 0, prio_hi = 0;
+  CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+  for (auto& st : side_) CK(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio_hi));
+  CK(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
+  for (auto& ev : ev_join_) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   CK(cudaMallocHost(&h_counters_, sizeof(int) * kCntNum));
   CK(cudaMallocHost(&h_efix_, sizeof(long long) * kENumSlots));
   CK(cudaMallocHost(&h_edbl_, sizeof(double) * kENumSlots));
@@ -137,6 +144,11 @@ Engine::~Engine() {
   if (h_efix_) cudaFreeHost(h_efix_);
   if (h_edbl_) cudaFreeHost(h_edbl_);
   if (stream_) cudaStreamDestroy(stream_);
+  for (auto st : side_)
+    if (st) cudaStreamDestroy(st);
+  if (ev_fork_) cudaEventDestroy(ev_fork_);
+  for (auto ev : ev_join_)
+    if (ev) cudaEventDestroy(ev);
 }
 
 void Engine::setup_ff(const caps_gpu_ff* ff) {
@@ -700,7 +712,14 @@ int32_t caps_gpu_compute_device(caps_gpu_engine* e, const double* d_x, const dou
   return guard(e, [&] { e->e->compute_dev(d_x, cell, d_f, out); });
 }
 
-int32_t caps_gpu_list_builds(const caps_gpu_engine* e) { return e ? e->e->list_builds() : 0; }
+int32_t caps_gpu_list_builds(const caps_gpu_engine* e) {
+  if (!e) return 0;
+  try {
+    return e->e->list_builds();
+  } catch (...) {
+    return -1;
+  }
+}
 
 int32_t caps_gpu_run(caps_gpu_engine* e, caps_gpu_state* state, const caps_gpu_md_opts* md, caps_gpu_progress_fn progress, caps_gpu_frame_fn frame,
                      void* user, char* report, int32_t report_cap) {
@@ -726,6 +745,7 @@ int32_t caps_gpu_diag_set_timing(caps_gpu_engine* e, int64_t flush_bytes) {
 double caps_gpu_diag_last_step_ms(const caps_gpu_engine* e) { return e ? e->e->last_step_ms_device() : 0.0; }
 
 int32_t caps_gpu_diag_step_kernels(const caps_gpu_engine* e) { return e ? e->e->graph_kernels() : 0; }
+int64_t caps_gpu_diag_kernels_run(const caps_gpu_engine* e) { return e ? e->e->kernels_run() : 0; }
 
 int32_t caps_gpu_diag_pair_timing(caps_gpu_engine* e, const double* x, const double* cell, int32_t launches, int64_t flush_bytes, double* avg_ms,
                                   double* pairs_in, double* pairs_listed, double* entries) {

@@ -104,7 +104,7 @@ class Engine {
   // compute on host arrays (copies in and out) or on device arrays
   void compute_host(const double* x, const double* cell, double* f, caps_gpu_terms* out);
   void compute_dev(const double* d_x, const double* cell, double* d_f, caps_gpu_terms* out);
-  int list_builds() const { return builds_; }
+  int list_builds();   // list builds so far (counted on the device)
   void run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progress_fn progress, caps_gpu_frame_fn frame, void* user, std::string* report);
   double last_steps_per_second() const { return last_sps_; }
   // measurement support (include/caps_gpu_diag.h)
@@ -113,6 +113,7 @@ class Engine {
                         double* pairs_listed, double* entries);
   double last_step_ms_device() const { return last_step_ms_; }
   int graph_kernels() const { return graph_kernels_; }
+  long long kernels_run() const { return kernels_run_; }
   std::string err;
 
   // --- internals used by the step kernels' launcher (integrate.cu) ---
@@ -128,6 +129,12 @@ class Engine {
   void set_cell(const double* cell);
   void ensure_list_capacity();
   void forces(const double* d_x, bool ener, bool vir, bool check_rebuild);   // everything up to d_f_ (device), async
+  // Concurrent branches of a force evaluation: `launch` runs with stream_ pointing at side stream k, after everything
+  // queued on the main stream so far; join(k) makes the main stream wait for it. Captured, these are graph branches.
+  void fork(int k, const std::function<void()>& launch);
+  void join(int k);
+  cudaStream_t side_[2] = {nullptr, nullptr};
+  cudaEvent_t ev_fork_ = nullptr, ev_join_[2] = {nullptr, nullptr};
   void read_terms(caps_gpu_terms* out, bool ener, bool vir);
   void check_errors();
   void launch_build(const double* d_x);
@@ -186,7 +193,6 @@ class Engine {
   DevBuf<unsigned long long> d_masks_;
   DevBuf<int4> d_work_;
   bool list_valid_ = false;
-  int builds_ = 0;
   int nsc_cap_ = 0;
 
   // packed positions, forces
@@ -215,6 +221,7 @@ class Engine {
   double last_sps_ = 0, last_step_ms_ = 0;
   int64_t timing_flush_ = -1;
   int graph_kernels_ = 0;
+  long long kernels_run_ = 0;
   DevBuf<unsigned char> d_flush_;
   int dev_sms_ = 148;
 };

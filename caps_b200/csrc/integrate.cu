@@ -91,24 +91,29 @@ struct HostRng {
 };
 
 // --- kernels --------------------------------------------------------------------------------------------------
-__global__ void k_kick(int n, double* __restrict__ v, const double* __restrict__ f, const double* __restrict__ invm, double h) {
+// Kick then drift, per atom: v = s v + hk kAcc f / m (s = sc[kScFactor] when `scale`, the thermostat's pending velocity
+// factor, else 1), x0 = x (the constraint reference), x += hd v. Non-finite positions raise the error word. With
+// `zero_cw` the constraint-virial sums of this step start at zero.
+__global__ void k_kick_drift(int n, double* __restrict__ x, double* __restrict__ v, double* __restrict__ x0, const double* __restrict__ f,
+                             const double* __restrict__ invm, double hk, double hd, double* sc, int scale, int zero_cw, int* counters) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (zero_cw && i < 6) sc[kScCW0 + i] = 0;
   if (i >= n) return;
-  const double a = h * kAcc * invm[i];
-  v[3 * i] += a * f[3 * i];
-  v[3 * i + 1] += a * f[3 * i + 1];
-  v[3 * i + 2] += a * f[3 * i + 2];
-}
-
-// drift: x0 = x (the constraint reference), x += h v; non-finite positions raise the error word
-__global__ void k_drift(int n, double* __restrict__ x, const double* __restrict__ v, double* __restrict__ x0, double h, int* counters) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= 3 * n) return;
-  const double xo = x[i];
-  x0[i] = xo;
-  const double xn = xo + h * v[i];
-  x[i] = xn;
-  if (!isfinite(xn)) atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), kErrNonFinite);
+  const double s = scale ? sc[kScFactor] : 1.0;
+  const double a = hk * kAcc * invm[i];
+  bool bad = false;
+  for (int r = 0; r < 3; ++r) {
+    double vr = v[3 * i + r];
+    if (scale) vr *= s;
+    vr += a * f[3 * i + r];
+    v[3 * i + r] = vr;
+    const double xo = x[3 * i + r];
+    x0[3 * i + r] = xo;
+    const double xn = xo + hd * vr;
+    x[3 * i + r] = xn;
+    bad |= !isfinite(xn);
+  }
+  if (bad) atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), kErrNonFinite);
 }
 
 struct ConsArgs {
@@ -178,11 +183,50 @@ __global__ void k_shake(ConsArgs C, double* __restrict__ x, const double* __rest
   }
 }
 
-// RATTLE: removes the relative velocity along each constraint (constraints.cpp:232-269); with h > 0 the impulses are
-// read as forces over a half kick and their virial (xx yy zz xy xz yz) is added to sc[kScCW0..].
-__global__ void k_rattle(ConsArgs C, const double* __restrict__ x, double* __restrict__ v, double h, double* sc, int* counters) {
+// The velocity update of one atom before RATTLE: a kick (v += hk kAcc f / m) or the Langevin O step
+// (v = c1 v + c2 sqrt(kB T kAcc / m) N(0, 1), Philox normals keyed by (seed, step, atom)).
+struct VelOp {
+  int kind;                  // 0 none, 1 kick, 2 Langevin O
+  const double* f;
+  double hk;
+  double c1, c2;
+  uint64_t seed;
+};
+__device__ __forceinline__ void vel_op(const VelOp& op, int g, double* vv, const double* __restrict__ invm, const double* sc) {
+  if (op.kind == 1) {
+    const double a = op.hk * kAcc * invm[g];
+    for (int r = 0; r < 3; ++r) vv[r] += a * op.f[3 * g + r];
+  } else if (op.kind == 2) {
+    double z[4];
+    normals4(op.seed, (uint64_t)sc[kScStep], uint32_t(g), 0x4C414E47u, z);
+    const double sd = sqrt(kB * sc[kScTnow] * kAcc * invm[g]);
+    for (int r = 0; r < 3; ++r) vv[r] = op.c1 * vv[r] + op.c2 * sd * z[r];
+  }
+}
+
+// The velocity update alone, one thread per atom (runs without constraints).
+__global__ void k_vel(int n, double* __restrict__ v, const double* __restrict__ invm, const double* sc, VelOp op) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double vv[3] = {v[3 * i], v[3 * i + 1], v[3 * i + 2]};
+  vel_op(op, i, vv, invm, sc);
+  for (int r = 0; r < 3; ++r) v[3 * i + r] = vv[r];
+}
+
+// Velocity update then RATTLE in one launch: threads [0, ncl) take one constraint cluster each (its atoms' update, then
+// the relative velocity along each constraint removed, core/src/constraints.cpp:232-269); threads [ncl, ncl + nfree)
+// update one unconstrained atom each. With h > 0 the impulses are read as forces over a half kick and their virial
+// (xx yy zz xy xz yz) is added to sc[kScCW0..].
+__global__ void k_vel_rattle(ConsArgs C, int nfree, const int* __restrict__ free_atoms, const double* __restrict__ x, double* __restrict__ v, VelOp op,
+                             double h, double* sc, int* counters) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   double w[6] = {0, 0, 0, 0, 0, 0};
+  if (c >= C.ncl && c < C.ncl + nfree) {
+    const int g = free_atoms[c - C.ncl];
+    double vv[3] = {v[3 * g], v[3 * g + 1], v[3 * g + 2]};
+    vel_op(op, g, vv, C.invm, sc);
+    for (int r = 0; r < 3; ++r) v[3 * g + r] = vv[r];
+  }
   if (c < C.ncl) {
     const int k0 = C.cl_start[c], k1 = C.cl_start[c + 1], a0 = C.cl_atom0[c], a1 = C.cl_atom0[c + 1];
     const int na = a1 - a0, nk = k1 - k0;
@@ -190,6 +234,7 @@ __global__ void k_rattle(ConsArgs C, const double* __restrict__ x, double* __res
     for (int a = 0; a < na; ++a) {
       const int g = C.cl_atoms[a0 + a];
       for (int r = 0; r < 3; ++r) pv[a][r] = v[3 * g + r];
+      vel_op(op, g, pv[a], C.invm, sc);
       im[a] = C.invm[g];
     }
     double rr[kMaxClCons][3], lam[kMaxClCons], dd[kMaxClCons];
@@ -244,43 +289,6 @@ __global__ void k_rattle(ConsArgs C, const double* __restrict__ x, double* __res
   }
 }
 
-// Kinetic energy (and, when asked, the kinetic tensor sum m v_a v_b / kAcc) into partials per block.
-__global__ void k_ke_partial(int n, const double* __restrict__ v, const double* __restrict__ m, double* __restrict__ part, int tensor) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double e = 0, t[6] = {0, 0, 0, 0, 0, 0};
-  if (i < n) {
-    const double vx = v[3 * i], vy = v[3 * i + 1], vz = v[3 * i + 2], mi = m[i];
-    e = mi * (vx * vx + vy * vy + vz * vz);
-    if (tensor) t[0] = mi * vx * vx, t[1] = mi * vy * vy, t[2] = mi * vz * vz, t[3] = mi * vx * vy, t[4] = mi * vx * vz, t[5] = mi * vy * vz;
-  }
-  __shared__ double scratch[32];
-  const double s = block_sum(e, scratch);
-  if (threadIdx.x == 0) part[blockIdx.x * 7] = s;
-  if (tensor)
-    for (int q = 0; q < 6; ++q) {
-      const double st = block_sum(t[q], scratch);
-      if (threadIdx.x == 0) part[blockIdx.x * 7 + 1 + q] = st;
-    }
-}
-
-// Sums the partials in block order (deterministic) into sc[slot] = 0.5 sum / kAcc, and the tensor into kScKin0.
-__global__ void k_ke_final(int nparts, const double* __restrict__ part, double* sc, int slot, int tensor) {
-  double e = 0, t[6] = {0, 0, 0, 0, 0, 0};
-  for (int b = threadIdx.x; b < nparts; b += blockDim.x) {
-    e += part[7 * b];
-    if (tensor)
-      for (int q = 0; q < 6; ++q) t[q] += part[7 * b + 1 + q];
-  }
-  __shared__ double scratch[32];
-  const double s = block_sum(e, scratch);
-  if (threadIdx.x == 0) sc[slot] = 0.5 * s / kAcc;
-  if (tensor)
-    for (int q = 0; q < 6; ++q) {
-      const double st = block_sum(t[q], scratch);
-      if (threadIdx.x == 0) sc[kScKin0 + q] = st / kAcc;
-    }
-}
-
 __global__ void k_scale_v(int n, double* __restrict__ v, const double* __restrict__ sc) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= 3 * n) return;
@@ -288,17 +296,18 @@ __global__ void k_scale_v(int n, double* __restrict__ v, const double* __restric
 }
 
 // The step counter and the thermostat target: T ramps linearly from t0 to t1 over `steps` when t1 >= 0.
-__global__ void k_step_begin(double* sc, double t0, double t1, long long steps, double ndof) {
+__device__ void step_begin_body(double* sc, double t0, double t1, long long steps, double ndof) {
   const double step = sc[kScStep] + 1;
   sc[kScStep] = step;
   const double t = (t1 >= 0 && steps > 0) ? t0 + (t1 - t0) * step / double(steps) : t0;
   sc[kScTnow] = t;
   sc[kScKtarget] = 0.5 * ndof * kB * t;
 }
+__global__ void k_step_begin(double* sc, double t0, double t1, long long steps, double ndof) { step_begin_body(sc, t0, t1, steps, ndof); }
 
 // Nose-Hoover chain over half a step (LAMMPS FixNH::nhc_temp_integrate, as dynamics.cpp:479-508): sets the velocity
 // factor in sc[kScFactor]; the caller scales v by it.
-__global__ void k_nhc(Chain* ch, double* sc, double ndof, double t_freq, double dt) {
+__device__ void nhc_body(Chain* ch, double* sc, double ndof, double t_freq, double dt) {
   const double dthalf = 0.5 * dt, dt4 = 0.25 * dt, dt8 = 0.125 * dt;
   const double tt = sc[kScTnow], kt = kB * tt, ke_target = ndof * kt;
   Chain& c = *ch;
@@ -329,7 +338,7 @@ __global__ void k_nhc(Chain* ch, double* sc, double ndof, double t_freq, double 
 
 // Bussi velocity rescaling (Bussi, Donadio & Parrinello 2007, appendix; dynamics.cpp:466-477) from this step's draws
 // (r1, sum of ndof - 1 squared normals) read from the host-made table.
-__global__ void k_bussi(double* sc, const double2* __restrict__ draws, long long first_step, double h, double tau, double ndof) {
+__device__ void bussi_body(double* sc, const double2* __restrict__ draws, long long first_step, double h, double tau, double ndof) {
   const double k = sc[kScKE];
   const long long step = (long long)sc[kScStep];
   if (k <= 0) {
@@ -344,22 +353,76 @@ __global__ void k_bussi(double* sc, const double2* __restrict__ draws, long long
   sc[kScBath] -= knew - k;
 }
 
-// Langevin O step: v = c1 v + c2 sqrt(kB T kAcc / m) N(0, 1), Philox normals keyed by (seed, step, atom)
-__global__ void k_langevin_o(int n, double* __restrict__ v, const double* __restrict__ invm, const double* __restrict__ sc, double c1, double c2,
-                             uint64_t seed) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const uint64_t step = (uint64_t)sc[kScStep];
-  double z[4];
-  normals4(seed, step, uint32_t(i), 0x4C414E47u, z);
-  const double sd = sqrt(kB * sc[kScTnow] * kAcc * invm[i]);
-  for (int r = 0; r < 3; ++r) v[3 * i + r] = c1 * v[3 * i + r] + c2 * sd * z[r];
-}
+// What the last block of k_ke does with the fresh kinetic energy.
+enum KeThen { kThenNone = 0, kThenNhc, kThenBussi, kThenBath };
+struct KeArgs {
+  int n;
+  const double* v;
+  const double* m;
+  double* part;          // 7 per block
+  unsigned* done;        // blocks finished; the last block resets it
+  double* sc;
+  int slot;              // sc slot receiving 0.5 sum m v^2 / kAcc
+  int tensor;            // also the kinetic tensor into kScKin0..
+  int begin;             // run the step-begin update first
+  int then;              // KeThen
+  double t0, t1, ndof;
+  long long steps;
+  Chain* chain;
+  double t_freq, dt;
+  const double2* draws;
+  long long draws_first;
+  double tau;
+};
 
-// bath -= KE(after) - KE(before)
-__global__ void k_bath_update(double* sc) { sc[kScBath] -= sc[kScKE] - sc[kScKE0]; }
-__global__ void k_zero_cw(double* sc) {
-  for (int q = 0; q < 6; ++q) sc[kScCW0 + q] = 0;
+// Kinetic energy (and the kinetic tensor sum m v_a v_b / kAcc on request), then a thermostat update, in one launch:
+// each block writes its partial sums; the last block to finish adds the partials in block order (deterministic) and
+// runs the scalar update. No block waits on another.
+__global__ void k_ke(KeArgs A) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0, t[6] = {0, 0, 0, 0, 0, 0};
+  if (i < A.n) {
+    const double vx = A.v[3 * i], vy = A.v[3 * i + 1], vz = A.v[3 * i + 2], mi = A.m[i];
+    e = mi * (vx * vx + vy * vy + vz * vz);
+    if (A.tensor) t[0] = mi * vx * vx, t[1] = mi * vy * vy, t[2] = mi * vz * vz, t[3] = mi * vx * vy, t[4] = mi * vx * vz, t[5] = mi * vy * vz;
+  }
+  __shared__ double scratch[32];
+  __shared__ bool last;
+  const double s = block_sum(e, scratch);
+  if (threadIdx.x == 0) A.part[blockIdx.x * 7] = s;
+  if (A.tensor)
+    for (int q = 0; q < 6; ++q) {
+      const double st = block_sum(t[q], scratch);
+      if (threadIdx.x == 0) A.part[blockIdx.x * 7 + 1 + q] = st;
+    }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(A.done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  e = 0;
+  for (int q = 0; q < 6; ++q) t[q] = 0;
+  for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+    e += __ldcg(A.part + 7 * b);
+    if (A.tensor)
+      for (int q = 0; q < 6; ++q) t[q] += __ldcg(A.part + 7 * b + 1 + q);
+  }
+  const double tot = block_sum(e, scratch);
+  double tt[6];
+  if (A.tensor)
+    for (int q = 0; q < 6; ++q) tt[q] = block_sum(t[q], scratch);
+  if (threadIdx.x != 0) return;
+  *A.done = 0;
+  double* sc = A.sc;
+  sc[A.slot] = 0.5 * tot / kAcc;
+  if (A.tensor)
+    for (int q = 0; q < 6; ++q) sc[kScKin0 + q] = tt[q] / kAcc;
+  if (A.begin) step_begin_body(sc, A.t0, A.t1, A.steps, A.ndof);
+  if (A.then == kThenNhc) nhc_body(A.chain, sc, A.ndof, A.t_freq, A.dt);
+  else if (A.then == kThenBussi) bussi_body(sc, A.draws, A.draws_first, A.dt, A.tau, A.ndof);
+  else if (A.then == kThenBath) sc[kScBath] -= sc[kScKE] - sc[kScKE0];
 }
 
 }  // namespace
@@ -370,6 +433,9 @@ struct Stepper {
   const caps_gpu_md_opts& o;
   int n;
   DevBuf<double> x, v, x0, invm, m, sc, part;
+  DevBuf<unsigned> done;       // k_ke's finished-block counter
+  DevBuf<int> free_atoms;      // atoms in no constraint cluster
+  int nfree = 0;
   DevBuf<Chain> chain;
   DevBuf<int> cl_start, cl_atom0, cl_atoms;
   DevBuf<int4> cons;
@@ -384,12 +450,13 @@ struct Stepper {
   std::unique_ptr<HostRng> rng;
   double* h_sc = nullptr;
   Chain* h_chain = nullptr;
-  cudaGraphExec_t graph = nullptr;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};   // the captured plain step and thermo step (energies and virial on)
+  int graph_kernels[2] = {0, 0};
   int nparts = 0;
 
   Stepper(Engine& e, const caps_gpu_md_opts& md) : E(e), o(md), n(e.n_) {}
   ~Stepper() {
-    if (graph) cudaGraphExecDestroy(graph);
+    drop_graphs();
     if (h_sc) cudaFreeHost(h_sc);
     if (h_chain) cudaFreeHost(h_chain);
   }
@@ -478,6 +545,13 @@ struct Stepper {
       st.push_back(int(cv.size()));
       a0.push_back(int(atoms.size()));
     }
+    std::vector<char> in_cluster(static_cast<size_t>(n), 0);
+    for (int a : atoms) in_cluster[size_t(a)] = 1;
+    std::vector<int> fa;
+    for (int a = 0; a < n; ++a)
+      if (!in_cluster[size_t(a)]) fa.push_back(a);
+    nfree = int(fa.size());
+    if (nfree) free_atoms.upload(fa, E.stream_);
     cl_start.upload(st, E.stream_);
     cl_atom0.upload(a0, E.stream_);
     cl_atoms.upload(atoms, E.stream_);
@@ -503,63 +577,126 @@ struct Stepper {
     for (int r = 0; r < 3; ++r) d[r] = c.h[r][0] * f[0] + c.h[r][1] * f[1] + c.h[r][2] * f[2];
   }
 
+  void drop_graphs() {
+    for (auto& g : graph)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
+  }
+
+  // Replays the step graph (capturing it on first use). Returns its kernel count.
+  int launch_step(bool thermo) {
+    const int k = thermo ? 1 : 0;
+    if (!graph[k]) {
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(E.stream_, cudaStreamCaptureModeThreadLocal));
+      step(thermo, thermo);
+      CK(cudaStreamEndCapture(E.stream_, &g));
+      size_t nn = 0;
+      CK(cudaGraphGetNodes(g, nullptr, &nn));
+      std::vector<cudaGraphNode_t> nodes(nn);
+      CK(cudaGraphGetNodes(g, nodes.data(), &nn));
+      int kernels = 0;
+      for (auto nd : nodes) {
+        cudaGraphNodeType ty;
+        CK(cudaGraphNodeGetType(nd, &ty));
+        kernels += ty == cudaGraphNodeTypeKernel;
+      }
+      graph_kernels[k] = kernels;
+      if (k == 0) E.graph_kernels_ = kernels;
+      CK(cudaGraphInstantiate(&graph[k], g, cudaGraphInstantiateFlagUseNodePriority));
+      CK(cudaGraphDestroy(g));
+    }
+    CK(cudaGraphLaunch(graph[k], E.stream_));
+    return graph_kernels[k];
+  }
+
   // --- step pieces (all asynchronous on E.stream_) ---
-  void ke(int slot, bool tensor) {
-    k_ke_partial<<<nparts, 256, 0, E.stream_>>>(n, v.p, m.p, part.p, tensor ? 1 : 0);
-    k_ke_final<<<1, 256, 0, E.stream_>>>(nparts, part.p, sc.p, slot, tensor ? 1 : 0);
+  KeArgs ke_args(int slot, bool tensor) const {
+    KeArgs A{};
+    A.n = n;
+    A.v = v.p;
+    A.m = m.p;
+    A.part = part.p;
+    A.done = done.p;
+    A.sc = sc.p;
+    A.slot = slot;
+    A.tensor = tensor ? 1 : 0;
+    A.t0 = o.temperature;
+    A.t1 = o.temperature_end;
+    A.steps = (long long)o.steps;
+    A.ndof = ndof;
+    A.chain = chain.p;
+    A.t_freq = t_freq;
+    A.dt = o.dt;
+    A.draws = draws.p;
+    A.draws_first = draws_first;
+    A.tau = o.tau_t;
+    return A;
   }
-  void kick(double h) { k_kick<<<blocks(size_t(n), 256), 256, 0, E.stream_>>>(n, v.p, E.d_f_.p, invm.p, h); }
-  void drift(double h) {
-    k_drift<<<blocks(size_t(3) * n, 256), 256, 0, E.stream_>>>(n, x.p, v.p, x0.p, h, E.d_counters_.p);
-    if (ncons) k_shake<<<blocks(size_t(C.ncl), 128), 128, 0, E.stream_>>>(C, x.p, x0.p, v.p, h, E.d_counters_.p);
+  void ke_launch(const KeArgs& A) { k_ke<<<nparts, 256, 0, E.stream_>>>(A); }
+  void ke(int slot, bool tensor) { ke_launch(ke_args(slot, tensor)); }
+  // half kick, then drift with SHAKE; `scale` applies the thermostat's pending factor first
+  void kick_drift(double hk, double hd, bool scale, bool zero_cw) {
+    k_kick_drift<<<blocks(size_t(n), 256), 256, 0, E.stream_>>>(n, x.p, v.p, x0.p, E.d_f_.p, invm.p, hk, hd, sc.p, scale ? 1 : 0, zero_cw ? 1 : 0,
+                                                                 E.d_counters_.p);
+    if (ncons) k_shake<<<blocks(size_t(C.ncl), 128), 128, 0, E.stream_>>>(C, x.p, x0.p, v.p, hd, E.d_counters_.p);
   }
-  void rattle(double h) {
-    if (!ncons) return;
-    if (h > 0) k_zero_cw<<<1, 1, 0, E.stream_>>>(sc.p);
-    k_rattle<<<blocks(size_t(C.ncl), 128), 128, 0, E.stream_>>>(C, x.p, v.p, h, sc.p, E.d_counters_.p);
+  // a velocity update, then RATTLE (constraint virial summed when h > 0)
+  void vel_rattle(const VelOp& op, double h) {
+    if (!ncons) {
+      if (op.kind != 0) k_vel<<<blocks(size_t(n), 256), 256, 0, E.stream_>>>(n, v.p, invm.p, sc.p, op);
+      return;
+    }
+    k_vel_rattle<<<blocks(size_t(C.ncl + nfree), 128), 128, 0, E.stream_>>>(C, nfree, free_atoms.p, x.p, v.p, op, h, sc.p, E.d_counters_.p);
+  }
+  VelOp kick_op(double hk) const { return VelOp{1, E.d_f_.p, hk, 0, 0, 0}; }
+  void rattle(double h) {   // RATTLE alone (initial velocities)
+    if (ncons) vel_rattle(VelOp{0, nullptr, 0, 0, 0, 0}, h);
   }
   void scale_v() { k_scale_v<<<blocks(size_t(3) * n, 256), 256, 0, E.stream_>>>(n, v.p, sc.p); }
-  void nhc_half(double dt) {
-    ke(kScKE, false);
-    k_nhc<<<1, 1, 0, E.stream_>>>(chain.p, sc.p, ndof, t_freq, dt);
-    scale_v();
-  }
   void forces(bool ener, bool vir) { E.forces(x.p, ener, vir, true); }
 
-  // One MD step (dynamics.cpp:606-666), energies and virial on request.
+  // One MD step (dynamics.cpp:606-666), energies and virial on request. Kernel sequence per step: NVT Nose-Hoover
+  // KE+chain, kick+drift, SHAKE, forces, kick+RATTLE, KE+chain, scale; Bussi step-begin, kick+drift, SHAKE, forces,
+  // kick+RATTLE, KE+Bussi, scale; Langevin (BAOAB) kick+drift, SHAKE, KE, O+RATTLE, KE+bath, drift, SHAKE, forces,
+  // kick+RATTLE.
   void step(bool ener, bool vir) {
     const double dt = o.dt;
-    k_step_begin<<<1, 1, 0, E.stream_>>>(sc.p, o.temperature, o.temperature_end, (long long)o.steps, ndof);
     if (langevin) {
       const double c1 = std::exp(-dt / std::max(o.tau_t, 1e-9)), c2 = std::sqrt(1 - c1 * c1);
-      kick(0.5 * dt);
-      drift(0.5 * dt);
-      ke(kScKE0, false);
-      k_langevin_o<<<blocks(size_t(n), 256), 256, 0, E.stream_>>>(n, v.p, invm.p, sc.p, c1, c2, o.seed);
-      rattle(0);
-      ke(kScKE, false);
-      k_bath_update<<<1, 1, 0, E.stream_>>>(sc.p);
-      drift(0.5 * dt);
+      kick_drift(0.5 * dt, 0.5 * dt, false, true);
+      KeArgs A = ke_args(kScKE0, false);
+      A.begin = 1;
+      ke_launch(A);
+      vel_rattle(VelOp{2, nullptr, 0, c1, c2, o.seed}, 0);
+      A = ke_args(kScKE, false);
+      A.then = kThenBath;
+      ke_launch(A);
+      kick_drift(0, 0.5 * dt, false, false);
       forces(ener, vir);
-      kick(0.5 * dt);
-      rattle(dt);
+      vel_rattle(kick_op(0.5 * dt), dt);
     } else if (nhc) {
-      nhc_half(dt);
-      kick(0.5 * dt);
-      drift(dt);
+      KeArgs A = ke_args(kScKE, false);
+      A.begin = 1;
+      A.then = kThenNhc;
+      ke_launch(A);
+      kick_drift(0.5 * dt, dt, true, true);
       forces(ener, vir);
-      kick(0.5 * dt);
-      rattle(dt);
-      nhc_half(dt);
+      vel_rattle(kick_op(0.5 * dt), dt);
+      A.begin = 0;
+      ke_launch(A);
+      scale_v();
     } else {
-      kick(0.5 * dt);
-      drift(dt);
+      k_step_begin<<<1, 1, 0, E.stream_>>>(sc.p, o.temperature, o.temperature_end, (long long)o.steps, ndof);
+      kick_drift(0.5 * dt, dt, false, true);
       forces(ener, vir);
-      kick(0.5 * dt);
-      rattle(dt);
+      vel_rattle(kick_op(0.5 * dt), dt);
       if (bussi) {
-        ke(kScKE, false);
-        k_bussi<<<1, 1, 0, E.stream_>>>(sc.p, draws.p, draws_first, dt, o.tau_t, ndof);
+        KeArgs A = ke_args(kScKE, false);
+        A.then = kThenBussi;
+        ke_launch(A);
         scale_v();
       }
     }
@@ -580,6 +717,7 @@ struct Stepper {
 };
 
 void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progress_fn progress, caps_gpu_frame_fn frame, void* user, std::string* report) {
+  const auto t_enter = std::chrono::steady_clock::now();
   const caps_gpu_md_opts& o = *md;
   if (n_ < 2) throw ModelError(CAPS_GPU_EFIELD, "dynamics needs at least two atoms");
   if (o.dt <= 0 || o.dt > 50) throw ModelError(CAPS_GPU_EINVAL, "time step must be in (0, 50] fs");
@@ -604,6 +742,8 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
   CK(cudaMemsetAsync(S.chain.p, 0, sizeof(Chain), stream_));
   S.nparts = blocks(size_t(n_), 256);
   S.part.alloc(size_t(7) * S.nparts);
+  S.done.alloc(1);
+  S.done.zero(stream_);
   CK(cudaMallocHost(&S.h_sc, sizeof(double) * kScNum));
   CK(cudaMallocHost(&S.h_chain, sizeof(Chain)));
   S.nhc = o.thermostat == 3;
@@ -721,10 +861,8 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
     vs.alloc(n3);
     CK(cudaMemcpyAsync(xs.p, S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     CK(cudaMemcpyAsync(vs.p, S.v.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
-    S.kick(0.5 * o.dt);
-    S.drift(o.dt);
-    S.kick(0.5 * o.dt);
-    S.rattle(o.dt);
+    S.kick_drift(0.5 * o.dt, o.dt, false, true);
+    S.vel_rattle(S.kick_op(0.5 * o.dt), o.dt);
     CK(cudaMemcpyAsync(S.x.p, xs.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     CK(cudaMemcpyAsync(S.v.p, vs.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     CK(cudaStreamSynchronize(stream_));
@@ -752,7 +890,7 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
   }
   const auto w0 = std::chrono::steady_clock::now();
   CK(cudaEventRecord(ev0, stream_));
-  bool have_graph = false;
+  long long kernels = 0, emits = 0, baro_steps = 0;
   for (long long s = 1; s <= o.steps; ++s) {
     if (timed) {
       if (timing_flush_ > 0) CK(cudaMemsetAsync(d_flush_.p, int(s & 255), size_t(timing_flush_), stream_));
@@ -769,39 +907,16 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
     if (S.bussi && s - S.draws_first >= S.draws_count) {
       CK(cudaStreamSynchronize(stream_));
       S.make_draws(s, std::min<long long>(o.steps - s + 1, 4096));
-      if (S.graph) {
-        cudaGraphExecDestroy(S.graph);
-        S.graph = nullptr;
-        have_graph = false;
-      }
-    }
-    if (!special(s)) {
-      if (!have_graph) {
-        cudaGraph_t g;
-        CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-        S.step(false, false);
-        CK(cudaStreamEndCapture(stream_, &g));
-        size_t nn = 0;
-        CK(cudaGraphGetNodes(g, nullptr, &nn));
-        std::vector<cudaGraphNode_t> nodes(nn);
-        CK(cudaGraphGetNodes(g, nodes.data(), &nn));
-        int kernels = 0;
-        for (auto nd : nodes) {
-          cudaGraphNodeType ty;
-          CK(cudaGraphNodeGetType(nd, &ty));
-          kernels += ty == cudaGraphNodeTypeKernel;
-        }
-        graph_kernels_ = kernels;
-        CK(cudaGraphInstantiate(&S.graph, g, 0));
-        CK(cudaGraphDestroy(g));
-        have_graph = true;
-      }
-      CK(cudaGraphLaunch(S.graph, stream_));
-      continue;
+      S.drop_graphs();   // the draw table's first step is a parameter of the captured thermostat kernel
     }
     const bool baro = o.barostat && s % baro_every == 0;
-    S.step(true, true);
+    if (!baro) {
+      kernels += S.launch_step(special(s));
+      if (!special(s)) continue;
+    }
     if (baro) {
+      S.step(true, true);
+      ++baro_steps;
       // stochastic cell rescaling (Bernetti & Bussi 2020, dynamics.cpp:684-723), isotropic
       S.ke(kScKE, true);
       sync_scalars();
@@ -841,17 +956,17 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
         S.rattle(0);
       }
       S.forces(true, true);
-      if (S.graph) {
-        cudaGraphExecDestroy(S.graph);
-        S.graph = nullptr;
-        have_graph = false;
-      }
+      S.drop_graphs();   // the cell is a parameter of the captured kernels
     }
-    if (s % thermo_every == 0 || s == o.steps) emit(s);
+    if (s % thermo_every == 0 || s == o.steps) {
+      emit(s);
+      ++emits;
+    }
     if (o.frame_every > 0 && (s % o.frame_every == 0 || s == o.steps)) emit_frame(s);
   }
   CK(cudaEventRecord(ev1, stream_));
   CK(cudaEventSynchronize(ev1));
+  kernels_run_ = kernels + emits + baro_steps * S.graph_kernels[1];
   float ms = 0;
   CK(cudaEventElapsedTime(&ms, ev0, ev1));
   if (timed && o.steps > 0) {
@@ -878,8 +993,10 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
   if (report) {
     char b[400];
     const double nsday = wall > 0 ? double(o.steps) * o.dt * 1e-6 / wall * 86400 : 0.0;
-    std::snprintf(b, sizeof b, "%lld steps of %.2f fs in %.3f s (device %.3f s) · %.2f ns/day · %d constraints · %.0f degrees of freedom · %s",
-                  (long long)o.steps, o.dt, wall, ms * 1e-3, nsday, S.ncons, S.ndof, mixed_ ? "mixed FP32/fixed-point" : "FP64");
+    const double setup = std::chrono::duration<double>(w0 - t_enter).count();
+    std::snprintf(b, sizeof b,
+                  "%lld steps of %.2f fs in %.3f s (device %.3f s, set-up %.3f s) · %.2f ns/day · %d constraints · %.0f degrees of freedom · %s",
+                  (long long)o.steps, o.dt, wall, ms * 1e-3, setup, nsday, S.ncons, S.ndof, mixed_ ? "mixed FP32/fixed-point" : "FP64");
     *report = b;
   }
 }

@@ -41,7 +41,9 @@ struct ListBufs {
   // per slot
   int* perm;
   // list
-  uint4* ent;         // x cj, y imask | image << 8, z mask index + 1, w the pruned imask (the pair kernels read w)
+  // x cj, y imask | image << 8, z mask index + 1, w the pruned masks the pair kernels read: bit c when j atoms 0-3
+  // (the cluster's lower-x half) come within the prune radius of i cluster c, bit 8 + c for j atoms 4-7
+  uint4* ent;
   float4* ent_shift;  // org(sc_j) + S - org(sc_i), for the FP32 kernel
   unsigned long long* masks;   // 8 per masked entry
   int4* work;         // x sc, y first entry, z count
@@ -51,7 +53,8 @@ struct ListBufs {
   int* counters;
 };
 
-enum Counter { kCntEnt = 0, kCntWork, kCntMask, kCntErr, kCntRebuild, kCntNsc, kCntMaxCol, kCntPrune, kCntNum = 8 };
+// Device counters: list sizes, the error word, the rebuild and prune flags, and running counts of builds and prunes.
+enum Counter { kCntEnt = 0, kCntWork, kCntMask, kCntErr, kCntRebuild, kCntNsc, kCntMaxCol, kCntPrune, kCntBuilds, kCntPrunes, kCntNum = 10 };
 
 __device__ __forceinline__ void raise_error(int* counters, unsigned bit) { atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), bit); }
 

@@ -42,7 +42,10 @@ static __global__ void k_end_build(int n, const double* __restrict__ x, double* 
   if (build_off(counters)) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < 3 * n) x0[i] = x[i];
-  if (i == 0) counters[kCntPrune] = 1;
+  if (i == 0) {
+    counters[kCntPrune] = 1;
+    counters[kCntBuilds] += 1;
+  }
 }
 static __global__ void k_lower_flag(int* counters) { counters[kCntRebuild] = 0; }
 
@@ -64,7 +67,10 @@ static __global__ void k_bin(int n, const double* __restrict__ x, DevCell cell, 
   const int cu = min(g.nu - 1, int(b.frac[3 * i] * g.nu)), cv = min(g.nv - 1, int(b.frac[3 * i + 1] * g.nv));
   const int c = cu * g.nv + cv;
   b.col[i] = c;
-  atomicAdd(b.col_count + c, 1);
+  // one atomic per distinct column in the warp (a column holds hundreds of atoms: the adds would contend)
+  const unsigned act = __activemask();
+  const unsigned same = __match_any_sync(act, c);
+  if ((threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(b.col_count + c, __popc(same));
 }
 
 // K-SCAN (one block): column starts, super-cluster starts (64 atoms each, the last one of a column partial), and the
@@ -125,7 +131,14 @@ static __global__ void k_scatter(int n, ListBufs b) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int c = b.col[i];
-  b.order[b.col_start[c] + atomicAdd(b.col_fill + c, 1)] = i;
+  // warp-aggregated: the lowest lane of each column group reserves the group's places
+  const unsigned act = __activemask();
+  const unsigned same = __match_any_sync(act, c);
+  const int lane = threadIdx.x & 31, leader = __ffs(same) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(b.col_fill + c, __popc(same));
+  base = __shfl_sync(same, base, leader);
+  b.order[b.col_start[c] + base + __popc(same & ((1u << lane) - 1))] = i;
 }
 
 // K-SORT (block per column): atoms by fractional c, ties by index (a rank sort in shared memory).
@@ -145,12 +158,16 @@ static __global__ void k_sort_columns(ListGeom g, ListBufs b) {
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
       const double kk = key[k];
       const int ik = id[k];
-      int rank = 0;
-      for (int u = 0; u < n; ++u) {
-        const double ku = key[u];
-        rank += (ku < kk) || (ku == kk && id[u] < ik);
+      int r0 = 0, r1 = 0, r2 = 0, r3 = 0;   // four independent counts: the loop is latency-bound otherwise
+      int u = 0;
+      for (; u + 4 <= n; u += 4) {
+        r0 += (key[u] < kk) || (key[u] == kk && id[u] < ik);
+        r1 += (key[u + 1] < kk) || (key[u + 1] == kk && id[u + 1] < ik);
+        r2 += (key[u + 2] < kk) || (key[u + 2] == kk && id[u + 2] < ik);
+        r3 += (key[u + 3] < kk) || (key[u + 3] == kk && id[u + 3] < ik);
       }
-      b.order[s0 + rank] = ik;
+      for (; u < n; ++u) r0 += (key[u] < kk) || (key[u] == kk && id[u] < ik);
+      b.order[s0 + r0 + r1 + r2 + r3] = ik;
     }
     __syncthreads();
   }
@@ -234,19 +251,24 @@ static __global__ void k_superclusters(DevCell cell, ListBufs b) {
 }
 
 // ---------------------------------------------------------------------------------------------------------------
-// K-SEARCH (warp per super-cluster). Exclusions (ForceField::excluded) hold at their nearest image only
-// (core/src/nbnxm.cpp:229-252): each of the super-cluster's excluded atom pairs is recorded with the image that is
-// nearest at the build, and an entry for that j cluster under that image carries masks with those pairs cleared.
-struct SearchShared {
-  uint2 rec[kExclRecMax];                 // x: j cluster, y: i local (6 bits) | j in cluster (3) << 6 | image << 9
-  unsigned long long key[kExclHash];      // distinct (j cluster, image) of the records; ~0 empty
+constexpr int kSearchWarps = 4;       // warps per super-cluster in the search
+
+// One warp's batch of entries in the making.
+struct SearchBatch {
   uint4 ent[2 * kBatch];
   float4 sh[2 * kBatch];
   unsigned char needs_mask[2 * kBatch];
   unsigned long long m[kBatch][8];
+  int nent;
+};
+
+struct SearchShared {
+  uint2 rec[kExclRecMax];                 // x: j cluster, y: i local (6 bits) | j in cluster (3) << 6 | image << 9
+  unsigned long long key[kExclHash];      // distinct (j cluster, image) of the records; ~0 empty
   double ibox[8][6];
   double org_i[3];
-  int nrec, nent;
+  int nrec;
+  SearchBatch batch[kSearchWarps];
 };
 
 __device__ __forceinline__ unsigned long long excl_key(unsigned cj, unsigned img) { return (unsigned long long)cj | ((unsigned long long)img << 32); }
@@ -272,15 +294,15 @@ static __device__ void key_insert(SearchShared& S, unsigned long long key, int* 
   raise_error(counters, kErrExclOverflow);
 }
 
-// Writes the batch [0, cnt) of S.ent as one work item (the masks of entries that need them first).
-static __device__ void flush_batch(SearchShared& S, int sc, int cnt, int lane, const ListBufs& b) {
+// Writes the batch [0, cnt) of B as one work item (the masks of entries that need them first).
+static __device__ void flush_batch(const SearchShared& S, SearchBatch& B, int sc, int cnt, int lane, const ListBufs& b) {
   if (cnt <= 0) return;
   // masks for the entries that need them: start from all pairs, drop exclusions and the lower triangle of a cluster
   // with itself under the zero image
   for (int e = 0; e < cnt; ++e) {
-    if (!S.needs_mask[e]) continue;
-    const unsigned cj = S.ent[e].x;
-    const unsigned img = (S.ent[e].y >> 8) & 0x1FFFFFu;
+    if (!B.needs_mask[e]) continue;
+    const unsigned cj = B.ent[e].x;
+    const unsigned img = (B.ent[e].y >> 8) & 0x1FFFFFu;
     if (lane < 8) {
       unsigned long long mm = ~0ull;
       if (cj == unsigned(8 * sc + lane) && img == pack_image(0, 0, 0)) {
@@ -289,14 +311,14 @@ static __device__ void flush_batch(SearchShared& S, int sc, int cnt, int lane, c
         for (int i = 0; i < 8; ++i)
           for (int j = i + 1; j < 8; ++j) mm |= 1ull << (8 * i + j);
       }
-      S.m[e][lane] = mm;
+      B.m[e][lane] = mm;
     }
     __syncwarp();
     for (int r = lane; r < S.nrec; r += 32) {
       const uint2 rc = S.rec[r];
       if (rc.x != cj || (rc.y >> 9) != img) continue;
       const unsigned il = rc.y & 63u, jl = (rc.y >> 6) & 7u;
-      atomicAnd(&S.m[e][il >> 3], ~(1ull << (8 * (il & 7) + jl)));
+      atomicAnd(&B.m[e][il >> 3], ~(1ull << (8 * (il & 7) + jl)));
     }
     __syncwarp();
   }
@@ -312,39 +334,46 @@ static __device__ void flush_batch(SearchShared& S, int sc, int cnt, int lane, c
     return;
   }
   for (int e = lane; e < cnt; e += 32) {
-    uint4 en = S.ent[e];
-    en.w = en.y & 255u;   // unpruned until the first prune
-    if (S.needs_mask[e]) {
+    uint4 en = B.ent[e];
+    en.w = (en.y & 255u) * 0x101u;   // unpruned until the first prune: both halves of every listed i cluster
+    if (B.needs_mask[e]) {
       const int mi = atomicAdd(b.counters + kCntMask, 1);
       if (mi < b.mask_cap) {
-        for (int k = 0; k < 8; ++k) b.masks[8 * size_t(mi) + k] = S.m[e][k];
+        for (int k = 0; k < 8; ++k) b.masks[8 * size_t(mi) + k] = B.m[e][k];
         en.z = unsigned(mi + 1);
       } else {
         raise_error(b.counters, kErrMaskOverflow);
       }
     }
     b.ent[base + e] = en;
-    b.ent_shift[base + e] = S.sh[e];
+    b.ent_shift[base + e] = B.sh[e];
   }
   if (lane == 0) b.work[wi] = make_int4(sc, base, cnt, 0);
 }
 
-static __global__ void __launch_bounds__(32) k_search(DevCell cell, ListGeom g, const uint32_t* __restrict__ excl_off, const uint32_t* __restrict__ excl_list,
-                                               ListBufs b) {
+// K-SEARCH: one block of kSearchWarps warps per super-cluster. The block records the super-cluster's excluded pairs;
+// then each warp takes a quarter of the neighbouring columns (with their images) and batches its own entries.
+// Exclusions (ForceField::excluded) hold at their nearest image only (core/src/nbnxm.cpp:229-252): each of the
+// super-cluster's excluded atom pairs is recorded with the image that is nearest at the build, and an entry for that j
+// cluster under that image carries masks with those pairs cleared.
+static __global__ void __launch_bounds__(32 * kSearchWarps) k_search(DevCell cell, ListGeom g, const uint32_t* __restrict__ excl_off,
+                                                                     const uint32_t* __restrict__ excl_list, ListBufs b) {
   if (build_off(b.counters)) return;
   extern __shared__ unsigned char smem_raw[];
   SearchShared& S = *reinterpret_cast<SearchShared*>(smem_raw);
-  const int lane = threadIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  SearchBatch& B = S.batch[warp];
   const int nsc = min(b.counters[kCntNsc], b.nsc_cap);
   for (int sc = blockIdx.x; sc < nsc; sc += gridDim.x) {
-    // --- the super-cluster's boxes and exclusion records
-    for (int t = lane; t < kExclHash; t += 32) S.key[t] = ~0ull;
-    if (lane < 8)
-      for (int r = 0; r < 6; ++r) S.ibox[lane][r] = b.cl_box[6 * (8 * sc + lane) + r];
-    if (lane < 3) S.org_i[lane] = b.sc_org[3 * sc + lane];
-    if (lane == 0) S.nrec = 0, S.nent = 0;
-    __syncwarp();
-    for (int t = lane; t < 64; t += 32) {
+    // --- the super-cluster's boxes and exclusion records (the whole block)
+    for (int t = threadIdx.x; t < kExclHash; t += blockDim.x) S.key[t] = ~0ull;
+    if (threadIdx.x < 8)
+      for (int r = 0; r < 6; ++r) S.ibox[threadIdx.x][r] = b.cl_box[6 * (8 * sc + threadIdx.x) + r];
+    if (threadIdx.x < 3) S.org_i[threadIdx.x] = b.sc_org[3 * sc + threadIdx.x];
+    if (threadIdx.x == 0) S.nrec = 0;
+    if (lane == 0) B.nent = 0;
+    __syncthreads();
+    for (int t = threadIdx.x; t < 64; t += blockDim.x) {
       const int a = b.perm[64 * sc + t];
       if (a < 0) continue;
       const double* fa = b.frac + 3 * a;
@@ -362,102 +391,105 @@ static __global__ void __launch_bounds__(32) k_search(DevCell cell, ListGeom g, 
         key_insert(S, excl_key(unsigned(sb >> 3), img), b.counters);
       }
     }
-    __syncwarp();
-    if (lane == 0 && S.nrec > kExclRecMax) S.nrec = kExclRecMax;
-    __syncwarp();
-    // --- candidates: neighbouring columns (with their images), super-clusters in c range, their 8 clusters
+    __syncthreads();
+    if (threadIdx.x == 0 && S.nrec > kExclRecMax) S.nrec = kExclRecMax;
+    __syncthreads();
+    // --- candidates: neighbouring columns (with their images), super-clusters in c range, their 8 clusters. Each warp
+    // takes a contiguous block of the columns, so that its entries (and the pair kernel's work items made of them) stay
+    // spatially together.
     const int col = b.sc_col[sc];
     const int cu = col / g.nv, cv = col % g.nv;
     const double zlo = b.sc_z[2 * sc], zhi = b.sc_z[2 * sc + 1];
     const int ci0 = 8 * sc;
-    for (int du = -g.ru; du <= g.ru; ++du) {
+    const int nvw = 2 * g.rv + 1, ncols = (2 * g.ru + 1) * nvw;
+    const int kper = (ncols + kSearchWarps - 1) / kSearchWarps;
+    for (int k = warp * kper; k < min(ncols, (warp + 1) * kper); ++k) {
+      const int du = k / nvw - g.ru, dv = k % nvw - g.rv;
       int U = cu + du;
       const int qa = (int)floor(double(U) / g.nu);
       U -= qa * g.nu;
-      for (int dv = -g.rv; dv <= g.rv; ++dv) {
-        int V = cv + dv;
-        const int qb = (int)floor(double(V) / g.nv);
-        V -= qb * g.nv;
-        const int cc = U * g.nv + V;
-        const int qc0 = max(-g.rq, (int)floor(zlo - g.dw)), qc1 = min(g.rq, (int)floor(zhi + g.dw));
-        for (int qc = qc0; qc <= qc1; ++qc) {
-          const double S0 = cell.h[0][0] * qa + cell.h[0][1] * qb + cell.h[0][2] * qc;
-          const double S1 = cell.h[1][0] * qa + cell.h[1][1] * qb + cell.h[1][2] * qc;
-          const double S2 = cell.h[2][0] * qa + cell.h[2][1] * qb + cell.h[2][2] * qc;
-          const bool zero = qa == 0 && qb == 0 && qc == 0;
-          const bool positive = qa > 0 || (qa == 0 && (qb > 0 || (qb == 0 && qc > 0)));
-          const unsigned img = pack_image(qa, qb, qc);
-          const double lo = zlo - g.dw - qc, hi = zhi + g.dw - qc;
-          // super-clusters of column cc whose c range meets [lo, hi]: their ranges rise along the column
-          int sj = b.col_sc[cc];
-          const int sje = min(b.col_sc[cc + 1], nsc);
-          {
-            int lo_i = sj, hi_i = sje;   // first with z_hi >= lo
-            while (lo_i < hi_i) {
-              const int mid = (lo_i + hi_i) >> 1;
-              if (b.sc_z[2 * mid + 1] < lo) lo_i = mid + 1;
-              else hi_i = mid;
-            }
-            sj = lo_i;
+      int V = cv + dv;
+      const int qb = (int)floor(double(V) / g.nv);
+      V -= qb * g.nv;
+      const int cc = U * g.nv + V;
+      const int qc0 = max(-g.rq, (int)floor(zlo - g.dw)), qc1 = min(g.rq, (int)floor(zhi + g.dw));
+      for (int qc = qc0; qc <= qc1; ++qc) {
+        const double S0 = cell.h[0][0] * qa + cell.h[0][1] * qb + cell.h[0][2] * qc;
+        const double S1 = cell.h[1][0] * qa + cell.h[1][1] * qb + cell.h[1][2] * qc;
+        const double S2 = cell.h[2][0] * qa + cell.h[2][1] * qb + cell.h[2][2] * qc;
+        const bool zero = qa == 0 && qb == 0 && qc == 0;
+        const bool positive = qa > 0 || (qa == 0 && (qb > 0 || (qb == 0 && qc > 0)));
+        const unsigned img = pack_image(qa, qb, qc);
+        const double lo = zlo - g.dw - qc, hi = zhi + g.dw - qc;
+        // super-clusters of column cc whose c range meets [lo, hi]: their ranges rise along the column
+        int sj = b.col_sc[cc];
+        const int sje = min(b.col_sc[cc + 1], nsc);
+        {
+          int lo_i = sj, hi_i = sje;   // first with z_hi >= lo
+          while (lo_i < hi_i) {
+            const int mid = (lo_i + hi_i) >> 1;
+            if (b.sc_z[2 * mid + 1] < lo) lo_i = mid + 1;
+            else hi_i = mid;
           }
-          for (; sj < sje && b.sc_z[2 * sj] <= hi; sj += 4) {
-            // four candidate super-clusters per pass: lane = 8 * which + j cluster
-            const int sjl = sj + (lane >> 3);
-            bool have = false;
-            unsigned imask = 0;
-            int cj = -1;
-            if (sjl < sje && b.sc_z[2 * sjl] <= hi) {
-              cj = 8 * sjl + (lane & 7);
-              const double* bj = b.cl_box + 6 * cj;
-              const double jlo[3] = {bj[0] + S0, bj[1] + S1, bj[2] + S2}, jhi[3] = {bj[3] + S0, bj[4] + S1, bj[5] + S2};
-              for (int c = 0; c < 8; ++c) {
-                const int ci = ci0 + c;
-                // half list: one side of each cluster pair by parity; a cluster with itself under zero or + images
-                bool keep;
-                if (cj != ci) keep = (cj > ci) == (((ci + cj) & 1) == 0);
-                else keep = zero || positive;
-                if (!keep) continue;
-                double d2 = 0;
-                for (int r = 0; r < 3; ++r) {
-                  const double g1 = jlo[r] - S.ibox[c][3 + r], g2 = S.ibox[c][r] - jhi[r];
-                  const double gg = g1 > 0 ? g1 : (g2 > 0 ? g2 : 0.0);
-                  d2 += gg * gg;
-                }
-                if (d2 < g.rlist2) imask |= 1u << c;
+          sj = lo_i;
+        }
+        for (; sj < sje && b.sc_z[2 * sj] <= hi; sj += 4) {
+          // four candidate super-clusters per pass: lane = 8 * which + j cluster
+          const int sjl = sj + (lane >> 3);
+          bool have = false;
+          unsigned imask = 0;
+          int cj = -1;
+          if (sjl < sje && b.sc_z[2 * sjl] <= hi) {
+            cj = 8 * sjl + (lane & 7);
+            const double* bj = b.cl_box + 6 * cj;
+            const double jlo[3] = {bj[0] + S0, bj[1] + S1, bj[2] + S2}, jhi[3] = {bj[3] + S0, bj[4] + S1, bj[5] + S2};
+            for (int c = 0; c < 8; ++c) {
+              const int ci = ci0 + c;
+              // half list: one side of each cluster pair by parity; a cluster with itself under zero or + images
+              bool keep;
+              if (cj != ci) keep = (cj > ci) == (((ci + cj) & 1) == 0);
+              else keep = zero || positive;
+              if (!keep) continue;
+              double d2 = 0;
+              for (int r = 0; r < 3; ++r) {
+                const double g1 = jlo[r] - S.ibox[c][3 + r], g2 = S.ibox[c][r] - jhi[r];
+                const double gg = g1 > 0 ? g1 : (g2 > 0 ? g2 : 0.0);
+                d2 += gg * gg;
               }
-              have = imask != 0;
+              if (d2 < g.rlist2) imask |= 1u << c;
             }
-            const unsigned ball = __ballot_sync(0xffffffffu, have);
-            if (have) {
-              const int pos = S.nent + __popc(ball & ((1u << lane) - 1));
-              const int sjc = cj >> 3;
-              S.ent[pos] = make_uint4(unsigned(cj), imask | (img << 8), 0u, 0u);
-              S.sh[pos] = make_float4(float(b.sc_org[3 * sjc] + S0 - S.org_i[0]), float(b.sc_org[3 * sjc + 1] + S1 - S.org_i[1]),
-                                      float(b.sc_org[3 * sjc + 2] + S2 - S.org_i[2]), 0.f);
-              S.needs_mask[pos] = (unsigned char)((zero && sjc == sc) || key_find(S, excl_key(unsigned(cj), img)));
+            have = imask != 0;
+          }
+          const unsigned ball = __ballot_sync(0xffffffffu, have);
+          if (have) {
+            const int pos = B.nent + __popc(ball & ((1u << lane) - 1));
+            const int sjc = cj >> 3;
+            B.ent[pos] = make_uint4(unsigned(cj), imask | (img << 8), 0u, 0u);
+            B.sh[pos] = make_float4(float(b.sc_org[3 * sjc] + S0 - S.org_i[0]), float(b.sc_org[3 * sjc + 1] + S1 - S.org_i[1]),
+                                    float(b.sc_org[3 * sjc + 2] + S2 - S.org_i[2]), 0.f);
+            B.needs_mask[pos] = (unsigned char)((zero && sjc == sc) || key_find(S, excl_key(unsigned(cj), img)));
+          }
+          __syncwarp();
+          if (lane == 0) B.nent += __popc(ball);
+          __syncwarp();
+          if (B.nent >= kBatch) {
+            flush_batch(S, B, sc, kBatch, lane, b);
+            __syncwarp();
+            const int rest = B.nent - kBatch;
+            for (int e = lane; e < rest; e += 32) {
+              B.ent[e] = B.ent[kBatch + e];
+              B.sh[e] = B.sh[kBatch + e];
+              B.needs_mask[e] = B.needs_mask[kBatch + e];
             }
             __syncwarp();
-            if (lane == 0) S.nent += __popc(ball);
+            if (lane == 0) B.nent = rest;
             __syncwarp();
-            if (S.nent >= kBatch) {
-              flush_batch(S, sc, kBatch, lane, b);
-              __syncwarp();
-              const int rest = S.nent - kBatch;
-              for (int e = lane; e < rest; e += 32) {
-                S.ent[e] = S.ent[kBatch + e];
-                S.sh[e] = S.sh[kBatch + e];
-                S.needs_mask[e] = S.needs_mask[kBatch + e];
-              }
-              __syncwarp();
-              if (lane == 0) S.nent = rest;
-              __syncwarp();
-            }
           }
         }
       }
     }
-    flush_batch(S, sc, S.nent, lane, b);
-    __syncwarp();
+    flush_batch(S, B, sc, B.nent, lane, b);
+    __syncthreads();   // S is rewritten for the next super-cluster
   }
 }
 

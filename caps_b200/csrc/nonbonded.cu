@@ -43,6 +43,28 @@ __global__ void k_reduce_f64(int n, const double* __restrict__ F, const double* 
 
 }  // namespace
 
+void Engine::fork(int k, const std::function<void()>& launch) {
+  CK(cudaEventRecord(ev_fork_, stream_));
+  CK(cudaStreamWaitEvent(side_[k], ev_fork_, 0));
+  struct Swap {
+    cudaStream_t& s;
+    cudaStream_t saved;
+    ~Swap() { s = saved; }
+  } swap{stream_, stream_};
+  stream_ = side_[k];
+  launch();
+  CK(cudaEventRecord(ev_join_[k], side_[k]));
+}
+
+void Engine::join(int k) { CK(cudaStreamWaitEvent(stream_, ev_join_[k], 0)); }
+
+int Engine::list_builds() {
+  int v = 0;
+  CK(cudaMemcpyAsync(&v, d_counters_.p + kCntBuilds, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+  CK(cudaStreamSynchronize(stream_));
+  return v;
+}
+
 // ---------------------------------------------------------------------------------------------------------------
 void Engine::launch_build(const double* d_x) {
   const ListGeom& g = geom_;
@@ -51,9 +73,10 @@ void Engine::launch_build(const double* d_x) {
   k_scan_columns<<<1, 1024, 0, stream_>>>(g, lb_);
   k_scatter<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, lb_);
   const size_t sort_smem = size_t(kSortMax) * (sizeof(double) + sizeof(int));
-  k_sort_columns<<<std::min(g.ncol, dev_sms_ * 8), 256, sort_smem, stream_>>>(g, lb_);
+  k_sort_columns<<<std::min(g.ncol, dev_sms_ * 8), 1024, sort_smem, stream_>>>(g, lb_);
   k_superclusters<<<std::max(1, std::min(blocks_for(size_t(nsc_cap_), 4), dev_sms_ * 16)), 128, 0, stream_>>>(dcell_, lb_);
-  k_search<<<std::max(1, std::min(nsc_cap_, dev_sms_ * 16)), 32, sizeof(SearchShared), stream_>>>(dcell_, g, d_excl_off_.p, d_excl_list_.p, lb_);
+  k_search<<<std::max(1, std::min(nsc_cap_, dev_sms_ * 8)), 32 * kSearchWarps, sizeof(SearchShared), stream_>>>(dcell_, g, d_excl_off_.p,
+                                                                                                          d_excl_list_.p, lb_);
   k_end_build<<<blocks_for(size_t(3) * n_, 256), 256, 0, stream_>>>(n_, d_x, d_x0_.p, lb_.counters);
   CK(cudaGetLastError());
 }
@@ -159,16 +182,6 @@ void Engine::pair_forces(bool ener, bool vir) {
 // forces reduced into d_f_ (AoS doubles). Asynchronous on stream_.
 void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild) {
   const bool nonb = (opt_.parts & 2) != 0;
-  if (nonb) {
-    if (!list_valid_) {
-      k_set_flag<<<1, 1, 0, stream_>>>(d_counters_.p, kCntRebuild, 1);
-      list_valid_ = true;
-      ++builds_;
-    } else if (check_rebuild) {
-      k_check_moved<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_x, d_x0_.p, 0.25 * skin_ * skin_, d_counters_.p);
-    }
-    launch_build(d_x);
-  }
   if (mixed_) {
     CK(cudaMemsetAsync(d_F_.p, 0, d_F_.n * sizeof(long long), stream_));
     if (nonb) CK(cudaMemsetAsync(d_Fs_.p, 0, d_Fs_.n * sizeof(long long), stream_));
@@ -176,9 +189,23 @@ void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild) 
     CK(cudaMemsetAsync(d_Fd_.p, 0, d_Fd_.n * sizeof(double), stream_));
     if (nonb) CK(cudaMemsetAsync(d_Fsd_.p, 0, d_Fsd_.n * sizeof(double), stream_));
   }
-  CK(cudaMemsetAsync(d_efix_.p, 0, d_efix_.n * sizeof(long long), stream_));
-  CK(cudaMemsetAsync(d_edbl_.p, 0, d_edbl_.n * sizeof(double), stream_));
+  if (ener || vir) {
+    CK(cudaMemsetAsync(d_efix_.p, 0, d_efix_.n * sizeof(long long), stream_));
+    CK(cudaMemsetAsync(d_edbl_.p, 0, d_edbl_.n * sizeof(double), stream_));
+  }
+  // Three branches: bonded terms and PME beside the list and pair kernels. All add into order-free fixed-point (or
+  // atomic FP64) sums, so how the branches interleave does not change the mixed path's result.
+  fork(0, [&] { bonded_forces(d_x, ener, vir); });
+  const bool pme = nonb && pme_;
+  if (pme) fork(1, [&] { pme_forces(d_x, ener, vir); });
   if (nonb) {
+    if (!list_valid_) {
+      k_set_flag<<<1, 1, 0, stream_>>>(d_counters_.p, kCntRebuild, 1);
+      list_valid_ = true;
+    } else if (check_rebuild) {
+      k_check_moved<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_x, d_x0_.p, 0.25 * skin_ * skin_, d_counters_.p);
+    }
+    launch_build(d_x);
     const size_t ns = size_t(nsc_cap_) * kScAtoms;
     if (mixed_)
       k_pack_f32<<<blocks_for(ns, 256), 256, 0, stream_>>>(int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_sc_org_.p, d_q_.p, d_type_.p, nt_,
@@ -189,8 +216,8 @@ void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild) 
     prune(d_x);
     pair_forces(ener, vir);
   }
-  bonded_forces(d_x, ener, vir);
-  if (nonb && pme_) pme_forces(d_x, ener, vir);
+  join(0);
+  if (pme) join(1);
   const size_t ns = size_t(nsc_cap_) * kScAtoms;
   if (mixed_) k_reduce_f32<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_F_.p, d_Fs_.p, int(ns), d_iperm_.p, d_f_.p, nonb ? 1 : 0);
   else k_reduce_f64<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_Fd_.p, d_Fsd_.p, int(ns), d_iperm_.p, d_f_.p, nonb ? 1 : 0);

@@ -91,6 +91,55 @@ struct PairArgs {
   int* err;              // the error word (range errors of the fixed-point sums)
 };
 
+// Sums the j forces (a: j atom q, b: j atom q + 4) over the 8 lanes of an i8 group (lanes xor 1, 2, 4): the first level
+// swaps halves so that each lane keeps one j atom's three components, the other two are a butterfly. 9 shuffles; lanes
+// with i8 < 4 end with a's sums, lanes with i8 >= 4 with b's.
+template <class T>
+__device__ __forceinline__ void reduce_j(int i8, T ax, T ay, T az, T bx, T by, T bz, T& kx, T& ky, T& kz) {
+  const bool hi = (i8 & 4) != 0;
+  kx = hi ? bx : ax, ky = hi ? by : ay, kz = hi ? bz : az;
+  const T sx = hi ? ax : bx, sy = hi ? ay : by, sz = hi ? az : bz;
+  kx += __shfl_xor_sync(0xffffffffu, sx, 4);
+  ky += __shfl_xor_sync(0xffffffffu, sy, 4);
+  kz += __shfl_xor_sync(0xffffffffu, sz, 4);
+#pragma unroll
+  for (int o = 1; o < 4; o <<= 1) {
+    kx += __shfl_xor_sync(0xffffffffu, kx, o);
+    ky += __shfl_xor_sync(0xffffffffu, ky, o);
+    kz += __shfl_xor_sync(0xffffffffu, kz, o);
+  }
+}
+
+// Sums the i forces of the 8 clusters over the 4 lanes of each i atom (lanes xor 8, 16) by halving: 18 shuffles. Lane
+// jq ends with clusters jq and jq + 4: out[0..2] = cluster jq (x, y, z), out[3..5] = cluster jq + 4.
+template <class T>
+__device__ __forceinline__ void reduce_i(int jq, const T fx[8], const T fy[8], const T fz[8], T out[6]) {
+  // level xor 16: keep the clusters c with (c & 2) == (jq & 2): c0 in {0, 1, 4, 5} or c0 ^ 2
+  const bool b1 = (jq & 2) != 0, b0 = (jq & 1) != 0;
+  T h[4][3];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int c0 = (k & 1) | ((k & 2) << 1);   // 0, 1, 4, 5
+    const int c2 = c0 ^ 2;
+    const T kx = b1 ? fx[c2] : fx[c0], ky = b1 ? fy[c2] : fy[c0], kz = b1 ? fz[c2] : fz[c0];
+    const T sx = b1 ? fx[c0] : fx[c2], sy = b1 ? fy[c0] : fy[c2], sz = b1 ? fz[c0] : fz[c2];
+    h[k][0] = kx + __shfl_xor_sync(0xffffffffu, sx, 16);
+    h[k][1] = ky + __shfl_xor_sync(0xffffffffu, sy, 16);
+    h[k][2] = kz + __shfl_xor_sync(0xffffffffu, sz, 16);
+  }
+  // level xor 8: of h[k] (k = 0, 1: clusters (jq & 2) + 0/1; k = 2, 3: the same + 4) keep (c & 1) == (jq & 1)
+#pragma unroll
+  for (int m = 0; m < 2; ++m) {
+    const int k0 = 2 * m, k1 = 2 * m + 1;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      const T kv = b0 ? h[k1][r] : h[k0][r];
+      const T sv = b0 ? h[k0][r] : h[k1][r];
+      out[3 * m + r] = kv + __shfl_xor_sync(0xffffffffu, sv, 8);
+    }
+  }
+}
+
 // --- FP32 path ---------------------------------------------------------------------------------------------------
 // COUL: 0 none; 1 Ewald real space (PME) and 2 damped shifted force through the rational fits of ewald_fit.cuh
 // (kappa r_c <= 4); 3 and 4 the same through erfcf and expf (any kappa).
@@ -136,8 +185,9 @@ static __global__ void __launch_bounds__(128, 4) k_pair_f32(PairArgs A) {
       const uint4 en = A.ent[e];
       const float4 sh = A.ent_shift[e];
       const int cj = int(en.x);
-      const unsigned imask = en.w & 255u;
-      if (!imask) continue;
+      const unsigned hmask = en.w & 0xffffu;   // pruned (i cluster, j half) pairs
+      if (!hmask) continue;
+      const unsigned imask = (hmask | (hmask >> 8)) & 255u;
       const int j0 = 8 * cj + jq, j1 = j0 + 4;
       const float4 a0 = A.xq[j0], a1 = A.xq[j1];
       const int t0 = A.tslot[j0], t1 = A.tslot[j1];
@@ -153,6 +203,7 @@ static __global__ void __launch_bounds__(128, 4) k_pair_f32(PairArgs A) {
         const bool oki = (ireal >> c) & 1u;
 #pragma unroll
         for (int jj = 0; jj < 2; ++jj) {
+          if (!((hmask >> (c + 8 * jj)) & 1u)) continue;   // this half of the j cluster is beyond the prune radius
           const float xj = jj ? xj1 : xj0, yj = jj ? yj1 : yj0, zj = jj ? zj1 : zj0;
           const float qj = jj ? a1.w : a0.w;
           const int tj = jj ? t1 : t0;
@@ -217,40 +268,31 @@ static __global__ void __launch_bounds__(128, 4) k_pair_f32(PairArgs A) {
           }
         }
       }
-      // j forces: sum over the 8 lanes holding the same j atoms, then one fixed-point add per component
-#pragma unroll
-      for (int o = 1; o < 8; o <<= 1) {
-        f0x += __shfl_xor_sync(0xffffffffu, f0x, o);
-        f0y += __shfl_xor_sync(0xffffffffu, f0y, o);
-        f0z += __shfl_xor_sync(0xffffffffu, f0z, o);
-        f1x += __shfl_xor_sync(0xffffffffu, f1x, o);
-        f1y += __shfl_xor_sync(0xffffffffu, f1y, o);
-        f1z += __shfl_xor_sync(0xffffffffu, f1z, o);
-      }
-      if (i8 < 6) {
-        const float v = i8 == 0 ? f0x : i8 == 1 ? f0y : i8 == 2 ? f0z : i8 == 3 ? f1x : i8 == 4 ? f1y : f1z;
-        const int js = i8 < 3 ? j0 : j1;
-        long long* dst = (i8 % 3 == 0) ? A.fsx : (i8 % 3 == 1) ? A.fsy : A.fsz;
-        if (v != 0.f) fix_add_f(dst + js, v, A.err);
+      // j forces: summed over the 8 lanes holding the same j atoms, then one fixed-point add per component
+      {
+        float kx, ky, kz;
+        reduce_j(i8, f0x, f0y, f0z, f1x, f1y, f1z, kx, ky, kz);
+        const int comp = i8 & 3;
+        if (comp < 3) {
+          const float v = comp == 0 ? kx : comp == 1 ? ky : kz;
+          long long* dst = comp == 0 ? A.fsx : comp == 1 ? A.fsy : A.fsz;
+          if (v != 0.f) fix_add_f(dst + ((i8 & 4) ? j1 : j0), v, A.err);
+        }
       }
     }
-    // i forces: sum over the 4 lanes of each i atom, then lanes share the adds
+    // i forces: summed over the 4 lanes of each i atom; lane jq adds clusters jq and jq + 4
+    {
+      float fo[6];
+      reduce_i(jq, fix, fiy, fiz, fo);
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      fix[c] += __shfl_xor_sync(0xffffffffu, fix[c], 8);
-      fiy[c] += __shfl_xor_sync(0xffffffffu, fiy[c], 8);
-      fiz[c] += __shfl_xor_sync(0xffffffffu, fiz[c], 8);
-      fix[c] += __shfl_xor_sync(0xffffffffu, fix[c], 16);
-      fiy[c] += __shfl_xor_sync(0xffffffffu, fiy[c], 16);
-      fiz[c] += __shfl_xor_sync(0xffffffffu, fiz[c], 16);
-    }
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      if ((c & 3) != jq || !((ireal >> c) & 1u)) continue;
-      const int s = 64 * sc + 8 * c + i8;
-      if (fix[c] != 0.f) fix_add_f(A.fsx + s, fix[c], A.err);
-      if (fiy[c] != 0.f) fix_add_f(A.fsy + s, fiy[c], A.err);
-      if (fiz[c] != 0.f) fix_add_f(A.fsz + s, fiz[c], A.err);
+      for (int m = 0; m < 2; ++m) {
+        const int c = jq + 4 * m;
+        if (!((ireal >> c) & 1u)) continue;
+        const int s = 64 * sc + 8 * c + i8;
+        if (fo[3 * m] != 0.f) fix_add_f(A.fsx + s, fo[3 * m], A.err);
+        if (fo[3 * m + 1] != 0.f) fix_add_f(A.fsy + s, fo[3 * m + 1], A.err);
+        if (fo[3 * m + 2] != 0.f) fix_add_f(A.fsz + s, fo[3 * m + 2], A.err);
+      }
     }
     if (ENER) {
       acc_v += double(warp_sum(ev));
@@ -327,8 +369,9 @@ static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
     for (int e = wk.y; e < wk.y + wk.z; ++e) {
       const uint4 en = A.ent[e];
       const int cj = int(en.x);
-      const unsigned imask = en.w & 255u;
-      if (!imask) continue;
+      const unsigned hmask = en.w & 0xffffu;
+      if (!hmask) continue;
+      const unsigned imask = (hmask | (hmask >> 8)) & 255u;
       int qa, qb, qc;
       unpack_image(en.y >> 8, qa, qb, qc);
       const double Sx = A.cell.h[0][0] * qa + A.cell.h[0][1] * qb + A.cell.h[0][2] * qc;
@@ -349,6 +392,7 @@ static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
         const double xs = xi.x - Sx, ys = xi.y - Sy, zs = xi.z - Sz;
 #pragma unroll
         for (int jj = 0; jj < 2; ++jj) {
+          if (!((hmask >> (c + 8 * jj)) & 1u)) continue;
           const double4 aj = jj ? a1 : a0;
           const int tj = jj ? t1 : t0;
           const int bit = 8 * i8 + jq + 4 * jj;
@@ -397,38 +441,29 @@ static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
           }
         }
       }
-#pragma unroll
-      for (int o = 1; o < 8; o <<= 1) {
-        f0x += __shfl_xor_sync(0xffffffffu, f0x, o);
-        f0y += __shfl_xor_sync(0xffffffffu, f0y, o);
-        f0z += __shfl_xor_sync(0xffffffffu, f0z, o);
-        f1x += __shfl_xor_sync(0xffffffffu, f1x, o);
-        f1y += __shfl_xor_sync(0xffffffffu, f1y, o);
-        f1z += __shfl_xor_sync(0xffffffffu, f1z, o);
-      }
-      if (i8 < 6) {
-        const double v = i8 == 0 ? f0x : i8 == 1 ? f0y : i8 == 2 ? f0z : i8 == 3 ? f1x : i8 == 4 ? f1y : f1z;
-        const int js = i8 < 3 ? j0 : j1;
-        double* dst = (i8 % 3 == 0) ? A.fdx : (i8 % 3 == 1) ? A.fdy : A.fdz;
-        if (v != 0.0) atomicAdd(dst + js, v);
+      {
+        double kx, ky, kz;
+        reduce_j(i8, f0x, f0y, f0z, f1x, f1y, f1z, kx, ky, kz);
+        const int comp = i8 & 3;
+        if (comp < 3) {
+          const double v = comp == 0 ? kx : comp == 1 ? ky : kz;
+          double* dst = comp == 0 ? A.fdx : comp == 1 ? A.fdy : A.fdz;
+          if (v != 0.0) atomicAdd(dst + ((i8 & 4) ? j1 : j0), v);
+        }
       }
     }
+    {
+      double fo[6];
+      reduce_i(jq, fix, fiy, fiz, fo);
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      fix[c] += __shfl_xor_sync(0xffffffffu, fix[c], 8);
-      fiy[c] += __shfl_xor_sync(0xffffffffu, fiy[c], 8);
-      fiz[c] += __shfl_xor_sync(0xffffffffu, fiz[c], 8);
-      fix[c] += __shfl_xor_sync(0xffffffffu, fix[c], 16);
-      fiy[c] += __shfl_xor_sync(0xffffffffu, fiy[c], 16);
-      fiz[c] += __shfl_xor_sync(0xffffffffu, fiz[c], 16);
-    }
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      if ((c & 3) != jq || !((ireal >> c) & 1u)) continue;
-      const int s = 64 * sc + 8 * c + i8;
-      if (fix[c] != 0.0) atomicAdd(A.fdx + s, fix[c]);
-      if (fiy[c] != 0.0) atomicAdd(A.fdy + s, fiy[c]);
-      if (fiz[c] != 0.0) atomicAdd(A.fdz + s, fiz[c]);
+      for (int m = 0; m < 2; ++m) {
+        const int c = jq + 4 * m;
+        if (!((ireal >> c) & 1u)) continue;
+        const int s = 64 * sc + 8 * c + i8;
+        if (fo[3 * m] != 0.0) atomicAdd(A.fdx + s, fo[3 * m]);
+        if (fo[3 * m + 1] != 0.0) atomicAdd(A.fdy + s, fo[3 * m + 1]);
+        if (fo[3 * m + 2] != 0.0) atomicAdd(A.fdz + s, fo[3 * m + 2]);
+      }
     }
     if (ENER) {
       acc_v += warp_sum(ev);
@@ -448,9 +483,10 @@ static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
   }
 }
 
-// K-PRUNE (dynamic pruning, as core/src/nbnxm.cpp:328-363 does on the CPU): each entry's i-cluster mask is rewritten
-// to the i clusters with at least one atom pair inside r_prune = r_c + b at the present positions; the pair kernels
-// read that mask. Pruned again once an atom has moved b/2 since the last prune, so no pair inside r_c is lost. Gated by
+// K-PRUNE (dynamic pruning, as core/src/nbnxm.cpp:328-363 does on the CPU): each entry's mask is rewritten to the
+// (i cluster, j half) pairs with at least one atom pair inside r_prune = r_c + b at the present positions; the pair
+// kernels read that mask. The j halves are the cluster's lower-x and upper-x four atoms (the cluster split orders its
+// atoms along x), so a half mask drops the far half of a j cluster that reaches an i cluster with its near half only. Pruned again once an atom has moved b/2 since the last prune, so no pair inside r_c is lost. Gated by
 // the prune flag, set by the displacement check and by every list build. FP32 path: packed float positions; FP64 path:
 // packed double positions.
 template <bool DBL>
@@ -506,15 +542,14 @@ static __global__ void __launch_bounds__(128) k_prune(PairArgs A, double rprune2
       for (int c = 0; c < 8; ++c) {
         if (!((built >> c) & 1u)) continue;
         const float4 xi = s_xi[wib][8 * c + i8];
-        bool in = false;
 #pragma unroll
         for (int jj = 0; jj < 2; ++jj) {
           // FP64 path: absolute positions rounded to float (1e-5 Å at 100 Å), far inside the 0.8 Å prune margin
           const float dx = xj[jj] - xi.x, dy = yj[jj] - xi.y, dz = zj[jj] - xi.z;
           const float r2 = dx * dx + dy * dy + dz * dz;
-          in |= xi.w != 0.f && rj[jj] && r2 < rp2;
+          const bool in = xi.w != 0.f && rj[jj] && r2 < rp2;
+          if (__any_sync(0xffffffffu, in)) keep |= 1u << (c + 8 * jj);
         }
-        if (__any_sync(0xffffffffu, in)) keep |= 1u << c;
       }
       if (lane == 0) {
         en.w = keep;
@@ -530,6 +565,7 @@ static __global__ void k_end_prune(int n, const double* __restrict__ x, double* 
   if (*(volatile const int*)(counters + kCntPrune) == 0) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < 3 * n) xp[i] = x[i];
+  if (i == 0) counters[kCntPrunes] += 1;
 }
 static __global__ void k_lower_prune(int* counters) { counters[kCntPrune] = 0; }
 

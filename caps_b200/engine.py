@@ -182,6 +182,10 @@ class Evaluator:
         """Kernel launches in one plain MD step of the last run (the captured graph's kernel nodes)."""
         return int(self.lib.caps_gpu_diag_step_kernels(self.h))
 
+    def kernels_run(self) -> int:
+        """Kernels the last run launched in its step loop (graph kernel nodes replayed, thermo-row kernels)."""
+        return int(self.lib.caps_gpu_diag_kernels_run(self.h))
+
     def pair_timing(self, x, cell, launches: int = 50, flush_bytes: int = 0) -> dict:
         """The pair kernel alone: mean launch time and the pairs it evaluates (include/caps_gpu_diag.h)."""
         x = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1))

@@ -16,8 +16,12 @@ extern "C" {
 int32_t caps_gpu_diag_set_timing(caps_gpu_engine* e, int64_t flush_bytes);
 /* Device milliseconds per MD step of the last run (the per-step events in measurement mode). */
 double caps_gpu_diag_last_step_ms(const caps_gpu_engine* e);
-/* Kernel launches in one plain MD step of the last run (the kernel nodes of its captured CUDA graph). */
+/* Kernel launches in one plain MD step of the last run (the kernel nodes of its captured CUDA graph; the list-build and
+ * prune kernels among them return at once on steps that do not need them). */
 int32_t caps_gpu_diag_step_kernels(const caps_gpu_engine* e);
+/* Kernels the last caps_gpu_run launched in its step loop: per step the kernel nodes of the step graph it replayed, plus
+ * the kinetic-energy kernel of each thermo row; a barostat step (run outside a graph) counts as one thermo step. */
+int64_t caps_gpu_diag_kernels_run(const caps_gpu_engine* e);
 /* Times the non-bonded pair kernel alone: one force evaluation at x (host, 3N) builds the list, then `launches`
  * launches of the pair kernel (forces only), each bracketed by CUDA events, an L2 flush of flush_bytes before each.
  * avg_ms: mean launch time; pairs_in: atom pairs inside the cut-off per launch; pairs_listed: atom pairs the kernel
