@@ -649,6 +649,14 @@ struct caps_gpu_engine {
 
 namespace {
 thread_local std::string g_create_error;
+}  // namespace
+
+namespace capsb {
+// The text caps_gpu_error(NULL) returns, for calls that fail without an engine.
+void set_call_error(const std::string& text) { g_create_error = text; }
+}  // namespace capsb
+
+namespace {
 
 int32_t guard(caps_gpu_engine* h, const std::function<void()>& fn) {
   try {

@@ -177,6 +177,19 @@ void caps_gpu_destroy(caps_gpu_engine* e);
 /* Text of the last error on this engine (or of the last failed caps_gpu_create when e is NULL). */
 const char* caps_gpu_error(const caps_gpu_engine* e);
 
+/* Kinetic energy and kinetic tensor of n atoms, computed without allocating any device memory. No counterpart in the
+ * reference: it is for callers that may not call cudaMalloc, such as a host whose memory manager owns all device memory
+ * and hands out its own buffers, or code running beside a long stream-ordered pipeline that an allocation would
+ * synchronise. d_v (3n doubles, Å/fs), d_mass (n doubles, g/mol) and d_out (7 doubles) are device pointers the caller
+ * owns; on completion d_out[0] = sum 0.5 m v² and d_out[1..6] = sum m v_a v_b (xx yy zz xy xz yz), in kcal/mol.
+ * stream: a cudaStream_t passed as a pointer (NULL: the default stream); the call only enqueues work on it.
+ * Limits: 1 <= n <= 1,048,576 (larger n is rejected with CAPS_GPU_EINVAL). The working memory is one fixed array of
+ * about 230 KB per GPU, held from the library's load until the process exits, and shared by every call on that GPU: calls
+ * whose work overlaps on the device (different streams, or other host threads) race on it and must be serialised by the
+ * caller. The first call on each device looks up that array's device address; make that first call before any stream
+ * capture. Errors: caps_gpu_error(NULL). */
+int32_t caps_gpu_kinetic_noalloc(const double* d_v, const double* d_mass, int32_t n, double* d_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
