@@ -25,6 +25,7 @@ void Engine::time_pair_kernel(const double* x, const double* cell, int launches,
     if (flush_bytes > 0) cudaMemsetAsync(d_flush_.p, k & 255, size_t(flush_bytes), stream_);
     if (mixed_) cudaMemsetAsync(d_Fs_.p, 0, d_Fs_.n * sizeof(long long), stream_);
     else cudaMemsetAsync(d_Fsd_.p, 0, d_Fsd_.n * sizeof(double), stream_);
+    cudaMemsetAsync(d_counters_.p + kCntPairNext, 0, sizeof(int), stream_);   // the pack kernel resets it in a force evaluation
     cudaEventRecord(ev[size_t(2 * k)], stream_);
     pair_forces(false, false);
     cudaEventRecord(ev[size_t(2 * k + 1)], stream_);

@@ -12,6 +12,7 @@
 // Marsaglia's polar normals, Marsaglia-Tsang gamma; core/include/caps/rng.hpp), uploaded ahead in chunks, so a Bussi or
 // NVE or Nose-Hoover run starts from the reference's velocities and draws the reference's numbers. Langevin noise, 3N
 // normals a step, comes from a counter-based Philox stream on the device (a pure function of seed, step and atom).
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -116,10 +117,16 @@ __global__ void k_kick_drift(int n, double* __restrict__ x, double* __restrict__
   if (bad) atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), kErrNonFinite);
 }
 
+// Constraint clusters. Star clusters (one centre bonded to 1-3 atoms, every constraint through the centre: CH, CH2, CH3)
+// come first, ordered by size (ends e1, e2, e3), each as {centre, a1, a2, a3} and the squared lengths of (centre, a_k) in
+// the reference's constraint order; the other clusters (rigid waters, chains) follow in the general layout.
 struct ConsArgs {
-  int ncl;
-  const int* cl_start;     // ncl + 1: constraints of each cluster
-  const int* cl_atom0;     // ncl + 1: atoms of each cluster in cl_atoms
+  int ncl;                 // all clusters: e3 star clusters, then ncl - e3 general ones
+  int e1, e2, e3;
+  const int4* star;        // e3: centre, then up to three partners (-1 unused)
+  const double4* star_d2;  // e3: squared lengths of (centre, partner k)
+  const int* cl_start;     // general clusters + 1: constraints of each cluster
+  const int* cl_atom0;     // general clusters + 1: atoms of each cluster in cl_atoms
   const int* cl_atoms;     // atom indices
   const int4* cons;        // x, y: local atom indices, z: global i, w: global j
   const double* d2;        // squared lengths
@@ -127,11 +134,72 @@ struct ConsArgs {
   DevCell cell;
 };
 
+// SHAKE on a star cluster with NK constraints, in registers. The same Gauss-Seidel sweep as the general kernel, with each
+// constraint taken as (centre, partner).
+template <int NK>
+__device__ void shake_star(const ConsArgs& C, int s, double* __restrict__ x, const double* __restrict__ x0, double* __restrict__ v, double h,
+                           int* counters) {
+  const int4 at = C.star[s];
+  const double4 d4 = C.star_d2[s];
+  const int ids[4] = {at.x, at.y, at.z, at.w};
+  const double dd[3] = {d4.x, d4.y, d4.z};
+  double p[NK + 1][3], o[NK + 1][3], im[NK + 1];
+#pragma unroll
+  for (int a = 0; a <= NK; ++a) {
+    const int g = ids[a];
+    for (int r = 0; r < 3; ++r) p[a][r] = x[3 * g + r], o[a][r] = x0[3 * g + r];
+    im[a] = C.invm[g];
+  }
+  double ref[NK][3];
+#pragma unroll
+  for (int k = 0; k < NK; ++k) {
+    double d0 = o[0][0] - o[k + 1][0], d1 = o[0][1] - o[k + 1][1], d2v = o[0][2] - o[k + 1][2];
+    min_image(C.cell, d0, d1, d2v);
+    ref[k][0] = d0, ref[k][1] = d1, ref[k][2] = d2v;
+  }
+  bool done = false;
+  for (int it = 0; it < kShakeIter && !done; ++it) {
+    done = true;
+#pragma unroll
+    for (int k = 0; k < NK; ++k) {
+      double sv[3];
+      for (int r = 0; r < 3; ++r) sv[r] = ref[k][r] + (p[0][r] - o[0][r]) - (p[k + 1][r] - o[k + 1][r]);
+      const double diff = dd[k] - (sv[0] * sv[0] + sv[1] * sv[1] + sv[2] * sv[2]);
+      if (fabs(diff) <= 2 * kShakeTol * dd[k]) continue;
+      done = false;
+      const double sr = sv[0] * ref[k][0] + sv[1] * ref[k][1] + sv[2] * ref[k][2];
+      if (sr < 1e-6 * dd[k]) {
+        atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), kErrShakeTurn);
+        return;
+      }
+      const double g = diff / (2 * (im[0] + im[k + 1]) * sr);
+      for (int r = 0; r < 3; ++r) {
+        p[0][r] += g * im[0] * ref[k][r];
+        p[k + 1][r] -= g * im[k + 1] * ref[k][r];
+      }
+    }
+  }
+  if (!done) atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), kErrShake);
+#pragma unroll
+  for (int a = 0; a <= NK; ++a) {
+    const int g = ids[a];
+    for (int r = 0; r < 3; ++r) {
+      const double xb = x[3 * g + r];
+      x[3 * g + r] = p[a][r];
+      if (h > 0) v[3 * g + r] += (p[a][r] - xb) / h;
+    }
+  }
+}
+
 // SHAKE on each cluster (Gauss-Seidel along the reference vectors, tol 1e-8 relative; core/src/constraints.cpp:196-230),
 // then v += (x - x_before) / h when h > 0.
 __global__ void k_shake(ConsArgs C, double* __restrict__ x, const double* __restrict__ x0, double* __restrict__ v, double h, int* counters) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= C.ncl) return;
+  const int cc = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cc >= C.ncl) return;
+  if (cc < C.e1) return shake_star<1>(C, cc, x, x0, v, h, counters);
+  if (cc < C.e2) return shake_star<2>(C, cc, x, x0, v, h, counters);
+  if (cc < C.e3) return shake_star<3>(C, cc, x, x0, v, h, counters);
+  const int c = cc - C.e3;
   const int k0 = C.cl_start[c], k1 = C.cl_start[c + 1], a0 = C.cl_atom0[c], a1 = C.cl_atom0[c + 1];
   const int na = a1 - a0, nk = k1 - k0;
   double px[kMaxClAtoms][3], ox[kMaxClAtoms][3], bx[kMaxClAtoms][3], im[kMaxClAtoms];
@@ -213,9 +281,67 @@ __global__ void k_vel(int n, double* __restrict__ v, const double* __restrict__ 
   for (int r = 0; r < 3; ++r) v[3 * i + r] = vv[r];
 }
 
+// RATTLE on a star cluster with NK constraints, in registers (the general kernel's sweep, constraints as (centre, partner)).
+template <int NK>
+__device__ void rattle_star(const ConsArgs& C, int s, const double* __restrict__ x, double* __restrict__ v, const VelOp& op, const double* sc,
+                            double h, double w[6], int* counters) {
+  const int4 at = C.star[s];
+  const double4 d4 = C.star_d2[s];
+  const int ids[4] = {at.x, at.y, at.z, at.w};
+  const double dd[3] = {d4.x, d4.y, d4.z};
+  double pv[NK + 1][3], im[NK + 1];
+#pragma unroll
+  for (int a = 0; a <= NK; ++a) {
+    const int g = ids[a];
+    for (int r = 0; r < 3; ++r) pv[a][r] = v[3 * g + r];
+    vel_op(op, g, pv[a], C.invm, sc);
+    im[a] = C.invm[g];
+  }
+  double rr[NK][3], lam[NK];
+#pragma unroll
+  for (int k = 0; k < NK; ++k) {
+    const int gi = ids[0], gj = ids[k + 1];
+    double d0 = x[3 * gi] - x[3 * gj], d1 = x[3 * gi + 1] - x[3 * gj + 1], d2v = x[3 * gi + 2] - x[3 * gj + 2];
+    min_image(C.cell, d0, d1, d2v);
+    rr[k][0] = d0, rr[k][1] = d1, rr[k][2] = d2v;
+    lam[k] = 0;
+  }
+  bool done = false;
+  for (int it = 0; it < kShakeIter && !done; ++it) {
+    done = true;
+#pragma unroll
+    for (int k = 0; k < NK; ++k) {
+      const double rv = rr[k][0] * (pv[0][0] - pv[k + 1][0]) + rr[k][1] * (pv[0][1] - pv[k + 1][1]) + rr[k][2] * (pv[0][2] - pv[k + 1][2]);
+      if (fabs(rv) <= kShakeTol * dd[k]) continue;
+      done = false;
+      const double g = -rv / ((im[0] + im[k + 1]) * dd[k]);
+      lam[k] += g;
+      for (int r = 0; r < 3; ++r) {
+        pv[0][r] += g * im[0] * rr[k][r];
+        pv[k + 1][r] -= g * im[k + 1] * rr[k][r];
+      }
+    }
+  }
+  if (!done) atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), kErrShake);
+#pragma unroll
+  for (int a = 0; a <= NK; ++a)
+    for (int r = 0; r < 3; ++r) v[3 * ids[a] + r] = pv[a][r];
+  if (h > 0)
+#pragma unroll
+    for (int k = 0; k < NK; ++k) {
+      const double sk = 2 * lam[k] / (h * kAcc);
+      w[0] += sk * rr[k][0] * rr[k][0];
+      w[1] += sk * rr[k][1] * rr[k][1];
+      w[2] += sk * rr[k][2] * rr[k][2];
+      w[3] += sk * rr[k][0] * rr[k][1];
+      w[4] += sk * rr[k][0] * rr[k][2];
+      w[5] += sk * rr[k][1] * rr[k][2];
+    }
+}
+
 // Velocity update then RATTLE in one launch: threads [0, ncl) take one constraint cluster each (its atoms' update, then
-// the relative velocity along each constraint removed, core/src/constraints.cpp:232-269); threads [ncl, ncl + nfree)
-// update one unconstrained atom each. With h > 0 the impulses are read as forces over a half kick and their virial
+// the relative velocity along each constraint removed, core/src/constraints.cpp:232-269; star clusters in registers);
+// threads [ncl, ncl + nfree) update one unconstrained atom each. With h > 0 the impulses are read as forces over a half kick and their virial
 // (xx yy zz xy xz yz) is added to sc[kScCW0..].
 __global__ void k_vel_rattle(ConsArgs C, int nfree, const int* __restrict__ free_atoms, const double* __restrict__ x, double* __restrict__ v, VelOp op,
                              double h, double* sc, int* counters) {
@@ -227,8 +353,12 @@ __global__ void k_vel_rattle(ConsArgs C, int nfree, const int* __restrict__ free
     vel_op(op, g, vv, C.invm, sc);
     for (int r = 0; r < 3; ++r) v[3 * g + r] = vv[r];
   }
-  if (c < C.ncl) {
-    const int k0 = C.cl_start[c], k1 = C.cl_start[c + 1], a0 = C.cl_atom0[c], a1 = C.cl_atom0[c + 1];
+  if (c < C.e1) rattle_star<1>(C, c, x, v, op, sc, h, w, counters);
+  else if (c < C.e2) rattle_star<2>(C, c, x, v, op, sc, h, w, counters);
+  else if (c < C.e3) rattle_star<3>(C, c, x, v, op, sc, h, w, counters);
+  else if (c < C.ncl) {
+    const int cg = c - C.e3;
+    const int k0 = C.cl_start[cg], k1 = C.cl_start[cg + 1], a0 = C.cl_atom0[cg], a1 = C.cl_atom0[cg + 1];
     const int na = a1 - a0, nk = k1 - k0;
     double pv[kMaxClAtoms][3], im[kMaxClAtoms];
     for (int a = 0; a < na; ++a) {
@@ -438,7 +568,8 @@ struct Stepper {
   int nfree = 0;
   DevBuf<Chain> chain;
   DevBuf<int> cl_start, cl_atom0, cl_atoms;
-  DevBuf<int4> cons;
+  DevBuf<int4> cons, star;
+  DevBuf<double4> star_d2;
   DevBuf<double> d2;
   DevBuf<double2> draws;
   long long draws_first = 0, draws_count = 0;
@@ -522,10 +653,49 @@ struct Stepper {
     for (auto& c : cs) root[size_t(find(c.i))] = find(c.j);
     std::map<int, std::vector<int>> comp_cons;
     for (int k = 0; k < ncons; ++k) comp_cons[find(cs[size_t(k)].i)].push_back(k);
-    std::vector<int> st{0}, a0{0}, atoms;
+    std::vector<int> st{0}, a0{0}, atoms, gen_atoms;   // atoms: every constrained atom; gen_atoms: the general clusters
     std::vector<int4> cv;
     std::vector<double> dv;
+    std::vector<int4> star_at[3];
+    std::vector<double4> star_dd[3];
     for (auto& [r, ks] : comp_cons) {
+      if (int(ks.size()) > kMaxClCons) throw ModelError(CAPS_GPU_EINVAL, "a constraint cluster has more than 8 atoms or constraints (the device SHAKE takes bonds to hydrogen and rigid waters)");
+      // a star: 1-3 constraints that all share one atom, each with a distinct partner
+      int centre = -1;
+      if (ks.size() <= 3) {
+        const Cn& c0 = cs[size_t(ks[0])];
+        for (int cand : {c0.i, c0.j}) {
+          bool all = true;
+          std::vector<int> partners;
+          for (int k : ks) {
+            const Cn& c = cs[size_t(k)];
+            if (c.i != cand && c.j != cand) all = false;
+            else partners.push_back(c.i == cand ? c.j : c.i);
+          }
+          std::vector<int> u = partners;
+          std::sort(u.begin(), u.end());
+          if (all && std::unique(u.begin(), u.end()) == u.end()) {
+            centre = cand;
+            break;
+          }
+        }
+      }
+      if (centre >= 0) {
+        int4 a = make_int4(centre, -1, -1, -1);
+        double dd[3] = {0, 0, 0};
+        int q = 0;
+        for (int k : ks) {
+          const Cn& c = cs[size_t(k)];
+          const int partner = c.i == centre ? c.j : c.i;
+          (q == 0 ? a.y : q == 1 ? a.z : a.w) = partner;
+          dd[q++] = c.d * c.d;
+          atoms.push_back(partner);
+        }
+        atoms.push_back(centre);
+        star_at[ks.size() - 1].push_back(a);
+        star_dd[ks.size() - 1].push_back(make_double4(dd[0], dd[1], dd[2], 0.0));
+        continue;
+      }
       std::vector<int> loc;
       auto local = [&](int a) {
         for (size_t q = 0; q < loc.size(); ++q)
@@ -539,12 +709,28 @@ struct Stepper {
         cv.push_back(make_int4(li, lj, c.i, c.j));
         dv.push_back(c.d * c.d);
       }
-      if (int(ks.size()) > kMaxClCons || int(loc.size()) > kMaxClAtoms)
+      if (int(loc.size()) > kMaxClAtoms)
         throw ModelError(CAPS_GPU_EINVAL, "a constraint cluster has more than 8 atoms or constraints (the device SHAKE takes bonds to hydrogen and rigid waters)");
+      gen_atoms.insert(gen_atoms.end(), loc.begin(), loc.end());
       atoms.insert(atoms.end(), loc.begin(), loc.end());
       st.push_back(int(cv.size()));
-      a0.push_back(int(atoms.size()));
+      a0.push_back(int(gen_atoms.size()));
     }
+    std::vector<int4> sa;
+    std::vector<double4> sd;
+    for (int k = 0; k < 3; ++k) {
+      sa.insert(sa.end(), star_at[k].begin(), star_at[k].end());
+      sd.insert(sd.end(), star_dd[k].begin(), star_dd[k].end());
+    }
+    C.e1 = int(star_at[0].size());
+    C.e2 = C.e1 + int(star_at[1].size());
+    C.e3 = C.e2 + int(star_at[2].size());
+    if (!sa.empty()) {
+      star.upload(sa, E.stream_);
+      star_d2.upload(sd, E.stream_);
+    }
+    C.star = star.p;
+    C.star_d2 = star_d2.p;
     std::vector<char> in_cluster(static_cast<size_t>(n), 0);
     for (int a : atoms) in_cluster[size_t(a)] = 1;
     std::vector<int> fa;
@@ -554,10 +740,12 @@ struct Stepper {
     if (nfree) free_atoms.upload(fa, E.stream_);
     cl_start.upload(st, E.stream_);
     cl_atom0.upload(a0, E.stream_);
-    cl_atoms.upload(atoms, E.stream_);
-    cons.upload(cv, E.stream_);
-    d2.upload(dv, E.stream_);
-    C.ncl = int(st.size()) - 1;
+    if (!gen_atoms.empty()) {
+      cl_atoms.upload(gen_atoms, E.stream_);
+      cons.upload(cv, E.stream_);
+      d2.upload(dv, E.stream_);
+    }
+    C.ncl = C.e3 + int(st.size()) - 1;
     C.cl_start = cl_start.p;
     C.cl_atom0 = cl_atom0.p;
     C.cl_atoms = cl_atoms.p;

@@ -54,7 +54,7 @@ struct ListBufs {
 };
 
 // Device counters: list sizes, the error word, the rebuild and prune flags, and running counts of builds and prunes.
-enum Counter { kCntEnt = 0, kCntWork, kCntMask, kCntErr, kCntRebuild, kCntNsc, kCntMaxCol, kCntPrune, kCntBuilds, kCntPrunes, kCntNum = 10 };
+enum Counter { kCntEnt = 0, kCntWork, kCntMask, kCntErr, kCntRebuild, kCntNsc, kCntMaxCol, kCntPrune, kCntBuilds, kCntPrunes, kCntPairNext, kCntNum = 11 };
 
 __device__ __forceinline__ void raise_error(int* counters, unsigned bit) { atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), bit); }
 

@@ -16,18 +16,23 @@
 namespace capsb {
 
 // ---------------------------------------------------------------------------------------------------------------
-// K-CHECK: has any atom moved more than half the skin since the last build? (core/src/field.cpp:800-838, the
-// constant-cell branch). Sets counters[kCntRebuild].
-static __global__ void k_check_moved(int n, const double* __restrict__ x, const double* __restrict__ x0, double lim2, int* counters,
-                                     int flag = kCntRebuild) {
+// K-CHECK: has any atom moved more than half the skin since the last build (x against x0, lim_b2; core/src/field.cpp:
+// 800-838, the constant-cell branch), or half the prune margin since the last prune (x against xp, lim_p2)? Sets the
+// rebuild and prune flags; the pair kernel lowers both once the step's list work is done.
+static __global__ void k_check_step(int n, const double* __restrict__ x, const double* __restrict__ x0, double lim_b2, const double* __restrict__ xp,
+                                    double lim_p2, int* counters) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  bool moved = false;
+  bool mb = false, mp = false;
   if (i < n) {
-    const double dx = x[3 * i] - x0[3 * i], dy = x[3 * i + 1] - x0[3 * i + 1], dz = x[3 * i + 2] - x0[3 * i + 2];
-    const double d2 = dx * dx + dy * dy + dz * dz;
-    moved = !(d2 <= lim2);   // NaN counts as moved
+    const double x_ = x[3 * i], y_ = x[3 * i + 1], z_ = x[3 * i + 2];
+    const double bx = x_ - x0[3 * i], by = y_ - x0[3 * i + 1], bz = z_ - x0[3 * i + 2];
+    const double px = x_ - xp[3 * i], py = y_ - xp[3 * i + 1], pz = z_ - xp[3 * i + 2];
+    mb = !(bx * bx + by * by + bz * bz <= lim_b2);   // NaN counts as moved
+    mp = !(px * px + py * py + pz * pz <= lim_p2);
   }
-  if (__any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) atomicOr(counters + flag, 1);
+  const bool lane0 = (threadIdx.x & 31) == 0;
+  if (__any_sync(0xffffffffu, mb) && lane0) atomicOr(counters + kCntRebuild, 1);
+  if (__any_sync(0xffffffffu, mp) && lane0) atomicOr(counters + kCntPrune, 1);
 }
 
 
@@ -47,7 +52,6 @@ static __global__ void k_end_build(int n, const double* __restrict__ x, double* 
     counters[kCntBuilds] += 1;
   }
 }
-static __global__ void k_lower_flag(int* counters) { counters[kCntRebuild] = 0; }
 
 // K-BIN: wrapped fractional coordinates, lattice offsets and the column of every atom; column counts.
 static __global__ void k_bin(int n, const double* __restrict__ x, DevCell cell, ListGeom g, ListBufs b) {

@@ -121,23 +121,21 @@ PairArgs Engine::pair_args() {
   return A;
 }
 
-// Dynamic pruning: when an atom has moved b/2 since the last prune (b = min(0.8 Å, skin), as field.cpp:1306-1312), or a
-// build set the flag, every entry's i-cluster mask is rewritten for r_c + b.
+// Dynamic pruning: when an atom has moved b/2 since the last prune (b = min(0.8 Å, skin), as field.cpp:1306-1312; the
+// step's check kernel tests it), or a build set the flag, every entry's masks are rewritten for r_c + b.
 void Engine::prune(const double* d_x) {
   const double b = std::min(0.8, skin_);
   const PairArgs A = pair_args();
-  k_check_moved<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_x, d_xp_.p, 0.25 * b * b, d_counters_.p, kCntPrune);
   const double rp = rc_ + b;
   if (mixed_) k_prune<false><<<dev_sms_ * 8, 128, 0, stream_>>>(A, rp * rp, d_ent_.p);
   else k_prune<true><<<dev_sms_ * 8, 128, 0, stream_>>>(A, rp * rp, d_ent_.p);
   k_end_prune<<<blocks_for(size_t(3) * n_, 256), 256, 0, stream_>>>(n_, d_x, d_xp_.p, d_counters_.p);
-  k_lower_prune<<<1, 1, 0, stream_>>>(d_counters_.p);
 }
 
 void Engine::pair_forces(bool ener, bool vir) {
   PairArgs A = pair_args();
   const int coul = coul_ ? (pme_ ? 1 : 2) : 0;
-  const int grid = dev_sms_ * 8;
+  // persistent grids: as many blocks as fit on the SMs at once; their warps fetch work items until none are left
   const int ntab = nt_ + 1;
   if (mixed_) {
     const size_t smem = sizeof(float4) * (size_t(ntab) * ntab + 4 * 64) + sizeof(int) * 4 * 64;
@@ -146,7 +144,9 @@ void Engine::pair_forces(bool ener, bool vir) {
 #define PAIR32(C, E, V)                                                                                              \
   do {                                                                                                               \
     if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_pair_f32<C, E, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
-    k_pair_f32<C, E, V><<<grid, 128, smem, stream_>>>(A);                                                            \
+    int per_sm = 0;                                                                                                  \
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_f32<C, E, V>, 128, smem));                      \
+    k_pair_f32<C, E, V><<<dev_sms_ * std::max(1, per_sm), 128, smem, stream_>>>(A);                                                            \
   } while (0)
 #define PAIR32C(C) { if (ener) { if (vir) PAIR32(C, true, true); else PAIR32(C, true, false); } else { if (vir) PAIR32(C, false, true); else PAIR32(C, false, false); } }
     switch (c32) {
@@ -163,7 +163,9 @@ void Engine::pair_forces(bool ener, bool vir) {
 #define PAIR64(C, ...)                                                                                               \
   do {                                                                                                               \
     if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_pair_f64<C, __VA_ARGS__>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
-    k_pair_f64<C, __VA_ARGS__><<<grid, 128, smem, stream_>>>(A);                                                     \
+    int per_sm = 0;                                                                                                  \
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_f64<C, __VA_ARGS__>, 128, smem));               \
+    k_pair_f64<C, __VA_ARGS__><<<dev_sms_ * std::max(1, per_sm), 128, smem, stream_>>>(A);                                                     \
   } while (0)
     if (opt_.force_cap > 0) {
       // push-off: energies and virial always on (a rare path, kept to one instantiation per Coulomb form)
@@ -203,7 +205,8 @@ void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild) 
       k_set_flag<<<1, 1, 0, stream_>>>(d_counters_.p, kCntRebuild, 1);
       list_valid_ = true;
     } else if (check_rebuild) {
-      k_check_moved<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_x, d_x0_.p, 0.25 * skin_ * skin_, d_counters_.p);
+      const double b = std::min(0.8, skin_);   // the prune margin (see prune())
+      k_check_step<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_x, d_x0_.p, 0.25 * skin_ * skin_, d_xp_.p, 0.25 * b * b, d_counters_.p);
     }
     launch_build(d_x);
     const size_t ns = size_t(nsc_cap_) * kScAtoms;
@@ -221,7 +224,6 @@ void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild) 
   const size_t ns = size_t(nsc_cap_) * kScAtoms;
   if (mixed_) k_reduce_f32<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_F_.p, d_Fs_.p, int(ns), d_iperm_.p, d_f_.p, nonb ? 1 : 0);
   else k_reduce_f64<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_Fd_.p, d_Fsd_.p, int(ns), d_iperm_.p, d_f_.p, nonb ? 1 : 0);
-  if (nonb) k_lower_flag<<<1, 1, 0, stream_>>>(d_counters_.p);
   CK(cudaGetLastError());
 }
 

@@ -23,8 +23,9 @@ constexpr float kPadFar = 1.0e5f;   // padding slots sit this far from their sup
 // K-PACK (FP32): per slot, float4 (position relative to the super-cluster origin, charge) and the type index.
 static __global__ void k_pack_f32(int nslots, const int* __restrict__ perm, const double* __restrict__ x, const int* __restrict__ ioff, DevCell cell,
                            const double* __restrict__ sc_org, const double* __restrict__ q, const int* __restrict__ type, int pad_type,
-                           float4* __restrict__ xq, int* __restrict__ tslot, const int* counters) {
+                           float4* __restrict__ xq, int* __restrict__ tslot, int* counters) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s == 0) counters[kCntPairNext] = 0;   // the pair kernel's work-item counter
   const int nsc = counters[kCntNsc];
   if (s >= nslots || s >= 64 * nsc) return;
   const int a = perm[s];
@@ -45,8 +46,9 @@ static __global__ void k_pack_f32(int nslots, const int* __restrict__ perm, cons
 // K-PACK (FP64): per slot, double4 (wrapped absolute position, charge) and the type index.
 static __global__ void k_pack_f64(int nslots, const int* __restrict__ perm, const double* __restrict__ x, const int* __restrict__ ioff, DevCell cell,
                            const double* __restrict__ q, const int* __restrict__ type, int pad_type, double4* __restrict__ xq, int* __restrict__ tslot,
-                           const int* counters) {
+                           int* counters) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s == 0) counters[kCntPairNext] = 0;   // the pair kernel's work-item counter
   const int nsc = counters[kCntNsc];
   if (s >= nslots || s >= 64 * nsc) return;
   const int a = perm[s];
@@ -90,6 +92,14 @@ struct PairArgs {
   int work_cap;
   int* err;              // the error word (range errors of the fixed-point sums)
 };
+
+// Work items are taken dynamically: each warp fetches the next unclaimed item from a device counter (reset by the pack
+// kernel before every force evaluation). Items differ in size, so a static split leaves SMs idle at the end of the launch.
+__device__ __forceinline__ int next_work_item(const int* counters, int lane) {
+  int w = 0;
+  if (lane == 0) w = atomicAdd(const_cast<int*>(counters) + kCntPairNext, 1);
+  return __shfl_sync(0xffffffffu, w, 0);
+}
 
 // Sums the j forces (a: j atom q, b: j atom q + 4) over the 8 lanes of an i8 group (lanes xor 1, 2, 4): the first level
 // swaps halves so that each lane keeps one j atom's three components, the other two are a butterfly. 9 shuffles; lanes
@@ -156,15 +166,19 @@ static __global__ void __launch_bounds__(128, 4) k_pair_f32(PairArgs A) {
   float4* xi_s = s_xi + 64 * wib;
   int* ti_s = s_ti + 64 * wib;
   // a list build that ran out of room leaves stale work items: skip the pass, the host reports the error
+  if (blockIdx.x == 0 && threadIdx.x == 0) {   // the step's list work is done: lower the rebuild and prune flags
+    int* c = const_cast<int*>(A.counters);
+    c[kCntRebuild] = 0;
+    c[kCntPrune] = 0;
+  }
   if (A.counters[kCntErr] & (kErrListOverflow | kErrMaskOverflow | kErrScOverflow | kErrColumnTooBig | kErrExclOverflow)) return;
   const int nwork = min(A.counters[kCntWork], A.work_cap);
   const int pad = A.ntab - 1;
   const float rc2 = float(A.rc2), beta = float(A.beta), kc = float(A.kc), kcoul = float(A.kcoul);
   const float ku = float(A.beta * A.beta / kEwUMax), kap3 = float(A.beta * A.beta * A.beta);
   const float e0 = float(A.dsf_e0), f0 = float(A.dsf_f0), rcf = float(A.rc);
-  const int nwarps = gridDim.x * 4;
   double acc_v = 0, acc_c = 0, acc_w[6] = {0, 0, 0, 0, 0, 0}, acc_np = 0, acc_nl = 0;
-  for (int w = blockIdx.x * 4 + wib; w < nwork; w += nwarps) {
+  for (int w = next_work_item(A.counters, lane); w < nwork; w = next_work_item(A.counters, lane)) {
     const int4 wk = A.work[w];
     const int sc = wk.x;
     for (int t = lane; t < 64; t += 32) {
@@ -344,12 +358,16 @@ static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
   const int i8 = lane & 7, jq = lane >> 3;
   double4* xi_s = s_xi + 64 * wib;
   int* ti_s = s_ti + 64 * wib;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {   // the step's list work is done: lower the rebuild and prune flags
+    int* c = const_cast<int*>(A.counters);
+    c[kCntRebuild] = 0;
+    c[kCntPrune] = 0;
+  }
   if (A.counters[kCntErr] & (kErrListOverflow | kErrMaskOverflow | kErrScOverflow | kErrColumnTooBig | kErrExclOverflow)) return;
   const int nwork = min(A.counters[kCntWork], A.work_cap);
   const int pad = A.ntab - 1;
-  const int nwarps = gridDim.x * 4;
   double acc_v = 0, acc_c = 0, acc_w[6] = {0, 0, 0, 0, 0, 0};
-  for (int w = blockIdx.x * 4 + wib; w < nwork; w += nwarps) {
+  for (int w = next_work_item(A.counters, lane); w < nwork; w = next_work_item(A.counters, lane)) {
     const int4 wk = A.work[w];
     const int sc = wk.x;
     for (int t = lane; t < 64; t += 32) {
@@ -560,13 +578,12 @@ static __global__ void __launch_bounds__(128) k_prune(PairArgs A, double rprune2
   }
 }
 
-// Ends a prune: keeps the positions it was done at and lowers the prune flag (one thread block per 256 coordinates).
+// Ends a prune: keeps the positions it was done at (one thread per coordinate) and counts the prune.
 static __global__ void k_end_prune(int n, const double* __restrict__ x, double* __restrict__ xp, int* counters) {
   if (*(volatile const int*)(counters + kCntPrune) == 0) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < 3 * n) xp[i] = x[i];
   if (i == 0) counters[kCntPrunes] += 1;
 }
-static __global__ void k_lower_prune(int* counters) { counters[kCntPrune] = 0; }
 
 }  // namespace capsb
