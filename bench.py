@@ -30,6 +30,10 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
+REF_SECONDS = 60.0           # bound on the reference arm's timed sample (CPU)
+CPU_SAMPLE_SECONDS = 15.0    # bound on the cpu_baseline sample beside the GPU run
+# DRAM bytes (read + write) of one k_pair_f32 launch on this workload, from ncu (profiles/pair_kernel_ps32k_ncu.md)
+PAIR_DRAM_BYTES = 10.66e6
 FLOPS_PER_PAIR = 59          # FP32 flops of one interacting pair on a force-only step (FMA as 2)
 FLUSH_BYTES = 256 << 20      # > 126 MB L2
 START = ROOT / "caps_b200" / "data" / "ps32k_start.npz"
@@ -113,9 +117,10 @@ def run_reference(args, rank: int) -> dict:
         return {"impl": "reference", "unavailable": "oracle/_ref/libcaps_ref.so is not built (make -C oracle where the reference sources are)"}
     ff, x, v, cell = workload()
     threads = os.cpu_count() or 1
-    if args.warmup > 0:
-        ref.run(ff, x, cell, options("mixed", min(args.warmup, 3), 1), v=v, threads=threads)
-    steps = max(1, args.steps)
+    # warm-up (at most 3 steps), then the timed sample: K steps, bounded to about REF_SECONDS of CPU time
+    probe = ref.run(ff, x, cell, options("mixed", max(3, min(args.warmup, 10)), 1), v=v, threads=threads)
+    per_step = probe["seconds"] / max(3, min(args.warmup, 10)) if probe["seconds"] > 0 else 0.01
+    steps = int(max(1, min(args.steps, REF_SECONDS / max(per_step, 1e-6))))
     t0 = time.perf_counter()
     out = ref.run(ff, x, cell, options("mixed", steps, 1), v=v, threads=threads)
     wall = time.perf_counter() - t0
@@ -279,7 +284,9 @@ def main():
             from oracle import ref
             if ref.available():
                 threads = os.cpu_count() or 1
-                steps_cpu = 10
+                probe = ref.run(ff, x2, cell, options("mixed", 5, seed), v=v2, threads=threads)
+                per_step = probe["seconds"] / 5 if probe["seconds"] > 0 else 0.01
+                steps_cpu = int(max(10, min(5000, CPU_SAMPLE_SECONDS / max(per_step, 1e-6))))
                 r = ref.run(ff, x2, cell, options("mixed", steps_cpu, seed), v=v2, threads=threads)
                 cpu = {"value": r["ns_per_day"], "unit": "ns/day", "cores": threads, "kind": "reference",
                        "sample": f"{steps_cpu} MD steps of the same cell through the reference's run_dynamics (mixed, its fastest), "
@@ -304,7 +311,11 @@ def main():
                          "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
                          "peak_note": "FP32 FMA issue rate, 148 SMs x 128 lanes x 2 at the measured max SM clock (nominal)",
                          "work": f"{pt['pairs_in_cutoff']:.0f} pairs inside the cut-off x {FLOPS_PER_PAIR} flops per launch",
-                         "pair_ms": pt["avg_ms"], "pairs_listed": pt["pairs_listed"], "entries": pt["entries"], "traffic": None},
+                         "pair_ms": pt["avg_ms"], "pairs_listed": pt["pairs_listed"], "entries": pt["entries"],
+                         "traffic": PAIR_DRAM_BYTES,
+                         "traffic_note": "DRAM bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum, cold L2)",
+                         "hbm_view": {"achieved_gbs": PAIR_DRAM_BYTES / (pt["avg_ms"] * 1e-3) / 1e9, "peak_gbs": peaks.get("hbm_gbs"),
+                                      "frac": (PAIR_DRAM_BYTES / (pt["avg_ms"] * 1e-3) / 1e9) / peaks["hbm_gbs"] if peaks.get("hbm_gbs") else None}},
             "gpu_launches": launches,
             "gpu_launches_note": "kernels launched in the timed step loop, counted by the engine: the step graphs' kernel nodes per replayed step (list-build and prune kernels included; they return at once on steps without a build or prune), plus one kinetic-energy kernel per thermo row",
             "clocks": clk.summary(),
