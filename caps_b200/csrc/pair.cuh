@@ -154,11 +154,16 @@ __device__ __forceinline__ void reduce_i(int jq, const T fx[8], const T fy[8], c
 // COUL: 0 none; 1 Ewald real space (PME) and 2 damped shifted force through the rational fits of ewald_fit.cuh
 // (kappa r_c <= 4); 3 and 4 the same through erfcf and expf (any kappa).
 template <int COUL, bool ENER, bool VIR>
-static __global__ void __launch_bounds__(128, 4) k_pair_f32(PairArgs A) {
+static __global__ void __launch_bounds__(128, 5) k_pair_f32(PairArgs A) {
   extern __shared__ float4 smem_f4[];
   float4* tab = smem_f4;                                  // ntab * ntab
   float4* s_xi = smem_f4 + A.ntab * A.ntab;               // 4 warps x 64
   int* s_ti = reinterpret_cast<int*>(s_xi + 4 * 64);      // 4 warps x 64
+  // a work item's entries and their j atoms, staged per warp in one batch of independent loads
+  uint4* s_en_all = reinterpret_cast<uint4*>(s_ti + 4 * 64);   // 4 warps x 32 entries
+  float4* s_sh_all = reinterpret_cast<float4*>(s_en_all + 4 * kBatch);
+  float4* s_xj_all = s_sh_all + 4 * kBatch;                     // 4 warps x 32 entries x 8 j atoms
+  int* s_tj_all = reinterpret_cast<int*>(s_xj_all + 4 * kBatch * 8);
   for (int t = threadIdx.x; t < A.ntab * A.ntab; t += blockDim.x) tab[t] = A.tab[t];
   __syncthreads();
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -195,16 +200,36 @@ static __global__ void __launch_bounds__(128, 4) k_pair_f32(PairArgs A) {
 #pragma unroll
     for (int c = 0; c < 8; ++c) fix[c] = fiy[c] = fiz[c] = 0.f;
     float ev = 0.f, ec = 0.f, vw[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, npair = 0.f, nlist = 0.f;
-    for (int e = wk.y; e < wk.y + wk.z; ++e) {
-      const uint4 en = A.ent[e];
-      const float4 sh = A.ent_shift[e];
+    uint4* s_en = s_en_all + kBatch * wib;
+    float4* s_sh = s_sh_all + kBatch * wib;
+    float4* s_xj = s_xj_all + kBatch * 8 * wib;
+    int* s_tj = s_tj_all + kBatch * 8 * wib;
+    const int ne = min(wk.z, kBatch);
+    if (lane < ne) {
+      s_en[lane] = A.ent[wk.y + lane];
+      s_sh[lane] = A.ent_shift[wk.y + lane];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int t = lane + 32 * k;   // entry t / 8, j atom t % 8
+      if (t < 8 * ne) {
+        const int ja = 8 * int(s_en[t >> 3].x) + (t & 7);
+        s_xj[t] = A.xq[ja];
+        s_tj[t] = A.tslot[ja];
+      }
+    }
+    __syncwarp();
+    for (int el = 0; el < ne; ++el) {
+      const uint4 en = s_en[el];
+      const float4 sh = s_sh[el];
       const int cj = int(en.x);
-      const unsigned hmask = en.w & 0xffffu;   // pruned (i cluster, j half) pairs
+      const unsigned hmask = en.w & 0xffffu;
       if (!hmask) continue;
       const unsigned imask = (hmask | (hmask >> 8)) & 255u;
       const int j0 = 8 * cj + jq, j1 = j0 + 4;
-      const float4 a0 = A.xq[j0], a1 = A.xq[j1];
-      const int t0 = A.tslot[j0], t1 = A.tslot[j1];
+      const float4 a0 = s_xj[8 * el + jq], a1 = s_xj[8 * el + jq + 4];
+      const int t0 = s_tj[8 * el + jq], t1 = s_tj[8 * el + jq + 4];
       const float xj0 = a0.x + sh.x, yj0 = a0.y + sh.y, zj0 = a0.z + sh.z;
       const float xj1 = a1.x + sh.x, yj1 = a1.y + sh.y, zj1 = a1.z + sh.z;
       float f0x = 0.f, f0y = 0.f, f0z = 0.f, f1x = 0.f, f1y = 0.f, f1z = 0.f;
