@@ -10,10 +10,10 @@
 
 namespace capsb {
 
-void Engine::bonded_forces(const double* d_x, bool ener, bool vir) {
+void Engine::bonded_forces(const double* d_x, bool ener, bool vir, int parts) {
   BondedArgs A{d_x, dcell_, EnergySink{d_efix_.p, d_edbl_.p}, mixed_ ? 1 : 0};
   const int T = 256;
-  const bool bonded = (opt_.parts & 1) != 0, nonb = (opt_.parts & 2) != 0;
+  const bool bonded = (parts & 1) != 0, nonb = (parts & 2) != 0;
   auto nblk = [&](int cnt) { return std::min(blocks_for(size_t(std::max(cnt, 1)), T), dev_sms_ * 4); };
 #define LAUNCH3(K, S, cnt, ...)                                                                                     \
   do {                                                                                                              \

@@ -128,7 +128,9 @@ class Engine {
   void setup_options();
   void set_cell(const double* cell);
   void ensure_list_capacity();
-  void forces(const double* d_x, bool ener, bool vir, bool check_rebuild);   // everything up to d_f_ (device), async
+  // One force evaluation up to the AoS doubles d_out (d_f_ by default), async. parts: 1 bonded, 2 non-bonded, 3 both (-1:
+  // the options' parts); clear_energies = false adds this evaluation's energies and virial to the previous one's.
+  void forces(const double* d_x, bool ener, bool vir, bool check_rebuild, int parts = -1, double* d_out = nullptr, bool clear_energies = true);
   // Concurrent branches of a force evaluation: `launch` runs with stream_ pointing at side stream k, after everything
   // queued on the main stream so far; join(k) makes the main stream wait for it. Captured, these are graph branches.
   void fork(int k, const std::function<void()>& launch);
@@ -144,7 +146,7 @@ class Engine {
   void pair_forces(bool ener, bool vir);
   PairArgs pair_args();
   void prune(const double* d_x);
-  void bonded_forces(const double* d_x, bool ener, bool vir);
+  void bonded_forces(const double* d_x, bool ener, bool vir, int parts);
   void host_constants(caps_gpu_terms* t, bool ener, bool vir) const;
 
   // force field (device)

@@ -92,21 +92,23 @@ struct HostRng {
 };
 
 // --- kernels --------------------------------------------------------------------------------------------------
-// Kick then drift, per atom: v = s v + hk kAcc f / m (s = sc[kScFactor] when `scale`, the thermostat's pending velocity
-// factor, else 1), x0 = x (the constraint reference), x += hd v. Non-finite positions raise the error word. With
+// Kick then drift, per atom: v = s v + (hk f + hk2 f2) kAcc / m (s = sc[kScFactor] when `scale`, the thermostat's
+// pending velocity factor, else 1; f2 may be null), x0 = x (the constraint reference), x += hd v. Non-finite positions raise the error word. With
 // `zero_cw` the constraint-virial sums of this step start at zero.
 __global__ void k_kick_drift(int n, double* __restrict__ x, double* __restrict__ v, double* __restrict__ x0, const double* __restrict__ f,
-                             const double* __restrict__ invm, double hk, double hd, double* sc, int scale, int zero_cw, int* counters) {
+                             const double* __restrict__ invm, double hk, const double* __restrict__ f2, double hk2, double hd, double* sc, int scale,
+                             int zero_cw, int* counters) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (zero_cw && i < 6) sc[kScCW0 + i] = 0;
   if (i >= n) return;
   const double s = scale ? sc[kScFactor] : 1.0;
-  const double a = hk * kAcc * invm[i];
+  const double a = hk * kAcc * invm[i], a2 = hk2 * kAcc * invm[i];
   bool bad = false;
   for (int r = 0; r < 3; ++r) {
     double vr = v[3 * i + r];
     if (scale) vr *= s;
     vr += a * f[3 * i + r];
+    if (f2) vr += a2 * f2[3 * i + r];   // r-RESPA: the slow and the fast forces in one kick
     v[3 * i + r] = vr;
     const double xo = x[3 * i + r];
     x0[3 * i + r] = xo;
@@ -119,12 +121,15 @@ __global__ void k_kick_drift(int n, double* __restrict__ x, double* __restrict__
 
 // Constraint clusters. Star clusters (one centre bonded to 1-3 atoms, every constraint through the centre: CH, CH2, CH3)
 // come first, ordered by size (ends e1, e2, e3), each as {centre, a1, a2, a3} and the squared lengths of (centre, a_k) in
-// the reference's constraint order; the other clusters (rigid waters, chains) follow in the general layout.
+// the reference's constraint order; then rigid waters (O-H1, O-H2, H1-H2 with equal O-H lengths and equal H masses),
+// solved by SETTLE; the other clusters follow in the general layout.
 struct ConsArgs {
-  int ncl;                 // all clusters: e3 star clusters, then ncl - e3 general ones
-  int e1, e2, e3;
+  int ncl;                 // all clusters: e3 star clusters, then e4 - e3 rigid waters, then ncl - e4 general ones
+  int e1, e2, e3, e4;
   const int4* star;        // e3: centre, then up to three partners (-1 unused)
   const double4* star_d2;  // e3: squared lengths of (centre, partner k)
+  const int4* water;       // e4 - e3: O, H1, H2
+  const double2* water_geo;   // e4 - e3: d(O-H), d(H-H)
   const int* cl_start;     // general clusters + 1: constraints of each cluster
   const int* cl_atom0;     // general clusters + 1: atoms of each cluster in cl_atoms
   const int* cl_atoms;     // atom indices
@@ -191,6 +196,93 @@ __device__ void shake_star(const ConsArgs& C, int s, double* __restrict__ x, con
   }
 }
 
+
+__device__ __forceinline__ void cross3d(const double a[3], const double b[3], double o[3]) {
+  o[0] = a[1] * b[2] - a[2] * b[1];
+  o[1] = a[2] * b[0] - a[0] * b[2];
+  o[2] = a[0] * b[1] - a[1] * b[0];
+}
+__device__ __forceinline__ double dot3d(const double a[3], const double b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+__device__ __forceinline__ void unit3d(double a[3]) {
+  const double s = rsqrt(dot3d(a, a));
+  for (int r = 0; r < 3; ++r) a[r] *= s;
+}
+
+// SETTLE (Miyamoto & Kollman, J. Comput. Chem. 13, 952 (1992)): the positions of a rigid water that satisfy its three
+// distances exactly, found analytically from the unconstrained positions and the previous (constrained) ones. The
+// molecule's centre of mass is kept; the canonical triangle (O at (0, ra, 0), H at (-+rc, -rb, 0) about the centre of
+// mass) is rotated by the angles phi, psi, theta the paper derives, in a frame with z normal to the previous plane and x
+// normal to the new O direction. The reference solves waters with SHAKE (constraints.cpp:196-230); SETTLE meets the
+// same distances exactly instead of to SHAKE's 1e-8 tolerance. Displacements are added to each atom's own image.
+__device__ void settle_water(const ConsArgs& C, int w, double* __restrict__ x, const double* __restrict__ x0, double* __restrict__ v, double h,
+                             int* counters) {
+  const int4 at = C.water[w];
+  const int ia = at.x, ib = at.y, ic = at.z;
+  const double2 geo = C.water_geo[w];
+  const double mo = 1.0 / C.invm[ia], mh = 1.0 / C.invm[ib];
+  const double mt = mo + 2 * mh;
+  const double rc = 0.5 * geo.y;
+  const double hgt = sqrt(geo.x * geo.x - rc * rc);
+  const double ra = 2 * mh * hgt / mt, rb = hgt - ra;
+  // previous and present positions of the hydrogens relative to their oxygen (nearest images)
+  double b0[3], c0[3], b1[3], c1[3];
+  for (int r = 0; r < 3; ++r) {
+    b0[r] = x0[3 * ib + r] - x0[3 * ia + r], c0[r] = x0[3 * ic + r] - x0[3 * ia + r];
+    b1[r] = x[3 * ib + r] - x[3 * ia + r], c1[r] = x[3 * ic + r] - x[3 * ia + r];
+  }
+  min_image(C.cell, b0[0], b0[1], b0[2]);
+  min_image(C.cell, c0[0], c0[1], c0[2]);
+  min_image(C.cell, b1[0], b1[1], b1[2]);
+  min_image(C.cell, c1[0], c1[1], c1[2]);
+  // present positions relative to their centre of mass
+  double A1[3], B1[3], C1[3];
+  for (int r = 0; r < 3; ++r) {
+    const double com = mh * (b1[r] + c1[r]) / mt;
+    A1[r] = -com, B1[r] = b1[r] - com, C1[r] = c1[r] - com;
+  }
+  double ez[3], ex[3], ey[3];
+  cross3d(b0, c0, ez);
+  cross3d(A1, ez, ex);
+  cross3d(ez, ex, ey);
+  unit3d(ex);
+  unit3d(ey);
+  unit3d(ez);
+  const double xb0 = dot3d(b0, ex), yb0 = dot3d(b0, ey), xc0 = dot3d(c0, ex), yc0 = dot3d(c0, ey);
+  const double za1 = dot3d(A1, ez);
+  const double xb1 = dot3d(B1, ex), yb1 = dot3d(B1, ey), zb1 = dot3d(B1, ez);
+  const double xc1 = dot3d(C1, ex), yc1 = dot3d(C1, ey), zc1 = dot3d(C1, ez);
+  const double sinphi = za1 / ra;
+  const double cphi2 = 1 - sinphi * sinphi;
+  const double cosphi = sqrt(fmax(cphi2, 0.0));
+  const double sinpsi = (zb1 - zc1) / (2 * rc * cosphi);
+  const double cpsi2 = 1 - sinpsi * sinpsi;
+  const double cospsi = sqrt(fmax(cpsi2, 0.0));
+  const double ya2 = ra * cosphi, xb2 = -rc * cospsi;
+  const double t1 = -rb * cosphi, t2 = rc * sinpsi * sinphi;
+  const double yb2 = t1 - t2, yc2 = t1 + t2;
+  const double alpha = xb2 * (xb0 - xc0) + yb0 * yb2 + yc0 * yc2;
+  const double beta = xb2 * (yc0 - yb0) + xb0 * yb2 + xc0 * yc2;
+  const double gamma = xb0 * yb1 - xb1 * yb0 + xc0 * yc1 - xc1 * yc0;
+  const double ab2 = alpha * alpha + beta * beta;
+  const double disc = ab2 - gamma * gamma;
+  if (!(cphi2 > 0) || !(cpsi2 >= 0) || !(disc >= 0) || !(ab2 > 0)) {   // moved too far in one step for a rigid water
+    atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), kErrShake);
+    return;
+  }
+  const double sinth = (alpha * gamma - beta * sqrt(disc)) / ab2;
+  const double costh = sqrt(fmax(1 - sinth * sinth, 0.0));
+  const double a3[3] = {-ya2 * sinth, ya2 * costh, za1};
+  const double b3[3] = {xb2 * costh - yb2 * sinth, xb2 * sinth + yb2 * costh, zb1};
+  const double c3[3] = {-xb2 * costh - yc2 * sinth, -xb2 * sinth + yc2 * costh, zc1};
+  for (int r = 0; r < 3; ++r) {
+    const double da = a3[0] * ex[r] + a3[1] * ey[r] + a3[2] * ez[r] - A1[r];
+    const double db = b3[0] * ex[r] + b3[1] * ey[r] + b3[2] * ez[r] - B1[r];
+    const double dc = c3[0] * ex[r] + c3[1] * ey[r] + c3[2] * ez[r] - C1[r];
+    x[3 * ia + r] += da, x[3 * ib + r] += db, x[3 * ic + r] += dc;
+    if (h > 0) v[3 * ia + r] += da / h, v[3 * ib + r] += db / h, v[3 * ic + r] += dc / h;
+  }
+}
+
 // SHAKE on each cluster (Gauss-Seidel along the reference vectors, tol 1e-8 relative; core/src/constraints.cpp:196-230),
 // then v += (x - x_before) / h when h > 0.
 __global__ void k_shake(ConsArgs C, double* __restrict__ x, const double* __restrict__ x0, double* __restrict__ v, double h, int* counters) {
@@ -199,7 +291,8 @@ __global__ void k_shake(ConsArgs C, double* __restrict__ x, const double* __rest
   if (cc < C.e1) return shake_star<1>(C, cc, x, x0, v, h, counters);
   if (cc < C.e2) return shake_star<2>(C, cc, x, x0, v, h, counters);
   if (cc < C.e3) return shake_star<3>(C, cc, x, x0, v, h, counters);
-  const int c = cc - C.e3;
+  if (cc < C.e4) return settle_water(C, cc - C.e3, x, x0, v, h, counters);
+  const int c = cc - C.e4;
   const int k0 = C.cl_start[c], k1 = C.cl_start[c + 1], a0 = C.cl_atom0[c], a1 = C.cl_atom0[c + 1];
   const int na = a1 - a0, nk = k1 - k0;
   double px[kMaxClAtoms][3], ox[kMaxClAtoms][3], bx[kMaxClAtoms][3], im[kMaxClAtoms];
@@ -254,16 +347,22 @@ __global__ void k_shake(ConsArgs C, double* __restrict__ x, const double* __rest
 // The velocity update of one atom before RATTLE: a kick (v += hk kAcc f / m) or the Langevin O step
 // (v = c1 v + c2 sqrt(kB T kAcc / m) N(0, 1), Philox normals keyed by (seed, step, atom)).
 struct VelOp {
-  int kind;                  // 0 none, 1 kick, 2 Langevin O
+  int kind;                  // 0 none, 1 kick (f, and f2 when not null), 2 Langevin O
   const double* f;
   double hk;
   double c1, c2;
   uint64_t seed;
+  const double* f2;
+  double hk2;
 };
 __device__ __forceinline__ void vel_op(const VelOp& op, int g, double* vv, const double* __restrict__ invm, const double* sc) {
   if (op.kind == 1) {
     const double a = op.hk * kAcc * invm[g];
     for (int r = 0; r < 3; ++r) vv[r] += a * op.f[3 * g + r];
+    if (op.f2) {
+      const double a2 = op.hk2 * kAcc * invm[g];
+      for (int r = 0; r < 3; ++r) vv[r] += a2 * op.f2[3 * g + r];
+    }
   } else if (op.kind == 2) {
     double z[4];
     normals4(op.seed, (uint64_t)sc[kScStep], uint32_t(g), 0x4C414E47u, z);
@@ -339,6 +438,65 @@ __device__ void rattle_star(const ConsArgs& C, int s, const double* __restrict__
     }
 }
 
+// RATTLE on a rigid water in registers: Gauss-Seidel over (O, H1), (O, H2), (H1, H2).
+__device__ void rattle_water(const ConsArgs& C, int wi, const double* __restrict__ x, double* __restrict__ v, const VelOp& op, const double* sc,
+                             double h, double w[6], int* counters) {
+  const int4 at = C.water[wi];
+  const double2 geo = C.water_geo[wi];
+  const int ids[3] = {at.x, at.y, at.z};
+  const int pi[3] = {0, 0, 1}, pj[3] = {1, 2, 2};
+  const double dd[3] = {geo.x * geo.x, geo.x * geo.x, geo.y * geo.y};
+  double pv[3][3], im[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int g = ids[a];
+    for (int r = 0; r < 3; ++r) pv[a][r] = v[3 * g + r];
+    vel_op(op, g, pv[a], C.invm, sc);
+    im[a] = C.invm[g];
+  }
+  double rr[3][3], lam[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int gi = ids[pi[k]], gj = ids[pj[k]];
+    double d0 = x[3 * gi] - x[3 * gj], d1 = x[3 * gi + 1] - x[3 * gj + 1], d2v = x[3 * gi + 2] - x[3 * gj + 2];
+    min_image(C.cell, d0, d1, d2v);
+    rr[k][0] = d0, rr[k][1] = d1, rr[k][2] = d2v;
+    lam[k] = 0;
+  }
+  bool done = false;
+  for (int it = 0; it < kShakeIter && !done; ++it) {
+    done = true;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int i = pi[k], j = pj[k];
+      const double rv = rr[k][0] * (pv[i][0] - pv[j][0]) + rr[k][1] * (pv[i][1] - pv[j][1]) + rr[k][2] * (pv[i][2] - pv[j][2]);
+      if (fabs(rv) <= kShakeTol * dd[k]) continue;
+      done = false;
+      const double g = -rv / ((im[i] + im[j]) * dd[k]);
+      lam[k] += g;
+      for (int r = 0; r < 3; ++r) {
+        pv[i][r] += g * im[i] * rr[k][r];
+        pv[j][r] -= g * im[j] * rr[k][r];
+      }
+    }
+  }
+  if (!done) atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), kErrShake);
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+    for (int r = 0; r < 3; ++r) v[3 * ids[a] + r] = pv[a][r];
+  if (h > 0)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double sk = 2 * lam[k] / (h * kAcc);
+      w[0] += sk * rr[k][0] * rr[k][0];
+      w[1] += sk * rr[k][1] * rr[k][1];
+      w[2] += sk * rr[k][2] * rr[k][2];
+      w[3] += sk * rr[k][0] * rr[k][1];
+      w[4] += sk * rr[k][0] * rr[k][2];
+      w[5] += sk * rr[k][1] * rr[k][2];
+    }
+}
+
 // Velocity update then RATTLE in one launch: threads [0, ncl) take one constraint cluster each (its atoms' update, then
 // the relative velocity along each constraint removed, core/src/constraints.cpp:232-269; star clusters in registers);
 // threads [ncl, ncl + nfree) update one unconstrained atom each. With h > 0 the impulses are read as forces over a half kick and their virial
@@ -356,8 +514,9 @@ __global__ void k_vel_rattle(ConsArgs C, int nfree, const int* __restrict__ free
   if (c < C.e1) rattle_star<1>(C, c, x, v, op, sc, h, w, counters);
   else if (c < C.e2) rattle_star<2>(C, c, x, v, op, sc, h, w, counters);
   else if (c < C.e3) rattle_star<3>(C, c, x, v, op, sc, h, w, counters);
+  else if (c < C.e4) rattle_water(C, c - C.e3, x, v, op, sc, h, w, counters);
   else if (c < C.ncl) {
-    const int cg = c - C.e3;
+    const int cg = c - C.e4;
     const int k0 = C.cl_start[cg], k1 = C.cl_start[cg + 1], a0 = C.cl_atom0[cg], a1 = C.cl_atom0[cg + 1];
     const int na = a1 - a0, nk = k1 - k0;
     double pv[kMaxClAtoms][3], im[kMaxClAtoms];
@@ -568,8 +727,9 @@ struct Stepper {
   int nfree = 0;
   DevBuf<Chain> chain;
   DevBuf<int> cl_start, cl_atom0, cl_atoms;
-  DevBuf<int4> cons, star;
+  DevBuf<int4> cons, star, water;
   DevBuf<double4> star_d2;
+  DevBuf<double2> water_g;
   DevBuf<double> d2;
   DevBuf<double2> draws;
   long long draws_first = 0, draws_count = 0;
@@ -656,8 +816,9 @@ struct Stepper {
     std::vector<int> st{0}, a0{0}, atoms, gen_atoms;   // atoms: every constrained atom; gen_atoms: the general clusters
     std::vector<int4> cv;
     std::vector<double> dv;
-    std::vector<int4> star_at[3];
+    std::vector<int4> star_at[3], water_at;
     std::vector<double4> star_dd[3];
+    std::vector<double2> water_geo;
     for (auto& [r, ks] : comp_cons) {
       if (int(ks.size()) > kMaxClCons) throw ModelError(CAPS_GPU_EINVAL, "a constraint cluster has more than 8 atoms or constraints (the device SHAKE takes bonds to hydrogen and rigid waters)");
       // a star: 1-3 constraints that all share one atom, each with a distinct partner
@@ -696,6 +857,27 @@ struct Stepper {
         star_dd[ks.size() - 1].push_back(make_double4(dd[0], dd[1], dd[2], 0.0));
         continue;
       }
+      if (ks.size() == 3) {
+        // a rigid water: the atom shared by two equal constraints (O) and two partners of equal mass joined by the third
+        const Cn& k0 = cs[size_t(ks[0])];
+        const Cn& k1 = cs[size_t(ks[1])];
+        const Cn& k2 = cs[size_t(ks[2])];
+        int ox = -1;
+        for (int cand : {k0.i, k0.j})
+          if ((k1.i == cand || k1.j == cand) && !(k2.i == cand || k2.j == cand)) ox = cand;
+        if (ox >= 0) {
+          const int h1 = k0.i == ox ? k0.j : k0.i, h2 = k1.i == ox ? k1.j : k1.i;
+          const bool tri = ((k2.i == h1 && k2.j == h2) || (k2.i == h2 && k2.j == h1)) && h1 != h2;
+          const bool eq_len = std::fabs(k0.d - k1.d) <= 1e-12 * k0.d;
+          const bool eq_mass = E.h_mass_[size_t(h1)] == E.h_mass_[size_t(h2)];
+          if (tri && eq_len && eq_mass) {
+            water_at.push_back(make_int4(ox, h1, h2, -1));
+            water_geo.push_back(make_double2(k0.d, k2.d));
+            atoms.push_back(ox), atoms.push_back(h1), atoms.push_back(h2);
+            continue;
+          }
+        }
+      }
       std::vector<int> loc;
       auto local = [&](int a) {
         for (size_t q = 0; q < loc.size(); ++q)
@@ -731,6 +913,13 @@ struct Stepper {
     }
     C.star = star.p;
     C.star_d2 = star_d2.p;
+    C.e4 = C.e3 + int(water_at.size());
+    if (!water_at.empty()) {
+      water.upload(water_at, E.stream_);
+      water_g.upload(water_geo, E.stream_);
+    }
+    C.water = water.p;
+    C.water_geo = water_g.p;
     std::vector<char> in_cluster(static_cast<size_t>(n), 0);
     for (int a : atoms) in_cluster[size_t(a)] = 1;
     std::vector<int> fa;
@@ -745,7 +934,7 @@ struct Stepper {
       cons.upload(cv, E.stream_);
       d2.upload(dv, E.stream_);
     }
-    C.ncl = C.e3 + int(st.size()) - 1;
+    C.ncl = C.e4 + int(st.size()) - 1;
     C.cl_start = cl_start.p;
     C.cl_atom0 = cl_atom0.p;
     C.cl_atoms = cl_atoms.p;
@@ -826,9 +1015,9 @@ struct Stepper {
   void ke_launch(const KeArgs& A) { k_ke<<<nparts, 256, 0, E.stream_>>>(A); }
   void ke(int slot, bool tensor) { ke_launch(ke_args(slot, tensor)); }
   // half kick, then drift with SHAKE; `scale` applies the thermostat's pending factor first
-  void kick_drift(double hk, double hd, bool scale, bool zero_cw) {
-    k_kick_drift<<<blocks(size_t(n), 256), 256, 0, E.stream_>>>(n, x.p, v.p, x0.p, E.d_f_.p, invm.p, hk, hd, sc.p, scale ? 1 : 0, zero_cw ? 1 : 0,
-                                                                 E.d_counters_.p);
+  void kick_drift(double hk, double hd, bool scale, bool zero_cw, const double* f = nullptr, const double* f2 = nullptr, double hk2 = 0) {
+    k_kick_drift<<<blocks(size_t(n), 256), 256, 0, E.stream_>>>(n, x.p, v.p, x0.p, f ? f : E.d_f_.p, invm.p, hk, f2, hk2, hd, sc.p, scale ? 1 : 0,
+                                                                 zero_cw ? 1 : 0, E.d_counters_.p);
     if (ncons) k_shake<<<blocks(size_t(C.ncl), 128), 128, 0, E.stream_>>>(C, x.p, x0.p, v.p, hd, E.d_counters_.p);
   }
   // a velocity update, then RATTLE (constraint virial summed when h > 0)
@@ -839,12 +1028,24 @@ struct Stepper {
     }
     k_vel_rattle<<<blocks(size_t(C.ncl + nfree), 128), 128, 0, E.stream_>>>(C, nfree, free_atoms.p, x.p, v.p, op, h, sc.p, E.d_counters_.p);
   }
-  VelOp kick_op(double hk) const { return VelOp{1, E.d_f_.p, hk, 0, 0, 0}; }
+  VelOp kick_op(double hk) const { return VelOp{1, E.d_f_.p, hk, 0, 0, 0, nullptr, 0}; }
   void rattle(double h) {   // RATTLE alone (initial velocities)
-    if (ncons) vel_rattle(VelOp{0, nullptr, 0, 0, 0, 0}, h);
+    if (ncons) vel_rattle(VelOp{0, nullptr, 0, 0, 0, 0, nullptr, 0}, h);
   }
   void scale_v() { k_scale_v<<<blocks(size_t(3) * n, 256), 256, 0, E.stream_>>>(n, v.p, sc.p); }
-  void forces(bool ener, bool vir) { E.forces(x.p, ener, vir, true); }
+  // r-RESPA force sets (dynamics.cpp:113-122, 318-326): the non-bonded (slow) and bonded (fast) parts in their own
+  // arrays; the evaluation at the end of a step computes both, with energies and virial summed over the two.
+  DevBuf<double> f_slow, f_fast;
+  int respa = 1;
+  void forces(bool ener, bool vir) {
+    if (respa > 1) {
+      E.forces(x.p, ener, vir, true, 2, f_slow.p, true);
+      E.forces(x.p, ener, vir, false, 1, f_fast.p, false);
+      return;
+    }
+    E.forces(x.p, ener, vir, true);
+  }
+  void fast_forces() { E.forces(x.p, false, false, false, 1, f_fast.p, true); }
 
   // One MD step (dynamics.cpp:606-666), energies and virial on request. Kernel sequence per step: NVT Nose-Hoover
   // KE+chain, kick+drift, SHAKE, forces, kick+RATTLE, KE+chain, scale; Bussi step-begin, kick+drift, SHAKE, forces,
@@ -852,13 +1053,33 @@ struct Stepper {
   // kick+RATTLE.
   void step(bool ener, bool vir) {
     const double dt = o.dt;
+    if (respa > 1) {
+      // r-RESPA (dynamics.cpp:643-657): outer half kick with the slow forces; `respa` velocity-Verlet steps of dt/respa
+      // with the fast ones; outer half kick. Adjacent kicks with the same forces are merged.
+      const double h = dt / respa;
+      k_step_begin<<<1, 1, 0, E.stream_>>>(sc.p, o.temperature, o.temperature_end, (long long)o.steps, ndof);
+      kick_drift(0.5 * dt, h, false, true, f_slow.p, f_fast.p, 0.5 * h);
+      for (int j = 0; j + 1 < respa; ++j) {
+        fast_forces();
+        kick_drift(h, h, false, false, f_fast.p);
+      }
+      forces(ener, vir);
+      vel_rattle(VelOp{1, f_fast.p, 0.5 * h, 0, 0, 0, f_slow.p, 0.5 * dt}, dt);
+      if (bussi) {
+        KeArgs A = ke_args(kScKE, false);
+        A.then = kThenBussi;
+        ke_launch(A);
+        scale_v();
+      }
+      return;
+    }
     if (langevin) {
       const double c1 = std::exp(-dt / std::max(o.tau_t, 1e-9)), c2 = std::sqrt(1 - c1 * c1);
       kick_drift(0.5 * dt, 0.5 * dt, false, true);
       KeArgs A = ke_args(kScKE0, false);
       A.begin = 1;
       ke_launch(A);
-      vel_rattle(VelOp{2, nullptr, 0, c1, c2, o.seed}, 0);
+      vel_rattle(VelOp{2, nullptr, 0, c1, c2, o.seed, nullptr, 0}, 0);
       A = ke_args(kScKE, false);
       A.then = kThenBath;
       ke_launch(A);
@@ -910,7 +1131,10 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
   if (n_ < 2) throw ModelError(CAPS_GPU_EFIELD, "dynamics needs at least two atoms");
   if (o.dt <= 0 || o.dt > 50) throw ModelError(CAPS_GPU_EINVAL, "time step must be in (0, 50] fs");
   if (o.steps < 0) throw ModelError(CAPS_GPU_EINVAL, "the number of steps must be 0 or more");
-  if (o.respa > 1) throw ModelError(CAPS_GPU_EINVAL, "r-RESPA is not on the device path yet");
+  if (o.respa < 0 || o.respa > 16) throw ModelError(CAPS_GPU_EINVAL, "r-RESPA inner steps must be 1 … 16");
+  if (o.respa > 1 && (o.thermostat == 2 || o.thermostat == 3)) throw ModelError(CAPS_GPU_EINVAL, "r-RESPA runs with the Bussi thermostat or none");
+  if (o.respa > 1 && o.constraints) throw ModelError(CAPS_GPU_EINVAL, "r-RESPA and bond constraints are alternatives: choose one");
+  if (o.respa > 1 && o.barostat) throw ModelError(CAPS_GPU_EINVAL, "the device path runs r-RESPA without a barostat");
   if (o.thermostat < 0 || o.thermostat > 3) throw ModelError(CAPS_GPU_EINVAL, "unknown thermostat");
   if (o.barostat != 0 && o.barostat != 1) throw ModelError(CAPS_GPU_EINVAL, "the device path takes stochastic cell rescaling or no barostat");
   if (o.barostat == 1 && o.thermostat == 0) throw ModelError(CAPS_GPU_EINVAL, "stochastic cell rescaling needs a thermostat");
@@ -932,6 +1156,11 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
   S.part.alloc(size_t(7) * S.nparts);
   S.done.alloc(1);
   S.done.zero(stream_);
+  S.respa = std::max(1, o.respa);
+  if (S.respa > 1) {
+    S.f_slow.alloc(n3);
+    S.f_fast.alloc(n3);
+  }
   CK(cudaMallocHost(&S.h_sc, sizeof(double) * kScNum));
   CK(cudaMallocHost(&S.h_chain, sizeof(Chain)));
   S.nhc = o.thermostat == 3;

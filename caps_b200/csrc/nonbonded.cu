@@ -184,8 +184,10 @@ void Engine::pair_forces(bool ener, bool vir) {
 
 // One force evaluation on device positions d_x (AoS, 3 n): accumulators cleared, list checked / rebuilt, every term,
 // forces reduced into d_f_ (AoS doubles). Asynchronous on stream_.
-void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild) {
-  const bool nonb = (opt_.parts & 2) != 0;
+void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild, int parts, double* d_out, bool clear_energies) {
+  const int pm = parts < 0 ? opt_.parts : parts;
+  const bool nonb = (pm & 2) != 0;
+  double* out = d_out ? d_out : d_f_.p;
   if (mixed_) {
     CK(cudaMemsetAsync(d_F_.p, 0, d_F_.n * sizeof(long long), stream_));
     if (nonb) CK(cudaMemsetAsync(d_Fs_.p, 0, d_Fs_.n * sizeof(long long), stream_));
@@ -193,13 +195,13 @@ void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild) 
     CK(cudaMemsetAsync(d_Fd_.p, 0, d_Fd_.n * sizeof(double), stream_));
     if (nonb) CK(cudaMemsetAsync(d_Fsd_.p, 0, d_Fsd_.n * sizeof(double), stream_));
   }
-  if (ener || vir) {
+  if ((ener || vir) && clear_energies) {
     CK(cudaMemsetAsync(d_efix_.p, 0, d_efix_.n * sizeof(long long), stream_));
     CK(cudaMemsetAsync(d_edbl_.p, 0, d_edbl_.n * sizeof(double), stream_));
   }
   // Three branches: bonded terms and PME beside the list and pair kernels. All add into order-free fixed-point (or
   // atomic FP64) sums, so how the branches interleave does not change the mixed path's result.
-  fork(0, [&] { bonded_forces(d_x, ener, vir); });
+  fork(0, [&] { bonded_forces(d_x, ener, vir, pm); });
   const bool pme = nonb && pme_;
   if (pme) fork(1, [&] { pme_forces(d_x, ener, vir); });
   if (nonb) {
@@ -224,8 +226,8 @@ void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild) 
   join(0);
   if (pme) join(1);
   const size_t ns = size_t(nsc_cap_) * kScAtoms;
-  if (mixed_) k_reduce_f32<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_F_.p, d_Fs_.p, int(ns), d_iperm_.p, d_f_.p, nonb ? 1 : 0);
-  else k_reduce_f64<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_Fd_.p, d_Fsd_.p, int(ns), d_iperm_.p, d_f_.p, nonb ? 1 : 0);
+  if (mixed_) k_reduce_f32<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_F_.p, d_Fs_.p, int(ns), d_iperm_.p, out, nonb ? 1 : 0);
+  else k_reduce_f64<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_Fd_.p, d_Fsd_.p, int(ns), d_iperm_.p, out, nonb ? 1 : 0);
   CK(cudaGetLastError());
 }
 

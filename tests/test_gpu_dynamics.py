@@ -48,6 +48,19 @@ def test_fp64_run_follows_reference(thermostat):
     assert np.max(np.abs(out["x"] - r["x"])) < 1e-8
 
 
+@pytest.mark.parametrize("thermostat", ["none", "bussi"])
+def test_fp64_respa_run_follows_reference(thermostat):
+    """r-RESPA (dynamics.cpp:643-657): bonded forces at dt / 3, non-bonded ones at dt; the reference's thermo rows."""
+    ref = _ref()
+    fx = load("ps_small")
+    o = _opts(thermostat=thermostat, respa=3, dt=1.5, steps=20)
+    ev = Evaluator(fx.ff, o.energy)
+    out = ev.run(fx.x, fx.cell, o)
+    r = ref.run(fx.ff, fx.x, fx.cell, o)
+    _compare(out["thermo"], r["thermo"], 1e-9)
+    assert np.max(np.abs(out["x"] - r["x"])) < 1e-8
+
+
 def test_fp64_shake_run_follows_reference():
     ref = _ref()
     fx = load("ps_small")
