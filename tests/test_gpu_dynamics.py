@@ -61,6 +61,29 @@ def test_fp64_respa_run_follows_reference(thermostat):
     assert np.max(np.abs(out["x"] - r["x"])) < 1e-8
 
 
+def test_fp64_rigid_water_settle_follows_reference_shake():
+    """Rigid SPC/E waters: the device solves them with SETTLE (exact distances), the reference with SHAKE (1e-8 relative
+    tolerance); from the same equilibrated state the thermo rows agree to SHAKE's tolerance."""
+    from caps_b200.systems import spce_water
+    ref = _ref()
+    ff, x, cell = spce_water(216, seed=5)
+    eo = EnergyOptions(cutoff=8.0, skin=1.0, electrostatics="pme", pme_order=4, precision="double")
+    eq = DynamicsOptions(dt=0.5, steps=400, temperature=300.0, thermostat="langevin", tau_t=20.0, constraints="h-bonds",
+                         thermo_every=400, seed=9, energy=eo)
+    r0 = ref.run(ff, x, cell, eq)
+    o = DynamicsOptions(dt=1.0, steps=20, temperature=300.0, thermostat="none", constraints="h-bonds", thermo_every=5, seed=9,
+                        energy=eo)
+    ev = Evaluator(ff, eo)
+    out = ev.run(r0["x"], cell, o, v=r0["v"])
+    r = ref.run(ff, r0["x"], cell, o, v=r0["v"])
+    _compare(out["thermo"], r["thermo"], 1e-6)
+    X = out["x"].reshape(-1, 3, 3)
+    d_oh = np.linalg.norm(X[:, 1:] - X[:, :1], axis=2)
+    d_hh = np.linalg.norm(X[:, 2] - X[:, 1], axis=1)
+    assert np.max(np.abs(d_oh - 1.0)) < 1e-10
+    assert np.max(np.abs(d_hh - 2 * np.sin(np.radians(109.47) / 2))) < 1e-10
+
+
 def test_fp64_shake_run_follows_reference():
     ref = _ref()
     fx = load("ps_small")
