@@ -4,8 +4,8 @@ The product is the C ABI library caps_b200/libcaps_b200.so (include/caps_gpu.h) 
 this package binds it with the reference's own names: Evaluator, EnergyOptions, DynamicsOptions, run_dynamics.
 """
 from .engine import (DeviceError, DynamicsCancelled, DynamicsOptions, EnergyOptions, Evaluator, FieldError,  # noqa: F401
-                     cell_array, run_dynamics)
+                     cell_array, run_batch, run_dynamics)
 from .forcefield import ForceField, read_capsff  # noqa: F401
 
-__all__ = ["Evaluator", "EnergyOptions", "DynamicsOptions", "run_dynamics", "ForceField", "read_capsff", "FieldError",
+__all__ = ["Evaluator", "EnergyOptions", "DynamicsOptions", "run_dynamics", "run_batch", "ForceField", "read_capsff", "FieldError",
            "DynamicsCancelled", "DeviceError", "cell_array"]

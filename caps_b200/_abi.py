@@ -59,7 +59,7 @@ class MdOpts(C.Structure):
         ("tau_p", C.c_double), ("compressibility", C.c_double), ("barostat_every", C.c_int32),
         ("constraints", C.c_int32), ("new_velocities", C.c_int32), ("seed", C.c_uint64), ("thermo_every", C.c_int32),
         ("frame_every", C.c_int32), ("step_offset", C.c_int64), ("respa", C.c_int32),
-        ("is_hydrogen", P), ("is_oxygen", P),
+        ("is_hydrogen", P), ("is_oxygen", P), ("respa_split", C.c_int32),
     ]
 
 
@@ -90,7 +90,7 @@ DIAG_EXPORTS = ["caps_gpu_diag_set_timing", "caps_gpu_diag_last_step_ms", "caps_
 
 EXPORTS = [
     "caps_gpu_abi_version", "caps_gpu_device_count", "caps_gpu_create", "caps_gpu_set_options", "caps_gpu_energies",
-    "caps_gpu_compute", "caps_gpu_compute_device", "caps_gpu_list_builds", "caps_gpu_run",
+    "caps_gpu_compute", "caps_gpu_compute_device", "caps_gpu_list_builds", "caps_gpu_run", "caps_gpu_run_batch",
     "caps_gpu_last_steps_per_second", "caps_gpu_destroy", "caps_gpu_error",
 ]
 
@@ -119,6 +119,8 @@ def load(path: Path | None = None) -> C.CDLL:
                                  C.c_char_p, C.c_int32]
     lib.caps_gpu_last_steps_per_second.restype = C.c_double
     lib.caps_gpu_last_steps_per_second.argtypes = [C.c_void_p]
+    lib.caps_gpu_run_batch.argtypes = [C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int32, PROGRESS_FN, FRAME_FN,
+                                       C.POINTER(C.c_void_p)]
     lib.caps_gpu_destroy.argtypes = [C.c_void_p]
     lib.caps_gpu_error.restype = C.c_char_p
     lib.caps_gpu_error.argtypes = [C.c_void_p]

@@ -13,7 +13,9 @@ namespace capsb {
 void Engine::bonded_forces(const double* d_x, bool ener, bool vir, int parts) {
   BondedArgs A{d_x, dcell_, EnergySink{d_efix_.p, d_edbl_.p}, mixed_ ? 1 : 0};
   const int T = 256;
-  const bool bonded = (parts & 1) != 0, nonb = (parts & 2) != 0;
+  // parts: 1 bonded terms, 2 short-range non-bonded (1-4 pairs; DSF exclusion corrections), 4 long-range (the PME
+  // exclusion corrections)
+  const bool bonded = (parts & 1) != 0, nonb = (parts & 2) != 0, excl = (parts & (pme_ ? 4 : 2)) != 0;
   auto nblk = [&](int cnt) { return std::min(blocks_for(size_t(std::max(cnt, 1)), T), dev_sms_ * 4); };
 #define LAUNCH3(K, S, cnt, ...)                                                                                     \
   do {                                                                                                              \
@@ -38,7 +40,7 @@ void Engine::bonded_forces(const double* d_x, bool ener, bool vir, int parts) {
     if (nonb && np14_)
       LAUNCH3(k_pairs14, S, np14_, np14_, d_p14_ij_.p, p14_scaled_ ? d_p14_scale_.p : nullptr, lj14_, d_type_.p, nt_, d_lj14_.p,
               opt_.force_cap > 0 ? (const double4*)d_cap14_.p : (const double4*)nullptr, A, F);
-    if (nonb && coul_ && nx_) {
+    if (excl && coul_ && nx_) {
       ExclArgs E{d_excl_ij_.p, d_excl_f_.p, d_q_.p, d_gtab_.p, ghi_, rc_, rc_ * rc_, kappa_, dsf_e0_, dsf_f0_, pme_ ? 1 : 0};
       LAUNCHX(S, nx_, E, A, F);
     }

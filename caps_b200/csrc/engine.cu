@@ -740,6 +740,22 @@ int32_t caps_gpu_run(caps_gpu_engine* e, caps_gpu_state* state, const caps_gpu_m
   return rc;
 }
 
+int32_t caps_gpu_run_batch(caps_gpu_engine* const* engines, caps_gpu_state* const* states, const caps_gpu_md_opts* const* md, int32_t count,
+                           caps_gpu_progress_fn progress, caps_gpu_frame_fn frame, void* const* user) {
+  if (!engines || !states || !md || count < 1) return CAPS_GPU_EINVAL;
+  std::vector<capsb::Engine*> es;
+  for (int32_t r = 0; r < count; ++r) {
+    if (!engines[r] || !states[r] || !md[r] || !states[r]->x || !states[r]->cell) return CAPS_GPU_EINVAL;
+    for (int32_t q = 0; q < r; ++q)
+      if (engines[q] == engines[r]) {
+        engines[0]->err = "caps_gpu_run_batch: an engine appears twice in the batch";
+        return CAPS_GPU_EINVAL;
+      }
+    es.push_back(engines[r]->e.get());
+  }
+  return guard(engines[0], [&] { capsb::run_batch(es, states, md, progress, frame, user); });
+}
+
 double caps_gpu_last_steps_per_second(const caps_gpu_engine* e) { return e ? e->e->last_steps_per_second() : 0.0; }
 
 void caps_gpu_destroy(caps_gpu_engine* e) { delete e; }

@@ -106,6 +106,7 @@ class Engine {
   void compute_dev(const double* d_x, const double* cell, double* d_f, caps_gpu_terms* out);
   int list_builds();   // list builds so far (counted on the device)
   void run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progress_fn progress, caps_gpu_frame_fn frame, void* user, std::string* report);
+  void validate_md(const caps_gpu_md_opts& o) const;   // the dynamics options the device path takes (throws otherwise)
   double last_steps_per_second() const { return last_sps_; }
   // measurement support (include/caps_gpu_diag.h)
   void set_timing(int64_t flush_bytes) { timing_flush_ = flush_bytes; }
@@ -124,12 +125,16 @@ class Engine {
 
  private:
   friend struct Stepper;
+  friend struct MdRun;
+  friend void run_batch(const std::vector<Engine*>&, caps_gpu_state* const*, const caps_gpu_md_opts* const*, caps_gpu_progress_fn,
+                        caps_gpu_frame_fn, void* const*);
   void setup_ff(const caps_gpu_ff* ff);
   void setup_options();
   void set_cell(const double* cell);
   void ensure_list_capacity();
-  // One force evaluation up to the AoS doubles d_out (d_f_ by default), async. parts: 1 bonded, 2 non-bonded, 3 both (-1:
-  // the options' parts); clear_energies = false adds this evaluation's energies and virial to the previous one's.
+  // One force evaluation up to the AoS doubles d_out (d_f_ by default), async. parts: a mask of 1 bonded, 2 short-range
+  // non-bonded, 4 long-range (PME) terms (-1: the options' parts); clear_energies = false adds this evaluation's
+  // energies and virial to the previous one's.
   void forces(const double* d_x, bool ener, bool vir, bool check_rebuild, int parts = -1, double* d_out = nullptr, bool clear_energies = true);
   // Concurrent branches of a force evaluation: `launch` runs with stream_ pointing at side stream k, after everything
   // queued on the main stream so far; join(k) makes the main stream wait for it. Captured, these are graph branches.
@@ -227,5 +232,9 @@ class Engine {
   DevBuf<unsigned char> d_flush_;
   int dev_sms_ = 148;
 };
+
+// Independent replicas (one engine each, on the current device) advanced in lock step; integrate.cu.
+void run_batch(const std::vector<Engine*>& es, caps_gpu_state* const* states, const caps_gpu_md_opts* const* mds, caps_gpu_progress_fn progress,
+               caps_gpu_frame_fn frame, void* const* users);
 
 }  // namespace capsb

@@ -1035,17 +1035,19 @@ struct Stepper {
   void scale_v() { k_scale_v<<<blocks(size_t(3) * n, 256), 256, 0, E.stream_>>>(n, v.p, sc.p); }
   // r-RESPA force sets (dynamics.cpp:113-122, 318-326): the non-bonded (slow) and bonded (fast) parts in their own
   // arrays; the evaluation at the end of a step computes both, with energies and virial summed over the two.
+  // The PME split puts the reciprocal sum (and its exclusion corrections) in the slow set and every other term in the
+  // fast one. Part masks as Engine::forces takes them.
   DevBuf<double> f_slow, f_fast;
-  int respa = 1;
+  int respa = 1, slow_parts = 6, fast_parts = 1;
   void forces(bool ener, bool vir) {
     if (respa > 1) {
-      E.forces(x.p, ener, vir, true, 2, f_slow.p, true);
-      E.forces(x.p, ener, vir, false, 1, f_fast.p, false);
+      E.forces(x.p, ener, vir, true, slow_parts, f_slow.p, true);
+      E.forces(x.p, ener, vir, true, fast_parts, f_fast.p, false);
       return;
     }
     E.forces(x.p, ener, vir, true);
   }
-  void fast_forces() { E.forces(x.p, false, false, false, 1, f_fast.p, true); }
+  void fast_forces() { E.forces(x.p, false, false, true, fast_parts, f_fast.p, true); }
 
   // One MD step (dynamics.cpp:606-666), energies and virial on request. Kernel sequence per step: NVT Nose-Hoover
   // KE+chain, kick+drift, SHAKE, forces, kick+RATTLE, KE+chain, scale; Bussi step-begin, kick+drift, SHAKE, forces,
@@ -1125,9 +1127,7 @@ struct Stepper {
   }
 };
 
-void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progress_fn progress, caps_gpu_frame_fn frame, void* user, std::string* report) {
-  const auto t_enter = std::chrono::steady_clock::now();
-  const caps_gpu_md_opts& o = *md;
+void Engine::validate_md(const caps_gpu_md_opts& o) const {
   if (n_ < 2) throw ModelError(CAPS_GPU_EFIELD, "dynamics needs at least two atoms");
   if (o.dt <= 0 || o.dt > 50) throw ModelError(CAPS_GPU_EINVAL, "time step must be in (0, 50] fs");
   if (o.steps < 0) throw ModelError(CAPS_GPU_EINVAL, "the number of steps must be 0 or more");
@@ -1135,18 +1135,117 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
   if (o.respa > 1 && (o.thermostat == 2 || o.thermostat == 3)) throw ModelError(CAPS_GPU_EINVAL, "r-RESPA runs with the Bussi thermostat or none");
   if (o.respa > 1 && o.constraints) throw ModelError(CAPS_GPU_EINVAL, "r-RESPA and bond constraints are alternatives: choose one");
   if (o.respa > 1 && o.barostat) throw ModelError(CAPS_GPU_EINVAL, "the device path runs r-RESPA without a barostat");
+  if (o.respa_split != 0 && o.respa_split != 1) throw ModelError(CAPS_GPU_EINVAL, "unknown r-RESPA split");
   if (o.thermostat < 0 || o.thermostat > 3) throw ModelError(CAPS_GPU_EINVAL, "unknown thermostat");
   if (o.barostat != 0 && o.barostat != 1) throw ModelError(CAPS_GPU_EINVAL, "the device path takes stochastic cell rescaling or no barostat");
   if (o.barostat == 1 && o.thermostat == 0) throw ModelError(CAPS_GPU_EINVAL, "stochastic cell rescaling needs a thermostat");
-  set_cell(st->cell);
-  Stepper S(*this, o);
-  const size_t n3 = size_t(3) * n_;
+}
+
+// One replica's run_dynamics on the device: set-up to step 0 (start), one step (advance), the state back (finish).
+// Engine::run drives one; caps_gpu_run_batch drives several in lock step, their plain steps in one graph.
+struct MdRun {
+  Engine& E;
+  const caps_gpu_md_opts& o;
+  caps_gpu_state* st;
+  caps_gpu_progress_fn progress;
+  caps_gpu_frame_fn frame;
+  void* user;
+  Stepper S;
+  size_t n3;
+  std::vector<double> hv;
+  int thermo_every = 1, baro_every = 1;
+  long long kernels = 0, emits = 0, baro_steps = 0;
+  int generation = 0;   // bumped whenever this replica's captured step changes (its graphs are dropped)
+
+  MdRun(Engine& e, caps_gpu_state* state, const caps_gpu_md_opts* md, caps_gpu_progress_fn prog, caps_gpu_frame_fn fr, void* u)
+      : E(e), o(*md), st(state), progress(prog), frame(fr), user(u), S(e, *md), n3(size_t(3) * e.n_) {}
+
+  double host_ke(const std::vector<double>& vv) const {
+    double k = 0;
+    for (int i = 0; i < E.n_; ++i)
+      k += E.h_mass_[size_t(i)] * (vv[3 * i] * vv[3 * i] + vv[3 * i + 1] * vv[3 * i + 1] + vv[3 * i + 2] * vv[3 * i + 2]);
+    return 0.5 * k / kAcc;
+  }
+
+  void row(long long step, caps_gpu_thermo& r) {
+    caps_gpu_terms t{};
+    E.read_terms(&t, true, true);
+    const double* sc = S.h_sc;
+    for (int c = 0; c < 6; ++c) t.w[c] += sc[kScCW0 + c];
+    t.virial = t.w[0] + t.w[1] + t.w[2];
+    std::memset(&r, 0, sizeof r);
+    r.step = step + o.step_offset;
+    r.time_ps = double(step + o.step_offset) * o.dt * 1e-3;
+    r.target_temperature = (o.temperature_end >= 0 && o.steps > 0) ? o.temperature + (o.temperature_end - o.temperature) * double(step) / double(o.steps)
+                                                                  : o.temperature;
+    r.kinetic = sc[kScKE];
+    r.temperature = 2 * r.kinetic / (S.ndof * kB);
+    r.potential = t.bond + t.angle + t.dihedral + t.improper + t.vdw + t.coulomb;
+    r.total = r.potential + r.kinetic;
+    r.volume = E.dcell_.vol;
+    double mtot = 0;
+    for (double mm : E.h_mass_) mtot += mm;
+    r.density = mtot / kNA / (r.volume * 1e-24);
+    r.pressure = (2 * r.kinetic + t.virial) / (3 * r.volume) * kAtm;
+    for (int c = 0; c < 6; ++c) r.p[c] = (sc[kScKin0 + c] + t.w[c]) / r.volume * kAtm;
+    if (S.nhc) {
+      const Chain& ch = *S.h_chain;
+      const double kt = kB * r.target_temperature;
+      double e = S.ndof * kt * ch.eta[0] + 0.5 * ch.eta_mass[0] * ch.eta_dot[0] * ch.eta_dot[0];
+      for (int c = 1; c < 3; ++c) e += kt * ch.eta[c] + 0.5 * ch.eta_mass[c] * ch.eta_dot[c] * ch.eta_dot[c];
+      r.conserved = r.total + e;
+    } else {
+      r.conserved = r.total + sc[kScBath] + (o.barostat ? o.pressure * r.volume / kAtm : 0.0);
+    }
+    r.terms = t;
+  }
+  void sync_scalars() {
+    cudaStream_t stream_ = E.stream_;
+    CK(cudaMemcpyAsync(S.h_sc, S.sc.p, sizeof(double) * kScNum, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(S.h_chain, S.chain.p, sizeof(Chain), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(E.h_counters_, E.d_counters_.p, sizeof(int) * kCntNum, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(E.h_efix_, E.d_efix_.p, sizeof(long long) * kENumSlots, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(E.h_edbl_, E.d_edbl_.p, sizeof(double) * kENumSlots, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    E.check_errors();
+  }
+  void emit(long long step) {
+    S.ke(kScKE, true);
+    sync_scalars();
+    caps_gpu_thermo r;
+    row(step, r);
+    if (progress && progress(&r, user) != 0) throw ModelError(CAPS_GPU_ECANCEL, "dynamics cancelled");
+  }
+  void emit_frame(long long step) {
+    if (!frame || o.frame_every <= 0) return;
+    std::vector<double> hx(n3);
+    CK(cudaMemcpyAsync(hx.data(), S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, E.stream_));
+    CK(cudaStreamSynchronize(E.stream_));
+    frame(hx.data(), E.cell_h_, step + o.step_offset, user);
+  }
+  bool refill_due(long long s) const { return S.bussi && s - S.draws_first >= S.draws_count; }
+  bool baro_due(long long s) const { return o.barostat && s % baro_every == 0; }
+  // a step that reports, records, rescales the cell or refills the thermostat's draws
+  bool special(long long s) const {
+    return s % thermo_every == 0 || s == o.steps || (o.frame_every > 0 && s % o.frame_every == 0) || baro_due(s) || refill_due(s);
+  }
+
+  void start();
+  void advance(long long s);
+  void baro_step(long long s);
+};
+
+void MdRun::start() {
+  cudaStream_t stream_ = E.stream_;
+  Engine& e = E;
+  const int n_ = E.n_;
+  e.set_cell(st->cell);
   S.x.upload(st->x, n3, stream_);
   S.x0.alloc(n3);
   S.v.alloc(n3);
-  S.m.upload(h_mass_, stream_);
+  S.m.upload(E.h_mass_, stream_);
   std::vector<double> im(static_cast<size_t>(n_));
-  for (int i = 0; i < n_; ++i) im[size_t(i)] = h_mass_[size_t(i)] > 0 ? 1.0 / h_mass_[size_t(i)] : 0.0;
+  for (int i = 0; i < n_; ++i) im[size_t(i)] = E.h_mass_[size_t(i)] > 0 ? 1.0 / E.h_mass_[size_t(i)] : 0.0;
   S.invm.upload(im, stream_);
   S.sc.alloc(kScNum);
   S.sc.zero(stream_);
@@ -1157,6 +1256,10 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
   S.done.alloc(1);
   S.done.zero(stream_);
   S.respa = std::max(1, o.respa);
+  if (o.respa_split == 1) {
+    if (!E.pme_) throw ModelError(CAPS_GPU_EINVAL, "the PME r-RESPA split needs PME electrostatics");
+    S.slow_parts = 4, S.fast_parts = 3;
+  }
   if (S.respa > 1) {
     S.f_slow.alloc(n3);
     S.f_fast.alloc(n3);
@@ -1167,35 +1270,30 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
   S.bussi = o.thermostat == 1;
   S.langevin = o.thermostat == 2;
   S.t_freq = 1.0 / std::max(o.tau_t, 1e-9);
-  S.C.cell = dcell_;
+  S.C.cell = E.dcell_;
   S.build_constraints(st->x);
   S.ndof = 3.0 * double(n_) - 3.0 - double(S.ncons);
   if (S.ndof < 1) throw ModelError(CAPS_GPU_EINVAL, "the constraints leave no degree of freedom");
   S.rng = std::make_unique<HostRng>(o.seed);
   if (S.ncons) {   // the constrained lengths hold from the start (dynamics.cpp:198-203)
     CK(cudaMemcpyAsync(S.x0.p, S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
-    k_shake<<<blocks(size_t(S.C.ncl), 128), 128, 0, stream_>>>(S.C, S.x.p, S.x0.p, S.v.p, 0.0, d_counters_.p);
+    k_shake<<<blocks(size_t(S.C.ncl), 128), 128, 0, stream_>>>(S.C, S.x.p, S.x0.p, S.v.p, 0.0, E.d_counters_.p);
   }
 
   // velocities: given, or Maxwell-Boltzmann from the reference's stream, no centre-of-mass motion, rescaled to T
-  std::vector<double> hv(n3, 0.0);
-  auto host_ke = [&](const std::vector<double>& vv) {
-    double k = 0;
-    for (int i = 0; i < n_; ++i) k += h_mass_[size_t(i)] * (vv[3 * i] * vv[3 * i] + vv[3 * i + 1] * vv[3 * i + 1] + vv[3 * i + 2] * vv[3 * i + 2]);
-    return 0.5 * k / kAcc;
-  };
+  hv.assign(n3, 0.0);
   const bool drawn = !(st->has_velocities && st->v && !o.new_velocities);
   if (!drawn) {
     std::memcpy(hv.data(), st->v, n3 * sizeof(double));
   } else {
     for (int i = 0; i < n_; ++i) {
-      const double sd = std::sqrt(kB * o.temperature * kAcc / h_mass_[size_t(i)]);
+      const double sd = std::sqrt(kB * o.temperature * kAcc / E.h_mass_[size_t(i)]);
       for (int k = 0; k < 3; ++k) hv[3 * size_t(i) + k] = sd * S.rng->gauss();
     }
     double p[3] = {0, 0, 0}, mf = 0;
     for (int i = 0; i < n_; ++i) {
-      mf += h_mass_[size_t(i)];
-      for (int k = 0; k < 3; ++k) p[k] += h_mass_[size_t(i)] * hv[3 * size_t(i) + k];
+      mf += E.h_mass_[size_t(i)];
+      for (int k = 0; k < 3; ++k) p[k] += E.h_mass_[size_t(i)] * hv[3 * size_t(i) + k];
     }
     for (int i = 0; i < n_; ++i)
       for (int k = 0; k < 3; ++k) hv[3 * size_t(i) + k] -= p[k] / mf;
@@ -1214,62 +1312,6 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
   if (S.bussi) S.make_draws(1, std::min<long long>(std::max<long long>(o.steps, 1), 4096));
 
   // the first force, energies and virial
-  auto row = [&](long long step, caps_gpu_thermo& r) {
-    caps_gpu_terms t{};
-    read_terms(&t, true, true);
-    const double* sc = S.h_sc;
-    for (int c = 0; c < 6; ++c) t.w[c] += sc[kScCW0 + c];
-    t.virial = t.w[0] + t.w[1] + t.w[2];
-    std::memset(&r, 0, sizeof r);
-    r.step = step + o.step_offset;
-    r.time_ps = double(step + o.step_offset) * o.dt * 1e-3;
-    r.target_temperature = (o.temperature_end >= 0 && o.steps > 0) ? o.temperature + (o.temperature_end - o.temperature) * double(step) / double(o.steps)
-                                                                  : o.temperature;
-    r.kinetic = sc[kScKE];
-    r.temperature = 2 * r.kinetic / (S.ndof * kB);
-    r.potential = t.bond + t.angle + t.dihedral + t.improper + t.vdw + t.coulomb;
-    r.total = r.potential + r.kinetic;
-    r.volume = dcell_.vol;
-    double mtot = 0;
-    for (double mm : h_mass_) mtot += mm;
-    r.density = mtot / kNA / (r.volume * 1e-24);
-    r.pressure = (2 * r.kinetic + t.virial) / (3 * r.volume) * kAtm;
-    for (int c = 0; c < 6; ++c) r.p[c] = (sc[kScKin0 + c] + t.w[c]) / r.volume * kAtm;
-    if (S.nhc) {
-      const Chain& ch = *S.h_chain;
-      const double kt = kB * r.target_temperature;
-      double e = S.ndof * kt * ch.eta[0] + 0.5 * ch.eta_mass[0] * ch.eta_dot[0] * ch.eta_dot[0];
-      for (int c = 1; c < 3; ++c) e += kt * ch.eta[c] + 0.5 * ch.eta_mass[c] * ch.eta_dot[c] * ch.eta_dot[c];
-      r.conserved = r.total + e;
-    } else {
-      r.conserved = r.total + sc[kScBath] + (o.barostat ? o.pressure * r.volume / kAtm : 0.0);
-    }
-    r.terms = t;
-  };
-  auto sync_scalars = [&]() {
-    CK(cudaMemcpyAsync(S.h_sc, S.sc.p, sizeof(double) * kScNum, cudaMemcpyDeviceToHost, stream_));
-    CK(cudaMemcpyAsync(S.h_chain, S.chain.p, sizeof(Chain), cudaMemcpyDeviceToHost, stream_));
-    CK(cudaMemcpyAsync(h_counters_, d_counters_.p, sizeof(int) * kCntNum, cudaMemcpyDeviceToHost, stream_));
-    CK(cudaMemcpyAsync(h_efix_, d_efix_.p, sizeof(long long) * kENumSlots, cudaMemcpyDeviceToHost, stream_));
-    CK(cudaMemcpyAsync(h_edbl_, d_edbl_.p, sizeof(double) * kENumSlots, cudaMemcpyDeviceToHost, stream_));
-    CK(cudaStreamSynchronize(stream_));
-    check_errors();
-  };
-  auto emit = [&](long long step) {
-    S.ke(kScKE, true);
-    sync_scalars();
-    caps_gpu_thermo r;
-    row(step, r);
-    if (progress && progress(&r, user) != 0) throw ModelError(CAPS_GPU_ECANCEL, "dynamics cancelled");
-  };
-  auto emit_frame = [&](long long step) {
-    if (!frame || o.frame_every <= 0) return;
-    std::vector<double> hx(n3);
-    CK(cudaMemcpyAsync(hx.data(), S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
-    CK(cudaStreamSynchronize(stream_));
-    frame(hx.data(), cell_h_, step + o.step_offset, user);
-  };
-
   S.forces(true, true);
   if (S.ncons) {
     // step 0's constraint virial from one trial step on copies (dynamics.cpp:582-600)
@@ -1287,13 +1329,87 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
   emit(0);
   emit_frame(0);
 
-  // the step loop: plain steps replay a captured graph; thermo / frame / barostat steps run uncaptured
-  const int thermo_every = std::max(1, o.thermo_every);
-  const int baro_every = std::max(1, o.barostat_every);
-  auto special = [&](long long s) {
-    return s % thermo_every == 0 || s == o.steps || (o.frame_every > 0 && s % o.frame_every == 0) || (o.barostat && s % baro_every == 0) ||
-           (S.bussi && s - S.draws_first >= S.draws_count);
-  };
+  thermo_every = std::max(1, o.thermo_every);
+  baro_every = std::max(1, o.barostat_every);
+}
+
+// One step s: the captured plain step, or a special one (thermo row, frame, cell rescaling, new thermostat draws).
+void MdRun::advance(long long s) {
+  if (refill_due(s)) {
+    CK(cudaStreamSynchronize(E.stream_));
+    S.make_draws(s, std::min<long long>(o.steps - s + 1, 4096));
+    S.drop_graphs();   // the draw table's first step is a parameter of the captured thermostat kernel
+    ++generation;
+  }
+  if (baro_due(s)) {
+    baro_step(s);
+  } else {
+    kernels += S.launch_step(special(s));
+    if (!special(s)) return;
+  }
+  if (s % thermo_every == 0 || s == o.steps) {
+    emit(s);
+    ++emits;
+  }
+  if (o.frame_every > 0 && (s % o.frame_every == 0 || s == o.steps)) emit_frame(s);
+}
+
+// A step with stochastic cell rescaling (Bernetti & Bussi 2020, dynamics.cpp:684-723), isotropic.
+void MdRun::baro_step(long long s) {
+  (void)s;
+  cudaStream_t stream_ = E.stream_;
+  S.step(true, true);
+  ++baro_steps;
+  S.ke(kScKE, true);
+  sync_scalars();
+  caps_gpu_terms t{};
+  E.read_terms(&t, true, true);
+  for (int c = 0; c < 6; ++c) t.w[c] += S.h_sc[kScCW0 + c];
+  t.virial = t.w[0] + t.w[1] + t.w[2];
+  const double k = S.h_sc[kScKE], vol = E.dcell_.vol;
+  const double p = (2 * k + t.virial) / (3 * vol) * kAtm;
+  const double hp = o.dt * baro_every;
+  const double tnow = S.h_sc[kScTnow];
+  double deps = -o.compressibility / o.tau_p * (o.pressure - p) * hp;
+  const double ktv = kB * tnow / vol * kAtm;
+  deps += o.compressibility / o.tau_p * ktv * hp + std::sqrt(2 * ktv * o.compressibility * hp / o.tau_p) * S.rng->gauss();
+  deps = std::max(-0.01, std::min(0.01, deps));
+  const double mu = std::exp(deps / 3);
+  std::vector<double> hx(n3);
+  CK(cudaMemcpyAsync(hx.data(), S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  CK(cudaMemcpyAsync(hv.data(), S.v.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  CK(cudaStreamSynchronize(stream_));
+  double cell[12];
+  std::memcpy(cell, E.cell_h_, sizeof cell);
+  for (int i = 0; i < E.n_; ++i)
+    for (int c = 0; c < 3; ++c) hx[3 * size_t(i) + c] = cell[c] + mu * (hx[3 * size_t(i) + c] - cell[c]);
+  for (int q = 3; q < 12; ++q) cell[q] *= mu;
+  for (auto& q : hv) q /= mu;
+  const double k2 = host_ke(hv);
+  S.h_sc[kScBath] -= k2 - k;
+  CK(cudaMemcpyAsync(S.sc.p + kScBath, S.h_sc + kScBath, sizeof(double), cudaMemcpyHostToDevice, stream_));
+  S.x.upload(hx, stream_);
+  S.v.upload(hv, stream_);
+  E.set_cell(cell);
+  S.C.cell = E.dcell_;
+  if (S.ncons) {
+    CK(cudaMemcpyAsync(S.x0.p, S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    k_shake<<<blocks(size_t(S.C.ncl), 128), 128, 0, stream_>>>(S.C, S.x.p, S.x0.p, S.v.p, 0.0, E.d_counters_.p);
+    S.rattle(0);
+  }
+  S.forces(true, true);
+  S.drop_graphs();   // the cell is a parameter of the captured kernels
+  ++generation;
+}
+
+void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progress_fn progress, caps_gpu_frame_fn frame, void* user, std::string* report) {
+  const auto t_enter = std::chrono::steady_clock::now();
+  validate_md(*md);
+  MdRun R(*this, st, md, progress, frame, user);
+  R.start();
+  const caps_gpu_md_opts& o = *md;
+  Stepper& S = R.S;
+  const size_t n3 = R.n3;
   cudaEvent_t ev0, ev1;
   CK(cudaEventCreate(&ev0));
   CK(cudaEventCreate(&ev1));
@@ -1307,7 +1423,6 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
   }
   const auto w0 = std::chrono::steady_clock::now();
   CK(cudaEventRecord(ev0, stream_));
-  long long kernels = 0, emits = 0, baro_steps = 0;
   for (long long s = 1; s <= o.steps; ++s) {
     if (timed) {
       if (timing_flush_ > 0) CK(cudaMemsetAsync(d_flush_.p, int(s & 255), size_t(timing_flush_), stream_));
@@ -1321,69 +1436,11 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
         if (on) cudaEventRecord(e, st);
       }
     } end_ev{timed, timed ? tev[size_t(2 * (s - 1) + 1)] : nullptr, stream_};
-    if (S.bussi && s - S.draws_first >= S.draws_count) {
-      CK(cudaStreamSynchronize(stream_));
-      S.make_draws(s, std::min<long long>(o.steps - s + 1, 4096));
-      S.drop_graphs();   // the draw table's first step is a parameter of the captured thermostat kernel
-    }
-    const bool baro = o.barostat && s % baro_every == 0;
-    if (!baro) {
-      kernels += S.launch_step(special(s));
-      if (!special(s)) continue;
-    }
-    if (baro) {
-      S.step(true, true);
-      ++baro_steps;
-      // stochastic cell rescaling (Bernetti & Bussi 2020, dynamics.cpp:684-723), isotropic
-      S.ke(kScKE, true);
-      sync_scalars();
-      caps_gpu_terms t{};
-      read_terms(&t, true, true);
-      for (int c = 0; c < 6; ++c) t.w[c] += S.h_sc[kScCW0 + c];
-      t.virial = t.w[0] + t.w[1] + t.w[2];
-      const double k = S.h_sc[kScKE], vol = dcell_.vol;
-      const double p = (2 * k + t.virial) / (3 * vol) * kAtm;
-      const double hp = o.dt * baro_every;
-      const double tnow = S.h_sc[kScTnow];
-      double deps = -o.compressibility / o.tau_p * (o.pressure - p) * hp;
-      const double ktv = kB * tnow / vol * kAtm;
-      deps += o.compressibility / o.tau_p * ktv * hp + std::sqrt(2 * ktv * o.compressibility * hp / o.tau_p) * S.rng->gauss();
-      deps = std::max(-0.01, std::min(0.01, deps));
-      const double mu = std::exp(deps / 3);
-      std::vector<double> hx(n3);
-      CK(cudaMemcpyAsync(hx.data(), S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
-      CK(cudaMemcpyAsync(hv.data(), S.v.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
-      CK(cudaStreamSynchronize(stream_));
-      double cell[12];
-      std::memcpy(cell, cell_h_, sizeof cell);
-      for (int i = 0; i < n_; ++i)
-        for (int c = 0; c < 3; ++c) hx[3 * size_t(i) + c] = cell[c] + mu * (hx[3 * size_t(i) + c] - cell[c]);
-      for (int q = 3; q < 12; ++q) cell[q] *= mu;
-      for (auto& q : hv) q /= mu;
-      const double k2 = host_ke(hv);
-      S.h_sc[kScBath] -= k2 - k;
-      CK(cudaMemcpyAsync(S.sc.p + kScBath, S.h_sc + kScBath, sizeof(double), cudaMemcpyHostToDevice, stream_));
-      S.x.upload(hx, stream_);
-      S.v.upload(hv, stream_);
-      set_cell(cell);
-      S.C.cell = dcell_;
-      if (S.ncons) {
-        CK(cudaMemcpyAsync(S.x0.p, S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
-        k_shake<<<blocks(size_t(S.C.ncl), 128), 128, 0, stream_>>>(S.C, S.x.p, S.x0.p, S.v.p, 0.0, d_counters_.p);
-        S.rattle(0);
-      }
-      S.forces(true, true);
-      S.drop_graphs();   // the cell is a parameter of the captured kernels
-    }
-    if (s % thermo_every == 0 || s == o.steps) {
-      emit(s);
-      ++emits;
-    }
-    if (o.frame_every > 0 && (s % o.frame_every == 0 || s == o.steps)) emit_frame(s);
+    R.advance(s);
   }
   CK(cudaEventRecord(ev1, stream_));
   CK(cudaEventSynchronize(ev1));
-  kernels_run_ = kernels + emits + baro_steps * S.graph_kernels[1];
+  kernels_run_ = R.kernels + R.emits + R.baro_steps * S.graph_kernels[1];
   float ms = 0;
   CK(cudaEventElapsedTime(&ms, ev0, ev1));
   if (timed && o.steps > 0) {
@@ -1400,7 +1457,7 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
   const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
   cudaEventDestroy(ev0);
   cudaEventDestroy(ev1);
-  sync_scalars();
+  R.sync_scalars();
   last_sps_ = o.steps > 0 && ms > 0 ? double(o.steps) / (ms * 1e-3) : 0.0;
   // state back to the caller
   CK(cudaMemcpyAsync(st->x, S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
@@ -1415,6 +1472,131 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
                   "%lld steps of %.2f fs in %.3f s (device %.3f s, set-up %.3f s) · %.2f ns/day · %d constraints · %.0f degrees of freedom · %s",
                   (long long)o.steps, o.dt, wall, ms * 1e-3, setup, nsday, S.ncons, S.ndof, mixed_ ? "mixed FP32/fixed-point" : "FP64");
     *report = b;
+  }
+}
+
+// Replicas in lock step (caps_gpu_run_batch). A step on which no replica reports, records, rescales or refills is one
+// CUDA graph holding every replica's step as a parallel branch (each on its own engine's streams); other steps run
+// replica by replica. The graph is captured again whenever a replica's captured step changes.
+void run_batch(const std::vector<Engine*>& es, caps_gpu_state* const* states, const caps_gpu_md_opts* const* mds, caps_gpu_progress_fn progress,
+               caps_gpu_frame_fn frame, void* const* users) {
+  const size_t R = es.size();
+  if (R == 0) return;
+  const long long steps = mds[0]->steps;
+  int dev0 = -1;
+  for (size_t r = 0; r < R; ++r) {
+    es[r]->validate_md(*mds[r]);
+    if (mds[r]->steps != steps) throw ModelError(CAPS_GPU_EINVAL, "the replicas of a batch run the same number of steps");
+    cudaPointerAttributes pa{};
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev0 < 0) dev0 = dev;
+    (void)pa;
+  }
+  std::vector<std::unique_ptr<MdRun>> runs;
+  for (size_t r = 0; r < R; ++r) {
+    runs.emplace_back(new MdRun(*es[r], states[r], mds[r], progress, frame, users ? users[r] : nullptr));
+    runs.back()->start();
+  }
+  struct Res {
+    cudaStream_t bs = nullptr;
+    cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr;
+    std::vector<cudaEvent_t> ev;
+    cudaGraphExec_t g = nullptr;
+    ~Res() {
+      if (g) cudaGraphExecDestroy(g);
+      for (auto e : ev)
+        if (e) cudaEventDestroy(e);
+      if (fork) cudaEventDestroy(fork);
+      if (t0) cudaEventDestroy(t0);
+      if (t1) cudaEventDestroy(t1);
+      if (bs) cudaStreamDestroy(bs);
+    }
+  } res;
+  CK(cudaStreamCreateWithFlags(&res.bs, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&res.fork, cudaEventDisableTiming));
+  CK(cudaEventCreate(&res.t0));
+  CK(cudaEventCreate(&res.t1));
+  res.ev.assign(R, nullptr);
+  for (auto& e : res.ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  std::vector<int> seen(R, -1);
+  long long batch_kernels = 0, graph_nodes = 0;
+  bool on_replicas = true;   // the replicas' own streams hold the latest work
+  // orders the batch stream after every replica stream, or every replica stream after the batch stream
+  auto join_to_batch = [&] {
+    for (size_t r = 0; r < R; ++r) {
+      CK(cudaEventRecord(res.ev[r], es[r]->stream_));
+      CK(cudaStreamWaitEvent(res.bs, res.ev[r], 0));
+    }
+  };
+  auto fork_to_replicas = [&] {
+    CK(cudaEventRecord(res.fork, res.bs));
+    for (size_t r = 0; r < R; ++r) CK(cudaStreamWaitEvent(es[r]->stream_, res.fork, 0));
+  };
+  join_to_batch();
+  CK(cudaEventRecord(res.t0, res.bs));
+  const auto w0 = std::chrono::steady_clock::now();
+  for (long long s = 1; s <= steps; ++s) {
+    bool plain = true;
+    for (size_t r = 0; r < R; ++r) plain = plain && !runs[r]->special(s);
+    if (!plain) {
+      if (!on_replicas) fork_to_replicas(), on_replicas = true;
+      for (size_t r = 0; r < R; ++r) runs[r]->advance(s);
+      continue;
+    }
+    if (on_replicas) join_to_batch(), on_replicas = false;
+    bool stale = res.g == nullptr;
+    for (size_t r = 0; r < R; ++r) stale = stale || seen[r] != runs[r]->generation;
+    if (stale) {
+      if (res.g) {
+        CK(cudaGraphExecDestroy(res.g));
+        res.g = nullptr;
+      }
+      cudaGraph_t graph;
+      CK(cudaStreamBeginCapture(res.bs, cudaStreamCaptureModeThreadLocal));
+      CK(cudaEventRecord(res.fork, res.bs));
+      for (size_t r = 0; r < R; ++r) {
+        CK(cudaStreamWaitEvent(es[r]->stream_, res.fork, 0));
+        runs[r]->S.step(false, false);
+        CK(cudaEventRecord(res.ev[r], es[r]->stream_));
+        CK(cudaStreamWaitEvent(res.bs, res.ev[r], 0));
+      }
+      CK(cudaStreamEndCapture(res.bs, &graph));
+      size_t nn = 0;
+      CK(cudaGraphGetNodes(graph, nullptr, &nn));
+      std::vector<cudaGraphNode_t> nodes(nn);
+      CK(cudaGraphGetNodes(graph, nodes.data(), &nn));
+      graph_nodes = 0;
+      for (auto nd : nodes) {
+        cudaGraphNodeType ty;
+        CK(cudaGraphNodeGetType(nd, &ty));
+        graph_nodes += ty == cudaGraphNodeTypeKernel;
+      }
+      CK(cudaGraphInstantiate(&res.g, graph, cudaGraphInstantiateFlagUseNodePriority));
+      CK(cudaGraphDestroy(graph));
+      for (size_t r = 0; r < R; ++r) seen[r] = runs[r]->generation;
+    }
+    CK(cudaGraphLaunch(res.g, res.bs));
+    batch_kernels += graph_nodes;
+  }
+  if (on_replicas) join_to_batch();
+  CK(cudaEventRecord(res.t1, res.bs));
+  CK(cudaEventSynchronize(res.t1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, res.t0, res.t1));
+  const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
+  (void)wall;
+  for (size_t r = 0; r < R; ++r) {
+    MdRun& M = *runs[r];
+    Engine& E = M.E;
+    M.sync_scalars();
+    E.last_step_ms_ = steps > 0 ? double(ms) / double(steps) : 0.0;
+    E.last_sps_ = steps > 0 && ms > 0 ? double(steps) / (ms * 1e-3) : 0.0;
+    E.kernels_run_ = M.kernels + M.emits + (r == 0 ? batch_kernels : 0);
+    CK(cudaMemcpyAsync(M.st->x, M.S.x.p, M.n3 * sizeof(double), cudaMemcpyDeviceToHost, E.stream_));
+    if (M.st->v) CK(cudaMemcpyAsync(M.st->v, M.S.v.p, M.n3 * sizeof(double), cudaMemcpyDeviceToHost, E.stream_));
+    CK(cudaStreamSynchronize(E.stream_));
+    std::memcpy(M.st->cell, E.cell_h_, sizeof E.cell_h_);
   }
 }
 

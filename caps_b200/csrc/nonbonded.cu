@@ -185,7 +185,9 @@ void Engine::pair_forces(bool ener, bool vir) {
 // One force evaluation on device positions d_x (AoS, 3 n): accumulators cleared, list checked / rebuilt, every term,
 // forces reduced into d_f_ (AoS doubles). Asynchronous on stream_.
 void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild, int parts, double* d_out, bool clear_energies) {
-  const int pm = parts < 0 ? opt_.parts : parts;
+  // internal part mask: 1 bonded, 2 short-range non-bonded (list, pair kernel, 1-4 pairs), 4 long-range (PME and its
+  // excluded-pair corrections); the options' non-bonded bit means both 2 and 4
+  const int pm = parts >= 0 ? parts : ((opt_.parts & 1) | ((opt_.parts & 2) ? 6 : 0));
   const bool nonb = (pm & 2) != 0;
   double* out = d_out ? d_out : d_f_.p;
   if (mixed_) {
@@ -202,7 +204,7 @@ void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild, 
   // Three branches: bonded terms and PME beside the list and pair kernels. All add into order-free fixed-point (or
   // atomic FP64) sums, so how the branches interleave does not change the mixed path's result.
   fork(0, [&] { bonded_forces(d_x, ener, vir, pm); });
-  const bool pme = nonb && pme_;
+  const bool pme = (pm & 4) != 0 && pme_;
   if (pme) fork(1, [&] { pme_forces(d_x, ener, vir); });
   if (nonb) {
     if (!list_valid_) {

@@ -91,6 +91,7 @@ class DynamicsOptions:
     frame_every: int = 0
     step_offset: int = 0
     respa: int = 1
+    respa_split: str = "bonded"        # "bonded": bonded terms inner (the reference's split); "pme": PME outer
     energy: EnergyOptions = field(default_factory=EnergyOptions)
 
     def to_struct(self, ff: ForceField, keep: list) -> _abi.MdOpts:
@@ -103,6 +104,7 @@ class DynamicsOptions:
         m.constraints = 0 if self.constraints in ("none", "", None) else 1
         m.new_velocities = int(bool(self.new_velocities))
         m.seed, m.thermo_every, m.frame_every, m.step_offset, m.respa = self.seed, self.thermo_every, self.frame_every, self.step_offset, self.respa
+        m.respa_split = {"bonded": 0, "pme": 1}[self.respa_split]
         if ff.element is not None:
             h = np.ascontiguousarray((ff.element == 1).astype(np.int8))
             o = np.ascontiguousarray((ff.element == 8).astype(np.int8))
@@ -237,3 +239,37 @@ def run_dynamics(ff: ForceField, x, cell, opts: DynamicsOptions, v=None, progres
         return ev.run(x, cell, opts, v=v, progress=progress, frame=frame)
     finally:
         ev.close()
+
+
+def run_batch(evaluators: list, xs: list, cells: list, opts: list, vs: list | None = None) -> list[dict]:
+    """Independent replicas in lock step (caps_gpu_run_batch): one Evaluator, structure and DynamicsOptions per replica,
+    all with the same number of steps. Returns one {x, v, cell, thermo} per replica."""
+    R = len(evaluators)
+    if not (len(xs) == len(cells) == len(opts) == R) or R == 0:
+        raise ValueError("one structure, cell and options per evaluator")
+    keep: list = []
+    xa, va, ca, st, ms = [], [], [], [], []
+    rows: list[list] = [[] for _ in range(R)]
+    for r, ev in enumerate(evaluators):
+        x = np.ascontiguousarray(np.asarray(xs[r], dtype=np.float64).reshape(-1)).copy()
+        v = np.zeros_like(x) if vs is None or vs[r] is None else np.ascontiguousarray(np.asarray(vs[r], dtype=np.float64).reshape(-1)).copy()
+        c = cell_array(cells[r]).copy()
+        xa.append(x), va.append(v), ca.append(c)
+        st.append(_abi.State(x.ctypes.data_as(C.c_void_p), v.ctypes.data_as(C.c_void_p), c.ctypes.data_as(C.c_void_p),
+                             0 if vs is None or vs[r] is None else 1))
+        ms.append(opts[r].to_struct(ev.ff, keep))
+
+    def _prog(row, user):
+        rows[int(user or 0)].append(row.contents.as_dict())
+        return 0
+
+    pf, ff_ = _abi.PROGRESS_FN(_prog), _abi.FRAME_FN(lambda *a: None)
+    eng = (C.c_void_p * R)(*[ev.h for ev in evaluators])
+    sp = (C.c_void_p * R)(*[C.cast(C.pointer(s_), C.c_void_p) for s_ in st])
+    mp = (C.c_void_p * R)(*[C.cast(C.pointer(m_), C.c_void_p) for m_ in ms])
+    users = (C.c_void_p * R)(*[C.c_void_p(r) for r in range(R)])
+    lib = evaluators[0].lib
+    rc = lib.caps_gpu_run_batch(eng, sp, mp, R, pf, ff_, users)
+    evaluators[0]._check(rc)
+    return [{"x": xa[r].reshape(-1, 3), "v": va[r].reshape(-1, 3), "cell": ca[r], "thermo": rows[r]} for r in range(R)]
+

@@ -122,6 +122,8 @@ typedef struct {
   int32_t respa;            /* r-RESPA inner steps (1 off) */
   const int8_t* is_hydrogen; /* [natoms] element == 1, for the constraint set; NULL: mass < 1.6 */
   const int8_t* is_oxygen;   /* [natoms] element == 8, for rigid waters; NULL: none */
+  int32_t respa_split;      /* with respa > 1: 0 bonded forces every dt/respa (the reference's split, dynamics.cpp:113);
+                               1 PME every dt, everything else every dt/respa (a split the reference does not have) */
 } caps_gpu_md_opts;
 
 /* caps::ThermoRow (dynamics.hpp:28-43), the fields the device step fills. */
@@ -171,6 +173,14 @@ int32_t caps_gpu_list_builds(const caps_gpu_engine* e);
  * for the options above. progress and frame may be NULL. report (may be NULL) receives a short text summary. */
 int32_t caps_gpu_run(caps_gpu_engine* e, caps_gpu_state* state, const caps_gpu_md_opts* md, caps_gpu_progress_fn progress,
                      caps_gpu_frame_fn frame, void* user, char* report, int32_t report_cap);
+/* Independent replicas in lock step, one engine each (own force field, state and dynamics options; the same number of
+ * steps). Replaces running run_dynamics once per replica (core/src/dynamics.cpp:71, called in turn for each rung of a
+ * Tg ladder or each seed of a protocol, e.g. core/src/mechanics.cpp:1381): a step on which no replica reports, records
+ * a frame, rescales its cell or refills its thermostat draws is one CUDA graph launch for all replicas. progress and
+ * frame receive user[r] for replica r. Errors: caps_gpu_error(engines[0]). Afterwards every engine's
+ * caps_gpu_last_steps_per_second is the batch's. */
+int32_t caps_gpu_run_batch(caps_gpu_engine* const* engines, caps_gpu_state* const* states, const caps_gpu_md_opts* const* md, int32_t count,
+                           caps_gpu_progress_fn progress, caps_gpu_frame_fn frame, void* const* user);
 /* The last run's throughput: steps per second over the step loop (first force excluded, as dynamics.cpp:601,776). */
 double caps_gpu_last_steps_per_second(const caps_gpu_engine* e);
 void caps_gpu_destroy(caps_gpu_engine* e);

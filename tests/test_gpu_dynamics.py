@@ -61,6 +61,21 @@ def test_fp64_respa_run_follows_reference(thermostat):
     assert np.max(np.abs(out["x"] - r["x"])) < 1e-8
 
 
+def test_pme_respa_split_conserves_energy():
+    """The PME split (the reciprocal sum once per 2 fs outer step, every other term every 1 fs): no reference has it, so
+    it must start from the plain run's step-0 row and conserve the total energy about as well as velocity Verlet at 1 fs."""
+    fx = load("ps_small")
+    eo = EnergyOptions(cutoff=8.0, skin=2.0, electrostatics="pme", pme_order=5, precision="double")
+    common = dict(temperature=300.0, thermostat="none", thermo_every=10, seed=4, energy=eo)
+    a = Evaluator(fx.ff, eo).run(fx.x, fx.cell, DynamicsOptions(dt=1.0, steps=400, **common))
+    b = Evaluator(fx.ff, eo).run(fx.x, fx.cell, DynamicsOptions(dt=2.0, steps=200, respa=2, respa_split="pme", **common))
+    for k in ("potential", "kinetic"):
+        assert abs(a["thermo"][0][k] - b["thermo"][0][k]) <= 1e-12 * abs(a["thermo"][0][k])
+    ea = np.array([r["total"] for r in a["thermo"]])
+    eb = np.array([r["total"] for r in b["thermo"]])
+    assert np.std(eb) < 3 * max(np.std(ea), 1e-7 * abs(ea.mean())), (np.std(ea), np.std(eb))
+
+
 def test_fp64_rigid_water_settle_follows_reference_shake():
     """Rigid SPC/E waters: the device solves them with SETTLE (exact distances), the reference with SHAKE (1e-8 relative
     tolerance); from the same equilibrated state the thermo rows agree to SHAKE's tolerance."""
