@@ -145,6 +145,7 @@ def main():
     ap.add_argument("--impl", default="caps_b200")
     ap.add_argument("--fp64-steps", type=int, default=None)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--replicas", type=int, default=8, help="batched-replica measurement with this many replicas (0: skip)")
     ap.add_argument("--profile-pair", type=int, default=0, metavar="LAUNCHES",
                     help="only time the pair kernel LAUNCHES times on the start structure (a small case for ncu captures)")
     ap.add_argument("--profile-md", type=int, default=0, metavar="STEPS",
@@ -268,6 +269,36 @@ def main():
     ms64 = max_over_ranks(ev64.last_step_ms())
     nsd64 = 1000.0 / ms64 * 86400e-6
     ev64.close()
+    # --- batched replicas (SURVEY config 4's target): R replicas of this cell, each at its own Langevin temperature,
+    # in lock step (one graph launch per plain step), against one equally large system (the cell tiled 2 x 2 x 2) ---
+    batch = None
+    if args.replicas > 0:
+        from caps_b200 import run_batch
+        from caps_b200.systems import tile
+        R = args.replicas
+        kb = max(50, args.steps // 10)
+        lang = [options("mixed", kb, seed + r, thermostat="langevin") for r in range(R)]
+        for r, o_ in enumerate(lang):
+            o_.temperature = 500.0 - 10.0 * r
+        evs = [Evaluator(ff, lang[0].energy) for _ in range(R)]
+        warm = [options("mixed", 20, seed + r, thermostat="langevin") for r in range(R)]
+        run_batch(evs, [x2] * R, [cell] * R, warm, vs=[v2] * R)
+        run_batch(evs, [x2] * R, [cell] * R, lang, vs=[v2] * R)
+        batch_sps = evs[0].steps_per_second()
+        for e_ in evs:
+            e_.close()
+        fb, xb, cb = tile(ff, x2, cell, (2, 2, 2))
+        vb = np.concatenate([v2] * 8)
+        eb = Evaluator(fb, lang[0].energy)
+        eb.run(xb, cb, options("mixed", 20, seed, thermostat="langevin"), v=vb)
+        eb.run(xb, cb, options("mixed", kb, seed, thermostat="langevin"), v=vb)
+        big_sps = eb.steps_per_second()
+        eb.close()
+        batch = {"replicas": R, "atoms_per_replica": n, "steps": kb, "thermostat": "Langevin, 500 K down in 10 K rungs",
+                 "atom_steps_per_s": batch_sps * R * n, "single_system_atoms": 8 * n, "single_system_atom_steps_per_s": big_sps * 8 * n,
+                 "efficiency": (batch_sps * R * n) / (big_sps * 8 * n) if big_sps > 0 else None,
+                 "note": "replicas of this cell (not the polyisoprene sizes of the config); the single system is the cell tiled 2x2x2; "
+                         "device time over the step loop, L2 not flushed"}
     # --- NVE drift of the mixed path (2 ps) ---
     nve = options("mixed", 2000, seed, thermostat="none", thermo_every=100)
     outn = ev.run(x2, cell, nve, v=v2)
@@ -305,6 +336,7 @@ def main():
             "force_error_vs_fp64": {"rms_relative": rms_rel, "per_atom_rms": float(np.sqrt(np.mean(per_atom ** 2))),
                                     "per_atom_max": float(per_atom.max()), "energy_relative": e_err},
             "nve_drift_kT_per_ns_per_atom": drift_kt_ns_atom,
+            "batched_replicas": batch,
             "e2e": {"value": e2e_nsd, "unit": "ns/day", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "call": "caps_gpu_run (C ABI) on host buffers, wall clock"},
             "roofline": {"bound": "fp32", "kernel": "k_pair_f32 (LJ + Ewald real space)", "achieved": achieved,

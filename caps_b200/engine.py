@@ -197,6 +197,10 @@ class Evaluator:
                                                        int(flush_bytes), C.byref(ms), C.byref(pin), C.byref(pl), C.byref(ne)))
         return {"avg_ms": ms.value, "pairs_in_cutoff": pin.value, "pairs_listed": pl.value, "entries": ne.value}
 
+    def steps_per_second(self) -> float:
+        """Throughput of the last run (or batch this evaluator was part of): steps per second of device time."""
+        return float(self.lib.caps_gpu_last_steps_per_second(self.h))
+
     def list_builds(self) -> int:
         return int(self.lib.caps_gpu_list_builds(self.h))
 

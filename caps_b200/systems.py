@@ -361,3 +361,40 @@ def spce_water(nmol: int = 100000, density: float = 0.997, seed: int = 1):
                     element=np.tile([8, 1, 1], nmol).astype(np.int32))
     cell = np.array([0, 0, 0, L, 0, 0, 0, L, 0, 0, 0, L], float)
     return ff, x, cell
+
+
+def tile(ff: ForceField, x, cell, reps=(2, 2, 2)):
+    """A periodic system repeated reps[0] x reps[1] x reps[2] times: the same periodic structure at a larger period
+    (every copy keeps its molecules' unwrapped coordinates). Returns (force field, positions, cell)."""
+    x = np.asarray(x, dtype=np.float64).reshape(-1, 3)
+    c = np.asarray(cell, dtype=np.float64).reshape(12)
+    n = ff.natoms
+    edges = c[3:].reshape(3, 3)
+    shifts = [i * edges[0] + j * edges[1] + k * edges[2] for i in range(reps[0]) for j in range(reps[1]) for k in range(reps[2])]
+    m = len(shifts)
+
+    def idx(a):
+        a = np.asarray(a, dtype=np.int64)
+        return np.concatenate([a + q * n for q in range(m)]).astype(np.uint32) if len(a) else a.astype(np.uint32)
+
+    def rep(a):
+        return None if a is None else np.concatenate([np.asarray(a)] * m)
+
+    off = np.asarray(ff.excl_offset, dtype=np.int64)
+    lst = np.asarray(ff.excl_list, dtype=np.int64)
+    excl_off = np.concatenate([off[:-1] + q * len(lst) for q in range(m)] + [[m * len(lst)]]).astype(np.uint32)
+    excl_list = np.concatenate([lst + q * n for q in range(m)]).astype(np.uint32) if len(lst) else lst.astype(np.uint32)
+    big = ForceField(type_index=rep(ff.type_index), charge=rep(ff.charge), mass=rep(ff.mass), pair_eps=ff.pair_eps, pair_sigma=ff.pair_sigma,
+                     bond_ij=idx(ff.bond_ij), bond_k_r0=rep(ff.bond_k_r0), angle_ijk=idx(ff.angle_ijk), angle_kt_theta0=rep(ff.angle_kt_theta0),
+                     dihedral_ijkl=idx(ff.dihedral_ijkl), dihedral_v_delta=rep(ff.dihedral_v_delta), dihedral_n=rep(ff.dihedral_n),
+                     improper_ijkl=idx(ff.improper_ijkl), improper_v_delta=rep(ff.improper_v_delta), improper_n=rep(ff.improper_n),
+                     pair14_ij=idx(ff.pair14_ij), pair14_lj=rep(ff.pair14_lj), pair14_coul=rep(ff.pair14_coul), lj14=ff.lj14, coul14=ff.coul14,
+                     excl_offset=excl_off, excl_list=excl_list, fene_ij=idx(ff.fene_ij), fene_k_r0_eps_sigma=rep(ff.fene_k_r0_eps_sigma),
+                     lj_shift=ff.lj_shift, model_cutoff=ff.model_cutoff, element=rep(ff.element))
+    xb = np.concatenate([x + s_ for s_ in shifts])
+    cb = c.copy()
+    cb[3:6] *= reps[0]
+    cb[6:9] *= reps[1]
+    cb[9:12] *= reps[2]
+    return big, xb, cb
+
