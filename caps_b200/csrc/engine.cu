@@ -415,6 +415,7 @@ void Engine::set_cell(const double* cell) {
   g.rv = int(std::floor(g.rlist * g.nv / g.w[1])) + 1;
   g.rq = int(std::ceil(g.rlist / g.w[2])) + 1;
   g.dw = g.rlist / g.w[2];
+  g.batch = batch_;
   if (g.ru / g.nu > 60 || g.rv / g.nv > 60 || g.rq > 60)
     throw ModelError(CAPS_GPU_EFIELD, "the cell is too small for the cut-off: more than 60 periodic images in range");
   const bool geom_changed = g.nu != geom_.nu || g.nv != geom_.nv;

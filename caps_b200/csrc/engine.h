@@ -141,6 +141,13 @@ class Engine {
   void fork(int k, const std::function<void()>& launch);
   void join(int k);
   cudaStream_t side_[2] = {nullptr, nullptr};
+  // Autotuning (timed on this system and GPU, once): the j-tile depth of the pair kernels' work items, and the PME
+  // line-transform block shapes per grid.
+  int batch_ = kBatch;
+  bool batch_tuned_ = false;
+  void tune_batch(const double* d_x);
+  template <class R> void fft_passes(PmePath<R>& P, bool ener, bool vir);
+  template <class R> void pme_tune(PmePath<R>& P);
   cudaEvent_t ev_fork_ = nullptr, ev_join_[2] = {nullptr, nullptr};
   void read_terms(caps_gpu_terms* out, bool ener, bool vir);
   void check_errors();

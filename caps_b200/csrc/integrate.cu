@@ -1465,12 +1465,14 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
   CK(cudaStreamSynchronize(stream_));
   std::memcpy(st->cell, cell_h_, sizeof cell_h_);
   if (report) {
-    char b[400];
+    char b[512];
     const double nsday = wall > 0 ? double(o.steps) * o.dt * 1e-6 / wall * 86400 : 0.0;
     const double setup = std::chrono::duration<double>(w0 - t_enter).count();
     std::snprintf(b, sizeof b,
-                  "%lld steps of %.2f fs in %.3f s (device %.3f s, set-up %.3f s) · %.2f ns/day · %d constraints · %.0f degrees of freedom · %s",
-                  (long long)o.steps, o.dt, wall, ms * 1e-3, setup, nsday, S.ncons, S.ndof, mixed_ ? "mixed FP32/fixed-point" : "FP64");
+                  "%lld steps of %.2f fs in %.3f s (device %.3f s, set-up %.3f s) · %.2f ns/day · %d constraints · %.0f degrees of freedom · %s"
+                  " · tuned: %d entries per work item, PME line blocks %d/%d/%d",
+                  (long long)o.steps, o.dt, wall, ms * 1e-3, setup, nsday, S.ncons, S.ndof, mixed_ ? "mixed FP32/fixed-point" : "FP64", batch_,
+                  lines_x_, lines_y_, lines_z_);
     *report = b;
   }
 }
@@ -1483,15 +1485,9 @@ void run_batch(const std::vector<Engine*>& es, caps_gpu_state* const* states, co
   const size_t R = es.size();
   if (R == 0) return;
   const long long steps = mds[0]->steps;
-  int dev0 = -1;
   for (size_t r = 0; r < R; ++r) {
     es[r]->validate_md(*mds[r]);
     if (mds[r]->steps != steps) throw ModelError(CAPS_GPU_EINVAL, "the replicas of a batch run the same number of steps");
-    cudaPointerAttributes pa{};
-    int dev = 0;
-    CK(cudaGetDevice(&dev));
-    if (dev0 < 0) dev0 = dev;
-    (void)pa;
   }
   std::vector<std::unique_ptr<MdRun>> runs;
   for (size_t r = 0; r < R; ++r) {

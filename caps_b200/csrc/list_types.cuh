@@ -17,6 +17,7 @@ struct ListGeom {
   double w[3];        // perpendicular widths of the cell
   double rlist, rlist2;
   double dw;          // rlist / w[2]
+  int batch;          // entries per work item (the pair kernels' j-tile depth), at most kBatch; chosen by timing
 };
 
 struct ListBufs {

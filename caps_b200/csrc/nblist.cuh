@@ -466,7 +466,7 @@ static __global__ void __launch_bounds__(32 * kSearchWarps) k_search(DevCell cel
           }
           const unsigned ball = __ballot_sync(0xffffffffu, have);
           if (have) {
-            const int pos = B.nent + __popc(ball & ((1u << lane) - 1));
+            const int pos = B.nent + __popc(ball & ((1u << lane) - 1));   // < batch + 32 <= 2 kBatch (flushed below)
             const int sjc = cj >> 3;
             B.ent[pos] = make_uint4(unsigned(cj), imask | (img << 8), 0u, 0u);
             B.sh[pos] = make_float4(float(b.sc_org[3 * sjc] + S0 - S.org_i[0]), float(b.sc_org[3 * sjc + 1] + S1 - S.org_i[1]),
@@ -476,14 +476,24 @@ static __global__ void __launch_bounds__(32 * kSearchWarps) k_search(DevCell cel
           __syncwarp();
           if (lane == 0) B.nent += __popc(ball);
           __syncwarp();
-          if (B.nent >= kBatch) {
-            flush_batch(S, B, sc, kBatch, lane, b);
+          while (B.nent >= g.batch) {   // a pass adds up to 32 entries: with a depth below 32 more than one batch fills
+            flush_batch(S, B, sc, g.batch, lane, b);
             __syncwarp();
-            const int rest = B.nent - kBatch;
-            for (int e = lane; e < rest; e += 32) {
-              B.ent[e] = B.ent[kBatch + e];
-              B.sh[e] = B.sh[kBatch + e];
-              B.needs_mask[e] = B.needs_mask[kBatch + e];
+            // the rest (< 2 kBatch - batch entries) moves down: read all, then write (the ranges can overlap)
+            const int rest = B.nent - g.batch;
+            uint4 te[2];
+            float4 ts[2];
+            unsigned char tm[2];
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+              const int e = lane + 32 * k;
+              if (e < rest) te[k] = B.ent[g.batch + e], ts[k] = B.sh[g.batch + e], tm[k] = B.needs_mask[g.batch + e];
+            }
+            __syncwarp();
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+              const int e = lane + 32 * k;
+              if (e < rest) B.ent[e] = te[k], B.sh[e] = ts[k], B.needs_mask[e] = tm[k];
             }
             __syncwarp();
             if (lane == 0) B.nent = rest;

@@ -58,6 +58,46 @@ void Engine::fork(int k, const std::function<void()>& launch) {
 
 void Engine::join(int k) { CK(cudaStreamWaitEvent(stream_, ev_join_[k], 0)); }
 
+// Autotuner for the j-tile depth: the list is built with 32, 24 and 16 entries per work item and the pair kernel timed
+// on each (fewer entries per item balance small systems better, more amortise the per-item work); the fastest is kept
+// for this engine. Runs once, at the first non-bonded evaluation (never inside a stream capture).
+void Engine::tune_batch(const double* d_x) {
+  batch_tuned_ = true;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int pick = batch_;
+  const size_t ns = size_t(nsc_cap_) * kScAtoms;
+  for (int bsz : {32, 24, 16}) {
+    geom_.batch = bsz;
+    k_set_flag<<<1, 1, 0, stream_>>>(d_counters_.p, kCntRebuild, 1);
+    launch_build(d_x);
+    if (mixed_)
+      k_pack_f32<<<blocks_for(ns, 256), 256, 0, stream_>>>(int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_sc_org_.p, d_q_.p, d_type_.p, nt_,
+                                                           d_xq_.p, d_tslot_.p, d_counters_.p);
+    else
+      k_pack_f64<<<blocks_for(ns, 256), 256, 0, stream_>>>(int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_q_.p, d_type_.p, nt_, d_xqd_.p, d_tslot_.p,
+                                                           d_counters_.p);
+    prune(d_x);
+    float ms = 0;
+    for (int rep = 0; rep < 4; ++rep) {
+      CK(cudaMemsetAsync(d_counters_.p + kCntPairNext, 0, sizeof(int), stream_));
+      if (rep == 1) CK(cudaEventRecord(e0, stream_));
+      pair_forces(false, false);
+    }
+    CK(cudaEventRecord(e1, stream_));
+    CK(cudaEventSynchronize(e1));
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best) best = ms, pick = bsz;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  batch_ = pick;
+  geom_.batch = pick;
+  list_valid_ = false;   // the evaluation that follows builds the list with the chosen depth
+}
+
 int Engine::list_builds() {
   int v = 0;
   CK(cudaMemcpyAsync(&v, d_counters_.p + kCntBuilds, sizeof(int), cudaMemcpyDeviceToHost, stream_));
@@ -190,6 +230,7 @@ void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild, 
   const int pm = parts >= 0 ? parts : ((opt_.parts & 1) | ((opt_.parts & 2) ? 6 : 0));
   const bool nonb = (pm & 2) != 0;
   double* out = d_out ? d_out : d_f_.p;
+  if (nonb && !batch_tuned_) tune_batch(d_x);
   if (mixed_) {
     CK(cudaMemsetAsync(d_F_.p, 0, d_F_.n * sizeof(long long), stream_));
     if (nonb) CK(cudaMemsetAsync(d_Fs_.p, 0, d_Fs_.n * sizeof(long long), stream_));

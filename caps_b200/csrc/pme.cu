@@ -1,6 +1,9 @@
 // Host side of PME: plans, twiddle tables and line blocking per grid, and the spread / transform / solve / gather
 // launch sequence.
 #include <algorithm>
+#include <array>
+#include <map>
+#include <mutex>
 #include <cmath>
 #include <cstring>
 #include <functional>
@@ -57,8 +60,81 @@ void Engine::pme_setup(PmePath<R>& P) {
   const int la = int(128 / sizeof(T));
   lines_y_ = std::max(1, std::min({la, cap / pk_[1], ph1_}));
   lines_z_ = std::max(1, std::min({la, cap / pk_[2], ph1_}));
+  pme_tune(P);
   green_valid_ = false;
   CK(cudaStreamSynchronize(stream_));
+}
+
+// The five line-transform passes of one PME evaluation (forward x, y; z with the solve; inverse y, x).
+template <class R>
+void Engine::fft_passes(PmePath<R>& P, bool ener, bool vir) {
+  using T = typename Cpx<R>::T;
+  PmeArgs A{pk_[0], pk_[1], pk_[2], ph1_, dcell_, nullptr, d_q_.p, n_};
+  // shared memory: twiddle table(s) + two line buffers
+  const size_t sx = (size_t(lines_x_) * 2 + 1) * pk_[0] * sizeof(T), sy = (size_t(lines_y_) * 2 + 1) * pk_[1] * sizeof(T),
+               sz = (size_t(lines_z_) + 1) * 2 * pk_[2] * sizeof(T);
+  const int nlx = pk_[1] * pk_[2];
+  k_fft_x_fwd<R><<<blocks_for(size_t(nlx), lines_x_), 128, sx, stream_>>>(A, mixed_ ? nullptr : d_grid_.p, mixed_ ? d_gridq_.p : nullptr, P.h.p,
+                                                                        P.plan[0][0], lines_x_);
+  const int gy = ((ph1_ + lines_y_ - 1) / lines_y_) * pk_[2];
+  k_fft_y<R><<<gy, 128, sy, stream_>>>(A, P.h.p, P.plan[1][0], lines_y_);
+  const int gz = ((ph1_ + lines_z_ - 1) / lines_z_) * pk_[1];
+  EnergySink en{d_efix_.p, d_edbl_.p};
+  if (ener) { if (vir) k_fft_z_solve<R, true, true><<<gz, 128, sz, stream_>>>(A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); else k_fft_z_solve<R, true, false><<<gz, 128, sz, stream_>>>(A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); }
+  else { if (vir) k_fft_z_solve<R, false, true><<<gz, 128, sz, stream_>>>(A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); else k_fft_z_solve<R, false, false><<<gz, 128, sz, stream_>>>(A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); }
+  k_fft_y<R><<<gy, 128, sy, stream_>>>(A, P.h.p, P.plan[1][1], lines_y_);
+  k_fft_x_inv<R><<<blocks_for(size_t(nlx), lines_x_), 128, sx, stream_>>>(A, P.h.p, P.gr.p, P.plan[0][1], lines_x_);
+}
+
+// Autotuner for the line transforms: every block shape that fits (x: 1-16 lines per block; y, z: 1-8 consecutive a per
+// block) is timed on this grid (the transforms' time does not depend on the values), and the fastest kept. Results are
+// cached per grid, precision and SM count for the process.
+template <class R>
+void Engine::pme_tune(PmePath<R>& P) {
+  using T = typename Cpx<R>::T;
+  static std::mutex mu;
+  static std::map<std::array<int, 5>, std::array<int, 3>> cache;
+  const std::array<int, 5> key{pk_[0], pk_[1], pk_[2], int(sizeof(R)), dev_sms_};
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+      lines_x_ = it->second[0], lines_y_ = it->second[1], lines_z_ = it->second[2];
+      return;
+    }
+  }
+  const size_t half = size_t(ph1_) * pk_[1] * pk_[2];
+  CK(cudaMemsetAsync(P.gt.p, 0, half * sizeof(R), stream_));
+  CK(cudaMemsetAsync(P.wt.p, 0, 6 * half * sizeof(R), stream_));
+  CK(cudaMemsetAsync(P.h.p, 0, half * sizeof(T), stream_));
+  if (mixed_) CK(cudaMemsetAsync(d_gridq_.p, 0, d_gridq_.n * sizeof(long long), stream_));
+  else CK(cudaMemsetAsync(d_grid_.p, 0, d_grid_.n * sizeof(double), stream_));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const size_t smax = 48 * 1024;
+  float best = 1e30f;
+  std::array<int, 3> pick{lines_x_, lines_y_, lines_z_};
+  for (int lx : {1, 2, 4, 8, 16})
+    for (int la : {1, 2, 4, 8}) {
+      if ((size_t(lx) * 2 + 1) * pk_[0] * sizeof(T) > smax) continue;
+      const int ly = std::min(la, ph1_), lz = std::min(la, ph1_);
+      if ((size_t(ly) * 2 + 1) * pk_[1] * sizeof(T) > smax || (size_t(lz) + 1) * 2 * pk_[2] * sizeof(T) > smax) continue;
+      lines_x_ = lx, lines_y_ = ly, lines_z_ = lz;
+      fft_passes(P, false, false);   // warm
+      CK(cudaEventRecord(e0, stream_));
+      for (int rep = 0; rep < 3; ++rep) fft_passes(P, false, false);
+      CK(cudaEventRecord(e1, stream_));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < best) best = ms, pick = {lx, ly, lz};
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  lines_x_ = pick[0], lines_y_ = pick[1], lines_z_ = pick[2];
+  std::lock_guard<std::mutex> lock(mu);
+  cache[key] = pick;
 }
 
 template <class R>
@@ -88,20 +164,7 @@ void Engine::pme_run(PmePath<R>& P, const double* d_x, bool ener, bool vir) {
     default: SPREAD(8); break;
   }
 #undef SPREAD
-  // shared memory: twiddle table(s) + two line buffers
-  const size_t sx = (size_t(lines_x_) * 2 + 1) * pk_[0] * sizeof(T), sy = (size_t(lines_y_) * 2 + 1) * pk_[1] * sizeof(T),
-               sz = (size_t(lines_z_) + 1) * 2 * pk_[2] * sizeof(T);
-  const int nlx = pk_[1] * pk_[2];
-  k_fft_x_fwd<R><<<blocks_for(size_t(nlx), lines_x_), 128, sx, stream_>>>(A, mixed_ ? nullptr : d_grid_.p, mixed_ ? d_gridq_.p : nullptr, P.h.p,
-                                                                        P.plan[0][0], lines_x_);
-  const int gy = ((ph1_ + lines_y_ - 1) / lines_y_) * pk_[2];
-  k_fft_y<R><<<gy, 128, sy, stream_>>>(A, P.h.p, P.plan[1][0], lines_y_);
-  const int gz = ((ph1_ + lines_z_ - 1) / lines_z_) * pk_[1];
-  EnergySink en{d_efix_.p, d_edbl_.p};
-  if (ener) { if (vir) k_fft_z_solve<R, true, true><<<gz, 128, sz, stream_>>>(A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); else k_fft_z_solve<R, true, false><<<gz, 128, sz, stream_>>>(A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); }
-  else { if (vir) k_fft_z_solve<R, false, true><<<gz, 128, sz, stream_>>>(A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); else k_fft_z_solve<R, false, false><<<gz, 128, sz, stream_>>>(A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); }
-  k_fft_y<R><<<gy, 128, sy, stream_>>>(A, P.h.p, P.plan[1][1], lines_y_);
-  k_fft_x_inv<R><<<blocks_for(size_t(nlx), lines_x_), 128, sx, stream_>>>(A, P.h.p, P.gr.p, P.plan[0][1], lines_x_);
+  fft_passes(P, ener, vir);
   const ForceSink<float> Ff{d_F_.p, d_F_.p + n_, d_F_.p + 2 * size_t(n_), d_counters_.p + kCntErr};
   const ForceSink<double> Fd{d_Fd_.p, d_Fd_.p + n_, d_Fd_.p + 2 * size_t(n_)};
 #define GATHER(P_)                                                                            \
@@ -126,5 +189,7 @@ void Engine::pme_forces(const double* d_x, bool ener, bool vir) { pme_run(pd_, d
 
 template void Engine::pme_setup<double>(PmePath<double>&);
 template void Engine::pme_run<double>(PmePath<double>&, const double*, bool, bool);
+template void Engine::fft_passes<double>(PmePath<double>&, bool, bool);
+template void Engine::pme_tune<double>(PmePath<double>&);
 
 }  // namespace capsb

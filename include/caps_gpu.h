@@ -174,7 +174,7 @@ int32_t caps_gpu_list_builds(const caps_gpu_engine* e);
 int32_t caps_gpu_run(caps_gpu_engine* e, caps_gpu_state* state, const caps_gpu_md_opts* md, caps_gpu_progress_fn progress,
                      caps_gpu_frame_fn frame, void* user, char* report, int32_t report_cap);
 /* Independent replicas in lock step, one engine each (own force field, state and dynamics options; the same number of
- * steps). Replaces running run_dynamics once per replica (core/src/dynamics.cpp:71, called in turn for each rung of a
+ * steps; all engines created on the current device). Replaces running run_dynamics once per replica (core/src/dynamics.cpp:71, called in turn for each rung of a
  * Tg ladder or each seed of a protocol, e.g. core/src/mechanics.cpp:1381): a step on which no replica reports, records
  * a frame, rescales its cell or refills its thermostat draws is one CUDA graph launch for all replicas. progress and
  * frame receive user[r] for replica r. Errors: caps_gpu_error(engines[0]). Afterwards every engine's
