@@ -422,6 +422,7 @@ void Engine::set_cell(const double* cell) {
   geom_ = g;
   if (geom_changed) {
     d_col_count_.alloc(size_t(g.ncol));
+    d_col_count_.zero(stream_);   // the scan clears it after every build
     d_col_fill_.alloc(size_t(g.ncol));
     d_col_start_.alloc(size_t(g.ncol) + 1);
     d_col_sc_.alloc(size_t(g.ncol) + 1);

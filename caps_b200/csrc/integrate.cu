@@ -642,6 +642,13 @@ __device__ void bussi_body(double* sc, const double2* __restrict__ draws, long l
   sc[kScBath] -= knew - k;
 }
 
+// The first Nose-Hoover half step of a step, on the kinetic energy the previous step left in sc[kScKE]: its second half
+// set it to the scaled velocities' value, and the velocities have not changed since.
+__global__ void k_nhc_begin(Chain* ch, double* sc, double t0, double t1, long long steps, double ndof, double t_freq, double dt) {
+  step_begin_body(sc, t0, t1, steps, ndof);
+  nhc_body(ch, sc, ndof, t_freq, dt);
+}
+
 // What the last block of k_ke does with the fresh kinetic energy.
 enum KeThen { kThenNone = 0, kThenNhc, kThenBussi, kThenBath };
 struct KeArgs {
@@ -1050,7 +1057,7 @@ struct Stepper {
   void fast_forces() { E.forces(x.p, false, false, true, fast_parts, f_fast.p, true); }
 
   // One MD step (dynamics.cpp:606-666), energies and virial on request. Kernel sequence per step: NVT Nose-Hoover
-  // KE+chain, kick+drift, SHAKE, forces, kick+RATTLE, KE+chain, scale; Bussi step-begin, kick+drift, SHAKE, forces,
+  // chain (on the kinetic energy the last step left), kick+drift, SHAKE, forces, kick+RATTLE, KE+chain, scale; Bussi step-begin, kick+drift, SHAKE, forces,
   // kick+RATTLE, KE+Bussi, scale; Langevin (BAOAB) kick+drift, SHAKE, KE, O+RATTLE, KE+bath, drift, SHAKE, forces,
   // kick+RATTLE.
   void step(bool ener, bool vir) {
@@ -1089,14 +1096,12 @@ struct Stepper {
       forces(ener, vir);
       vel_rattle(kick_op(0.5 * dt), dt);
     } else if (nhc) {
-      KeArgs A = ke_args(kScKE, false);
-      A.begin = 1;
-      A.then = kThenNhc;
-      ke_launch(A);
+      k_nhc_begin<<<1, 1, 0, E.stream_>>>(chain.p, sc.p, o.temperature, o.temperature_end, (long long)o.steps, ndof, t_freq, dt);
       kick_drift(0.5 * dt, dt, true, true);
       forces(ener, vir);
       vel_rattle(kick_op(0.5 * dt), dt);
-      A.begin = 0;
+      KeArgs A = ke_args(kScKE, false);
+      A.then = kThenNhc;
       ke_launch(A);
       scale_v();
     } else {
@@ -1398,6 +1403,7 @@ void MdRun::baro_step(long long s) {
     S.rattle(0);
   }
   S.forces(true, true);
+  S.ke(kScKE, false);   // the rescaled velocities' kinetic energy, which the next Nose-Hoover step starts from
   S.drop_graphs();   // the cell is a parameter of the captured kernels
   ++generation;
 }

@@ -36,23 +36,6 @@ static __global__ void k_check_step(int n, const double* __restrict__ x, const d
 }
 
 
-// Clears the column counts before a build (gated like the rest of the build).
-static __global__ void k_clear_columns(ListGeom g, ListBufs b) {
-  if (build_off(b.counters)) return;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < g.ncol; c += gridDim.x * blockDim.x) b.col_count[c] = 0;
-}
-
-// Ends a build: keeps the positions the list was built at; a fresh list is pruned at once.
-static __global__ void k_end_build(int n, const double* __restrict__ x, double* __restrict__ x0, int* counters) {
-  if (build_off(counters)) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < 3 * n) x0[i] = x[i];
-  if (i == 0) {
-    counters[kCntPrune] = 1;
-    counters[kCntBuilds] += 1;
-  }
-}
-
 // K-BIN: wrapped fractional coordinates, lattice offsets and the column of every atom; column counts.
 static __global__ void k_bin(int n, const double* __restrict__ x, DevCell cell, ListGeom g, ListBufs b) {
   if (build_off(b.counters)) return;
@@ -88,6 +71,7 @@ static __global__ void k_scan_columns(ListGeom g, ListBufs b) {
   for (int base = 0; base < g.ncol; base += blockDim.x) {
     const int c = base + threadIdx.x;
     const int cnt = c < g.ncol ? b.col_count[c] : 0;
+    if (c < g.ncol) b.col_count[c] = 0;   // cleared for the next build's binning
     if (c < g.ncol) atomicMax(&s_max, cnt);
     s_a[threadIdx.x] = cnt;
     s_s[threadIdx.x] = (cnt + kScAtoms - 1) / kScAtoms;

@@ -75,10 +75,10 @@ void Engine::tune_batch(const double* d_x) {
     launch_build(d_x);
     if (mixed_)
       k_pack_f32<<<blocks_for(ns, 256), 256, 0, stream_>>>(int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_sc_org_.p, d_q_.p, d_type_.p, nt_,
-                                                           d_xq_.p, d_tslot_.p, d_counters_.p);
+                                                           d_xq_.p, d_tslot_.p, d_counters_.p, d_x0_.p);
     else
       k_pack_f64<<<blocks_for(ns, 256), 256, 0, stream_>>>(int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_q_.p, d_type_.p, nt_, d_xqd_.p, d_tslot_.p,
-                                                           d_counters_.p);
+                                                           d_counters_.p, d_x0_.p);
     prune(d_x);
     float ms = 0;
     for (int rep = 0; rep < 4; ++rep) {
@@ -108,7 +108,6 @@ int Engine::list_builds() {
 // ---------------------------------------------------------------------------------------------------------------
 void Engine::launch_build(const double* d_x) {
   const ListGeom& g = geom_;
-  k_clear_columns<<<blocks_for(size_t(g.ncol), 256), 256, 0, stream_>>>(g, lb_);
   k_bin<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_x, dcell_, g, lb_);
   k_scan_columns<<<1, 1024, 0, stream_>>>(g, lb_);
   k_scatter<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, lb_);
@@ -117,7 +116,6 @@ void Engine::launch_build(const double* d_x) {
   k_superclusters<<<std::max(1, std::min(blocks_for(size_t(nsc_cap_), 4), dev_sms_ * 16)), 128, 0, stream_>>>(dcell_, lb_);
   k_search<<<std::max(1, std::min(nsc_cap_, dev_sms_ * 8)), 32 * kSearchWarps, sizeof(SearchShared), stream_>>>(dcell_, g, d_excl_off_.p,
                                                                                                           d_excl_list_.p, lb_);
-  k_end_build<<<blocks_for(size_t(3) * n_, 256), 256, 0, stream_>>>(n_, d_x, d_x0_.p, lb_.counters);
   CK(cudaGetLastError());
 }
 
@@ -167,9 +165,8 @@ void Engine::prune(const double* d_x) {
   const double b = std::min(0.8, skin_);
   const PairArgs A = pair_args();
   const double rp = rc_ + b;
-  if (mixed_) k_prune<false><<<dev_sms_ * 8, 128, 0, stream_>>>(A, rp * rp, d_ent_.p);
-  else k_prune<true><<<dev_sms_ * 8, 128, 0, stream_>>>(A, rp * rp, d_ent_.p);
-  k_end_prune<<<blocks_for(size_t(3) * n_, 256), 256, 0, stream_>>>(n_, d_x, d_xp_.p, d_counters_.p);
+  if (mixed_) k_prune<false><<<dev_sms_ * 8, 128, 0, stream_>>>(A, rp * rp, d_ent_.p, n_, d_x, d_xp_.p);
+  else k_prune<true><<<dev_sms_ * 8, 128, 0, stream_>>>(A, rp * rp, d_ent_.p, n_, d_x, d_xp_.p);
 }
 
 void Engine::pair_forces(bool ener, bool vir) {
@@ -259,10 +256,10 @@ void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild, 
     const size_t ns = size_t(nsc_cap_) * kScAtoms;
     if (mixed_)
       k_pack_f32<<<blocks_for(ns, 256), 256, 0, stream_>>>(int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_sc_org_.p, d_q_.p, d_type_.p, nt_,
-                                                           d_xq_.p, d_tslot_.p, d_counters_.p);
+                                                           d_xq_.p, d_tslot_.p, d_counters_.p, d_x0_.p);
     else
       k_pack_f64<<<blocks_for(ns, 256), 256, 0, stream_>>>(int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_q_.p, d_type_.p, nt_, d_xqd_.p, d_tslot_.p,
-                                                           d_counters_.p);
+                                                           d_counters_.p, d_x0_.p);
     prune(d_x);
     pair_forces(ener, vir);
   }

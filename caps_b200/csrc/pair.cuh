@@ -23,9 +23,16 @@ constexpr float kPadFar = 1.0e5f;   // padding slots sit this far from their sup
 // K-PACK (FP32): per slot, float4 (position relative to the super-cluster origin, charge) and the type index.
 static __global__ void k_pack_f32(int nslots, const int* __restrict__ perm, const double* __restrict__ x, const int* __restrict__ ioff, DevCell cell,
                            const double* __restrict__ sc_org, const double* __restrict__ q, const int* __restrict__ type, int pad_type,
-                           float4* __restrict__ xq, int* __restrict__ tslot, int* counters) {
+                           float4* __restrict__ xq, int* __restrict__ tslot, int* counters, double* __restrict__ x0) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s == 0) counters[kCntPairNext] = 0;   // the pair kernel's work-item counter
+  const bool built = counters[kCntRebuild] != 0;   // a build ran this step: the list was built at these positions
+  if (s == 0) {
+    counters[kCntPairNext] = 0;   // the pair kernel's work-item counter
+    if (built) {
+      counters[kCntPrune] = 1;    // a fresh list is pruned at once
+      counters[kCntBuilds] += 1;
+    }
+  }
   const int nsc = counters[kCntNsc];
   if (s >= nslots || s >= 64 * nsc) return;
   const int a = perm[s];
@@ -34,6 +41,8 @@ static __global__ void k_pack_f32(int nslots, const int* __restrict__ perm, cons
     tslot[s] = pad_type;
     return;
   }
+  if (built)
+    for (int r = 0; r < 3; ++r) x0[3 * a + r] = x[3 * a + r];
   const int sc = s >> 6;
   const int o0 = ioff[3 * a], o1 = ioff[3 * a + 1], o2 = ioff[3 * a + 2];
   float p[3];
@@ -46,9 +55,16 @@ static __global__ void k_pack_f32(int nslots, const int* __restrict__ perm, cons
 // K-PACK (FP64): per slot, double4 (wrapped absolute position, charge) and the type index.
 static __global__ void k_pack_f64(int nslots, const int* __restrict__ perm, const double* __restrict__ x, const int* __restrict__ ioff, DevCell cell,
                            const double* __restrict__ q, const int* __restrict__ type, int pad_type, double4* __restrict__ xq, int* __restrict__ tslot,
-                           int* counters) {
+                           int* counters, double* __restrict__ x0) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s == 0) counters[kCntPairNext] = 0;   // the pair kernel's work-item counter
+  const bool built = counters[kCntRebuild] != 0;
+  if (s == 0) {
+    counters[kCntPairNext] = 0;
+    if (built) {
+      counters[kCntPrune] = 1;
+      counters[kCntBuilds] += 1;
+    }
+  }
   const int nsc = counters[kCntNsc];
   if (s >= nslots || s >= 64 * nsc) return;
   const int a = perm[s];
@@ -57,6 +73,8 @@ static __global__ void k_pack_f64(int nslots, const int* __restrict__ perm, cons
     tslot[s] = pad_type;
     return;
   }
+  if (built)
+    for (int r = 0; r < 3; ++r) x0[3 * a + r] = x[3 * a + r];
   const int o0 = ioff[3 * a], o1 = ioff[3 * a + 1], o2 = ioff[3 * a + 2];
   double p[3];
   for (int r = 0; r < 3; ++r) p[r] = x[3 * a + r] + (cell.h[r][0] * o0 + cell.h[r][1] * o1 + cell.h[r][2] * o2);
@@ -533,8 +551,12 @@ static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
 // the prune flag, set by the displacement check and by every list build. FP32 path: packed float positions; FP64 path:
 // packed double positions.
 template <bool DBL>
-static __global__ void __launch_bounds__(128) k_prune(PairArgs A, double rprune2, uint4* __restrict__ ent) {
+static __global__ void __launch_bounds__(128) k_prune(PairArgs A, double rprune2, uint4* __restrict__ ent, int n, const double* __restrict__ x,
+                                                     double* __restrict__ xp) {
   if (*(volatile const int*)(A.counters + kCntPrune) == 0) return;
+  // the positions of this prune, for the next displacement check; and the prune count
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * n; i += gridDim.x * blockDim.x) xp[i] = x[i];
+  if (blockIdx.x == 0 && threadIdx.x == 0) const_cast<int*>(A.counters)[kCntPrunes] += 1;
   if (A.counters[kCntErr] & (kErrListOverflow | kErrMaskOverflow | kErrScOverflow | kErrColumnTooBig | kErrExclOverflow)) return;
   __shared__ float4 s_xi[4][64];
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -603,12 +625,5 @@ static __global__ void __launch_bounds__(128) k_prune(PairArgs A, double rprune2
   }
 }
 
-// Ends a prune: keeps the positions it was done at (one thread per coordinate) and counts the prune.
-static __global__ void k_end_prune(int n, const double* __restrict__ x, double* __restrict__ xp, int* counters) {
-  if (*(volatile const int*)(counters + kCntPrune) == 0) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < 3 * n) xp[i] = x[i];
-  if (i == 0) counters[kCntPrunes] += 1;
-}
 
 }  // namespace capsb
