@@ -200,7 +200,10 @@ static __global__ void __launch_bounds__(128, 5) k_pair_f32(PairArgs A) {
   const float rc2 = float(A.rc2), beta = float(A.beta), kc = float(A.kc), kcoul = float(A.kcoul);
   const float ku = float(A.beta * A.beta / kEwUMax), kap3 = float(A.beta * A.beta * A.beta);
   const float e0 = float(A.dsf_e0), f0 = float(A.dsf_f0), rcf = float(A.rc);
-  double acc_v = 0, acc_c = 0, acc_w[6] = {0, 0, 0, 0, 0, 0}, acc_np = 0, acc_nl = 0;
+  // energy and virial: each work item's sums rounded to fixed point on their own, so that the totals do not depend on
+  // which warp took which item
+  long long acc_v = 0, acc_c = 0, acc_w[6] = {0, 0, 0, 0, 0, 0};
+  double acc_np = 0, acc_nl = 0;
   for (int w = next_work_item(A.counters, lane); w < nwork; w = next_work_item(A.counters, lane)) {
     const int4 wk = A.work[w];
     const int sc = wk.x;
@@ -352,24 +355,24 @@ static __global__ void __launch_bounds__(128, 5) k_pair_f32(PairArgs A) {
       }
     }
     if (ENER) {
-      acc_v += double(warp_sum(ev));
-      acc_c += double(warp_sum(ec));
-      acc_np += double(warp_sum(npair));
+      acc_v += to_fix(double(warp_sum(ev)), kFixE);
+      acc_c += to_fix(double(warp_sum(ec)), kFixE);
+      acc_np += double(warp_sum(npair));   // whole numbers: exact in any order
       acc_nl += double(warp_sum(nlist));
     }
     if (VIR)
-      for (int k = 0; k < 6; ++k) acc_w[k] += double(warp_sum(vw[k]));
+      for (int k = 0; k < 6; ++k) acc_w[k] += to_fix(double(warp_sum(vw[k])), kFixE);
     __syncwarp();
   }
   if (lane == 0) {
     if (ENER) {
-      A.en.add(kEVdw, acc_v, true);
-      A.en.add(kECoul, acc_c, true);
+      atomic_add_fix(A.en.fix + kEVdw, acc_v);
+      atomic_add_fix(A.en.fix + kECoul, acc_c);
       A.en.add(kEPairs, acc_np, true);
       A.en.add(kEListed, acc_nl, true);
     }
     if (VIR)
-      for (int k = 0; k < 6; ++k) A.en.add(kEW0 + k, acc_w[k], true);
+      for (int k = 0; k < 6; ++k) atomic_add_fix(A.en.fix + kEW0 + k, acc_w[k]);
   }
 }
 
@@ -558,7 +561,10 @@ static __global__ void __launch_bounds__(128) k_prune(PairArgs A, double rprune2
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * n; i += gridDim.x * blockDim.x) xp[i] = x[i];
   if (blockIdx.x == 0 && threadIdx.x == 0) const_cast<int*>(A.counters)[kCntPrunes] += 1;
   if (A.counters[kCntErr] & (kErrListOverflow | kErrMaskOverflow | kErrScOverflow | kErrColumnTooBig | kErrExclOverflow)) return;
+  // per warp: the work item's i atoms, its entries' j atoms (w: 1 real, 0 padding) and the new half masks
   __shared__ float4 s_xi[4][64];
+  __shared__ float4 s_xj[4][kBatch * 8];
+  __shared__ unsigned s_keep[4][kBatch];
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i8 = lane & 7, jq = lane >> 3;
   const int nwork = min(A.counters[kCntWork], A.work_cap);
@@ -567,6 +573,23 @@ static __global__ void __launch_bounds__(128) k_prune(PairArgs A, double rprune2
   for (int w = blockIdx.x * 4 + wib; w < nwork; w += gridDim.x * 4) {
     const int4 wk = A.work[w];
     const int sc = wk.x;
+    const int ne = min(wk.z, kBatch);
+    // one batch of independent loads: i atoms, the entries, then every entry's 8 j atoms with the entry's image shift
+    uint4 en = make_uint4(0u, 0u, 0u, 0u);
+    float sx = 0.f, sy = 0.f, sz = 0.f;
+    if (lane < ne) {
+      en = ent[wk.y + lane];
+      if (DBL) {
+        int qa, qb, qc;
+        unpack_image(en.y >> 8, qa, qb, qc);
+        sx = float(A.cell.h[0][0] * qa + A.cell.h[0][1] * qb + A.cell.h[0][2] * qc);
+        sy = float(A.cell.h[1][0] * qa + A.cell.h[1][1] * qb + A.cell.h[1][2] * qc);
+        sz = float(A.cell.h[2][0] * qa + A.cell.h[2][1] * qb + A.cell.h[2][2] * qc);
+      } else {
+        const float4 sh = A.ent_shift[wk.y + lane];
+        sx = sh.x, sy = sh.y, sz = sh.z;
+      }
+    }
     for (int t = lane; t < 64; t += 32) {
       float4 v;
       if (DBL) {
@@ -578,30 +601,32 @@ static __global__ void __launch_bounds__(128) k_prune(PairArgs A, double rprune2
       v.w = A.tslot[64 * sc + t] != pad ? 1.f : 0.f;
       s_xi[wib][t] = v;
     }
-    __syncwarp();
-    for (int e = wk.y; e < wk.y + wk.z; ++e) {
-      uint4 en = ent[e];
-      const unsigned built = en.y & 255u;
-      const int j0 = 8 * int(en.x) + jq, j1 = j0 + 4;
-      float xj[2], yj[2], zj[2];
-      bool rj[2];
-      if (DBL) {
-        int qa, qb, qc;
-        unpack_image(en.y >> 8, qa, qb, qc);
-        const double Sx = A.cell.h[0][0] * qa + A.cell.h[0][1] * qb + A.cell.h[0][2] * qc;
-        const double Sy = A.cell.h[1][0] * qa + A.cell.h[1][1] * qb + A.cell.h[1][2] * qc;
-        const double Sz = A.cell.h[2][0] * qa + A.cell.h[2][1] * qb + A.cell.h[2][2] * qc;
-        const double4 b0 = A.xqd[j0], b1 = A.xqd[j1];
-        xj[0] = float(b0.x + Sx), yj[0] = float(b0.y + Sy), zj[0] = float(b0.z + Sz);
-        xj[1] = float(b1.x + Sx), yj[1] = float(b1.y + Sy), zj[1] = float(b1.z + Sz);
-      } else {
-        const float4 sh = A.ent_shift[e];
-        const float4 b0 = A.xq[j0], b1 = A.xq[j1];
-        xj[0] = b0.x + sh.x, yj[0] = b0.y + sh.y, zj[0] = b0.z + sh.z;
-        xj[1] = b1.x + sh.x, yj[1] = b1.y + sh.y, zj[1] = b1.z + sh.z;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int t = lane + 32 * k;   // entry t / 8, j atom t % 8
+      const int e = t >> 3;
+      const unsigned cj = __shfl_sync(0xffffffffu, en.x, e & 31);
+      const float ex = __shfl_sync(0xffffffffu, sx, e & 31), ey = __shfl_sync(0xffffffffu, sy, e & 31),
+                  ez = __shfl_sync(0xffffffffu, sz, e & 31);
+      if (e < ne) {
+        const int ja = 8 * int(cj) + (t & 7);
+        float4 v;
+        // FP64 path: absolute positions rounded to float (1e-5 Å at 100 Å), far inside the 0.8 Å prune margin
+        if (DBL) {
+          const double4 d = A.xqd[ja];
+          v = make_float4(float(d.x), float(d.y), float(d.z), 0.f);
+        } else {
+          v = A.xq[ja];
+        }
+        v.x += ex, v.y += ey, v.z += ez;
+        v.w = A.tslot[ja] != pad ? 1.f : 0.f;
+        s_xj[wib][t] = v;
       }
-      rj[0] = A.tslot[j0] != pad;
-      rj[1] = A.tslot[j1] != pad;
+    }
+    __syncwarp();
+    for (int el = 0; el < ne; ++el) {
+      const unsigned built = __shfl_sync(0xffffffffu, en.y, el) & 255u;
+      const float4 a0 = s_xj[wib][8 * el + jq], a1 = s_xj[wib][8 * el + jq + 4];
       unsigned keep = 0;
 #pragma unroll
       for (int c = 0; c < 8; ++c) {
@@ -609,17 +634,19 @@ static __global__ void __launch_bounds__(128) k_prune(PairArgs A, double rprune2
         const float4 xi = s_xi[wib][8 * c + i8];
 #pragma unroll
         for (int jj = 0; jj < 2; ++jj) {
-          // FP64 path: absolute positions rounded to float (1e-5 Å at 100 Å), far inside the 0.8 Å prune margin
-          const float dx = xj[jj] - xi.x, dy = yj[jj] - xi.y, dz = zj[jj] - xi.z;
+          const float4 xj = jj ? a1 : a0;
+          const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
           const float r2 = dx * dx + dy * dy + dz * dz;
-          const bool in = xi.w != 0.f && rj[jj] && r2 < rp2;
+          const bool in = xi.w != 0.f && xj.w != 0.f && r2 < rp2;
           if (__any_sync(0xffffffffu, in)) keep |= 1u << (c + 8 * jj);
         }
       }
-      if (lane == 0) {
-        en.w = keep;
-        ent[e] = en;
-      }
+      if (lane == 0) s_keep[wib][el] = keep;
+    }
+    __syncwarp();
+    if (lane < ne) {
+      en.w = s_keep[wib][lane];
+      ent[wk.y + lane] = en;
     }
     __syncwarp();
   }
