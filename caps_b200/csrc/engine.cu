@@ -474,7 +474,7 @@ void Engine::ensure_list_capacity() {
     d_ent_.alloc(ecap);
     d_ent_shift_.alloc(ecap);
     d_work_.alloc(ecap / 4 + size_t(nsc_cap_) * 2 + 64);
-    d_masks_.alloc(size_t(8) * 64 * nsc_cap_ + 8 * 256);
+    d_masks_.alloc(size_t(8) * 96 * nsc_cap_ + 8 * 256);   // 8 rows per (j cluster, image) with exclusions, per super-cluster
   }
   d_col_.alloc(size_t(n_));
   d_frac_.alloc(size_t(3) * n_);

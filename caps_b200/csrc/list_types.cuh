@@ -46,7 +46,7 @@ struct ListBufs {
   // (the cluster's lower-x half) come within the prune radius of i cluster c, bit 8 + c for j atoms 4-7
   uint4* ent;
   float4* ent_shift;  // org(sc_j) + S - org(sc_i), for the FP32 kernel
-  unsigned long long* masks;   // 8 per masked entry
+  unsigned long long* masks;   // 8 rows (i clusters) per (super-cluster, j cluster, image) with exclusions
   int4* work;         // x sc, y first entry, z count
   // capacities
   int nsc_cap, ent_cap, mask_cap, work_cap;

@@ -129,7 +129,8 @@ static __global__ void k_scatter(int n, ListBufs b) {
   b.order[b.col_start[c] + base + __popc(same & ((1u << lane) - 1))] = i;
 }
 
-// K-SORT (block per column): atoms by fractional c, ties by index (a rank sort in shared memory).
+// K-SORT (block per column): atoms by fractional c, ties by index. A bitonic sorting network in shared memory over the
+// column padded to a power of two (pad keys sort last): log2(n)(log2(n)+1)/2 compare-exchange rounds, one barrier each.
 static __global__ void k_sort_columns(ListGeom g, ListBufs b) {
   if (build_off(b.counters)) return;
   extern __shared__ unsigned char smem_raw[];
@@ -137,36 +138,46 @@ static __global__ void k_sort_columns(ListGeom g, ListBufs b) {
   int* id = reinterpret_cast<int*>(key + kSortMax);
   for (int c = blockIdx.x; c < g.ncol; c += gridDim.x) {
     const int s0 = b.col_start[c], n = min(b.col_start[c + 1] - s0, kSortMax);
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-      const int a = b.order[s0 + k];
-      id[k] = a;
-      key[k] = b.frac[3 * a + 2];
+    int np = 1;
+    while (np < n) np <<= 1;
+    for (int k = threadIdx.x; k < np; k += blockDim.x) {
+      if (k < n) {
+        const int a = b.order[s0 + k];
+        id[k] = a;
+        key[k] = b.frac[3 * a + 2];
+      } else {
+        id[k] = 0x7fffffff;
+        key[k] = 2.0;   // fractional coordinates are below 1
+      }
     }
     __syncthreads();
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-      const double kk = key[k];
-      const int ik = id[k];
-      int r0 = 0, r1 = 0, r2 = 0, r3 = 0;   // four independent counts: the loop is latency-bound otherwise
-      int u = 0;
-      for (; u + 4 <= n; u += 4) {
-        r0 += (key[u] < kk) || (key[u] == kk && id[u] < ik);
-        r1 += (key[u + 1] < kk) || (key[u + 1] == kk && id[u + 1] < ik);
-        r2 += (key[u + 2] < kk) || (key[u + 2] == kk && id[u + 2] < ik);
-        r3 += (key[u + 3] < kk) || (key[u + 3] == kk && id[u + 3] < ik);
+    for (int kk = 2; kk <= np; kk <<= 1)
+      for (int j = kk >> 1; j > 0; j >>= 1) {
+        for (int t = threadIdx.x; t < (np >> 1); t += blockDim.x) {
+          const int lo = 2 * j * (t / j) + (t & (j - 1)), hi = lo + j;
+          const double ka = key[lo], kb = key[hi];
+          const int ia = id[lo], ib = id[hi];
+          const bool gt = ka > kb || (ka == kb && ia > ib);
+          if (gt == ((lo & kk) == 0)) {
+            key[lo] = kb, key[hi] = ka;
+            id[lo] = ib, id[hi] = ia;
+          }
+        }
+        __syncthreads();
       }
-      for (; u < n; ++u) r0 += (key[u] < kk) || (key[u] == kk && id[u] < ik);
-      b.order[s0 + r0 + r1 + r2 + r3] = ik;
-    }
+    for (int k = threadIdx.x; k < n; k += blockDim.x) b.order[s0 + k] = id[k];
     __syncthreads();
   }
 }
 
 // K-SUPER (warp per super-cluster): the 2 x 2 x 2 split into clusters, perm / iperm, cluster boxes and real-atom
-// masks, the super-cluster's origin and its c range.
+// masks, the super-cluster's origin and its c range. Lane l holds atoms l (lower c half) and l + 32 (upper c half):
+// the ranks along y and x come from shuffles, the boxes from butterfly reductions over the 8 lanes of a cluster.
 static __global__ void k_superclusters(DevCell cell, ListBufs b) {
   if (build_off(b.counters)) return;
-  __shared__ double s_y[4][64], s_x[4][64], s_w[4][64][3];
-  __shared__ int s_id[4][64], s_slot[4][64], s_ry[4][64];
+  __shared__ double s_w[4][64][3];   // world position by local slot
+  __shared__ int s_a[4][64];         // atom by local slot, -1 padding
+  const unsigned full = 0xffffffffu;
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nsc = min(b.counters[kCntNsc], b.nsc_cap);
   for (int sc = blockIdx.x * 4 + wib; sc < nsc; sc += gridDim.x * 4) {
@@ -174,85 +185,115 @@ static __global__ void k_superclusters(DevCell cell, ListBufs b) {
     const int k = sc - b.col_sc[c];
     const int s0 = b.col_start[c] + kScAtoms * k;
     const int m = min(kScAtoms, b.col_start[c + 1] - s0);
-    for (int t = lane; t < 64; t += 32) {
-      b.perm[64 * sc + t] = -1;
+    if (m <= 0) {   // not made by the scan (every super-cluster holds at least one atom); kept empty
+      b.perm[64 * sc + lane] = b.perm[64 * sc + lane + 32] = -1;
+      continue;
+    }
+    int id[2];
+    double fx[2], fy[2], w[2][3];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int t = lane + 32 * h;
+      id[h] = -1;
+      fx[h] = fy[h] = 0;
+      w[h][0] = w[h][1] = w[h][2] = 0;
       if (t < m) {
         const int a = b.order[s0 + t];
-        s_id[wib][t] = a;
+        id[h] = a;
         const double f0 = b.frac[3 * a], f1 = b.frac[3 * a + 1], f2 = b.frac[3 * a + 2];
-        s_x[wib][t] = f0;
-        s_y[wib][t] = f1;
-        for (int r = 0; r < 3; ++r) s_w[wib][t][r] = cell.o[r] + cell.h[r][0] * f0 + cell.h[r][1] * f1 + cell.h[r][2] * f2;
+        fx[h] = f0, fy[h] = f1;
+        for (int r = 0; r < 3; ++r) w[h][r] = cell.o[r] + cell.h[r][0] * f0 + cell.h[r][1] * f1 + cell.h[r][2] * f2;
+      }
+      s_a[wib][t] = -1;
+    }
+    // rank along y within the c half, then along x within the y half of the c half (ties by atom index)
+    int ry[2] = {0, 0}, rx[2] = {0, 0};
+    for (int u = 0; u < 32; ++u) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const double yu = __shfl_sync(full, fy[h], u);
+        const int iu = __shfl_sync(full, id[h], u);
+        ry[h] += (u + 32 * h < m) && (yu < fy[h] || (yu == fy[h] && iu < id[h]));
+      }
+    }
+    for (int u = 0; u < 32; ++u) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const double xu = __shfl_sync(full, fx[h], u);
+        const int iu = __shfl_sync(full, id[h], u);
+        const int qu = __shfl_sync(full, ry[h] >> 4, u);
+        rx[h] += (u + 32 * h < m) && qu == (ry[h] >> 4) && (xu < fx[h] || (xu == fx[h] && iu < id[h]));
       }
     }
     __syncwarp();
-    for (int t = lane; t < m; t += 32) {
-      const int h = t >> 5;                // z half (positions are sorted along c)
-      const int hb = h * 32, he = min(m, hb + 32);
-      int ry = 0;
-      for (int u = hb; u < he; ++u) ry += (s_y[wib][u] < s_y[wib][t]) || (s_y[wib][u] == s_y[wib][t] && s_id[wib][u] < s_id[wib][t]);
-      s_ry[wib][t] = ry;   // the rank along y within the z half
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (lane + 32 * h >= m) continue;
+      const int slot = 8 * (4 * h + 2 * (ry[h] >> 4) + (rx[h] >> 3)) + (rx[h] & 7);
+      s_a[wib][slot] = id[h];
+      for (int r = 0; r < 3; ++r) s_w[wib][slot][r] = w[h][r];
+      b.iperm[id[h]] = 64 * sc + slot;
     }
     __syncwarp();
-    for (int t = lane; t < m; t += 32) {
-      const int h = t >> 5, hb = h * 32, he = min(m, hb + 32);
-      const int q = s_ry[wib][t] >> 4;   // y half within the z half
-      int rx = 0;
-      for (int u = hb; u < he; ++u) {
-        if ((s_ry[wib][u] >> 4) != q) continue;
-        rx += (s_x[wib][u] < s_x[wib][t]) || (s_x[wib][u] == s_x[wib][t] && s_id[wib][u] < s_id[wib][t]);
+    // cluster boxes and real masks: slot lane + 32 h belongs to cluster (lane >> 3) + 4 h
+    double slo[3] = {1e300, 1e300, 1e300}, shi[3] = {-1e300, -1e300, -1e300};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int t = lane + 32 * h;
+      const int a = s_a[wib][t];
+      b.perm[64 * sc + t] = a;
+      double lo[3], hi[3];
+      for (int r = 0; r < 3; ++r) {
+        lo[r] = a >= 0 ? s_w[wib][t][r] : 1e300;
+        hi[r] = a >= 0 ? s_w[wib][t][r] : -1e300;
       }
-      const int cl = 4 * h + 2 * q + (rx >> 3);
-      s_slot[wib][t] = 64 * sc + 8 * cl + (rx & 7);
-    }
-    __syncwarp();
-    for (int t = lane; t < m; t += 32) {
-      const int slot = s_slot[wib][t], a = s_id[wib][t];
-      b.perm[slot] = a;
-      b.iperm[a] = slot;
-    }
-    __syncwarp();
-    // cluster boxes: lane l < 8 takes cluster l
-    if (lane < 8) {
-      double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-      unsigned real = 0;
-      for (int t = 0; t < m; ++t) {
-        const int slot = s_slot[wib][t] - 64 * sc;
-        if ((slot >> 3) != lane) continue;
-        real |= 1u << (slot & 7);
-        for (int r = 0; r < 3; ++r) lo[r] = fmin(lo[r], s_w[wib][t][r]), hi[r] = fmax(hi[r], s_w[wib][t][r]);
+#pragma unroll
+      for (int o = 1; o < 8; o <<= 1)
+        for (int r = 0; r < 3; ++r) {
+          lo[r] = fmin(lo[r], __shfl_xor_sync(full, lo[r], o));
+          hi[r] = fmax(hi[r], __shfl_xor_sync(full, hi[r], o));
+        }
+      const unsigned real = __ballot_sync(full, a >= 0);
+      if ((lane & 7) == 0) {
+        const int cg = 8 * sc + (lane >> 3) + 4 * h;
+        for (int r = 0; r < 3; ++r) b.cl_box[6 * cg + r] = lo[r], b.cl_box[6 * cg + 3 + r] = hi[r];
+        b.cl_real[cg] = (unsigned char)((real >> (lane & 24)) & 255u);
       }
-      const int cg = 8 * sc + lane;
-      for (int r = 0; r < 3; ++r) b.cl_box[6 * cg + r] = lo[r], b.cl_box[6 * cg + 3 + r] = hi[r];
-      b.cl_real[cg] = (unsigned char)real;
+      for (int r = 0; r < 3; ++r) slo[r] = fmin(slo[r], lo[r]), shi[r] = fmax(shi[r], hi[r]);
     }
+#pragma unroll
+    for (int o = 8; o < 32; o <<= 1)
+      for (int r = 0; r < 3; ++r) {
+        slo[r] = fmin(slo[r], __shfl_xor_sync(full, slo[r], o));
+        shi[r] = fmax(shi[r], __shfl_xor_sync(full, shi[r], o));
+      }
+    const int last = m - 1;
+    const int id_first = __shfl_sync(full, id[0], 0);
+    const int id_last = __shfl_sync(full, (last >> 5) ? id[1] : id[0], last & 31);
     if (lane == 0) {
-      double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-      for (int t = 0; t < m; ++t)
-        for (int r = 0; r < 3; ++r) lo[r] = fmin(lo[r], s_w[wib][t][r]), hi[r] = fmax(hi[r], s_w[wib][t][r]);
-      for (int r = 0; r < 3; ++r) b.sc_org[3 * sc + r] = 0.5 * (lo[r] + hi[r]);
-      b.sc_z[2 * sc] = b.frac[3 * s_id[wib][0] + 2];
-      b.sc_z[2 * sc + 1] = b.frac[3 * s_id[wib][m - 1] + 2];
+      for (int r = 0; r < 3; ++r) b.sc_org[3 * sc + r] = 0.5 * (slo[r] + shi[r]);
+      b.sc_z[2 * sc] = b.frac[3 * id_first + 2];
+      b.sc_z[2 * sc + 1] = b.frac[3 * id_last + 2];
     }
     __syncwarp();
   }
 }
 
 // ---------------------------------------------------------------------------------------------------------------
-constexpr int kSearchWarps = 4;       // warps per super-cluster in the search
+constexpr int kSearchWarps = 8;       // warps per super-cluster in the search
 
 // One warp's batch of entries in the making.
 struct SearchBatch {
   uint4 ent[2 * kBatch];
   float4 sh[2 * kBatch];
-  unsigned char needs_mask[2 * kBatch];
-  unsigned long long m[kBatch][8];
   int nent;
 };
 
 struct SearchShared {
   uint2 rec[kExclRecMax];                 // x: j cluster, y: i local (6 bits) | j in cluster (3) << 6 | image << 9
   unsigned long long key[kExclHash];      // distinct (j cluster, image) of the records; ~0 empty
+  unsigned short krank[kExclHash];        // rank of each occupied key slot: its masks are number mbase + rank
+  int mbase;
   double ibox[8][6];
   double org_i[3];
   int nrec;
@@ -261,59 +302,38 @@ struct SearchShared {
 
 __device__ __forceinline__ unsigned long long excl_key(unsigned cj, unsigned img) { return (unsigned long long)cj | ((unsigned long long)img << 32); }
 
-static __device__ bool key_find(const SearchShared& S, unsigned long long key) {
+// The slot of a key in the open-addressing table, or -1.
+static __device__ int key_slot(const SearchShared& S, unsigned long long key) {
   unsigned h = (unsigned)(key * 0x9E3779B97F4A7C15ull >> 56) & (kExclHash - 1);
   for (int p = 0; p < kExclHash; ++p) {
     const unsigned long long v = S.key[h];
-    if (v == key) return true;
-    if (v == ~0ull) return false;
+    if (v == key) return int(h);
+    if (v == ~0ull) return -1;
     h = (h + 1) & (kExclHash - 1);
   }
-  return false;
+  return -1;
 }
 
-static __device__ void key_insert(SearchShared& S, unsigned long long key, int* counters) {
+static __device__ int key_insert(SearchShared& S, unsigned long long key, int* counters) {
   unsigned h = (unsigned)(key * 0x9E3779B97F4A7C15ull >> 56) & (kExclHash - 1);
   for (int p = 0; p < kExclHash; ++p) {
     const unsigned long long old = atomicCAS(&S.key[h], ~0ull, key);
-    if (old == ~0ull || old == key) return;
+    if (old == ~0ull || old == key) return int(h);
     h = (h + 1) & (kExclHash - 1);
   }
   raise_error(counters, kErrExclOverflow);
+  return -1;
 }
-
-// Writes the batch [0, cnt) of B as one work item (the masks of entries that need them first).
-static __device__ void flush_batch(const SearchShared& S, SearchBatch& B, int sc, int cnt, int lane, const ListBufs& b) {
+// Writes the batch [0, cnt) of B as one work item. One atomic reserves the entries and the work item: the entry and work
+// counters are the two halves of one 64-bit word (entries low, work items high), shared by every warp of the build.
+static __device__ void flush_batch(SearchBatch& B, int sc, int cnt, int lane, const ListBufs& b) {
   if (cnt <= 0) return;
-  // masks for the entries that need them: start from all pairs, drop exclusions and the lower triangle of a cluster
-  // with itself under the zero image
-  for (int e = 0; e < cnt; ++e) {
-    if (!B.needs_mask[e]) continue;
-    const unsigned cj = B.ent[e].x;
-    const unsigned img = (B.ent[e].y >> 8) & 0x1FFFFFu;
-    if (lane < 8) {
-      unsigned long long mm = ~0ull;
-      if (cj == unsigned(8 * sc + lane) && img == pack_image(0, 0, 0)) {
-        // a cluster with itself: each pair once (j > i): bit 8 i + j
-        mm = 0;
-        for (int i = 0; i < 8; ++i)
-          for (int j = i + 1; j < 8; ++j) mm |= 1ull << (8 * i + j);
-      }
-      B.m[e][lane] = mm;
-    }
-    __syncwarp();
-    for (int r = lane; r < S.nrec; r += 32) {
-      const uint2 rc = S.rec[r];
-      if (rc.x != cj || (rc.y >> 9) != img) continue;
-      const unsigned il = rc.y & 63u, jl = (rc.y >> 6) & 7u;
-      atomicAnd(&B.m[e][il >> 3], ~(1ull << (8 * (il & 7) + jl)));
-    }
-    __syncwarp();
-  }
+  static_assert(kCntEnt == 0 && kCntWork == 1, "entry and work counters form one 64-bit word");
   int base = 0, wi = 0;
   if (lane == 0) {
-    base = atomicAdd(b.counters + kCntEnt, cnt);
-    wi = atomicAdd(b.counters + kCntWork, 1);
+    const unsigned long long old = atomicAdd(reinterpret_cast<unsigned long long*>(b.counters + kCntEnt), (1ull << 32) | unsigned(cnt));
+    base = int(unsigned(old & 0xffffffffull));
+    wi = int(unsigned(old >> 32));
   }
   base = __shfl_sync(0xffffffffu, base, 0);
   wi = __shfl_sync(0xffffffffu, wi, 0);
@@ -324,27 +344,20 @@ static __device__ void flush_batch(const SearchShared& S, SearchBatch& B, int sc
   for (int e = lane; e < cnt; e += 32) {
     uint4 en = B.ent[e];
     en.w = (en.y & 255u) * 0x101u;   // unpruned until the first prune: both halves of every listed i cluster
-    if (B.needs_mask[e]) {
-      const int mi = atomicAdd(b.counters + kCntMask, 1);
-      if (mi < b.mask_cap) {
-        for (int k = 0; k < 8; ++k) b.masks[8 * size_t(mi) + k] = B.m[e][k];
-        en.z = unsigned(mi + 1);
-      } else {
-        raise_error(b.counters, kErrMaskOverflow);
-      }
-    }
     b.ent[base + e] = en;
     b.ent_shift[base + e] = B.sh[e];
   }
   if (lane == 0) b.work[wi] = make_int4(sc, base, cnt, 0);
 }
 
-// K-SEARCH: one block of kSearchWarps warps per super-cluster. The block records the super-cluster's excluded pairs;
-// then each warp takes a quarter of the neighbouring columns (with their images) and batches its own entries.
-// Exclusions (ForceField::excluded) hold at their nearest image only (core/src/nbnxm.cpp:229-252): each of the
-// super-cluster's excluded atom pairs is recorded with the image that is nearest at the build, and an entry for that j
-// cluster under that image carries masks with those pairs cleared.
-static __global__ void __launch_bounds__(32 * kSearchWarps) k_search(DevCell cell, ListGeom g, const uint32_t* __restrict__ excl_off,
+// K-SEARCH: one block of kSearchWarps warps per super-cluster. The block records the super-cluster's excluded pairs and
+// builds the atom masks of every (j cluster, image) they touch; then each warp takes a contiguous share of the
+// neighbouring columns (with their images) and batches its own entries. Exclusions (ForceField::excluded) hold at their
+// nearest image only (core/src/nbnxm.cpp:229-252): each of the super-cluster's excluded atom pairs is recorded with the
+// image that is nearest at the build, and the entry for that j cluster under that image carries masks with those pairs
+// cleared. The super-cluster's own clusters under the zero image always carry masks (each pair of a cluster with
+// itself once).
+static __global__ void __launch_bounds__(32 * kSearchWarps, 4) k_search(DevCell cell, ListGeom g, const uint32_t* __restrict__ excl_off,
                                                                      const uint32_t* __restrict__ excl_list, ListBufs b) {
   if (build_off(b.counters)) return;
   extern __shared__ unsigned char smem_raw[];
@@ -361,11 +374,14 @@ static __global__ void __launch_bounds__(32 * kSearchWarps) k_search(DevCell cel
     if (threadIdx.x == 0) S.nrec = 0;
     if (lane == 0) B.nent = 0;
     __syncthreads();
-    for (int t = threadIdx.x; t < 64; t += blockDim.x) {
+    if (threadIdx.x < 8) key_insert(S, excl_key(unsigned(8 * sc + threadIdx.x), pack_image(0, 0, 0)), b.counters);
+    // kSearchWarps / 2 threads per atom, each taking every (kSearchWarps / 2)-th of the atom's excluded partners
+    for (int u = threadIdx.x; u < 64 * (kSearchWarps / 2); u += blockDim.x) {
+      const int t = u & 63;
       const int a = b.perm[64 * sc + t];
       if (a < 0) continue;
       const double* fa = b.frac + 3 * a;
-      for (uint32_t p = excl_off[a]; p < excl_off[a + 1]; ++p) {
+      for (uint32_t p = excl_off[a] + uint32_t(u >> 6); p < excl_off[a + 1]; p += kSearchWarps / 2) {
         const int bb = int(excl_list[p]);
         const int sb = b.iperm[bb];
         const double* fb = b.frac + 3 * bb;
@@ -381,10 +397,64 @@ static __global__ void __launch_bounds__(32 * kSearchWarps) k_search(DevCell cel
     }
     __syncthreads();
     if (threadIdx.x == 0 && S.nrec > kExclRecMax) S.nrec = kExclRecMax;
+    // masks: one set of 8 rows (i cluster r against the key's j cluster) per occupied key slot, numbered by the slot's
+    // rank from a base reserved with one atomic; rows start as all pairs (each pair once for a cluster with itself under
+    // the zero image), then every record clears its pair
+    if (warp == 0) {
+      constexpr int per = kExclHash / 32;
+      unsigned occ = 0;
+#pragma unroll
+      for (int q = 0; q < per; ++q) occ |= unsigned(S.key[lane * per + q] != ~0ull) << q;
+      const unsigned tot = __popc(occ);
+      unsigned run = tot;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, run, o);
+        if (lane >= o) run += y;
+      }
+      unsigned start = run - tot;
+#pragma unroll
+      for (int q = 0; q < per; ++q) {
+        S.krank[lane * per + q] = (unsigned short)start;
+        start += (occ >> q) & 1u;
+      }
+      const unsigned nkeys = __shfl_sync(0xffffffffu, run, 31);
+      if (lane == 0) {
+        const int m0 = atomicAdd(b.counters + kCntMask, int(nkeys));
+        if (m0 + int(nkeys) > b.mask_cap) raise_error(b.counters, kErrMaskOverflow);
+        S.mbase = m0;
+      }
+    }
     __syncthreads();
+    for (int t = threadIdx.x; t < 8 * kExclHash; t += blockDim.x) {
+      const int h = t >> 3, r = t & 7;
+      const unsigned long long key = S.key[h];
+      if (key == ~0ull) continue;
+      const int mi = S.mbase + S.krank[h];
+      if (mi >= b.mask_cap) continue;
+      unsigned long long mm = ~0ull;
+      if (key == excl_key(unsigned(8 * sc + r), pack_image(0, 0, 0))) {
+        mm = 0;
+        for (int i = 0; i < 8; ++i)
+          for (int j = i + 1; j < 8; ++j) mm |= 1ull << (8 * i + j);
+      }
+      b.masks[8 * size_t(mi) + r] = mm;
+    }
+    __syncthreads();   // the rows are written before any record clears a bit of them
+    for (int r = threadIdx.x; r < S.nrec; r += blockDim.x) {
+      const uint2 rc = S.rec[r];
+      const int h = key_slot(S, excl_key(rc.x, rc.y >> 9));
+      if (h < 0) continue;
+      const int mi = S.mbase + S.krank[h];
+      if (mi >= b.mask_cap) continue;
+      const unsigned il = rc.y & 63u, jl = (rc.y >> 6) & 7u;
+      atomicAnd(b.masks + 8 * size_t(mi) + (il >> 3), ~(1ull << (8 * (il & 7) + jl)));
+    }
     // --- candidates: neighbouring columns (with their images), super-clusters in c range, their 8 clusters. Each warp
-    // takes a contiguous block of the columns, so that its entries (and the pair kernel's work items made of them) stay
-    // spatially together.
+    // takes a contiguous block of the columns: its entries (and the pair kernel's work items made of them) stay spatially
+    // together, which measured faster in the pair kernel than an interleaved split. The split is fixed, so every build
+    // groups the same entries into the same work items (the pair kernel's float partial sums, and so the forces, do not
+    // depend on timing).
     const int col = b.sc_col[sc];
     const int cu = col / g.nv, cv = col % g.nv;
     const double zlo = b.sc_z[2 * sc], zhi = b.sc_z[2 * sc + 1];
@@ -452,32 +522,32 @@ static __global__ void __launch_bounds__(32 * kSearchWarps) k_search(DevCell cel
           if (have) {
             const int pos = B.nent + __popc(ball & ((1u << lane) - 1));   // < batch + 32 <= 2 kBatch (flushed below)
             const int sjc = cj >> 3;
-            B.ent[pos] = make_uint4(unsigned(cj), imask | (img << 8), 0u, 0u);
+            const int h = key_slot(S, excl_key(unsigned(cj), img));
+            const int mi = h >= 0 ? S.mbase + S.krank[h] : -1;
+            B.ent[pos] = make_uint4(unsigned(cj), imask | (img << 8), mi >= 0 && mi < b.mask_cap ? unsigned(mi + 1) : 0u, 0u);
             B.sh[pos] = make_float4(float(b.sc_org[3 * sjc] + S0 - S.org_i[0]), float(b.sc_org[3 * sjc + 1] + S1 - S.org_i[1]),
                                     float(b.sc_org[3 * sjc + 2] + S2 - S.org_i[2]), 0.f);
-            B.needs_mask[pos] = (unsigned char)((zero && sjc == sc) || key_find(S, excl_key(unsigned(cj), img)));
           }
           __syncwarp();
           if (lane == 0) B.nent += __popc(ball);
           __syncwarp();
           while (B.nent >= g.batch) {   // a pass adds up to 32 entries: with a depth below 32 more than one batch fills
-            flush_batch(S, B, sc, g.batch, lane, b);
+            flush_batch(B, sc, g.batch, lane, b);
             __syncwarp();
             // the rest (< 2 kBatch - batch entries) moves down: read all, then write (the ranges can overlap)
             const int rest = B.nent - g.batch;
             uint4 te[2];
             float4 ts[2];
-            unsigned char tm[2];
 #pragma unroll
             for (int k = 0; k < 2; ++k) {
               const int e = lane + 32 * k;
-              if (e < rest) te[k] = B.ent[g.batch + e], ts[k] = B.sh[g.batch + e], tm[k] = B.needs_mask[g.batch + e];
+              if (e < rest) te[k] = B.ent[g.batch + e], ts[k] = B.sh[g.batch + e];
             }
             __syncwarp();
 #pragma unroll
             for (int k = 0; k < 2; ++k) {
               const int e = lane + 32 * k;
-              if (e < rest) B.ent[e] = te[k], B.sh[e] = ts[k], B.needs_mask[e] = tm[k];
+              if (e < rest) B.ent[e] = te[k], B.sh[e] = ts[k];
             }
             __syncwarp();
             if (lane == 0) B.nent = rest;
@@ -486,7 +556,7 @@ static __global__ void __launch_bounds__(32 * kSearchWarps) k_search(DevCell cel
         }
       }
     }
-    flush_batch(S, B, sc, B.nent, lane, b);
+    flush_batch(B, sc, B.nent, lane, b);
     __syncthreads();   // S is rewritten for the next super-cluster
   }
 }

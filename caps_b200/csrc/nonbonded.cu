@@ -114,6 +114,7 @@ void Engine::launch_build(const double* d_x) {
   const size_t sort_smem = size_t(kSortMax) * (sizeof(double) + sizeof(int));
   k_sort_columns<<<std::min(g.ncol, dev_sms_ * 8), 1024, sort_smem, stream_>>>(g, lb_);
   k_superclusters<<<std::max(1, std::min(blocks_for(size_t(nsc_cap_), 4), dev_sms_ * 16)), 128, 0, stream_>>>(dcell_, lb_);
+  if (sizeof(SearchShared) > 48 * 1024) CK(cudaFuncSetAttribute(k_search, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(SearchShared))));
   k_search<<<std::max(1, std::min(nsc_cap_, dev_sms_ * 8)), 32 * kSearchWarps, sizeof(SearchShared), stream_>>>(dcell_, g, d_excl_off_.p,
                                                                                                           d_excl_list_.p, lb_);
   CK(cudaGetLastError());
