@@ -135,7 +135,9 @@ class Engine {
   // One force evaluation up to the AoS doubles d_out (d_f_ by default), async. parts: a mask of 1 bonded, 2 short-range
   // non-bonded, 4 long-range (PME) terms (-1: the options' parts); clear_energies = false adds this evaluation's
   // energies and virial to the previous one's.
-  void forces(const double* d_x, bool ener, bool vir, bool check_rebuild, int parts = -1, double* d_out = nullptr, bool clear_energies = true);
+  // reduce = false leaves the forces in the fixed-point (or FP64) sums, for a kick that reads them itself
+  void forces(const double* d_x, bool ener, bool vir, bool check_rebuild, int parts = -1, double* d_out = nullptr, bool clear_energies = true,
+              bool reduce = true);
   // Concurrent branches of a force evaluation: `launch` runs with stream_ pointing at side stream k, after everything
   // queued on the main stream so far; join(k) makes the main stream wait for it. Captured, these are graph branches.
   void fork(int k, const std::function<void()>& launch);

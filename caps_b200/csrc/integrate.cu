@@ -354,11 +354,44 @@ struct VelOp {
   uint64_t seed;
   const double* f2;
   double hk2;
+  // kick from the force evaluation's own sums instead of f (when fq or fd is set): atom-order sums plus the pair
+  // kernel's slot-order sums at iperm (the reduction Engine::forces otherwise runs as a kernel of its own); the total is
+  // stored to fout for the next step's first kick
+  const long long* fq;       // FP32 path: fixed point, 3 x nat then 3 x nslots
+  const long long* fsq;
+  const double* fd;          // FP64 path
+  const double* fsd;
+  const int* iperm;
+  int nat, nslots;
+  double* fout;
 };
+// The force on atom g for a kick: f, or the evaluation's sums (stored to fout).
+__device__ __forceinline__ void kick_force(const VelOp& op, int g, double f[3]) {
+  if (!op.fq && !op.fd) {
+    for (int r = 0; r < 3; ++r) f[r] = op.f[3 * g + r];
+    return;
+  }
+  const int s = op.iperm ? op.iperm[g] : -1;
+  const bool ok = s >= 0 && s < op.nslots;   // as the reduction: a build that overflowed can leave iperm stale (reported)
+  for (int r = 0; r < 3; ++r) {
+    if (op.fq) {
+      long long q = op.fq[size_t(r) * op.nat + g];
+      if (ok) q += op.fsq[size_t(r) * op.nslots + s];
+      f[r] = double(q) * kInvFixF;
+    } else {
+      double q = op.fd[size_t(r) * op.nat + g];
+      if (ok) q += op.fsd[size_t(r) * op.nslots + s];
+      f[r] = q;
+    }
+    op.fout[3 * g + r] = f[r];
+  }
+}
 __device__ __forceinline__ void vel_op(const VelOp& op, int g, double* vv, const double* __restrict__ invm, const double* sc) {
   if (op.kind == 1) {
     const double a = op.hk * kAcc * invm[g];
-    for (int r = 0; r < 3; ++r) vv[r] += a * op.f[3 * g + r];
+    double f[3];
+    kick_force(op, g, f);
+    for (int r = 0; r < 3; ++r) vv[r] += a * f[r];
     if (op.f2) {
       const double a2 = op.hk2 * kAcc * invm[g];
       for (int r = 0; r < 3; ++r) vv[r] += a2 * op.f2[3 * g + r];
@@ -497,12 +530,155 @@ __device__ void rattle_water(const ConsArgs& C, int wi, const double* __restrict
     }
 }
 
+__global__ void k_scale_v(int n, double* __restrict__ v, const double* __restrict__ sc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 3 * n) return;
+  v[i] *= sc[kScFactor];
+}
+
+// The step counter and the thermostat target: T ramps linearly from t0 to t1 over `steps` when t1 >= 0.
+__device__ void step_begin_body(double* sc, double t0, double t1, long long steps, double ndof) {
+  const double step = sc[kScStep] + 1;
+  sc[kScStep] = step;
+  const double t = (t1 >= 0 && steps > 0) ? t0 + (t1 - t0) * step / double(steps) : t0;
+  sc[kScTnow] = t;
+  sc[kScKtarget] = 0.5 * ndof * kB * t;
+}
+__global__ void k_step_begin(double* sc, double t0, double t1, long long steps, double ndof) { step_begin_body(sc, t0, t1, steps, ndof); }
+
+// Nose-Hoover chain over half a step (LAMMPS FixNH::nhc_temp_integrate, as dynamics.cpp:479-508): sets the velocity
+// factor in sc[kScFactor]; the caller scales v by it.
+__device__ void nhc_body(Chain* ch, double* sc, double ndof, double t_freq, double dt) {
+  const double dthalf = 0.5 * dt, dt4 = 0.25 * dt, dt8 = 0.125 * dt;
+  const double tt = sc[kScTnow], kt = kB * tt, ke_target = ndof * kt;
+  Chain& c = *ch;
+  c.eta_mass[0] = ndof * kt / (t_freq * t_freq);
+  for (int q = 1; q < 3; ++q) c.eta_mass[q] = kt / (t_freq * t_freq);
+  double kecur = 2 * sc[kScKE];
+  c.eta_dotdot[0] = (kecur - ke_target) / c.eta_mass[0];
+  for (int q = 2; q > 0; --q) {
+    const double ex = exp(-dt8 * c.eta_dot[q + 1]);
+    c.eta_dot[q] = (c.eta_dot[q] * ex + c.eta_dotdot[q] * dt4) * ex;
+  }
+  double ex = exp(-dt8 * c.eta_dot[1]);
+  c.eta_dot[0] = (c.eta_dot[0] * ex + c.eta_dotdot[0] * dt4) * ex;
+  const double factor = exp(-dthalf * c.eta_dot[0]);
+  kecur *= factor * factor;
+  c.eta_dotdot[0] = (kecur - ke_target) / c.eta_mass[0];
+  for (int q = 0; q < 3; ++q) c.eta[q] += dthalf * c.eta_dot[q];
+  c.eta_dot[0] = (c.eta_dot[0] * ex + c.eta_dotdot[0] * dt4) * ex;
+  for (int q = 1; q < 3; ++q) {
+    ex = exp(-dt8 * c.eta_dot[q + 1]);
+    c.eta_dot[q] *= ex;
+    c.eta_dotdot[q] = (c.eta_mass[q - 1] * c.eta_dot[q - 1] * c.eta_dot[q - 1] - kt) / c.eta_mass[q];
+    c.eta_dot[q] = (c.eta_dot[q] + c.eta_dotdot[q] * dt4) * ex;
+  }
+  sc[kScFactor] = factor;
+  sc[kScKE] = 0.5 * kecur;
+}
+
+// Bussi velocity rescaling (Bussi, Donadio & Parrinello 2007, appendix; dynamics.cpp:466-477) from this step's draws
+// (r1, sum of ndof - 1 squared normals) read from the host-made table.
+__device__ void bussi_body(double* sc, const double2* __restrict__ draws, long long first_step, double h, double tau, double ndof) {
+  const double k = sc[kScKE];
+  const long long step = (long long)sc[kScStep];
+  if (k <= 0) {
+    sc[kScFactor] = 1;
+    return;
+  }
+  const double2 d = draws[step - first_step];
+  const double c = exp(-h / tau), kt = sc[kScKtarget];
+  const double r1 = d.x, sum = d.y;
+  const double knew = k + (1 - c) * (kt * (r1 * r1 + sum) / ndof - k) + 2 * r1 * sqrt(c * (1 - c) * kt * k / ndof);
+  sc[kScFactor] = sqrt(fmax(knew, 0.0) / k);
+  sc[kScBath] -= knew - k;
+}
+
+// What the last block of k_ke does with the fresh kinetic energy.
+enum KeThen { kThenNone = 0, kThenNhc, kThenBussi, kThenBath };
+struct KeArgs {
+  int n;
+  const double* v;
+  const double* m;
+  double* part;          // 7 per block
+  unsigned* done;        // blocks finished; the last block resets it
+  double* sc;
+  int slot;              // sc slot receiving 0.5 sum m v^2 / kAcc
+  int tensor;            // also the kinetic tensor into kScKin0..
+  int begin;             // run the step-begin update first
+  int then;              // KeThen
+  double t0, t1, ndof;
+  long long steps;
+  Chain* chain;
+  double t_freq, dt;
+  const double2* draws;
+  long long draws_first;
+  double tau;
+};
+
+// One atom's share: m v^2, and the tensor terms on request.
+__device__ __forceinline__ void ke_atom(const KeArgs& A, int i, double& e, double t[6]) {
+  const double vx = A.v[3 * i], vy = A.v[3 * i + 1], vz = A.v[3 * i + 2], mi = A.m[i];
+  e += mi * (vx * vx + vy * vy + vz * vz);
+  if (A.tensor) t[0] += mi * vx * vx, t[1] += mi * vy * vy, t[2] += mi * vz * vz, t[3] += mi * vx * vy, t[4] += mi * vx * vz, t[5] += mi * vy * vz;
+}
+
+// The block sums of every thread's share into A.part (7 per block), then in the last block to finish: the partials in
+// block order and the scalar update. Every thread of every block calls it.
+__device__ void ke_blocks(const KeArgs& A, double e, double t[6]) {
+  __shared__ double scratch[32];
+  __shared__ bool last;
+  const double s = block_sum(e, scratch);
+  if (threadIdx.x == 0) A.part[blockIdx.x * 7] = s;
+  if (A.tensor)
+    for (int q = 0; q < 6; ++q) {
+      const double st = block_sum(t[q], scratch);
+      if (threadIdx.x == 0) A.part[blockIdx.x * 7 + 1 + q] = st;
+    }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(A.done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  e = 0;
+  for (int q = 0; q < 6; ++q) t[q] = 0;
+  for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+    e += __ldcg(A.part + 7 * b);
+    if (A.tensor)
+      for (int q = 0; q < 6; ++q) t[q] += __ldcg(A.part + 7 * b + 1 + q);
+  }
+  const double tot = block_sum(e, scratch);
+  double tt[6];
+  if (A.tensor)
+    for (int q = 0; q < 6; ++q) tt[q] = block_sum(t[q], scratch);
+  if (threadIdx.x != 0) return;
+  *A.done = 0;
+  double* sc = A.sc;
+  sc[A.slot] = 0.5 * tot / kAcc;
+  if (A.tensor)
+    for (int q = 0; q < 6; ++q) sc[kScKin0 + q] = tt[q] / kAcc;
+  if (A.begin) step_begin_body(sc, A.t0, A.t1, A.steps, A.ndof);
+  if (A.then == kThenNhc) nhc_body(A.chain, sc, A.ndof, A.t_freq, A.dt);
+  else if (A.then == kThenBussi) bussi_body(sc, A.draws, A.draws_first, A.dt, A.tau, A.ndof);
+  else if (A.then == kThenBath) sc[kScBath] -= sc[kScKE] - sc[kScKE0];
+}
+
+// The first Nose-Hoover half step of a step, on the kinetic energy the previous step left in sc[kScKE]: its second half
+// set it to the scaled velocities' value, and the velocities have not changed since.
+__global__ void k_nhc_begin(Chain* ch, double* sc, double t0, double t1, long long steps, double ndof, double t_freq, double dt) {
+  step_begin_body(sc, t0, t1, steps, ndof);
+  nhc_body(ch, sc, ndof, t_freq, dt);
+}
+
 // Velocity update then RATTLE in one launch: threads [0, ncl) take one constraint cluster each (its atoms' update, then
 // the relative velocity along each constraint removed, core/src/constraints.cpp:232-269; star clusters in registers);
 // threads [ncl, ncl + nfree) update one unconstrained atom each. With h > 0 the impulses are read as forces over a half kick and their virial
-// (xx yy zz xy xz yz) is added to sc[kScCW0..].
+// (xx yy zz xy xz yz) is added to sc[kScCW0..]. With K.n > 0 the launch also takes the kinetic energy of the new
+// velocities and runs K's thermostat update in its last block (what k_ke does in a launch of its own).
 __global__ void k_vel_rattle(ConsArgs C, int nfree, const int* __restrict__ free_atoms, const double* __restrict__ x, double* __restrict__ v, VelOp op,
-                             double h, double* sc, int* counters) {
+                             double h, double* sc, int* counters, KeArgs K) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   double w[6] = {0, 0, 0, 0, 0, 0};
   if (c >= C.ncl && c < C.ncl + nfree) {
@@ -576,100 +752,29 @@ __global__ void k_vel_rattle(ConsArgs C, int nfree, const int* __restrict__ free
       if (threadIdx.x == 0 && s != 0) atomicAdd(sc + kScCW0 + q, s);
     }
   }
-}
-
-__global__ void k_scale_v(int n, double* __restrict__ v, const double* __restrict__ sc) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= 3 * n) return;
-  v[i] *= sc[kScFactor];
-}
-
-// The step counter and the thermostat target: T ramps linearly from t0 to t1 over `steps` when t1 >= 0.
-__device__ void step_begin_body(double* sc, double t0, double t1, long long steps, double ndof) {
-  const double step = sc[kScStep] + 1;
-  sc[kScStep] = step;
-  const double t = (t1 >= 0 && steps > 0) ? t0 + (t1 - t0) * step / double(steps) : t0;
-  sc[kScTnow] = t;
-  sc[kScKtarget] = 0.5 * ndof * kB * t;
-}
-__global__ void k_step_begin(double* sc, double t0, double t1, long long steps, double ndof) { step_begin_body(sc, t0, t1, steps, ndof); }
-
-// Nose-Hoover chain over half a step (LAMMPS FixNH::nhc_temp_integrate, as dynamics.cpp:479-508): sets the velocity
-// factor in sc[kScFactor]; the caller scales v by it.
-__device__ void nhc_body(Chain* ch, double* sc, double ndof, double t_freq, double dt) {
-  const double dthalf = 0.5 * dt, dt4 = 0.25 * dt, dt8 = 0.125 * dt;
-  const double tt = sc[kScTnow], kt = kB * tt, ke_target = ndof * kt;
-  Chain& c = *ch;
-  c.eta_mass[0] = ndof * kt / (t_freq * t_freq);
-  for (int q = 1; q < 3; ++q) c.eta_mass[q] = kt / (t_freq * t_freq);
-  double kecur = 2 * sc[kScKE];
-  c.eta_dotdot[0] = (kecur - ke_target) / c.eta_mass[0];
-  for (int q = 2; q > 0; --q) {
-    const double ex = exp(-dt8 * c.eta_dot[q + 1]);
-    c.eta_dot[q] = (c.eta_dot[q] * ex + c.eta_dotdot[q] * dt4) * ex;
+  // the kinetic energy of the updated velocities (this thread's atoms, read back) and the thermostat update, as k_ke
+  if (K.n > 0) {
+    double e = 0, t[6] = {0, 0, 0, 0, 0, 0};
+    if (c >= C.ncl && c < C.ncl + nfree) {
+      ke_atom(K, free_atoms[c - C.ncl], e, t);
+    } else if (c < C.e3) {
+      const int4 at = C.star[c];
+      const int ids[4] = {at.x, at.y, at.z, at.w};
+      for (int a = 0; a < 4; ++a)
+        if (ids[a] >= 0) ke_atom(K, ids[a], e, t);
+    } else if (c < C.e4) {
+      const int4 at = C.water[c - C.e3];
+      ke_atom(K, at.x, e, t);
+      ke_atom(K, at.y, e, t);
+      ke_atom(K, at.z, e, t);
+    } else if (c < C.ncl) {
+      const int cg = c - C.e4;
+      for (int a = C.cl_atom0[cg]; a < C.cl_atom0[cg + 1]; ++a) ke_atom(K, C.cl_atoms[a], e, t);
+    }
+    ke_blocks(K, e, t);
   }
-  double ex = exp(-dt8 * c.eta_dot[1]);
-  c.eta_dot[0] = (c.eta_dot[0] * ex + c.eta_dotdot[0] * dt4) * ex;
-  const double factor = exp(-dthalf * c.eta_dot[0]);
-  kecur *= factor * factor;
-  c.eta_dotdot[0] = (kecur - ke_target) / c.eta_mass[0];
-  for (int q = 0; q < 3; ++q) c.eta[q] += dthalf * c.eta_dot[q];
-  c.eta_dot[0] = (c.eta_dot[0] * ex + c.eta_dotdot[0] * dt4) * ex;
-  for (int q = 1; q < 3; ++q) {
-    ex = exp(-dt8 * c.eta_dot[q + 1]);
-    c.eta_dot[q] *= ex;
-    c.eta_dotdot[q] = (c.eta_mass[q - 1] * c.eta_dot[q - 1] * c.eta_dot[q - 1] - kt) / c.eta_mass[q];
-    c.eta_dot[q] = (c.eta_dot[q] + c.eta_dotdot[q] * dt4) * ex;
-  }
-  sc[kScFactor] = factor;
-  sc[kScKE] = 0.5 * kecur;
 }
 
-// Bussi velocity rescaling (Bussi, Donadio & Parrinello 2007, appendix; dynamics.cpp:466-477) from this step's draws
-// (r1, sum of ndof - 1 squared normals) read from the host-made table.
-__device__ void bussi_body(double* sc, const double2* __restrict__ draws, long long first_step, double h, double tau, double ndof) {
-  const double k = sc[kScKE];
-  const long long step = (long long)sc[kScStep];
-  if (k <= 0) {
-    sc[kScFactor] = 1;
-    return;
-  }
-  const double2 d = draws[step - first_step];
-  const double c = exp(-h / tau), kt = sc[kScKtarget];
-  const double r1 = d.x, sum = d.y;
-  const double knew = k + (1 - c) * (kt * (r1 * r1 + sum) / ndof - k) + 2 * r1 * sqrt(c * (1 - c) * kt * k / ndof);
-  sc[kScFactor] = sqrt(fmax(knew, 0.0) / k);
-  sc[kScBath] -= knew - k;
-}
-
-// The first Nose-Hoover half step of a step, on the kinetic energy the previous step left in sc[kScKE]: its second half
-// set it to the scaled velocities' value, and the velocities have not changed since.
-__global__ void k_nhc_begin(Chain* ch, double* sc, double t0, double t1, long long steps, double ndof, double t_freq, double dt) {
-  step_begin_body(sc, t0, t1, steps, ndof);
-  nhc_body(ch, sc, ndof, t_freq, dt);
-}
-
-// What the last block of k_ke does with the fresh kinetic energy.
-enum KeThen { kThenNone = 0, kThenNhc, kThenBussi, kThenBath };
-struct KeArgs {
-  int n;
-  const double* v;
-  const double* m;
-  double* part;          // 7 per block
-  unsigned* done;        // blocks finished; the last block resets it
-  double* sc;
-  int slot;              // sc slot receiving 0.5 sum m v^2 / kAcc
-  int tensor;            // also the kinetic tensor into kScKin0..
-  int begin;             // run the step-begin update first
-  int then;              // KeThen
-  double t0, t1, ndof;
-  long long steps;
-  Chain* chain;
-  double t_freq, dt;
-  const double2* draws;
-  long long draws_first;
-  double tau;
-};
 
 // Kinetic energy (and the kinetic tensor sum m v_a v_b / kAcc on request), then a thermostat update, in one launch:
 // each block writes its partial sums; the last block to finish adds the partials in block order (deterministic) and
@@ -677,48 +782,8 @@ struct KeArgs {
 __global__ void k_ke(KeArgs A) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double e = 0, t[6] = {0, 0, 0, 0, 0, 0};
-  if (i < A.n) {
-    const double vx = A.v[3 * i], vy = A.v[3 * i + 1], vz = A.v[3 * i + 2], mi = A.m[i];
-    e = mi * (vx * vx + vy * vy + vz * vz);
-    if (A.tensor) t[0] = mi * vx * vx, t[1] = mi * vy * vy, t[2] = mi * vz * vz, t[3] = mi * vx * vy, t[4] = mi * vx * vz, t[5] = mi * vy * vz;
-  }
-  __shared__ double scratch[32];
-  __shared__ bool last;
-  const double s = block_sum(e, scratch);
-  if (threadIdx.x == 0) A.part[blockIdx.x * 7] = s;
-  if (A.tensor)
-    for (int q = 0; q < 6; ++q) {
-      const double st = block_sum(t[q], scratch);
-      if (threadIdx.x == 0) A.part[blockIdx.x * 7 + 1 + q] = st;
-    }
-  if (threadIdx.x == 0) {
-    __threadfence();
-    last = atomicAdd(A.done, 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  e = 0;
-  for (int q = 0; q < 6; ++q) t[q] = 0;
-  for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
-    e += __ldcg(A.part + 7 * b);
-    if (A.tensor)
-      for (int q = 0; q < 6; ++q) t[q] += __ldcg(A.part + 7 * b + 1 + q);
-  }
-  const double tot = block_sum(e, scratch);
-  double tt[6];
-  if (A.tensor)
-    for (int q = 0; q < 6; ++q) tt[q] = block_sum(t[q], scratch);
-  if (threadIdx.x != 0) return;
-  *A.done = 0;
-  double* sc = A.sc;
-  sc[A.slot] = 0.5 * tot / kAcc;
-  if (A.tensor)
-    for (int q = 0; q < 6; ++q) sc[kScKin0 + q] = tt[q] / kAcc;
-  if (A.begin) step_begin_body(sc, A.t0, A.t1, A.steps, A.ndof);
-  if (A.then == kThenNhc) nhc_body(A.chain, sc, A.ndof, A.t_freq, A.dt);
-  else if (A.then == kThenBussi) bussi_body(sc, A.draws, A.draws_first, A.dt, A.tau, A.ndof);
-  else if (A.then == kThenBath) sc[kScBath] -= sc[kScKE] - sc[kScKE0];
+  if (i < A.n) ke_atom(A, i, e, t);
+  ke_blocks(A, e, t);
 }
 
 }  // namespace
@@ -1027,15 +1092,33 @@ struct Stepper {
                                                                  zero_cw ? 1 : 0, E.d_counters_.p);
     if (ncons) k_shake<<<blocks(size_t(C.ncl), 128), 128, 0, E.stream_>>>(C, x.p, x0.p, v.p, hd, E.d_counters_.p);
   }
-  // a velocity update, then RATTLE (constraint virial summed when h > 0)
-  void vel_rattle(const VelOp& op, double h) {
+  // a velocity update, then RATTLE (constraint virial summed when h > 0); with ke, also the kinetic energy and ke's
+  // thermostat update (constraints only: the caller launches k_ke otherwise)
+  void vel_rattle(const VelOp& op, double h, const KeArgs* ke = nullptr) {
     if (!ncons) {
       if (op.kind != 0) k_vel<<<blocks(size_t(n), 256), 256, 0, E.stream_>>>(n, v.p, invm.p, sc.p, op);
       return;
     }
-    k_vel_rattle<<<blocks(size_t(C.ncl + nfree), 128), 128, 0, E.stream_>>>(C, nfree, free_atoms.p, x.p, v.p, op, h, sc.p, E.d_counters_.p);
+    KeArgs K{};
+    if (ke) K = *ke;
+    k_vel_rattle<<<blocks(size_t(C.ncl + nfree), 128), 128, 0, E.stream_>>>(C, nfree, free_atoms.p, x.p, v.p, op, h, sc.p, E.d_counters_.p, K);
   }
   VelOp kick_op(double hk) const { return VelOp{1, E.d_f_.p, hk, 0, 0, 0, nullptr, 0}; }
+  // the kick from the force evaluation's sums (its reduction skipped), storing the forces to E.d_f_
+  VelOp kick_op_sums(double hk) const {
+    VelOp op = kick_op(hk);
+    op.f = nullptr;
+    const bool pairs = (E.opt_.parts & 2) != 0;
+    if (E.mixed_) op.fq = E.d_F_.p, op.fsq = pairs ? E.d_Fs_.p : nullptr;
+    else op.fd = E.d_Fd_.p, op.fsd = pairs ? E.d_Fsd_.p : nullptr;
+    op.iperm = pairs ? E.d_iperm_.p : nullptr;
+    op.nat = n;
+    op.nslots = int(size_t(E.nsc_cap_) * kScAtoms);
+    op.fout = E.d_f_.p;
+    return op;
+  }
+  // the kick + RATTLE + kinetic energy + thermostat tail in one launch (constraints, no r-RESPA)
+  bool fused_tail() const { return ncons > 0 && respa == 1; }
   void rattle(double h) {   // RATTLE alone (initial velocities)
     if (ncons) vel_rattle(VelOp{0, nullptr, 0, 0, 0, 0, nullptr, 0}, h);
   }
@@ -1046,22 +1129,24 @@ struct Stepper {
   // fast one. Part masks as Engine::forces takes them.
   DevBuf<double> f_slow, f_fast;
   int respa = 1, slow_parts = 6, fast_parts = 1;
-  void forces(bool ener, bool vir) {
+  void forces(bool ener, bool vir, bool reduce = true) {
     if (respa > 1) {
       E.forces(x.p, ener, vir, true, slow_parts, f_slow.p, true);
       E.forces(x.p, ener, vir, true, fast_parts, f_fast.p, false);
       return;
     }
-    E.forces(x.p, ener, vir, true);
+    E.forces(x.p, ener, vir, true, -1, nullptr, true, reduce);
   }
   void fast_forces() { E.forces(x.p, false, false, true, fast_parts, f_fast.p, true); }
 
   // One MD step (dynamics.cpp:606-666), energies and virial on request. Kernel sequence per step: NVT Nose-Hoover
-  // chain (on the kinetic energy the last step left), kick+drift, SHAKE, forces, kick+RATTLE, KE+chain, scale; Bussi step-begin, kick+drift, SHAKE, forces,
-  // kick+RATTLE, KE+Bussi, scale; Langevin (BAOAB) kick+drift, SHAKE, KE, O+RATTLE, KE+bath, drift, SHAKE, forces,
-  // kick+RATTLE.
+  // chain (on the kinetic energy the last step left), kick+drift, SHAKE, forces, kick+RATTLE+KE+chain (with constraints
+  // the kick reads the force sums and the kinetic energy and chain update run in the RATTLE launch's last block), scale;
+  // Bussi step-begin, kick+drift, SHAKE, forces, kick+RATTLE+KE+Bussi, scale; Langevin (BAOAB) kick+drift, SHAKE, KE,
+  // O+RATTLE, KE+bath, drift, SHAKE, forces, kick+RATTLE.
   void step(bool ener, bool vir) {
     const double dt = o.dt;
+    const double hw = vir ? dt : 0.0;   // the constraint virial only on steps that report it
     if (respa > 1) {
       // r-RESPA (dynamics.cpp:643-657): outer half kick with the slow forces; `respa` velocity-Verlet steps of dt/respa
       // with the fast ones; outer half kick. Adjacent kicks with the same forces are merged.
@@ -1073,7 +1158,7 @@ struct Stepper {
         kick_drift(h, h, false, false, f_fast.p);
       }
       forces(ener, vir);
-      vel_rattle(VelOp{1, f_fast.p, 0.5 * h, 0, 0, 0, f_slow.p, 0.5 * dt}, dt);
+      vel_rattle(VelOp{1, f_fast.p, 0.5 * h, 0, 0, 0, f_slow.p, 0.5 * dt}, hw);
       if (bussi) {
         KeArgs A = ke_args(kScKE, false);
         A.then = kThenBussi;
@@ -1094,27 +1179,35 @@ struct Stepper {
       ke_launch(A);
       kick_drift(0, 0.5 * dt, false, false);
       forces(ener, vir);
-      vel_rattle(kick_op(0.5 * dt), dt);
+      vel_rattle(kick_op(0.5 * dt), hw);
     } else if (nhc) {
       k_nhc_begin<<<1, 1, 0, E.stream_>>>(chain.p, sc.p, o.temperature, o.temperature_end, (long long)o.steps, ndof, t_freq, dt);
       kick_drift(0.5 * dt, dt, true, true);
-      forces(ener, vir);
-      vel_rattle(kick_op(0.5 * dt), dt);
       KeArgs A = ke_args(kScKE, false);
       A.then = kThenNhc;
-      ke_launch(A);
+      if (fused_tail()) {
+        forces(ener, vir, false);
+        vel_rattle(kick_op_sums(0.5 * dt), hw, &A);
+      } else {
+        forces(ener, vir);
+        vel_rattle(kick_op(0.5 * dt), hw);
+        ke_launch(A);
+      }
       scale_v();
     } else {
       k_step_begin<<<1, 1, 0, E.stream_>>>(sc.p, o.temperature, o.temperature_end, (long long)o.steps, ndof);
       kick_drift(0.5 * dt, dt, false, true);
-      forces(ener, vir);
-      vel_rattle(kick_op(0.5 * dt), dt);
-      if (bussi) {
-        KeArgs A = ke_args(kScKE, false);
-        A.then = kThenBussi;
-        ke_launch(A);
-        scale_v();
+      KeArgs A = ke_args(kScKE, false);
+      A.then = kThenBussi;
+      if (fused_tail()) {
+        forces(ener, vir, false);
+        vel_rattle(kick_op_sums(0.5 * dt), hw, bussi ? &A : nullptr);
+      } else {
+        forces(ener, vir);
+        vel_rattle(kick_op(0.5 * dt), hw);
+        if (bussi) ke_launch(A);
       }
+      if (bussi) scale_v();
     }
   }
 
@@ -1257,7 +1350,7 @@ void MdRun::start() {
   S.chain.alloc(1);
   CK(cudaMemsetAsync(S.chain.p, 0, sizeof(Chain), stream_));
   S.nparts = blocks(size_t(n_), 256);
-  S.part.alloc(size_t(7) * S.nparts);
+  S.part.alloc(size_t(7) * std::max(S.nparts, blocks(size_t(n_), 128)));   // k_ke's blocks, or k_vel_rattle's
   S.done.alloc(1);
   S.done.zero(stream_);
   S.respa = std::max(1, o.respa);

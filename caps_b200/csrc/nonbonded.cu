@@ -222,7 +222,7 @@ void Engine::pair_forces(bool ener, bool vir) {
 
 // One force evaluation on device positions d_x (AoS, 3 n): accumulators cleared, list checked / rebuilt, every term,
 // forces reduced into d_f_ (AoS doubles). Asynchronous on stream_.
-void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild, int parts, double* d_out, bool clear_energies) {
+void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild, int parts, double* d_out, bool clear_energies, bool reduce) {
   // internal part mask: 1 bonded, 2 short-range non-bonded (list, pair kernel, 1-4 pairs), 4 long-range (PME and its
   // excluded-pair corrections); the options' non-bonded bit means both 2 and 4
   const int pm = parts >= 0 ? parts : ((opt_.parts & 1) | ((opt_.parts & 2) ? 6 : 0));
@@ -266,6 +266,7 @@ void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild, 
   }
   join(0);
   if (pme) join(1);
+  if (!reduce) return;   // the caller's kick reads the sums (with iperm) itself
   const size_t ns = size_t(nsc_cap_) * kScAtoms;
   if (mixed_) k_reduce_f32<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_F_.p, d_Fs_.p, int(ns), d_iperm_.p, out, nonb ? 1 : 0);
   else k_reduce_f64<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_Fd_.p, d_Fsd_.p, int(ns), d_iperm_.p, out, nonb ? 1 : 0);
