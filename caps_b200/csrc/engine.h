@@ -146,6 +146,7 @@ class Engine {
   // Autotuning (timed on this system and GPU, once): the j-tile depth of the pair kernels' work items, and the PME
   // line-transform block shapes per grid.
   int batch_ = kBatch;
+  bool sums_cleared_ = false;   // the atom-order force sums were cleared by the integrator's kick (the next forces() skips it)
   bool batch_tuned_ = false;
   void tune_batch(const double* d_x);
   template <class R> void fft_passes(PmePath<R>& P, bool ener, bool vir);

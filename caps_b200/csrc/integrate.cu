@@ -93,30 +93,51 @@ struct HostRng {
 
 // --- kernels --------------------------------------------------------------------------------------------------
 // Kick then drift, per atom: v = s v + (hk f + hk2 f2) kAcc / m (s = sc[kScFactor] when `scale`, the thermostat's
-// pending velocity factor, else 1; f2 may be null), x0 = x (the constraint reference), x += hd v. Non-finite positions raise the error word. With
-// `zero_cw` the constraint-virial sums of this step start at zero.
-__global__ void k_kick_drift(int n, double* __restrict__ x, double* __restrict__ v, double* __restrict__ x0, const double* __restrict__ f,
-                             const double* __restrict__ invm, double hk, const double* __restrict__ f2, double hk2, double hd, double* sc, int scale,
-                             int zero_cw, int* counters) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (zero_cw && i < 6) sc[kScCW0 + i] = 0;
-  if (i >= n) return;
-  const double s = scale ? sc[kScFactor] : 1.0;
-  const double a = hk * kAcc * invm[i], a2 = hk2 * kAcc * invm[i];
+// pending velocity factor, else 1; f2 may be null), x0 = x (the constraint reference), x += hd v. Non-finite positions
+// raise the error word. With `zero_cw` the constraint-virial sums of this step start at zero. With fq (FP32 path) or fd
+// (FP64 path) set, the atom's rows of the force evaluation's atom-order sums are cleared for the evaluation that follows
+// (its own clearing is then skipped).
+struct KickArgs {
+  int n;
+  double* x;
+  double* v;
+  double* x0;
+  const double* f;
+  const double* invm;
+  double hk;
+  const double* f2;
+  double hk2;
+  double hd;
+  double* sc;
+  int scale, zero_cw;
+  int* counters;
+  long long* fq;
+  double* fd;
+};
+__device__ __forceinline__ void kick_drift_atom(const KickArgs& K, int i, double s) {
+  const double a = K.hk * kAcc * K.invm[i], a2 = K.hk2 * kAcc * K.invm[i];
   bool bad = false;
   for (int r = 0; r < 3; ++r) {
-    double vr = v[3 * i + r];
-    if (scale) vr *= s;
-    vr += a * f[3 * i + r];
-    if (f2) vr += a2 * f2[3 * i + r];   // r-RESPA: the slow and the fast forces in one kick
-    v[3 * i + r] = vr;
-    const double xo = x[3 * i + r];
-    x0[3 * i + r] = xo;
-    const double xn = xo + hd * vr;
-    x[3 * i + r] = xn;
+    double vr = K.v[3 * i + r];
+    if (K.scale) vr *= s;
+    vr += a * K.f[3 * i + r];
+    if (K.f2) vr += a2 * K.f2[3 * i + r];   // r-RESPA: the slow and the fast forces in one kick
+    K.v[3 * i + r] = vr;
+    const double xo = K.x[3 * i + r];
+    K.x0[3 * i + r] = xo;
+    const double xn = xo + K.hd * vr;
+    K.x[3 * i + r] = xn;
     bad |= !isfinite(xn);
+    if (K.fq) K.fq[size_t(r) * K.n + i] = 0;
+    if (K.fd) K.fd[size_t(r) * K.n + i] = 0;
   }
-  if (bad) atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), kErrNonFinite);
+  if (bad) atomicOr(reinterpret_cast<unsigned*>(K.counters + kCntErr), kErrNonFinite);
+}
+__global__ void k_kick_drift(KickArgs K) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (K.zero_cw && i < 6) K.sc[kScCW0 + i] = 0;
+  if (i >= K.n) return;
+  kick_drift_atom(K, i, K.scale ? K.sc[kScFactor] : 1.0);
 }
 
 // Constraint clusters. Star clusters (one centre bonded to 1-3 atoms, every constraint through the centre: CH, CH2, CH3)
@@ -1087,10 +1108,14 @@ struct Stepper {
   void ke_launch(const KeArgs& A) { k_ke<<<nparts, 256, 0, E.stream_>>>(A); }
   void ke(int slot, bool tensor) { ke_launch(ke_args(slot, tensor)); }
   // half kick, then drift with SHAKE; `scale` applies the thermostat's pending factor first
+  // kick + drift, then SHAKE; the kick also clears the force evaluation's atom-order sums for the evaluation that
+  // follows (Engine::forces then skips its own clearing)
   void kick_drift(double hk, double hd, bool scale, bool zero_cw, const double* f = nullptr, const double* f2 = nullptr, double hk2 = 0) {
-    k_kick_drift<<<blocks(size_t(n), 256), 256, 0, E.stream_>>>(n, x.p, v.p, x0.p, f ? f : E.d_f_.p, invm.p, hk, f2, hk2, hd, sc.p, scale ? 1 : 0,
-                                                                 zero_cw ? 1 : 0, E.d_counters_.p);
+    KickArgs K{n, x.p, v.p, x0.p, f ? f : E.d_f_.p, invm.p, hk, f2, hk2, hd, sc.p, scale ? 1 : 0, zero_cw ? 1 : 0, E.d_counters_.p,
+               E.mixed_ ? E.d_F_.p : nullptr, E.mixed_ ? nullptr : E.d_Fd_.p};
+    k_kick_drift<<<blocks(size_t(n), 256), 256, 0, E.stream_>>>(K);
     if (ncons) k_shake<<<blocks(size_t(C.ncl), 128), 128, 0, E.stream_>>>(C, x.p, x0.p, v.p, hd, E.d_counters_.p);
+    E.sums_cleared_ = true;
   }
   // a velocity update, then RATTLE (constraint virial summed when h > 0); with ke, also the kinetic energy and ke's
   // thermostat update (constraints only: the caller launches k_ke otherwise)

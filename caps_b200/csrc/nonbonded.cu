@@ -75,10 +75,10 @@ void Engine::tune_batch(const double* d_x) {
     launch_build(d_x);
     if (mixed_)
       k_pack_f32<<<blocks_for(ns, 256), 256, 0, stream_>>>(int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_sc_org_.p, d_q_.p, d_type_.p, nt_,
-                                                           d_xq_.p, d_tslot_.p, d_counters_.p, d_x0_.p);
+                                                           d_xq_.p, d_tslot_.p, d_counters_.p, d_x0_.p, d_Fs_.p);
     else
       k_pack_f64<<<blocks_for(ns, 256), 256, 0, stream_>>>(int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_q_.p, d_type_.p, nt_, d_xqd_.p, d_tslot_.p,
-                                                           d_counters_.p, d_x0_.p);
+                                                           d_counters_.p, d_x0_.p, d_Fsd_.p);
     prune(d_x);
     float ms = 0;
     for (int rep = 0; rep < 4; ++rep) {
@@ -229,13 +229,13 @@ void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild, 
   const bool nonb = (pm & 2) != 0;
   double* out = d_out ? d_out : d_f_.p;
   if (nonb && !batch_tuned_) tune_batch(d_x);
-  if (mixed_) {
-    CK(cudaMemsetAsync(d_F_.p, 0, d_F_.n * sizeof(long long), stream_));
-    if (nonb) CK(cudaMemsetAsync(d_Fs_.p, 0, d_Fs_.n * sizeof(long long), stream_));
-  } else {
-    CK(cudaMemsetAsync(d_Fd_.p, 0, d_Fd_.n * sizeof(double), stream_));
-    if (nonb) CK(cudaMemsetAsync(d_Fsd_.p, 0, d_Fsd_.n * sizeof(double), stream_));
+  // the atom-order sums start at zero (the integrator's kick may have cleared them already); the pack kernel clears the
+  // pair kernel's slot-order sums
+  if (!sums_cleared_) {
+    if (mixed_) CK(cudaMemsetAsync(d_F_.p, 0, d_F_.n * sizeof(long long), stream_));
+    else CK(cudaMemsetAsync(d_Fd_.p, 0, d_Fd_.n * sizeof(double), stream_));
   }
+  sums_cleared_ = false;
   if ((ener || vir) && clear_energies) {
     CK(cudaMemsetAsync(d_efix_.p, 0, d_efix_.n * sizeof(long long), stream_));
     CK(cudaMemsetAsync(d_edbl_.p, 0, d_edbl_.n * sizeof(double), stream_));
@@ -257,10 +257,10 @@ void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild, 
     const size_t ns = size_t(nsc_cap_) * kScAtoms;
     if (mixed_)
       k_pack_f32<<<blocks_for(ns, 256), 256, 0, stream_>>>(int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_sc_org_.p, d_q_.p, d_type_.p, nt_,
-                                                           d_xq_.p, d_tslot_.p, d_counters_.p, d_x0_.p);
+                                                           d_xq_.p, d_tslot_.p, d_counters_.p, d_x0_.p, d_Fs_.p);
     else
       k_pack_f64<<<blocks_for(ns, 256), 256, 0, stream_>>>(int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_q_.p, d_type_.p, nt_, d_xqd_.p, d_tslot_.p,
-                                                           d_counters_.p, d_x0_.p);
+                                                           d_counters_.p, d_x0_.p, d_Fsd_.p);
     prune(d_x);
     pair_forces(ener, vir);
   }

@@ -23,8 +23,11 @@ constexpr float kPadFar = 1.0e5f;   // padding slots sit this far from their sup
 // K-PACK (FP32): per slot, float4 (position relative to the super-cluster origin, charge) and the type index.
 static __global__ void k_pack_f32(int nslots, const int* __restrict__ perm, const double* __restrict__ x, const int* __restrict__ ioff, DevCell cell,
                            const double* __restrict__ sc_org, const double* __restrict__ q, const int* __restrict__ type, int pad_type,
-                           float4* __restrict__ xq, int* __restrict__ tslot, int* counters, double* __restrict__ x0) {
+                           float4* __restrict__ xq, int* __restrict__ tslot, int* counters, double* __restrict__ x0,
+                           long long* __restrict__ fs) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < nslots)   // the pair kernel's slot-order sums (3 x nslots) start at zero
+    for (int r = 0; r < 3; ++r) fs[size_t(r) * nslots + s] = 0;
   const bool built = counters[kCntRebuild] != 0;   // a build ran this step: the list was built at these positions
   if (s == 0) {
     counters[kCntPairNext] = 0;   // the pair kernel's work-item counter
@@ -55,8 +58,10 @@ static __global__ void k_pack_f32(int nslots, const int* __restrict__ perm, cons
 // K-PACK (FP64): per slot, double4 (wrapped absolute position, charge) and the type index.
 static __global__ void k_pack_f64(int nslots, const int* __restrict__ perm, const double* __restrict__ x, const int* __restrict__ ioff, DevCell cell,
                            const double* __restrict__ q, const int* __restrict__ type, int pad_type, double4* __restrict__ xq, int* __restrict__ tslot,
-                           int* counters, double* __restrict__ x0) {
+                           int* counters, double* __restrict__ x0, double* __restrict__ fs) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < nslots)   // the pair kernel's slot-order sums (3 x nslots) start at zero
+    for (int r = 0; r < 3; ++r) fs[size_t(r) * nslots + s] = 0;
   const bool built = counters[kCntRebuild] != 0;
   if (s == 0) {
     counters[kCntPairNext] = 0;
