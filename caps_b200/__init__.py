@@ -6,6 +6,7 @@ this package binds it with the reference's own names: Evaluator, EnergyOptions, 
 from .engine import (DeviceError, DynamicsCancelled, DynamicsOptions, EnergyOptions, Evaluator, FieldError,  # noqa: F401
                      cell_array, run_batch, run_dynamics)
 from .forcefield import ForceField, read_capsff  # noqa: F401
+from .cooling import CoolingOptions, fit_tg, run_cooling  # noqa: F401
 
 __all__ = ["Evaluator", "EnergyOptions", "DynamicsOptions", "run_dynamics", "run_batch", "ForceField", "read_capsff", "FieldError",
-           "DynamicsCancelled", "DeviceError", "cell_array"]
+           "DynamicsCancelled", "DeviceError", "cell_array", "CoolingOptions", "run_cooling", "fit_tg"]

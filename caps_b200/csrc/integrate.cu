@@ -1347,6 +1347,18 @@ struct MdRun {
     frame(hx.data(), E.cell_h_, step + o.step_offset, user);
   }
   bool refill_due(long long s) const { return S.bussi && s - S.draws_first >= S.draws_count; }
+  // Bussi draws are made ahead for steps [s, s + chunk). With the barostat on, a chunk ends at the next barostat step:
+  // the reference draws each step's thermostat numbers and then, on a barostat step, the barostat's normal from the
+  // same stream (dynamics.cpp:665, 709-711), so the host stream is consumed in that order.
+  long long draw_chunk(long long s) const {
+    long long c = std::min<long long>(std::max<long long>(o.steps - s + 1, 1), 4096);
+    if (o.barostat) {
+      const long long be = std::max(1, o.barostat_every);
+      const long long next = (s + be - 1) / be * be;
+      c = std::min(c, next - s + 1);
+    }
+    return c;
+  }
   bool baro_due(long long s) const { return o.barostat && s % baro_every == 0; }
   // a step that reports, records, rescales the cell or refills the thermostat's draws
   bool special(long long s) const {
@@ -1432,7 +1444,7 @@ void MdRun::start() {
     S.v.upload(hv, stream_);
   }
   if (S.ncons) S.rattle(0);
-  if (S.bussi) S.make_draws(1, std::min<long long>(std::max<long long>(o.steps, 1), 4096));
+  if (S.bussi) S.make_draws(1, draw_chunk(1));
 
   // the first force, energies and virial
   S.forces(true, true);
@@ -1460,7 +1472,7 @@ void MdRun::start() {
 void MdRun::advance(long long s) {
   if (refill_due(s)) {
     CK(cudaStreamSynchronize(E.stream_));
-    S.make_draws(s, std::min<long long>(o.steps - s + 1, 4096));
+    S.make_draws(s, draw_chunk(s));
     S.drop_graphs();   // the draw table's first step is a parameter of the captured thermostat kernel
     ++generation;
   }

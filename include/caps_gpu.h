@@ -187,6 +187,24 @@ void caps_gpu_destroy(caps_gpu_engine* e);
 /* Text of the last error on this engine (or of the last failed caps_gpu_create when e is NULL). */
 const char* caps_gpu_error(const caps_gpu_engine* e);
 
+/* A glass-transition fit of a cooling scan's points (y against T): BilinearFit (core/include/caps/mechanics.hpp:303-311). */
+typedef struct {
+  int32_t ok;
+  double tg, tg_err;                 /* K; tg_err from a bootstrap (NaN: no estimate) */
+  double slope_low, slope_high;      /* dy/dT below and above Tg */
+  double value_at_tg;
+  double alpha_low, alpha_high;      /* (1/y) dy/dT at Tg */
+  double rss;
+  char note[256];                    /* empty, or why the fit is doubtful or failed */
+} caps_gpu_tg_fit;
+
+/* Tg from points (T[i], y[i]), i < n: method 0 a continuous two-line fit with the hinge free (fit_bilinear,
+ * core/src/mechanics.cpp:1218, needs n >= 5), 1 two straight lines through a glassy range (T <= glassy_max) and a rubbery
+ * range (T >= rubbery_min) that cross at Tg (fit_two_ranges, mechanics.cpp:1310; 0 for either: the lowest and highest
+ * thirds). Host code, no device needed; the same points give the reference's Tg and bootstrap error. A fit that cannot
+ * be made returns 0 with out->ok = 0 and the reason in out->note. */
+int32_t caps_gpu_fit_tg(const double* T, const double* y, int32_t n, int32_t method, double glassy_max, double rubbery_min, caps_gpu_tg_fit* out);
+
 /* Kinetic energy and kinetic tensor of n atoms, computed without allocating any device memory. No counterpart in the
  * reference: it is for callers that may not call cudaMalloc, such as a host whose memory manager owns all device memory
  * and hands out its own buffers, or code running beside a long stream-ordered pipeline that an allocation would

@@ -47,6 +47,9 @@ def lib() -> C.CDLL:
         L.ref_pme.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_int]
         L.ref_build_ps_gaff.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_uint64, C.c_char_p]
         L.ref_build_kg.argtypes = [C.c_int, C.c_int, C.c_double, C.c_uint64, C.c_char_p]
+        L.ref_fit_tg.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.POINTER(_abi.TgFit)]
+        L.ref_run_cooling.argtypes = [C.POINTER(_abi.FF), C.POINTER(_abi.Opts), C.POINTER(_abi.State), C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(_abi.TgFit)]
         _lib = L
     return _lib
 
@@ -96,6 +99,40 @@ def run(ff: ForceField, x, cell, opts: DynamicsOptions, v=None, threads: int = 1
         raise RuntimeError(lib().ref_error().decode())
     th = [rows[k].as_dict() for k in range(min(nrows.value, max_rows))]
     return {"x": xx.reshape(-1, 3), "v": vv.reshape(-1, 3), "cell": c, "thermo": th, "seconds": sec.value, "ns_per_day": nsd.value}
+
+
+def fit_tg(T, y, method: int = 0, glassy_max: float = 0.0, rubbery_min: float = 0.0) -> dict:
+    """caps::fit_bilinear (method 0) or caps::fit_two_ranges (method 1) on the given points."""
+    t = np.ascontiguousarray(np.asarray(T, dtype=np.float64).reshape(-1))
+    v = np.ascontiguousarray(np.asarray(y, dtype=np.float64).reshape(-1))
+    out = _abi.TgFit()
+    if lib().ref_fit_tg(_vp(t), _vp(v), int(t.size), int(method), float(glassy_max), float(rubbery_min), C.byref(out)) != 0:
+        raise RuntimeError(lib().ref_error().decode())
+    return out.as_dict()
+
+
+def run_cooling(ff: ForceField, x, cell, co, v=None, threads: int = 1, max_points: int = 1000) -> dict:
+    """caps::run_cooling in the reference core on one structure; co: a caps_b200.cooling.CoolingOptions. Returns
+    {points, fit, x, v, cell}."""
+    s, keep = ff.to_struct()
+    o = co.energy.to_struct()
+    xx = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1)).copy()
+    vv = np.zeros_like(xx) if v is None else np.ascontiguousarray(np.asarray(v, dtype=np.float64).reshape(-1)).copy()
+    c = cell_array(cell).copy()
+    st = _abi.State(_vp(xx), _vp(vv), _vp(c), 0 if v is None else 1)
+    opt = np.array([co.t_start, co.t_end, co.t_step, co.ps_per_step, co.equilibrate_ps, co.average_from, co.dt, co.tau_t, co.tau_p,
+                    co.pressure, co.compressibility, co.glassy_max, co.rubbery_min], dtype=np.float64)
+    iopt = np.array([0 if co.barostat.lower() == "none" else 1, co.seed, int(bool(co.new_velocities)), co.property, co.fit], dtype=np.int64)
+    el = np.ascontiguousarray(ff.element if ff.element is not None else np.full(ff.natoms, 6), dtype=np.int32)
+    pts = np.zeros((max_points, 5))
+    npts = C.c_int()
+    fit = _abi.TgFit()
+    if lib().ref_run_cooling(C.byref(s), C.byref(o), C.byref(st), _vp(opt), _vp(iopt), _vp(el), threads, _vp(pts), max_points, C.byref(npts),
+                             C.byref(fit)) != 0:
+        raise RuntimeError(lib().ref_error().decode())
+    keys = ("temperature", "density", "density_err", "specific_volume", "potential")
+    points = [dict(zip(keys, map(float, pts[k]))) for k in range(min(npts.value, max_points))]
+    return {"points": points, "fit": fit.as_dict(), "x": xx.reshape(-1, 3), "v": vv.reshape(-1, 3), "cell": c}
 
 
 def ewald_beta(rc: float, rtol: float) -> float:

@@ -6,6 +6,8 @@
 //   ref_compute  -> caps::Evaluator::compute      (core/src/field.cpp:1249)
 //   ref_run      -> caps::run_dynamics            (core/src/dynamics.cpp:71)
 //   ref_pme      -> caps::pme_reciprocal (threaded, core/src/kspace.cpp:80)
+//   ref_fit_tg   -> caps::fit_bilinear / caps::fit_two_ranges (core/src/mechanics.cpp:1218, 1310)
+//   ref_run_cooling -> caps::run_cooling      (core/src/mechanics.cpp:1381)
 //   ref_build_*  -> the reference builders (grow + relax + assign_gaff as tests/test_nbnxm.cpp:19-34; kremer_grest),
 //                   written to a flat binary file the Python side reads (tests/golden fixtures are made from these).
 #include <chrono>
@@ -23,6 +25,7 @@
 #include "caps/grow.hpp"
 #include "caps/kremer_grest.hpp"
 #include "caps/kspace.hpp"
+#include "caps/mechanics.hpp"
 #include "caps/relax.hpp"
 #include "kspace_pool.hpp"
 #include "parallel.hpp"
@@ -234,6 +237,35 @@ void export_system(const System& s, const ForceField& ff, const char* path) {
   w.s("name", ff.name);
 }
 
+System to_system(const caps_gpu_ff* p, const std::shared_ptr<ForceField>& ff, const caps_gpu_state* st, const int32_t* element) {
+  System s;
+  const int n = p->natoms;
+  s.atoms.resize(size_t(n));
+  for (int i = 0; i < n; ++i) {
+    for (int k = 0; k < 3; ++k) s.atoms[size_t(i)].pos[k] = st->x[3 * i + k];
+    s.atoms[size_t(i)].element = element ? element[i] : 6;
+    s.atoms[size_t(i)].charge = p->charge[i];
+    s.atoms[size_t(i)].type = p->type_index[i] + 1;
+  }
+  for (const auto& b : ff->bonds) s.bonds.push_back({b.i, b.j, 1});
+  for (const auto& b : ff->bonds_x) s.bonds.push_back({b.i, b.j, 1});
+  s.cell = to_cell(st->cell);
+  if (st->has_velocities && st->v) {
+    s.velocities.resize(size_t(n));
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k < 3; ++k) s.velocities[size_t(i)][k] = st->v[3 * i + k];
+  }
+  return s;
+}
+
+void to_fit(const BilinearFit& f, caps_gpu_tg_fit* out) {
+  std::memset(out, 0, sizeof *out);
+  out->ok = f.ok ? 1 : 0;
+  out->tg = f.tg, out->tg_err = f.tg_err, out->slope_low = f.slope_low, out->slope_high = f.slope_high;
+  out->value_at_tg = f.value_at_tg, out->alpha_low = f.alpha_low, out->alpha_high = f.alpha_high, out->rss = f.rss;
+  std::strncpy(out->note, f.note.c_str(), sizeof out->note - 1);
+}
+
 }  // namespace
 
 extern "C" {
@@ -411,6 +443,60 @@ int ref_build_kg(int chains, int beads, double density, uint64_t seed, const cha
     System s = kremer_grest(o);
     const ForceField ff = kremer_grest_forcefield(s, o);
     export_system(s, ff, path);
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+// The reference's Tg fits on given points: method 0 fit_bilinear, 1 fit_two_ranges.
+int ref_fit_tg(const double* T, const double* y, int n, int method, double glassy_max, double rubbery_min, caps_gpu_tg_fit* out) {
+  try {
+    const std::vector<double> t(T, T + n), v(y, y + n);
+    to_fit(method == 1 ? fit_two_ranges(t, v, glassy_max, rubbery_min) : fit_bilinear(t, v), out);
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+// run_cooling on a System rebuilt from the arrays. opt: t_start, t_end, t_step, ps_per_step, equilibrate_ps,
+// average_from, dt, tau_t, tau_p, pressure, compressibility, glassy_max, rubbery_min; iopt: barostat (0 none, 1
+// c-rescale), seed, new_velocities, property, fit. points: up to max_points x 5 (T, density, density_err,
+// specific volume, potential). The end state is written back to st.
+int ref_run_cooling(const caps_gpu_ff* p, const caps_gpu_opts* eo, caps_gpu_state* st, const double* opt, const int64_t* iopt,
+                    const int32_t* element, int threads, double* points, int max_points, int* npoints, caps_gpu_tg_fit* fit) {
+  try {
+    auto ff = to_ff(p);
+    System s = to_system(p, ff, st, element);
+    CoolingOptions o;
+    o.field = ff;
+    o.energy = to_eo(eo, threads);
+    o.t_start = opt[0], o.t_end = opt[1], o.t_step = opt[2], o.ps_per_step = opt[3], o.equilibrate_ps = opt[4];
+    o.average_from = opt[5], o.dt = opt[6], o.tau_t = opt[7], o.tau_p = opt[8], o.pressure = opt[9], o.compressibility = opt[10];
+    o.glassy_max = opt[11], o.rubbery_min = opt[12];
+    o.barostat = iopt[0] == 1 ? Barostat::CRescale : Barostat::None;
+    o.seed = uint64_t(iopt[1]);
+    o.new_velocities = iopt[2] != 0;
+    o.property = int(iopt[3]);
+    o.fit = int(iopt[4]);
+    const CoolingResult r = run_cooling(s, o);
+    *npoints = int(r.points.size());
+    for (int k = 0; k < std::min(*npoints, max_points); ++k) {
+      const CoolingPoint& q = r.points[size_t(k)];
+      double* d = points + 5 * k;
+      d[0] = q.temperature, d[1] = q.density, d[2] = q.density_err, d[3] = q.specific_volume, d[4] = q.potential;
+    }
+    to_fit(r.fit, fit);
+    const int n = p->natoms;
+    for (int i = 0; i < n; ++i)
+      for (int c = 0; c < 3; ++c) {
+        st->x[3 * i + c] = s.atoms[size_t(i)].pos[c];
+        if (st->v) st->v[3 * i + c] = s.velocities[size_t(i)][c];
+      }
+    from_cell(s.cell, st->cell);
     return 0;
   } catch (const std::exception& e) {
     g_err = e.what();
