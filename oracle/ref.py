@@ -50,6 +50,8 @@ def lib() -> C.CDLL:
         L.ref_fit_tg.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.POINTER(_abi.TgFit)]
         L.ref_run_cooling.argtypes = [C.POINTER(_abi.FF), C.POINTER(_abi.Opts), C.POINTER(_abi.State), C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(_abi.TgFit)]
+        L.ref_equilibrate.argtypes = [C.POINTER(_abi.FF), C.POINTER(_abi.Opts), C.POINTER(_abi.State), C.POINTER(_abi.MdOpts), C.c_int,
+                                      C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_int, C.c_void_p]
         _lib = L
     return _lib
 
@@ -133,6 +135,27 @@ def run_cooling(ff: ForceField, x, cell, co, v=None, threads: int = 1, max_point
     keys = ("temperature", "density", "density_err", "specific_volume", "potential")
     points = [dict(zip(keys, map(float, pts[k]))) for k in range(min(npts.value, max_points))]
     return {"points": points, "fit": fit.as_dict(), "x": xx.reshape(-1, 3), "v": vv.reshape(-1, 3), "cell": c}
+
+
+def equilibrate(ff: ForceField, x, cell, eq, v=None, threads: int = 1) -> dict:
+    """caps::equilibrate in the reference core; eq: a caps_b200.equilibrate.EquilibrateOptions. Returns {stages (ps,
+    temperature, pressure, density, potential, density_end per stage), x, v, cell}."""
+    s, keep = ff.to_struct()
+    o = eq.md.energy.to_struct()
+    xx = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1)).copy()
+    vv = np.zeros_like(xx) if v is None else np.ascontiguousarray(np.asarray(v, dtype=np.float64).reshape(-1)).copy()
+    c = cell_array(cell).copy()
+    st = _abi.State(_vp(xx), _vp(vv), _vp(c), 0 if v is None else 1)
+    m = eq.md.to_struct(ff, keep)
+    ens = np.array([{"nvt": 0, "npt": 1, "nve": 2}[g.ensemble] for g in eq.stages], dtype=np.int32)
+    sd = np.array([[g.ps, g.t_start, g.t_end, g.pressure, g.force_cap] for g in eq.stages], dtype=np.float64).reshape(-1)
+    el = np.ascontiguousarray(ff.element if ff.element is not None else np.full(ff.natoms, 6), dtype=np.int32)
+    out = np.zeros((len(eq.stages), 6))
+    if lib().ref_equilibrate(C.byref(s), C.byref(o), C.byref(st), C.byref(m), len(eq.stages), _vp(ens), _vp(sd), float(eq.thermo_ps), _vp(el),
+                             threads, _vp(out)) != 0:
+        raise RuntimeError(lib().ref_error().decode())
+    keys = ("ps", "temperature", "pressure", "density", "potential", "density_end")
+    return {"stages": [dict(zip(keys, map(float, r))) for r in out], "x": xx.reshape(-1, 3), "v": vv.reshape(-1, 3), "cell": c}
 
 
 def ewald_beta(rc: float, rtol: float) -> float:

@@ -8,6 +8,7 @@
 //   ref_pme      -> caps::pme_reciprocal (threaded, core/src/kspace.cpp:80)
 //   ref_fit_tg   -> caps::fit_bilinear / caps::fit_two_ranges (core/src/mechanics.cpp:1218, 1310)
 //   ref_run_cooling -> caps::run_cooling      (core/src/mechanics.cpp:1381)
+//   ref_equilibrate -> caps::equilibrate      (core/src/equilibrate.cpp:199)
 //   ref_build_*  -> the reference builders (grow + relax + assign_gaff as tests/test_nbnxm.cpp:19-34; kremer_grest),
 //                   written to a flat binary file the Python side reads (tests/golden fixtures are made from these).
 #include <chrono>
@@ -26,6 +27,7 @@
 #include "caps/kremer_grest.hpp"
 #include "caps/kspace.hpp"
 #include "caps/mechanics.hpp"
+#include "caps/equilibrate.hpp"
 #include "caps/relax.hpp"
 #include "kspace_pool.hpp"
 #include "parallel.hpp"
@@ -249,6 +251,17 @@ System to_system(const caps_gpu_ff* p, const std::shared_ptr<ForceField>& ff, co
   }
   for (const auto& b : ff->bonds) s.bonds.push_back({b.i, b.j, 1});
   for (const auto& b : ff->bonds_x) s.bonds.push_back({b.i, b.j, 1});
+  // the types' masses, as a data file's Masses section gives them (System::mass_of reads these before element masses)
+  std::vector<char> seen(size_t(p->ntypes), 0);
+  for (int i = 0; i < n; ++i) {
+    const int t = p->type_index[i];
+    if (t < 0 || t >= p->ntypes || seen[size_t(t)]) continue;
+    seen[size_t(t)] = 1;
+    TypeInfo ti;
+    ti.type = t + 1;
+    ti.mass = p->mass[i];
+    s.types.push_back(ti);
+  }
   s.cell = to_cell(st->cell);
   if (st->has_velocities && st->v) {
     s.velocities.resize(size_t(n));
@@ -490,6 +503,56 @@ int ref_run_cooling(const caps_gpu_ff* p, const caps_gpu_opts* eo, caps_gpu_stat
       d[0] = q.temperature, d[1] = q.density, d[2] = q.density_err, d[3] = q.specific_volume, d[4] = q.potential;
     }
     to_fit(r.fit, fit);
+    const int n = p->natoms;
+    for (int i = 0; i < n; ++i)
+      for (int c = 0; c < 3; ++c) {
+        st->x[3 * i + c] = s.atoms[size_t(i)].pos[c];
+        if (st->v) st->v[3 * i + c] = s.velocities[size_t(i)][c];
+      }
+    from_cell(s.cell, st->cell);
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+// equilibrate over given stages. ensemble[k]: 0 NVT, 1 NPT, 2 NVE; sd[5k..]: ps, t_start, t_end, pressure, force_cap.
+// md: the base dynamics options (dt, thermostat, tau_t, barostat, tau_p, compressibility, seed; energy from eo).
+// out[6k..]: ps, temperature, pressure, density, potential, density_end of each stage. The end state goes back to st.
+int ref_equilibrate(const caps_gpu_ff* p, const caps_gpu_opts* eo, caps_gpu_state* st, const caps_gpu_md_opts* md, int nstages,
+                    const int32_t* ensemble, const double* sd, double thermo_ps, const int32_t* element, int threads, double* out) {
+  try {
+    auto ff = to_ff(p);
+    System s = to_system(p, ff, st, element);
+    EquilibrateOptions o;
+    for (int k = 0; k < nstages; ++k) {
+      Stage g;
+      g.label = "stage " + std::to_string(k + 1);
+      g.ensemble = ensemble[k] == 1 ? Ensemble::NPT : ensemble[k] == 2 ? Ensemble::NVE : Ensemble::NVT;
+      g.ps = sd[5 * k], g.t_start = sd[5 * k + 1], g.t_end = sd[5 * k + 2], g.pressure = sd[5 * k + 3], g.force_cap = sd[5 * k + 4];
+      o.stages.push_back(g);
+    }
+    o.md.field = ff;
+    o.md.dt = md->dt;
+    const Thermostat th[4] = {Thermostat::None, Thermostat::Bussi, Thermostat::Langevin, Thermostat::NoseHoover};
+    o.md.thermostat = th[md->thermostat & 3];
+    o.md.tau_t = md->tau_t;
+    o.md.barostat = md->barostat == 1 ? Barostat::CRescale : Barostat::None;
+    o.md.tau_p = md->tau_p;
+    o.md.compressibility = md->compressibility;
+    o.md.barostat_every = md->barostat_every;
+    o.md.constraints = md->constraints ? ConstraintMode::HBonds : ConstraintMode::None;
+    o.md.seed = md->seed;
+    o.md.energy = to_eo(eo, threads);
+    o.thermo_ps = thermo_ps;
+    EquilibrateReport rep;
+    equilibrate(s, o, &rep);
+    for (size_t k = 0; k < rep.stages.size() && int(k) < nstages; ++k) {
+      const StageSummary& q = rep.stages[k];
+      double* d = out + 6 * k;
+      d[0] = q.ps, d[1] = q.temperature, d[2] = q.pressure, d[3] = q.density, d[4] = q.potential, d[5] = q.density_end;
+    }
     const int n = p->natoms;
     for (int i = 0; i < n; ++i)
       for (int c = 0; c < 3; ++c) {
