@@ -7,8 +7,10 @@ from .engine import (DeviceError, DynamicsCancelled, DynamicsOptions, EnergyOpti
                      cell_array, run_batch, run_dynamics)
 from .forcefield import ForceField, read_capsff  # noqa: F401
 from .cooling import CoolingOptions, fit_tg, run_cooling  # noqa: F401
+from .minimise import MinimiseOptions, minimise  # noqa: F401
 from .equilibrate import EquilibrateOptions, ProtocolParams, Stage, equilibrate, parse_protocol, protocol_by_name  # noqa: F401
 
 __all__ = ["Evaluator", "EnergyOptions", "DynamicsOptions", "run_dynamics", "run_batch", "ForceField", "read_capsff", "FieldError",
            "DynamicsCancelled", "DeviceError", "cell_array", "CoolingOptions", "run_cooling", "fit_tg", "EquilibrateOptions",
-           "ProtocolParams", "Stage", "equilibrate", "parse_protocol", "protocol_by_name"]
+           "ProtocolParams", "Stage", "equilibrate", "parse_protocol", "protocol_by_name", "MinimiseOptions",
+           "minimise"]

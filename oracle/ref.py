@@ -52,6 +52,8 @@ def lib() -> C.CDLL:
                                       C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(_abi.TgFit)]
         L.ref_equilibrate.argtypes = [C.POINTER(_abi.FF), C.POINTER(_abi.Opts), C.POINTER(_abi.State), C.POINTER(_abi.MdOpts), C.c_int,
                                       C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_int, C.c_void_p]
+        L.ref_minimise.argtypes = [C.POINTER(_abi.FF), C.POINTER(_abi.Opts), C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_int,
+                                   C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]
         _lib = L
     return _lib
 
@@ -156,6 +158,25 @@ def equilibrate(ff: ForceField, x, cell, eq, v=None, threads: int = 1) -> dict:
         raise RuntimeError(lib().ref_error().decode())
     keys = ("ps", "temperature", "pressure", "density", "potential", "density_end")
     return {"stages": [dict(zip(keys, map(float, r))) for r in out], "x": xx.reshape(-1, 3), "v": vv.reshape(-1, 3), "cell": c}
+
+
+def minimise(ff: ForceField, energy: EnergyOptions, x, cell, mo) -> dict:
+    """caps::minimise in the reference core; mo: a caps_b200.minimise.MinimiseOptions."""
+    s, keep = ff.to_struct()
+    o = energy.to_struct()
+    xx = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1)).copy()
+    c = cell_array(cell).copy()
+    code = {"sd": 0, "steepest": 0, "cg": 1, "lbfgs": 2, "l-bfgs": 2, "fire": 3}[mo.method.lower()]
+    fixed = None if mo.fixed is None else np.ascontiguousarray(np.asarray(mo.fixed, dtype=np.int8))
+    rs = np.ascontiguousarray(np.asarray(mo.restraints, dtype=np.float64).reshape(-1, 4)) if mo.restraints else np.zeros((0, 4))
+    ds = np.ascontiguousarray(np.asarray(mo.dihedral_restraints, dtype=np.float64).reshape(-1, 6)) if mo.dihedral_restraints else np.zeros((0, 6))
+    res = np.zeros(4)
+    stopped = C.c_int()
+    if lib().ref_minimise(C.byref(s), C.byref(o), _vp(xx), _vp(c), code, mo.ftol, mo.etol, mo.max_iterations,
+                          None if fixed is None else _vp(fixed), len(rs), _vp(rs), len(ds), _vp(ds), _vp(res), C.byref(stopped)) != 0:
+        raise RuntimeError(lib().ref_error().decode())
+    return {"iterations": int(res[0]), "energy": float(res[1]), "fmax": float(res[2]), "evaluations": int(res[3]),
+            "stopped_by": ("force", "energy", "iterations", "line search")[stopped.value], "x": xx.reshape(-1, 3)}
 
 
 def ewald_beta(rc: float, rtol: float) -> float:

@@ -9,6 +9,7 @@
 //   ref_fit_tg   -> caps::fit_bilinear / caps::fit_two_ranges (core/src/mechanics.cpp:1218, 1310)
 //   ref_run_cooling -> caps::run_cooling      (core/src/mechanics.cpp:1381)
 //   ref_equilibrate -> caps::equilibrate      (core/src/equilibrate.cpp:199)
+//   ref_minimise -> caps::minimise              (core/src/relax.cpp:65)
 //   ref_build_*  -> the reference builders (grow + relax + assign_gaff as tests/test_nbnxm.cpp:19-34; kremer_grest),
 //                   written to a flat binary file the Python side reads (tests/golden fixtures are made from these).
 #include <chrono>
@@ -560,6 +561,44 @@ int ref_equilibrate(const caps_gpu_ff* p, const caps_gpu_opts* eo, caps_gpu_stat
         if (st->v) st->v[3 * i + c] = s.velocities[size_t(i)][c];
       }
     from_cell(s.cell, st->cell);
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+// minimise on an evaluator of the arrays' force field. method: 0 SD, 1 CG, 2 L-BFGS, 3 FIRE. fixed: [natoms] or NULL.
+// restr: nr x (i, j, r0, k); dihed: nd x (i, j, k, l, phi0, kphi). res: iterations, energy, fmax, evaluations; stopped:
+// 0 force, 1 energy, 2 iterations, 3 line search. x is minimised in place.
+int ref_minimise(const caps_gpu_ff* p, const caps_gpu_opts* eo, double* x, const double* cell, int method, double ftol, double etol, int max_it,
+                 const char* fixed, int nr, const double* restr, int nd, const double* dihed, double* res, int* stopped) {
+  try {
+    auto ff = to_ff(p);
+    RelaxOptions o;
+    const Minimiser ms[4] = {Minimiser::SteepestDescent, Minimiser::ConjugateGradient, Minimiser::LBFGS, Minimiser::FIRE};
+    o.method = ms[method & 3];
+    o.ftol = ftol, o.etol = etol, o.max_iterations = max_it;
+    o.energy = to_eo(eo, 1);
+    if (fixed) o.fixed.assign(fixed, fixed + p->natoms);
+    for (int k = 0; k < nr; ++k) {
+      RelaxOptions::Restraint r;
+      r.i = uint32_t(restr[4 * k]), r.j = uint32_t(restr[4 * k + 1]), r.r0 = restr[4 * k + 2], r.k = restr[4 * k + 3];
+      o.restraints.push_back(r);
+    }
+    for (int k = 0; k < nd; ++k) {
+      RelaxOptions::DihedralRestraint r;
+      const double* q = dihed + 6 * k;
+      r.i = uint32_t(q[0]), r.j = uint32_t(q[1]), r.k = uint32_t(q[2]), r.l = uint32_t(q[3]), r.phi0 = q[4], r.kphi = q[5];
+      o.dihedral_restraints.push_back(r);
+    }
+    Evaluator ev(*ff, o.energy);
+    std::vector<double> xv(x, x + 3 * size_t(p->natoms));
+    int nev = 0;
+    const RelaxStage st = minimise(ev, xv, to_cell(cell), o, "minimise", &nev);
+    std::memcpy(x, xv.data(), xv.size() * sizeof(double));
+    res[0] = st.iterations, res[1] = st.energy, res[2] = st.fmax, res[3] = nev;
+    *stopped = st.stopped_by == "force" ? 0 : st.stopped_by == "energy" ? 1 : st.stopped_by == "iterations" ? 2 : 3;
     return 0;
   } catch (const std::exception& e) {
     g_err = e.what();
