@@ -26,7 +26,7 @@ class FF(C.Structure):
         ("lj14", C.c_double), ("coul14", C.c_double),
         ("excl_offset", P), ("excl_list", P),
         ("nfene", C.c_int32), ("fene_ij", P), ("fene_k_r0_eps_sigma", P),
-        ("lj_shift", C.c_int32), ("model_cutoff", C.c_double),
+        ("lj_shift", C.c_int32), ("model_cutoff", C.c_double), ("lj_form", C.c_int32),
     ]
 
 

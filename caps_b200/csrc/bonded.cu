@@ -39,7 +39,7 @@ void Engine::bonded_forces(const double* d_x, bool ener, bool vir, int parts) {
     }
     if (nonb && np14_)
       LAUNCH3(k_pairs14, S, np14_, np14_, d_p14_ij_.p, p14_scaled_ ? d_p14_scale_.p : nullptr, lj14_, d_type_.p, nt_, d_lj14_.p,
-              opt_.force_cap > 0 ? (const double4*)d_cap14_.p : (const double4*)nullptr, A, F);
+              opt_.force_cap > 0 ? (const double4*)d_cap14_.p : (const double4*)nullptr, A, F, lj96_ ? 1 : 0);
     if (excl && coul_ && nx_) {
       ExclArgs E{d_excl_ij_.p, d_excl_f_.p, d_q_.p, d_gtab_.p, ghi_, rc_, rc_ * rc_, kappa_, dsf_e0_, dsf_f0_, pme_ ? 1 : 0};
       LAUNCHX(S, nx_, E, A, F);

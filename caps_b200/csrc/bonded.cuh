@@ -171,10 +171,11 @@ static __global__ void k_torsions(int ngroups, const int* __restrict__ gs, const
 }
 
 // 1-4 pairs: LJ times the 1-4 scale (and the same cut-off shift as the pairs), at the nearest image (field.cpp:2019-2043).
-// lj: per type pair (eps, sigma^6, energy shift of 4 eps (q_c^2 - q_c) or 0, 0); capped: (rcap^2, ecap, fcap, 0).
+// lj: per type pair (eps, sigma^6, the pairs' energy shift or 0, 0); capped: (rcap^2, ecap, fcap, 0). lj96: the class II
+// form eps (2 q^(3/2) - 3 q), q = (s/r)^6 (field.cpp:1471-1475), else 4 eps (q^2 - q).
 template <class R, class S, bool ENER, bool VIR>
 static __global__ void k_pairs14(int np, const uint32_t* __restrict__ ij, const double* __restrict__ scale, double lj14, const int* __restrict__ type, int nt,
-                          const double4* __restrict__ lj, const double4* __restrict__ cap, BondedArgs A, S F) {
+                          const double4* __restrict__ lj, const double4* __restrict__ cap, BondedArgs A, S F, int lj96) {
   Tally<VIR> T;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < np; t += gridDim.x * blockDim.x) {
     const int i = int(ij[2 * t]), j = int(ij[2 * t + 1]);
@@ -192,8 +193,14 @@ static __global__ void k_pairs14(int np, const uint32_t* __restrict__ ij, const 
       fr = sc * R(cp.z) / r;
     } else {
       const R q = R(c.y) / (r2 * r2 * r2);
-      ev = sc * 4 * R(c.x) * (q * q - q);
-      fr = sc * 24 * R(c.x) * (2 * q * q - q) / r2;
+      if (lj96) {
+        const R q9 = q * sqrt(q);
+        ev = sc * R(c.x) * (2 * q9 - 3 * q);
+        fr = sc * 18 * R(c.x) * (q9 - q) / r2;
+      } else {
+        ev = sc * 4 * R(c.x) * (q * q - q);
+        fr = sc * 24 * R(c.x) * (2 * q * q - q) / r2;
+      }
     }
     if (ENER) T.e += double(ev - sc * R(c.z));
     const R fx = dx * fr, fy = dy * fr, fz = dz * fr;

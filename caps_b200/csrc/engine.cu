@@ -273,6 +273,8 @@ void Engine::setup_ff(const caps_gpu_ff* ff) {
   }
   lj_shift_model_ = ff->lj_shift != 0;
   model_cutoff_ = ff->model_cutoff;
+  if (ff->lj_form != 0 && ff->lj_form != 1) throw ModelError(CAPS_GPU_EFIELD, "unknown pair form (0 lj12-6, 1 lj9-6)");
+  lj96_ = ff->lj_form == 1;
   CK(cudaStreamSynchronize(stream_));
 }
 
@@ -336,9 +338,11 @@ void Engine::setup_options() {
     for (int b0 = 0; b0 < nt_; ++b0) {
       const double eps = h_eps_[size_t(a0) * nt_ + b0], sg = h_sig_[size_t(a0) * nt_ + b0];
       const double s6 = std::pow(sg, 6);
-      const double c6 = eps > 0 ? 4 * eps * s6 : 0.0, c12 = eps > 0 ? 4 * eps * s6 * s6 : 0.0;
+      // 12-6: c6 r^-6 with c6 = 4 eps s^6, and 4 eps s^12 r^-12; 9-6 (field.cpp:860-861): 3 eps s^6 and 2 eps s^9 r^-9
+      const double c6 = eps > 0 ? (lj96_ ? 3 : 4) * eps * s6 : 0.0;
+      const double c12 = eps > 0 ? (lj96_ ? 2 * eps * s6 * std::sqrt(s6) : 4 * eps * s6 * s6) : 0.0;
       const double qc = s6 / (rc2 * rc2 * rc2);
-      const double sh = shifted_ && eps > 0 ? 4 * eps * (qc * qc - qc) : 0.0;
+      const double sh = shifted_ && eps > 0 ? (lj96_ ? eps * (2 * qc * std::sqrt(qc) - 3 * qc) : 4 * eps * (qc * qc - qc)) : 0.0;
       tab[size_t(a0) * ntab + b0] = make_float4(float(c6), float(c12), float(sh), 0.f);
       tabd[size_t(a0) * ntab + b0] = make_double4(c6, c12, sh, 0.0);
       l14[size_t(a0) * nt_ + b0] = make_double4(eps, s6, sh, 0.0);
@@ -355,17 +359,22 @@ void Engine::setup_options() {
         if (e <= 0) continue;
         const double sg = std::pow(s6, 1.0 / 6);
         auto force = [&](double r) {
+          if (lj96_) {
+            const double q = sg / r, q3 = q * q * q;
+            return 18 * e / r * (q3 * q3 * q3 - q3 * q3);
+          }
           const double q = s6 / std::pow(r, 6);
           return 24 * e / r * (2 * q * q - q);
         };
-        double lo = 0.3 * sg, hi = std::pow(2 * s6, 1.0 / 6);
+        double lo = 0.3 * sg, hi = lj96_ ? sg : std::pow(2 * s6, 1.0 / 6);   // F(hi) = 0
         if (force(lo) < opt_.force_cap) continue;
         for (int it = 0; it < 80; ++it) {
           const double m = 0.5 * (lo + hi);
           (force(m) > opt_.force_cap ? lo : hi) = m;
         }
         const double r = hi, q = s6 / std::pow(r, 6);
-        cap[size_t(a0) * ntab + b0] = make_double4(r * r, 4 * e * (q * q - q), force(r), 0.0);
+        const double ec = lj96_ ? e * (2 * std::pow(sg / r, 9) - 3 * q) : 4 * e * (q * q - q);
+        cap[size_t(a0) * ntab + b0] = make_double4(r * r, ec, force(r), 0.0);
         cap14[size_t(a0) * nt_ + b0] = cap[size_t(a0) * ntab + b0];
       }
   d_tabcap_.upload(cap, stream_);
@@ -566,6 +575,12 @@ void Engine::host_constants(caps_gpu_terms* t, bool ener, bool vir) const {
       for (int b0 = 0; b0 < nt_; ++b0) {
         const double eps = h_eps_[size_t(a0) * nt_ + b0], s6 = std::pow(h_sig_[size_t(a0) * nt_ + b0], 6), s12 = s6 * s6;
         const double nn = type_count_[size_t(a0)] * type_count_[size_t(b0)];
+        if (lj96_) {   // lj/class2 (field.cpp:2523-2529)
+          const double s3 = std::sqrt(s6), rc6 = rc3 * rc3;
+          et += nn * 2 * kPi * eps * s6 * (s3 - 3 * rc3) / (3 * rc6);
+          wt += nn * 3 * 2 * kPi * eps * s6 * (s3 - 2 * rc3) / rc6;
+          continue;
+        }
         et += nn * 2 * kPi * 4 * eps * (s12 / (9 * rc9) - s6 / (3 * rc3));
         wt += nn * 2 * kPi * 4 * eps * (4 * s12 / (3 * rc9) - 2 * s6 / rc3);
       }

@@ -188,6 +188,7 @@ class Engine {
   double lj14_ = 0.5;
   bool p14_scaled_ = false;
   bool lj_shift_model_ = false;
+  bool lj96_ = false;   // class II 9-6 pair form (ForceField::pair_form "lj9-6")
   double model_cutoff_ = 0;
 
   // options derived

@@ -181,12 +181,17 @@ void Engine::pair_forces(bool ener, bool vir) {
                         4 * kBatch * (sizeof(uint4) + sizeof(float4) + 8 * sizeof(float4) + 8 * sizeof(int));
     // the rational fits hold for (kappa r_c)^2 <= 16; past that the library erfc form
     const int c32 = coul == 0 ? 0 : (kappa_ * kappa_ * rc_ * rc_ <= double(kEwUMax) ? coul : coul + 2);
+#define PAIR32L(C, E, V, L)                                                                                          \
+  do {                                                                                                               \
+    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_pair_f32<C, E, V, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
+    int per_sm = 0;                                                                                                  \
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_f32<C, E, V, L>, 128, smem));                   \
+    k_pair_f32<C, E, V, L><<<dev_sms_ * std::max(1, per_sm), 128, smem, stream_>>>(A);                               \
+  } while (0)
 #define PAIR32(C, E, V)                                                                                              \
   do {                                                                                                               \
-    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_pair_f32<C, E, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
-    int per_sm = 0;                                                                                                  \
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_f32<C, E, V>, 128, smem));                      \
-    k_pair_f32<C, E, V><<<dev_sms_ * std::max(1, per_sm), 128, smem, stream_>>>(A);                                                            \
+    if (lj96_) PAIR32L(C, E, V, true);                                                                               \
+    else PAIR32L(C, E, V, false);                                                                                    \
   } while (0)
 #define PAIR32C(C) { if (ener) { if (vir) PAIR32(C, true, true); else PAIR32(C, true, false); } else { if (vir) PAIR32(C, false, true); else PAIR32(C, false, false); } }
     switch (c32) {
@@ -198,24 +203,31 @@ void Engine::pair_forces(bool ener, bool vir) {
     }
 #undef PAIR32C
 #undef PAIR32
+#undef PAIR32L
   } else {
     const size_t smem = sizeof(double4) * (size_t(ntab) * ntab + 4 * 64) + sizeof(double) * 2 * size_t(coul ? gnodes_ : 0) + sizeof(int) * 4 * 64;
-#define PAIR64(C, ...)                                                                                               \
+#define PAIR64L(C, E, V, CAP, L)                                                                                     \
   do {                                                                                                               \
-    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_pair_f64<C, __VA_ARGS__>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
+    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_pair_f64<C, E, V, CAP, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
     int per_sm = 0;                                                                                                  \
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_f64<C, __VA_ARGS__>, 128, smem));               \
-    k_pair_f64<C, __VA_ARGS__><<<dev_sms_ * std::max(1, per_sm), 128, smem, stream_>>>(A);                                                     \
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_f64<C, E, V, CAP, L>, 128, smem));              \
+    k_pair_f64<C, E, V, CAP, L><<<dev_sms_ * std::max(1, per_sm), 128, smem, stream_>>>(A);                          \
+  } while (0)
+#define PAIR64(C, E, V, CAP)                                                                                         \
+  do {                                                                                                               \
+    if (lj96_) PAIR64L(C, E, V, CAP, true);                                                                          \
+    else PAIR64L(C, E, V, CAP, false);                                                                               \
   } while (0)
     if (opt_.force_cap > 0) {
       // push-off: energies and virial always on (a rare path, kept to one instantiation per Coulomb form)
       if (coul == 1) PAIR64(1, true, true, true);
       else if (coul == 2) PAIR64(2, true, true, true);
       else PAIR64(0, true, true, true);
-    } else if (coul == 1) { if (ener) { if (vir) PAIR64(1, true, true); else PAIR64(1, true, false); } else { if (vir) PAIR64(1, false, true); else PAIR64(1, false, false); } }
-    else if (coul == 2) { if (ener) { if (vir) PAIR64(2, true, true); else PAIR64(2, true, false); } else { if (vir) PAIR64(2, false, true); else PAIR64(2, false, false); } }
-    else { if (ener) { if (vir) PAIR64(0, true, true); else PAIR64(0, true, false); } else { if (vir) PAIR64(0, false, true); else PAIR64(0, false, false); } }
+    } else if (coul == 1) { if (ener) { if (vir) PAIR64(1, true, true, false); else PAIR64(1, true, false, false); } else { if (vir) PAIR64(1, false, true, false); else PAIR64(1, false, false, false); } }
+    else if (coul == 2) { if (ener) { if (vir) PAIR64(2, true, true, false); else PAIR64(2, true, false, false); } else { if (vir) PAIR64(2, false, true, false); else PAIR64(2, false, false, false); } }
+    else { if (ener) { if (vir) PAIR64(0, true, true, false); else PAIR64(0, true, false, false); } else { if (vir) PAIR64(0, false, true, false); else PAIR64(0, false, false, false); } }
 #undef PAIR64
+#undef PAIR64L
   }
   CK(cudaGetLastError());
 }

@@ -176,7 +176,7 @@ __device__ __forceinline__ void reduce_i(int jq, const T fx[8], const T fy[8], c
 // --- FP32 path ---------------------------------------------------------------------------------------------------
 // COUL: 0 none; 1 Ewald real space (PME) and 2 damped shifted force through the rational fits of ewald_fit.cuh
 // (kappa r_c <= 4); 3 and 4 the same through erfcf and expf (any kappa).
-template <int COUL, bool ENER, bool VIR>
+template <int COUL, bool ENER, bool VIR, bool LJ96 = false>
 static __global__ void __launch_bounds__(128, 5) k_pair_f32(PairArgs A) {
   extern __shared__ float4 smem_f4[];
   float4* tab = smem_f4;                                  // ntab * ntab
@@ -285,8 +285,9 @@ static __global__ void __launch_bounds__(128, 5) k_pair_f32(PairArgs A) {
           const float r2i = rinv * rinv;
           const float r6i = r2i * r2i * r2i;
           const float4 cc = tab[ti * A.ntab + tj];
-          const float a12 = cc.y * r6i;
-          float fr = r6i * fmaf(12.f, a12, -6.f * cc.x) * r2i;
+          // 12-6: a = c12 r^-6; 9-6: a = c9 r^-3 (cc.y holds c12 or c9): E = r^-6 (a - c6) - shift
+          const float a12 = cc.y * (LJ96 ? r2i * rinv : r6i);
+          float fr = r6i * fmaf(LJ96 ? 9.f : 12.f, a12, -6.f * cc.x) * r2i;
           if (ENER) ev += ok ? fmaf(r6i, a12 - cc.x, -cc.z) : 0.f;
           if (COUL == 1 || COUL == 2) {
             // E = qq (1/r - kappa g(u)), F = qq (1/r^3 - kappa^3 h(u)), u = (kappa r)^2: FMAs and one division
@@ -394,7 +395,7 @@ __device__ __forceinline__ void ewald_ef(const double* __restrict__ gt, double g
   F = rinv * rinv * rinv + 2 * dG;
 }
 
-template <int COUL, bool ENER, bool VIR, bool CAP = false>
+template <int COUL, bool ENER, bool VIR, bool CAP = false, bool LJ96 = false>
 static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
   extern __shared__ double4 smem_d4[];
   double4* tab = smem_d4;                                   // ntab * ntab
@@ -479,8 +480,14 @@ static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
             fr = cp.z / r * rinv;
             if (ENER) ev += cp.y + cp.z * (rcp - r) - cc.z;
           } else {
-            fr = r6i * (12 * cc.y * r6i - 6 * cc.x) * r2i;
-            if (ENER) ev += r6i * (cc.y * r6i - cc.x) - cc.z;
+            if (LJ96) {   // field.cpp:1658-1661
+              const double r9i = r6i * r2i * rinv;
+              fr = (9 * cc.y * r9i - 6 * cc.x * r6i) * r2i;
+              if (ENER) ev += cc.y * r9i - cc.x * r6i - cc.z;
+            } else {
+              fr = r6i * (12 * cc.y * r6i - 6 * cc.x) * r2i;
+              if (ENER) ev += r6i * (cc.y * r6i - cc.x) - cc.z;
+            }
           }
           if (COUL != 0) {
             const double qq = xi.w * aj.w;

@@ -54,6 +54,7 @@ class ForceField:
     fene_k_r0_eps_sigma: np.ndarray = field(default_factory=lambda: np.zeros((0, 4)))
     lj_shift: bool = False
     model_cutoff: float = 0.0
+    pair_form: str = "lj12-6"        # "lj12-6" | "lj9-6" (class II)
     element: np.ndarray | None = None      # [n] atomic numbers (constraints: hydrogens, rigid waters)
 
     def __post_init__(self):
@@ -122,6 +123,9 @@ class ForceField:
         s.excl_offset, s.excl_list = ptr(self.excl_offset), ptr(self.excl_list)
         s.nfene, s.fene_ij, s.fene_k_r0_eps_sigma = len(self.fene_ij), ptr(self.fene_ij), ptr(self.fene_k_r0_eps_sigma)
         s.lj_shift, s.model_cutoff = int(bool(self.lj_shift)), float(self.model_cutoff)
+        if self.pair_form not in ("lj12-6", "lj9-6"):
+            raise ValueError(f"unknown pair form '{self.pair_form}' (lj12-6, lj9-6)")
+        s.lj_form = 1 if self.pair_form == "lj9-6" else 0
         return s, keep
 
     def arrays(self) -> dict:

@@ -24,7 +24,7 @@
 extern "C" {
 #endif
 
-#define CAPS_GPU_ABI_VERSION 1
+#define CAPS_GPU_ABI_VERSION 2
 
 /* Status codes (negative). The text is in caps_gpu_error(). */
 #define CAPS_GPU_OK 0
@@ -74,6 +74,8 @@ typedef struct {
   const double* fene_k_r0_eps_sigma; /* [4*nfene] */
   int32_t lj_shift;               /* ForceField::lj_shift: LJ shifted to zero at the cut-off, no tail correction */
   double model_cutoff;            /* ForceField::cutoff: > 0 replaces the options' cut-off */
+  int32_t lj_form;                /* ForceField::pair_form (field.cpp:505-506): 0 "lj12-6" 4 eps ((s/r)^12 - (s/r)^6), 1 "lj9-6"
+                                   * (class II) eps (2 (s/r)^9 - 3 (s/r)^6); pair_eps / pair_sigma are the mixed values either way */
 } caps_gpu_ff;
 
 /* caps::EnergyOptions (field.hpp:274-308), the fields the device path takes. */

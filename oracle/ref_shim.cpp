@@ -76,7 +76,7 @@ std::shared_ptr<ForceField> to_ff(const caps_gpu_ff* p) {
   for (int a = 0; a < nt; ++a)
     for (int b = a; b < nt; ++b) ff->pair_override[{a, b}] = PairType{p->pair_eps[a * nt + b], p->pair_sigma[a * nt + b]};
   ff->mixing = "geometric";
-  ff->pair_form = "lj12-6";
+  ff->pair_form = p->lj_form == 1 ? "lj9-6" : "lj12-6";
   ff->charge.assign(p->charge, p->charge + n);
   ff->mass.assign(p->mass, p->mass + n);
   for (int k = 0; k < p->nbonds; ++k) ff->bonds.push_back({p->bond_ij[2 * k], p->bond_ij[2 * k + 1], p->bond_k_r0[2 * k], p->bond_k_r0[2 * k + 1]});
