@@ -60,6 +60,7 @@ class MdOpts(C.Structure):
         ("constraints", C.c_int32), ("new_velocities", C.c_int32), ("seed", C.c_uint64), ("thermo_every", C.c_int32),
         ("frame_every", C.c_int32), ("step_offset", C.c_int64), ("respa", C.c_int32),
         ("is_hydrogen", P), ("is_oxygen", P), ("respa_split", C.c_int32),
+        ("checkpoint_every", C.c_int64), ("checkpoint", C.c_void_p), ("checkpoint_user", C.c_void_p),
     ]
 
 
@@ -97,6 +98,7 @@ class TgFit(C.Structure):
 
 PROGRESS_FN = C.CFUNCTYPE(C.c_int32, C.POINTER(Thermo), C.c_void_p)
 FRAME_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int64, C.c_void_p)
+CHECKPOINT_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int64, C.c_void_p)
 
 DIAG_EXPORTS = ["caps_gpu_diag_set_timing", "caps_gpu_diag_last_step_ms", "caps_gpu_diag_pair_timing", "caps_gpu_diag_step_kernels",
                 "caps_gpu_diag_kernels_run"]
@@ -105,6 +107,8 @@ EXPORTS = [
     "caps_gpu_abi_version", "caps_gpu_device_count", "caps_gpu_create", "caps_gpu_set_options", "caps_gpu_energies",
     "caps_gpu_compute", "caps_gpu_compute_device", "caps_gpu_list_builds", "caps_gpu_run", "caps_gpu_run_batch",
     "caps_gpu_last_steps_per_second", "caps_gpu_destroy", "caps_gpu_error", "caps_gpu_fit_tg",
+    "caps_gpu_request_stop", "caps_gpu_stop_requested", "caps_gpu_traj_open", "caps_gpu_traj_append", "caps_gpu_traj_frame",
+    "caps_gpu_traj_frames", "caps_gpu_traj_close",
 ]
 
 _lib = None
@@ -138,6 +142,15 @@ def load(path: Path | None = None) -> C.CDLL:
     lib.caps_gpu_fit_tg.argtypes = [P, P, C.c_int32, C.c_int32, C.c_double, C.c_double, C.POINTER(TgFit)]
     lib.caps_gpu_error.restype = C.c_char_p
     lib.caps_gpu_error.argtypes = [C.c_void_p]
+    lib.caps_gpu_request_stop.argtypes = [C.c_int32]
+    lib.caps_gpu_stop_requested.restype = C.c_int32
+    lib.caps_gpu_traj_open.restype = C.c_void_p
+    lib.caps_gpu_traj_open.argtypes = [C.c_char_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_double]
+    lib.caps_gpu_traj_append.argtypes = [C.c_void_p, P, P, C.c_int64]
+    lib.caps_gpu_traj_frame.argtypes = [P, P, C.c_int64, C.c_void_p]
+    lib.caps_gpu_traj_frames.restype = C.c_int64
+    lib.caps_gpu_traj_frames.argtypes = [C.c_void_p]
+    lib.caps_gpu_traj_close.argtypes = [C.c_void_p]
     # measurement entry points (include/caps_gpu_diag.h)
     lib.caps_gpu_diag_set_timing.argtypes = [C.c_void_p, C.c_int64]
     lib.caps_gpu_diag_last_step_ms.restype = C.c_double

@@ -13,6 +13,7 @@
 // NVE or Nose-Hoover run starts from the reference's velocities and draws the reference's numbers. Langevin noise, 3N
 // normals a step, comes from a counter-based Philox stream on the device (a pure function of seed, step and atom).
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -1264,6 +1265,72 @@ void Engine::validate_md(const caps_gpu_md_opts& o) const {
   if (o.barostat == 1 && o.thermostat == 0) throw ModelError(CAPS_GPU_EINVAL, "stochastic cell rescaling needs a thermostat");
 }
 
+// A stop asked for from outside (caps_gpu_request_stop): read once per step by the run loops.
+std::atomic<int> g_stop{0};
+
+// Frames and checkpoints leave the device through a ring of snapshot slots. At a recorded step the run's stream copies x
+// (and v, for a checkpoint) into a slot's device buffers, which takes a microsecond, and a copy stream moves them into
+// the slot's pinned host buffers while the next steps run. The callbacks get the slots in step order at the next step
+// that reports or records, once the device has queued that step's work, or when the ring is full, or at the end of the
+// run: the host writes a frame while the device integrates the steps after it.
+struct SnapRing {
+  static constexpr int kSlots = 4;
+  struct Slot {
+    DevBuf<double> dx, dv;
+    double* hx = nullptr;
+    double* hv = nullptr;
+    double cell[12];
+    long long step = 0;
+    bool frame = false;
+    int checkpoints = 0;   // 2: a regular checkpoint and the one a stop takes, both of this step (dynamics.cpp:759-770)
+    cudaEvent_t copied = nullptr;
+  };
+  Slot slot[kSlots];
+  int head = 0, count = 0;
+  cudaStream_t cs = nullptr;
+  cudaEvent_t taken = nullptr;
+  size_t n3 = 0;
+  ~SnapRing() {
+    if (cs) cudaStreamSynchronize(cs);
+    for (auto& q : slot) {
+      if (q.hx) cudaFreeHost(q.hx);
+      if (q.hv) cudaFreeHost(q.hv);
+      if (q.copied) cudaEventDestroy(q.copied);
+    }
+    if (taken) cudaEventDestroy(taken);
+    if (cs) cudaStreamDestroy(cs);
+  }
+  void init(size_t n) {
+    if (cs) return;
+    n3 = n;
+    CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&taken, cudaEventDisableTiming));
+    for (auto& q : slot) CK(cudaEventCreateWithFlags(&q.copied, cudaEventDisableTiming));
+  }
+  // copies of x (and v) of the stream's current step into the next slot; the ring must have room
+  void take(cudaStream_t st, const double* x, const double* v, const double* cell, long long step, bool frame, int checkpoints) {
+    Slot& q = slot[(head + count) % kSlots];
+    q.dx.alloc(n3);
+    if (!q.hx) CK(cudaMallocHost(&q.hx, n3 * sizeof(double)));
+    CK(cudaMemcpyAsync(q.dx.p, x, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    if (checkpoints > 0) {
+      q.dv.alloc(n3);
+      if (!q.hv) CK(cudaMallocHost(&q.hv, n3 * sizeof(double)));
+      CK(cudaMemcpyAsync(q.dv.p, v, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    }
+    CK(cudaEventRecord(taken, st));
+    CK(cudaStreamWaitEvent(cs, taken, 0));
+    CK(cudaMemcpyAsync(q.hx, q.dx.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, cs));
+    if (checkpoints > 0) CK(cudaMemcpyAsync(q.hv, q.dv.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, cs));
+    CK(cudaEventRecord(q.copied, cs));
+    std::memcpy(q.cell, cell, sizeof q.cell);
+    q.step = step;
+    q.frame = frame;
+    q.checkpoints = checkpoints;
+    ++count;
+  }
+};
+
 // One replica's run_dynamics on the device: set-up to step 0 (start), one step (advance), the state back (finish).
 // Engine::run drives one; caps_gpu_run_batch drives several in lock step, their plain steps in one graph.
 struct MdRun {
@@ -1279,6 +1346,8 @@ struct MdRun {
   int thermo_every = 1, baro_every = 1;
   long long kernels = 0, emits = 0, baro_steps = 0;
   int generation = 0;   // bumped whenever this replica's captured step changes (its graphs are dropped)
+  SnapRing snaps;
+  long long stopped_at = -1;   // the step a stop ended the run at
 
   MdRun(Engine& e, caps_gpu_state* state, const caps_gpu_md_opts* md, caps_gpu_progress_fn prog, caps_gpu_frame_fn fr, void* u)
       : E(e), o(*md), st(state), progress(prog), frame(fr), user(u), S(e, *md), n3(size_t(3) * e.n_) {}
@@ -1339,12 +1408,40 @@ struct MdRun {
     row(step, r);
     if (progress && progress(&r, user) != 0) throw ModelError(CAPS_GPU_ECANCEL, "dynamics cancelled");
   }
-  void emit_frame(long long step) {
-    if (!frame || o.frame_every <= 0) return;
-    std::vector<double> hx(n3);
-    CK(cudaMemcpyAsync(hx.data(), S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, E.stream_));
-    CK(cudaStreamSynchronize(E.stream_));
-    frame(hx.data(), E.cell_h_, step + o.step_offset, user);
+  bool frame_due(long long s) const { return frame && o.frame_every > 0 && (s % o.frame_every == 0 || s == o.steps); }
+  bool checkpoint_due(long long s) const { return o.checkpoint && o.checkpoint_every > 0 && s % o.checkpoint_every == 0 && s < o.steps; }
+  // a snapshot of step s for its frame and checkpoints
+  void take(long long s, bool fr, int checkpoints) {
+    if (!fr && checkpoints == 0) return;
+    snaps.init(n3);
+    if (snaps.count == SnapRing::kSlots) deliver_one();
+    snaps.take(E.stream_, S.x.p, S.v.p, E.cell_h_, s, fr, checkpoints);
+  }
+  // the oldest snapshot to its callbacks, once its copy is in host memory; a checkpoint only of a state whose coordinates
+  // and velocities are all finite (dynamics.cpp:758-760)
+  void deliver_one() {
+    SnapRing::Slot& q = snaps.slot[snaps.head];
+    CK(cudaEventSynchronize(q.copied));
+    snaps.head = (snaps.head + 1) % SnapRing::kSlots;
+    --snaps.count;
+    const long long step = q.step + o.step_offset;
+    if (q.frame) frame(q.hx, q.cell, step, user);
+    if (q.checkpoints > 0) {
+      bool finite = true;
+      for (size_t k = 0; k < n3 && finite; ++k) finite = std::isfinite(q.hx[k]) && std::isfinite(q.hv[k]);
+      if (finite)
+        for (int c = 0; c < q.checkpoints; ++c) o.checkpoint(q.hx, q.hv, q.cell, step, o.checkpoint_user);
+    }
+  }
+  // every snapshot of a step before `before`
+  void deliver(long long before) {
+    while (snaps.count > 0 && snaps.slot[snaps.head].step < before) deliver_one();
+  }
+  // a stop after step s, whose regular frame and checkpoint have been taken: the stop's own checkpoint, every callback
+  void stop_here(long long s) {
+    take(s, false, o.checkpoint ? 1 : 0);
+    deliver(s + 1);
+    stopped_at = s;
   }
   bool refill_due(long long s) const { return S.bussi && s - S.draws_first >= S.draws_count; }
   // Bussi draws are made ahead for steps [s, s + chunk). With the barostat on, a chunk ends at the next barostat step:
@@ -1362,11 +1459,12 @@ struct MdRun {
   bool baro_due(long long s) const { return o.barostat && s % baro_every == 0; }
   // a step that reports, records, rescales the cell or refills the thermostat's draws
   bool special(long long s) const {
-    return s % thermo_every == 0 || s == o.steps || (o.frame_every > 0 && s % o.frame_every == 0) || baro_due(s) || refill_due(s);
+    return s % thermo_every == 0 || s == o.steps || frame_due(s) || checkpoint_due(s) || baro_due(s) || refill_due(s);
   }
 
   void start();
-  void advance(long long s);
+  // step s; stop: a stop was asked for before it (and s < steps), so the run ends after it
+  void advance(long long s, bool stop = false);
   void baro_step(long long s);
 };
 
@@ -1462,14 +1560,14 @@ void MdRun::start() {
     CK(cudaStreamSynchronize(stream_));
   }
   emit(0);
-  emit_frame(0);
+  take(0, frame_due(0), 0);
 
   thermo_every = std::max(1, o.thermo_every);
   baro_every = std::max(1, o.barostat_every);
 }
 
 // One step s: the captured plain step, or a special one (thermo row, frame, cell rescaling, new thermostat draws).
-void MdRun::advance(long long s) {
+void MdRun::advance(long long s, bool stop) {
   if (refill_due(s)) {
     CK(cudaStreamSynchronize(E.stream_));
     S.make_draws(s, draw_chunk(s));
@@ -1480,13 +1578,22 @@ void MdRun::advance(long long s) {
     baro_step(s);
   } else {
     kernels += S.launch_step(special(s));
-    if (!special(s)) return;
+    if (!special(s) && !stop) return;
   }
+  // the order of dynamics.cpp:754-770: the thermo row, the frame, the checkpoint, and on a stop one more checkpoint;
+  // the snapshots of earlier steps reach their callbacks before this step's row
+  take(s, frame_due(s), (checkpoint_due(s) ? 1 : 0) + (stop && o.checkpoint ? 1 : 0));
+  deliver(s);
   if (s % thermo_every == 0 || s == o.steps) {
     emit(s);
     ++emits;
   }
-  if (o.frame_every > 0 && (s % o.frame_every == 0 || s == o.steps)) emit_frame(s);
+  if (stop) {
+    deliver(s + 1);
+    stopped_at = s;
+  } else if (s < o.steps && g_stop.load(std::memory_order_relaxed) != 0) {
+    stop_here(s);   // asked for during this step's callbacks: the reference's check comes after them (dynamics.cpp:765)
+  }
 }
 
 // A step with stochastic cell rescaling (Bernetti & Bussi 2020, dynamics.cpp:684-723), isotropic.
@@ -1572,16 +1679,19 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
         if (on) cudaEventRecord(e, st);
       }
     } end_ev{timed, timed ? tev[size_t(2 * (s - 1) + 1)] : nullptr, stream_};
-    R.advance(s);
+    R.advance(s, g_stop.load(std::memory_order_relaxed) != 0 && s < o.steps);
+    if (R.stopped_at >= 0) break;
   }
   CK(cudaEventRecord(ev1, stream_));
   CK(cudaEventSynchronize(ev1));
+  R.deliver(o.steps + 1);
   kernels_run_ = R.kernels + R.emits + R.baro_steps * S.graph_kernels[1];
   float ms = 0;
   CK(cudaEventElapsedTime(&ms, ev0, ev1));
-  if (timed && o.steps > 0) {
+  const long long done = R.stopped_at >= 0 ? R.stopped_at : o.steps;   // steps run
+  if (timed && done > 0) {
     double sum = 0;
-    for (long long k = 0; k < o.steps; ++k) {
+    for (long long k = 0; k < done; ++k) {
       float t = 0;
       CK(cudaEventElapsedTime(&t, tev[size_t(2 * k)], tev[size_t(2 * k + 1)]));
       sum += t;
@@ -1589,12 +1699,12 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
     for (auto& e : tev) cudaEventDestroy(e);
     ms = float(sum);
   }
-  last_step_ms_ = o.steps > 0 ? double(ms) / double(o.steps) : 0.0;
+  last_step_ms_ = done > 0 ? double(ms) / double(done) : 0.0;
   const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
   cudaEventDestroy(ev0);
   cudaEventDestroy(ev1);
   R.sync_scalars();
-  last_sps_ = o.steps > 0 && ms > 0 ? double(o.steps) / (ms * 1e-3) : 0.0;
+  last_sps_ = done > 0 && ms > 0 ? double(done) / (ms * 1e-3) : 0.0;
   // state back to the caller
   CK(cudaMemcpyAsync(st->x, S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
   if (st->v) CK(cudaMemcpyAsync(st->v, S.v.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
@@ -1602,15 +1712,16 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
   std::memcpy(st->cell, cell_h_, sizeof cell_h_);
   if (report) {
     char b[512];
-    const double nsday = wall > 0 ? double(o.steps) * o.dt * 1e-6 / wall * 86400 : 0.0;
+    const double nsday = wall > 0 ? double(done) * o.dt * 1e-6 / wall * 86400 : 0.0;
     const double setup = std::chrono::duration<double>(w0 - t_enter).count();
     std::snprintf(b, sizeof b,
                   "%lld steps of %.2f fs in %.3f s (device %.3f s, set-up %.3f s) · %.2f ns/day · %d constraints · %.0f degrees of freedom · %s"
                   " · tuned: %d entries per work item, PME line blocks %d/%d/%d",
-                  (long long)o.steps, o.dt, wall, ms * 1e-3, setup, nsday, S.ncons, S.ndof, mixed_ ? "mixed FP32/fixed-point" : "FP64", batch_,
+                  (long long)done, o.dt, wall, ms * 1e-3, setup, nsday, S.ncons, S.ndof, mixed_ ? "mixed FP32/fixed-point" : "FP64", batch_,
                   lines_x_, lines_y_, lines_z_);
     *report = b;
   }
+  if (R.stopped_at >= 0) throw ModelError(CAPS_GPU_ESTOPPED, "stopped at step " + std::to_string(R.stopped_at + o.step_offset) + " (a stop was asked for)");
 }
 
 // Replicas in lock step (caps_gpu_run_batch). A step on which no replica reports, records, rescales or refills is one
@@ -1668,12 +1779,24 @@ void run_batch(const std::vector<Engine*>& es, caps_gpu_state* const* states, co
   join_to_batch();
   CK(cudaEventRecord(res.t0, res.bs));
   const auto w0 = std::chrono::steady_clock::now();
+  long long stopped_at = -1;
   for (long long s = 1; s <= steps; ++s) {
-    bool plain = true;
+    const bool stop = g_stop.load(std::memory_order_relaxed) != 0 && s < steps;
+    bool plain = !stop;
     for (size_t r = 0; r < R; ++r) plain = plain && !runs[r]->special(s);
     if (!plain) {
       if (!on_replicas) fork_to_replicas(), on_replicas = true;
-      for (size_t r = 0; r < R; ++r) runs[r]->advance(s);
+      bool any = false;
+      for (size_t r = 0; r < R; ++r) {
+        runs[r]->advance(s, stop);
+        any = any || runs[r]->stopped_at >= 0;
+      }
+      if (any) {   // a stop seen by one replica (asked for in its callbacks) ends every replica at this step
+        for (size_t r = 0; r < R; ++r)
+          if (runs[r]->stopped_at < 0) runs[r]->stop_here(s);
+        stopped_at = s;
+        break;
+      }
       continue;
     }
     if (on_replicas) join_to_batch(), on_replicas = false;
@@ -1718,18 +1841,27 @@ void run_batch(const std::vector<Engine*>& es, caps_gpu_state* const* states, co
   CK(cudaEventElapsedTime(&ms, res.t0, res.t1));
   const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
   (void)wall;
+  for (size_t r = 0; r < R; ++r) runs[r]->deliver(steps + 1);
+  const long long done = stopped_at >= 0 ? stopped_at : steps;
   for (size_t r = 0; r < R; ++r) {
     MdRun& M = *runs[r];
     Engine& E = M.E;
     M.sync_scalars();
-    E.last_step_ms_ = steps > 0 ? double(ms) / double(steps) : 0.0;
-    E.last_sps_ = steps > 0 && ms > 0 ? double(steps) / (ms * 1e-3) : 0.0;
+    E.last_step_ms_ = done > 0 ? double(ms) / double(done) : 0.0;
+    E.last_sps_ = done > 0 && ms > 0 ? double(done) / (ms * 1e-3) : 0.0;
     E.kernels_run_ = M.kernels + M.emits + (r == 0 ? batch_kernels : 0);
     CK(cudaMemcpyAsync(M.st->x, M.S.x.p, M.n3 * sizeof(double), cudaMemcpyDeviceToHost, E.stream_));
     if (M.st->v) CK(cudaMemcpyAsync(M.st->v, M.S.v.p, M.n3 * sizeof(double), cudaMemcpyDeviceToHost, E.stream_));
     CK(cudaStreamSynchronize(E.stream_));
     std::memcpy(M.st->cell, E.cell_h_, sizeof E.cell_h_);
   }
+  if (stopped_at >= 0)
+    throw ModelError(CAPS_GPU_ESTOPPED, "stopped at step " + std::to_string(stopped_at + mds[0]->step_offset) + " (a stop was asked for)");
 }
 
 }  // namespace capsb
+
+extern "C" {
+void caps_gpu_request_stop(int32_t on) { capsb::g_stop.store(on != 0 ? 1 : 0); }
+int32_t caps_gpu_stop_requested(void) { return capsb::g_stop.load() != 0 ? 1 : 0; }
+}

@@ -28,6 +28,27 @@ class DeviceError(RuntimeError):
     """A CUDA call failed, or there is no device (the engine has no CPU fallback)."""
 
 
+class DynamicsInterrupted(RuntimeError):
+    """caps::DynamicsInterrupted (core/include/caps/dynamics.hpp:173-176): a stop was asked for (request_stop) and the run
+    ended at `step` (with step_offset) after its checkpoint. `state` holds the run's result at that step (x, v, cell,
+    thermo rows), as the reference leaves it in the System."""
+
+    def __init__(self, text: str, state: dict | None = None):
+        super().__init__(text)
+        words = text.split()
+        self.step = int(words[3]) if len(words) > 3 and words[3].lstrip("-").isdigit() else -1
+        self.state = state
+
+
+def request_stop(on: bool = True):
+    """caps::request_stop (core/include/caps/live.hpp:29): process-wide; every run checks it at each step."""
+    _abi.load().caps_gpu_request_stop(int(bool(on)))
+
+
+def stop_requested() -> bool:
+    return bool(_abi.load().caps_gpu_stop_requested())
+
+
 def _raise(code: int, text: str):
     if code == -3 or code == -4:
         raise FieldError(text)
@@ -35,6 +56,8 @@ def _raise(code: int, text: str):
         raise DynamicsCancelled(text)
     if code == -2 or code == -6:
         raise DeviceError(text)
+    if code == -7:
+        raise DynamicsInterrupted(text)
     raise ValueError(text)
 
 
@@ -89,6 +112,7 @@ class DynamicsOptions:
     seed: int = 1
     thermo_every: int = 100
     frame_every: int = 0
+    checkpoint_every: int = 0          # steps between checkpoints (0: none), with a checkpoint callback
     step_offset: int = 0
     respa: int = 1
     respa_split: str = "bonded"        # "bonded": bonded terms inner (the reference's split); "pme": PME outer
@@ -105,6 +129,7 @@ class DynamicsOptions:
         m.new_velocities = int(bool(self.new_velocities))
         m.seed, m.thermo_every, m.frame_every, m.step_offset, m.respa = self.seed, self.thermo_every, self.frame_every, self.step_offset, self.respa
         m.respa_split = {"bonded": 0, "pme": 1}[self.respa_split]
+        m.checkpoint_every = int(self.checkpoint_every)
         if ff.element is not None:
             h = np.ascontiguousarray((ff.element == 1).astype(np.int8))
             o = np.ascontiguousarray((ff.element == 8).astype(np.int8))
@@ -204,8 +229,13 @@ class Evaluator:
     def list_builds(self) -> int:
         return int(self.lib.caps_gpu_list_builds(self.h))
 
-    def run(self, x, cell, opts: DynamicsOptions, v=None, progress=None, frame=None) -> dict:
-        """run_dynamics on this evaluator's force field: returns {x, v, cell, thermo, report, steps_per_second}."""
+    def run(self, x, cell, opts: DynamicsOptions, v=None, progress=None, frame=None, checkpoint=None) -> dict:
+        """run_dynamics on this evaluator's force field: returns {x, v, cell, thermo, report, steps_per_second}.
+
+        progress(row) -> False cancels (DynamicsCancelled). frame(x, cell, step) receives each recorded frame, or frame is
+        a TrajectoryWriter, whose native writer then takes the frames with no Python call per frame. checkpoint(x, v,
+        cell, step) receives each checkpoint (opts.checkpoint_every). A stop asked for with request_stop ends the run
+        with DynamicsInterrupted, whose `state` is this method's result at the stopped step."""
         x = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1)).copy()
         vv = np.zeros_like(x) if v is None else np.ascontiguousarray(np.asarray(v, dtype=np.float64).reshape(-1)).copy()
         c = cell_array(cell).copy()
@@ -222,32 +252,51 @@ class Evaluator:
                 return 1
             return 0
 
-        def _frame(xp, cp, step, user):
-            if frame is not None:
-                n = self.ff.natoms
-                frame(np.ctypeslib.as_array(xp, shape=(3 * n,)).copy().reshape(-1, 3),
-                      np.ctypeslib.as_array(cp, shape=(12,)).copy(), int(step))
-
-        pf, ff_ = _abi.PROGRESS_FN(_prog), _abi.FRAME_FN(_frame)
+        n = self.ff.natoms
+        fuser = None
+        if frame is None:
+            ff_ = _abi.FRAME_FN()
+        elif hasattr(frame, "native_frame_fn"):
+            ff_, fuser = frame.native_frame_fn()
+        else:
+            def _frame(xp, cp, step, user):
+                frame(np.ctypeslib.as_array(xp, shape=(3 * n,)).copy().reshape(-1, 3), np.ctypeslib.as_array(cp, shape=(12,)).copy(), int(step))
+            ff_ = _abi.FRAME_FN(_frame)
+        if checkpoint is not None:
+            def _ckpt(xp, vp, cp, step, user):
+                checkpoint(np.ctypeslib.as_array(xp, shape=(3 * n,)).copy().reshape(-1, 3), np.ctypeslib.as_array(vp, shape=(3 * n,)).copy().reshape(-1, 3),
+                           np.ctypeslib.as_array(cp, shape=(12,)).copy(), int(step))
+            cf = _abi.CHECKPOINT_FN(_ckpt)
+            keep.append(cf)
+            m.checkpoint = C.cast(cf, C.c_void_p)
+        pf = _abi.PROGRESS_FN(_prog)
         buf = C.create_string_buffer(4096)
-        rc = self.lib.caps_gpu_run(self.h, C.byref(st), C.byref(m), pf, ff_, None, buf, 4096)
-        self._check(rc)
-        return {"x": x.reshape(-1, 3), "v": vv.reshape(-1, 3), "cell": c, "thermo": rows, "report": buf.value.decode(),
-                "steps_per_second": float(self.lib.caps_gpu_last_steps_per_second(self.h))}
+        rc = self.lib.caps_gpu_run(self.h, C.byref(st), C.byref(m), pf, ff_, fuser, buf, 4096)
+        out = {"x": x.reshape(-1, 3), "v": vv.reshape(-1, 3), "cell": c, "thermo": rows, "report": buf.value.decode(),
+               "steps_per_second": float(self.lib.caps_gpu_last_steps_per_second(self.h))}
+        try:
+            self._check(rc)
+        except DynamicsInterrupted as e:
+            e.state = out
+            raise
+        return out
 
 
-def run_dynamics(ff: ForceField, x, cell, opts: DynamicsOptions, v=None, progress=None, frame=None) -> dict:
+def run_dynamics(ff: ForceField, x, cell, opts: DynamicsOptions, v=None, progress=None, frame=None, checkpoint=None) -> dict:
     """caps::run_dynamics on the device (dynamics.hpp:180)."""
     ev = Evaluator(ff, opts.energy)
     try:
-        return ev.run(x, cell, opts, v=v, progress=progress, frame=frame)
+        return ev.run(x, cell, opts, v=v, progress=progress, frame=frame, checkpoint=checkpoint)
     finally:
         ev.close()
 
 
-def run_batch(evaluators: list, xs: list, cells: list, opts: list, vs: list | None = None) -> list[dict]:
+def run_batch(evaluators: list, xs: list, cells: list, opts: list, vs: list | None = None, frames: list | None = None,
+              checkpoints: list | None = None) -> list[dict]:
     """Independent replicas in lock step (caps_gpu_run_batch): one Evaluator, structure and DynamicsOptions per replica,
-    all with the same number of steps. Returns one {x, v, cell, thermo} per replica."""
+    all with the same number of steps. Returns one {x, v, cell, thermo} per replica. frames / checkpoints: per replica a
+    callback (x, cell, step) / (x, v, cell, step) or None; a frame entry may be a TrajectoryWriter. A stop asked for
+    with request_stop raises DynamicsInterrupted, whose `state` is the list of results."""
     R = len(evaluators)
     if not (len(xs) == len(cells) == len(opts) == R) or R == 0:
         raise ValueError("one structure, cell and options per evaluator")
@@ -264,16 +313,50 @@ def run_batch(evaluators: list, xs: list, cells: list, opts: list, vs: list | No
         ms.append(opts[r].to_struct(ev.ff, keep))
 
     def _prog(row, user):
-        rows[int(user or 0)].append(row.contents.as_dict())
+        rows[replica_of[user]].append(row.contents.as_dict())
         return 0
 
-    pf, ff_ = _abi.PROGRESS_FN(_prog), _abi.FRAME_FN(lambda *a: None)
+    frames = list(frames) if frames is not None else [None] * R
+    checkpoints = list(checkpoints) if checkpoints is not None else [None] * R
+    if len(frames) != R or len(checkpoints) != R:
+        raise ValueError("one frame and one checkpoint entry per replica")
+    users = (C.c_void_p * R)(*[C.c_void_p(r) for r in range(R)])
+    natoms = [ev.ff.natoms for ev in evaluators]
+    if all(f is None for f in frames):
+        ff_ = _abi.FRAME_FN()
+    elif all(hasattr(f, "native_frame_fn") for f in frames):
+        ff_ = frames[0].native_frame_fn()[0]
+        for r, f in enumerate(frames):
+            users[r] = f.native_frame_fn()[1]
+    else:
+        def _frame(xp, cp, step, user):
+            r = int(user or 0)
+            if frames[r] is not None:
+                n = natoms[r]
+                frames[r](np.ctypeslib.as_array(xp, shape=(3 * n,)).copy().reshape(-1, 3), np.ctypeslib.as_array(cp, shape=(12,)).copy(), int(step))
+        ff_ = _abi.FRAME_FN(_frame)
+    replica_of = {users[r]: r for r in range(R)}   # progress and frame callbacks get the same user pointer
+    for r, cb in enumerate(checkpoints):
+        if cb is None:
+            continue
+
+        def _ckpt(xp, vp, cp, step, user, cb=cb, n=natoms[r]):
+            cb(np.ctypeslib.as_array(xp, shape=(3 * n,)).copy().reshape(-1, 3), np.ctypeslib.as_array(vp, shape=(3 * n,)).copy().reshape(-1, 3),
+               np.ctypeslib.as_array(cp, shape=(12,)).copy(), int(step))
+        cf = _abi.CHECKPOINT_FN(_ckpt)
+        keep.append(cf)
+        ms[r].checkpoint = C.cast(cf, C.c_void_p)
+    pf = _abi.PROGRESS_FN(_prog)
     eng = (C.c_void_p * R)(*[ev.h for ev in evaluators])
     sp = (C.c_void_p * R)(*[C.cast(C.pointer(s_), C.c_void_p) for s_ in st])
     mp = (C.c_void_p * R)(*[C.cast(C.pointer(m_), C.c_void_p) for m_ in ms])
-    users = (C.c_void_p * R)(*[C.c_void_p(r) for r in range(R)])
     lib = evaluators[0].lib
     rc = lib.caps_gpu_run_batch(eng, sp, mp, R, pf, ff_, users)
-    evaluators[0]._check(rc)
-    return [{"x": xa[r].reshape(-1, 3), "v": va[r].reshape(-1, 3), "cell": ca[r], "thermo": rows[r]} for r in range(R)]
+    out = [{"x": xa[r].reshape(-1, 3), "v": va[r].reshape(-1, 3), "cell": ca[r], "thermo": rows[r]} for r in range(R)]
+    try:
+        evaluators[0]._check(rc)
+    except DynamicsInterrupted as e:
+        e.state = out
+        raise
+    return out
 

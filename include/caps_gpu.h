@@ -12,6 +12,8 @@
  *   caps_gpu_list_builds Evaluator::list_builds()                                       core/include/caps/field.hpp:341
  *   caps_gpu_run        run_dynamics(System&, const DynamicsOptions&, DynamicsReport*)   core/include/caps/dynamics.hpp:180
  *   caps_gpu_destroy    Evaluator::~Evaluator()                                          core/include/caps/field.hpp:333
+ *   caps_gpu_traj_*     write_trajectory(const Trajectory&, path, dt_fs)                 core/include/caps/io.hpp:142, io_traj.cpp:47
+ *   caps_gpu_request_stop request_stop(bool)                                            core/include/caps/live.hpp:29
  *   caps_gpu_error      FieldError text / caps_last_error()                              capi/include/caps_c.h:63
  *
  * Units are the reference's (LAMMPS "real"): Å, fs, kcal/mol, e, g/mol, K, atm.
@@ -24,7 +26,7 @@
 extern "C" {
 #endif
 
-#define CAPS_GPU_ABI_VERSION 2
+#define CAPS_GPU_ABI_VERSION 3
 
 /* Status codes (negative). The text is in caps_gpu_error(). */
 #define CAPS_GPU_OK 0
@@ -34,6 +36,8 @@ extern "C" {
 #define CAPS_GPU_ECONSTRAINT (-4) /* SHAKE/RATTLE did not converge or a bond turned past 90 degrees */
 #define CAPS_GPU_ECANCEL (-5)     /* the progress callback asked to stop (DynamicsCancelled) */
 #define CAPS_GPU_ENODEV (-6)      /* no CUDA device: there is no CPU fallback */
+#define CAPS_GPU_ESTOPPED (-7)    /* a stop was asked for (caps_gpu_request_stop): DynamicsInterrupted; the state is the
+                                     stopped step's */
 
 /* The force field as the device path consumes it: the subset of caps::ForceField (core/include/caps/field.hpp:154-249)
  * that the MD hot path reads, flattened to arrays. Pair coefficients are given per type pair after mixing
@@ -102,6 +106,10 @@ typedef struct {
   double tail_energy, tail_virial;
 } caps_gpu_terms;
 
+/* Called with each checkpoint: positions (3N, unwrapped), velocities (3N, Å/fs), cell[12] and step (with step_offset).
+ * DynamicsOptions::checkpoint (core/include/caps/dynamics.hpp:143-146). */
+typedef void (*caps_gpu_checkpoint_fn)(const double* x, const double* v, const double* cell, int64_t step, void* user);
+
 /* caps::DynamicsOptions (dynamics.hpp:60-154), the fields the device step takes. */
 typedef struct {
   double dt;                /* fs */
@@ -126,6 +134,10 @@ typedef struct {
   const int8_t* is_oxygen;   /* [natoms] element == 8, for rigid waters; NULL: none */
   int32_t respa_split;      /* with respa > 1: 0 bonded forces every dt/respa (the reference's split, dynamics.cpp:113);
                                1 PME every dt, everything else every dt/respa (a split the reference does not have) */
+  int64_t checkpoint_every; /* 0 none; at steps s % checkpoint_every == 0, s < steps, whose x and v are finite
+                               (dynamics.cpp:758-763) */
+  caps_gpu_checkpoint_fn checkpoint;   /* NULL none */
+  void* checkpoint_user;
 } caps_gpu_md_opts;
 
 /* caps::ThermoRow (dynamics.hpp:28-43), the fields the device step fills. */
@@ -139,7 +151,12 @@ typedef struct {
 
 /* Called with each thermo row; non-zero cancels the run (DynamicsCancelled). */
 typedef int32_t (*caps_gpu_progress_fn)(const caps_gpu_thermo* row, void* user);
-/* Called with each recorded frame: positions (3N, unwrapped), cell[12] (origin, a, b, c) and step. */
+/* Called with each recorded frame: positions (3N, unwrapped), cell[12] (origin, a, b, c) and step.
+ * Frames and checkpoints leave the device asynchronously: a recorded step's state is copied aside on the device, moved to
+ * pinned host memory on a copy stream while the next steps run, and handed to the callbacks on the calling thread at the
+ * next step that reports or records, or at the end of the run. The order of the calls is the reference's: the thermo row
+ * of a step, then its frame, then its checkpoint; every frame and checkpoint before the next row. The pointers are valid
+ * during the call only. */
 typedef void (*caps_gpu_frame_fn)(const double* x, const double* cell, int64_t step, void* user);
 
 /* The state a run works on, in place: positions (3N unwrapped), velocities (3N, Å/fs; may be NULL to draw them),
@@ -183,6 +200,12 @@ int32_t caps_gpu_run(caps_gpu_engine* e, caps_gpu_state* state, const caps_gpu_m
  * caps_gpu_last_steps_per_second is the batch's. */
 int32_t caps_gpu_run_batch(caps_gpu_engine* const* engines, caps_gpu_state* const* states, const caps_gpu_md_opts* const* md, int32_t count,
                            caps_gpu_progress_fn progress, caps_gpu_frame_fn frame, void* const* user);
+/* A stop asked for from outside (caps::request_stop, core/include/caps/live.hpp:27-29): process-wide. A run checks it at
+ * every step; at the first step s < steps that sees it, it takes a checkpoint of step s (when it has a checkpoint
+ * callback and the state is finite), writes that state back and returns CAPS_GPU_ESTOPPED with the text
+ * "stopped at step N (a stop was asked for)" (DynamicsInterrupted, dynamics.hpp:173-176). A batch stops every replica. */
+void caps_gpu_request_stop(int32_t on);
+int32_t caps_gpu_stop_requested(void);
 /* The last run's throughput: steps per second over the step loop (first force excluded, as dynamics.cpp:601,776). */
 double caps_gpu_last_steps_per_second(const caps_gpu_engine* e);
 void caps_gpu_destroy(caps_gpu_engine* e);
@@ -206,6 +229,27 @@ typedef struct {
  * thirds). Host code, no device needed; the same points give the reference's Tg and bootstrap error. A fit that cannot
  * be made returns 0 with out->ok = 0 and the reason in out->note. */
 int32_t caps_gpu_fit_tg(const double* T, const double* y, int32_t n, int32_t method, double glassy_max, double rubbery_min, caps_gpu_tg_fit* out);
+
+/* Trajectory writers, frame by frame (write_trajectory, core/src/io_traj.cpp:47; write_dcd, core/src/io_binary.cpp:415;
+ * write_lammps_dump, core/src/io_lammps.cpp:612): the file the reference writes for the same frames, byte for byte, but
+ * written as the frames arrive instead of from a Trajectory held in memory. The format is the path's extension:
+ * .lammpstrj / .dump (LAMMPS text dump: id mol type xu yu zu, the cell turned into LAMMPS's form), .dcd (LAMMPS's
+ * CHARMM-style DCD with a unit-cell record per frame; the frame count and step range in the header are completed by
+ * caps_gpu_traj_close; the unit-cell flag is the first frame's), .trr (GROMACS, single precision, nm).
+ * ids, mols: [natoms] LAMMPS atom and molecule ids (NULL: 1..N and 1); types: [natoms] 1-based types (NULL: 1);
+ * title: the DCD's second title line (NULL: empty); dt_fs: the time step, for DCD's time unit and TRR's times.
+ * NULL on error with the text in caps_gpu_error(NULL). Host code: no device needed. */
+typedef struct caps_gpu_traj caps_gpu_traj;
+caps_gpu_traj* caps_gpu_traj_open(const char* path, int32_t natoms, const int64_t* ids, const int64_t* mols, const int32_t* types,
+                                  const char* title, double dt_fs);
+/* One frame: x (3N, Å), cell[12] (origin, a, b, c; a zero cell is no cell), step. */
+int32_t caps_gpu_traj_append(caps_gpu_traj* t, const double* x, const double* cell, int64_t step);
+/* A caps_gpu_frame_fn that appends to the writer passed as user: caps_gpu_run(..., caps_gpu_traj_frame, writer, ...)
+ * streams a run's frames to the file with no other code in between. A write error is kept and returned by close. */
+void caps_gpu_traj_frame(const double* x, const double* cell, int64_t step, void* user);
+int64_t caps_gpu_traj_frames(const caps_gpu_traj* t);
+/* Completes the header, closes the file and frees the writer; the first error met while writing, if any. */
+int32_t caps_gpu_traj_close(caps_gpu_traj* t);
 
 /* Kinetic energy and kinetic tensor of n atoms, computed without allocating any device memory. No counterpart in the
  * reference: it is for callers that may not call cudaMalloc, such as a host whose memory manager owns all device memory

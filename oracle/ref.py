@@ -39,7 +39,11 @@ def lib() -> C.CDLL:
         L.ref_compute.argtypes = [C.POINTER(_abi.FF), C.POINTER(_abi.Opts), C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(_abi.Terms), C.c_int]
         L.ref_time_compute.argtypes = [C.POINTER(_abi.FF), C.POINTER(_abi.Opts), C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]
         L.ref_run.argtypes = [C.POINTER(_abi.FF), C.POINTER(_abi.Opts), C.POINTER(_abi.State), C.POINTER(_abi.MdOpts), C.c_void_p, C.c_int,
-                              C.POINTER(_abi.Thermo), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+                              C.POINTER(_abi.Thermo), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                              _abi.FRAME_FN, C.c_void_p]
+        L.ref_request_stop.argtypes = [C.c_int]
+        L.ref_write_trajectory.argtypes = [C.c_char_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_int, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_double]
         L.ref_ewald_beta.restype = C.c_double
         L.ref_ewald_beta.argtypes = [C.c_double, C.c_double]
         L.ref_pme_grid.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_void_p]
@@ -86,8 +90,11 @@ def time_compute(ff: ForceField, opts: EnergyOptions, x, cell, reps: int, thread
     return sec.value
 
 
-def run(ff: ForceField, x, cell, opts: DynamicsOptions, v=None, threads: int = 1, max_rows: int = 100000) -> dict:
-    """caps::run_dynamics in the reference core; returns {x, v, cell, thermo, seconds, ns_per_day}."""
+def run(ff: ForceField, x, cell, opts: DynamicsOptions, v=None, threads: int = 1, max_rows: int = 100000, frames: bool = False,
+        checkpoints: bool = False, events: list | None = None) -> dict:
+    """caps::run_dynamics in the reference core; returns {x, v, cell, thermo, seconds, ns_per_day}, plus "frames" [(x,
+    cell, step)] and "checkpoints" [(x, v, cell, step)] when asked for, and "interrupted" (the DynamicsInterrupted text)
+    when a stop ended the run. events, when given, receives ("row" | "frame" | "checkpoint", step) in call order."""
     s, keep = ff.to_struct()
     o = opts.energy.to_struct()
     xx = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1)).copy()
@@ -98,11 +105,63 @@ def run(ff: ForceField, x, cell, opts: DynamicsOptions, v=None, threads: int = 1
     el = np.ascontiguousarray(ff.element if ff.element is not None else np.full(ff.natoms, 6), dtype=np.int32)
     rows = (_abi.Thermo * max_rows)()
     nrows, sec, nsd = C.c_int(), C.c_double(), C.c_double()
-    if lib().ref_run(C.byref(s), C.byref(o), C.byref(st), C.byref(m), _vp(el), threads, rows, max_rows, C.byref(nrows), C.byref(sec),
-                     C.byref(nsd)) != 0:
+    n = ff.natoms
+    fr, ck = [], []
+
+    def _frame(xp, cp, step, user):
+        fr.append((np.ctypeslib.as_array(xp, shape=(3 * n,)).copy().reshape(-1, 3), np.ctypeslib.as_array(cp, shape=(12,)).copy(), int(step)))
+        if events is not None:
+            events.append(("frame", int(step)))
+
+    def _ckpt(xp, vp, cp, step, user):
+        ck.append((np.ctypeslib.as_array(xp, shape=(3 * n,)).copy().reshape(-1, 3), np.ctypeslib.as_array(vp, shape=(3 * n,)).copy().reshape(-1, 3),
+                   np.ctypeslib.as_array(cp, shape=(12,)).copy(), int(step)))
+        if events is not None:
+            events.append(("checkpoint", int(step)))
+
+    ff_ = _abi.FRAME_FN(_frame) if frames else _abi.FRAME_FN()
+    cf = _abi.CHECKPOINT_FN(_ckpt)
+    if checkpoints:
+        m.checkpoint = C.cast(cf, C.c_void_p)
+    rc = lib().ref_run(C.byref(s), C.byref(o), C.byref(st), C.byref(m), _vp(el), threads, rows, max_rows, C.byref(nrows), C.byref(sec),
+                       C.byref(nsd), ff_, None)
+    if rc < 0:
         raise RuntimeError(lib().ref_error().decode())
     th = [rows[k].as_dict() for k in range(min(nrows.value, max_rows))]
-    return {"x": xx.reshape(-1, 3), "v": vv.reshape(-1, 3), "cell": c, "thermo": th, "seconds": sec.value, "ns_per_day": nsd.value}
+    if events is not None:
+        # the rows arrive through a table, not a callback: put them back in call order, each before its step's frame
+        merged, k = [], 0
+        for kind, step in events:
+            while k < len(th) and th[k]["step"] <= step:
+                merged.append(("row", th[k]["step"]))
+                k += 1
+            merged.append((kind, step))
+        merged += [("row", r["step"]) for r in th[k:]]
+        events[:] = merged
+    out = {"x": xx.reshape(-1, 3), "v": vv.reshape(-1, 3), "cell": c, "thermo": th, "seconds": sec.value, "ns_per_day": nsd.value,
+           "frames": fr, "checkpoints": ck}
+    if rc == 1:
+        out["interrupted"] = lib().ref_error().decode()
+    return out
+
+
+def request_stop(on: bool = True):
+    """caps::request_stop in the reference core (its own flag, apart from the device engine's)."""
+    lib().ref_request_stop(int(bool(on)))
+
+
+def write_trajectory(path, frames, ids, mols, types, title: str = "", dt_fs: float = 1.0):
+    """caps::write_trajectory on the frames [(x, cell, step)] of atoms with the given ids, mols and types."""
+    n = len(ids)
+    x = np.ascontiguousarray(np.array([np.asarray(f[0], dtype=np.float64).reshape(-1) for f in frames]).reshape(-1)) if frames else np.zeros(0)
+    c = np.ascontiguousarray(np.array([cell_array(f[1]) for f in frames]).reshape(-1)) if frames else np.zeros(0)
+    st = np.ascontiguousarray(np.array([int(f[2]) for f in frames], dtype=np.int64))
+    ia = np.ascontiguousarray(np.asarray(ids, dtype=np.int64))
+    ma = np.ascontiguousarray(np.asarray(mols, dtype=np.int64))
+    ta = np.ascontiguousarray(np.asarray(types, dtype=np.int32))
+    if lib().ref_write_trajectory(str(path).encode(), n, _vp(ia), _vp(ma), _vp(ta), title.encode(), len(frames), _vp(x), _vp(c), _vp(st),
+                                  float(dt_fs)) != 0:
+        raise RuntimeError(lib().ref_error().decode())
 
 
 def fit_tg(T, y, method: int = 0, glassy_max: float = 0.0, rubbery_min: float = 0.0) -> dict:

@@ -25,6 +25,8 @@
 #include "caps/dynamics.hpp"
 #include "caps/field.hpp"
 #include "caps/grow.hpp"
+#include "caps/io.hpp"
+#include "caps/live.hpp"
 #include "caps/kremer_grest.hpp"
 #include "caps/kspace.hpp"
 #include "caps/mechanics.hpp"
@@ -321,8 +323,10 @@ int ref_time_compute(const caps_gpu_ff* p, const caps_gpu_opts* o, const double*
 
 // run_dynamics on a System rebuilt from the arrays. element: [natoms] atomic numbers (for SHAKE's hydrogens and rigid
 // waters). rows: up to max_rows thermo rows out. seconds and ns_per_day from the reference's own report.
+// frame (may be NULL): each recorded frame with `user`; md->checkpoint (may be NULL): each checkpoint. A stop asked for
+// with ref_request_stop ends the run with DynamicsInterrupted: the state is written back and 1 returned.
 int ref_run(const caps_gpu_ff* p, const caps_gpu_opts* eo, caps_gpu_state* st, const caps_gpu_md_opts* md, const int32_t* element, int threads,
-            caps_gpu_thermo* rows, int max_rows, int* nrows, double* seconds, double* ns_per_day) {
+            caps_gpu_thermo* rows, int max_rows, int* nrows, double* seconds, double* ns_per_day, caps_gpu_frame_fn frame, void* user) {
   try {
     auto ff = to_ff(p);
     System s;
@@ -360,7 +364,20 @@ int ref_run(const caps_gpu_ff* p, const caps_gpu_opts* eo, caps_gpu_state* st, c
     o.new_velocities = md->new_velocities != 0;
     o.seed = md->seed;
     o.thermo_every = md->thermo_every;
-    o.frame_every = 0;
+    o.frame_every = frame ? md->frame_every : 0;
+    if (frame)
+      o.frame = [&](const std::vector<double>& x, const Cell& c, int64_t step) {
+        double cc[12];
+        from_cell(c, cc);
+        frame(x.data(), cc, step, user);
+      };
+    o.checkpoint_every = md->checkpoint_every;
+    if (md->checkpoint)
+      o.checkpoint = [&](const std::vector<double>& x, const std::vector<double>& v, const Cell& c, int64_t step) {
+        double cc[12];
+        from_cell(c, cc);
+        md->checkpoint(x.data(), v.data(), cc, step, md->checkpoint_user);
+      };
     o.step_offset = md->step_offset;
     o.respa = md->respa > 1 ? md->respa : 1;
     o.energy = to_eo(eo, threads);
@@ -386,7 +403,13 @@ int ref_run(const caps_gpu_ff* p, const caps_gpu_opts* eo, caps_gpu_state* st, c
       return true;
     };
     DynamicsReport rep;
-    run_dynamics(s, o, &rep);
+    int rc = 0;
+    try {
+      run_dynamics(s, o, &rep);
+    } catch (const DynamicsInterrupted& di) {
+      g_err = di.what();
+      rc = 1;
+    }
     *nrows = k;
     *seconds = rep.seconds;
     *ns_per_day = rep.ns_per_day;
@@ -396,6 +419,41 @@ int ref_run(const caps_gpu_ff* p, const caps_gpu_opts* eo, caps_gpu_state* st, c
         if (st->v) st->v[3 * i + c] = s.velocities[size_t(i)][c];
       }
     from_cell(s.cell, st->cell);
+    return rc;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+void ref_request_stop(int on) { request_stop(on != 0); }
+
+// caps::write_trajectory (io_traj.cpp:47) on a Trajectory of nf frames: x [nf][3n], cells [nf][12], steps [nf]; the
+// topology's atoms carry ids, mols and types, its title the DCD's second title line.
+int ref_write_trajectory(const char* path, int n, const int64_t* ids, const int64_t* mols, const int32_t* types, const char* title, int nf,
+                         const double* x, const double* cells, const int64_t* steps, double dt_fs) {
+  try {
+    Trajectory t;
+    t.topology.atoms.resize(size_t(n));
+    for (int i = 0; i < n; ++i) {
+      Atom& a = t.topology.atoms[size_t(i)];
+      a.id = ids[i];
+      a.mol = mols[i];
+      a.type = types[i];
+      a.element = 6;
+      for (int k = 0; k < 3; ++k) a.pos[k] = x[3 * size_t(i) + size_t(k)];
+    }
+    t.topology.title = title ? title : "";
+    for (int f = 0; f < nf; ++f) {
+      std::vector<Vec3> pos(static_cast<size_t>(n));
+      for (int i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) pos[size_t(i)][k] = x[(size_t(f) * size_t(n) + size_t(i)) * 3 + size_t(k)];
+      t.positions.push_back(std::move(pos));
+      t.cells.push_back(to_cell(cells + 12 * size_t(f)));
+      t.timesteps.push_back(steps[f]);
+    }
+    if (nf > 0) t.topology.cell = t.cells.front();
+    write_trajectory(t, path, dt_fs);
     return 0;
   } catch (const std::exception& e) {
     g_err = e.what();

@@ -53,3 +53,29 @@ def rel_max(f, ref) -> float:
     """Largest component error relative to the RMS force."""
     f, ref = np.asarray(f).reshape(-1), np.asarray(ref).reshape(-1)
     return float(np.max(np.abs(f - ref)) / np.sqrt(np.mean(ref ** 2)))
+
+
+# Trajectory writer cases: seeded frames in cells of every shape the writers treat apart (LAMMPS's own form, a cell
+# needing the rotation, a left-handed one, an orthogonal one, none).
+TRAJ_CELLS = {
+    "lammps_form": [1.0, 2.0, 3.0, 20.0, 0.0, 0.0, 1.5, 18.0, 0.0, -2.0, 3.0, 21.0],
+    "rotated": [0.5, -0.2, 0.1, 20.0, 0.3, -0.4, 1.5, 18.0, 0.7, -2.0, 3.0, 21.0],
+    "orthogonal": [0.0, 0.0, 0.0, 20.0, 0.0, 0.0, 0.0, 18.0, 0.0, 0.0, 0.0, 21.0],
+    "left_handed": [0.0, 0.0, 0.0, 20.0, 0.0, 0.0, 0.0, 18.0, 0.0, 0.0, 0.0, -21.0],
+    "no_cell": [0.0] * 12,
+}
+TRAJ_FORMATS = ["lammpstrj", "dcd", "trr"]
+
+
+def trajectory_case(cell_name: str, natoms: int = 37, nframes: int = 5, seed: int = 11):
+    """(ids, mols, types, frames [(x, cell, step)]) of one writer case; the same numbers on every machine."""
+    rng = np.random.default_rng(seed)
+    ids = np.arange(1, natoms + 1, dtype=np.int64) * 2 + 5
+    mols = np.arange(natoms, dtype=np.int64) // 4 + 1
+    types = (np.arange(natoms, dtype=np.int32) % 5) + 1
+    cell0 = np.asarray(TRAJ_CELLS[cell_name], dtype=np.float64)
+    frames = []
+    for k in range(nframes):
+        x = rng.normal(0.0, 6.0, size=(natoms, 3)) + 10.0
+        frames.append((x, cell0 * (1.0 + 0.003 * k), 1000 + 250 * k))
+    return ids, mols, types, frames

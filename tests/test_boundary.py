@@ -36,7 +36,7 @@ def test_library_exports_every_declared_symbol(lib):
     for name in declared_functions():
         assert hasattr(lib, name), name
     assert set(_abi.EXPORTS) | set(_abi.DIAG_EXPORTS) <= set(declared_functions())
-    assert lib.caps_gpu_abi_version() == 2
+    assert lib.caps_gpu_abi_version() == 3
 
 
 def test_no_torch_in_the_boundary():
@@ -54,7 +54,7 @@ def _c_layout():
 int main(void) {
   S(caps_gpu_ff) S(caps_gpu_opts) S(caps_gpu_terms) S(caps_gpu_md_opts) S(caps_gpu_thermo) S(caps_gpu_state)
   O(caps_gpu_ff, lj14) O(caps_gpu_ff, excl_offset) O(caps_gpu_ff, model_cutoff) O(caps_gpu_ff, lj_form) O(caps_gpu_ff, fene_k_r0_eps_sigma)
-  O(caps_gpu_opts, precision) O(caps_gpu_opts, parts) O(caps_gpu_md_opts, seed) O(caps_gpu_md_opts, is_oxygen)
+  O(caps_gpu_opts, precision) O(caps_gpu_opts, parts) O(caps_gpu_md_opts, seed) O(caps_gpu_md_opts, is_oxygen) O(caps_gpu_md_opts, checkpoint_every) O(caps_gpu_md_opts, checkpoint_user)
   O(caps_gpu_thermo, p) O(caps_gpu_thermo, terms) O(caps_gpu_terms, tail_virial)
   return 0;
 }
