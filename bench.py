@@ -104,6 +104,8 @@ def options(precision: str, steps: int, seed: int, thermostat: str = "nose-hoove
                            thermo_every=thermo_every or max(steps, 1), energy=eo)
 
 
+E2E_CALLS = 3
+
 # An earlier measurement on B200s of the same kind (HBM copy GB/s, max SM clock), used when no measured-peaks file is present
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "sm_max_mhz": 1965.0}
 
@@ -243,11 +245,15 @@ def main():
     sps = 1000.0 / ms_step
     nsd = sps * 1.0 * 86400e-6            # dt = 1 fs
     value = nsd * world                    # whole job: the replicas' simulated time per day
-    # --- e2e: the C ABI call with host buffers, wall clock around it ---
-    t0 = time.perf_counter()
-    eo_run = ev.run(x2, cell, options("mixed", args.steps, seed), v=v2)
-    e2e_wall = time.perf_counter() - t0
-    print(f"[bench] e2e run: {eo_run['report']}", file=sys.stderr, flush=True)
+    # --- e2e: the C ABI call with host buffers, wall clock around it; the best of E2E_CALLS calls, since the host is
+    # shared and a call's set-up and launches can stall behind other processes ---
+    walls = []
+    for _ in range(E2E_CALLS):
+        t0 = time.perf_counter()
+        eo_run = ev.run(x2, cell, options("mixed", args.steps, seed), v=v2)
+        walls.append(time.perf_counter() - t0)
+        print(f"[bench] e2e run: {eo_run['report']}", file=sys.stderr, flush=True)
+    e2e_wall = min(walls)
     e2e_nsd = args.steps * 1.0 * 1e-6 / e2e_wall * 86400 * world
     h2d = (2 * 3 * n * 8 + 12 * 8) / args.steps
     d2h = (2 * 3 * n * 8 + 12 * 8 + 2 * 232) / args.steps
@@ -347,6 +353,7 @@ def main():
             "nve_drift_kT_per_ns_per_atom": drift_kt_ns_atom,
             "batched_replicas": batch,
             "e2e": {"value": e2e_nsd, "unit": "ns/day", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "calls_s": [round(w, 4) for w in walls], "taken": f"best of {E2E_CALLS} calls",
                     "call": "caps_gpu_run (C ABI) on host buffers, wall clock"},
             "roofline": {"bound": "fp32", "kernel": "k_pair_f32 (LJ + Ewald real space)", "achieved": achieved,
                          "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,

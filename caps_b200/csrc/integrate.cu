@@ -1577,7 +1577,8 @@ void MdRun::advance(long long s, bool stop) {
   if (baro_due(s)) {
     baro_step(s);
   } else {
-    kernels += S.launch_step(special(s));
+    // energies and virial only for a thermo row: a step that only records, refills or stops runs the plain graph
+    kernels += S.launch_step(s % thermo_every == 0 || s == o.steps);
     if (!special(s) && !stop) return;
   }
   // the order of dynamics.cpp:754-770: the thermo row, the frame, the checkpoint, and on a stop one more checkpoint;

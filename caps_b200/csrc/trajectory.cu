@@ -7,12 +7,14 @@
 // Host code, no device needed.
 #include <algorithm>
 #include <cerrno>
+#include <charconv>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "caps_gpu.h"
@@ -91,6 +93,8 @@ struct caps_gpu_traj {
   std::string err;
   std::vector<float> fbuf;
   std::string text;
+  std::vector<std::string> chunks;
+  std::vector<unsigned char> bebuf;
 
   void fail(const std::string& what) {
     if (err.empty()) err = what;
@@ -200,12 +204,55 @@ struct caps_gpu_traj {
     }
     text += b;
     text += "ITEM: ATOMS id mol type xu yu zu\n";
-    for (int32_t i = 0; i < n; ++i) {
-      const V3 r = fr.to_frame(V3{{x[3 * size_t(i)], x[3 * size_t(i) + 1], x[3 * size_t(i) + 2]}});
-      const int len = std::snprintf(b, sizeof b, "%lld %lld %d %.5f %.5f %.5f\n", ids[size_t(i)], mols[size_t(i)], types[size_t(i)], r[0], r[1], r[2]);
-      text.append(b, size_t(len));
-    }
     put(text.data(), text.size());
+    // the atom lines ("%lld %lld %d %.5f %.5f %.5f\n") by std::to_chars, whose fixed form is printf's to the digit, in
+    // chunks formatted on parallel threads for large frames
+    const int nt = n >= 16384 ? int(std::min<unsigned>(8, std::max(1u, std::thread::hardware_concurrency()))) : 1;
+    chunks.resize(size_t(nt));
+    auto lines = [&](int t) {
+      std::string& out = chunks[size_t(t)];
+      out.clear();
+      const int32_t i0 = int32_t(int64_t(n) * t / nt), i1 = int32_t(int64_t(n) * (t + 1) / nt);
+      out.reserve(size_t(i1 - i0) * 48);
+      char line[160];
+      for (int32_t i = i0; i < i1; ++i) {
+        const V3 r = fr.to_frame(V3{{x[3 * size_t(i)], x[3 * size_t(i) + 1], x[3 * size_t(i) + 2]}});
+        char* p = line;
+        char* const end = line + sizeof line;
+        p = std::to_chars(p, p + 24, ids[size_t(i)]).ptr;   // an integer takes at most 20 characters
+        *p++ = ' ';
+        p = std::to_chars(p, p + 24, mols[size_t(i)]).ptr;
+        *p++ = ' ';
+        p = std::to_chars(p, p + 24, types[size_t(i)]).ptr;
+        bool fits = true;
+        for (int d = 0; d < 3 && fits; ++d) {
+          *p++ = ' ';
+          const auto res = std::to_chars(p, end - 1, r[d], std::chars_format::fixed, 5);
+          fits = res.ec == std::errc();
+          p = res.ptr;
+        }
+        if (fits) {
+          *p++ = '\n';
+          out.append(line, size_t(p - line));
+        } else {
+          // more digits than the line holds (|x| > 1e100): the reference's own 256-byte line, cut where it cuts it
+          char buf[256];
+          std::snprintf(buf, sizeof buf, "%lld %lld %d %.5f %.5f %.5f\n", ids[size_t(i)], mols[size_t(i)], types[size_t(i)], r[0], r[1], r[2]);
+          out.append(buf);
+        }
+      }
+    };
+    std::vector<std::thread> pool;
+    pool.reserve(size_t(nt));
+    int started = 1;
+    try {
+      for (; started < nt; ++started) pool.emplace_back(lines, started);
+    } catch (const std::exception&) {   // no thread to be had: the rest on this one
+    }
+    for (int t = started; t < nt; ++t) lines(t);
+    lines(0);
+    for (auto& th : pool) th.join();
+    for (const auto& c : chunks) put(c.data(), c.size());
   }
 
   // io_traj.cpp:81-107
@@ -225,8 +272,17 @@ struct caps_gpu_traj {
     if (box)
       for (const V3* v : {&c.a, &c.b, &c.c})
         for (int d = 0; d < 3; ++d) f32be(float((*v)[d] / 10.0));
-    for (int32_t i = 0; i < n; ++i)
-      for (int d = 0; d < 3; ++d) f32be(float(x[3 * size_t(i) + size_t(d)] / 10.0));
+    // the positions, big-endian, in one write
+    bebuf.resize(size_t(n) * 12);
+    unsigned char* q = bebuf.data();
+    for (size_t k = 0; k < size_t(n) * 3; ++k, q += 4) {
+      const float fv = float(x[k] / 10.0);
+      uint32_t u;
+      std::memcpy(&u, &fv, 4);
+      q[0] = static_cast<unsigned char>(u >> 24), q[1] = static_cast<unsigned char>(u >> 16), q[2] = static_cast<unsigned char>(u >> 8),
+      q[3] = static_cast<unsigned char>(u);
+    }
+    put(bebuf.data(), bebuf.size());
   }
 
   void append(const double* x, const double* cellp, int64_t step) {

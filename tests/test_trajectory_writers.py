@@ -113,3 +113,23 @@ def test_write_trajectory_helper(tmp_path):
     assert text[4] == "ITEM: BOX BOUNDS xy xz yz pp pp pp"
     assert text[8] == "ITEM: ATOMS id mol type xu yu zu"
     assert text[9].split()[:3] == ["7", "1", "1"]
+
+
+def test_large_dump_with_edge_values_matches_reference(tmp_path):
+    """A frame large enough for the parallel formatter, with the values where fixed-point formatting is delicate:
+    exact ties at the fifth decimal (k / 2^17), signed zeros and tiny negatives that print as -0.00000, and numbers too
+    long for the formatter's line (printf's own digits)."""
+    ref = _ref()
+    n = 20011
+    rng = np.random.default_rng(9)
+    x = rng.normal(0.0, 30.0, size=(n, 3))
+    x.reshape(-1)[: 3 * 4000] = np.arange(-6000, 6000) / 131072.0
+    x[4000:4010] = [[-0.0, 0.0, -1e-7], [-4.9999e-6, 5e-6, 2.5e-6], [1e15, -1e15, 123456789.123456], [1e120, -3e150, 7.0],
+                    [1.0 / 64, -1.0 / 64, 3.0 / 128], [0.000015, -0.000025, 0.000035], [99999.999995, -99999.999995, 0.5e-5],
+                    [1e-300, -1e-300, 5e-324], [2.0 ** 40 + 0.5, -(2.0 ** 40) - 0.5, 0.1], [0.3, 0.7, 0.9]]
+    ids = np.arange(1, n + 1)
+    mols = np.arange(n) // 7 + 1
+    types = np.arange(n) % 4 + 1
+    frames = [(x, TRAJ_CELLS["rotated"], 0), (x, TRAJ_CELLS["lammps_form"], 10)]
+    ref.write_trajectory(tmp_path / "r.lammpstrj", frames, ids, mols, types)
+    assert (tmp_path / "r.lammpstrj").read_bytes() == _mine(tmp_path / "m.lammpstrj", ids, mols, types, frames)
