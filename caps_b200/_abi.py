@@ -108,7 +108,8 @@ EXPORTS = [
     "caps_gpu_compute", "caps_gpu_compute_device", "caps_gpu_list_builds", "caps_gpu_run", "caps_gpu_run_batch",
     "caps_gpu_last_steps_per_second", "caps_gpu_destroy", "caps_gpu_error", "caps_gpu_fit_tg",
     "caps_gpu_request_stop", "caps_gpu_stop_requested", "caps_gpu_traj_open", "caps_gpu_traj_append", "caps_gpu_traj_frame",
-    "caps_gpu_traj_frames", "caps_gpu_traj_close",
+    "caps_gpu_traj_frames", "caps_gpu_traj_close", "caps_gpu_reload", "caps_gpu_freeze_pairs", "caps_gpu_unfreeze", "caps_gpu_pairs",
+    "caps_gpu_threads",
 ]
 
 _lib = None
@@ -142,6 +143,12 @@ def load(path: Path | None = None) -> C.CDLL:
     lib.caps_gpu_fit_tg.argtypes = [P, P, C.c_int32, C.c_int32, C.c_double, C.c_double, C.POINTER(TgFit)]
     lib.caps_gpu_error.restype = C.c_char_p
     lib.caps_gpu_error.argtypes = [C.c_void_p]
+    lib.caps_gpu_reload.argtypes = [C.c_void_p, C.POINTER(FF)]
+    lib.caps_gpu_freeze_pairs.argtypes = [C.c_void_p, P, P]
+    lib.caps_gpu_unfreeze.argtypes = [C.c_void_p]
+    lib.caps_gpu_pairs.restype = C.c_int64
+    lib.caps_gpu_pairs.argtypes = [C.c_void_p]
+    lib.caps_gpu_threads.argtypes = [C.c_void_p]
     lib.caps_gpu_request_stop.argtypes = [C.c_int32]
     lib.caps_gpu_stop_requested.restype = C.c_int32
     lib.caps_gpu_traj_open.restype = C.c_void_p

@@ -387,6 +387,8 @@ void Engine::setup_options() {
     cell_set_ = false;
     set_cell(c);
   }
+  // the mixed path's fixed-point spread grid, also after a switch of precision on an unchanged grid
+  if (pme_ && mixed_ && pk_[0] > 0) d_gridq_.alloc(size_t(pk_[0]) * pk_[1] * pk_[2]);
   CK(cudaStreamSynchronize(stream_));
 }
 
@@ -406,6 +408,9 @@ void Engine::set_cell(const double* cell) {
   const double* a = cell + 3;
   const double* b = cell + 6;
   const double* c = cell + 9;
+  // a frozen pair set keeps its list through a deformation: the images and offsets follow the new cell (the pair
+  // kernel and the pack take them from the cell matrix), as the reference's rescale_images (field.cpp:1316-1317)
+  const bool keep_list = frozen_;
   double bc[3], ca[3], ab[3];
   cross3(b, c, bc);
   cross3(c, a, ca);
@@ -427,8 +432,8 @@ void Engine::set_cell(const double* cell) {
   g.batch = batch_;
   if (g.ru / g.nu > 60 || g.rv / g.nv > 60 || g.rq > 60)
     throw ModelError(CAPS_GPU_EFIELD, "the cell is too small for the cut-off: more than 60 periodic images in range");
-  const bool geom_changed = g.nu != geom_.nu || g.nv != geom_.nv;
-  geom_ = g;
+  const bool geom_changed = !keep_list && (g.nu != geom_.nu || g.nv != geom_.nv);
+  if (!keep_list) geom_ = g;
   if (geom_changed) {
     d_col_count_.alloc(size_t(g.ncol));
     d_col_count_.zero(stream_);   // the scan clears it after every build
@@ -436,8 +441,10 @@ void Engine::set_cell(const double* cell) {
     d_col_start_.alloc(size_t(g.ncol) + 1);
     d_col_sc_.alloc(size_t(g.ncol) + 1);
   }
-  ensure_list_capacity();
-  list_valid_ = false;
+  if (!keep_list) {
+    ensure_list_capacity();
+    list_valid_ = false;
+  }
   green_valid_ = false;
   if (pme_) {
     int k[3];
@@ -475,15 +482,18 @@ void Engine::ensure_list_capacity() {
     d_cl_real_.alloc(size_t(8) * nsc_cap_);
     d_perm_.alloc(ns);
     d_xq_.alloc(ns);
-    if (!mixed_) d_xqd_.alloc(ns);
     d_tslot_.alloc(ns);
     d_Fs_.alloc(3 * ns);
-    if (!mixed_) d_Fsd_.alloc(3 * ns);
     const size_t ecap = std::max(ent, d_ent_.n);
     d_ent_.alloc(ecap);
     d_ent_shift_.alloc(ecap);
     d_work_.alloc(ecap / 4 + size_t(nsc_cap_) * 2 + 64);
     d_masks_.alloc(size_t(8) * 96 * nsc_cap_ + 8 * 256);   // 8 rows per (j cluster, image) with exclusions, per super-cluster
+  }
+  if (!mixed_) {   // the FP64 path's packed positions and slot sums, also after a switch of precision
+    const size_t ns = size_t(nsc_cap_) * kScAtoms;
+    d_xqd_.alloc(ns);
+    d_Fsd_.alloc(3 * ns);
   }
   d_col_.alloc(size_t(n_));
   d_frac_.alloc(size_t(3) * n_);
@@ -736,6 +746,43 @@ int32_t caps_gpu_compute_device(caps_gpu_engine* e, const double* d_x, const dou
   if (!e || !d_x || !cell || !d_f) return CAPS_GPU_EINVAL;
   return guard(e, [&] { e->e->compute_dev(d_x, cell, d_f, out); });
 }
+
+int32_t caps_gpu_reload(caps_gpu_engine* e, const caps_gpu_ff* ff) {
+  if (!e || !ff) return CAPS_GPU_EINVAL;
+  return guard(e, [&] {
+    Engine& old = *e->e;
+    if (ff->natoms != old.n_) throw capsb::ModelError(CAPS_GPU_EINVAL, "reload: the force field has another number of atoms");
+    caps_gpu_opts o = old.opt_;
+    if (old.frozen()) old.unfreeze();   // reload ends a frozen list (field.cpp:432), and restores the precision it switched
+    o = old.opt_;
+    auto fresh = std::make_unique<Engine>(ff, &o);
+    fresh->energies(old.energies_on());
+    fresh->set_timing(old.timing_flush());
+    e->e = std::move(fresh);
+  });
+}
+
+int32_t caps_gpu_freeze_pairs(caps_gpu_engine* e, const double* x, const double* cell) {
+  if (!e || !x || !cell) return CAPS_GPU_EINVAL;
+  return guard(e, [&] { e->e->freeze_pairs(x, cell); });
+}
+
+int32_t caps_gpu_unfreeze(caps_gpu_engine* e) {
+  if (!e) return CAPS_GPU_EINVAL;
+  return guard(e, [&] { e->e->unfreeze(); });
+}
+
+int64_t caps_gpu_pairs(caps_gpu_engine* e) {
+  if (!e) return -1;
+  try {
+    return e->e->pairs();
+  } catch (const std::exception& x) {
+    e->err = x.what();
+    return -1;
+  }
+}
+
+int32_t caps_gpu_threads(const caps_gpu_engine* e) { return e ? e->e->sms() : 0; }
 
 int32_t caps_gpu_list_builds(const caps_gpu_engine* e) {
   if (!e) return 0;

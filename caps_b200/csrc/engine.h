@@ -105,6 +105,16 @@ class Engine {
   void compute_host(const double* x, const double* cell, double* f, caps_gpu_terms* out);
   void compute_dev(const double* d_x, const double* cell, double* d_f, caps_gpu_terms* out);
   int list_builds();   // list builds so far (counted on the device)
+  // Evaluator::freeze_pairs / unfreeze (field.hpp:341-347): later evaluations take exactly the pairs inside the cut-off
+  // at (x, cell), on the FP64 path, and never rebuild the list
+  void freeze_pairs(const double* x, const double* cell);
+  void unfreeze();
+  bool frozen() const { return frozen_; }
+  // Evaluator::pairs() (field.hpp:348): atom pairs in the FP64 pair list (within r_c + skin at its last build)
+  long long pairs();
+  bool energies_on() const { return energies_; }
+  int64_t timing_flush() const { return timing_flush_; }
+  int sms() const { return dev_sms_; }
   void run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progress_fn progress, caps_gpu_frame_fn frame, void* user, std::string* report);
   void validate_md(const caps_gpu_md_opts& o) const;   // the dynamics options the device path takes (throws otherwise)
   double last_steps_per_second() const { return last_sps_; }
@@ -211,6 +221,12 @@ class Engine {
   DevBuf<unsigned long long> d_masks_;
   DevBuf<int4> d_work_;
   bool list_valid_ = false;
+  // a frozen pair set: per entry and i cluster, the 64 atom pairs that interact; the precision to restore at unfreeze
+  bool frozen_ = false;
+  int frozen_saved_precision_ = -1;
+  DevBuf<unsigned long long> d_frozen_;
+  long long frozen_pairs_ = 0;   // pairs() as the reference reports it on its cluster path: the list of the last freeze
+  long long count_pairs();
   int nsc_cap_ = 0;
 
   // packed positions, forces

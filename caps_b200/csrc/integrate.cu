@@ -1253,6 +1253,7 @@ struct Stepper {
 
 void Engine::validate_md(const caps_gpu_md_opts& o) const {
   if (n_ < 2) throw ModelError(CAPS_GPU_EFIELD, "dynamics needs at least two atoms");
+  if (frozen_) throw ModelError(CAPS_GPU_EINVAL, "the pair list is frozen (freeze_pairs): unfreeze it before dynamics");
   if (o.dt <= 0 || o.dt > 50) throw ModelError(CAPS_GPU_EINVAL, "time step must be in (0, 50] fs");
   if (o.steps < 0) throw ModelError(CAPS_GPU_EINVAL, "the number of steps must be 0 or more");
   if (o.respa < 0 || o.respa > 16) throw ModelError(CAPS_GPU_EINVAL, "r-RESPA inner steps must be 1 … 16");

@@ -126,6 +126,7 @@ PairArgs Engine::pair_args() {
   A.ent = d_ent_.p;
   A.ent_shift = d_ent_shift_.p;
   A.masks = d_masks_.p;
+  A.frozen = d_frozen_.p;
   A.counters = d_counters_.p;
   A.tslot = d_tslot_.p;
   A.xq = d_xq_.p;
@@ -206,19 +207,30 @@ void Engine::pair_forces(bool ener, bool vir) {
 #undef PAIR32L
   } else {
     const size_t smem = sizeof(double4) * (size_t(ntab) * ntab + 4 * 64) + sizeof(double) * 2 * size_t(coul ? gnodes_ : 0) + sizeof(int) * 4 * 64;
-#define PAIR64L(C, E, V, CAP, L)                                                                                     \
+#define PAIR64LF(C, E, V, CAP, L, F)                                                                                 \
   do {                                                                                                               \
-    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_pair_f64<C, E, V, CAP, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
+    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_pair_f64<C, E, V, CAP, L, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
     int per_sm = 0;                                                                                                  \
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_f64<C, E, V, CAP, L>, 128, smem));              \
-    k_pair_f64<C, E, V, CAP, L><<<dev_sms_ * std::max(1, per_sm), 128, smem, stream_>>>(A);                          \
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_f64<C, E, V, CAP, L, F>, 128, smem));           \
+    k_pair_f64<C, E, V, CAP, L, F><<<dev_sms_ * std::max(1, per_sm), 128, smem, stream_>>>(A);                       \
   } while (0)
+#define PAIR64L(C, E, V, CAP, L) PAIR64LF(C, E, V, CAP, L, false)
 #define PAIR64(C, E, V, CAP)                                                                                         \
   do {                                                                                                               \
     if (lj96_) PAIR64L(C, E, V, CAP, true);                                                                          \
     else PAIR64L(C, E, V, CAP, false);                                                                               \
   } while (0)
-    if (opt_.force_cap > 0) {
+#define PAIR64FROZEN(C)                                                                                              \
+  do {                                                                                                               \
+    if (lj96_) PAIR64LF(C, true, true, false, true, true);                                                           \
+    else PAIR64LF(C, true, true, false, false, true);                                                                \
+  } while (0)
+    if (frozen_) {
+      // a frozen pair set: energies and virial always on (finite-difference second derivatives read them)
+      if (coul == 1) PAIR64FROZEN(1);
+      else if (coul == 2) PAIR64FROZEN(2);
+      else PAIR64FROZEN(0);
+    } else if (opt_.force_cap > 0) {
       // push-off: energies and virial always on (a rare path, kept to one instantiation per Coulomb form)
       if (coul == 1) PAIR64(1, true, true, true);
       else if (coul == 2) PAIR64(2, true, true, true);
@@ -226,10 +238,63 @@ void Engine::pair_forces(bool ener, bool vir) {
     } else if (coul == 1) { if (ener) { if (vir) PAIR64(1, true, true, false); else PAIR64(1, true, false, false); } else { if (vir) PAIR64(1, false, true, false); else PAIR64(1, false, false, false); } }
     else if (coul == 2) { if (ener) { if (vir) PAIR64(2, true, true, false); else PAIR64(2, true, false, false); } else { if (vir) PAIR64(2, false, true, false); else PAIR64(2, false, false, false); } }
     else { if (ener) { if (vir) PAIR64(0, true, true, false); else PAIR64(0, true, false, false); } else { if (vir) PAIR64(0, false, true, false); else PAIR64(0, false, false, false); } }
+#undef PAIR64FROZEN
 #undef PAIR64
 #undef PAIR64L
+#undef PAIR64LF
   }
   CK(cudaGetLastError());
+}
+
+long long Engine::count_pairs() {
+  if (!list_valid_ || mixed_) return 0;
+  DevBuf<unsigned long long> cnt;
+  cnt.alloc(1);
+  cnt.zero(stream_);
+  k_count_pairs<<<dev_sms_ * 4, 128, 0, stream_>>>(pair_args(), d_ent_.p, d_perm_.p, d_x0_.p, d_ioff_.p, (rc_ + skin_) * (rc_ + skin_), cnt.p);
+  CK(cudaGetLastError());
+  unsigned long long v = 0;
+  CK(cudaMemcpyAsync(&v, cnt.p, sizeof v, cudaMemcpyDeviceToHost, stream_));
+  CK(cudaStreamSynchronize(stream_));
+  return static_cast<long long>(v);
+}
+
+// The reference's pairs() is the size of its FP64 atom-pair list; on its cluster (mixed) path that list is only built by
+// freeze_pairs, so a mixed evaluator reports the list of its last freeze, or none.
+long long Engine::pairs() {
+  if (frozen_) return frozen_pairs_;
+  return mixed_ ? frozen_pairs_ : count_pairs();
+}
+
+void Engine::freeze_pairs(const double* x, const double* cell) {
+  if (opt_.force_cap > 0) throw ModelError(CAPS_GPU_EINVAL, "freeze_pairs: the device path freezes no list under a force cap");
+  unfreeze();
+  if (mixed_) {   // a frozen list runs on the reference's FP64 atom-pair path (field.cpp:845), so on this engine's FP64 path
+    frozen_saved_precision_ = opt_.precision;
+    opt_.precision = 1;
+    setup_options();
+  }
+  // the list built at (x, cell), then the pairs inside r_c there
+  list_valid_ = false;
+  std::vector<double> f(3 * size_t(n_));
+  caps_gpu_terms t{};
+  compute_host(x, cell, f.data(), &t);
+  frozen_pairs_ = count_pairs();
+  d_frozen_.alloc(size_t(8) * d_ent_.n);
+  k_freeze<<<dev_sms_ * 4, 128, 0, stream_>>>(pair_args(), d_ent_.p, d_frozen_.p);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(stream_));
+  frozen_ = true;
+}
+
+void Engine::unfreeze() {
+  if (!frozen_) return;
+  frozen_ = false;
+  if (frozen_saved_precision_ >= 0) {
+    opt_.precision = frozen_saved_precision_;
+    frozen_saved_precision_ = -1;
+  }
+  setup_options();   // the cell may have changed while frozen: geometry, capacity and list from scratch
 }
 
 // One force evaluation on device positions d_x (AoS, 3 n): accumulators cleared, list checked / rebuilt, every term,
@@ -258,14 +323,16 @@ void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild, 
   const bool pme = (pm & 4) != 0 && pme_;
   if (pme) fork(1, [&] { pme_forces(d_x, ener, vir); });
   if (nonb) {
-    if (!list_valid_) {
+    if (frozen_) {
+      // a frozen pair set: no displacement check, build or prune; the pack and the pair kernel run on the frozen list
+    } else if (!list_valid_) {
       k_set_flag<<<1, 1, 0, stream_>>>(d_counters_.p, kCntRebuild, 1);
       list_valid_ = true;
     } else if (check_rebuild) {
       const double b = std::min(0.8, skin_);   // the prune margin (see prune())
       k_check_step<<<blocks_for(size_t(n_), 256), 256, 0, stream_>>>(n_, d_x, d_x0_.p, 0.25 * skin_ * skin_, d_xp_.p, 0.25 * b * b, d_counters_.p);
     }
-    launch_build(d_x);
+    if (!frozen_) launch_build(d_x);
     const size_t ns = size_t(nsc_cap_) * kScAtoms;
     if (mixed_)
       k_pack_f32<<<blocks_for(ns, 256), 256, 0, stream_>>>(int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_sc_org_.p, d_q_.p, d_type_.p, nt_,
@@ -273,7 +340,7 @@ void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild, 
     else
       k_pack_f64<<<blocks_for(ns, 256), 256, 0, stream_>>>(int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_q_.p, d_type_.p, nt_, d_xqd_.p, d_tslot_.p,
                                                            d_counters_.p, d_x0_.p, d_Fsd_.p);
-    prune(d_x);
+    if (!frozen_) prune(d_x);
     pair_forces(ener, vir);
   }
   join(0);

@@ -92,6 +92,7 @@ struct PairArgs {
   const uint4* ent;
   const float4* ent_shift;
   const unsigned long long* masks;
+  const unsigned long long* frozen;   // a frozen pair set: 8 per entry (one per i cluster), the pairs that interact
   const int* counters;
   const int* tslot;
   const float4* xq;      // FP32 path
@@ -395,7 +396,18 @@ __device__ __forceinline__ void ewald_ef(const double* __restrict__ gt, double g
   F = rinv * rinv * rinv + 2 * dG;
 }
 
-template <int COUL, bool ENER, bool VIR, bool CAP = false, bool LJ96 = false>
+// erfc(x) and exp(-x^2) by Abramowitz & Stegun 7.1.26, the reference's erfc_exp (field.cpp:585-590): the closed form a
+// frozen pair takes beyond the cut-off, where the Ewald table ends.
+__device__ __forceinline__ double erfc_exp_as(double x, double& ex2) {
+  const double P = 0.3275911, A1 = 0.254829592, A2 = -0.284496736, A3 = 1.421413741, A4 = -1.453152027, A5 = 1.061405429;
+  ex2 = exp(-x * x);
+  const double t = 1.0 / (1.0 + P * x);
+  return t * (A1 + t * (A2 + t * (A3 + t * (A4 + t * A5)))) * ex2;
+}
+
+// FROZEN: the pairs are those of the frozen set (A.frozen), whatever their distance now (field.cpp:1700); one beyond
+// the cut-off takes the closed-form Coulomb term (field.cpp:1759-1768).
+template <int COUL, bool ENER, bool VIR, bool CAP = false, bool LJ96 = false, bool FROZEN = false>
 static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
   extern __shared__ double4 smem_d4[];
   double4* tab = smem_d4;                                   // ntab * ntab
@@ -454,7 +466,7 @@ static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
 #pragma unroll 2
       for (int c = 0; c < 8; ++c) {
         if (!((imask >> c) & 1u)) continue;
-        const unsigned long long mm = en.z ? A.masks[8 * size_t(en.z - 1) + c] : ~0ull;
+        const unsigned long long mm = FROZEN ? A.frozen[8 * size_t(e) + c] : en.z ? A.masks[8 * size_t(en.z - 1) + c] : ~0ull;
         const double4 xi = xi_s[8 * c + i8];
         const int ti = ti_s[8 * c + i8];
         const bool oki = (ireal >> c) & 1u;
@@ -468,7 +480,7 @@ static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
           const int bit = 8 * i8 + jq + 4 * jj;
           const double dx = aj.x - xs, dy = aj.y - ys, dz = aj.z - zs;
           const double r2 = dx * dx + dy * dy + dz * dz;
-          const bool ok = oki && ((mm >> bit) & 1ull) && (r2 < A.rc2);
+          const bool ok = oki && ((mm >> bit) & 1ull) && (FROZEN || r2 < A.rc2);
           if (!ok) continue;
           const double r2i = 1 / r2, r6i = r2i * r2i * r2i, rinv = sqrt(r2i);
           const double4 cc = tab[ti * A.ntab + tj];
@@ -489,7 +501,19 @@ static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
               if (ENER) ev += r6i * (cc.y * r6i - cc.x) - cc.z;
             }
           }
-          if (COUL != 0) {
+          if (COUL != 0 && FROZEN && !(r2 < A.rc2)) {
+            const double qq = xi.w * aj.w;
+            const double r = sqrt(r2);
+            double ex2;
+            const double er = erfc_exp_as(A.beta * r, ex2);   // beta: the Ewald or DSF coefficient; kc = 2 beta / sqrt(pi)
+            if (COUL == 1) {
+              if (ENER) ec += qq * er / r;
+              fr += qq * (er / r2 + A.kc * ex2 / r) / r;
+            } else {
+              if (ENER) ec += qq * (er / r - A.dsf_e0 + A.dsf_f0 * (r - A.rc));
+              fr += qq * (er / r2 + A.kc * ex2 / r - A.dsf_f0) / r;
+            }
+          } else if (COUL != 0) {
             const double qq = xi.w * aj.w;
             double E, Fc;
             ewald_ef(gt, A.ghi, r2, rinv, E, Fc);
@@ -557,6 +581,101 @@ static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
     if (VIR)
       for (int k = 0; k < 6; ++k) A.en.add(kEW0 + k, acc_w[k], false);
   }
+}
+
+// K-FREEZE: the frozen pair set of Evaluator::freeze_pairs (field.cpp:2541-2559) on the FP64 path: per entry and i
+// cluster the 64 atom pairs that are listed, real, not excluded and inside r_c at the packed positions; the entry's
+// half mask becomes their union, so that the pair kernel visits exactly those halves. One thread per entry.
+static __global__ void __launch_bounds__(128) k_freeze(PairArgs A, uint4* __restrict__ ent, unsigned long long* __restrict__ frozen) {
+  if (A.counters[kCntErr] & (kErrListOverflow | kErrMaskOverflow | kErrScOverflow | kErrColumnTooBig | kErrExclOverflow)) return;
+  const int nwork = min(A.counters[kCntWork], A.work_cap);
+  const int pad = A.ntab - 1;
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nwork; w += nwarps) {
+    const int4 wk = A.work[w];
+    for (int e = wk.y + lane; e < wk.y + wk.z; e += 32) {
+      uint4 en = ent[e];
+      int qa, qb, qc;
+      unpack_image(en.y >> 8, qa, qb, qc);
+      const double Sx = A.cell.h[0][0] * qa + A.cell.h[0][1] * qb + A.cell.h[0][2] * qc;
+      const double Sy = A.cell.h[1][0] * qa + A.cell.h[1][1] * qb + A.cell.h[1][2] * qc;
+      const double Sz = A.cell.h[2][0] * qa + A.cell.h[2][1] * qb + A.cell.h[2][2] * qc;
+      const unsigned built = en.y & 255u;
+      unsigned keep = 0;
+      for (int c = 0; c < 8; ++c) {
+        unsigned long long m = 0;
+        if ((built >> c) & 1u) {
+          const unsigned long long mm = en.z ? A.masks[8 * size_t(en.z - 1) + c] : ~0ull;
+          for (int i8 = 0; i8 < 8; ++i8) {
+            const int si = 64 * wk.x + 8 * c + i8;
+            if (A.tslot[si] == pad) continue;
+            const double4 xi = A.xqd[si];
+            const double xs = xi.x - Sx, ys = xi.y - Sy, zs = xi.z - Sz;
+            for (int jl = 0; jl < 8; ++jl) {
+              const int bit = 8 * i8 + jl;
+              const int sj = 8 * int(en.x) + jl;
+              if (!((mm >> bit) & 1ull) || A.tslot[sj] == pad) continue;
+              const double4 aj = A.xqd[sj];
+              const double dx = aj.x - xs, dy = aj.y - ys, dz = aj.z - zs;
+              if (dx * dx + dy * dy + dz * dz < A.rc2) m |= 1ull << bit;
+            }
+          }
+        }
+        frozen[8 * size_t(e) + c] = m;
+        if (m & 0x0f0f0f0f0f0f0f0full) keep |= 1u << c;         // j atoms 0-3: the lower half
+        if (m & 0xf0f0f0f0f0f0f0f0ull) keep |= 1u << (c + 8);   // j atoms 4-7: the upper half
+      }
+      en.w = keep;
+      ent[e] = en;
+    }
+  }
+}
+
+// K-COUNT-PAIRS: the atom pairs of the list within r_list = r_c + skin at the positions of its build (x0), real and not
+// excluded, each unordered pair once: Evaluator::pairs() of the reference's FP64 atom-pair list (field.cpp:1030-1049).
+static __global__ void __launch_bounds__(128) k_count_pairs(PairArgs A, const uint4* __restrict__ ent, const int* __restrict__ perm,
+                                                           const double* __restrict__ x0, const int* __restrict__ ioff, double rl2,
+                                                           unsigned long long* __restrict__ out) {
+  if (A.counters[kCntErr] & (kErrListOverflow | kErrMaskOverflow | kErrScOverflow | kErrColumnTooBig | kErrExclOverflow)) return;
+  const int nwork = min(A.counters[kCntWork], A.work_cap);
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  unsigned long long cnt = 0;
+  auto pos = [&](int a, double p[3]) {
+    const int o0 = ioff[3 * a], o1 = ioff[3 * a + 1], o2 = ioff[3 * a + 2];
+    for (int r = 0; r < 3; ++r) p[r] = x0[3 * a + r] + (A.cell.h[r][0] * o0 + A.cell.h[r][1] * o1 + A.cell.h[r][2] * o2);
+  };
+  for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nwork; w += nwarps) {
+    const int4 wk = A.work[w];
+    for (int e = wk.y + lane; e < wk.y + wk.z; e += 32) {
+      const uint4 en = ent[e];
+      int qa, qb, qc;
+      unpack_image(en.y >> 8, qa, qb, qc);
+      const double S[3] = {A.cell.h[0][0] * qa + A.cell.h[0][1] * qb + A.cell.h[0][2] * qc, A.cell.h[1][0] * qa + A.cell.h[1][1] * qb + A.cell.h[1][2] * qc,
+                           A.cell.h[2][0] * qa + A.cell.h[2][1] * qb + A.cell.h[2][2] * qc};
+      const unsigned built = en.y & 255u;
+      for (int c = 0; c < 8; ++c) {
+        if (!((built >> c) & 1u)) continue;
+        const unsigned long long mm = en.z ? A.masks[8 * size_t(en.z - 1) + c] : ~0ull;
+        for (int i8 = 0; i8 < 8; ++i8) {
+          const int ai = perm[64 * wk.x + 8 * c + i8];
+          if (ai < 0) continue;
+          double pi[3];
+          pos(ai, pi);
+          for (int jl = 0; jl < 8; ++jl) {
+            const int aj = perm[8 * int(en.x) + jl];
+            if (aj < 0 || !((mm >> (8 * i8 + jl)) & 1ull)) continue;
+            double pj[3];
+            pos(aj, pj);
+            const double dx = pj[0] - (pi[0] - S[0]), dy = pj[1] - (pi[1] - S[1]), dz = pj[2] - (pi[2] - S[2]);
+            cnt += dx * dx + dy * dy + dz * dz < rl2 ? 1 : 0;
+          }
+        }
+      }
+    }
+  }
+  if (cnt) atomicAdd(out, cnt);
 }
 
 // K-PRUNE (dynamic pruning, as core/src/nbnxm.cpp:328-363 does on the CPU): each entry's mask is rewritten to the

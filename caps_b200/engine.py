@@ -189,6 +189,36 @@ class Evaluator:
     def energies(self, on: bool):
         self._check(self.lib.caps_gpu_energies(self.h, int(bool(on))))
 
+    def reload(self, ff: ForceField | None = None):
+        """Evaluator::reload (field.hpp:349-352): the force field changed (same atoms); set up again from `ff` (default:
+        this evaluator's own ForceField object, changed in place)."""
+        if ff is not None:
+            if ff.natoms != self.ff.natoms:
+                raise ValueError("reload: the force field has another number of atoms")
+            self.ff = ff
+        s, keep = self.ff.to_struct()
+        self._check(self.lib.caps_gpu_reload(self.h, C.byref(s)))
+
+    def freeze_pairs(self, x, cell):
+        """Evaluator::freeze_pairs (field.hpp:341-346): later computes take exactly the pairs inside the cut-off at
+        (x, cell), on the FP64 path, with no list rebuild (small deformations)."""
+        x = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1))
+        c = cell_array(cell)
+        self._check(self.lib.caps_gpu_freeze_pairs(self.h, x.ctypes.data_as(C.c_void_p), c.ctypes.data_as(C.c_void_p)))
+
+    def unfreeze(self):
+        self._check(self.lib.caps_gpu_unfreeze(self.h))
+
+    def pairs(self) -> int:
+        """Evaluator::pairs() (field.hpp:348): the atom pairs of the FP64 pair list."""
+        v = int(self.lib.caps_gpu_pairs(self.h))
+        if v < 0:
+            _raise(-1, self.lib.caps_gpu_error(self.h).decode())
+        return v
+
+    def threads(self) -> int:
+        return int(self.lib.caps_gpu_threads(self.h))
+
     def compute(self, x, cell) -> tuple[dict, np.ndarray]:
         x = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1))
         c = cell_array(cell)

@@ -10,6 +10,10 @@
  *   caps_gpu_energies   Evaluator::energies(bool)                                       core/include/caps/field.hpp:344
  *   caps_gpu_compute    Evaluator::compute(x, cell, f) -> EnergyTerms                    core/include/caps/field.hpp:340
  *   caps_gpu_list_builds Evaluator::list_builds()                                       core/include/caps/field.hpp:341
+ *   caps_gpu_reload     Evaluator::reload()                                              core/include/caps/field.hpp:349-352
+ *   caps_gpu_freeze_pairs Evaluator::freeze_pairs(x, cell) / unfreeze()                 core/include/caps/field.hpp:341-347
+ *   caps_gpu_pairs      Evaluator::pairs()                                               core/include/caps/field.hpp:348
+ *   caps_gpu_threads    Evaluator::threads()                                             core/include/caps/field.hpp:333
  *   caps_gpu_run        run_dynamics(System&, const DynamicsOptions&, DynamicsReport*)   core/include/caps/dynamics.hpp:180
  *   caps_gpu_destroy    Evaluator::~Evaluator()                                          core/include/caps/field.hpp:333
  *   caps_gpu_traj_*     write_trajectory(const Trajectory&, path, dt_fs)                 core/include/caps/io.hpp:142, io_traj.cpp:47
@@ -188,6 +192,20 @@ int32_t caps_gpu_compute(caps_gpu_engine* e, const double* x, const double* cell
 int32_t caps_gpu_compute_device(caps_gpu_engine* e, const double* d_x, const double* cell, double* d_f, caps_gpu_terms* out);
 /* Replaces Evaluator::list_builds (field.hpp:341). */
 int32_t caps_gpu_list_builds(const caps_gpu_engine* e);
+/* Replaces Evaluator::reload (field.hpp:349-352): the force field changed (bonds, types, charges, bonded terms or
+ * exclusions; the same number of atoms): everything taken from it is set up again from `ff`, with the engine's options,
+ * and the list is rebuilt at the next call. A frozen list ends. */
+int32_t caps_gpu_reload(caps_gpu_engine* e, const caps_gpu_ff* ff);
+/* Replace Evaluator::freeze_pairs / unfreeze (field.hpp:341-347): later calls take exactly the atom pairs inside the
+ * cut-off at (x, cell), whatever their distance then (a pair beyond the cut-off takes the closed-form Coulomb term),
+ * on the FP64 path, and never rebuild the list; the cell may deform. Dynamics refuses a frozen engine. */
+int32_t caps_gpu_freeze_pairs(caps_gpu_engine* e, const double* x, const double* cell);
+int32_t caps_gpu_unfreeze(caps_gpu_engine* e);
+/* Replaces Evaluator::pairs (field.hpp:348): the atom pairs of the FP64 pair list (within cut-off + skin at its last
+ * build); on the mixed path, as the reference's cluster path, those of the last freeze_pairs (0 without one). -1 on error. */
+int64_t caps_gpu_pairs(caps_gpu_engine* e);
+/* Replaces Evaluator::threads (field.hpp:333): the device's streaming multiprocessors, the engine's parallel workers. */
+int32_t caps_gpu_threads(const caps_gpu_engine* e);
 /* Molecular dynamics in place on `state` (host memory). Replaces run_dynamics (dynamics.hpp:180; dynamics.cpp:71-815)
  * for the options above. progress and frame may be NULL. report (may be NULL) receives a short text summary. */
 int32_t caps_gpu_run(caps_gpu_engine* e, caps_gpu_state* state, const caps_gpu_md_opts* md, caps_gpu_progress_fn progress,

@@ -42,6 +42,11 @@ def lib() -> C.CDLL:
                               C.POINTER(_abi.Thermo), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double),
                               _abi.FRAME_FN, C.c_void_p]
         L.ref_request_stop.argtypes = [C.c_int]
+        L.ref_freeze_compute.argtypes = [C.POINTER(_abi.FF), C.POINTER(_abi.Opts), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.POINTER(_abi.Terms), C.POINTER(C.c_int64), C.c_int]
+        L.ref_pairs.argtypes = [C.POINTER(_abi.FF), C.POINTER(_abi.Opts), C.c_void_p, C.c_void_p, C.POINTER(C.c_int64), C.c_int]
+        L.ref_reload_compute.argtypes = [C.POINTER(_abi.FF), C.POINTER(_abi.FF), C.POINTER(_abi.Opts), C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.POINTER(_abi.Terms), C.c_int]
         L.ref_write_trajectory.argtypes = [C.c_char_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_int, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.c_double]
         L.ref_ewald_beta.restype = C.c_double
@@ -143,6 +148,48 @@ def run(ff: ForceField, x, cell, opts: DynamicsOptions, v=None, threads: int = 1
     if rc == 1:
         out["interrupted"] = lib().ref_error().decode()
     return out
+
+
+def freeze_compute(ff: ForceField, opts: EnergyOptions, x0, cell0, x1, cell1, threads: int = 1) -> tuple[dict, np.ndarray, int]:
+    """Evaluator::freeze_pairs(x0, cell0), then compute(x1, cell1): (terms, forces, pairs())."""
+    s, keep = ff.to_struct()
+    o = opts.to_struct()
+    a = np.ascontiguousarray(np.asarray(x0, dtype=np.float64).reshape(-1))
+    b = np.ascontiguousarray(np.asarray(x1, dtype=np.float64).reshape(-1))
+    c0, c1 = cell_array(cell0), cell_array(cell1)
+    f = np.zeros_like(b)
+    t = _abi.Terms()
+    npairs = C.c_int64()
+    if lib().ref_freeze_compute(C.byref(s), C.byref(o), _vp(a), _vp(c0), _vp(b), _vp(c1), _vp(f), C.byref(t), C.byref(npairs), threads) != 0:
+        raise RuntimeError(lib().ref_error().decode())
+    return t.as_dict(), f.reshape(-1, 3), npairs.value
+
+
+def pairs(ff: ForceField, opts: EnergyOptions, x, cell, threads: int = 1) -> int:
+    """Evaluator::pairs() after one compute at (x, cell)."""
+    s, keep = ff.to_struct()
+    o = opts.to_struct()
+    a = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1))
+    c = cell_array(cell)
+    npairs = C.c_int64()
+    if lib().ref_pairs(C.byref(s), C.byref(o), _vp(a), _vp(c), C.byref(npairs), threads) != 0:
+        raise RuntimeError(lib().ref_error().decode())
+    return npairs.value
+
+
+def reload_compute(ff1: ForceField, ff2: ForceField, opts: EnergyOptions, x, cell, threads: int = 1) -> tuple[dict, np.ndarray]:
+    """An evaluator on ff1 computes at (x, cell); its force field becomes ff2 in place and is reloaded; the second
+    compute's (terms, forces)."""
+    s1, k1 = ff1.to_struct()
+    s2, k2 = ff2.to_struct()
+    o = opts.to_struct()
+    a = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1))
+    c = cell_array(cell)
+    f = np.zeros_like(a)
+    t = _abi.Terms()
+    if lib().ref_reload_compute(C.byref(s1), C.byref(s2), C.byref(o), _vp(a), _vp(c), _vp(f), C.byref(t), threads) != 0:
+        raise RuntimeError(lib().ref_error().decode())
+    return t.as_dict(), f.reshape(-1, 3)
 
 
 def request_stop(on: bool = True):

@@ -428,6 +428,63 @@ int ref_run(const caps_gpu_ff* p, const caps_gpu_opts* eo, caps_gpu_state* st, c
 
 void ref_request_stop(int on) { request_stop(on != 0); }
 
+// Evaluator::freeze_pairs at (x0, cell0), then compute at (x1, cell1): forces, terms and pairs().
+int ref_freeze_compute(const caps_gpu_ff* p, const caps_gpu_opts* o, const double* x0, const double* cell0, const double* x1, const double* cell1,
+                       double* f, caps_gpu_terms* out, int64_t* npairs, int threads) {
+  try {
+    auto ff = to_ff(p);
+    Evaluator ev(*ff, to_eo(o, threads));
+    const size_t n3 = 3 * size_t(p->natoms);
+    std::vector<double> a(x0, x0 + n3), b(x1, x1 + n3), fv;
+    ev.freeze_pairs(a, to_cell(cell0));
+    const EnergyTerms t = ev.compute(b, to_cell(cell1), fv);
+    std::memcpy(f, fv.data(), n3 * sizeof(double));
+    to_terms(t, out);
+    *npairs = int64_t(ev.pairs());
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+// compute at (x, cell), then pairs().
+int ref_pairs(const caps_gpu_ff* p, const caps_gpu_opts* o, const double* x, const double* cell, int64_t* npairs, int threads) {
+  try {
+    auto ff = to_ff(p);
+    Evaluator ev(*ff, to_eo(o, threads));
+    std::vector<double> a(x, x + 3 * size_t(p->natoms)), fv;
+    ev.compute(a, to_cell(cell), fv);
+    *npairs = int64_t(ev.pairs());
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+// An evaluator on force field p1 computes at (x, cell); the force field is then changed in place to p2 and reloaded
+// (Evaluator::reload, as a bond-exchange move does), and computes again: forces and terms of the second call.
+int ref_reload_compute(const caps_gpu_ff* p1, const caps_gpu_ff* p2, const caps_gpu_opts* o, const double* x, const double* cell, double* f,
+                       caps_gpu_terms* out, int threads) {
+  try {
+    auto ff = to_ff(p1);
+    Evaluator ev(*ff, to_eo(o, threads));
+    const size_t n3 = 3 * size_t(p1->natoms);
+    std::vector<double> a(x, x + n3), fv;
+    ev.compute(a, to_cell(cell), fv);
+    *ff = *to_ff(p2);
+    ev.reload();
+    const EnergyTerms t = ev.compute(a, to_cell(cell), fv);
+    std::memcpy(f, fv.data(), n3 * sizeof(double));
+    to_terms(t, out);
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
 // caps::write_trajectory (io_traj.cpp:47) on a Trajectory of nf frames: x [nf][3n], cells [nf][12], steps [nf]; the
 // topology's atoms carry ids, mols and types, its title the DCD's second title line.
 int ref_write_trajectory(const char* path, int n, const int64_t* ids, const int64_t* mols, const int32_t* types, const char* title, int nf,
