@@ -79,3 +79,18 @@ def trajectory_case(cell_name: str, natoms: int = 37, nframes: int = 5, seed: in
         x = rng.normal(0.0, 6.0, size=(natoms, 3)) + 10.0
         frames.append((x, cell0 * (1.0 + 0.003 * k), 1000 + 250 * k))
     return ids, mols, types, frames
+
+
+def ps32k():
+    """The 32,000-atom polystyrene PME melt of the benchmark (40 chains x 50 units x 16 atoms at 1.04 g/cm3): its force
+    field from caps_b200.systems and the committed equilibrated start structure. (ff, x, v, cell)"""
+    from caps_b200.systems import polystyrene_melt
+    z = np.load(Path(__file__).resolve().parent.parent / "caps_b200" / "data" / "ps32k_start.npz")
+    ff, _, _ = polystyrene_melt(40, 50, 1.04, seed=1, grow=False)
+    return ff, z["x"].astype(np.float64), z["v"].astype(np.float64), z["cell"].astype(np.float64)
+
+
+def ps32k_options(precision: str, tail: bool = True) -> EnergyOptions:
+    """The benchmark's energy options: r_c 12 Å + 2 Å skin, PME rtol 1e-5, 1 Å spacing, order 4."""
+    return EnergyOptions(cutoff=12.0, skin=2.0, electrostatics="pme", ewald_rtol=1e-5, pme_spacing=1.0, pme_order=4, tail=tail,
+                         precision=precision)
