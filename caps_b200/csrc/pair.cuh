@@ -183,11 +183,12 @@ static __global__ void __launch_bounds__(128, 5) k_pair_f32(PairArgs A) {
   float4* tab = smem_f4;                                  // ntab * ntab
   float4* s_xi = smem_f4 + A.ntab * A.ntab;               // 4 warps x 64
   int* s_ti = reinterpret_cast<int*>(s_xi + 4 * 64);      // 4 warps x 64
-  // a work item's entries and their j atoms, staged per warp in one batch of independent loads
+  // a work item's entries, their j atoms and their exclusion masks, staged per warp in one batch of independent loads
   uint4* s_en_all = reinterpret_cast<uint4*>(s_ti + 4 * 64);   // 4 warps x 32 entries
   float4* s_sh_all = reinterpret_cast<float4*>(s_en_all + 4 * kBatch);
   float4* s_xj_all = s_sh_all + 4 * kBatch;                     // 4 warps x 32 entries x 8 j atoms
   int* s_tj_all = reinterpret_cast<int*>(s_xj_all + 4 * kBatch * 8);
+  unsigned long long* s_mk_all = reinterpret_cast<unsigned long long*>(s_tj_all + 4 * kBatch * 8);
   for (int t = threadIdx.x; t < A.ntab * A.ntab; t += blockDim.x) tab[t] = A.tab[t];
   __syncthreads();
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -231,6 +232,7 @@ static __global__ void __launch_bounds__(128, 5) k_pair_f32(PairArgs A) {
     float4* s_sh = s_sh_all + kBatch * wib;
     float4* s_xj = s_xj_all + kBatch * 8 * wib;
     int* s_tj = s_tj_all + kBatch * 8 * wib;
+    unsigned long long* s_mk = s_mk_all + kBatch * 8 * wib;
     const int ne = min(wk.z, kBatch);
     if (lane < ne) {
       s_en[lane] = A.ent[wk.y + lane];
@@ -241,9 +243,11 @@ static __global__ void __launch_bounds__(128, 5) k_pair_f32(PairArgs A) {
     for (int k = 0; k < 8; ++k) {
       const int t = lane + 32 * k;   // entry t / 8, j atom t % 8
       if (t < 8 * ne) {
-        const int ja = 8 * int(s_en[t >> 3].x) + (t & 7);
+        const uint4 e4 = s_en[t >> 3];
+        const int ja = 8 * int(e4.x) + (t & 7);
         s_xj[t] = A.xq[ja];
         s_tj[t] = A.tslot[ja];
+        s_mk[t] = e4.z ? A.masks[8 * size_t(e4.z - 1) + (t & 7)] : ~0ull;   // entry t / 8, i cluster t % 8
       }
     }
     __syncwarp();
@@ -263,23 +267,24 @@ static __global__ void __launch_bounds__(128, 5) k_pair_f32(PairArgs A) {
 #pragma unroll
       for (int c = 0; c < 8; ++c) {
         if (!((imask >> c) & 1u)) continue;
-        const unsigned long long mm = en.z ? A.masks[8 * size_t(en.z - 1) + c] : ~0ull;
+        const unsigned long long mm = s_mk[8 * el + c];
         const float4 xi = xi_s[8 * c + i8];
         const int ti = ti_s[8 * c + i8];
-        const bool oki = (ireal >> c) & 1u;
+        // this lane's two pairs of the i cluster (j atoms jq and jq + 4): bits 0 and 4, real i atom and not excluded
+        const unsigned lb = ((ireal >> c) & 1u) ? unsigned(mm >> (8 * i8 + jq)) & 0x11u : 0u;
 #pragma unroll
         for (int jj = 0; jj < 2; ++jj) {
           if (!((hmask >> (c + 8 * jj)) & 1u)) continue;   // this half of the j cluster is beyond the prune radius
           const float xj = jj ? xj1 : xj0, yj = jj ? yj1 : yj0, zj = jj ? zj1 : zj0;
           const float qj = jj ? a1.w : a0.w;
           const int tj = jj ? t1 : t0;
-          const int bit = 8 * i8 + jq + 4 * jj;
+          const bool listed = (lb >> (4 * jj)) & 1u;
           const float dx = xj - xi.x, dy = yj - xi.y, dz = zj - xi.z;
           const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-          const bool ok = oki && ((mm >> bit) & 1ull) && (r2 < rc2);
+          const bool ok = listed && (r2 < rc2);
           if (ENER) {
             npair += ok ? 1.f : 0.f;
-            nlist += (oki && ((mm >> bit) & 1ull)) ? 1.f : 0.f;
+            nlist += listed ? 1.f : 0.f;
           }
           const float r2s = ok ? r2 : 1.f;
           const float rinv = rsqrtf(r2s);
