@@ -32,9 +32,12 @@ sys.path.insert(0, str(ROOT))
 
 REF_SECONDS = 60.0           # bound on the reference arm's timed sample (CPU)
 CPU_SAMPLE_SECONDS = 15.0    # bound on the cpu_baseline sample beside the GPU run
-# DRAM bytes (read + write) of one k_pair_f32 launch on this workload, from ncu (profiles/pair_kernel_ps32k_ncu.md)
-PAIR_DRAM_BYTES = 10.66e6
-FLOPS_PER_PAIR = 59          # FP32 flops of one interacting pair on a force-only step (FMA as 2)
+# DRAM bytes (read + write) of one k_pair_f32 launch on this workload, from an ncu capture of that kernel (cold L2)
+PAIR_DRAM_BYTES = 10.83e6
+# FP32 flops of one interacting pair on a force-only step, FMA as 2: separation, r^2 and its inverse powers 11 (the
+# reciprocal square root not counted), LJ 12-6 6, the Ewald real-space term through its rational fit 33, force
+# components and their sums 9
+FLOPS_PER_PAIR = 59
 FLUSH_BYTES = 256 << 20      # > 126 MB L2
 START = ROOT / "caps_b200" / "data" / "ps32k_start.npz"
 WORKLOAD = {"workload": "polystyrene PME melt, 40 chains x 50 units x 16 atoms = 32,000 atoms", "box_A": None, "density_g_cm3": 1.04,
