@@ -136,7 +136,7 @@ PairArgs Engine::pair_args() {
   A.tabcap = d_tabcap_.p;
   A.gtab = d_gtab_.p;
   A.ntab = nt_ + 1;
-  A.gnodes = gnodes_;
+  A.gnodes = coul_ ? gnodes_ : 0;   // a table only with Coulomb: the FP64 kernel's shared memory holds it then
   A.ghi = ghi_;
   A.cell = dcell_;
   A.rc2 = rc_ * rc_;

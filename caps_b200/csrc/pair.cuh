@@ -416,8 +416,8 @@ template <int COUL, bool ENER, bool VIR, bool CAP = false, bool LJ96 = false, bo
 static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
   extern __shared__ double4 smem_d4[];
   double4* tab = smem_d4;                                   // ntab * ntab
-  double* gt = reinterpret_cast<double*>(tab + A.ntab * A.ntab);   // 2 * gnodes
-  double4* s_xi = reinterpret_cast<double4*>(gt + 2 * A.gnodes);   // 4 x 64
+  double* gt = reinterpret_cast<double*>(tab + A.ntab * A.ntab);   // 2 * gnodes with Coulomb, none without (as the launch sizes it)
+  double4* s_xi = reinterpret_cast<double4*>(gt + (COUL != 0 ? 2 * A.gnodes : 0));   // 4 x 64
   int* s_ti = reinterpret_cast<int*>(s_xi + 4 * 64);
   for (int t = threadIdx.x; t < A.ntab * A.ntab; t += blockDim.x) tab[t] = A.tabd[t];
   if (COUL != 0)
@@ -494,7 +494,7 @@ static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
           if (CAP && r2 < cp.x) {
             // the push-off cap (field.cpp:1534-1538): LJ continued linearly inside the radius where |F| reaches the cap
             const double r = r2 * rinv, rcp = sqrt(cp.x);
-            fr = cp.z / r * rinv;
+            fr = cp.z * rinv;   // F / r with |F| = the cap
             if (ENER) ev += cp.y + cp.z * (rcp - r) - cc.z;
           } else {
             if (LJ96) {   // field.cpp:1658-1661

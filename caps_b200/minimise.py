@@ -30,13 +30,61 @@ class MinimiseOptions:
 def max_force(f: np.ndarray) -> float:
     """The largest atomic force (relax.cpp:47-51)."""
     f = f.reshape(-1, 3)
-    return float(math.sqrt(float(np.max(np.einsum("ij,ij->i", f, f))))) if f.size else 0.0
+    return float(math.sqrt(float(np.max(f[:, 0] * f[:, 0] + f[:, 1] * f[:, 1] + f[:, 2] * f[:, 2])))) if f.size else 0.0
+
+
+def dotv(a: np.ndarray, b: np.ndarray) -> float:
+    """The reference's dotv (relax.cpp:55-59): the products summed in order, so that the minimiser's path is the
+    reference's to the last bit (a BLAS dot sums in another order)."""
+    return float(np.cumsum(a * b)[-1]) if a.size else 0.0
+
+
+# --- the reference's cell geometry (core/src/system.cpp), restated in its operation order ----------------------------
+
+def dot3(a, b) -> float:
+    return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]
+
+
+def cross3(a, b):
+    return (a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0])
+
+
+def cell_volume(c) -> float:
+    return abs(dot3(c[3:6], cross3(c[6:9], c[9:12])))
+
+
+def cell_valid(c) -> bool:
+    return cell_volume(c) > 1e-9   # Cell::valid (core/src/system.cpp:14)
+
+
+def round_half_away(v: float) -> float:
+    """std::round rounds halves away from zero."""
+    return math.floor(v + 0.5) if v >= 0 else -math.floor(-v + 0.5)
+
+
+def minimum_image(c, d):
+    """Cell::minimum_image (core/src/system.cpp:27-45), the neighbouring images checked for skewed cells."""
+    d = tuple(float(q) for q in d)
+    if not cell_valid(c):
+        return d
+    a, b, cc = tuple(float(q) for q in c[3:6]), tuple(float(q) for q in c[6:9]), tuple(float(q) for q in c[9:12])
+    v = dot3(a, cross3(b, cc))
+    f = [dot3(d, cross3(b, cc)) / v, dot3(d, cross3(cc, a)) / v, dot3(d, cross3(a, b)) / v]
+    f = [q - round_half_away(q) for q in f]
+    r = tuple(a[k] * f[0] + b[k] * f[1] + cc[k] * f[2] for k in range(3))
+    best, out = dot3(r, r), r
+    for i in (-1, 0, 1):
+        for j in (-1, 0, 1):
+            for k in (-1, 0, 1):
+                t = tuple(r[m] + a[m] * i + b[m] * j + cc[m] * k for m in range(3))
+                q = dot3(t, t)
+                if q < best - 1e-12:
+                    best, out = q, t
+    return r if best == dot3(r, r) else out
 
 
 def _minimum_image(cell: np.ndarray, d: np.ndarray) -> np.ndarray:
-    h = np.asarray(cell[3:12], dtype=np.float64).reshape(3, 3).T   # columns a, b, c
-    s = np.linalg.solve(h, d)
-    return h @ (s - np.round(s))
+    return np.array(minimum_image(cell, d))
 
 
 def minimise(ev, x, cell, opts: MinimiseOptions, name: str = "minimise") -> dict:
@@ -66,7 +114,7 @@ def minimise(ev, x, cell, opts: MinimiseOptions, name: str = "minimise") -> dict
         en = float(terms["total"])
         for (i, j, r0, k) in opts.restraints:
             dv = _minimum_image(cell, p[3 * j:3 * j + 3] - p[3 * i:3 * i + 3])
-            r = float(np.linalg.norm(dv))
+            r = math.sqrt(dot3(dv, dv))
             if r < 1e-9:
                 continue
             en += k * (r - r0) * (r - r0)
@@ -78,17 +126,17 @@ def minimise(ev, x, cell, opts: MinimiseOptions, name: str = "minimise") -> dict
             b1 = _minimum_image(cell, at(j) - at(i))
             b2 = _minimum_image(cell, at(kk) - at(j))
             b3 = _minimum_image(cell, at(l) - at(kk))
-            m, nn = np.cross(b1, b2), np.cross(b2, b3)
-            m2, n2, lb2 = float(m @ m), float(nn @ nn), float(np.linalg.norm(b2))
+            m, nn = np.array(cross3(b1, b2)), np.array(cross3(b2, b3))
+            m2, n2, lb2 = dot3(m, m), dot3(nn, nn), math.sqrt(dot3(b2, b2))
             if m2 < 1e-12 or n2 < 1e-12 or lb2 < 1e-9:
                 continue
-            phi = math.atan2(lb2 * float(b1 @ nn), float(m @ nn))
+            phi = math.atan2(lb2 * dot3(b1, nn), dot3(m, nn))
             dphi = phi - phi0 * math.pi / 180.0
             dphi -= 2 * math.pi * round_half_away(dphi / (2 * math.pi))
             en += kphi * dphi * dphi
             dE = 2 * kphi * dphi
             gi, gl = m * (-lb2 / m2), nn * (lb2 / n2)
-            s1, s3 = float(b1 @ b2) / (lb2 * lb2), float(b3 @ b2) / (lb2 * lb2)
+            s1, s3 = dot3(b1, b2) / (lb2 * lb2), dot3(b3, b2) / (lb2 * lb2)
             gj, gk = gi * (-s1 - 1) + gl * s3, gi * s1 + gl * (-s3 - 1)
             f[3 * i:3 * i + 3] -= dE * gi
             f[3 * j:3 * j + 3] -= dE * gj
@@ -107,9 +155,9 @@ def minimise(ev, x, cell, opts: MinimiseOptions, name: str = "minimise") -> dict
         dt, alpha, npos = 0.05, astart, 0
         v = np.zeros(n3)
         while it < opts.max_iterations and stopped != "force":
-            pw = float(f @ v)
+            pw = dotv(f, v)
             if pw > 0:
-                vn, fnn = math.sqrt(float(v @ v)), math.sqrt(float(f @ f))
+                vn, fnn = math.sqrt(dotv(v, v)), math.sqrt(dotv(f, f))
                 v = (1 - alpha) * v + alpha * vn * f / max(fnn, 1e-300)
                 npos += 1
                 if npos > nmin:
@@ -143,26 +191,26 @@ def minimise(ev, x, cell, opts: MinimiseOptions, name: str = "minimise") -> dict
                 if fprev is None:
                     d = f.copy()
                 else:
-                    den = float(fprev @ fprev)
-                    num = float(f @ (f - fprev))
+                    den = dotv(fprev, fprev)
+                    num = dotv(f, f - fprev)
                     beta = max(0.0, num / den) if den > 0 else 0.0
                     d = f + beta * dprev
             else:   # L-BFGS two-loop on the gradient g = -f
                 q = -f.copy()
                 al = [0.0] * len(S)
                 for jj in range(len(S) - 1, -1, -1):
-                    al[jj] = rho[jj] * float(S[jj] @ q)
+                    al[jj] = rho[jj] * dotv(S[jj], q)
                     q -= al[jj] * Y[jj]
-                gamma = float(S[-1] @ Y[-1]) / float(Y[-1] @ Y[-1]) if S else 1.0 / 300.0
+                gamma = dotv(S[-1], Y[-1]) / dotv(Y[-1], Y[-1]) if S else 1.0 / 300.0
                 q *= gamma
                 for jj in range(len(S)):
-                    b = rho[jj] * float(Y[jj] @ q)
+                    b = rho[jj] * dotv(Y[jj], q)
                     q += S[jj] * (al[jj] - b)
                 d = -q
-            slope = float(f @ d)
+            slope = dotv(f, d)
             if slope <= 0:
                 d = f.copy()
-                slope = float(f @ f)
+                slope = dotv(f, f)
                 S.clear(), Y.clear(), rho.clear()
             md = max_force(d)
             a = min(1.0, step_max / md) if (method == "lbfgs" and S) else step / md
@@ -196,7 +244,7 @@ def minimise(ev, x, cell, opts: MinimiseOptions, name: str = "minimise") -> dict
             step = min(max(moved * 1.5, 1e-4), step_max)
             if method == "lbfgs":
                 s_, y_ = xn - x, f - fn
-                sy = float(s_ @ y_)
+                sy = dotv(s_, y_)
                 if sy > 1e-10:
                     S.append(s_), Y.append(y_), rho.append(1.0 / sy)
                     if len(S) > mhist:
@@ -221,8 +269,3 @@ def minimise(ev, x, cell, opts: MinimiseOptions, name: str = "minimise") -> dict
                 cg_restarted = False
             it += 1
     return {"name": name, "iterations": it, "energy": e, "fmax": fmax, "stopped_by": stopped, "evaluations": nev, "x": x.reshape(-1, 3)}
-
-
-def round_half_away(v: float) -> float:
-    """std::round rounds halves away from zero."""
-    return math.floor(v + 0.5) if v >= 0 else -math.floor(-v + 0.5)

@@ -42,6 +42,14 @@ def lib() -> C.CDLL:
                               C.POINTER(_abi.Thermo), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_double),
                               _abi.FRAME_FN, C.c_void_p]
         L.ref_request_stop.argtypes = [C.c_int]
+        L.ref_ev_create.restype = C.c_void_p
+        L.ref_ev_create.argtypes = [C.POINTER(_abi.FF), C.POINTER(_abi.Opts), C.c_int]
+        L.ref_ev_set_options.argtypes = [C.c_void_p, C.POINTER(_abi.Opts), C.c_int]
+        L.ref_ev_compute.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(_abi.Terms)]
+        L.ref_ev_list_builds.argtypes = [C.c_void_p]
+        L.ref_ev_destroy.argtypes = [C.c_void_p]
+        L.ref_relax.argtypes = [C.POINTER(_abi.FF), C.POINTER(_abi.Opts), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                C.c_void_p, C.c_int, C.c_void_p, C.c_char_p, C.c_int, C.c_char_p, C.c_int]
         L.ref_freeze_compute.argtypes = [C.POINTER(_abi.FF), C.POINTER(_abi.Opts), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.POINTER(_abi.Terms), C.POINTER(C.c_int64), C.c_int]
         L.ref_pairs.argtypes = [C.POINTER(_abi.FF), C.POINTER(_abi.Opts), C.c_void_p, C.c_void_p, C.POINTER(C.c_int64), C.c_int]
@@ -322,3 +330,74 @@ def build_kg(chains: int, beads: int, density: float, seed: int):
         if lib().ref_build_kg(chains, beads, density, seed, p.encode()) != 0:
             raise RuntimeError(lib().ref_error().decode())
         return read_capsff(p)
+
+
+def relax(ff: ForceField, x, cell, ro) -> dict:
+    """caps::relax in the reference core (check_cell_fit off); ro: a caps_b200.relax.RelaxOptions. Returns the report
+    fields, the stages and the relaxed x (N x 3) and cell."""
+    s, keep = ff.to_struct()
+    o = ro.energy.to_struct()
+    xx = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1)).copy()
+    c = cell_array(cell).copy()
+    code = {"sd": 0, "steepest": 0, "cg": 1, "lbfgs": 2, "l-bfgs": 2, "fire": 3}[ro.method.lower()]
+    opt = np.array([code, ro.ftol, ro.etol, ro.max_iterations, int(ro.pushoff), ro.pushoff_ramp_ps, ro.pushoff_cap, ro.pushoff_temperature,
+                    ro.pushoff_ramp_segments, ro.target_density, ro.compress_step, int(ro.relax_box), ro.pressure, ro.pressure_tol,
+                    ro.box_cycles, int(ro.box_anisotropic), *[int(bool(a)) for a in ro.box_axes]], dtype=np.float64)
+    caps = np.ascontiguousarray(np.asarray(ro.pushoff_caps, dtype=np.float64))
+    fixed = None if ro.fixed is None else np.ascontiguousarray(np.asarray(ro.fixed, dtype=np.int8))
+    res = np.zeros(16)
+    st = np.zeros(6 * 256)
+    names, notes = C.create_string_buffer(65536), C.create_string_buffer(65536)
+    if lib().ref_relax(C.byref(s), C.byref(o), _vp(xx), _vp(c), _vp(opt), len(caps), _vp(caps), None if fixed is None else _vp(fixed),
+                       _vp(res), 256, _vp(st), names, 65536, notes, 65536) != 0:
+        raise RuntimeError(lib().ref_error().decode())
+    nst = int(res[10])
+    nm = names.value.decode().split("\n")[:nst]
+    stopped = ("force", "energy", "iterations", "line search", "time")
+    stages = [{"name": nm[k], "iterations": int(st[6 * k]), "energy": st[6 * k + 1], "fmax": st[6 * k + 2], "density": st[6 * k + 3],
+               "pressure": st[6 * k + 4], "stopped_by": stopped[int(st[6 * k + 5])]} for k in range(min(nst, 256))]
+    return {"fmax_initial": res[0], "fmax_final": res[1], "density_initial": res[2], "density_final": res[3], "pressure_final": res[4],
+            "iterations": int(res[5]), "evaluations": int(res[6]), "converged": bool(res[7]), "initial_total": res[8], "final_total": res[9],
+            "stages": stages, "notes": [n for n in notes.value.decode().split("\n") if n], "x": xx.reshape(-1, 3), "cell": c}
+
+
+class Evaluator:
+    """A persistent caps::Evaluator of the reference core, in caps_b200.Evaluator's calling convention (compute,
+    set_options, list_builds, ff): a driver run on it makes the reference's own sequence of calls on one evaluator."""
+
+    def __init__(self, ff: ForceField, options: EnergyOptions, threads: int = 1):
+        self.ff, self.options, self.threads = ff, options, threads
+        s, self._keep = ff.to_struct()
+        o = options.to_struct()
+        self.h = lib().ref_ev_create(C.byref(s), C.byref(o), threads)
+        if not self.h:
+            raise RuntimeError(lib().ref_error().decode())
+
+    def set_options(self, options: EnergyOptions):
+        self.options = options
+        o = options.to_struct()
+        if lib().ref_ev_set_options(self.h, C.byref(o), self.threads) != 0:
+            raise RuntimeError(lib().ref_error().decode())
+
+    def compute(self, x, cell):
+        xx = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1))
+        c = cell_array(cell)
+        f = np.zeros_like(xx)
+        t = _abi.Terms()
+        if lib().ref_ev_compute(self.h, _vp(xx), _vp(c), _vp(f), C.byref(t)) != 0:
+            raise RuntimeError(lib().ref_error().decode())
+        return t.as_dict(), f.reshape(-1, 3)
+
+    def list_builds(self) -> int:
+        return int(lib().ref_ev_list_builds(self.h))
+
+    def close(self):
+        if self.h:
+            lib().ref_ev_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -721,4 +721,102 @@ int ref_minimise(const caps_gpu_ff* p, const caps_gpu_opts* eo, double* x, const
   }
 }
 
+// A persistent reference evaluator: the same Evaluator object across calls, so that its pair list keeps the history a
+// driver's evaluator has (the order of the pair sums, and so the last bits, follow it).
+struct RefEv {
+  std::shared_ptr<ForceField> ff;
+  std::unique_ptr<Evaluator> ev;
+};
+void* ref_ev_create(const caps_gpu_ff* p, const caps_gpu_opts* o, int threads) {
+  try {
+    auto h = std::make_unique<RefEv>();
+    h->ff = to_ff(p);
+    h->ev = std::make_unique<Evaluator>(*h->ff, to_eo(o, threads));
+    return h.release();
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return nullptr;
+  }
+}
+int ref_ev_set_options(void* h, const caps_gpu_opts* o, int threads) {
+  try {
+    static_cast<RefEv*>(h)->ev->set_options(to_eo(o, threads));
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+int ref_ev_compute(void* h, const double* x, const double* cell, double* f, caps_gpu_terms* out) {
+  try {
+    RefEv* r = static_cast<RefEv*>(h);
+    const size_t n3 = 3 * r->ff->atom_type.size();
+    std::vector<double> xv(x, x + n3), fv;
+    const EnergyTerms t = r->ev->compute(xv, to_cell(cell), fv);
+    std::memcpy(f, fv.data(), n3 * sizeof(double));
+    to_terms(t, out);
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+int ref_ev_list_builds(void* h) { return static_cast<RefEv*>(h)->ev->list_builds(); }
+void ref_ev_destroy(void* h) { delete static_cast<RefEv*>(h); }
+
+// relax (relax.cpp:343) with the given force field on a System built from the arrays (check_cell_fit off). opt: method,
+// ftol, etol, max_iterations, pushoff, pushoff_ramp_ps, pushoff_cap, pushoff_temperature, pushoff_ramp_segments,
+// target_density, compress_step, relax_box, pressure, pressure_tol, box_cycles, box_anisotropic, box axis x, y, z
+// (18 numbers); caps: ncaps push-off caps. Out: x and cell in place; res: fmax_initial, fmax_final, density_initial,
+// density_final, pressure_final, iterations, evaluations, converged, initial total, final total, stages; per stage (up to
+// max_stages) iterations, energy, fmax, density, pressure, stopped_by code in st[6 k..]; names and notes joined by '\n'.
+int ref_relax(const caps_gpu_ff* p, const caps_gpu_opts* eo, double* x, double* cell, const double* opt, int ncaps, const double* caps,
+              const char* fixed, double* res, int max_stages, double* st, char* names, int names_cap, char* notes, int notes_cap) {
+  try {
+    auto ff = to_ff(p);
+    caps_gpu_state state{x, nullptr, cell, 0};
+    System s = to_system(p, ff, &state, nullptr);
+    RelaxOptions o;
+    const Minimiser ms[4] = {Minimiser::SteepestDescent, Minimiser::ConjugateGradient, Minimiser::LBFGS, Minimiser::FIRE};
+    o.method = ms[int(opt[0]) & 3];
+    o.ftol = opt[1], o.etol = opt[2], o.max_iterations = int(opt[3]);
+    o.check_cell_fit = false;
+    o.energy = to_eo(eo, 1);
+    o.field = ff;
+    o.pushoff = opt[4] != 0;
+    o.pushoff_ramp_ps = opt[5], o.pushoff_cap = opt[6], o.pushoff_temperature = opt[7], o.pushoff_ramp_segments = int(opt[8]);
+    o.target_density = opt[9], o.compress_step = opt[10];
+    o.relax_box = opt[11] != 0;
+    o.pressure = opt[12], o.pressure_tol = opt[13], o.box_cycles = int(opt[14]);
+    o.box_anisotropic = opt[15] != 0;
+    for (int k = 0; k < 3; ++k) o.box_axes[k] = opt[16 + k] != 0;
+    o.pushoff_caps.assign(caps, caps + ncaps);
+    if (fixed) o.fixed.assign(fixed, fixed + p->natoms);
+    RelaxReport rep;
+    relax(s, o, &rep);
+    for (int i = 0; i < p->natoms; ++i)
+      for (int k = 0; k < 3; ++k) x[3 * i + k] = s.atoms[size_t(i)].pos[k];
+    from_cell(s.cell, cell);
+    res[0] = rep.fmax_initial, res[1] = rep.fmax_final, res[2] = rep.density_initial, res[3] = rep.density_final;
+    res[4] = rep.pressure_final, res[5] = rep.iterations, res[6] = rep.evaluations, res[7] = rep.converged ? 1 : 0;
+    res[8] = rep.initial.total(), res[9] = rep.final.total(), res[10] = double(rep.stages.size());
+    std::string nm, nt;
+    for (size_t k = 0; k < rep.stages.size(); ++k) {
+      const RelaxStage& r = rep.stages[k];
+      nm += r.name + "\n";
+      if (int(k) >= max_stages) continue;
+      const std::string& b = r.stopped_by;
+      st[6 * k] = r.iterations, st[6 * k + 1] = r.energy, st[6 * k + 2] = r.fmax, st[6 * k + 3] = r.density, st[6 * k + 4] = r.pressure;
+      st[6 * k + 5] = b == "force" ? 0 : b == "energy" ? 1 : b == "iterations" ? 2 : b == "line search" ? 3 : 4;
+    }
+    for (const auto& n : rep.notes) nt += n + "\n";
+    std::snprintf(names, size_t(names_cap), "%s", nm.c_str());
+    std::snprintf(notes, size_t(notes_cap), "%s", nt.c_str());
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
 }  // extern "C"
