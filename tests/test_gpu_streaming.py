@@ -192,3 +192,21 @@ def test_batch_native_writers_keep_rows_apart(tmp_path):
     for w in ws:
         w.close()
     assert [[row["step"] for row in o["thermo"]] for o in out] == [[0, 10, 20, 24]] * 2
+
+
+
+def test_stop_ends_every_replica_of_a_batch():
+    """A stop asked for before a batch starts ends every replica at step 1, each with its own stop checkpoint, and the
+    error carries every replica's state."""
+    fx = load("ps_small")
+    opts = [_opts(seed=3 + r, frame_every=0, checkpoint_every=0, thermo_every=5) for r in range(2)]
+    evs = [Evaluator(fx.ff, o.energy) for o in opts]
+    got = [[], []]
+    request_stop(True)
+    try:
+        with pytest.raises(DynamicsInterrupted, match="stopped at step 1 ") as ei:
+            run_batch(evs, [fx.x] * 2, [fx.cell] * 2, opts, checkpoints=[lambda x, v, c, s: got[0].append(s), lambda x, v, c, s: got[1].append(s)])
+    finally:
+        request_stop(False)
+    assert got == [[1], [1]]
+    assert ei.value.step == 1 and len(ei.value.state) == 2
