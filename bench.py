@@ -288,7 +288,7 @@ def main():
     ms64 = max_over_ranks(ev64.last_step_ms())
     nsd64 = 1000.0 / ms64 * 86400e-6
     ev64.close()
-    # --- batched replicas (SURVEY config 4's target): R replicas of this cell, each at its own Langevin temperature,
+    # --- batched replicas (the 64-replica cooling workload's efficiency target): R replicas of this cell, each at its own Langevin temperature,
     # in lock step (one graph launch per plain step), against one equally large system (the cell tiled 2 x 2 x 2) ---
     batch = None
     if args.replicas > 0:
