@@ -45,6 +45,22 @@ WORKLOAD = {"workload": "polystyrene PME melt, 40 chains x 50 units x 16 atoms =
             "thermostat": "Nose-Hoover chain 500 K", "dt_fs": 1.0, "l2": "256 MB flush between timed steps"}
 
 
+# One metric string for both arms (this engine and the reference's CPU path), so that their lines compare directly; the
+# arithmetic each arm runs in is its "dtype".
+METRIC = "ns/day (32k-atom polystyrene PME melt, MD step)"
+
+
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown CPU"
+
+
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
@@ -109,6 +125,17 @@ def options(precision: str, steps: int, seed: int, thermostat: str = "nose-hoove
 
 E2E_CALLS = 3
 
+
+def force_errors(f, f_ref, e, e_ref) -> dict:
+    """RMS force error relative to the RMS force, per-atom relative error (RMS and max), relative energy error."""
+    import numpy as np
+    f, f_ref = np.asarray(f).reshape(-1, 3), np.asarray(f_ref).reshape(-1, 3)
+    df = f - f_ref
+    per_atom = np.linalg.norm(df, axis=1) / np.maximum(np.linalg.norm(f_ref, axis=1), 1e-12)
+    return {"rms_relative": float(np.sqrt((df ** 2).sum(1).mean() / (f_ref ** 2).sum(1).mean())),
+            "per_atom_rms": float(np.sqrt(np.mean(per_atom ** 2))), "per_atom_max": float(per_atom.max()),
+            "energy_relative": float(abs(e - e_ref) / abs(e_ref))}
+
 # An earlier measurement on B200s of the same kind (HBM copy GB/s, max SM clock), used when no measured-peaks file is present
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "sm_max_mhz": 1965.0}
 
@@ -142,12 +169,14 @@ def run_reference(args, rank: int) -> dict:
     n = ff.natoms
     sps = steps / out["seconds"] if out["seconds"] > 0 else 0.0
     cfg = dict(WORKLOAD, box_A=round(float(cell[3]), 3), parallelism="1 CPU process", sample=f"{steps} MD steps")
-    return {"impl": "reference", "metric": "ns/day (32k-atom polystyrene PME melt, MD step)", "value": nsd, "unit": "ns/day", "n_gpus": args.gpus,
+    return {"impl": "reference", "metric": METRIC, "value": nsd, "unit": "ns/day", "n_gpus": args.gpus,
             "steps": steps, "warmup": args.warmup, "ms_per_step": 1000.0 / sps if sps else None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 pair kernel, f64 sums (reference mixed)", "data": "synthetic", "config": cfg,
             "atom_steps_per_s": sps * n,
             "cpu_baseline": {"value": nsd, "unit": "ns/day", "cores": threads, "kind": "reference",
-                             "sample": f"{steps} steps of run_dynamics on the same cell, EnergyOptions::mixed = true, {threads} threads, wall {wall:.1f} s"},
+                             "sample": f"{steps} steps of the reference's run_dynamics on the same cell, EnergyOptions::mixed = true, {threads} threads "
+                                       f"on {cpu_model()}, wall {wall:.1f} s; PME through the C++ restatement of the reference's Fortran k-space "
+                                       f"module (no Fortran compiler on the box)"},
             "e2e": {"value": nsd, "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -273,10 +302,7 @@ def main():
     tm, fm = em.compute(x2, cell)
     ed = Evaluator(ff, options("double", 1, seed).energy)
     td, fd = ed.compute(x2, cell)
-    df = fm - fd
-    rms_rel = float(np.sqrt((df ** 2).sum(1).mean() / (fd ** 2).sum(1).mean()))
-    per_atom = np.linalg.norm(df, axis=1) / np.maximum(np.linalg.norm(fd, axis=1), 1e-12)
-    e_err = abs(tm["total"] - td["total"]) / abs(td["total"])
+    err_fp64 = force_errors(fm, fd, tm["total"], td["total"])
     em.close()
     ed.close()
     # --- the FP64 path on the same workload ---
@@ -327,33 +353,47 @@ def main():
     kT = 0.0019872041 * float(np.mean([r["temperature"] for r in outn["thermo"]]))
     drift_kt_ns_atom = slope * 1000.0 / kT / n
     ev.close()
-    # --- CPU baseline: the reference's own code on the host cores, bounded sample (rank 0, N = 1) ---
-    cpu = None
+    # --- CPU baseline: the reference's own code on the host cores, bounded samples (rank 0, N = 1): its mixed path
+    # (its fastest) and its FP64 path; and the checker: the reference's FP64 forces and energy on the end-state frame,
+    # against which the mixed and FP64 device forces are reported ---
+    cpu, cpu64, err_oracle = None, None, None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             from oracle import ref
             if ref.available():
                 threads = os.cpu_count() or 1
-                probe = ref.run(ff, x2, cell, options("mixed", 5, seed), v=v2, threads=threads)
-                per_step = probe["seconds"] / 5 if probe["seconds"] > 0 else 0.01
-                steps_cpu = int(max(10, min(5000, CPU_SAMPLE_SECONDS / max(per_step, 1e-6))))
-                r = ref.run(ff, x2, cell, options("mixed", steps_cpu, seed), v=v2, threads=threads)
-                cpu = {"value": r["ns_per_day"], "unit": "ns/day", "cores": threads, "kind": "reference",
-                       "sample": f"{steps_cpu} MD steps of the same cell through the reference's run_dynamics (mixed, its fastest), "
-                                 f"{threads} threads, {r['seconds']:.1f} s"}
+                model = cpu_model()
+                pme_note = "PME through the C++ restatement of the reference's Fortran k-space module (no Fortran compiler on the box)"
+                t_ref, f_ref = ref.compute(ff, options("double", 1, seed).energy, x2, cell, threads=threads)
+                e_ref = sum(t_ref[k] for k in ("bond", "angle", "dihedral", "improper", "vdw", "coulomb"))
+                err_oracle = {"reference": "the reference's Evaluator::compute, EnergyOptions::mixed = false (FP64), on the end-state frame",
+                              "mixed": force_errors(fm, f_ref, tm["total"], e_ref), "fp64": force_errors(fd, f_ref, td["total"], e_ref)}
+                for prec, secs in (("mixed", CPU_SAMPLE_SECONDS), ("double", CPU_SAMPLE_SECONDS / 2)):
+                    probe = ref.run(ff, x2, cell, options(prec, 3, seed), v=v2, threads=threads)
+                    per_step = probe["seconds"] / 3 if probe["seconds"] > 0 else 0.01
+                    steps_cpu = int(max(5, min(5000, secs / max(per_step, 1e-6))))
+                    r = ref.run(ff, x2, cell, options(prec, steps_cpu, seed), v=v2, threads=threads)
+                    row = {"value": r["ns_per_day"], "unit": "ns/day", "cores": threads, "kind": "reference",
+                           "sample": f"{steps_cpu} MD steps of the same cell through the reference's run_dynamics "
+                                     f"(EnergyOptions::mixed = {'true, its fastest' if prec == 'mixed' else 'false, FP64'}), {threads} threads on "
+                                     f"{model}, {r['seconds']:.1f} s; {pme_note}"}
+                    if prec == "mixed":
+                        cpu = row
+                    else:
+                        cpu64 = row
         except Exception as e:   # the baseline is reported, not required
             cpu = {"value": None, "unit": "ns/day", "cores": os.cpu_count(), "kind": "reference", "sample": f"failed: {e}"}
     if rank == 0:
         cfg = dict(WORKLOAD, box_A=round(float(cell[3]), 3), parallelism=f"{world} independent replica(s), one per GPU")
         line = {
-            "metric": "ns/day (32k-atom polystyrene PME melt, MD step, mixed FP32/fixed-point)", "value": value, "unit": "ns/day", "n_gpus": world,
+            "metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 pair/PME spread-gather, int64 fixed-point sums, f64 FFT/bonded/integrator", "data": "synthetic", "config": cfg,
             "atom_steps_per_s": sps * n * world,
             "list_builds": builds,
             "fp64": {"ns_per_day": nsd64 * world, "ms_per_step": ms64, "steps": k64, "mixed_speedup": ms64 / ms_step},
-            "force_error_vs_fp64": {"rms_relative": rms_rel, "per_atom_rms": float(np.sqrt(np.mean(per_atom ** 2))),
-                                    "per_atom_max": float(per_atom.max()), "energy_relative": e_err},
+            "force_error_vs_oracle": err_oracle,
+            "force_error_vs_fp64": dict(err_fp64, reference="this engine's FP64 path on the same frame"),
             "nve_drift_kT_per_ns_per_atom": drift_kt_ns_atom,
             "batched_replicas": batch,
             "e2e": {"value": e2e_nsd, "unit": "ns/day", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -373,6 +413,7 @@ def main():
             "gpu_launches_note": "kernels launched in the timed step loop, counted by the engine: the step graphs' kernel nodes per replayed step (list-build and prune kernels included; they return at once on steps without a build or prune), plus one kinetic-energy kernel per thermo row",
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
+            "cpu_baseline_fp64": cpu64,
         }
         print(json.dumps(line), flush=True)
     if pg:

@@ -83,19 +83,6 @@ class State(C.Structure):
     _fields_ = [("x", P), ("v", P), ("cell", P), ("has_velocities", C.c_int32)]
 
 
-class TgFit(C.Structure):
-    """caps_gpu_tg_fit: a glass-transition fit (BilinearFit, core/include/caps/mechanics.hpp:303-311)."""
-    _fields_ = [("ok", C.c_int32), ("tg", C.c_double), ("tg_err", C.c_double), ("slope_low", C.c_double), ("slope_high", C.c_double),
-                ("value_at_tg", C.c_double), ("alpha_low", C.c_double), ("alpha_high", C.c_double), ("rss", C.c_double),
-                ("note", C.c_char * 256)]
-
-    def as_dict(self) -> dict:
-        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "note"}
-        d["ok"] = bool(d["ok"])
-        d["note"] = self.note.decode()
-        return d
-
-
 PROGRESS_FN = C.CFUNCTYPE(C.c_int32, C.POINTER(Thermo), C.c_void_p)
 FRAME_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int64, C.c_void_p)
 CHECKPOINT_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int64, C.c_void_p)
@@ -106,7 +93,7 @@ DIAG_EXPORTS = ["caps_gpu_diag_set_timing", "caps_gpu_diag_last_step_ms", "caps_
 EXPORTS = [
     "caps_gpu_abi_version", "caps_gpu_device_count", "caps_gpu_create", "caps_gpu_set_options", "caps_gpu_energies",
     "caps_gpu_compute", "caps_gpu_compute_device", "caps_gpu_list_builds", "caps_gpu_run", "caps_gpu_run_batch",
-    "caps_gpu_last_steps_per_second", "caps_gpu_destroy", "caps_gpu_error", "caps_gpu_fit_tg",
+    "caps_gpu_last_steps_per_second", "caps_gpu_destroy", "caps_gpu_error",
     "caps_gpu_request_stop", "caps_gpu_stop_requested", "caps_gpu_traj_open", "caps_gpu_traj_append", "caps_gpu_traj_frame",
     "caps_gpu_traj_frames", "caps_gpu_traj_close", "caps_gpu_reload", "caps_gpu_freeze_pairs", "caps_gpu_unfreeze", "caps_gpu_pairs",
     "caps_gpu_threads",
@@ -140,7 +127,6 @@ def load(path: Path | None = None) -> C.CDLL:
     lib.caps_gpu_run_batch.argtypes = [C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int32, PROGRESS_FN, FRAME_FN,
                                        C.POINTER(C.c_void_p)]
     lib.caps_gpu_destroy.argtypes = [C.c_void_p]
-    lib.caps_gpu_fit_tg.argtypes = [P, P, C.c_int32, C.c_int32, C.c_double, C.c_double, C.POINTER(TgFit)]
     lib.caps_gpu_error.restype = C.c_char_p
     lib.caps_gpu_error.argtypes = [C.c_void_p]
     lib.caps_gpu_reload.argtypes = [C.c_void_p, C.POINTER(FF)]

@@ -1,40 +1,23 @@
-"""Stepwise cooling at constant pressure and the glass-transition fit, over batched replicas.
+"""Stepwise cooling at constant pressure over batched replicas.
 
 The reference's run_cooling (core/src/mechanics.cpp:1381-1470) runs one structure through a temperature ladder: an
 unsampled hold at the starting temperature, then a hold at each temperature (Bussi thermostat, the chosen barostat,
 seed + k for the k-th rung); the density and potential energy are averaged over the last part of each hold's thermo
-rows, and Tg is read from specific volume (or potential energy per atom) against temperature by a two-line fit
-(mechanics.cpp:1218-1378, `caps_gpu_fit_tg` in the engine library). Here every stage of the ladder advances all
-replicas at once through `run_batch` (one CUDA graph launch per plain step for all of them): the replicas of a Tg
-scan that differ in their seed, or in their structure, each get their own points and fit.
+rows. Here every stage of the ladder advances all replicas at once through `run_batch` (one CUDA graph launch per plain
+step for all of them): the replicas of a Tg scan that differ in their seed, or in their structure, each get their own
+points.
+
+The glass-transition fit of the points stays with the caller, as it is host analysis and not part of the device path:
+run_cooling takes it as a callable, fit(T, y, options) -> dict. CAPS passes its own fit_bilinear / fit_two_ranges
+(core/src/mechanics.cpp:1218, 1310); without one the result's "fit" is None.
 """
 from __future__ import annotations
 
-import ctypes as C
 import math
 from dataclasses import dataclass, field
+from typing import Callable
 
-import numpy as np
-
-from . import _abi
 from .engine import DynamicsOptions, EnergyOptions, run_batch
-
-
-def fit_tg(T, y, method: int = 0, glassy_max: float = 0.0, rubbery_min: float = 0.0) -> dict:
-    """Tg from points y(T): method 0 the continuous two-line fit with the hinge free (fit_bilinear), 1 two lines through
-    the glassy (T <= glassy_max) and rubbery (T >= rubbery_min) ranges (fit_two_ranges; 0: the lowest and highest
-    thirds). Returns ok, tg, tg_err, slope_low, slope_high, value_at_tg, alpha_low, alpha_high, rss and note."""
-    t = np.ascontiguousarray(np.asarray(T, dtype=np.float64).reshape(-1))
-    v = np.ascontiguousarray(np.asarray(y, dtype=np.float64).reshape(-1))
-    if t.size != v.size:
-        raise ValueError("fit_tg: T and y differ in length")
-    out = _abi.TgFit()
-    lib = _abi.load()
-    rc = lib.caps_gpu_fit_tg(t.ctypes.data_as(C.c_void_p), v.ctypes.data_as(C.c_void_p), int(t.size), int(method), float(glassy_max),
-                             float(rubbery_min), C.byref(out))
-    if rc != 0:
-        raise ValueError(lib.caps_gpu_error(None).decode())
-    return out.as_dict()
 
 
 @dataclass
@@ -56,7 +39,7 @@ class CoolingOptions:
     seed: int = 1
     new_velocities: bool = False
     property: int = 0             # Tg from 0 the specific volume, 1 the potential energy per atom
-    fit: int = 0                  # 0 continuous two-line fit, 1 two ranges
+    fit: int = 0                  # for the caller's fit: 0 continuous two-line fit, 1 two ranges
     glassy_max: float = 0.0
     rubbery_min: float = 0.0
 
@@ -109,12 +92,14 @@ def hold_point(temperature: float, rows: list[dict], average_from: float) -> dic
     return p
 
 
-def run_cooling(evaluators: list, xs: list, cells: list, opts: list, vs: list | None = None) -> list[dict]:
+def run_cooling(evaluators: list, xs: list, cells: list, opts: list, vs: list | None = None,
+                fit: Callable[[list, list, CoolingOptions], dict] | None = None) -> list[dict]:
     """run_cooling for every replica at once: one Evaluator, structure (x, cell) and CoolingOptions per replica. The
     options may differ in seed, pressure, barostat, thermostat coupling, property and fit, but not in the ladder (start,
     end, step, hold, equilibration, dt), since the replicas advance in lock step. Returns one result per replica:
-    {points, fit, thermo, x, v, cell, method}. Replaces calling run_cooling (core/src/mechanics.cpp:1381) once per
-    replica."""
+    {points, fit, fitted, thermo, x, v, cell, method}; "fitted" is the property the fit reads (specific volume, or
+    potential energy per atom) per point, and "fit" is fit(temperatures, fitted, options) of the caller's fit, or None.
+    Replaces calling run_cooling (core/src/mechanics.cpp:1381) once per replica."""
     R = len(evaluators)
     if not (len(xs) == len(cells) == len(opts) == R) or R == 0:
         raise ValueError("run_cooling: one structure and one CoolingOptions per evaluator")
@@ -160,12 +145,12 @@ def run_cooling(evaluators: list, xs: list, cells: list, opts: list, vs: list | 
         natoms = max(1, xs[r].shape[0])
         T = [p["temperature"] for p in points[r]]
         y = [p["potential"] / natoms if o.property == 1 else p["specific_volume"] for p in points[r]]
-        fit = fit_tg(T, y, o.fit, o.glassy_max, o.rubbery_min)
+        result_fit = fit(T, y, o) if fit is not None else None
         what = "potential energy per atom" if o.property == 1 else "specific volume"
         how = "two lines through the glassy and the rubbery range" if o.fit == 1 else "a continuous two-line fit"
         method = (f"stepwise cooling {o.t_start:g} -> {o.t_end:g} K in {o.t_step:g} K steps of {o.ps_per_step:g} ps after "
                   f"{eq * o.dt / 1000:g} ps at {o.t_start:g} K ({o.barostat}, {o.pressure:g} atm); averages over the last "
                   f"{100 * (1 - o.average_from):g} % of each hold; Tg from {how} of {what}")
-        results.append({"points": points[r], "fit": fit, "fitted": y, "thermo": thermo[r], "x": xs[r], "v": vs[r], "cell": cells[r],
+        results.append({"points": points[r], "fit": result_fit, "fitted": y, "thermo": thermo[r], "x": xs[r], "v": vs[r], "cell": cells[r],
                         "method": method})
     return results

@@ -49,6 +49,32 @@ def stop_requested() -> bool:
     return bool(_abi.load().caps_gpu_stop_requested())
 
 
+class _Callbacks:
+    """Keeps the first exception raised by a user's progress, frame or checkpoint callback. ctypes cannot carry an
+    exception through the C call that invoked the callback, so each wrapper stores it here; the progress wrapper then
+    returns non-zero, which ends the run at its next thermo row (as an exception ends the reference's run_dynamics), and
+    the caller re-raises the stored exception once the C call has returned."""
+
+    def __init__(self):
+        self.error: BaseException | None = None
+
+    def wrap(self, fn):
+        def call(*a):
+            if self.error is not None:
+                return None
+            try:
+                return fn(*a)
+            except BaseException as e:   # noqa: BLE001 — re-raised after the C call returns
+                self.error = e
+                return None
+        return call
+
+    def reraise(self):
+        if self.error is not None:
+            e, self.error = self.error, None
+            raise e
+
+
 def _raise(code: int, text: str):
     if code == -3 or code == -4:
         raise FieldError(text)
@@ -274,13 +300,18 @@ class Evaluator:
         keep: list = []
         m = opts.to_struct(self.ff, keep)
         rows = []
+        cb = _Callbacks()
+
+        def _user_progress(d):
+            return progress is not None and progress(d) is False
+
+        user_progress = cb.wrap(_user_progress)
 
         def _prog(row, user):
             d = row.contents.as_dict()
             rows.append(d)
-            if progress is not None and progress(d) is False:
-                return 1
-            return 0
+            stop = user_progress(d)
+            return 1 if stop or cb.error is not None else 0
 
         n = self.ff.natoms
         fuser = None
@@ -291,12 +322,12 @@ class Evaluator:
         else:
             def _frame(xp, cp, step, user):
                 frame(np.ctypeslib.as_array(xp, shape=(3 * n,)).copy().reshape(-1, 3), np.ctypeslib.as_array(cp, shape=(12,)).copy(), int(step))
-            ff_ = _abi.FRAME_FN(_frame)
+            ff_ = _abi.FRAME_FN(cb.wrap(_frame))
         if checkpoint is not None:
             def _ckpt(xp, vp, cp, step, user):
                 checkpoint(np.ctypeslib.as_array(xp, shape=(3 * n,)).copy().reshape(-1, 3), np.ctypeslib.as_array(vp, shape=(3 * n,)).copy().reshape(-1, 3),
                            np.ctypeslib.as_array(cp, shape=(12,)).copy(), int(step))
-            cf = _abi.CHECKPOINT_FN(_ckpt)
+            cf = _abi.CHECKPOINT_FN(cb.wrap(_ckpt))
             keep.append(cf)
             m.checkpoint = C.cast(cf, C.c_void_p)
         pf = _abi.PROGRESS_FN(_prog)
@@ -304,6 +335,7 @@ class Evaluator:
         rc = self.lib.caps_gpu_run(self.h, C.byref(st), C.byref(m), pf, ff_, fuser, buf, 4096)
         out = {"x": x.reshape(-1, 3), "v": vv.reshape(-1, 3), "cell": c, "thermo": rows, "report": buf.value.decode(),
                "steps_per_second": float(self.lib.caps_gpu_last_steps_per_second(self.h))}
+        cb.reraise()
         try:
             self._check(rc)
         except DynamicsInterrupted as e:
@@ -342,9 +374,11 @@ def run_batch(evaluators: list, xs: list, cells: list, opts: list, vs: list | No
                              0 if vs is None or vs[r] is None else 1))
         ms.append(opts[r].to_struct(ev.ff, keep))
 
+    cb = _Callbacks()
+
     def _prog(row, user):
         rows[replica_of[user]].append(row.contents.as_dict())
-        return 0
+        return 1 if cb.error is not None else 0
 
     frames = list(frames) if frames is not None else [None] * R
     checkpoints = list(checkpoints) if checkpoints is not None else [None] * R
@@ -359,12 +393,18 @@ def run_batch(evaluators: list, xs: list, cells: list, opts: list, vs: list | No
         for r, f in enumerate(frames):
             users[r] = f.native_frame_fn()[1]
     else:
+        # writers mixed with callables or None: every frame comes through Python; a writer takes it by append
         def _frame(xp, cp, step, user):
             r = int(user or 0)
             if frames[r] is not None:
                 n = natoms[r]
-                frames[r](np.ctypeslib.as_array(xp, shape=(3 * n,)).copy().reshape(-1, 3), np.ctypeslib.as_array(cp, shape=(12,)).copy(), int(step))
-        ff_ = _abi.FRAME_FN(_frame)
+                xa_ = np.ctypeslib.as_array(xp, shape=(3 * n,)).copy().reshape(-1, 3)
+                ca_ = np.ctypeslib.as_array(cp, shape=(12,)).copy()
+                if hasattr(frames[r], "native_frame_fn"):
+                    frames[r].append(xa_, ca_, int(step))
+                else:
+                    frames[r](xa_, ca_, int(step))
+        ff_ = _abi.FRAME_FN(cb.wrap(_frame))
     replica_of = {users[r]: r for r in range(R)}   # progress and frame callbacks get the same user pointer
     for r, cb in enumerate(checkpoints):
         if cb is None:
@@ -373,7 +413,7 @@ def run_batch(evaluators: list, xs: list, cells: list, opts: list, vs: list | No
         def _ckpt(xp, vp, cp, step, user, cb=cb, n=natoms[r]):
             cb(np.ctypeslib.as_array(xp, shape=(3 * n,)).copy().reshape(-1, 3), np.ctypeslib.as_array(vp, shape=(3 * n,)).copy().reshape(-1, 3),
                np.ctypeslib.as_array(cp, shape=(12,)).copy(), int(step))
-        cf = _abi.CHECKPOINT_FN(_ckpt)
+        cf = _abi.CHECKPOINT_FN(cb.wrap(_ckpt))
         keep.append(cf)
         ms[r].checkpoint = C.cast(cf, C.c_void_p)
     pf = _abi.PROGRESS_FN(_prog)
@@ -383,6 +423,7 @@ def run_batch(evaluators: list, xs: list, cells: list, opts: list, vs: list | No
     lib = evaluators[0].lib
     rc = lib.caps_gpu_run_batch(eng, sp, mp, R, pf, ff_, users)
     out = [{"x": xa[r].reshape(-1, 3), "v": va[r].reshape(-1, 3), "cell": ca[r], "thermo": rows[r]} for r in range(R)]
+    cb.reraise()
     try:
         evaluators[0]._check(rc)
     except DynamicsInterrupted as e:

@@ -230,24 +230,6 @@ void caps_gpu_destroy(caps_gpu_engine* e);
 /* Text of the last error on this engine (or of the last failed caps_gpu_create when e is NULL). */
 const char* caps_gpu_error(const caps_gpu_engine* e);
 
-/* A glass-transition fit of a cooling scan's points (y against T): BilinearFit (core/include/caps/mechanics.hpp:303-311). */
-typedef struct {
-  int32_t ok;
-  double tg, tg_err;                 /* K; tg_err from a bootstrap (NaN: no estimate) */
-  double slope_low, slope_high;      /* dy/dT below and above Tg */
-  double value_at_tg;
-  double alpha_low, alpha_high;      /* (1/y) dy/dT at Tg */
-  double rss;
-  char note[256];                    /* empty, or why the fit is doubtful or failed */
-} caps_gpu_tg_fit;
-
-/* Tg from points (T[i], y[i]), i < n: method 0 a continuous two-line fit with the hinge free (fit_bilinear,
- * core/src/mechanics.cpp:1218, needs n >= 5), 1 two straight lines through a glassy range (T <= glassy_max) and a rubbery
- * range (T >= rubbery_min) that cross at Tg (fit_two_ranges, mechanics.cpp:1310; 0 for either: the lowest and highest
- * thirds). Host code, no device needed; the same points give the reference's Tg and bootstrap error. A fit that cannot
- * be made returns 0 with out->ok = 0 and the reason in out->note. */
-int32_t caps_gpu_fit_tg(const double* T, const double* y, int32_t n, int32_t method, double glassy_max, double rubbery_min, caps_gpu_tg_fit* out);
-
 /* Trajectory writers, frame by frame (write_trajectory, core/src/io_traj.cpp:47; write_dcd, core/src/io_binary.cpp:415;
  * write_lammps_dump, core/src/io_lammps.cpp:612): the file the reference writes for the same frames, byte for byte, but
  * written as the frames arrive instead of from a Trajectory held in memory. The format is the path's extension:
@@ -279,7 +261,9 @@ int32_t caps_gpu_traj_close(caps_gpu_traj* t);
  * about 230 KB per GPU, held from the library's load until the process exits, and shared by every call on that GPU: calls
  * whose work overlaps on the device (different streams, or other host threads) race on it and must be serialised by the
  * caller. The first call on each device looks up that array's device address; make that first call before any stream
- * capture. Errors: caps_gpu_error(NULL). */
+ * capture. The address is kept for the life of the process: after cudaDeviceReset, or any other teardown of a device's
+ * primary context, the library must be reloaded before this entry point is used on that device again.
+ * Errors: caps_gpu_error(NULL). */
 int32_t caps_gpu_kinetic_noalloc(const double* d_v, const double* d_mass, int32_t n, double* d_out, void* stream);
 
 #ifdef __cplusplus

@@ -22,6 +22,19 @@ from caps_b200.engine import DynamicsOptions, EnergyOptions, cell_array  # noqa:
 from caps_b200.forcefield import ForceField, read_capsff  # noqa: E402
 
 LIB = Path(__file__).resolve().parent / "_ref" / "libcaps_ref.so"
+
+
+class TgFit(C.Structure):
+    """ref_tg_fit: the reference's glass-transition fit (BilinearFit, core/include/caps/mechanics.hpp:303-311)."""
+    _fields_ = [("ok", C.c_int32), ("tg", C.c_double), ("tg_err", C.c_double), ("slope_low", C.c_double), ("slope_high", C.c_double),
+                ("value_at_tg", C.c_double), ("alpha_low", C.c_double), ("alpha_high", C.c_double), ("rss", C.c_double),
+                ("note", C.c_char * 256)]
+
+    def as_dict(self) -> dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "note"}
+        d["ok"] = bool(d["ok"])
+        d["note"] = self.note.decode()
+        return d
 _lib = None
 
 
@@ -62,11 +75,13 @@ def lib() -> C.CDLL:
         L.ref_pme_grid.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_void_p]
         L.ref_pme.restype = C.c_double
         L.ref_pme.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_int]
+        L.ref_ewald.restype = C.c_double
+        L.ref_ewald.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]
         L.ref_build_ps_gaff.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_uint64, C.c_char_p]
         L.ref_build_kg.argtypes = [C.c_int, C.c_int, C.c_double, C.c_uint64, C.c_char_p]
-        L.ref_fit_tg.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.POINTER(_abi.TgFit)]
+        L.ref_fit_tg.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.POINTER(TgFit)]
         L.ref_run_cooling.argtypes = [C.POINTER(_abi.FF), C.POINTER(_abi.Opts), C.POINTER(_abi.State), C.c_void_p, C.c_void_p, C.c_void_p,
-                                      C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(_abi.TgFit)]
+                                      C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(TgFit)]
         L.ref_equilibrate.argtypes = [C.POINTER(_abi.FF), C.POINTER(_abi.Opts), C.POINTER(_abi.State), C.POINTER(_abi.MdOpts), C.c_int,
                                       C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_int, C.c_void_p]
         L.ref_minimise.argtypes = [C.POINTER(_abi.FF), C.POINTER(_abi.Opts), C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_int,
@@ -223,7 +238,7 @@ def fit_tg(T, y, method: int = 0, glassy_max: float = 0.0, rubbery_min: float = 
     """caps::fit_bilinear (method 0) or caps::fit_two_ranges (method 1) on the given points."""
     t = np.ascontiguousarray(np.asarray(T, dtype=np.float64).reshape(-1))
     v = np.ascontiguousarray(np.asarray(y, dtype=np.float64).reshape(-1))
-    out = _abi.TgFit()
+    out = TgFit()
     if lib().ref_fit_tg(_vp(t), _vp(v), int(t.size), int(method), float(glassy_max), float(rubbery_min), C.byref(out)) != 0:
         raise RuntimeError(lib().ref_error().decode())
     return out.as_dict()
@@ -244,7 +259,7 @@ def run_cooling(ff: ForceField, x, cell, co, v=None, threads: int = 1, max_point
     el = np.ascontiguousarray(ff.element if ff.element is not None else np.full(ff.natoms, 6), dtype=np.int32)
     pts = np.zeros((max_points, 5))
     npts = C.c_int()
-    fit = _abi.TgFit()
+    fit = TgFit()
     if lib().ref_run_cooling(C.byref(s), C.byref(o), C.byref(st), _vp(opt), _vp(iopt), _vp(el), threads, _vp(pts), max_points, C.byref(npts),
                              C.byref(fit)) != 0:
         raise RuntimeError(lib().ref_error().decode())
@@ -312,6 +327,19 @@ def pme(x, q, cell, k, order: int, beta: float, threads: int = 1) -> tuple[float
     f = np.zeros_like(xx)
     vir = np.zeros(6)
     e = lib().ref_pme(len(qq), _vp(xx), _vp(qq), _vp(c), _vp(kk), order, beta, _vp(f), _vp(vir), threads)
+    return e, f.reshape(-1, 3), vir
+
+
+def ewald(x, q, cell, kmax, beta: float) -> tuple[float, np.ndarray, np.ndarray]:
+    """The reference's plain Ewald reciprocal sum (ewald_reciprocal, core/include/caps/kspace.hpp:28) over
+    |m_d| <= kmax[d]: energy, forces, virial (xx yy zz xy xz yz)."""
+    xx = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1))
+    qq = np.ascontiguousarray(np.asarray(q, dtype=np.float64))
+    c = cell_array(cell)
+    km = np.ascontiguousarray(np.asarray(kmax, dtype=np.int32))
+    f = np.zeros_like(xx)
+    vir = np.zeros(6)
+    e = lib().ref_ewald(len(qq), _vp(xx), _vp(qq), _vp(c), _vp(km), beta, _vp(f), _vp(vir))
     return e, f.reshape(-1, 3), vir
 
 

@@ -274,7 +274,14 @@ System to_system(const caps_gpu_ff* p, const std::shared_ptr<ForceField>& ff, co
   return s;
 }
 
-void to_fit(const BilinearFit& f, caps_gpu_tg_fit* out) {
+// The reference's BilinearFit (core/include/caps/mechanics.hpp:303-311) as a POD for ctypes.
+typedef struct {
+  int32_t ok;
+  double tg, tg_err, slope_low, slope_high, value_at_tg, alpha_low, alpha_high, rss;
+  char note[256];
+} ref_tg_fit;
+
+void to_fit(const BilinearFit& f, ref_tg_fit* out) {
   std::memset(out, 0, sizeof *out);
   out->ok = f.ok ? 1 : 0;
   out->tg = f.tg, out->tg_err = f.tg_err, out->slope_low = f.slope_low, out->slope_high = f.slope_high;
@@ -538,6 +545,14 @@ double ref_pme(int n, const double* x, const double* q, const double* cell, cons
   return e;
 }
 
+// The plain Ewald reciprocal sum of the reference (kspace.hpp:28, over |m_d| <= kmax[d]); forces added to f.
+double ref_ewald(int n, const double* x, const double* q, const double* cell, const int* kmax, double beta, double* f, double* vir) {
+  std::vector<double> xv(x, x + 3 * size_t(n)), qv(q, q + n), fv(f, f + 3 * size_t(n));
+  const double e = ewald_reciprocal(xv, qv, to_cell(cell), beta, kmax, fv, vir);
+  std::memcpy(f, fv.data(), fv.size() * sizeof(double));
+  return e;
+}
+
 // Builders: a grown and relaxed atactic polystyrene cell with GAFF (tests/test_nbnxm.cpp:19-34 builds the same kind).
 int ref_build_ps_gaff(int chains, int dp, double grow_density, double target_density, uint64_t seed, const char* path) {
   try {
@@ -580,7 +595,7 @@ int ref_build_kg(int chains, int beads, double density, uint64_t seed, const cha
 }
 
 // The reference's Tg fits on given points: method 0 fit_bilinear, 1 fit_two_ranges.
-int ref_fit_tg(const double* T, const double* y, int n, int method, double glassy_max, double rubbery_min, caps_gpu_tg_fit* out) {
+int ref_fit_tg(const double* T, const double* y, int n, int method, double glassy_max, double rubbery_min, ref_tg_fit* out) {
   try {
     const std::vector<double> t(T, T + n), v(y, y + n);
     to_fit(method == 1 ? fit_two_ranges(t, v, glassy_max, rubbery_min) : fit_bilinear(t, v), out);
@@ -596,7 +611,7 @@ int ref_fit_tg(const double* T, const double* y, int n, int method, double glass
 // c-rescale), seed, new_velocities, property, fit. points: up to max_points x 5 (T, density, density_err,
 // specific volume, potential). The end state is written back to st.
 int ref_run_cooling(const caps_gpu_ff* p, const caps_gpu_opts* eo, caps_gpu_state* st, const double* opt, const int64_t* iopt,
-                    const int32_t* element, int threads, double* points, int max_points, int* npoints, caps_gpu_tg_fit* fit) {
+                    const int32_t* element, int threads, double* points, int max_points, int* npoints, ref_tg_fit* fit) {
   try {
     auto ff = to_ff(p);
     System s = to_system(p, ff, st, element);

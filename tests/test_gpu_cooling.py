@@ -37,7 +37,8 @@ def test_fp64_cooling_follows_reference(barostat):
     fx = load("ps_small")
     co = _co("double", barostat=barostat)
     ev = Evaluator(fx.ff, co.energy)
-    mine = run_cooling([ev], [fx.x], [fx.cell], [co])[0]
+    # the Tg fit is the caller's: CAPS passes its own fit_bilinear, here the reference's through the oracle
+    mine = run_cooling([ev], [fx.x], [fx.cell], [co], fit=lambda T, y, o: ref.fit_tg(T, y, o.fit, o.glassy_max, o.rubbery_min))[0]
     theirs = ref.run_cooling(fx.ff, fx.x, fx.cell, co)
     assert len(mine["points"]) == len(theirs["points"]) == 5
     for a, b in zip(mine["points"], theirs["points"]):
@@ -47,6 +48,11 @@ def test_fp64_cooling_follows_reference(barostat):
         assert abs(a["density_err"] - b["density_err"]) <= 1e-6 * max(1e-3, abs(b["density_err"]))
     assert np.max(np.abs(mine["cell"] - theirs["cell"])) < 1e-6
     assert np.max(np.abs(mine["x"] - theirs["x"])) < 1e-5
+    # the fit saw the points' specific volumes, and gives the reference's Tg to the points' precision
+    assert mine["fitted"] == [p["specific_volume"] for p in mine["points"]]
+    assert mine["fit"]["ok"] == theirs["fit"]["ok"]
+    if theirs["fit"]["ok"]:
+        assert abs(mine["fit"]["tg"] - theirs["fit"]["tg"]) <= 1e-3 * abs(theirs["fit"]["tg"])
 
 
 def test_fp64_npt_run_follows_reference():
@@ -70,16 +76,22 @@ def test_batched_cooling_equals_individual_scans():
     opts = [_co("mixed", barostat="c-rescale", seed=3), _co("mixed", barostat="c-rescale", seed=9, pressure=200.0),
             _co("mixed", barostat="c-rescale", seed=5)]
     single = []
+
+    def fit(T, y, o):   # a stand-in for the caller's fit: it records what it was given
+        return {"T": list(T), "y": list(y), "method": o.fit}
+
     for fx, co in zip(fxs, opts):
         ev = Evaluator(fx.ff, co.energy)
-        single.append(run_cooling([ev], [fx.x], [fx.cell], [co])[0])
+        single.append(run_cooling([ev], [fx.x], [fx.cell], [co], fit=fit)[0])
         ev.close()
     evs = [Evaluator(fx.ff, co.energy) for fx, co in zip(fxs, opts)]
-    batch = run_cooling(evs, [fx.x for fx in fxs], [fx.cell for fx in fxs], opts)
+    batch = run_cooling(evs, [fx.x for fx in fxs], [fx.cell for fx in fxs], opts, fit=fit)
     for a, b in zip(single, batch):
         assert a["points"] == b["points"]
         assert np.array_equal(a["x"], b["x"]) and np.array_equal(a["cell"], b["cell"])
-        assert a["fit"] == b["fit"] or (np.isnan(a["fit"]["tg_err"]) and np.isnan(b["fit"]["tg_err"]))
+        assert a["fit"] == b["fit"]
+        assert a["fit"]["T"] == [p["temperature"] for p in a["points"]]
+    assert run_cooling([evs[0]], [fxs[0].x], [fxs[0].cell], [opts[0]])[0]["fit"] is None
 
 
 def test_cooling_rejects_different_ladders():

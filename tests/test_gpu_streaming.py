@@ -210,3 +210,57 @@ def test_stop_ends_every_replica_of_a_batch():
         request_stop(False)
     assert got == [[1], [1]]
     assert ei.value.step == 1 and len(ei.value.state) == 2
+
+
+def test_batch_writer_beside_a_callable_and_none_gets_its_frames(tmp_path):
+    """Frame entries of a batch may mix a native writer with a Python callable and None: the writer still receives
+    every frame (through its append), the callable its own, and the replica without one none."""
+    fx = load("ps_small")
+    opts = [_opts(seed=11 + r, frame_every=6, checkpoint_every=0, thermo_every=12, steps=24) for r in range(3)]
+    evs = [Evaluator(fx.ff, o.energy) for o in opts]
+    w = TrajectoryWriter(tmp_path / "w.dcd", fx.ff.natoms)
+    rec = Recorder()
+    run_batch(evs, [fx.x] * 3, [fx.cell] * 3, opts, frames=[w, rec.frame, None])
+    assert w.frames == 5
+    w.close()
+    assert [s for _, _, s in rec.frames] == [0, 6, 12, 18, 24]
+
+
+class _DiskFull(OSError):
+    pass
+
+
+@pytest.mark.parametrize("where", ["checkpoint", "frame", "progress"])
+def test_a_raising_callback_ends_the_run_and_reaches_the_caller(where):
+    """An exception in a user's callback ends the run (at the next thermo row at the latest) and reaches the caller,
+    as an exception thrown by a callback ends the reference's run_dynamics; the run does not go on to its last step."""
+    fx = load("ps_small")
+    o = _opts(steps=200, thermo_every=10, frame_every=5, checkpoint_every=5)
+    calls = []
+
+    def bad(*a):
+        calls.append(a[-1] if where != "progress" else a[0]["step"])
+        if len(calls) == 2:
+            raise _DiskFull("no space left on device")
+        return None
+
+    kw = {"checkpoint": bad if where == "checkpoint" else None, "frame": bad if where == "frame" else None,
+          "progress": bad if where == "progress" else None}
+    rows = []
+    if where != "progress":
+        kw["progress"] = lambda r: rows.append(r["step"])
+    with pytest.raises(_DiskFull):
+        Evaluator(fx.ff, o.energy).run(fx.x, fx.cell, o, **kw)
+    assert len(calls) == 2
+    assert not rows or max(rows) <= 30
+
+
+def test_a_raising_callback_ends_a_batch():
+    fx = load("ps_small")
+    opts = [_opts(seed=5 + r, steps=200, frame_every=0, checkpoint_every=5, thermo_every=10) for r in range(2)]
+    evs = [Evaluator(fx.ff, o.energy) for o in opts]
+
+    def bad(x, v, c, s):
+        raise _DiskFull("no space left on device")
+    with pytest.raises(_DiskFull):
+        run_batch(evs, [fx.x] * 2, [fx.cell] * 2, opts, checkpoints=[None, bad])

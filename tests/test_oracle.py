@@ -1,5 +1,6 @@
 """The oracle (oracle/_ref: the reference core built from its sources, with the C++ restatement of its Fortran PME) is
 pinned by the reference's own tests and reproduces the committed golden fixtures."""
+import os
 import subprocess
 from pathlib import Path
 
@@ -9,7 +10,7 @@ import pytest
 from tests.fixtures import NAMES, load
 
 ROOT = Path(__file__).resolve().parent.parent
-REF_SRC = Path("/root/reference/tests")
+REF_SRC = Path(os.environ.get("CAPS_REFERENCE_ROOT", "/root/reference")) / "tests"
 
 
 def _ref():
@@ -44,12 +45,24 @@ def test_oracle_reproduces_the_golden_fixture(name):
 
 
 def test_golden_pme_matches_plain_ewald_known_answer():
-    """The reference's PME (through the restatement) on the triclinic fixture agrees with the plain Ewald sum, as the
-    reference's own test requires (energy 1e-4 relative, forces 1e-3 RMS)."""
+    """The reference's PME (through the restatement) on the triclinic fixture (1100 charges) agrees with the reference's
+    plain Ewald sum (converged: kmax 14 and 18 agree), with the acceptance of the reference's own test
+    (tests/test_kspace.cpp:107-158): energy within 1e-4 relative, forces within 1e-3 RMS relative, each virial component
+    within 1e-3 of the energy. On this denser cell that takes a 0.6 Å grid at order 6 (the reference's test cell of 200
+    charges meets it at 0.8 Å); finer grids and higher orders must converge further."""
     ref = _ref()
     fx = load("lj_triclinic")
     beta = ref.ewald_beta(9.0, 1e-5)
-    k = ref.pme_grid(fx.cell, beta, 0.8, 6)
-    e, f, vir = ref.pme(fx.x, fx.ff.charge, fx.cell, k, 6, beta)
-    assert np.isfinite(e) and np.all(np.isfinite(f))
-    assert k == [ref.pme_grid(fx.cell, beta, 0.8, 6)[i] for i in range(3)]
+    ee, fe, ve = ref.ewald(fx.x, fx.ff.charge, fx.cell, [14, 14, 14], beta)
+    errs = []
+    for spacing, order in ((0.8, 6), (0.6, 6), (0.4, 8)):
+        k = ref.pme_grid(fx.cell, beta, spacing, order)
+        ep, fp, vp = ref.pme(fx.x, fx.ff.charge, fx.cell, k, order, beta)
+        errs.append((abs(ep - ee) / abs(ee), float(np.sqrt(((fp - fe) ** 2).sum() / (fe ** 2).sum())), float(np.abs(vp - ve).max())))
+        if spacing == 0.6:
+            assert abs(ep - ee) <= 1e-4 * abs(ee) + 1e-4, (ep, ee)
+            assert errs[-1][1] < 1e-3, errs[-1]
+            assert np.all(np.abs(vp - ve) <= 1e-3 * abs(ee) + 1e-3), (vp, ve)
+    for q in range(3):
+        assert errs[0][q] > errs[1][q] > errs[2][q], errs
+    assert errs[2][0] < 1e-7 and errs[2][1] < 1e-6, errs[2]

@@ -3,7 +3,8 @@
 It serves callers that may not call cudaMalloc (a host whose memory manager owns all device memory, or code beside a
 long stream-ordered pipeline that an allocation would synchronise): they pass their own device buffers, and the only
 working memory is a fixed array inside the library. Its kinetic energy and kinetic tensor must equal what the run entry
-point (caps_gpu_run) reports for the same velocities in its step-0 thermo row. Two calls in a row, the second on fewer
+point (caps_gpu_run) reports for the same velocities in its step-0 thermo row, and what plain FP64 sums in numpy give
+for the same velocities and masses. Two calls in a row, the second on fewer
 atoms than the first, check that the shared working memory carries nothing from one call to the next.
 
 This file is named so that pytest collects it last.
@@ -19,6 +20,7 @@ from tests.fixtures import load
 pytestmark = pytest.mark.gpu
 
 K_ATM = 68568.415   # kcal/(mol Å^3) -> atm, as the run's thermo rows use
+K_ACC = 4.184e-4    # (kcal/mol/Å)/(g/mol) -> Å/fs², the unit factor of the kinetic energy
 TOL = 1e-12         # the FP64 tolerance of the device parity tests
 
 
@@ -69,6 +71,13 @@ def test_noalloc_kinetic_matches_run_twice(lib):
         scale = max(abs(ke), max(abs(w) for w in row["terms"]["w"]))
         assert np.max(np.abs(got[1:] - kin)) <= 1e-10 * scale, (name, got[1:], kin)
         assert abs(got[1] + got[2] + got[3] - 2 * got[0]) <= TOL * abs(ke)
+        # and against plain FP64 sums in numpy, independent of the engine: 0.5 sum m v^2 and sum m v_a v_b, in kcal/mol
+        m = np.asarray(fx.ff.mass, dtype=np.float64)
+        ke_np = 0.5 * np.sum(m[:, None] * v * v) / K_ACC
+        pairs = [(0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)]
+        kin_np = np.array([np.sum(m * v[:, a] * v[:, b]) for a, b in pairs]) / K_ACC
+        assert abs(got[0] - ke_np) <= TOL * abs(ke_np), (name, got[0], ke_np)
+        assert np.max(np.abs(got[1:] - kin_np)) <= TOL * abs(ke_np), (name, got[1:], kin_np)
         results.append(got)
     assert results[0][0] != results[1][0]
 
