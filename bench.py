@@ -82,6 +82,12 @@ class Clocks:
             self.proc = None
         return self
 
+    def wait_first(self, seconds: float = 5.0):
+        """Waits (a few seconds at most) for nvidia-smi's first sample, so that the sampling covers what follows."""
+        t0 = time.perf_counter()
+        while self.proc and not self.rows and time.perf_counter() - t0 < seconds:
+            time.sleep(0.05)
+
     def _read(self):
         for line in self.proc.stdout:
             self.rows.append([c.strip() for c in line.split(",")])
@@ -104,7 +110,9 @@ class Clocks:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for r in load for k in range(4) if r[5 + k].lower().startswith("active")})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
-                "reasons": reasons, "samples": len(load)}
+                "reasons": reasons, "samples": len(load),
+                "window": "from the warm-up to the end of the GPU work (timed steps, end-to-end calls, pair-kernel timing, FP64 and "
+                          "NVE runs); samples with the GPU busy"}
 
 
 def workload():
@@ -150,6 +158,182 @@ def measured_peaks() -> dict:
     return dict(FALLBACK_PEAKS, source="fallback")
 
 
+# --- the other configurations (python bench.py --config NAME): one JSON line each, beside the headline ---------------
+CONFIGS = ("kg", "water", "replicas", "composite")
+
+
+def _timed(ev, x, cell, opts, v=None) -> tuple[float, dict]:
+    """Device ms per step of a run in measurement mode (per-step events, L2 flushed between steps), and its result."""
+    ev.set_timing(FLUSH_BYTES)
+    out = ev.run(x, cell, opts, v=v)
+    ev.set_timing(-1)
+    return ev.last_step_ms(), out
+
+
+def _errors_vs(ff, eo_mixed, eo_fp64, x, cell, oracle: bool) -> dict:
+    """Mixed forces against this engine's FP64 forces on one frame, and against the reference's (oracle) when asked."""
+    from caps_b200 import Evaluator
+    em, ed = Evaluator(ff, eo_mixed), Evaluator(ff, eo_fp64)
+    tm, fm = em.compute(x, cell)
+    td, fd = ed.compute(x, cell)
+    em.close()
+    ed.close()
+    out = {"vs_fp64": force_errors(fm, fd, tm["total"], td["total"])}
+    if oracle:
+        try:
+            from oracle import ref
+            if ref.available():
+                tr, fr = ref.compute(ff, eo_fp64, x, cell, threads=os.cpu_count() or 1)
+                er = sum(tr[k] for k in ("bond", "angle", "dihedral", "improper", "vdw", "coulomb"))
+                out["vs_oracle"] = force_errors(fm, fr, tm["total"], er)
+                out["fp64_vs_oracle"] = force_errors(fd, fr, td["total"], er)
+        except Exception as e:   # the check is reported, not required
+            out["vs_oracle"] = f"failed: {e}"
+    return out
+
+
+def _drift(rows, n) -> float:
+    """NVE drift of the conserved energy, kT per ns per atom, from a linear fit over the thermo rows."""
+    import numpy as np
+    cons = np.array([r["conserved"] for r in rows])
+    tps = np.array([r["time_ps"] for r in rows])
+    slope = float(np.polyfit(tps, cons, 1)[0]) if len(cons) > 2 else 0.0
+    kT = 0.0019872041 * float(np.mean([r["temperature"] for r in rows]))
+    return slope * 1000.0 / kT / n
+
+
+def _line(name: str, n: int, dt: float, ms: float, ms64: float | None, extra: dict) -> dict:
+    sps = 1000.0 / ms
+    line = {"config": name, "metric": f"ns/day ({name})", "unit": "ns/day", "value": sps * dt * 86400e-6, "ms_per_step": ms,
+            "atom_steps_per_s": sps * n, "atoms": n, "dt_fs": dt, "n_gpus": 1, "data": "synthetic",
+            "l2": "256 MB flush between timed steps"}
+    if ms64:
+        line["fp64"] = {"ns_per_day": 1000.0 / ms64 * dt * 86400e-6, "ms_per_step": ms64, "atom_steps_per_s": 1000.0 / ms64 * n,
+                        "mixed_speedup": ms64 / ms}
+    line.update(extra)
+    return line
+
+
+def run_config(args) -> dict:
+    import numpy as np
+
+    from caps_b200 import DynamicsOptions, EnergyOptions, Evaluator, run_batch
+    from caps_b200 import systems as S
+    t_build = time.perf_counter()
+    if args.config == "kg":
+        # Kremer-Grest 100 x 50 beads at 0.85 sigma^-3, sigma = 1 Å, eps = 1 kcal/mol, m = 1 g/mol: tau = 48.888 fs,
+        # dt = 0.01 tau, T* = 1 is 1/kB K, Langevin gamma = 0.5/tau (tau_t = 2 tau)
+        tau = 48.888
+        ff, x, cell = S.kg_melt(100, 50, 0.85, seed=1)
+        kw = dict(cutoff=2.0 ** (1 / 6), skin=0.4, coulomb=False, tail=False)
+        T = 1.0 / 0.0019872041
+        x = S.push_off(ff, x, cell, kw, temperature=T, steps=400, log=log)
+        dyn = lambda prec, steps, seed: DynamicsOptions(dt=0.01 * tau, steps=steps, temperature=T, thermostat="langevin", tau_t=2 * tau,
+                                                        seed=seed, thermo_every=max(steps, 1), energy=EnergyOptions(**kw, precision=prec))
+        dt = 0.01 * tau
+    elif args.config == "water":
+        ff, x, cell = S.spce_water(100000, 0.997, seed=1)
+        kw = dict(cutoff=10.0, skin=2.0, electrostatics="pme", ewald_rtol=1e-5, pme_spacing=1.2, pme_order=4, tail=True)
+        x = S.push_off(ff, x, cell, kw, temperature=300.0, steps=300, log=log)
+        dyn = lambda prec, steps, seed: DynamicsOptions(dt=2.0, steps=steps, temperature=300.0, thermostat="bussi", tau_t=100.0,
+                                                        constraints="h-bonds", seed=seed, thermo_every=max(steps, 1),
+                                                        energy=EnergyOptions(**kw, precision=prec))
+        dt = 2.0
+    elif args.config == "composite":
+        ff, x, cell = S.rubber_composite(1_000_000, sheets=4, units=200, density=0.91, seed=1)
+        kw = dict(cutoff=12.0, skin=2.0, electrostatics="pme", ewald_rtol=1e-5, pme_spacing=1.0, pme_order=4, tail=True)
+        x = S.push_off(ff, x, cell, kw, temperature=300.0, steps=300, log=log)
+        dyn = lambda prec, steps, seed: DynamicsOptions(dt=1.0, steps=steps, temperature=300.0, thermostat="bussi", tau_t=100.0,
+                                                        barostat="c-rescale", pressure=1.0, tau_p=1000.0, barostat_every=10, respa=2,
+                                                        respa_split="pme", seed=seed, thermo_every=max(steps, 1),
+                                                        energy=EnergyOptions(**kw, precision=prec))
+        dt = 1.0
+    elif args.config == "replicas":
+        return run_replicas(args)
+    else:
+        raise SystemExit(f"--config takes one of {', '.join(CONFIGS)}")
+    n = ff.natoms
+    build_s = time.perf_counter() - t_build
+    log(f"[bench] {args.config}: {n} atoms built and pushed off in {build_s:.0f} s")
+    ev = Evaluator(ff, dyn("mixed", 1, 1).energy)
+    out = ev.run(x, cell, dyn("mixed", max(args.warmup, 200), 3))
+    x1, v1, c1 = out["x"], out["v"], out["cell"]
+    ms, out = _timed(ev, x1, c1, dyn("mixed", args.steps, 5), v1)
+    x2, v2, c2 = out["x"], out["v"], out["cell"]
+    ev.close()
+    e64 = Evaluator(ff, dyn("double", 1, 1).energy)
+    e64.run(x1, c1, dyn("double", 20, 3), v=v1)
+    ms64, _ = _timed(e64, x1, c1, dyn("double", max(20, args.steps // 4), 5), v1)
+    e64.close()
+    extra = {"build_s": build_s, "errors_end_frame": _errors_vs(ff, dyn("mixed", 1, 1).energy, dyn("double", 1, 1).energy, x2, c2,
+                                                                 oracle=args.config != "composite" or n <= 1_100_000)}
+    if args.config == "water":
+        # NVE drift of both paths over args.drift_ps picoseconds from the same state (SETTLE, 2 fs)
+        nsteps = int(args.drift_ps * 1000 / dt)
+        drift = {}
+        for prec in ("mixed", "double"):
+            o = dyn(prec, nsteps, 9)
+            o.thermostat = "none"
+            o.thermo_every = max(1, nsteps // 100)
+            e = Evaluator(ff, o.energy)
+            rows = e.run(x2, c2, o, v=v2)["thermo"]
+            e.close()
+            drift[prec] = {"kT_per_ns_per_atom": _drift(rows, n), "ps": args.drift_ps}
+        extra["nve_drift"] = drift
+    if args.config == "composite":
+        extra["density_g_cm3_end"] = float(ff.mass.sum() / 6.02214076e23 / (abs(np.linalg.det(c2[3:].reshape(3, 3))) * 1e-24))
+        extra["run"] = "Bussi 300 K, c-rescale 1 atm every 10 steps, r-RESPA with PME every 2 steps (PME outer, the rest inner at 0.5 fs)"
+    return _line(args.config, n, dt, ms, ms64, extra)
+
+
+def run_replicas(args) -> dict:
+    """64 cis-polyisoprene melts of 4-46 chains x 100 units (5.2k-59.8k atoms), each at its own rung of a 500 -> 150 K
+    ladder (replica k at 500 - 10 (k mod 36) K), Langevin, dt 1 fs, in lock step through run_batch, against one system
+    of the same total size (one melt of all their chains)."""
+    import numpy as np
+
+    from caps_b200 import DynamicsOptions, EnergyOptions, Evaluator, run_batch
+    from caps_b200 import systems as S
+    rng = np.random.default_rng(2024)
+    R = args.replicas_count
+    chains = rng.integers(4, 47, size=R)
+    kw = dict(cutoff=10.0, skin=2.0, electrostatics="pme", ewald_rtol=1e-5, pme_spacing=1.0, pme_order=4, tail=True)
+    t0 = time.perf_counter()
+    systems = [S.polyisoprene_melt(int(c), 100, 0.91, seed=100 + r) for r, c in enumerate(chains)]
+    ffs = [s_[0] for s_ in systems]
+    cells = [s_[2] for s_ in systems]
+    xs = S.push_off_batch(ffs, [s_[1] for s_ in systems], cells, kw, temperature=400.0, steps=300, log=log)
+    temps = [500.0 - 10.0 * (k % 36) for k in range(R)]
+    lang = lambda r, steps, prec="mixed": DynamicsOptions(dt=1.0, steps=steps, temperature=temps[r], thermostat="langevin", tau_t=100.0,
+                                                           seed=11 + r, thermo_every=max(steps, 1), energy=EnergyOptions(**kw, precision=prec))
+    evs = [Evaluator(ff, lang(r, 1).energy) for r, ff in enumerate(ffs)]
+    out = run_batch(evs, xs, cells, [lang(r, max(args.warmup, 100)) for r in range(R)])
+    xs, vs = [o["x"] for o in out], [o["v"] for o in out]
+    run_batch(evs, xs, cells, [lang(r, args.steps) for r in range(R)], vs=vs)
+    batch_sps = evs[0].steps_per_second()
+    for e in evs:
+        e.close()
+    n_total = int(sum(ff.natoms for ff in ffs))
+    # one system of the same size: a melt of all the replicas' chains
+    fb, xb, cb = S.polyisoprene_melt(int(chains.sum()), 100, 0.91, seed=7)
+    xb = S.push_off(fb, xb, cb, kw, temperature=400.0, steps=300, log=log)
+    big = DynamicsOptions(dt=1.0, steps=max(args.warmup, 100), temperature=400.0, thermostat="langevin", tau_t=100.0, seed=3,
+                          thermo_every=max(args.warmup, 100), energy=EnergyOptions(**kw, precision="mixed"))
+    eb = Evaluator(fb, big.energy)
+    ob = eb.run(xb, cb, big)
+    big.steps, big.thermo_every = args.steps, args.steps
+    eb.run(ob["x"], cb, big, v=ob["v"])
+    big_sps = eb.steps_per_second()
+    eb.close()
+    eff = batch_sps * n_total / (big_sps * fb.natoms) if big_sps > 0 else None
+    return {"config": "replicas", "metric": "atom-steps/s (64 uneven polyisoprene replicas, one graph per step)", "unit": "atom-steps/s",
+            "value": batch_sps * n_total, "replicas": R, "atoms_total": n_total, "atoms_min": int(min(ff.natoms for ff in ffs)),
+            "atoms_max": int(max(ff.natoms for ff in ffs)), "ns_per_day_each": batch_sps * 86400e-6, "steps": args.steps,
+            "single_system_atoms": fb.natoms, "single_system_atom_steps_per_s": big_sps * fb.natoms, "efficiency": eff,
+            "ladder": "replica k at 500 - 10 (k mod 36) K, Langevin, dt 1 fs, mixed", "build_s": time.perf_counter() - t0,
+            "timing": "device time over the step loop (CUDA events), L2 not flushed", "data": "synthetic"}
+
+
 def run_reference(args, rank: int) -> dict:
     """The reference's own CPU implementation (oracle/_ref: the reference core built from its sources) on this
     workload: run_dynamics in its fastest form (EnergyOptions::mixed = true), all host threads."""
@@ -191,6 +375,13 @@ def main():
     ap.add_argument("--replicas", type=int, default=8, help="batched-replica measurement with this many replicas (0: skip)")
     ap.add_argument("--profile-pair", type=int, default=0, metavar="LAUNCHES",
                     help="only time the pair kernel LAUNCHES times on the start structure (a small case for ncu captures)")
+    ap.add_argument("--config", default=None, choices=CONFIGS,
+                    help="measure another configuration instead of the headline one: kg (5k-bead Kremer-Grest melt), water (300k-atom "
+                         "SPC/E, NVE drift), replicas (64 uneven polyisoprene melts in lock step), composite (1M-atom rubber/graphene)")
+    ap.add_argument("--drift-ps", type=float, default=100.0, help="NVE drift run length of --config water (ps)")
+    ap.add_argument("--replicas-count", type=int, default=64, help="replicas of --config replicas")
+    ap.add_argument("--profile-phases", type=int, default=0, metavar="LAUNCHES",
+                    help="only time the force evaluation's branches alone and together, and the MD step, in both precisions")
     ap.add_argument("--profile-md", type=int, default=0, metavar="STEPS",
                     help="only run the mixed MD: --warmup steps, then STEPS steps (the command for ncu launch lists)")
     args = ap.parse_args()
@@ -207,6 +398,22 @@ def main():
             ev.close()
         return
 
+    if args.profile_phases:
+        from caps_b200 import Evaluator
+        ff, x, v, cell = workload()
+        for prec in ("mixed", "double"):
+            ev = Evaluator(ff, options(prec, 1, 1).energy)
+            ph = ev.phase_timing(x, cell, launches=args.profile_phases, flush_bytes=FLUSH_BYTES)
+            pt = ev.pair_timing(x, cell, launches=args.profile_phases, flush_bytes=FLUSH_BYTES)
+            o = options(prec, args.warmup, 7)
+            out = ev.run(x, cell, o, v=v)
+            ev.set_timing(FLUSH_BYTES)
+            ev.run(out["x"], cell, options(prec, max(args.steps, 50), 7), v=out["v"])
+            print(json.dumps({"precision": prec, **ph, "pair_ms": pt["avg_ms"], "step_ms": ev.last_step_ms(),
+                              "step_kernels": ev.step_kernels()}), flush=True)
+            ev.close()
+        return
+
     if args.profile_md:
         from caps_b200 import Evaluator
         ff, x, v, cell = workload()
@@ -216,6 +423,10 @@ def main():
         out = ev.run(out["x"], cell, options("mixed", args.profile_md, 7), v=out["v"])
         print(json.dumps({"profile_md": args.profile_md, "report": out["report"], "kernels_run": ev.kernels_run()}), flush=True)
         ev.close()
+        return
+
+    if args.config:
+        print(json.dumps(run_config(args)), flush=True)
         return
 
     if args.impl == "reference":
@@ -257,6 +468,11 @@ def main():
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         return float(t.item())
 
+    # Clocks are sampled from before the warm-up to the end of the GPU work (the K timed steps last milliseconds, less
+    # than the 200 ms sampling period; the samples under load span the timed steps, the end-to-end calls, the FP64 run
+    # and the NVE run)
+    clk = Clocks(local).__enter__()
+    clk.wait_first()
     # --- mixed FP32/fixed-point: warm-up, then K timed steps (events per step, L2 flushed between steps) ---
     o = options("mixed", args.warmup, seed)
     ev = Evaluator(ff, o.energy)
@@ -265,8 +481,7 @@ def main():
     ev.set_timing(FLUSH_BYTES)
     barrier()
     b0 = ev.list_builds()
-    with Clocks(local) as clk:
-        out = ev.run(x1, cell, options("mixed", args.steps, seed), v=v1)
+    out = ev.run(x1, cell, options("mixed", args.steps, seed), v=v1)
     barrier()
     builds = ev.list_builds() - b0
     ms_step = max_over_ranks(ev.last_step_ms())
@@ -279,7 +494,6 @@ def main():
     value = nsd * world                    # whole job: the replicas' simulated time per day
     # --- e2e: the C ABI call with host buffers, wall clock around it; the best of E2E_CALLS calls, since the host is
     # shared and a call's set-up and launches can stall behind other processes ---
-    ev.run(x2, cell, options("mixed", args.steps, seed), v=v2)   # one untimed call first: the clock sampler's exit settles
     walls = []
     for _ in range(E2E_CALLS):
         t0 = time.perf_counter()
@@ -353,6 +567,7 @@ def main():
     kT = 0.0019872041 * float(np.mean([r["temperature"] for r in outn["thermo"]]))
     drift_kt_ns_atom = slope * 1000.0 / kT / n
     ev.close()
+    clk.__exit__(None, None, None)
     # --- CPU baseline: the reference's own code on the host cores, bounded samples (rank 0, N = 1): its mixed path
     # (its fastest) and its FP64 path; and the checker: the reference's FP64 forces and energy on the end-state frame,
     # against which the mixed and FP64 device forces are reported ---

@@ -1,4 +1,4 @@
-// Host side of the bonded terms, 1-4 pairs and excluded-pair corrections: one launch per term kind.
+// Host side of the bonded terms, 1-4 pairs and excluded-pair corrections: every kind in one launch (k_bonded).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -16,40 +16,47 @@ void Engine::bonded_forces(const double* d_x, bool ener, bool vir, int parts) {
   // parts: 1 bonded terms, 2 short-range non-bonded (1-4 pairs; DSF exclusion corrections), 4 long-range (the PME
   // exclusion corrections)
   const bool bonded = (parts & 1) != 0, nonb = (parts & 2) != 0, excl = (parts & (pme_ ? 4 : 2)) != 0;
-  auto nblk = [&](int cnt) { return std::min(blocks_for(size_t(std::max(cnt, 1)), T), dev_sms_ * 4); };
-#define LAUNCH3(K, S, cnt, ...)                                                                                     \
-  do {                                                                                                              \
-    if (ener) { if (vir) K<double, S, true, true><<<nblk(cnt), T, 0, stream_>>>(__VA_ARGS__); else K<double, S, true, false><<<nblk(cnt), T, 0, stream_>>>(__VA_ARGS__); } \
-    else { if (vir) K<double, S, false, true><<<nblk(cnt), T, 0, stream_>>>(__VA_ARGS__); else K<double, S, false, false><<<nblk(cnt), T, 0, stream_>>>(__VA_ARGS__); } \
-  } while (0)
-#define LAUNCHX(S, ...)                                                                                             \
-  do {                                                                                                              \
-    if (ener) { if (vir) k_excl_f64<S, true, true><<<nblk(nx_), T, 0, stream_>>>(__VA_ARGS__); else k_excl_f64<S, true, false><<<nblk(nx_), T, 0, stream_>>>(__VA_ARGS__); } \
-    else { if (vir) k_excl_f64<S, false, true><<<nblk(nx_), T, 0, stream_>>>(__VA_ARGS__); else k_excl_f64<S, false, false><<<nblk(nx_), T, 0, stream_>>>(__VA_ARGS__); } \
-  } while (0)
+  BondedWork W{};
+  int blocks = 0;
+  auto segment = [&](int kind, int cnt) {
+    if (cnt <= 0) return;
+    W.kind[W.nseg] = kind;
+    W.first[W.nseg] = blocks;
+    blocks += std::min(blocks_for(size_t(cnt), T), dev_sms_ * 4);
+    ++W.nseg;
+  };
+  if (bonded) {
+    segment(kBkDihedrals, ndg_);   // the costliest terms first, so that their blocks start first
+    segment(kBkImpropers, nig_);
+    segment(kBkAngles, na_);
+    segment(kBkBonds, nb_);
+    segment(kBkFene, nfene_);
+  }
+  if (nonb) segment(kBkPairs14, np14_);
+  if (excl && coul_) segment(kBkExcl, nx_);
+  if (!W.nseg) return;
+  W.first[W.nseg] = blocks;
+  W.nb = nb_, W.na = na_, W.ndg = ndg_, W.nig = nig_, W.nf = nfene_, W.np14 = np14_, W.nx = nx_;
+  W.bond_ij = d_bond_ij_.p, W.bond_kr = d_bond_kr_.p;
+  W.angle_ijk = d_angle_ijk_.p, W.angle_kt = d_angle_kt_.p;
+  W.dih_grp = d_dih_grp_.p, W.dih_ijkl = d_dih_ijkl_.p, W.dih_vd = d_dih_vd_.p, W.dih_n = d_dih_n_.p;
+  W.imp_grp = d_imp_grp_.p, W.imp_ijkl = d_imp_ijkl_.p, W.imp_vd = d_imp_vd_.p, W.imp_n = d_imp_n_.p;
+  W.fene_ij = d_fene_ij_.p, W.fene_p = d_fene_p_.p, W.counters = d_counters_.p;
+  W.p14_ij = d_p14_ij_.p, W.p14_scale = p14_scaled_ ? d_p14_scale_.p : nullptr, W.lj14 = lj14_, W.type = d_type_.p, W.nt = nt_;
+  W.lj14_tab = d_lj14_.p, W.cap14_tab = opt_.force_cap > 0 ? (const double4*)d_cap14_.p : (const double4*)nullptr, W.lj96 = lj96_ ? 1 : 0;
+  W.X = ExclArgs{d_excl_ij_.p, d_excl_f_.p, d_q_.p, d_gtab_.p, ghi_, rc_, rc_ * rc_, kappa_, dsf_e0_, dsf_f0_, pme_ ? 1 : 0};
   auto run = [&](auto sink) {
     using S = decltype(sink);
-    const S F = sink;
-    if (bonded) {
-      if (nb_) LAUNCH3(k_bonds, S, nb_, nb_, d_bond_ij_.p, d_bond_kr_.p, A, F);
-      if (na_) LAUNCH3(k_angles, S, na_, na_, d_angle_ijk_.p, d_angle_kt_.p, A, F);
-      if (ndg_) LAUNCH3(k_torsions, S, ndg_, ndg_, d_dih_grp_.p, d_dih_ijkl_.p, d_dih_vd_.p, d_dih_n_.p, A, F, int(kEDihedral));
-      if (nig_) LAUNCH3(k_torsions, S, nig_, nig_, d_imp_grp_.p, d_imp_ijkl_.p, d_imp_vd_.p, d_imp_n_.p, A, F, int(kEImproper));
-      if (nfene_) LAUNCH3(k_fene, S, nfene_, nfene_, d_fene_ij_.p, d_fene_p_.p, A, F, d_counters_.p);
-    }
-    if (nonb && np14_)
-      LAUNCH3(k_pairs14, S, np14_, np14_, d_p14_ij_.p, p14_scaled_ ? d_p14_scale_.p : nullptr, lj14_, d_type_.p, nt_, d_lj14_.p,
-              opt_.force_cap > 0 ? (const double4*)d_cap14_.p : (const double4*)nullptr, A, F, lj96_ ? 1 : 0);
-    if (excl && coul_ && nx_) {
-      ExclArgs E{d_excl_ij_.p, d_excl_f_.p, d_q_.p, d_gtab_.p, ghi_, rc_, rc_ * rc_, kappa_, dsf_e0_, dsf_f0_, pme_ ? 1 : 0};
-      LAUNCHX(S, nx_, E, A, F);
+    if (ener) {
+      if (vir) launch_pdl(k_bonded<double, S, true, true>, blocks, T, 0, stream_, W, A, sink);
+      else launch_pdl(k_bonded<double, S, true, false>, blocks, T, 0, stream_, W, A, sink);
+    } else {
+      if (vir) launch_pdl(k_bonded<double, S, false, true>, blocks, T, 0, stream_, W, A, sink);
+      else launch_pdl(k_bonded<double, S, false, false>, blocks, T, 0, stream_, W, A, sink);
     }
   };
   if (mixed_) run(ForceSink<float>{d_F_.p, d_F_.p + n_, d_F_.p + 2 * size_t(n_), d_counters_.p + kCntErr});
   else run(ForceSink<double>{d_Fd_.p, d_Fd_.p + n_, d_Fd_.p + 2 * size_t(n_)});
-#undef LAUNCH3
-#undef LAUNCHX
-  CK(cudaGetLastError());
 }
 
 }  // namespace capsb

@@ -1,4 +1,5 @@
-// K-BOND: bonded terms, 1-4 pairs, the Coulomb corrections of excluded pairs and FENE bonds, one thread per term.
+// K-BOND: bonded terms, 1-4 pairs, the Coulomb corrections of excluded pairs and FENE bonds, one thread per term, all
+// kinds in one launch (k_bonded).
 // Reference: Evaluator::compute's bonded phase (core/src/field.cpp:1863-2283): harmonic bonds (:1986-1995), harmonic
 // angles (:1996-2010), Fourier torsion groups for dihedrals and impropers (:1875-1920, 2011-2018), 1-4 pairs (:2019-2043),
 // excluded-pair electrostatics (:2206-2266), FENE + WCA (:2152-2166). These run in double arithmetic on both paths (the
@@ -58,9 +59,9 @@ template <> __device__ __forceinline__ float rsq<float>(float v) { return sqrtf(
 
 // harmonic bonds: k (r - r0)^2
 template <class R, class S, bool ENER, bool VIR>
-static __global__ void k_bonds(int nb, const uint32_t* __restrict__ ij, const double* __restrict__ kr, BondedArgs A, S F) {
+__device__ __forceinline__ void bonds_body(int blk, int nblk, int nb, const uint32_t* __restrict__ ij, const double* __restrict__ kr, BondedArgs A, S F) {
   Tally<VIR> T;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nb; t += gridDim.x * blockDim.x) {
+  for (int t = blk * blockDim.x + threadIdx.x; t < nb; t += nblk * blockDim.x) {
     const int i = int(ij[2 * t]), j = int(ij[2 * t + 1]);
     R dx, dy, dz;
     sep(A, i, j, dx, dy, dz);
@@ -78,9 +79,9 @@ static __global__ void k_bonds(int nb, const uint32_t* __restrict__ ij, const do
 
 // harmonic angles: kt (theta - theta0)^2, j the vertex
 template <class R, class S, bool ENER, bool VIR>
-static __global__ void k_angles(int na, const uint32_t* __restrict__ ijk, const double* __restrict__ kt0, BondedArgs A, S F) {
+__device__ __forceinline__ void angles_body(int blk, int nblk, int na, const uint32_t* __restrict__ ijk, const double* __restrict__ kt0, BondedArgs A, S F) {
   Tally<VIR> T;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < na; t += gridDim.x * blockDim.x) {
+  for (int t = blk * blockDim.x + threadIdx.x; t < na; t += nblk * blockDim.x) {
     const int i = int(ijk[3 * t]), j = int(ijk[3 * t + 1]), k = int(ijk[3 * t + 2]);
     R ux, uy, uz, vx, vy, vz;
     sep(A, j, i, ux, uy, uz);   // u = x_i - x_j
@@ -110,10 +111,10 @@ static __global__ void k_angles(int na, const uint32_t* __restrict__ ijk, const 
 // Fourier torsion groups: terms [gs[g], gs[g+1]) share one quadruple; v [1 + cos(n phi - delta)], phi IUPAC, cos/sin of
 // n phi by recurrence (field.cpp:1875-1920).
 template <class R, class S, bool ENER, bool VIR>
-static __global__ void k_torsions(int ngroups, const int* __restrict__ gs, const uint32_t* __restrict__ ijkl, const double* __restrict__ vd,
+__device__ __forceinline__ void torsions_body(int blk, int nblk, int ngroups, const int* __restrict__ gs, const uint32_t* __restrict__ ijkl, const double* __restrict__ vd,
                            const int* __restrict__ nn, BondedArgs A, S F, int slot) {
   Tally<VIR> T;
-  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ngroups; g += gridDim.x * blockDim.x) {
+  for (int g = blk * blockDim.x + threadIdx.x; g < ngroups; g += nblk * blockDim.x) {
     const int t0 = gs[g], t1 = gs[g + 1];
     const int i = int(ijkl[4 * t0]), j = int(ijkl[4 * t0 + 1]), k = int(ijkl[4 * t0 + 2]), l = int(ijkl[4 * t0 + 3]);
     R b1x, b1y, b1z, b2x, b2y, b2z, b3x, b3y, b3z;
@@ -174,10 +175,10 @@ static __global__ void k_torsions(int ngroups, const int* __restrict__ gs, const
 // lj: per type pair (eps, sigma^6, the pairs' energy shift or 0, 0); capped: (rcap^2, ecap, fcap, 0). lj96: the class II
 // form eps (2 q^(3/2) - 3 q), q = (s/r)^6 (field.cpp:1471-1475), else 4 eps (q^2 - q).
 template <class R, class S, bool ENER, bool VIR>
-static __global__ void k_pairs14(int np, const uint32_t* __restrict__ ij, const double* __restrict__ scale, double lj14, const int* __restrict__ type, int nt,
+__device__ __forceinline__ void pairs14_body(int blk, int nblk, int np, const uint32_t* __restrict__ ij, const double* __restrict__ scale, double lj14, const int* __restrict__ type, int nt,
                           const double4* __restrict__ lj, const double4* __restrict__ cap, BondedArgs A, S F, int lj96) {
   Tally<VIR> T;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < np; t += gridDim.x * blockDim.x) {
+  for (int t = blk * blockDim.x + threadIdx.x; t < np; t += nblk * blockDim.x) {
     const int i = int(ij[2 * t]), j = int(ij[2 * t + 1]);
     R dx, dy, dz;
     sep(A, i, j, dx, dy, dz);
@@ -232,10 +233,10 @@ __device__ __forceinline__ double erfc_as(double x, double& ex2) {   // Abramowi
 }
 
 template <class S, bool ENER, bool VIR>
-static __global__ void k_excl_f64(int nx, ExclArgs E, BondedArgs A, S F) {
+__device__ __forceinline__ void excl_body(int blk, int nblk, int nx, ExclArgs E, BondedArgs A, S F) {
   Tally<VIR> T;
   const double sp = 2 / sqrt(kPi), kap = E.kappa;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nx; t += gridDim.x * blockDim.x) {
+  for (int t = blk * blockDim.x + threadIdx.x; t < nx; t += nblk * blockDim.x) {
     const int i = int(E.ij[2 * t]), j = int(E.ij[2 * t + 1]);
     if (E.q[i] == 0 || E.q[j] == 0) continue;
     double dx, dy, dz;
@@ -285,9 +286,9 @@ static __global__ void k_excl_f64(int nx, ExclArgs E, BondedArgs A, S F) {
 // FENE (-1/2 K R0^2 ln(1 - (r/R0)^2)) plus WCA below 2^(1/6) sigma (LAMMPS bond fene; field.cpp:2152-2166). A bond
 // stretched to R0 or past raises kErrFene (the reference throws FieldError there).
 template <class R, class S, bool ENER, bool VIR>
-static __global__ void k_fene(int nf, const uint32_t* __restrict__ ij, const double* __restrict__ p, BondedArgs A, S F, int* counters) {
+__device__ __forceinline__ void fene_body(int blk, int nblk, int nf, const uint32_t* __restrict__ ij, const double* __restrict__ p, BondedArgs A, S F, int* counters) {
   Tally<VIR> T;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nf; t += gridDim.x * blockDim.x) {
+  for (int t = blk * blockDim.x + threadIdx.x; t < nf; t += nblk * blockDim.x) {
     const int i = int(ij[2 * t]), j = int(ij[2 * t + 1]);
     R dx, dy, dz;
     sep(A, i, j, dx, dy, dz);
@@ -313,6 +314,50 @@ static __global__ void k_fene(int nf, const uint32_t* __restrict__ ij, const dou
     T.vir(dx, dy, dz, fx, fy, fz);
   }
   T.flush(A, kEBond, ENER);
+}
+
+// All bonded work of one force evaluation in one launch: the grid is cut into segments of blocks, one per term kind, each
+// segment sized to its term count; a block runs the body of its segment's kind over that segment's terms. One launch
+// instead of one per kind keeps the short bonded branch from queuing kernel after kernel beside the pair kernel.
+enum BondedKind { kBkBonds = 0, kBkAngles, kBkDihedrals, kBkImpropers, kBkFene, kBkPairs14, kBkExcl, kBkKinds };
+
+struct BondedWork {
+  int nseg;
+  int kind[kBkKinds];
+  int first[kBkKinds + 1];   // first block of each segment; first[nseg] is the grid size
+  int nb, na, ndg, nig, nf, np14, nx;
+  const uint32_t *bond_ij, *angle_ijk, *dih_ijkl, *imp_ijkl, *fene_ij, *p14_ij;
+  const double *bond_kr, *angle_kt, *dih_vd, *imp_vd, *fene_p, *p14_scale;
+  const int *dih_grp, *dih_n, *imp_grp, *imp_n;
+  int* counters;
+  double lj14;
+  const int* type;
+  int nt, lj96;
+  const double4 *lj14_tab, *cap14_tab;
+  ExclArgs X;
+};
+
+template <class R, class S, bool ENER, bool VIR>
+static __global__ void __launch_bounds__(256) k_bonded(BondedWork W, BondedArgs A, S F) {
+  pdl_begin();
+  int sgm = 0;
+  while (sgm + 1 < W.nseg && int(blockIdx.x) >= W.first[sgm + 1]) ++sgm;
+  const int blk = int(blockIdx.x) - W.first[sgm], nblk = W.first[sgm + 1] - W.first[sgm];
+  switch (W.kind[sgm]) {
+    case kBkBonds: bonds_body<R, S, ENER, VIR>(blk, nblk, W.nb, W.bond_ij, W.bond_kr, A, F); break;
+    case kBkAngles: angles_body<R, S, ENER, VIR>(blk, nblk, W.na, W.angle_ijk, W.angle_kt, A, F); break;
+    case kBkDihedrals:
+      torsions_body<R, S, ENER, VIR>(blk, nblk, W.ndg, W.dih_grp, W.dih_ijkl, W.dih_vd, W.dih_n, A, F, int(kEDihedral));
+      break;
+    case kBkImpropers:
+      torsions_body<R, S, ENER, VIR>(blk, nblk, W.nig, W.imp_grp, W.imp_ijkl, W.imp_vd, W.imp_n, A, F, int(kEImproper));
+      break;
+    case kBkFene: fene_body<R, S, ENER, VIR>(blk, nblk, W.nf, W.fene_ij, W.fene_p, A, F, W.counters); break;
+    case kBkPairs14:
+      pairs14_body<R, S, ENER, VIR>(blk, nblk, W.np14, W.p14_ij, W.p14_scale, W.lj14, W.type, W.nt, W.lj14_tab, W.cap14_tab, A, F, W.lj96);
+      break;
+    default: excl_body<S, ENER, VIR>(blk, nblk, W.nx, W.X, A, F); break;
+  }
 }
 
 }  // namespace capsb

@@ -140,6 +140,7 @@ Engine::Engine(const caps_gpu_ff* ff, const caps_gpu_opts* o) {
 
 Engine::~Engine() {
   if (stream_) cudaStreamSynchronize(stream_);
+  stepper_.reset();
   if (h_counters_) cudaFreeHost(h_counters_);
   if (h_efix_) cudaFreeHost(h_efix_);
   if (h_edbl_) cudaFreeHost(h_edbl_);
@@ -393,8 +394,24 @@ void Engine::setup_options() {
 }
 
 void Engine::set_options(const caps_gpu_opts* o) {
+  drop_run_state();
   opt_ = *o;
   setup_options();
+}
+
+std::string Engine::capture_state() const {
+  std::string k;
+  auto put = [&k](const void* p, size_t bytes) { k.append(static_cast<const char*>(p), bytes); };
+  const unsigned long long epoch = g_buffer_epoch.load(std::memory_order_relaxed);
+  put(&epoch, sizeof epoch);
+  put(&opt_, sizeof opt_);
+  const int flags[] = {mixed_ ? 1 : 0, energies_ ? 1 : 0, list_valid_ ? 1 : 0, green_valid_ ? 1 : 0, frozen_ ? 1 : 0, batch_tuned_ ? 1 : 0,
+                       batch_, lines_x_, lines_y_, lines_z_, nsc_cap_, pk_[0], pk_[1], pk_[2], n_};
+  put(flags, sizeof flags);
+  put(cell_h_, sizeof cell_h_);
+  put(&dcell_, sizeof dcell_);
+  put(&geom_, sizeof geom_);
+  return k;
 }
 
 // The cell: matrices, list geometry (columns about as wide as a cubic 64-atom super-cluster, reach in columns and
@@ -839,6 +856,11 @@ int32_t caps_gpu_diag_pair_timing(caps_gpu_engine* e, const double* x, const dou
                                   double* pairs_in, double* pairs_listed, double* entries) {
   if (!e || !x || !cell || launches < 1) return CAPS_GPU_EINVAL;
   return guard(e, [&] { e->e->time_pair_kernel(x, cell, launches, flush_bytes, avg_ms, pairs_in, pairs_listed, entries); });
+}
+
+int32_t caps_gpu_diag_phase_timing(caps_gpu_engine* e, const double* x, const double* cell, int32_t launches, int64_t flush_bytes, double* ms) {
+  if (!e || !x || !cell || !ms || launches < 1) return CAPS_GPU_EINVAL;
+  return guard(e, [&] { e->e->time_phases(x, cell, launches, flush_bytes, ms); });
 }
 
 const char* caps_gpu_error(const caps_gpu_engine* e) { return e ? e->err.c_str() : g_create_error.c_str(); }

@@ -5,12 +5,14 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <cstdint>
 #include <functional>
 #include <map>
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "caps_gpu.h"
@@ -21,8 +23,17 @@
 namespace capsb {
 
 struct PairArgs;
+struct Stepper;
+struct StepperDeleter {
+  void operator()(Stepper* s) const;   // integrate.cu
+};
 
 inline int blocks_for(size_t n, int threads) { return int(std::max<size_t>(1, (n + size_t(threads) - 1) / size_t(threads))); }
+
+// Bumped whenever any device buffer of the library is allocated or freed. A captured CUDA graph holds buffer addresses,
+// so a run that finds this count unchanged since its step graph was captured (with everything else that shaped the
+// capture) may replay that graph instead of capturing it again.
+inline std::atomic<unsigned long long> g_buffer_epoch{0};
 
 template <class T>
 struct DevBuf {
@@ -33,7 +44,10 @@ struct DevBuf {
   DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      cudaFree(p);
+      g_buffer_epoch.fetch_add(1, std::memory_order_relaxed);
+    }
     p = nullptr;
     n = 0;
   }
@@ -65,6 +79,7 @@ void DevBuf<T>::alloc(size_t count) {
     throw CudaError(std::string("cudaMalloc: ") + cudaGetErrorString(e));
   }
   n = count;
+  g_buffer_epoch.fetch_add(1, std::memory_order_relaxed);
 }
 template <class T>
 void DevBuf<T>::upload(const T* h, size_t count, cudaStream_t s) {
@@ -79,6 +94,25 @@ void DevBuf<T>::zero(cudaStream_t s) {
   const cudaError_t e = cudaMemsetAsync(p, 0, n * sizeof(T), s);
   if (e != cudaSuccess) throw CudaError(std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
 }
+// Launches a kernel with programmatic stream serialisation: it may be launched while the kernel before it in the stream
+// is still running, and waits for it in its pdl_begin() (common.cuh). Captured into a graph, the pair becomes a
+// programmatic dependency edge. Arguments convert to the kernel's parameter types.
+template <class... KP, class... A>
+void launch_pdl(void (*kernel)(KP...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream, A&&... args) {
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+  if (e != cudaSuccess) throw CudaError(std::string("kernel launch: ") + cudaGetErrorString(e));
+}
+
 struct ModelError : std::runtime_error {   // the reference's FieldError and argument errors
   int code;
   ModelError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
@@ -122,10 +156,16 @@ class Engine {
   void set_timing(int64_t flush_bytes) { timing_flush_ = flush_bytes; }
   void time_pair_kernel(const double* x, const double* cell, int launches, int64_t flush_bytes, double* avg_ms, double* pairs_in,
                         double* pairs_listed, double* entries);
+  void time_phases(const double* x, const double* cell, int launches, int64_t flush_bytes, double* ms);
   double last_step_ms_device() const { return last_step_ms_; }
   int graph_kernels() const { return graph_kernels_; }
   long long kernels_run() const { return kernels_run_; }
   std::string err;
+  // Host state that shapes a captured step graph besides the run's own options: the buffer epoch, the options, the
+  // cell, the list and PME set-up and the flags forces() reads while it is captured. Two captures made with the same
+  // state (and the same run options) record the same graph.
+  std::string capture_state() const;
+  void drop_run_state();   // the MD state kept between runs is set up again at the next run
 
   // --- internals used by the step kernels' launcher (integrate.cu) ---
   int n_ = 0, nt_ = 0;
@@ -258,6 +298,9 @@ class Engine {
   long long kernels_run_ = 0;
   DevBuf<unsigned char> d_flush_;
   int dev_sms_ = 148;
+  // The MD state kept between runs (integrate.cu): state and work buffers, pinned scalars, the constraint clusters and
+  // the instantiated step graphs, so that a run on the same engine pays none of their set-up again.
+  std::unique_ptr<Stepper, StepperDeleter> stepper_;
 };
 
 // Independent replicas (one engine each, on the current device) advanced in lock step; integrate.cu.

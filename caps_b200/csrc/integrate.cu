@@ -135,6 +135,7 @@ __device__ __forceinline__ void kick_drift_atom(const KickArgs& K, int i, double
   if (bad) atomicOr(reinterpret_cast<unsigned*>(K.counters + kCntErr), kErrNonFinite);
 }
 __global__ void k_kick_drift(KickArgs K) {
+  pdl_begin();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (K.zero_cw && i < 6) K.sc[kScCW0 + i] = 0;
   if (i >= K.n) return;
@@ -308,6 +309,7 @@ __device__ void settle_water(const ConsArgs& C, int w, double* __restrict__ x, c
 // SHAKE on each cluster (Gauss-Seidel along the reference vectors, tol 1e-8 relative; core/src/constraints.cpp:196-230),
 // then v += (x - x_before) / h when h > 0.
 __global__ void k_shake(ConsArgs C, double* __restrict__ x, const double* __restrict__ x0, double* __restrict__ v, double h, int* counters) {
+  pdl_begin();
   const int cc = blockIdx.x * blockDim.x + threadIdx.x;
   if (cc >= C.ncl) return;
   if (cc < C.e1) return shake_star<1>(C, cc, x, x0, v, h, counters);
@@ -428,6 +430,7 @@ __device__ __forceinline__ void vel_op(const VelOp& op, int g, double* vv, const
 
 // The velocity update alone, one thread per atom (runs without constraints).
 __global__ void k_vel(int n, double* __restrict__ v, const double* __restrict__ invm, const double* sc, VelOp op) {
+  pdl_begin();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double vv[3] = {v[3 * i], v[3 * i + 1], v[3 * i + 2]};
@@ -553,6 +556,7 @@ __device__ void rattle_water(const ConsArgs& C, int wi, const double* __restrict
 }
 
 __global__ void k_scale_v(int n, double* __restrict__ v, const double* __restrict__ sc) {
+  pdl_begin();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= 3 * n) return;
   v[i] *= sc[kScFactor];
@@ -566,7 +570,10 @@ __device__ void step_begin_body(double* sc, double t0, double t1, long long step
   sc[kScTnow] = t;
   sc[kScKtarget] = 0.5 * ndof * kB * t;
 }
-__global__ void k_step_begin(double* sc, double t0, double t1, long long steps, double ndof) { step_begin_body(sc, t0, t1, steps, ndof); }
+__global__ void k_step_begin(double* sc, double t0, double t1, long long steps, double ndof) {
+  pdl_begin();
+  step_begin_body(sc, t0, t1, steps, ndof);
+}
 
 // Nose-Hoover chain over half a step (LAMMPS FixNH::nhc_temp_integrate, as dynamics.cpp:479-508): sets the velocity
 // factor in sc[kScFactor]; the caller scales v by it.
@@ -690,6 +697,7 @@ __device__ void ke_blocks(const KeArgs& A, double e, double t[6]) {
 // The first Nose-Hoover half step of a step, on the kinetic energy the previous step left in sc[kScKE]: its second half
 // set it to the scaled velocities' value, and the velocities have not changed since.
 __global__ void k_nhc_begin(Chain* ch, double* sc, double t0, double t1, long long steps, double ndof, double t_freq, double dt) {
+  pdl_begin();
   step_begin_body(sc, t0, t1, steps, ndof);
   nhc_body(ch, sc, ndof, t_freq, dt);
 }
@@ -701,6 +709,7 @@ __global__ void k_nhc_begin(Chain* ch, double* sc, double t0, double t1, long lo
 // velocities and runs K's thermostat update in its last block (what k_ke does in a launch of its own).
 __global__ void k_vel_rattle(ConsArgs C, int nfree, const int* __restrict__ free_atoms, const double* __restrict__ x, double* __restrict__ v, VelOp op,
                              double h, double* sc, int* counters, KeArgs K) {
+  pdl_begin();
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   double w[6] = {0, 0, 0, 0, 0, 0};
   if (c >= C.ncl && c < C.ncl + nfree) {
@@ -802,6 +811,7 @@ __global__ void k_vel_rattle(ConsArgs C, int nfree, const int* __restrict__ free
 // each block writes its partial sums; the last block to finish adds the partials in block order (deterministic) and
 // runs the scalar update. No block waits on another.
 __global__ void k_ke(KeArgs A) {
+  pdl_begin();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double e = 0, t[6] = {0, 0, 0, 0, 0, 0};
   if (i < A.n) ke_atom(A, i, e, t);
@@ -811,9 +821,11 @@ __global__ void k_ke(KeArgs A) {
 }  // namespace
 
 // ---------------------------------------------------------------------------------------------------------------
+// The MD state of one engine. It is kept by the engine between runs (Engine::stepper_), so that a run pays the set-up of
+// its buffers, pinned scalars, constraint clusters and step graphs only when something they depend on has changed.
 struct Stepper {
   Engine& E;
-  const caps_gpu_md_opts& o;
+  caps_gpu_md_opts o{};   // the current run's options
   int n;
   DevBuf<double> x, v, x0, invm, m, sc, part;
   DevBuf<unsigned> done;       // k_ke's finished-block counter
@@ -836,21 +848,53 @@ struct Stepper {
   double* h_sc = nullptr;
   Chain* h_chain = nullptr;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};   // the captured plain step and thermo step (energies and virial on)
+  std::string graph_key[2];                          // what each was captured with (capture_key)
+  bool graph_valid[2] = {false, false};
   int graph_kernels[2] = {0, 0};
   int nparts = 0;
+  // kept between runs: host velocities, the copies for step 0's trial step, the masses, the constraint set and what it
+  // was built from, the run's timing events
+  std::vector<double> hv;
+  DevBuf<double> xs, vs;
+  bool masses_ready = false;
+  bool cons_built = false, cons_from_positions = false;
+  int cons_flag = -1;
+  std::vector<int8_t> cons_h, cons_o;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
-  Stepper(Engine& e, const caps_gpu_md_opts& md) : E(e), o(md), n(e.n_) {}
+  explicit Stepper(Engine& e) : E(e), n(e.n_) {}
   ~Stepper() {
-    drop_graphs();
+    for (auto& g : graph)
+      if (g) cudaGraphExecDestroy(g);
     if (h_sc) cudaFreeHost(h_sc);
     if (h_chain) cudaFreeHost(h_chain);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
   }
 
   // The constraint set of ConstraintMode::HBonds (core/src/constraints.cpp:40-103): every bond to a hydrogen at its r0
   // (or its present length without one), and rigid waters (an oxygen bonded to exactly two hydrogens: their H-H
   // distance from r0 and theta0). Connected constraints form a cluster, solved by one thread.
   void build_constraints(const double* hx) {
-    if (!o.constraints) return;
+    std::vector<int8_t> hflags, oflags;
+    if (o.constraints && o.is_hydrogen) hflags.assign(o.is_hydrogen, o.is_hydrogen + n);
+    if (o.constraints && o.is_oxygen) oflags.assign(o.is_oxygen, o.is_oxygen + n);
+    // the set depends on the options, the element flags and the force field; on the positions only where a bond has no
+    // usable r0 or a water no angle
+    if (cons_built && !cons_from_positions && cons_flag == o.constraints && hflags == cons_h && oflags == cons_o) return;
+    cons_built = false;
+    cons_from_positions = false;
+    ncons = 0;
+    nfree = 0;
+    C = ConsArgs{};
+    C.invm = invm.p;
+    cons_flag = o.constraints;
+    cons_h = hflags;
+    cons_o = oflags;
+    if (!o.constraints) {
+      cons_built = true;
+      return;
+    }
     const auto& hm = E.h_mass_;
     auto is_h = [&](int a) { return o.is_hydrogen ? o.is_hydrogen[a] != 0 : hm[size_t(a)] < 1.6; };
     auto is_o = [&](int a) { return o.is_oxygen ? o.is_oxygen[a] != 0 : false; };
@@ -860,6 +904,7 @@ struct Stepper {
     std::vector<std::vector<int>> nb(static_cast<size_t>(n));
     for (auto& b : bonds) nb[b[0]].push_back(int(b[1])), nb[b[1]].push_back(int(b[0]));
     auto dist = [&](int i, int j) {
+      cons_from_positions = true;
       double d[3] = {hx[3 * j] - hx[3 * i], hx[3 * j + 1] - hx[3 * i + 1], hx[3 * j + 2] - hx[3 * i + 2]};
       min_image_host(d);
       return std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
@@ -888,6 +933,7 @@ struct Stepper {
         if (int(t[1]) == ox && ((int(t[0]) == a && int(t[2]) == b) || (int(t[0]) == b && int(t[2]) == a))) th = E.hth0_[k];
       }
       if (th < 0) {
+        cons_from_positions = true;
         double u[3] = {hx[3 * a] - hx[3 * ox], hx[3 * a + 1] - hx[3 * ox + 1], hx[3 * a + 2] - hx[3 * ox + 2]};
         double w[3] = {hx[3 * b] - hx[3 * ox], hx[3 * b + 1] - hx[3 * ox + 1], hx[3 * b + 2] - hx[3 * ox + 2]};
         min_image_host(u);
@@ -899,7 +945,10 @@ struct Stepper {
       cs.push_back({a, b, std::sqrt(da * da + db * db - 2 * da * db * std::cos(th))});
     }
     ncons = int(cs.size());
-    if (!ncons) return;
+    if (!ncons) {
+      cons_built = true;
+      return;
+    }
     // clusters: connected components of the constraint graph
     std::vector<int> root(static_cast<size_t>(n));
     for (int i = 0; i < n; ++i) root[size_t(i)] = i;
@@ -1036,6 +1085,7 @@ struct Stepper {
     C.d2 = d2.p;
     C.invm = invm.p;
     CK(cudaStreamSynchronize(E.stream_));
+    cons_built = true;
   }
 
   void min_image_host(double* d) const {
@@ -1048,18 +1098,33 @@ struct Stepper {
     for (int r = 0; r < 3; ++r) d[r] = c.h[r][0] * f[0] + c.h[r][1] * f[1] + c.h[r][2] * f[2];
   }
 
-  void drop_graphs() {
-    for (auto& g : graph)
-      if (g) {
-        cudaGraphExecDestroy(g);
-        g = nullptr;
-      }
+  // The captured steps no longer match the run (new thermostat draws, a rescaled cell): the next launch captures again
+  // and updates the instantiated graph in place.
+  void drop_graphs() { graph_valid[0] = graph_valid[1] = false; }
+
+  // Everything a capture of step() records besides the kernels themselves: the engine's capture state and this run's
+  // scalars and buffers. Equal keys give equal graphs.
+  std::string capture_key(bool thermo) const {
+    std::string k = E.capture_state();
+    auto put = [&k](const void* p, size_t bytes) { k.append(static_cast<const char*>(p), bytes); };
+    const double dv[] = {o.dt, o.temperature, o.temperature_end, o.tau_t, ndof, t_freq};
+    put(dv, sizeof dv);
+    const long long iv[] = {(long long)o.steps, (long long)o.seed, o.thermostat, o.respa, o.respa_split, o.constraints, draws_first,
+                            ncons, nfree, nparts, respa, slow_parts, fast_parts, thermo ? 1 : 0};
+    put(iv, sizeof iv);
+    put(&C, sizeof C);
+    const void* ptrs[] = {x.p, v.p, x0.p, invm.p, m.p, sc.p, part.p, done.p, chain.p, draws.p, free_atoms.p, f_slow.p, f_fast.p};
+    put(ptrs, sizeof ptrs);
+    return k;
   }
 
-  // Replays the step graph (capturing it on first use). Returns its kernel count.
+  // Replays the step graph. It is captured when the run's key differs from the one it was made with; an instantiated
+  // graph is then updated in place (cudaGraphExecUpdate), and instantiated anew only if the update is refused.
+  // Returns its kernel count.
   int launch_step(bool thermo) {
     const int k = thermo ? 1 : 0;
-    if (!graph[k]) {
+    std::string key = capture_key(thermo);
+    if (!graph[k] || !graph_valid[k] || key != graph_key[k]) {
       cudaGraph_t g;
       CK(cudaStreamBeginCapture(E.stream_, cudaStreamCaptureModeThreadLocal));
       step(thermo, thermo);
@@ -1075,10 +1140,23 @@ struct Stepper {
         kernels += ty == cudaGraphNodeTypeKernel;
       }
       graph_kernels[k] = kernels;
-      if (k == 0) E.graph_kernels_ = kernels;
-      CK(cudaGraphInstantiate(&graph[k], g, cudaGraphInstantiateFlagUseNodePriority));
+      bool updated = false;
+      if (graph[k]) {
+        cudaGraphExecUpdateResultInfo info{};
+        updated = cudaGraphExecUpdate(graph[k], g, &info) == cudaSuccess;
+        if (!updated) {
+          (void)cudaGetLastError();   // the refusal is not an error of the run
+          CK(cudaGraphExecDestroy(graph[k]));
+          graph[k] = nullptr;
+        }
+      }
+      if (!updated) CK(cudaGraphInstantiate(&graph[k], g, cudaGraphInstantiateFlagUseNodePriority));
       CK(cudaGraphDestroy(g));
+      // the capture state is read after the capture: step() may have changed host flags it holds
+      graph_key[k] = capture_key(thermo);
+      graph_valid[k] = graph_key[k] == key;
     }
+    if (k == 0) E.graph_kernels_ = graph_kernels[k];
     CK(cudaGraphLaunch(graph[k], E.stream_));
     return graph_kernels[k];
   }
@@ -1106,7 +1184,7 @@ struct Stepper {
     A.tau = o.tau_t;
     return A;
   }
-  void ke_launch(const KeArgs& A) { k_ke<<<nparts, 256, 0, E.stream_>>>(A); }
+  void ke_launch(const KeArgs& A) { launch_pdl(k_ke, nparts, 256, 0, E.stream_, A); }
   void ke(int slot, bool tensor) { ke_launch(ke_args(slot, tensor)); }
   // half kick, then drift with SHAKE; `scale` applies the thermostat's pending factor first
   // kick + drift, then SHAKE; the kick also clears the force evaluation's atom-order sums for the evaluation that
@@ -1114,20 +1192,20 @@ struct Stepper {
   void kick_drift(double hk, double hd, bool scale, bool zero_cw, const double* f = nullptr, const double* f2 = nullptr, double hk2 = 0) {
     KickArgs K{n, x.p, v.p, x0.p, f ? f : E.d_f_.p, invm.p, hk, f2, hk2, hd, sc.p, scale ? 1 : 0, zero_cw ? 1 : 0, E.d_counters_.p,
                E.mixed_ ? E.d_F_.p : nullptr, E.mixed_ ? nullptr : E.d_Fd_.p};
-    k_kick_drift<<<blocks(size_t(n), 256), 256, 0, E.stream_>>>(K);
-    if (ncons) k_shake<<<blocks(size_t(C.ncl), 128), 128, 0, E.stream_>>>(C, x.p, x0.p, v.p, hd, E.d_counters_.p);
+    launch_pdl(k_kick_drift, blocks(size_t(n), 256), 256, 0, E.stream_, K);
+    if (ncons) launch_pdl(k_shake, blocks(size_t(C.ncl), 128), 128, 0, E.stream_, C, x.p, x0.p, v.p, hd, E.d_counters_.p);
     E.sums_cleared_ = true;
   }
   // a velocity update, then RATTLE (constraint virial summed when h > 0); with ke, also the kinetic energy and ke's
   // thermostat update (constraints only: the caller launches k_ke otherwise)
   void vel_rattle(const VelOp& op, double h, const KeArgs* ke = nullptr) {
     if (!ncons) {
-      if (op.kind != 0) k_vel<<<blocks(size_t(n), 256), 256, 0, E.stream_>>>(n, v.p, invm.p, sc.p, op);
+      if (op.kind != 0) launch_pdl(k_vel, blocks(size_t(n), 256), 256, 0, E.stream_, n, v.p, invm.p, sc.p, op);
       return;
     }
     KeArgs K{};
     if (ke) K = *ke;
-    k_vel_rattle<<<blocks(size_t(C.ncl + nfree), 128), 128, 0, E.stream_>>>(C, nfree, free_atoms.p, x.p, v.p, op, h, sc.p, E.d_counters_.p, K);
+    launch_pdl(k_vel_rattle, blocks(size_t(C.ncl + nfree), 128), 128, 0, E.stream_, C, nfree, free_atoms.p, x.p, v.p, op, h, sc.p, E.d_counters_.p, K);
   }
   VelOp kick_op(double hk) const { return VelOp{1, E.d_f_.p, hk, 0, 0, 0, nullptr, 0}; }
   // the kick from the force evaluation's sums (its reduction skipped), storing the forces to E.d_f_
@@ -1148,7 +1226,7 @@ struct Stepper {
   void rattle(double h) {   // RATTLE alone (initial velocities)
     if (ncons) vel_rattle(VelOp{0, nullptr, 0, 0, 0, 0, nullptr, 0}, h);
   }
-  void scale_v() { k_scale_v<<<blocks(size_t(3) * n, 256), 256, 0, E.stream_>>>(n, v.p, sc.p); }
+  void scale_v() { launch_pdl(k_scale_v, blocks(size_t(3) * n, 256), 256, 0, E.stream_, n, v.p, sc.p); }
   // r-RESPA force sets (dynamics.cpp:113-122, 318-326): the non-bonded (slow) and bonded (fast) parts in their own
   // arrays; the evaluation at the end of a step computes both, with energies and virial summed over the two.
   // The PME split puts the reciprocal sum (and its exclusion corrections) in the slow set and every other term in the
@@ -1177,7 +1255,7 @@ struct Stepper {
       // r-RESPA (dynamics.cpp:643-657): outer half kick with the slow forces; `respa` velocity-Verlet steps of dt/respa
       // with the fast ones; outer half kick. Adjacent kicks with the same forces are merged.
       const double h = dt / respa;
-      k_step_begin<<<1, 1, 0, E.stream_>>>(sc.p, o.temperature, o.temperature_end, (long long)o.steps, ndof);
+      launch_pdl(k_step_begin, 1, 1, 0, E.stream_, sc.p, o.temperature, o.temperature_end, (long long)o.steps, ndof);
       kick_drift(0.5 * dt, h, false, true, f_slow.p, f_fast.p, 0.5 * h);
       for (int j = 0; j + 1 < respa; ++j) {
         fast_forces();
@@ -1207,7 +1285,7 @@ struct Stepper {
       forces(ener, vir);
       vel_rattle(kick_op(0.5 * dt), hw);
     } else if (nhc) {
-      k_nhc_begin<<<1, 1, 0, E.stream_>>>(chain.p, sc.p, o.temperature, o.temperature_end, (long long)o.steps, ndof, t_freq, dt);
+      launch_pdl(k_nhc_begin, 1, 1, 0, E.stream_, chain.p, sc.p, o.temperature, o.temperature_end, (long long)o.steps, ndof, t_freq, dt);
       kick_drift(0.5 * dt, dt, true, true);
       KeArgs A = ke_args(kScKE, false);
       A.then = kThenNhc;
@@ -1221,7 +1299,7 @@ struct Stepper {
       }
       scale_v();
     } else {
-      k_step_begin<<<1, 1, 0, E.stream_>>>(sc.p, o.temperature, o.temperature_end, (long long)o.steps, ndof);
+      launch_pdl(k_step_begin, 1, 1, 0, E.stream_, sc.p, o.temperature, o.temperature_end, (long long)o.steps, ndof);
       kick_drift(0.5 * dt, dt, false, true);
       KeArgs A = ke_args(kScKE, false);
       A.then = kThenBussi;
@@ -1238,6 +1316,7 @@ struct Stepper {
   }
 
   // Bussi draws for steps [first, first + count): r1 = gauss, then the chi-squared of ndof - 1 by a fresh Gamma
+  static constexpr long long kDrawChunk = 4096;   // draws made ahead at most (the buffer holds one chunk and one more)
   void make_draws(long long first, long long count) {
     std::vector<double2> d(static_cast<size_t>(count));
     for (long long s = 0; s < count; ++s) {
@@ -1251,6 +1330,13 @@ struct Stepper {
   }
 };
 
+void StepperDeleter::operator()(Stepper* s) const { delete s; }
+
+void Engine::drop_run_state() {
+  if (stream_) CK(cudaStreamSynchronize(stream_));
+  stepper_.reset();
+}
+
 void Engine::validate_md(const caps_gpu_md_opts& o) const {
   if (n_ < 2) throw ModelError(CAPS_GPU_EFIELD, "dynamics needs at least two atoms");
   if (frozen_) throw ModelError(CAPS_GPU_EINVAL, "the pair list is frozen (freeze_pairs): unfreeze it before dynamics");
@@ -1259,7 +1345,6 @@ void Engine::validate_md(const caps_gpu_md_opts& o) const {
   if (o.respa < 0 || o.respa > 16) throw ModelError(CAPS_GPU_EINVAL, "r-RESPA inner steps must be 1 … 16");
   if (o.respa > 1 && (o.thermostat == 2 || o.thermostat == 3)) throw ModelError(CAPS_GPU_EINVAL, "r-RESPA runs with the Bussi thermostat or none");
   if (o.respa > 1 && o.constraints) throw ModelError(CAPS_GPU_EINVAL, "r-RESPA and bond constraints are alternatives: choose one");
-  if (o.respa > 1 && o.barostat) throw ModelError(CAPS_GPU_EINVAL, "the device path runs r-RESPA without a barostat");
   if (o.respa_split != 0 && o.respa_split != 1) throw ModelError(CAPS_GPU_EINVAL, "unknown r-RESPA split");
   if (o.thermostat < 0 || o.thermostat > 3) throw ModelError(CAPS_GPU_EINVAL, "unknown thermostat");
   if (o.barostat != 0 && o.barostat != 1) throw ModelError(CAPS_GPU_EINVAL, "the device path takes stochastic cell rescaling or no barostat");
@@ -1341,17 +1426,29 @@ struct MdRun {
   caps_gpu_progress_fn progress;
   caps_gpu_frame_fn frame;
   void* user;
-  Stepper S;
+  Stepper& S;
   size_t n3;
-  std::vector<double> hv;
+  std::vector<double>& hv;
   int thermo_every = 1, baro_every = 1;
   long long kernels = 0, emits = 0, baro_steps = 0;
   int generation = 0;   // bumped whenever this replica's captured step changes (its graphs are dropped)
   SnapRing snaps;
   long long stopped_at = -1;   // the step a stop ended the run at
+  bool completed = false;      // the run reached its end (or its stop) without an error
 
+  // The engine's kept MD state, made on its first run.
+  static Stepper& kept_state(Engine& e) {
+    if (!e.stepper_) e.stepper_.reset(new Stepper(e));
+    return *e.stepper_;
+  }
   MdRun(Engine& e, caps_gpu_state* state, const caps_gpu_md_opts* md, caps_gpu_progress_fn prog, caps_gpu_frame_fn fr, void* u)
-      : E(e), o(*md), st(state), progress(prog), frame(fr), user(u), S(e, *md), n3(size_t(3) * e.n_) {}
+      : E(e), o(*md), st(state), progress(prog), frame(fr), user(u), S(kept_state(e)), n3(size_t(3) * e.n_), hv(S.hv) {
+    S.o = *md;
+  }
+  // a run that ended in an error may have left its captured steps half-way: the next run captures them again
+  ~MdRun() {
+    if (!completed) S.drop_graphs();
+  }
 
   double host_ke(const std::vector<double>& vv) const {
     double k = 0;
@@ -1449,7 +1546,7 @@ struct MdRun {
   // the reference draws each step's thermostat numbers and then, on a barostat step, the barostat's normal from the
   // same stream (dynamics.cpp:665, 709-711), so the host stream is consumed in that order.
   long long draw_chunk(long long s) const {
-    long long c = std::min<long long>(std::max<long long>(o.steps - s + 1, 1), 4096);
+    long long c = std::min<long long>(std::max<long long>(o.steps - s + 1, 1), Stepper::kDrawChunk);
     if (o.barostat) {
       const long long be = std::max(1, o.barostat_every);
       const long long next = (s + be - 1) / be * be;
@@ -1477,10 +1574,14 @@ void MdRun::start() {
   S.x.upload(st->x, n3, stream_);
   S.x0.alloc(n3);
   S.v.alloc(n3);
-  S.m.upload(E.h_mass_, stream_);
-  std::vector<double> im(static_cast<size_t>(n_));
-  for (int i = 0; i < n_; ++i) im[size_t(i)] = E.h_mass_[size_t(i)] > 0 ? 1.0 / E.h_mass_[size_t(i)] : 0.0;
-  S.invm.upload(im, stream_);
+  if (!S.masses_ready) {   // the masses are the force field's: set once per engine
+    S.m.upload(E.h_mass_, stream_);
+    std::vector<double> im(static_cast<size_t>(n_));
+    for (int i = 0; i < n_; ++i) im[size_t(i)] = E.h_mass_[size_t(i)] > 0 ? 1.0 / E.h_mass_[size_t(i)] : 0.0;
+    S.invm.upload(im, stream_);
+    CK(cudaStreamSynchronize(stream_));
+    S.masses_ready = true;
+  }
   S.sc.alloc(kScNum);
   S.sc.zero(stream_);
   S.chain.alloc(1);
@@ -1489,7 +1590,9 @@ void MdRun::start() {
   S.part.alloc(size_t(7) * std::max(S.nparts, blocks(size_t(n_), 128)));   // k_ke's blocks, or k_vel_rattle's
   S.done.alloc(1);
   S.done.zero(stream_);
+  S.draws.alloc(size_t(Stepper::kDrawChunk) + 1);
   S.respa = std::max(1, o.respa);
+  S.slow_parts = 6, S.fast_parts = 1;
   if (o.respa_split == 1) {
     if (!E.pme_) throw ModelError(CAPS_GPU_EINVAL, "the PME r-RESPA split needs PME electrostatics");
     S.slow_parts = 4, S.fast_parts = 3;
@@ -1498,28 +1601,30 @@ void MdRun::start() {
     S.f_slow.alloc(n3);
     S.f_fast.alloc(n3);
   }
-  CK(cudaMallocHost(&S.h_sc, sizeof(double) * kScNum));
-  CK(cudaMallocHost(&S.h_chain, sizeof(Chain)));
+  if (!S.h_sc) CK(cudaMallocHost(&S.h_sc, sizeof(double) * kScNum));
+  if (!S.h_chain) CK(cudaMallocHost(&S.h_chain, sizeof(Chain)));
   S.nhc = o.thermostat == 3;
   S.bussi = o.thermostat == 1;
   S.langevin = o.thermostat == 2;
   S.t_freq = 1.0 / std::max(o.tau_t, 1e-9);
   S.C.cell = E.dcell_;
   S.build_constraints(st->x);
+  S.C.cell = E.dcell_;
   S.ndof = 3.0 * double(n_) - 3.0 - double(S.ncons);
   if (S.ndof < 1) throw ModelError(CAPS_GPU_EINVAL, "the constraints leave no degree of freedom");
   S.rng = std::make_unique<HostRng>(o.seed);
   if (S.ncons) {   // the constrained lengths hold from the start (dynamics.cpp:198-203)
     CK(cudaMemcpyAsync(S.x0.p, S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
-    k_shake<<<blocks(size_t(S.C.ncl), 128), 128, 0, stream_>>>(S.C, S.x.p, S.x0.p, S.v.p, 0.0, E.d_counters_.p);
+    launch_pdl(k_shake, blocks(size_t(S.C.ncl), 128), 128, 0, stream_, S.C, S.x.p, S.x0.p, S.v.p, 0.0, E.d_counters_.p);
   }
 
   // velocities: given, or Maxwell-Boltzmann from the reference's stream, no centre-of-mass motion, rescaled to T
-  hv.assign(n3, 0.0);
+  hv.resize(n3);
   const bool drawn = !(st->has_velocities && st->v && !o.new_velocities);
   if (!drawn) {
     std::memcpy(hv.data(), st->v, n3 * sizeof(double));
   } else {
+    std::fill(hv.begin(), hv.end(), 0.0);
     for (int i = 0; i < n_; ++i) {
       const double sd = std::sqrt(kB * o.temperature * kAcc / E.h_mass_[size_t(i)]);
       for (int k = 0; k < 3; ++k) hv[3 * size_t(i) + k] = sd * S.rng->gauss();
@@ -1549,7 +1654,8 @@ void MdRun::start() {
   S.forces(true, true);
   if (S.ncons) {
     // step 0's constraint virial from one trial step on copies (dynamics.cpp:582-600)
-    DevBuf<double> xs, vs;
+    DevBuf<double>& xs = S.xs;
+    DevBuf<double>& vs = S.vs;
     xs.alloc(n3);
     vs.alloc(n3);
     CK(cudaMemcpyAsync(xs.p, S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
@@ -1638,7 +1744,7 @@ void MdRun::baro_step(long long s) {
   S.C.cell = E.dcell_;
   if (S.ncons) {
     CK(cudaMemcpyAsync(S.x0.p, S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
-    k_shake<<<blocks(size_t(S.C.ncl), 128), 128, 0, stream_>>>(S.C, S.x.p, S.x0.p, S.v.p, 0.0, E.d_counters_.p);
+    launch_pdl(k_shake, blocks(size_t(S.C.ncl), 128), 128, 0, stream_, S.C, S.x.p, S.x0.p, S.v.p, 0.0, E.d_counters_.p);
     S.rattle(0);
   }
   S.forces(true, true);
@@ -1655,9 +1761,9 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
   const caps_gpu_md_opts& o = *md;
   Stepper& S = R.S;
   const size_t n3 = R.n3;
-  cudaEvent_t ev0, ev1;
-  CK(cudaEventCreate(&ev0));
-  CK(cudaEventCreate(&ev1));
+  if (!S.ev0) CK(cudaEventCreate(&S.ev0));
+  if (!S.ev1) CK(cudaEventCreate(&S.ev1));
+  cudaEvent_t ev0 = S.ev0, ev1 = S.ev1;
   // measurement mode (include/caps_gpu_diag.h): an event pair around every step and an L2 flush between steps
   const bool timed = timing_flush_ >= 0;
   std::vector<cudaEvent_t> tev;
@@ -1703,8 +1809,6 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
   }
   last_step_ms_ = done > 0 ? double(ms) / double(done) : 0.0;
   const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
-  cudaEventDestroy(ev0);
-  cudaEventDestroy(ev1);
   R.sync_scalars();
   last_sps_ = done > 0 && ms > 0 ? double(done) / (ms * 1e-3) : 0.0;
   // state back to the caller
@@ -1723,6 +1827,7 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
                   lines_x_, lines_y_, lines_z_);
     *report = b;
   }
+  R.completed = true;
   if (R.stopped_at >= 0) throw ModelError(CAPS_GPU_ESTOPPED, "stopped at step " + std::to_string(R.stopped_at + o.step_offset) + " (a stop was asked for)");
 }
 
@@ -1737,6 +1842,8 @@ void run_batch(const std::vector<Engine*>& es, caps_gpu_state* const* states, co
   for (size_t r = 0; r < R; ++r) {
     es[r]->validate_md(*mds[r]);
     if (mds[r]->steps != steps) throw ModelError(CAPS_GPU_EINVAL, "the replicas of a batch run the same number of steps");
+    for (size_t q = 0; q < r; ++q)
+      if (es[q] == es[r]) throw ModelError(CAPS_GPU_EINVAL, "each replica of a batch needs its own engine");
   }
   std::vector<std::unique_ptr<MdRun>> runs;
   for (size_t r = 0; r < R; ++r) {
@@ -1856,6 +1963,7 @@ void run_batch(const std::vector<Engine*>& es, caps_gpu_state* const* states, co
     if (M.st->v) CK(cudaMemcpyAsync(M.st->v, M.S.v.p, M.n3 * sizeof(double), cudaMemcpyDeviceToHost, E.stream_));
     CK(cudaStreamSynchronize(E.stream_));
     std::memcpy(M.st->cell, E.cell_h_, sizeof E.cell_h_);
+    M.completed = true;
   }
   if (stopped_at >= 0)
     throw ModelError(CAPS_GPU_ESTOPPED, "stopped at step " + std::to_string(stopped_at + mds[0]->step_offset) + " (a stop was asked for)");

@@ -278,6 +278,16 @@ class Evaluator:
                                                        int(flush_bytes), C.byref(ms), C.byref(pin), C.byref(pl), C.byref(ne)))
         return {"avg_ms": ms.value, "pairs_in_cutoff": pin.value, "pairs_listed": pl.value, "entries": ne.value}
 
+    def phase_timing(self, x, cell, launches: int = 50, flush_bytes: int = 0) -> dict:
+        """The force evaluation's branches timed alone and together, force-only (include/caps_gpu_diag.h): mean ms of
+        the bonded branch, PME, the short-range branch and the whole evaluation."""
+        x = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1))
+        c = cell_array(cell)
+        ms = np.zeros(4)
+        self._check(self.lib.caps_gpu_diag_phase_timing(self.h, x.ctypes.data_as(C.c_void_p), c.ctypes.data_as(C.c_void_p), launches,
+                                                        int(flush_bytes), ms.ctypes.data_as(C.c_void_p)))
+        return dict(zip(("bonded_ms", "pme_ms", "short_range_ms", "forces_ms"), map(float, ms)))
+
     def steps_per_second(self) -> float:
         """Throughput of the last run (or batch this evaluator was part of): steps per second of device time."""
         return float(self.lib.caps_gpu_last_steps_per_second(self.h))

@@ -398,3 +398,375 @@ def tile(ff: ForceField, x, cell, reps=(2, 2, 2)):
     cb[9:12] *= reps[2]
     return big, xb, cb
 
+
+
+# --- cis-1,4-polyisoprene and graphene (the rubber configurations) ---------------------------------------------------
+# OPLS-AA-style classes: CT sp3 carbon, CM sp2 carbon, HC hydrogen on sp3 carbon, HM hydrogen on sp2 carbon, CG graphene
+# carbon (neutral; eps 0.293 kJ/mol, sigma 3.55 Å).
+_PI_LJ = {"CT": (0.066, 3.50), "CM": (0.076, 3.55), "HC": (0.030, 2.50), "HM": (0.030, 2.42), "CG": (0.293 / 4.184, 3.55)}
+_PI_BOND = {("CT", "CT"): (268.0, 1.529), ("CT", "CM"): (317.0, 1.510), ("CM", "CM"): (549.0, 1.340), ("CT", "HC"): (340.0, 1.090),
+            ("CM", "HM"): (340.0, 1.080), ("CG", "CG"): (469.0, 1.420)}
+_PI_ANGLE = {("CT", "CT", "CM"): (63.0, 111.1), ("CT", "CT", "HC"): (37.5, 110.7), ("HC", "CT", "CM"): (35.0, 109.5),
+             ("HC", "CT", "HC"): (33.0, 107.8), ("CT", "CM", "CM"): (70.0, 122.0), ("CT", "CM", "CT"): (70.0, 116.0),
+             ("CM", "CM", "HM"): (35.0, 120.0), ("HM", "CM", "CT"): (35.0, 118.0), ("CG", "CG", "CG"): (63.0, 120.0)}
+# Fourier V1, V2, V3 as in the polystyrene table; torsions not listed carry no term
+_PI_TORS = {("CT", "CM", "CM", "CT"): (0.0, 14.0, 0.0), ("CT", "CM", "CM", "HM"): (0.0, 14.0, 0.0),
+            ("CM", "CM", "CT", "CT"): (0.346, 0.405, -0.940), ("CM", "CM", "CT", "HC"): (0.0, 0.0, -0.372),
+            ("CM", "CT", "CT", "CM"): (1.740, -0.157, 0.279), ("CM", "CT", "CT", "HC"): (0.0, 0.0, 0.300),
+            ("HC", "CT", "CT", "HC"): (0.0, 0.0, 0.300), ("CT", "CM", "CT", "HC"): (0.0, 0.0, 0.300),
+            ("HM", "CM", "CT", "HC"): (0.0, 0.0, 0.300), ("HM", "CM", "CT", "CT"): (0.0, 0.0, 0.300),
+            ("CG", "CG", "CG", "CG"): (0.0, 7.250, 0.0)}
+# charges per position in the unit: CH2 -0.12 / H +0.06, quaternary sp2 C 0, =CH- -0.115 / H +0.115, CH3 -0.18 / H +0.06
+_PI_UNIT_Q = [-0.12, 0.0, -0.115, -0.12, -0.18, 0.06, 0.06, 0.115, 0.06, 0.06, 0.06, 0.06, 0.06]
+_PI_CLASSES = ["CT", "CM", "HC", "HM", "CG"]
+# one repeat unit -CH2-C(CH3)=CH-CH2-: C1 C2 C3 C4 C5(methyl) H1 H1 H3 H4 H4 H5 H5 H5
+_PI_UNIT = ["CT", "CM", "CM", "CT", "CT", "HC", "HC", "HM", "HC", "HC", "HC", "HC", "HC"]
+_PI_UNIT_BONDS = [(0, 1), (1, 2), (2, 3), (1, 4), (0, 5), (0, 6), (2, 7), (3, 8), (3, 9), (4, 10), (4, 11), (4, 12)]
+
+
+def _topology_terms(cls: list[str], bonds: np.ndarray, bond_t: dict, angle_t: dict, tors_t: dict):
+    """Bond, angle and torsion parameters for a molecule from per-atom classes (bonds given); torsions without an
+    entry carry no term."""
+    n = len(cls)
+    nb = _graph(n, bonds)
+    bk = np.array([_key_sym(bond_t, (cls[i], cls[j])) for i, j in bonds], float).reshape(-1, 2)
+    ang = angles_from_bonds(nb)
+    ak = np.array([(lambda p: (p[0], math.radians(p[1])))(_key_sym(angle_t, (cls[i], cls[j], cls[k]))) for i, j, k in ang],
+                  float).reshape(-1, 2)
+    d_ijkl, d_vd, d_n = [], [], []
+    for i, j, k, l in dihedrals_from_bonds(nb, bonds):
+        v = _key_sym(tors_t, (cls[i], cls[j], cls[k], cls[l]))
+        if v is None:
+            continue
+        for nn, (vv, delta) in enumerate(((v[0] / 2, 0.0), (v[1] / 2, math.pi), (v[2] / 2, 0.0)), start=1):
+            if vv != 0.0:
+                d_ijkl.append((i, j, k, l))
+                d_vd.append((vv, delta))
+                d_n.append(nn)
+    off, lst, p14 = exclusions(n, nb)
+    return dict(bond_ij=bonds, bond_k_r0=bk, angle_ijk=ang, angle_kt_theta0=ak, dihedral_ijkl=np.array(d_ijkl, np.uint32).reshape(-1, 4),
+                dihedral_v_delta=np.array(d_vd, float).reshape(-1, 2), dihedral_n=np.array(d_n, np.int32), pair14_ij=p14,
+                excl_offset=off, excl_list=lst)
+
+
+def _replicate(template: dict, natoms: int, copies: int) -> dict:
+    """The terms of `copies` copies of a molecule of `natoms` atoms, each shifted by natoms in index."""
+    out = {}
+    for k in ("bond_ij", "angle_ijk", "dihedral_ijkl", "improper_ijkl", "pair14_ij"):
+        a = np.asarray(template.get(k, np.zeros((0, 2), np.uint32)), dtype=np.int64)
+        out[k] = (a[None] + natoms * np.arange(copies)[:, None, None]).reshape(-1, a.shape[1]).astype(np.uint32) if a.size else a.astype(np.uint32)
+    for k in ("bond_k_r0", "angle_kt_theta0", "dihedral_v_delta", "dihedral_n", "improper_v_delta", "improper_n"):
+        a = np.asarray(template.get(k, np.zeros((0,))))
+        out[k] = np.concatenate([a] * copies) if a.size else a
+    off = np.asarray(template["excl_offset"], dtype=np.int64)
+    lst = np.asarray(template["excl_list"], dtype=np.int64)
+    out["excl_offset"] = np.concatenate([off[:-1] + q * len(lst) for q in range(copies)] + [[copies * len(lst)]]).astype(np.uint32)
+    out["excl_list"] = (lst[None] + natoms * np.arange(copies)[:, None]).reshape(-1).astype(np.uint32)
+    return out
+
+
+def _concat_terms(parts: list[tuple[dict, int]]) -> dict:
+    """Joins the terms of molecules placed one after another (each with its atom count)."""
+    out, base, ebase = {}, 0, 0
+    keys_idx = ("bond_ij", "angle_ijk", "dihedral_ijkl", "improper_ijkl", "pair14_ij")
+    keys_val = ("bond_k_r0", "angle_kt_theta0", "dihedral_v_delta", "dihedral_n", "improper_v_delta", "improper_n")
+    acc = {k: [] for k in keys_idx + keys_val}
+    offs, lsts = [], []
+    for t, n in parts:
+        for k in keys_idx:
+            a = np.asarray(t.get(k, np.zeros((0, 2))), dtype=np.int64)
+            if a.size:
+                acc[k].append(a + base)
+        for k in keys_val:
+            a = np.asarray(t.get(k, np.zeros((0,))))
+            if a.size:
+                acc[k].append(a)
+        off = np.asarray(t["excl_offset"], dtype=np.int64)
+        offs.append(off[:-1] + ebase)
+        lsts.append(np.asarray(t["excl_list"], dtype=np.int64) + base)
+        ebase += int(off[-1])
+        base += n
+    for k in keys_idx:
+        w = {"bond_ij": 2, "pair14_ij": 2, "angle_ijk": 3}.get(k, 4)
+        out[k] = np.concatenate(acc[k]).astype(np.uint32) if acc[k] else np.zeros((0, w), np.uint32)
+    for k in keys_val:
+        out[k] = np.concatenate(acc[k]) if acc[k] else np.zeros((0,))
+    out["excl_offset"] = np.concatenate(offs + [[ebase]]).astype(np.uint32)
+    out["excl_list"] = np.concatenate(lsts).astype(np.uint32)
+    return out
+
+
+def _pi_chain_terms(units: int) -> tuple[list[str], dict]:
+    """Classes and terms of one cis-1,4-polyisoprene chain of `units` repeat units (13 atoms each, chain ends open)."""
+    cls = _PI_UNIT * units
+    bonds = []
+    for u in range(units):
+        o = 13 * u
+        bonds += [(o + a, o + b) for a, b in _PI_UNIT_BONDS]
+        if u > 0:
+            bonds.append((o - 13 + 3, o))   # C4 of the previous unit to C1
+    terms = _topology_terms(cls, np.array(bonds, np.uint32), _PI_BOND, _PI_ANGLE, _PI_TORS)
+    # impropers holding the sp2 carbons planar: C2 (C1, C3; C5) and C3 (C2, C4; H), v [1 + cos(2 phi - pi)], v = 7.5
+    imp = []
+    for u in range(units):
+        o = 13 * u
+        imp += [(o, o + 2, o + 1, o + 4), (o + 1, o + 3, o + 2, o + 7)]
+    terms["improper_ijkl"] = np.array(imp, np.uint32)
+    terms["improper_v_delta"] = np.tile([7.5, math.pi], (len(imp), 1))
+    terms["improper_n"] = np.full(len(imp), 2, np.int32)
+    return cls, terms
+
+
+class _Occupancy:
+    """Counts of placed heavy atoms on a periodic voxel grid, for steering chain growth away from occupied space."""
+
+    def __init__(self, L: float, voxel: float = 2.2):
+        self.n = max(4, int(L / voxel))
+        self.h = L / self.n
+        self.count = np.zeros((self.n,) * 3, np.int32)
+        self.L = L
+
+    def _idx(self, p):
+        return (np.floor(np.mod(p, self.L) / self.h).astype(np.int64)) % self.n
+
+    def add(self, p):
+        i = self._idx(np.asarray(p).reshape(-1, 3))
+        np.add.at(self.count, (i[:, 0], i[:, 1], i[:, 2]), 1)
+
+    def crowding(self, p):
+        """Occupied counts in the 3 x 3 x 3 voxels around each point of p (... x 3)."""
+        shp = p.shape[:-1]
+        i = self._idx(p.reshape(-1, 3))
+        s = np.zeros(len(i), np.int64)
+        for d in ((a, b, c) for a in (-1, 0, 1) for b in (-1, 0, 1) for c in (-1, 0, 1)):
+            j = (i + np.array(d)) % self.n
+            s += self.count[j[:, 0], j[:, 1], j[:, 2]]
+        return s.reshape(shp)
+
+
+def _nerf_v(a, b, c, bond, angle, torsion):
+    """Vectorised _nerf: rows of a, b, c (m x 3); bond, angle, torsion scalars or (m,) arrays."""
+    bc = c - b
+    bc /= np.linalg.norm(bc, axis=-1, keepdims=True)
+    nrm = np.cross(b - a, bc)
+    nrm /= np.linalg.norm(nrm, axis=-1, keepdims=True)
+    m2 = np.cross(nrm, bc)
+    d0 = -bond * np.cos(angle)
+    d1 = bond * np.sin(angle) * np.cos(torsion)
+    d2 = bond * np.sin(angle) * np.sin(torsion)
+    return c + bc * np.asarray(d0)[..., None] + m2 * np.asarray(d1)[..., None] + nrm * np.asarray(d2)[..., None]
+
+
+def _grow_pi_chains(chains: int, units: int, L: float, rng, occ: _Occupancy, tries: int = 8) -> np.ndarray:
+    """Positions (chains, 13 units, 3) of cis-1,4-polyisoprene chains grown together in a periodic cube: every backbone
+    step takes, of `tries` torsions drawn from the allowed states (cis about the double bond), the least crowded."""
+    nb = 4 * units
+    bb = np.zeros((chains, nb, 3))
+    blen = {0: 1.529, 1: 1.510, 2: 1.340, 3: 1.510}                 # bond into backbone atom k, by k % 4
+    bang = {0: 111.1, 1: 111.1, 2: 122.0, 3: 122.0}                 # angle at atom k - 1, by k % 4
+    # seeds: a random point and a random zig-zag of three atoms
+    p0 = rng.uniform(0, L, (chains, 3))
+    d1 = rng.normal(size=(chains, 3))
+    d1 /= np.linalg.norm(d1, axis=1, keepdims=True)
+    perp = np.cross(d1, rng.normal(size=(chains, 3)))
+    perp /= np.linalg.norm(perp, axis=1, keepdims=True)
+    bb[:, 0] = p0
+    bb[:, 1] = p0 + 1.510 * d1
+    t = math.radians(122.0)
+    bb[:, 2] = bb[:, 1] + 1.340 * (-math.cos(t) * d1 + math.sin(t) * perp)
+    prev = bb[:, 0] - 1.529 * (math.cos(math.pi - math.radians(111.1)) * d1 + math.sin(math.pi - math.radians(111.1)) * perp)
+    occ.add(bb[:, :3])
+    for k in range(3, nb):
+        a = bb[:, k - 3] if k >= 3 else prev
+        centre = (k - 2) % 4                                         # the bond (k-2, k-1) the torsion turns about
+        if centre == 1:
+            choices = np.zeros((chains, tries))                      # cis about C2=C3
+        elif centre == 3:
+            choices = rng.choice([math.pi, math.pi / 3, -math.pi / 3], size=(chains, tries), p=[0.6, 0.2, 0.2])
+        else:
+            choices = rng.choice([math.pi, 2 * math.pi / 3, -2 * math.pi / 3], size=(chains, tries))
+        choices = choices + rng.normal(0, math.radians(12), size=(chains, tries)) * (centre != 1)
+        A = np.repeat(a[:, None], tries, 1).reshape(-1, 3)
+        B = np.repeat(bb[:, k - 2, None], tries, 1).reshape(-1, 3)
+        Cc = np.repeat(bb[:, k - 1, None], tries, 1).reshape(-1, 3)
+        cand = _nerf_v(A, B, Cc, blen[k % 4], math.radians(bang[k % 4]), choices.reshape(-1)).reshape(chains, tries, 3)
+        crowd = occ.crowding(cand) + rng.uniform(0, 0.5, (chains, tries))
+        pick = np.argmin(crowd, axis=1)
+        bb[:, k] = cand[np.arange(chains), pick]
+        occ.add(bb[:, k])
+    # side atoms per unit: methyl C5 and the hydrogens, from the local backbone geometry
+    X = np.zeros((chains, units, 13, 3))
+    X[:, :, 0:4] = bb.reshape(chains, units, 4, 3)
+    c1, c2, c3, c4 = (X[:, :, q] for q in range(4))
+    # the neighbours across the unit boundaries; at the chain ends, stand-ins where the chain would continue
+    end = _nerf_v(bb[:, -3], bb[:, -2], bb[:, -1], 1.529, math.radians(111.1), math.pi)
+    prev_c4 = np.concatenate([prev[:, None], c4[:, :-1]], axis=1)
+    next_c1 = np.concatenate([c1[:, 1:], end[:, None]], axis=1)
+
+    def unit(v):
+        return v / np.linalg.norm(v, axis=-1, keepdims=True)
+
+    def planar(centre, n1, n2, length):
+        return centre + length * unit(-(unit(n1 - centre) + unit(n2 - centre)))
+
+    def tetra2(centre, n1, n2, length):
+        u1, u2 = unit(n1 - centre), unit(n2 - centre)
+        bis, nrm = unit(-(u1 + u2)), unit(np.cross(u1, u2))
+        ang = math.radians(54.75)
+        return (centre + length * unit(bis * math.cos(ang) + nrm * math.sin(ang)), centre + length * unit(bis * math.cos(ang) - nrm * math.sin(ang)))
+
+    X[:, :, 4] = planar(c2, c1, c3, 1.510)                         # methyl carbon in the double bond's plane
+    X[:, :, 5], X[:, :, 6] = tetra2(c1, prev_c4, c2, 1.090)
+    X[:, :, 7] = planar(c3, c2, c4, 1.080)
+    X[:, :, 8], X[:, :, 9] = tetra2(c4, c3, next_c1, 1.090)
+    c5 = X[:, :, 4]
+    ax = unit(c5 - c2)
+    ref = unit(np.cross(ax, c1 - c2))
+    ref2 = np.cross(ax, ref)
+    for q, phi in enumerate((0.0, 2 * math.pi / 3, 4 * math.pi / 3)):
+        d = ax * math.cos(math.radians(180 - 109.5)) + math.sin(math.radians(180 - 109.5)) * (ref * math.cos(phi) + ref2 * math.sin(phi))
+        X[:, :, 10 + q] = c5 + 1.090 * unit(d)
+    occ.add(X[:, :, 4])
+    return X
+
+
+def _pair_tables(classes: list[str]):
+    eps = np.array([_PI_LJ[c][0] for c in classes])
+    sig = np.array([_PI_LJ[c][1] for c in classes])
+    return np.sqrt(np.outer(eps, eps)), np.sqrt(np.outer(sig, sig))
+
+
+def _pi_forcefield(n_chain_atoms: list[int], units_per_chain: int, extra: list[tuple[list[str], dict, int]] | None = None) -> ForceField:
+    """The force field of the given polyisoprene chains (one template repeated) followed by other molecules
+    (classes, terms, atoms)."""
+    cls1, t1 = _pi_chain_terms(units_per_chain)
+    parts, cls = [], []
+    nchains = len(n_chain_atoms)
+    rep = _replicate(t1, len(cls1), nchains)
+    parts.append((rep, len(cls1) * nchains))
+    cls += cls1 * nchains
+    for ecls, eterms, en in extra or []:
+        parts.append((eterms, en))
+        cls += ecls
+    terms = _concat_terms(parts)
+    tidx = np.array([_PI_CLASSES.index(c) for c in cls], np.int32)
+    pe, ps = _pair_tables(_PI_CLASSES)
+    q = np.concatenate([np.tile(_PI_UNIT_Q, units_per_chain * nchains), np.zeros(len(cls) - 13 * units_per_chain * nchains)])
+    mass = np.array([M_C if c in ("CT", "CM", "CG") else M_H for c in cls])
+    el = np.array([6 if c in ("CT", "CM", "CG") else 1 for c in cls], np.int32)
+    return ForceField(type_index=tidx, charge=q, mass=mass, pair_eps=pe, pair_sigma=ps, lj14=0.5, coul14=0.5, element=el, **terms)
+
+
+def polyisoprene_melt(chains: int, units: int = 100, density: float = 0.91, seed: int = 1) -> tuple[ForceField, np.ndarray, np.ndarray]:
+    """cis-1,4-polyisoprene, `chains` x `units` repeat units of 13 atoms (-CH2-C(CH3)=CH-CH2-: 5 C + 8 H; chain ends
+    open), OPLS-AA-style (geometric mixing, 1-4 at 0.5; CH2 -0.12 / H +0.06, =CH- -0.115 / +0.115 on its H, the
+    quaternary sp2 C 0, CH3 -0.18 / H +0.06: every unit neutral), grown at `density` g/cm^3 in a cubic periodic box.
+    Returns (force field, x [n, 3], cell[12]); the overlaps a dense growth leaves are pushed off on the device."""
+    rng = np.random.default_rng(seed)
+    mass_unit = 5 * M_C + 8 * M_H
+    L = (chains * units * mass_unit / (density * NA) * 1e24) ** (1.0 / 3.0)
+    occ = _Occupancy(L)
+    X = _grow_pi_chains(chains, units, L, rng, occ)
+    ff = _pi_forcefield([13 * units] * chains, units)
+    cell = np.array([0, 0, 0, L, 0, 0, 0, L, 0, 0, 0, L], float)
+    return ff, X.reshape(-1, 3), cell
+
+
+def graphene_sheet(lx: float = 100.0, ly: float = 100.0, cc: float = 1.42) -> tuple[np.ndarray, np.ndarray]:
+    """A flat honeycomb flake in the xy plane (rectangular cell sqrt(3) cc x 3 cc with four atoms, repeated to about
+    lx x ly, edges left open), and its C-C bonds. Returns (positions [n, 3], bonds [m, 2])."""
+    from scipy.spatial import cKDTree
+    a, h = math.sqrt(3.0) * cc, 3.0 * cc
+    nx, ny = max(3, int(round(lx / a))), max(2, int(round(ly / h)))
+    basis = np.array([[0, 0], [a / 2, cc / 2], [a / 2, 1.5 * cc], [0, 2 * cc]])
+    ij = np.array([(i, j) for i in range(nx) for j in range(ny)], float)
+    xy = (ij[:, None, :] * np.array([a, h]) + basis[None]).reshape(-1, 2)
+    x = np.concatenate([xy, np.zeros((len(xy), 1))], axis=1)
+    pairs = np.array(sorted(cKDTree(x).query_pairs(1.15 * cc)), np.uint32).reshape(-1, 2)
+    return x, pairs
+
+
+def rubber_composite(natoms: int = 1_000_000, sheets: int = 4, units: int = 200, density: float = 0.91, seed: int = 1,
+                     sheet_size: float = 100.0) -> tuple[ForceField, np.ndarray, np.ndarray]:
+    """cis-1,4-polyisoprene chains of `units` repeat units packed around `sheets` neutral graphene flakes (about
+    sheet_size x sheet_size Å, eps 0.293 kJ/mol, sigma 3.55 Å, bonded with angle and planarity terms) at `density`
+    g/cm^3, about `natoms` atoms in all. The sheets lie flat at evenly spaced heights, alternately centred on two
+    diagonal points of the cell; the chains grow around them. Returns (force field, x, cell)."""
+    rng = np.random.default_rng(seed)
+    gx, gb = graphene_sheet(sheet_size, sheet_size)
+    ng = len(gx)
+    chains = max(1, int(round((natoms - sheets * ng) / (13 * units))))
+    mass = chains * units * (5 * M_C + 8 * M_H) + sheets * ng * M_C
+    L = (mass / (density * NA) * 1e24) ** (1.0 / 3.0)
+    occ = _Occupancy(L)
+    sheet_x = []
+    centre = gx[:, :2].mean(0)
+    for s in range(sheets):
+        c2 = (np.array([0.25, 0.25]) if s % 2 == 0 else np.array([0.75, 0.75])) * L
+        z = (s + 0.5) * L / sheets
+        p = gx.copy()
+        p[:, :2] += c2 - centre
+        p[:, 2] = z
+        sheet_x.append(p)
+        occ.add(p)
+        occ.add(p + np.array([0, 0, 1.7]))    # keep chains a van der Waals radius off the faces
+        occ.add(p - np.array([0, 0, 1.7]))
+    X = _grow_pi_chains(chains, units, L, rng, occ)
+    # graphene terms: bonds, angles, ring torsions (planarity), no charges
+    gcls = ["CG"] * ng
+    gterms = _topology_terms(gcls, gb, _PI_BOND, _PI_ANGLE, _PI_TORS)
+    gterms_all = _replicate(gterms, ng, sheets)
+    ff = _pi_forcefield([13 * units] * chains, units, extra=[(gcls * sheets, gterms_all, ng * sheets)])
+    x = np.concatenate([X.reshape(-1, 3)] + sheet_x)
+    cell = np.array([0, 0, 0, L, 0, 0, 0, L, 0, 0, 0, L], float)
+    return ff, x, cell
+
+
+def push_off(ff: ForceField, x, cell, energy_kw: dict, temperature: float = 300.0, steps: int = 600,
+             caps=(5.0, 20.0, 100.0, 500.0), log=None) -> np.ndarray:
+    """Removes the overlaps a dense growth leaves: FP64 Langevin dynamics (dt 0.5 fs) under an LJ force cap raised stage
+    by stage with Coulomb off, then one stage at the last cap with Coulomb on (the reference's relax push-off does the
+    same with its force caps). energy_kw: the EnergyOptions fields of the run (cut-off, electrostatics ...). Returns x."""
+    from .engine import DynamicsOptions, EnergyOptions, Evaluator
+    stages = [(c, False) for c in caps] + [(caps[-1], True)]
+    ev = None
+    for k, (cap, coul) in enumerate(stages):
+        eo = EnergyOptions(**{**energy_kw, "coulomb": coul and energy_kw.get("coulomb", True), "precision": "double", "force_cap": cap})
+        o = DynamicsOptions(dt=0.5, steps=steps, temperature=temperature, thermostat="langevin", tau_t=20.0, thermo_every=steps,
+                            seed=7 + k, energy=eo, new_velocities=True)
+        if ev is None:
+            ev = Evaluator(ff, eo)
+        else:
+            ev.set_options(eo)
+        out = ev.run(x, cell, o)
+        x = out["x"]
+        if log:
+            log(f"push-off cap {cap:6.0f} coulomb {coul}: T {out['thermo'][-1]['temperature']:.0f} K, E {out['thermo'][-1]['potential']:.0f} kcal/mol")
+    ev.close()
+    return x
+
+
+def push_off_batch(ffs: list, xs: list, cells: list, energy_kw: dict, temperature: float = 300.0, steps: int = 600,
+                   caps=(5.0, 20.0, 100.0, 500.0), log=None) -> list:
+    """push_off for independent systems at once: every stage one run_batch over all of them."""
+    from .engine import DynamicsOptions, EnergyOptions, Evaluator, run_batch
+    stages = [(c, False) for c in caps] + [(caps[-1], True)]
+    evs = []
+    xs = [np.asarray(x, dtype=np.float64).reshape(-1, 3) for x in xs]
+    for k, (cap, coul) in enumerate(stages):
+        eo = EnergyOptions(**{**energy_kw, "coulomb": coul and energy_kw.get("coulomb", True), "precision": "double", "force_cap": cap})
+        opts = [DynamicsOptions(dt=0.5, steps=steps, temperature=temperature, thermostat="langevin", tau_t=20.0, thermo_every=steps,
+                                seed=7 + k + 1000 * r, energy=eo, new_velocities=True) for r in range(len(ffs))]
+        if not evs:
+            evs = [Evaluator(ff, eo) for ff in ffs]
+        else:
+            for ev in evs:
+                ev.set_options(eo)
+        out = run_batch(evs, xs, cells, opts)
+        xs = [o["x"] for o in out]
+        if log:
+            log(f"push-off cap {cap:6.0f} coulomb {coul}: {len(ffs)} systems, mean T "
+                f"{np.mean([o['thermo'][-1]['temperature'] for o in out]):.0f} K")
+    for ev in evs:
+        ev.close()
+    return xs

@@ -29,6 +29,12 @@ int64_t caps_gpu_diag_kernels_run(const caps_gpu_engine* e);
 int32_t caps_gpu_diag_pair_timing(caps_gpu_engine* e, const double* x, const double* cell, int32_t launches, int64_t flush_bytes, double* avg_ms,
                                   double* pairs_in, double* pairs_listed, double* entries);
 
+/* The force evaluation's concurrent branches timed one at a time and together (force-only, on the list built at x):
+ * ms[0] the bonded branch (bonded terms, 1-4 pairs, excluded-pair corrections), ms[1] PME, ms[2] the short-range branch
+ * (displacement check, pack, prune check, pair kernel), ms[3] the whole evaluation; means over `launches` repetitions,
+ * CUDA events, an L2 flush of flush_bytes before each. */
+int32_t caps_gpu_diag_phase_timing(caps_gpu_engine* e, const double* x, const double* cell, int32_t launches, int64_t flush_bytes, double* ms);
+
 #ifdef __cplusplus
 }
 #endif

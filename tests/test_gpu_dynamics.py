@@ -61,6 +61,31 @@ def test_fp64_respa_run_follows_reference(thermostat):
     assert np.max(np.abs(out["x"] - r["x"])) < 1e-8
 
 
+def test_fp64_respa_with_cell_rescaling_follows_reference():
+    """r-RESPA (bonded forces at dt / 2) with the Bussi thermostat and stochastic cell rescaling every 5 steps, as the
+    reference allows them together (dynamics.cpp:90-94): its thermo rows, volume included."""
+    ref = _ref()
+    fx = load("ps_small")
+    o = _opts(thermostat="bussi", respa=2, dt=1.5, steps=30, barostat="c-rescale", tau_p=200.0, barostat_every=5, thermo_every=5)
+    out = Evaluator(fx.ff, o.energy).run(fx.x, fx.cell, o)
+    r = ref.run(fx.ff, fx.x, fx.cell, o)
+    _compare(out["thermo"], r["thermo"], 1e-7, keys=("potential", "kinetic", "conserved", "volume", "pressure"))
+    assert out["thermo"][-1]["volume"] != out["thermo"][0]["volume"]
+
+
+def test_pme_split_with_cell_rescaling_runs_npt():
+    """The PME split (PME every 2 fs) with Bussi and stochastic cell rescaling, the composite configuration's
+    integrator: the cell moves, the temperature holds near its target and the state stays finite."""
+    fx = load("ps_medium")
+    eo = EnergyOptions(cutoff=10.0, skin=2.0, electrostatics="pme", pme_order=4, precision="mixed")
+    o = DynamicsOptions(dt=2.0, steps=300, temperature=350.0, thermostat="bussi", tau_t=50.0, barostat="c-rescale", tau_p=500.0,
+                        barostat_every=10, respa=2, respa_split="pme", thermo_every=50, seed=5, energy=eo, new_velocities=True)
+    out = Evaluator(fx.ff, eo).run(fx.x, fx.cell, o)
+    vols = [r["volume"] for r in out["thermo"]]
+    assert len(set(vols)) > 1 and np.all(np.isfinite(out["x"]))
+    assert abs(np.mean([r["temperature"] for r in out["thermo"][2:]]) - 350.0) < 40.0
+
+
 def test_pme_respa_split_conserves_energy():
     """The PME split (the reciprocal sum once per 2 fs outer step, every other term every 1 fs): no reference has it, so
     it must start from the plain run's step-0 row and conserve the total energy about as well as velocity Verlet at 1 fs."""
