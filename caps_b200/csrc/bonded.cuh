@@ -286,7 +286,8 @@ __device__ __forceinline__ void excl_body(int blk, int nblk, int nx, ExclArgs E,
 // FENE (-1/2 K R0^2 ln(1 - (r/R0)^2)) plus WCA below 2^(1/6) sigma (LAMMPS bond fene; field.cpp:2152-2166). A bond
 // stretched to R0 or past raises kErrFene (the reference throws FieldError there).
 template <class R, class S, bool ENER, bool VIR>
-__device__ __forceinline__ void fene_body(int blk, int nblk, int nf, const uint32_t* __restrict__ ij, const double* __restrict__ p, BondedArgs A, S F, int* counters) {
+__device__ __forceinline__ void fene_body(int blk, int nblk, int nf, const uint32_t* __restrict__ ij, const double* __restrict__ p, BondedArgs A, S F, int* counters,
+                                          double* info) {
   Tally<VIR> T;
   for (int t = blk * blockDim.x + threadIdx.x; t < nf; t += nblk * blockDim.x) {
     const int i = int(ij[2 * t]), j = int(ij[2 * t + 1]);
@@ -296,7 +297,13 @@ __device__ __forceinline__ void fene_body(int blk, int nblk, int nf, const uint3
     const R r = rsq(dx * dx + dy * dy + dz * dz);
     const R q = r / R0;
     if (!(q < R(1))) {
-      atomicOr(reinterpret_cast<unsigned*>(counters + 3), kErrFene);
+      atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), kErrFene);
+      if (info && atomicCAS(counters + kCntFeneClaim, 0, 1) == 0) {   // the first one found: its bond and length
+        double ex = A.x[3 * j] - A.x[3 * i], ey = A.x[3 * j + 1] - A.x[3 * i + 1], ez = A.x[3 * j + 2] - A.x[3 * i + 2];
+        min_image(A.cell, ex, ey, ez);
+        info[kInfoFeneBond] = double(t);
+        info[kInfoFeneR] = sqrt(ex * ex + ey * ey + ez * ez);
+      }
       continue;
     }
     R e = -R(0.5) * K * R0 * R0 * log(R(1) - q * q);
@@ -330,6 +337,7 @@ struct BondedWork {
   const double *bond_kr, *angle_kt, *dih_vd, *imp_vd, *fene_p, *p14_scale;
   const int *dih_grp, *dih_n, *imp_grp, *imp_n;
   int* counters;
+  double* info;
   double lj14;
   const int* type;
   int nt, lj96;
@@ -352,7 +360,7 @@ static __global__ void __launch_bounds__(256) k_bonded(BondedWork W, BondedArgs 
     case kBkImpropers:
       torsions_body<R, S, ENER, VIR>(blk, nblk, W.nig, W.imp_grp, W.imp_ijkl, W.imp_vd, W.imp_n, A, F, int(kEImproper));
       break;
-    case kBkFene: fene_body<R, S, ENER, VIR>(blk, nblk, W.nf, W.fene_ij, W.fene_p, A, F, W.counters); break;
+    case kBkFene: fene_body<R, S, ENER, VIR>(blk, nblk, W.nf, W.fene_ij, W.fene_p, A, F, W.counters, W.info); break;
     case kBkPairs14:
       pairs14_body<R, S, ENER, VIR>(blk, nblk, W.np14, W.p14_ij, W.p14_scale, W.lj14, W.type, W.nt, W.lj14_tab, W.cap14_tab, A, F, W.lj96);
       break;

@@ -33,7 +33,12 @@ enum ErrorBits : unsigned {
   kErrMaskOverflow = 1u << 8,     // exclusion masks past capacity
   kErrImageRange = 1u << 9,       // an image shift outside +-63 cells
   kErrFixRange = 1u << 10,        // a force or energy outside the fixed-point range (overlapping atoms: push off first)
+  kErrRattle = 1u << 11,          // RATTLE (the velocity constraints) did not converge
 };
+
+// What the first failure of a kind leaves for the host's message (the engine's error-detail array, doubles): the
+// stretched FENE bond and its length, and the step whose positions stopped being finite.
+enum ErrInfo { kInfoFeneBond = 0, kInfoFeneR, kInfoNonFiniteStep, kInfoNum = 4 };
 
 // Periodic cell: origin o, edge vectors a, b, c (columns of h) and h^-1 (rows: reciprocal vectors without 2 pi).
 struct DevCell {

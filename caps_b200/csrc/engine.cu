@@ -271,6 +271,8 @@ void Engine::setup_ff(const caps_gpu_ff* ff) {
     check_idx(ff->fene_ij, size_t(2) * nfene_, "fene");
     d_fene_ij_.upload(ff->fene_ij, size_t(2) * nfene_, stream_);
     d_fene_p_.upload(ff->fene_k_r0_eps_sigma, size_t(4) * nfene_, stream_);
+    h_fene_r0_.resize(size_t(nfene_));
+    for (int k = 0; k < nfene_; ++k) h_fene_r0_[size_t(k)] = ff->fene_k_r0_eps_sigma[4 * k + 1];
   }
   lj_shift_model_ = ff->lj_shift != 0;
   model_cutoff_ = ff->model_cutoff;
@@ -447,8 +449,14 @@ void Engine::set_cell(const double* cell) {
   g.rq = int(std::ceil(g.rlist / g.w[2])) + 1;
   g.dw = g.rlist / g.w[2];
   g.batch = batch_;
+  // periodic images in range along each axis: 2 ceil(r_list / w) + 1 for the perpendicular width w (the reference counts
+  // the images its bins reach the same way and refuses more than 65536 in all, field.cpp:966-972); the device list also
+  // encodes at most +-60 images per axis
+  double images = 1;
+  for (int d = 0; d < 3; ++d) images *= 2 * std::ceil(g.rlist / g.w[d]) + 1;
+  if (images > 65536) throw ModelError(CAPS_GPU_EFIELD, "the cell is too small for the cut-off: more than 65536 periodic images in range");
   if (g.ru / g.nu > 60 || g.rv / g.nv > 60 || g.rq > 60)
-    throw ModelError(CAPS_GPU_EFIELD, "the cell is too small for the cut-off: more than 60 periodic images in range");
+    throw ModelError(CAPS_GPU_EFIELD, "the cell is too small for the cut-off: more than 60 periodic images along one axis (the device list's limit)");
   const bool geom_changed = !keep_list && (g.nu != geom_.nu || g.nv != geom_.nv);
   if (!keep_list) geom_ = g;
   if (geom_changed) {
@@ -522,6 +530,8 @@ void Engine::ensure_list_capacity() {
   if (!d_counters_.p) {
     d_counters_.alloc(kCntNum);
     CK(cudaMemsetAsync(d_counters_.p, 0, sizeof(int) * kCntNum, stream_));
+    d_errinfo_.alloc(kInfoNum);
+    d_errinfo_.zero(stream_);
   }
   d_F_.alloc(size_t(3) * n_);
   if (!mixed_) d_Fd_.alloc(size_t(3) * n_);
@@ -559,18 +569,33 @@ void Engine::ensure_list_capacity() {
 void Engine::check_errors() {
   const unsigned e = unsigned(h_counters_[kCntErr]);
   if (!e) return;
+  // the details the failing kernels left (read once, then cleared with the error word and the claims)
+  double info[kInfoNum] = {0, 0, 0, 0};
+  CK(cudaMemcpy(info, d_errinfo_.p, sizeof info, cudaMemcpyDeviceToHost));
   CK(cudaMemsetAsync(d_counters_.p + kCntErr, 0, sizeof(int), stream_));
-  if (e & kErrFene) throw ModelError(CAPS_GPU_EFIELD, "a FENE bond is stretched past R0; lower --dt or relax the structure first");
+  CK(cudaMemsetAsync(d_counters_.p + kCntFeneClaim, 0, 2 * sizeof(int), stream_));
+  d_errinfo_.zero(stream_);
+  CK(cudaStreamSynchronize(stream_));
+  if (e & kErrFene) {   // the reference's text (field.cpp:2157-2159), with the first stretched bond found
+    const int b = int(info[kInfoFeneBond]);
+    const double r0 = b >= 0 && b < int(h_fene_r0_.size()) ? h_fene_r0_[size_t(b)] : 0.0;
+    throw ModelError(CAPS_GPU_EFIELD, "a FENE bond is stretched to r = " + std::to_string(info[kInfoFeneR]) + " Å, past R0 = " + std::to_string(r0) +
+                                          " Å; lower --dt or relax the structure first");
+  }
   if (e & (kErrListOverflow | kErrMaskOverflow | kErrScOverflow)) throw ModelError(-100, "pair list capacity exceeded");
   if (e & kErrColumnTooBig) throw ModelError(CAPS_GPU_EINVAL, "a grid column holds more atoms than the device sort takes (the cell is too dense or too thin)");
   if (e & kErrExclOverflow) throw ModelError(CAPS_GPU_EINVAL, "too many excluded partners in one super-cluster for the device list");
   if (e & kErrImageRange) throw ModelError(CAPS_GPU_EFIELD, "an excluded pair is more than 63 cells apart: unwrap the molecules first");
+  // the reference's texts (constraints.cpp:219, 227, 259)
   if (e & (kErrShake | kErrShakeTurn))
     throw ModelError(CAPS_GPU_ECONSTRAINT, (e & kErrShakeTurn) ? "a constrained bond turned by more than 90° in one step; lower the time step or relax first"
                                                                  : "the bond constraints did not converge (SHAKE); lower the time step or relax first");
+  if (e & kErrRattle) throw ModelError(CAPS_GPU_ECONSTRAINT, "the bond constraints did not converge (RATTLE); lower the time step");
   if (e & kErrFixRange)
     throw ModelError(CAPS_GPU_EFIELD, "a force beyond the fixed-point range (2e9 kcal/mol/Å): overlapping atoms; push the structure off first (FP64 with a force cap)");
-  if (e & kErrNonFinite) throw ModelError(CAPS_GPU_EFIELD, "the simulation became unstable; lower the time step or relax first");
+  if (e & kErrNonFinite)   // the reference's text (dynamics.cpp:757), with the step whose positions were not finite
+    throw ModelError(CAPS_GPU_EFIELD, "the simulation became unstable at step " + std::to_string((long long)info[kInfoNonFiniteStep]) +
+                                          "; lower the time step or relax first");
   throw ModelError(CAPS_GPU_EINVAL, "device error word " + std::to_string(e));
 }
 
@@ -672,6 +697,8 @@ void Engine::compute_dev(const double* d_x, const double* cell, double* d_f, cap
 }
 
 void Engine::compute_host(const double* x, const double* cell, double* f, caps_gpu_terms* out) {
+  for (size_t k = 0; k < size_t(3) * n_; ++k)
+    if (!std::isfinite(x[k])) throw ModelError(CAPS_GPU_EFIELD, "non-finite coordinates: atom " + std::to_string(k / 3 + 1));
   set_cell(cell);
   CK(cudaMemcpyAsync(d_x_.p, x, sizeof(double) * 3 * size_t(n_), cudaMemcpyHostToDevice, stream_));
   compute_dev(d_x_.p, cell, d_f_.p, out);

@@ -231,6 +231,8 @@ class Engine {
   double ghi_ = 0;
   DevBuf<uint32_t> d_bond_ij_, d_angle_ijk_, d_dih_ijkl_, d_imp_ijkl_, d_p14_ij_, d_excl_ij_, d_fene_ij_;
   DevBuf<double> d_bond_kr_, d_angle_kt_, d_dih_vd_, d_imp_vd_, d_p14_scale_, d_fene_p_;
+  std::vector<double> h_fene_r0_;   // R0 of each FENE bond, for the overstretch message
+  DevBuf<double> d_errinfo_;        // error details left by the kernels (ErrInfo)
   DevBuf<int> d_dih_n_, d_imp_n_, d_dih_grp_, d_imp_grp_;
   DevBuf<double> d_excl_f_;
   DevBuf<uint32_t> d_excl_off_, d_excl_list_;

@@ -114,6 +114,8 @@ struct KickArgs {
   int* counters;
   long long* fq;
   double* fd;
+  double* info;   // the engine's error details (the step of the first non-finite position)
+  int step_ahead; // 1 when this step's counter is advanced after this kick (the Langevin step's first kick)
 };
 __device__ __forceinline__ void kick_drift_atom(const KickArgs& K, int i, double s) {
   const double a = K.hk * kAcc * K.invm[i], a2 = K.hk2 * kAcc * K.invm[i];
@@ -132,7 +134,10 @@ __device__ __forceinline__ void kick_drift_atom(const KickArgs& K, int i, double
     if (K.fq) K.fq[size_t(r) * K.n + i] = 0;
     if (K.fd) K.fd[size_t(r) * K.n + i] = 0;
   }
-  if (bad) atomicOr(reinterpret_cast<unsigned*>(K.counters + kCntErr), kErrNonFinite);
+  if (bad) {
+    atomicOr(reinterpret_cast<unsigned*>(K.counters + kCntErr), kErrNonFinite);
+    if (K.info && atomicCAS(K.counters + kCntNanClaim, 0, 1) == 0) K.info[kInfoNonFiniteStep] = K.sc[kScStep] + K.step_ahead;
+  }
 }
 __global__ void k_kick_drift(KickArgs K) {
   pdl_begin();
@@ -479,7 +484,7 @@ __device__ void rattle_star(const ConsArgs& C, int s, const double* __restrict__
       }
     }
   }
-  if (!done) atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), kErrShake);
+  if (!done) atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), kErrRattle);
 #pragma unroll
   for (int a = 0; a <= NK; ++a)
     for (int r = 0; r < 3; ++r) v[3 * ids[a] + r] = pv[a][r];
@@ -538,7 +543,7 @@ __device__ void rattle_water(const ConsArgs& C, int wi, const double* __restrict
       }
     }
   }
-  if (!done) atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), kErrShake);
+  if (!done) atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), kErrRattle);
 #pragma unroll
   for (int a = 0; a < 3; ++a)
     for (int r = 0; r < 3; ++r) v[3 * ids[a] + r] = pv[a][r];
@@ -760,7 +765,7 @@ __global__ void k_vel_rattle(ConsArgs C, int nfree, const int* __restrict__ free
         }
       }
     }
-    if (!done) atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), kErrShake);
+    if (!done) atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), kErrRattle);
     for (int a = 0; a < na; ++a) {
       const int g = C.cl_atoms[a0 + a];
       for (int r = 0; r < 3; ++r) v[3 * g + r] = pv[a][r];
@@ -1189,9 +1194,10 @@ struct Stepper {
   // half kick, then drift with SHAKE; `scale` applies the thermostat's pending factor first
   // kick + drift, then SHAKE; the kick also clears the force evaluation's atom-order sums for the evaluation that
   // follows (Engine::forces then skips its own clearing)
-  void kick_drift(double hk, double hd, bool scale, bool zero_cw, const double* f = nullptr, const double* f2 = nullptr, double hk2 = 0) {
+  void kick_drift(double hk, double hd, bool scale, bool zero_cw, const double* f = nullptr, const double* f2 = nullptr, double hk2 = 0,
+                  int step_ahead = 0) {
     KickArgs K{n, x.p, v.p, x0.p, f ? f : E.d_f_.p, invm.p, hk, f2, hk2, hd, sc.p, scale ? 1 : 0, zero_cw ? 1 : 0, E.d_counters_.p,
-               E.mixed_ ? E.d_F_.p : nullptr, E.mixed_ ? nullptr : E.d_Fd_.p};
+               E.mixed_ ? E.d_F_.p : nullptr, E.mixed_ ? nullptr : E.d_Fd_.p, E.d_errinfo_.p, step_ahead};
     launch_pdl(k_kick_drift, blocks(size_t(n), 256), 256, 0, E.stream_, K);
     if (ncons) launch_pdl(k_shake, blocks(size_t(C.ncl), 128), 128, 0, E.stream_, C, x.p, x0.p, v.p, hd, E.d_counters_.p);
     E.sums_cleared_ = true;
@@ -1273,7 +1279,7 @@ struct Stepper {
     }
     if (langevin) {
       const double c1 = std::exp(-dt / std::max(o.tau_t, 1e-9)), c2 = std::sqrt(1 - c1 * c1);
-      kick_drift(0.5 * dt, 0.5 * dt, false, true);
+      kick_drift(0.5 * dt, 0.5 * dt, false, true, nullptr, nullptr, 0, 1);
       KeArgs A = ke_args(kScKE0, false);
       A.begin = 1;
       ke_launch(A);

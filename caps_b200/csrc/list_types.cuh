@@ -55,7 +55,8 @@ struct ListBufs {
 };
 
 // Device counters: list sizes, the error word, the rebuild and prune flags, and running counts of builds and prunes.
-enum Counter { kCntEnt = 0, kCntWork, kCntMask, kCntErr, kCntRebuild, kCntNsc, kCntMaxCol, kCntPrune, kCntBuilds, kCntPrunes, kCntPairNext, kCntNum = 11 };
+enum Counter { kCntEnt = 0, kCntWork, kCntMask, kCntErr, kCntRebuild, kCntNsc, kCntMaxCol, kCntPrune, kCntBuilds, kCntPrunes, kCntPairNext,
+               kCntFeneClaim, kCntNanClaim, kCntNum = 13 };   // *Claim: 1 once the first failure of that kind left its details
 
 __device__ __forceinline__ void raise_error(int* counters, unsigned bit) { atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), bit); }
 
