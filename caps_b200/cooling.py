@@ -17,6 +17,8 @@ import math
 from dataclasses import dataclass, field
 from typing import Callable
 
+import numpy as np
+
 from .engine import DynamicsOptions, EnergyOptions, run_batch
 
 

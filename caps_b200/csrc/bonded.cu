@@ -48,11 +48,11 @@ void Engine::bonded_forces(const double* d_x, bool ener, bool vir, int parts) {
   auto run = [&](auto sink) {
     using S = decltype(sink);
     if (ener) {
-      if (vir) launch_pdl(k_bonded<double, S, true, true>, blocks, T, 0, stream_, W, A, sink);
-      else launch_pdl(k_bonded<double, S, true, false>, blocks, T, 0, stream_, W, A, sink);
+      if (vir) launch_k(k_bonded<double, S, true, true>, blocks, T, 0, stream_, W, A, sink);
+      else launch_k(k_bonded<double, S, true, false>, blocks, T, 0, stream_, W, A, sink);
     } else {
-      if (vir) launch_pdl(k_bonded<double, S, false, true>, blocks, T, 0, stream_, W, A, sink);
-      else launch_pdl(k_bonded<double, S, false, false>, blocks, T, 0, stream_, W, A, sink);
+      if (vir) launch_k(k_bonded<double, S, false, true>, blocks, T, 0, stream_, W, A, sink);
+      else launch_k(k_bonded<double, S, false, false>, blocks, T, 0, stream_, W, A, sink);
     }
   };
   if (mixed_) run(ForceSink<float>{d_F_.p, d_F_.p + n_, d_F_.p + 2 * size_t(n_), d_counters_.p + kCntErr});

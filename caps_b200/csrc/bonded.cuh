@@ -347,7 +347,6 @@ struct BondedWork {
 
 template <class R, class S, bool ENER, bool VIR>
 static __global__ void __launch_bounds__(256) k_bonded(BondedWork W, BondedArgs A, S F) {
-  pdl_begin();
   int sgm = 0;
   while (sgm + 1 < W.nseg && int(blockIdx.x) >= W.first[sgm + 1]) ++sgm;
   const int blk = int(blockIdx.x) - W.first[sgm], nblk = W.first[sgm + 1] - W.first[sgm];

@@ -66,15 +66,6 @@ __device__ __forceinline__ void min_image(const DevCell& c, R& dx, R& dy, R& dz)
   dz = R(c.h[2][0] * f[0] + c.h[2][1] * f[1] + c.h[2][2] * f[2]);
 }
 
-// Programmatic dependent launch. Every kernel of the library starts with pdl_begin(): it waits until the grid launched
-// before it in the stream has completed and its memory is visible (griddepcontrol.wait; a no-op for a kernel launched
-// without the attribute), then lets the next grid be launched early (griddepcontrol.launch_dependents), so that grid's
-// launch overlaps this one's execution instead of following its completion. Nothing is read or written before the wait.
-__device__ __forceinline__ void pdl_begin() {
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-
 __device__ __forceinline__ long long to_fix(double v, double scale) { return __double2ll_rn(v * scale); }
 __device__ __forceinline__ long long to_fixf(float v) { return __float2ll_rn(v * 4294967296.0f); }
 

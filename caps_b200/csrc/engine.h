@@ -94,21 +94,15 @@ void DevBuf<T>::zero(cudaStream_t s) {
   const cudaError_t e = cudaMemsetAsync(p, 0, n * sizeof(T), s);
   if (e != cudaSuccess) throw CudaError(std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
 }
-// Launches a kernel with programmatic stream serialisation: it may be launched while the kernel before it in the stream
-// is still running, and waits for it in its pdl_begin() (common.cuh). Captured into a graph, the pair becomes a
-// programmatic dependency edge. Arguments convert to the kernel's parameter types.
+// Launches a kernel on a stream and turns a launch error into an exception. Arguments convert to the kernel's parameter
+// types.
 template <class... KP, class... A>
-void launch_pdl(void (*kernel)(KP...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream, A&&... args) {
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
+void launch_k(void (*kernel)(KP...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream, A&&... args) {
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = grid;
   cfg.blockDim = block;
   cfg.dynamicSmemBytes = smem;
   cfg.stream = stream;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
   const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
   if (e != cudaSuccess) throw CudaError(std::string("kernel launch: ") + cudaGetErrorString(e));
 }

@@ -140,7 +140,6 @@ __device__ __forceinline__ void kick_drift_atom(const KickArgs& K, int i, double
   }
 }
 __global__ void k_kick_drift(KickArgs K) {
-  pdl_begin();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (K.zero_cw && i < 6) K.sc[kScCW0 + i] = 0;
   if (i >= K.n) return;
@@ -314,7 +313,6 @@ __device__ void settle_water(const ConsArgs& C, int w, double* __restrict__ x, c
 // SHAKE on each cluster (Gauss-Seidel along the reference vectors, tol 1e-8 relative; core/src/constraints.cpp:196-230),
 // then v += (x - x_before) / h when h > 0.
 __global__ void k_shake(ConsArgs C, double* __restrict__ x, const double* __restrict__ x0, double* __restrict__ v, double h, int* counters) {
-  pdl_begin();
   const int cc = blockIdx.x * blockDim.x + threadIdx.x;
   if (cc >= C.ncl) return;
   if (cc < C.e1) return shake_star<1>(C, cc, x, x0, v, h, counters);
@@ -435,7 +433,6 @@ __device__ __forceinline__ void vel_op(const VelOp& op, int g, double* vv, const
 
 // The velocity update alone, one thread per atom (runs without constraints).
 __global__ void k_vel(int n, double* __restrict__ v, const double* __restrict__ invm, const double* sc, VelOp op) {
-  pdl_begin();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double vv[3] = {v[3 * i], v[3 * i + 1], v[3 * i + 2]};
@@ -561,7 +558,6 @@ __device__ void rattle_water(const ConsArgs& C, int wi, const double* __restrict
 }
 
 __global__ void k_scale_v(int n, double* __restrict__ v, const double* __restrict__ sc) {
-  pdl_begin();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= 3 * n) return;
   v[i] *= sc[kScFactor];
@@ -576,7 +572,6 @@ __device__ void step_begin_body(double* sc, double t0, double t1, long long step
   sc[kScKtarget] = 0.5 * ndof * kB * t;
 }
 __global__ void k_step_begin(double* sc, double t0, double t1, long long steps, double ndof) {
-  pdl_begin();
   step_begin_body(sc, t0, t1, steps, ndof);
 }
 
@@ -702,7 +697,6 @@ __device__ void ke_blocks(const KeArgs& A, double e, double t[6]) {
 // The first Nose-Hoover half step of a step, on the kinetic energy the previous step left in sc[kScKE]: its second half
 // set it to the scaled velocities' value, and the velocities have not changed since.
 __global__ void k_nhc_begin(Chain* ch, double* sc, double t0, double t1, long long steps, double ndof, double t_freq, double dt) {
-  pdl_begin();
   step_begin_body(sc, t0, t1, steps, ndof);
   nhc_body(ch, sc, ndof, t_freq, dt);
 }
@@ -714,7 +708,6 @@ __global__ void k_nhc_begin(Chain* ch, double* sc, double t0, double t1, long lo
 // velocities and runs K's thermostat update in its last block (what k_ke does in a launch of its own).
 __global__ void k_vel_rattle(ConsArgs C, int nfree, const int* __restrict__ free_atoms, const double* __restrict__ x, double* __restrict__ v, VelOp op,
                              double h, double* sc, int* counters, KeArgs K) {
-  pdl_begin();
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   double w[6] = {0, 0, 0, 0, 0, 0};
   if (c >= C.ncl && c < C.ncl + nfree) {
@@ -816,7 +809,6 @@ __global__ void k_vel_rattle(ConsArgs C, int nfree, const int* __restrict__ free
 // each block writes its partial sums; the last block to finish adds the partials in block order (deterministic) and
 // runs the scalar update. No block waits on another.
 __global__ void k_ke(KeArgs A) {
-  pdl_begin();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double e = 0, t[6] = {0, 0, 0, 0, 0, 0};
   if (i < A.n) ke_atom(A, i, e, t);
@@ -1189,7 +1181,7 @@ struct Stepper {
     A.tau = o.tau_t;
     return A;
   }
-  void ke_launch(const KeArgs& A) { launch_pdl(k_ke, nparts, 256, 0, E.stream_, A); }
+  void ke_launch(const KeArgs& A) { launch_k(k_ke, nparts, 256, 0, E.stream_, A); }
   void ke(int slot, bool tensor) { ke_launch(ke_args(slot, tensor)); }
   // half kick, then drift with SHAKE; `scale` applies the thermostat's pending factor first
   // kick + drift, then SHAKE; the kick also clears the force evaluation's atom-order sums for the evaluation that
@@ -1198,20 +1190,20 @@ struct Stepper {
                   int step_ahead = 0) {
     KickArgs K{n, x.p, v.p, x0.p, f ? f : E.d_f_.p, invm.p, hk, f2, hk2, hd, sc.p, scale ? 1 : 0, zero_cw ? 1 : 0, E.d_counters_.p,
                E.mixed_ ? E.d_F_.p : nullptr, E.mixed_ ? nullptr : E.d_Fd_.p, E.d_errinfo_.p, step_ahead};
-    launch_pdl(k_kick_drift, blocks(size_t(n), 256), 256, 0, E.stream_, K);
-    if (ncons) launch_pdl(k_shake, blocks(size_t(C.ncl), 128), 128, 0, E.stream_, C, x.p, x0.p, v.p, hd, E.d_counters_.p);
+    launch_k(k_kick_drift, blocks(size_t(n), 256), 256, 0, E.stream_, K);
+    if (ncons) launch_k(k_shake, blocks(size_t(C.ncl), 128), 128, 0, E.stream_, C, x.p, x0.p, v.p, hd, E.d_counters_.p);
     E.sums_cleared_ = true;
   }
   // a velocity update, then RATTLE (constraint virial summed when h > 0); with ke, also the kinetic energy and ke's
   // thermostat update (constraints only: the caller launches k_ke otherwise)
   void vel_rattle(const VelOp& op, double h, const KeArgs* ke = nullptr) {
     if (!ncons) {
-      if (op.kind != 0) launch_pdl(k_vel, blocks(size_t(n), 256), 256, 0, E.stream_, n, v.p, invm.p, sc.p, op);
+      if (op.kind != 0) launch_k(k_vel, blocks(size_t(n), 256), 256, 0, E.stream_, n, v.p, invm.p, sc.p, op);
       return;
     }
     KeArgs K{};
     if (ke) K = *ke;
-    launch_pdl(k_vel_rattle, blocks(size_t(C.ncl + nfree), 128), 128, 0, E.stream_, C, nfree, free_atoms.p, x.p, v.p, op, h, sc.p, E.d_counters_.p, K);
+    launch_k(k_vel_rattle, blocks(size_t(C.ncl + nfree), 128), 128, 0, E.stream_, C, nfree, free_atoms.p, x.p, v.p, op, h, sc.p, E.d_counters_.p, K);
   }
   VelOp kick_op(double hk) const { return VelOp{1, E.d_f_.p, hk, 0, 0, 0, nullptr, 0}; }
   // the kick from the force evaluation's sums (its reduction skipped), storing the forces to E.d_f_
@@ -1232,7 +1224,7 @@ struct Stepper {
   void rattle(double h) {   // RATTLE alone (initial velocities)
     if (ncons) vel_rattle(VelOp{0, nullptr, 0, 0, 0, 0, nullptr, 0}, h);
   }
-  void scale_v() { launch_pdl(k_scale_v, blocks(size_t(3) * n, 256), 256, 0, E.stream_, n, v.p, sc.p); }
+  void scale_v() { launch_k(k_scale_v, blocks(size_t(3) * n, 256), 256, 0, E.stream_, n, v.p, sc.p); }
   // r-RESPA force sets (dynamics.cpp:113-122, 318-326): the non-bonded (slow) and bonded (fast) parts in their own
   // arrays; the evaluation at the end of a step computes both, with energies and virial summed over the two.
   // The PME split puts the reciprocal sum (and its exclusion corrections) in the slow set and every other term in the
@@ -1261,7 +1253,7 @@ struct Stepper {
       // r-RESPA (dynamics.cpp:643-657): outer half kick with the slow forces; `respa` velocity-Verlet steps of dt/respa
       // with the fast ones; outer half kick. Adjacent kicks with the same forces are merged.
       const double h = dt / respa;
-      launch_pdl(k_step_begin, 1, 1, 0, E.stream_, sc.p, o.temperature, o.temperature_end, (long long)o.steps, ndof);
+      launch_k(k_step_begin, 1, 1, 0, E.stream_, sc.p, o.temperature, o.temperature_end, (long long)o.steps, ndof);
       kick_drift(0.5 * dt, h, false, true, f_slow.p, f_fast.p, 0.5 * h);
       for (int j = 0; j + 1 < respa; ++j) {
         fast_forces();
@@ -1291,7 +1283,7 @@ struct Stepper {
       forces(ener, vir);
       vel_rattle(kick_op(0.5 * dt), hw);
     } else if (nhc) {
-      launch_pdl(k_nhc_begin, 1, 1, 0, E.stream_, chain.p, sc.p, o.temperature, o.temperature_end, (long long)o.steps, ndof, t_freq, dt);
+      launch_k(k_nhc_begin, 1, 1, 0, E.stream_, chain.p, sc.p, o.temperature, o.temperature_end, (long long)o.steps, ndof, t_freq, dt);
       kick_drift(0.5 * dt, dt, true, true);
       KeArgs A = ke_args(kScKE, false);
       A.then = kThenNhc;
@@ -1305,7 +1297,7 @@ struct Stepper {
       }
       scale_v();
     } else {
-      launch_pdl(k_step_begin, 1, 1, 0, E.stream_, sc.p, o.temperature, o.temperature_end, (long long)o.steps, ndof);
+      launch_k(k_step_begin, 1, 1, 0, E.stream_, sc.p, o.temperature, o.temperature_end, (long long)o.steps, ndof);
       kick_drift(0.5 * dt, dt, false, true);
       KeArgs A = ke_args(kScKE, false);
       A.then = kThenBussi;
@@ -1621,7 +1613,7 @@ void MdRun::start() {
   S.rng = std::make_unique<HostRng>(o.seed);
   if (S.ncons) {   // the constrained lengths hold from the start (dynamics.cpp:198-203)
     CK(cudaMemcpyAsync(S.x0.p, S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
-    launch_pdl(k_shake, blocks(size_t(S.C.ncl), 128), 128, 0, stream_, S.C, S.x.p, S.x0.p, S.v.p, 0.0, E.d_counters_.p);
+    launch_k(k_shake, blocks(size_t(S.C.ncl), 128), 128, 0, stream_, S.C, S.x.p, S.x0.p, S.v.p, 0.0, E.d_counters_.p);
   }
 
   // velocities: given, or Maxwell-Boltzmann from the reference's stream, no centre-of-mass motion, rescaled to T
@@ -1750,7 +1742,7 @@ void MdRun::baro_step(long long s) {
   S.C.cell = E.dcell_;
   if (S.ncons) {
     CK(cudaMemcpyAsync(S.x0.p, S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
-    launch_pdl(k_shake, blocks(size_t(S.C.ncl), 128), 128, 0, stream_, S.C, S.x.p, S.x0.p, S.v.p, 0.0, E.d_counters_.p);
+    launch_k(k_shake, blocks(size_t(S.C.ncl), 128), 128, 0, stream_, S.C, S.x.p, S.x0.p, S.v.p, 0.0, E.d_counters_.p);
     S.rattle(0);
   }
   S.forces(true, true);

@@ -21,7 +21,6 @@ namespace capsb {
 // rebuild and prune flags; the pair kernel lowers both once the step's list work is done.
 static __global__ void k_check_step(int n, const double* __restrict__ x, const double* __restrict__ x0, double lim_b2, const double* __restrict__ xp,
                                     double lim_p2, int* counters) {
-  pdl_begin();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   bool mb = false, mp = false;
   if (i < n) {
@@ -39,7 +38,6 @@ static __global__ void k_check_step(int n, const double* __restrict__ x, const d
 
 // K-BIN: wrapped fractional coordinates, lattice offsets and the column of every atom; column counts.
 static __global__ void k_bin(int n, const double* __restrict__ x, DevCell cell, ListGeom g, ListBufs b) {
-  pdl_begin();
   if (build_off(b.counters)) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -65,7 +63,6 @@ static __global__ void k_bin(int n, const double* __restrict__ x, DevCell cell, 
 // K-SCAN (one block): column starts, super-cluster starts (64 atoms each, the last one of a column partial), and the
 // column of every super-cluster. Also resets the list counters for the search.
 static __global__ void k_scan_columns(ListGeom g, ListBufs b) {
-  pdl_begin();
   if (build_off(b.counters)) return;
   __shared__ int s_a[1024], s_s[1024];
   __shared__ int carry_a, carry_s, s_max;
@@ -118,7 +115,6 @@ static __global__ void k_scan_columns(ListGeom g, ListBufs b) {
 
 // K-SCATTER: atoms into their column's range (unordered; the sort that follows fixes the order).
 static __global__ void k_scatter(int n, ListBufs b) {
-  pdl_begin();
   if (build_off(b.counters)) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -136,7 +132,6 @@ static __global__ void k_scatter(int n, ListBufs b) {
 // K-SORT (block per column): atoms by fractional c, ties by index. A bitonic sorting network in shared memory over the
 // column padded to a power of two (pad keys sort last): log2(n)(log2(n)+1)/2 compare-exchange rounds, one barrier each.
 static __global__ void k_sort_columns(ListGeom g, ListBufs b) {
-  pdl_begin();
   if (build_off(b.counters)) return;
   extern __shared__ unsigned char smem_raw[];
   double* key = reinterpret_cast<double*>(smem_raw);
@@ -179,7 +174,6 @@ static __global__ void k_sort_columns(ListGeom g, ListBufs b) {
 // masks, the super-cluster's origin and its c range. Lane l holds atoms l (lower c half) and l + 32 (upper c half):
 // the ranks along y and x come from shuffles, the boxes from butterfly reductions over the 8 lanes of a cluster.
 static __global__ void k_superclusters(DevCell cell, ListBufs b) {
-  pdl_begin();
   if (build_off(b.counters)) return;
   __shared__ double s_w[4][64][3];   // world position by local slot
   __shared__ int s_a[4][64];         // atom by local slot, -1 padding
@@ -365,7 +359,6 @@ static __device__ void flush_batch(SearchBatch& B, int sc, int cnt, int lane, co
 // itself once).
 static __global__ void __launch_bounds__(32 * kSearchWarps, 4) k_search(DevCell cell, ListGeom g, const uint32_t* __restrict__ excl_off,
                                                                      const uint32_t* __restrict__ excl_list, ListBufs b) {
-  pdl_begin();
   if (build_off(b.counters)) return;
   extern __shared__ unsigned char smem_raw[];
   SearchShared& S = *reinterpret_cast<SearchShared*>(smem_raw);

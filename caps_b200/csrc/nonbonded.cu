@@ -14,14 +14,12 @@ namespace capsb {
 namespace {
 
 __global__ void k_set_flag(int* counters, int slot, int v) {
-  pdl_begin();
   counters[slot] = v;
 }
 
 // Forces to the caller's AoS doubles: atom-order sums plus the pair kernel's slot-order sums.
 __global__ void k_reduce_f32(int n, const long long* __restrict__ F, const long long* __restrict__ Fs, int nslots, const int* __restrict__ iperm,
                              double* __restrict__ f, int with_pairs) {
-  pdl_begin();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int s = with_pairs ? iperm[i] : -1;
@@ -34,7 +32,6 @@ __global__ void k_reduce_f32(int n, const long long* __restrict__ F, const long 
 }
 __global__ void k_reduce_f64(int n, const double* __restrict__ F, const double* __restrict__ Fs, int nslots, const int* __restrict__ iperm,
                              double* __restrict__ f, int with_pairs) {
-  pdl_begin();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int s = with_pairs ? iperm[i] : -1;
@@ -76,13 +73,13 @@ void Engine::tune_batch(const double* d_x) {
   const size_t ns = size_t(nsc_cap_) * kScAtoms;
   for (int bsz : {32, 24, 16}) {
     geom_.batch = bsz;
-    launch_pdl(k_set_flag, 1, 1, 0, stream_, d_counters_.p, kCntRebuild, 1);
+    launch_k(k_set_flag, 1, 1, 0, stream_, d_counters_.p, kCntRebuild, 1);
     launch_build(d_x);
     if (mixed_)
-      launch_pdl(k_pack_f32, blocks_for(ns, 256), 256, 0, stream_, int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_sc_org_.p, d_q_.p, d_type_.p, nt_,
+      launch_k(k_pack_f32, blocks_for(ns, 256), 256, 0, stream_, int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_sc_org_.p, d_q_.p, d_type_.p, nt_,
                                                            d_xq_.p, d_tslot_.p, d_counters_.p, d_x0_.p, d_Fs_.p);
     else
-      launch_pdl(k_pack_f64, blocks_for(ns, 256), 256, 0, stream_, int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_q_.p, d_type_.p, nt_, d_xqd_.p, d_tslot_.p,
+      launch_k(k_pack_f64, blocks_for(ns, 256), 256, 0, stream_, int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_q_.p, d_type_.p, nt_, d_xqd_.p, d_tslot_.p,
                                                            d_counters_.p, d_x0_.p, d_Fsd_.p);
     prune(d_x);
     float ms = 0;
@@ -113,14 +110,14 @@ int Engine::list_builds() {
 // ---------------------------------------------------------------------------------------------------------------
 void Engine::launch_build(const double* d_x) {
   const ListGeom& g = geom_;
-  launch_pdl(k_bin, blocks_for(size_t(n_), 256), 256, 0, stream_, n_, d_x, dcell_, g, lb_);
-  launch_pdl(k_scan_columns, 1, 1024, 0, stream_, g, lb_);
-  launch_pdl(k_scatter, blocks_for(size_t(n_), 256), 256, 0, stream_, n_, lb_);
+  launch_k(k_bin, blocks_for(size_t(n_), 256), 256, 0, stream_, n_, d_x, dcell_, g, lb_);
+  launch_k(k_scan_columns, 1, 1024, 0, stream_, g, lb_);
+  launch_k(k_scatter, blocks_for(size_t(n_), 256), 256, 0, stream_, n_, lb_);
   const size_t sort_smem = size_t(kSortMax) * (sizeof(double) + sizeof(int));
-  launch_pdl(k_sort_columns, std::min(g.ncol, dev_sms_ * 8), 1024, sort_smem, stream_, g, lb_);
-  launch_pdl(k_superclusters, std::max(1, std::min(blocks_for(size_t(nsc_cap_), 4), dev_sms_ * 16)), 128, 0, stream_, dcell_, lb_);
+  launch_k(k_sort_columns, std::min(g.ncol, dev_sms_ * 8), 1024, sort_smem, stream_, g, lb_);
+  launch_k(k_superclusters, std::max(1, std::min(blocks_for(size_t(nsc_cap_), 4), dev_sms_ * 16)), 128, 0, stream_, dcell_, lb_);
   if (sizeof(SearchShared) > 48 * 1024) CK(cudaFuncSetAttribute(k_search, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(SearchShared))));
-  launch_pdl(k_search, std::max(1, std::min(nsc_cap_, dev_sms_ * 8)), 32 * kSearchWarps, sizeof(SearchShared), stream_, dcell_, g, d_excl_off_.p,
+  launch_k(k_search, std::max(1, std::min(nsc_cap_, dev_sms_ * 8)), 32 * kSearchWarps, sizeof(SearchShared), stream_, dcell_, g, d_excl_off_.p,
                                                                                                           d_excl_list_.p, lb_);
   CK(cudaGetLastError());
 }
@@ -172,8 +169,8 @@ void Engine::prune(const double* d_x) {
   const double b = std::min(0.8, skin_);
   const PairArgs A = pair_args();
   const double rp = rc_ + b;
-  if (mixed_) launch_pdl(k_prune<false>, dev_sms_ * 8, 128, 0, stream_, A, rp * rp, d_ent_.p, n_, d_x, d_xp_.p);
-  else launch_pdl(k_prune<true>, dev_sms_ * 8, 128, 0, stream_, A, rp * rp, d_ent_.p, n_, d_x, d_xp_.p);
+  if (mixed_) launch_k(k_prune<false>, dev_sms_ * 8, 128, 0, stream_, A, rp * rp, d_ent_.p, n_, d_x, d_xp_.p);
+  else launch_k(k_prune<true>, dev_sms_ * 8, 128, 0, stream_, A, rp * rp, d_ent_.p, n_, d_x, d_xp_.p);
 }
 
 void Engine::pair_forces(bool ener, bool vir) {
@@ -192,7 +189,7 @@ void Engine::pair_forces(bool ener, bool vir) {
     if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_pair_f32<C, E, V, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
     int per_sm = 0;                                                                                                  \
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_f32<C, E, V, L>, 128, smem));                   \
-    launch_pdl(k_pair_f32<C, E, V, L>, dev_sms_ * std::max(1, per_sm), 128, smem, stream_, A);                               \
+    launch_k(k_pair_f32<C, E, V, L>, dev_sms_ * std::max(1, per_sm), 128, smem, stream_, A);                               \
   } while (0)
 #define PAIR32(C, E, V)                                                                                              \
   do {                                                                                                               \
@@ -217,7 +214,7 @@ void Engine::pair_forces(bool ener, bool vir) {
     if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_pair_f64<C, E, V, CAP, L, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
     int per_sm = 0;                                                                                                  \
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_f64<C, E, V, CAP, L, F>, 128, smem));           \
-    launch_pdl(k_pair_f64<C, E, V, CAP, L, F>, dev_sms_ * std::max(1, per_sm), 128, smem, stream_, A);                       \
+    launch_k(k_pair_f64<C, E, V, CAP, L, F>, dev_sms_ * std::max(1, per_sm), 128, smem, stream_, A);                       \
   } while (0)
 #define PAIR64L(C, E, V, CAP, L) PAIR64LF(C, E, V, CAP, L, false)
 #define PAIR64(C, E, V, CAP)                                                                                         \
@@ -256,7 +253,7 @@ long long Engine::count_pairs() {
   DevBuf<unsigned long long> cnt;
   cnt.alloc(1);
   cnt.zero(stream_);
-  launch_pdl(k_count_pairs, dev_sms_ * 4, 128, 0, stream_, pair_args(), d_ent_.p, d_perm_.p, d_x0_.p, d_ioff_.p, (rc_ + skin_) * (rc_ + skin_), cnt.p);
+  launch_k(k_count_pairs, dev_sms_ * 4, 128, 0, stream_, pair_args(), d_ent_.p, d_perm_.p, d_x0_.p, d_ioff_.p, (rc_ + skin_) * (rc_ + skin_), cnt.p);
   CK(cudaGetLastError());
   unsigned long long v = 0;
   CK(cudaMemcpyAsync(&v, cnt.p, sizeof v, cudaMemcpyDeviceToHost, stream_));
@@ -286,7 +283,7 @@ void Engine::freeze_pairs(const double* x, const double* cell) {
   compute_host(x, cell, f.data(), &t);
   frozen_pairs_ = count_pairs();
   d_frozen_.alloc(size_t(8) * d_ent_.n);
-  launch_pdl(k_freeze, dev_sms_ * 4, 128, 0, stream_, pair_args(), d_ent_.p, d_frozen_.p);
+  launch_k(k_freeze, dev_sms_ * 4, 128, 0, stream_, pair_args(), d_ent_.p, d_frozen_.p);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(stream_));
   frozen_ = true;
@@ -331,19 +328,19 @@ void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild, 
     if (frozen_) {
       // a frozen pair set: no displacement check, build or prune; the pack and the pair kernel run on the frozen list
     } else if (!list_valid_) {
-      launch_pdl(k_set_flag, 1, 1, 0, stream_, d_counters_.p, kCntRebuild, 1);
+      launch_k(k_set_flag, 1, 1, 0, stream_, d_counters_.p, kCntRebuild, 1);
       list_valid_ = true;
     } else if (check_rebuild) {
       const double b = std::min(0.8, skin_);   // the prune margin (see prune())
-      launch_pdl(k_check_step, blocks_for(size_t(n_), 256), 256, 0, stream_, n_, d_x, d_x0_.p, 0.25 * skin_ * skin_, d_xp_.p, 0.25 * b * b, d_counters_.p);
+      launch_k(k_check_step, blocks_for(size_t(n_), 256), 256, 0, stream_, n_, d_x, d_x0_.p, 0.25 * skin_ * skin_, d_xp_.p, 0.25 * b * b, d_counters_.p);
     }
     if (!frozen_) launch_build(d_x);
     const size_t ns = size_t(nsc_cap_) * kScAtoms;
     if (mixed_)
-      launch_pdl(k_pack_f32, blocks_for(ns, 256), 256, 0, stream_, int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_sc_org_.p, d_q_.p, d_type_.p, nt_,
+      launch_k(k_pack_f32, blocks_for(ns, 256), 256, 0, stream_, int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_sc_org_.p, d_q_.p, d_type_.p, nt_,
                                                            d_xq_.p, d_tslot_.p, d_counters_.p, d_x0_.p, d_Fs_.p);
     else
-      launch_pdl(k_pack_f64, blocks_for(ns, 256), 256, 0, stream_, int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_q_.p, d_type_.p, nt_, d_xqd_.p, d_tslot_.p,
+      launch_k(k_pack_f64, blocks_for(ns, 256), 256, 0, stream_, int(ns), d_perm_.p, d_x, d_ioff_.p, dcell_, d_q_.p, d_type_.p, nt_, d_xqd_.p, d_tslot_.p,
                                                            d_counters_.p, d_x0_.p, d_Fsd_.p);
     if (!frozen_) prune(d_x);
     pair_forces(ener, vir);
@@ -352,8 +349,8 @@ void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild, 
   if (pme) join(1);
   if (!reduce) return;   // the caller's kick reads the sums (with iperm) itself
   const size_t ns = size_t(nsc_cap_) * kScAtoms;
-  if (mixed_) launch_pdl(k_reduce_f32, blocks_for(size_t(n_), 256), 256, 0, stream_, n_, d_F_.p, d_Fs_.p, int(ns), d_iperm_.p, out, nonb ? 1 : 0);
-  else launch_pdl(k_reduce_f64, blocks_for(size_t(n_), 256), 256, 0, stream_, n_, d_Fd_.p, d_Fsd_.p, int(ns), d_iperm_.p, out, nonb ? 1 : 0);
+  if (mixed_) launch_k(k_reduce_f32, blocks_for(size_t(n_), 256), 256, 0, stream_, n_, d_F_.p, d_Fs_.p, int(ns), d_iperm_.p, out, nonb ? 1 : 0);
+  else launch_k(k_reduce_f64, blocks_for(size_t(n_), 256), 256, 0, stream_, n_, d_Fd_.p, d_Fsd_.p, int(ns), d_iperm_.p, out, nonb ? 1 : 0);
   CK(cudaGetLastError());
 }
 

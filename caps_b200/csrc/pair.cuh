@@ -25,7 +25,6 @@ static __global__ void k_pack_f32(int nslots, const int* __restrict__ perm, cons
                            const double* __restrict__ sc_org, const double* __restrict__ q, const int* __restrict__ type, int pad_type,
                            float4* __restrict__ xq, int* __restrict__ tslot, int* counters, double* __restrict__ x0,
                            long long* __restrict__ fs) {
-  pdl_begin();
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s < nslots)   // the pair kernel's slot-order sums (3 x nslots) start at zero
     for (int r = 0; r < 3; ++r) fs[size_t(r) * nslots + s] = 0;
@@ -60,7 +59,6 @@ static __global__ void k_pack_f32(int nslots, const int* __restrict__ perm, cons
 static __global__ void k_pack_f64(int nslots, const int* __restrict__ perm, const double* __restrict__ x, const int* __restrict__ ioff, DevCell cell,
                            const double* __restrict__ q, const int* __restrict__ type, int pad_type, double4* __restrict__ xq, int* __restrict__ tslot,
                            int* counters, double* __restrict__ x0, double* __restrict__ fs) {
-  pdl_begin();
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s < nslots)   // the pair kernel's slot-order sums (3 x nslots) start at zero
     for (int r = 0; r < 3; ++r) fs[size_t(r) * nslots + s] = 0;
@@ -181,7 +179,6 @@ __device__ __forceinline__ void reduce_i(int jq, const T fx[8], const T fy[8], c
 // (kappa r_c <= 4); 3 and 4 the same through erfcf and expf (any kappa).
 template <int COUL, bool ENER, bool VIR, bool LJ96 = false>
 static __global__ void __launch_bounds__(128, 5) k_pair_f32(PairArgs A) {
-  pdl_begin();
   extern __shared__ float4 smem_f4[];
   float4* tab = smem_f4;                                  // ntab * ntab
   float4* s_xi = smem_f4 + A.ntab * A.ntab;               // 4 warps x 64
@@ -417,7 +414,6 @@ __device__ __forceinline__ double erfc_exp_as(double x, double& ex2) {
 // the cut-off takes the closed-form Coulomb term (field.cpp:1759-1768).
 template <int COUL, bool ENER, bool VIR, bool CAP = false, bool LJ96 = false, bool FROZEN = false>
 static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
-  pdl_begin();
   extern __shared__ double4 smem_d4[];
   double4* tab = smem_d4;                                   // ntab * ntab
   double* gt = reinterpret_cast<double*>(tab + A.ntab * A.ntab);   // 2 * gnodes with Coulomb, none without (as the launch sizes it)
@@ -596,7 +592,6 @@ static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
 // cluster the 64 atom pairs that are listed, real, not excluded and inside r_c at the packed positions; the entry's
 // half mask becomes their union, so that the pair kernel visits exactly those halves. One thread per entry.
 static __global__ void __launch_bounds__(128) k_freeze(PairArgs A, uint4* __restrict__ ent, unsigned long long* __restrict__ frozen) {
-  pdl_begin();
   if (A.counters[kCntErr] & (kErrListOverflow | kErrMaskOverflow | kErrScOverflow | kErrColumnTooBig | kErrExclOverflow)) return;
   const int nwork = min(A.counters[kCntWork], A.work_cap);
   const int pad = A.ntab - 1;
@@ -647,7 +642,6 @@ static __global__ void __launch_bounds__(128) k_freeze(PairArgs A, uint4* __rest
 static __global__ void __launch_bounds__(128) k_count_pairs(PairArgs A, const uint4* __restrict__ ent, const int* __restrict__ perm,
                                                            const double* __restrict__ x0, const int* __restrict__ ioff, double rl2,
                                                            unsigned long long* __restrict__ out) {
-  pdl_begin();
   if (A.counters[kCntErr] & (kErrListOverflow | kErrMaskOverflow | kErrScOverflow | kErrColumnTooBig | kErrExclOverflow)) return;
   const int nwork = min(A.counters[kCntWork], A.work_cap);
   const int lane = threadIdx.x & 31;
@@ -698,7 +692,6 @@ static __global__ void __launch_bounds__(128) k_count_pairs(PairArgs A, const ui
 template <bool DBL>
 static __global__ void __launch_bounds__(128) k_prune(PairArgs A, double rprune2, uint4* __restrict__ ent, int n, const double* __restrict__ x,
                                                      double* __restrict__ xp) {
-  pdl_begin();
   if (*(volatile const int*)(A.counters + kCntPrune) == 0) return;
   // the positions of this prune, for the next displacement check; and the prune count
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * n; i += gridDim.x * blockDim.x) xp[i] = x[i];

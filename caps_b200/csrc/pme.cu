@@ -74,16 +74,16 @@ void Engine::fft_passes(PmePath<R>& P, bool ener, bool vir) {
   const size_t sx = (size_t(lines_x_) * 2 + 1) * pk_[0] * sizeof(T), sy = (size_t(lines_y_) * 2 + 1) * pk_[1] * sizeof(T),
                sz = (size_t(lines_z_) + 1) * 2 * pk_[2] * sizeof(T);
   const int nlx = pk_[1] * pk_[2];
-  launch_pdl(k_fft_x_fwd<R>, blocks_for(size_t(nlx), lines_x_), 128, sx, stream_, A, mixed_ ? nullptr : d_grid_.p, mixed_ ? d_gridq_.p : nullptr, P.h.p,
+  launch_k(k_fft_x_fwd<R>, blocks_for(size_t(nlx), lines_x_), 128, sx, stream_, A, mixed_ ? nullptr : d_grid_.p, mixed_ ? d_gridq_.p : nullptr, P.h.p,
                                                                         P.plan[0][0], lines_x_);
   const int gy = ((ph1_ + lines_y_ - 1) / lines_y_) * pk_[2];
-  launch_pdl(k_fft_y<R>, gy, 128, sy, stream_, A, P.h.p, P.plan[1][0], lines_y_);
+  launch_k(k_fft_y<R>, gy, 128, sy, stream_, A, P.h.p, P.plan[1][0], lines_y_);
   const int gz = ((ph1_ + lines_z_ - 1) / lines_z_) * pk_[1];
   EnergySink en{d_efix_.p, d_edbl_.p};
-  if (ener) { if (vir) launch_pdl(k_fft_z_solve<R, true, true>, gz, 128, sz, stream_, A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); else launch_pdl(k_fft_z_solve<R, true, false>, gz, 128, sz, stream_, A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); }
-  else { if (vir) launch_pdl(k_fft_z_solve<R, false, true>, gz, 128, sz, stream_, A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); else launch_pdl(k_fft_z_solve<R, false, false>, gz, 128, sz, stream_, A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); }
-  launch_pdl(k_fft_y<R>, gy, 128, sy, stream_, A, P.h.p, P.plan[1][1], lines_y_);
-  launch_pdl(k_fft_x_inv<R>, blocks_for(size_t(nlx), lines_x_), 128, sx, stream_, A, P.h.p, P.gr.p, P.plan[0][1], lines_x_);
+  if (ener) { if (vir) launch_k(k_fft_z_solve<R, true, true>, gz, 128, sz, stream_, A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); else launch_k(k_fft_z_solve<R, true, false>, gz, 128, sz, stream_, A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); }
+  else { if (vir) launch_k(k_fft_z_solve<R, false, true>, gz, 128, sz, stream_, A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); else launch_k(k_fft_z_solve<R, false, false>, gz, 128, sz, stream_, A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); }
+  launch_k(k_fft_y<R>, gy, 128, sy, stream_, A, P.h.p, P.plan[1][1], lines_y_);
+  launch_k(k_fft_x_inv<R>, blocks_for(size_t(nlx), lines_x_), 128, sx, stream_, A, P.h.p, P.gr.p, P.plan[0][1], lines_x_);
 }
 
 // Autotuner for the line transforms: every block shape that fits (x: 1-16 lines per block; y, z: 1-8 consecutive a per
@@ -143,7 +143,7 @@ void Engine::pme_run(PmePath<R>& P, const double* d_x, bool ener, bool vir) {
   PmeArgs A{pk_[0], pk_[1], pk_[2], ph1_, dcell_, d_x, d_q_.p, n_};
   if (!green_valid_ || std::memcmp(green_cell_, cell_h_, sizeof cell_h_) != 0) {
     const size_t half = size_t(ph1_) * pk_[1] * pk_[2];
-    launch_pdl(k_pme_green<R>, blocks_for(half, 256), 256, 0, stream_, A, d_bsp_[0].p, d_bsp_[1].p, d_bsp_[2].p, beta_, kCoulomb, P.gt.p, P.wt.p);
+    launch_k(k_pme_green<R>, blocks_for(half, 256), 256, 0, stream_, A, d_bsp_[0].p, d_bsp_[1].p, d_bsp_[2].p, beta_, kCoulomb, P.gt.p, P.wt.p);
     std::memcpy(green_cell_, cell_h_, sizeof cell_h_);
     green_valid_ = true;
   }
@@ -152,8 +152,8 @@ void Engine::pme_run(PmePath<R>& P, const double* d_x, bool ener, bool vir) {
   else CK(cudaMemsetAsync(d_grid_.p, 0, d_grid_.n * sizeof(double), stream_));
 #define SPREAD(P_)                                                                            \
   do {                                                                                        \
-    if (mixed_) launch_pdl(k_spread<float, P_>, nb, 128, 0, stream_, A, d_grid_.p, d_gridq_.p);      \
-    else launch_pdl(k_spread<double, P_>, nb, 128, 0, stream_, A, d_grid_.p, d_gridq_.p);            \
+    if (mixed_) launch_k(k_spread<float, P_>, nb, 128, 0, stream_, A, d_grid_.p, d_gridq_.p);      \
+    else launch_k(k_spread<double, P_>, nb, 128, 0, stream_, A, d_grid_.p, d_gridq_.p);            \
   } while (0)
   switch (order_) {
     case 3: SPREAD(3); break;
@@ -169,8 +169,8 @@ void Engine::pme_run(PmePath<R>& P, const double* d_x, bool ener, bool vir) {
   const ForceSink<double> Fd{d_Fd_.p, d_Fd_.p + n_, d_Fd_.p + 2 * size_t(n_)};
 #define GATHER(P_)                                                                            \
   do {                                                                                        \
-    if (mixed_) launch_pdl(k_gather<float, R, P_>, nb, 128, 0, stream_, A, P.gr.p, Ff);              \
-    else launch_pdl(k_gather<double, R, P_>, nb, 128, 0, stream_, A, P.gr.p, Fd);                     \
+    if (mixed_) launch_k(k_gather<float, R, P_>, nb, 128, 0, stream_, A, P.gr.p, Ff);              \
+    else launch_k(k_gather<double, R, P_>, nb, 128, 0, stream_, A, P.gr.p, Fd);                     \
   } while (0)
   switch (order_) {
     case 3: GATHER(3); break;

@@ -154,7 +154,6 @@ __device__ __forceinline__ int wrapk(int v, int K) {
 // K-SPREAD. FP64: double atomics into g. FP32: fixed point (2^40 per e) into gq, exact and order-free.
 template <class R, int P>
 static __global__ void k_spread(PmeArgs A, double* __restrict__ g, long long* __restrict__ gq) {
-  pdl_begin();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.n) return;
   const double qi = A.q[i];
@@ -186,7 +185,6 @@ static __global__ void k_spread(PmeArgs A, double* __restrict__ g, long long* __
 template <class R>
 static __global__ void __launch_bounds__(128) k_fft_x_fwd(PmeArgs A, const double* __restrict__ g, const long long* __restrict__ gq,
                                                           typename Cpx<R>::T* __restrict__ h, FftPlan<R> P, int lines_per_block) {
-  pdl_begin();
   using T = typename Cpx<R>::T;
   extern __shared__ unsigned char smem_raw[];
   T* tw = reinterpret_cast<T*>(smem_raw);
@@ -213,7 +211,6 @@ static __global__ void __launch_bounds__(128) k_fft_x_fwd(PmeArgs A, const doubl
 template <class R>
 static __global__ void __launch_bounds__(128) k_fft_x_inv(PmeArgs A, const typename Cpx<R>::T* __restrict__ h, R* __restrict__ gr, FftPlan<R> P,
                                                           int lines_per_block) {
-  pdl_begin();
   using T = typename Cpx<R>::T;
   extern __shared__ unsigned char smem_raw[];
   T* tw = reinterpret_cast<T*>(smem_raw);
@@ -242,7 +239,6 @@ static __global__ void __launch_bounds__(128) k_fft_x_inv(PmeArgs A, const typen
 // K-FFT-Y: lines along b for fixed (a, c); a block takes `la` consecutive a (coalesced rows) of one c.
 template <class R>
 static __global__ void __launch_bounds__(128) k_fft_y(PmeArgs A, typename Cpx<R>::T* __restrict__ h, FftPlan<R> P, int la) {
-  pdl_begin();
   using T = typename Cpx<R>::T;
   extern __shared__ unsigned char smem_raw[];
   T* tw = reinterpret_cast<T*>(smem_raw);
@@ -270,7 +266,6 @@ template <class R, bool ENER, bool VIR>
 static __global__ void __launch_bounds__(128) k_fft_z_solve(PmeArgs A, typename Cpx<R>::T* __restrict__ h, const R* __restrict__ gt,
                                                             const R* __restrict__ wt, FftPlan<R> Pf, FftPlan<R> Pi, int la, EnergySink en,
                                                             int fixed) {
-  pdl_begin();
   using T = typename Cpx<R>::T;
   extern __shared__ unsigned char smem_raw[];
   T* twf = reinterpret_cast<T*>(smem_raw);
@@ -334,7 +329,6 @@ static __global__ void __launch_bounds__(128) k_fft_z_solve(PmeArgs A, typename 
 template <class R>
 static __global__ void k_pme_green(PmeArgs A, const double* __restrict__ b1, const double* __restrict__ b2, const double* __restrict__ b3, double beta,
                             double kcoul, R* __restrict__ gt, R* __restrict__ wt) {
-  pdl_begin();
   const size_t total = size_t(A.h1) * A.k2 * A.k3;
   const double fac = kPi * kPi / (beta * beta);
   const int K[3] = {A.k1, A.k2, A.k3};
@@ -388,7 +382,6 @@ static __global__ void k_pme_green(PmeArgs A, const double* __restrict__ b1, con
 // K-GATHER: F_i -= q_i sum_d K_d (row d of h^-1) dE/du_d (caps_kspace.f90:965-992).
 template <class R, class G, int P>
 static __global__ void k_gather(PmeArgs A, const G* __restrict__ gr, ForceSink<R> F) {
-  pdl_begin();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.n) return;
   const double qi = A.q[i];

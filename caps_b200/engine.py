@@ -416,12 +416,12 @@ def run_batch(evaluators: list, xs: list, cells: list, opts: list, vs: list | No
                     frames[r](xa_, ca_, int(step))
         ff_ = _abi.FRAME_FN(cb.wrap(_frame))
     replica_of = {users[r]: r for r in range(R)}   # progress and frame callbacks get the same user pointer
-    for r, cb in enumerate(checkpoints):
-        if cb is None:
+    for r, ck in enumerate(checkpoints):
+        if ck is None:
             continue
 
-        def _ckpt(xp, vp, cp, step, user, cb=cb, n=natoms[r]):
-            cb(np.ctypeslib.as_array(xp, shape=(3 * n,)).copy().reshape(-1, 3), np.ctypeslib.as_array(vp, shape=(3 * n,)).copy().reshape(-1, 3),
+        def _ckpt(xp, vp, cp, step, user, ck=ck, n=natoms[r]):
+            ck(np.ctypeslib.as_array(xp, shape=(3 * n,)).copy().reshape(-1, 3), np.ctypeslib.as_array(vp, shape=(3 * n,)).copy().reshape(-1, 3),
                np.ctypeslib.as_array(cp, shape=(12,)).copy(), int(step))
         cf = _abi.CHECKPOINT_FN(cb.wrap(_ckpt))
         keep.append(cf)
