@@ -123,11 +123,14 @@ Engine::Engine(const caps_gpu_ff* ff, const caps_gpu_opts* o) {
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&dev_sms_, cudaDevAttrMultiProcessorCount, dev));
   CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-  // the side streams (bonded terms, PME) run at the highest priority: their short kernels take SM slots as the long
-  // pair kernel frees them
+  // the main stream (integrator, displacement check, list, pack, prune, pair kernel) runs at the highest priority and
+  // the side streams (bonded terms, PME) at the lowest: the chain that leads to the pair kernel takes SM slots first,
+  // the side branches fill what it leaves
   int prio_lo = 0, prio_hi = 0;
   CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
-  for (auto& st : side_) CK(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio_hi));
+  CK(cudaStreamDestroy(stream_));
+  CK(cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, prio_hi));
+  for (auto& st : side_) CK(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio_lo));
   CK(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
   for (auto& ev : ev_join_) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   CK(cudaMallocHost(&h_counters_, sizeof(int) * kCntNum));
@@ -390,8 +393,9 @@ void Engine::setup_options() {
     cell_set_ = false;
     set_cell(c);
   }
-  // the mixed path's fixed-point spread grid, also after a switch of precision on an unchanged grid
-  if (pme_ && mixed_ && pk_[0] > 0) d_gridq_.alloc(size_t(pk_[0]) * pk_[1] * pk_[2]);
+  // the active path's PME plans and the mixed path's fixed-point spread grid, also after a switch of precision on an
+  // unchanged grid
+  ensure_pme();
   CK(cudaStreamSynchronize(stream_));
 }
 
@@ -408,7 +412,7 @@ std::string Engine::capture_state() const {
   put(&epoch, sizeof epoch);
   put(&opt_, sizeof opt_);
   const int flags[] = {mixed_ ? 1 : 0, energies_ ? 1 : 0, list_valid_ ? 1 : 0, green_valid_ ? 1 : 0, frozen_ ? 1 : 0, batch_tuned_ ? 1 : 0,
-                       batch_, lines_x_, lines_y_, lines_z_, nsc_cap_, pk_[0], pk_[1], pk_[2], n_};
+                       batch_, pme_lines()[0], pme_lines()[1], pme_lines()[2], nsc_cap_, pk_[0], pk_[1], pk_[2], n_, pair_cut_, pme_cap_};
   put(flags, sizeof flags);
   put(cell_h_, sizeof cell_h_);
   put(&dcell_, sizeof dcell_);
@@ -483,8 +487,8 @@ void Engine::set_cell(const double* cell) {
         bspline_moduli(pk_[d], order_, bsp);
         d_bsp_[d].upload(bsp, stream_);
       }
-      pme_setup(pd_);
     }
+    ensure_pme();
   }
 }
 

@@ -121,6 +121,8 @@ struct PmePath {
   DevBuf<R> gt, wt;     // influence function, virial weights
   DevBuf<T> tw[3][2];   // twiddles per axis: forward, inverse
   FftPlan<R> plan[3][2];
+  int k[3] = {0, 0, 0};      // the grid these were set up for
+  int lines[3] = {1, 1, 1};  // line-transform block shapes (x lines per block; y, z consecutive a per block), tuned
 };
 
 class Engine {
@@ -187,9 +189,12 @@ class Engine {
   void fork(int k, const std::function<void()>& launch);
   void join(int k);
   cudaStream_t side_[2] = {nullptr, nullptr};
+  int counter(int slot);   // a device counter (synchronises the stream)
   // Autotuning (timed on this system and GPU, once): the j-tile depth of the pair kernels' work items, and the PME
   // line-transform block shapes per grid.
   int batch_ = kBatch;
+  int pair_cut_ = 0;   // the pair kernel's persistent grid leaves this many block slots per SM to the other branches
+  int pme_cap_ = 0;    // at most this many blocks per PME line-transform launch (0: one per line group)
   bool sums_cleared_ = false;   // the atom-order force sums were cleared by the integrator's kick (the next forces() skips it)
   bool batch_tuned_ = false;
   void tune_batch(const double* d_x);
@@ -283,10 +288,12 @@ class Engine {
   DevBuf<double> d_bsp_[3];
   DevBuf<double> d_grid_;           // FP64 spread grid
   DevBuf<long long> d_gridq_;       // FP32 path: fixed-point spread grid
-  PmePath<double> pd_;
+  PmePath<double> pd_;              // FP64 transforms: the FP64 path
+  PmePath<float> pf_;               // FP32 transforms: the mixed path
   double green_cell_[12] = {0};
-  bool green_valid_ = false;
-  int lines_x_ = 1, lines_y_ = 1, lines_z_ = 1;
+  bool green_valid_ = false;        // the active path's influence function matches cell_h_
+  void ensure_pme();                // the active path's plans, buffers and block shapes for the current grid
+  const int* pme_lines() const { return mixed_ ? pf_.lines : pd_.lines; }
 
   double last_sps_ = 0, last_step_ms_ = 0;
   int64_t timing_flush_ = -1;

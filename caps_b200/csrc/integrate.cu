@@ -26,6 +26,13 @@
 
 namespace capsb {
 
+// Whether a captured graph node is a kernel node.
+static bool is_kernel_node(cudaGraphNode_t nd) {
+  cudaGraphNodeType ty;
+  CK(cudaGraphNodeGetType(nd, &ty));
+  return ty == cudaGraphNodeTypeKernel;
+}
+
 
 namespace {
 
@@ -1120,22 +1127,34 @@ struct Stepper {
   // Returns its kernel count.
   int launch_step(bool thermo) {
     const int k = thermo ? 1 : 0;
+    ensure_graph(thermo);
+    if (k == 0) E.graph_kernels_ = graph_kernels[k];
+    CK(cudaGraphLaunch(graph[k], E.stream_));
+    return graph_kernels[k];
+  }
+  // Captures (or updates) the plain or thermo step graph when the run's key differs from the one it was made with.
+  void ensure_graph(bool thermo) {
+    const int k = thermo ? 1 : 0;
     std::string key = capture_key(thermo);
     if (!graph[k] || !graph_valid[k] || key != graph_key[k]) {
       cudaGraph_t g;
       CK(cudaStreamBeginCapture(E.stream_, cudaStreamCaptureModeThreadLocal));
-      step(thermo, thermo);
+      try {
+        step(thermo, thermo);
+      } catch (...) {   // leave no capture open behind an error
+        cudaGraph_t junk = nullptr;
+        (void)cudaStreamEndCapture(E.stream_, &junk);
+        if (junk) cudaGraphDestroy(junk);
+        (void)cudaGetLastError();
+        throw;
+      }
       CK(cudaStreamEndCapture(E.stream_, &g));
       size_t nn = 0;
       CK(cudaGraphGetNodes(g, nullptr, &nn));
       std::vector<cudaGraphNode_t> nodes(nn);
       CK(cudaGraphGetNodes(g, nodes.data(), &nn));
       int kernels = 0;
-      for (auto nd : nodes) {
-        cudaGraphNodeType ty;
-        CK(cudaGraphNodeGetType(nd, &ty));
-        kernels += ty == cudaGraphNodeTypeKernel;
-      }
+      for (auto nd : nodes) kernels += is_kernel_node(nd);
       graph_kernels[k] = kernels;
       bool updated = false;
       if (graph[k]) {
@@ -1153,9 +1172,6 @@ struct Stepper {
       graph_key[k] = capture_key(thermo);
       graph_valid[k] = graph_key[k] == key;
     }
-    if (k == 0) E.graph_kernels_ = graph_kernels[k];
-    CK(cudaGraphLaunch(graph[k], E.stream_));
-    return graph_kernels[k];
   }
 
   // --- step pieces (all asynchronous on E.stream_) ---
@@ -1770,6 +1786,12 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
     for (auto& e : tev) CK(cudaEventCreate(&e));
     if (timing_flush_ > 0) d_flush_.alloc(size_t(timing_flush_));
   }
+  // the step graphs are captured before the step loop, as set-up (like the first force evaluation), so that no step's
+  // time holds a capture
+  if (o.steps > 0 && !R.baro_due(1) && !R.refill_due(1)) {
+    S.ensure_graph(false);
+    S.ensure_graph(true);
+  }
   const auto w0 = std::chrono::steady_clock::now();
   CK(cudaEventRecord(ev0, stream_));
   for (long long s = 1; s <= o.steps; ++s) {
@@ -1820,9 +1842,9 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
     const double setup = std::chrono::duration<double>(w0 - t_enter).count();
     std::snprintf(b, sizeof b,
                   "%lld steps of %.2f fs in %.3f s (device %.3f s, set-up %.3f s) · %.2f ns/day · %d constraints · %.0f degrees of freedom · %s"
-                  " · tuned: %d entries per work item, PME line blocks %d/%d/%d",
+                  " · tuned: %d entries per work item, pair grid %d block(s) per SM short of full, PME line blocks %d/%d/%d, PME grid cap %d",
                   (long long)done, o.dt, wall, ms * 1e-3, setup, nsday, S.ncons, S.ndof, mixed_ ? "mixed FP32/fixed-point" : "FP64", batch_,
-                  lines_x_, lines_y_, lines_z_);
+                  pair_cut_, pme_lines()[0], pme_lines()[1], pme_lines()[2], pme_cap_);
     *report = b;
   }
   R.completed = true;
@@ -1916,12 +1938,20 @@ void run_batch(const std::vector<Engine*>& es, caps_gpu_state* const* states, co
       }
       cudaGraph_t graph;
       CK(cudaStreamBeginCapture(res.bs, cudaStreamCaptureModeThreadLocal));
-      CK(cudaEventRecord(res.fork, res.bs));
-      for (size_t r = 0; r < R; ++r) {
-        CK(cudaStreamWaitEvent(es[r]->stream_, res.fork, 0));
-        runs[r]->S.step(false, false);
-        CK(cudaEventRecord(res.ev[r], es[r]->stream_));
-        CK(cudaStreamWaitEvent(res.bs, res.ev[r], 0));
+      try {
+        CK(cudaEventRecord(res.fork, res.bs));
+        for (size_t r = 0; r < R; ++r) {
+          CK(cudaStreamWaitEvent(es[r]->stream_, res.fork, 0));
+          runs[r]->S.step(false, false);
+          CK(cudaEventRecord(res.ev[r], es[r]->stream_));
+          CK(cudaStreamWaitEvent(res.bs, res.ev[r], 0));
+        }
+      } catch (...) {   // leave no capture open behind an error
+        cudaGraph_t junk = nullptr;
+        (void)cudaStreamEndCapture(res.bs, &junk);
+        if (junk) cudaGraphDestroy(junk);
+        (void)cudaGetLastError();
+        throw;
       }
       CK(cudaStreamEndCapture(res.bs, &graph));
       size_t nn = 0;
@@ -1929,11 +1959,7 @@ void run_batch(const std::vector<Engine*>& es, caps_gpu_state* const* states, co
       std::vector<cudaGraphNode_t> nodes(nn);
       CK(cudaGraphGetNodes(graph, nodes.data(), &nn));
       graph_nodes = 0;
-      for (auto nd : nodes) {
-        cudaGraphNodeType ty;
-        CK(cudaGraphNodeGetType(nd, &ty));
-        graph_nodes += ty == cudaGraphNodeTypeKernel;
-      }
+      for (auto nd : nodes) graph_nodes += is_kernel_node(nd);
       CK(cudaGraphInstantiate(&res.g, graph, cudaGraphInstantiateFlagUseNodePriority));
       CK(cudaGraphDestroy(graph));
       for (size_t r = 0; r < R; ++r) seen[r] = runs[r]->generation;

@@ -35,7 +35,6 @@ static __global__ void k_check_step(int n, const double* __restrict__ x, const d
   if (__any_sync(0xffffffffu, mp) && lane0) atomicOr(counters + kCntPrune, 1);
 }
 
-
 // K-BIN: wrapped fractional coordinates, lattice offsets and the column of every atom; column counts.
 static __global__ void k_bin(int n, const double* __restrict__ x, DevCell cell, ListGeom g, ListBufs b) {
   if (build_off(b.counters)) return;

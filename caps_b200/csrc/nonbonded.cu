@@ -93,16 +93,47 @@ void Engine::tune_batch(const double* d_x) {
     CK(cudaEventElapsedTime(&ms, e0, e1));
     if (ms < best) best = ms, pick = bsz;
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   batch_ = pick;
   geom_.batch = pick;
   list_valid_ = false;   // the evaluation that follows builds the list with the chosen depth
+  // The pair kernel's persistent grid holds every SM slot while it runs, so the bonded and PME branches of the same
+  // evaluation wait for it to end unless it leaves room; PME's line transforms, on the other hand, run in fewer waves
+  // on the slots left when their grid is capped. Time whole force-only evaluations for each pair (pair grid full or one
+  // block per SM fewer; PME grid uncapped, one or two blocks per SM), in alternating rounds, and keep the fastest.
+  const int caps[3] = {0, dev_sms_, 2 * dev_sms_};
+  float bestc[2][3];
+  for (auto& r : bestc)
+    for (float& v : r) v = 1e30f;
+  for (int round = 0; round < 3; ++round)
+    for (int cut = 0; cut < 2; ++cut)
+      for (int ci = 0; ci < (pme_ ? 3 : 1); ++ci) {
+        pair_cut_ = cut;
+        pme_cap_ = caps[ci];
+        for (int rep = 0; rep < 4; ++rep) {
+          if (rep == 1) CK(cudaEventRecord(e0, stream_));
+          forces(d_x, false, false, false);
+        }
+        CK(cudaEventRecord(e1, stream_));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        bestc[cut][ci] = std::min(bestc[cut][ci], ms);
+      }
+  int bc = 0, bi = 0;
+  for (int cut = 0; cut < 2; ++cut)
+    for (int ci = 0; ci < 3; ++ci)
+      if (bestc[cut][ci] < bestc[bc][bi]) bc = cut, bi = ci;
+  pair_cut_ = bc;
+  pme_cap_ = caps[bi];
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
 }
 
-int Engine::list_builds() {
+int Engine::list_builds() { return counter(kCntBuilds); }
+
+int Engine::counter(int slot) {
   int v = 0;
-  CK(cudaMemcpyAsync(&v, d_counters_.p + kCntBuilds, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+  CK(cudaMemcpyAsync(&v, d_counters_.p + slot, sizeof(int), cudaMemcpyDeviceToHost, stream_));
   CK(cudaStreamSynchronize(stream_));
   return v;
 }
@@ -176,7 +207,8 @@ void Engine::prune(const double* d_x) {
 void Engine::pair_forces(bool ener, bool vir) {
   PairArgs A = pair_args();
   const int coul = coul_ ? (pme_ ? 1 : 2) : 0;
-  // persistent grids: as many blocks as fit on the SMs at once; their warps fetch work items until none are left
+  // persistent grids: as many blocks as fit on the SMs at once (less pair_cut_ per SM, the tuner's choice); their warps
+  // fetch work items until none are left
   const int ntab = nt_ + 1;
   if (mixed_) {
     // LJ table, the 4 warps' i atoms, and their staged entries with the entries' j atoms and exclusion masks
@@ -189,7 +221,7 @@ void Engine::pair_forces(bool ener, bool vir) {
     if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_pair_f32<C, E, V, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
     int per_sm = 0;                                                                                                  \
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_f32<C, E, V, L>, 128, smem));                   \
-    launch_k(k_pair_f32<C, E, V, L>, dev_sms_ * std::max(1, per_sm), 128, smem, stream_, A);                               \
+    launch_k(k_pair_f32<C, E, V, L>, dev_sms_ * std::max(1, per_sm - pair_cut_), 128, smem, stream_, A);                               \
   } while (0)
 #define PAIR32(C, E, V)                                                                                              \
   do {                                                                                                               \
@@ -214,7 +246,7 @@ void Engine::pair_forces(bool ener, bool vir) {
     if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_pair_f64<C, E, V, CAP, L, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
     int per_sm = 0;                                                                                                  \
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_f64<C, E, V, CAP, L, F>, 128, smem));           \
-    launch_k(k_pair_f64<C, E, V, CAP, L, F>, dev_sms_ * std::max(1, per_sm), 128, smem, stream_, A);                       \
+    launch_k(k_pair_f64<C, E, V, CAP, L, F>, dev_sms_ * std::max(1, per_sm - pair_cut_), 128, smem, stream_, A);                       \
   } while (0)
 #define PAIR64L(C, E, V, CAP, L) PAIR64LF(C, E, V, CAP, L, false)
 #define PAIR64(C, E, V, CAP)                                                                                         \
@@ -332,7 +364,8 @@ void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild, 
       list_valid_ = true;
     } else if (check_rebuild) {
       const double b = std::min(0.8, skin_);   // the prune margin (see prune())
-      launch_k(k_check_step, blocks_for(size_t(n_), 256), 256, 0, stream_, n_, d_x, d_x0_.p, 0.25 * skin_ * skin_, d_xp_.p, 0.25 * b * b, d_counters_.p);
+      launch_k(k_check_step, blocks_for(size_t(n_), 256), 256, 0, stream_, n_, d_x, d_x0_.p, 0.25 * skin_ * skin_, d_xp_.p, 0.25 * b * b,
+               d_counters_.p);
     }
     if (!frozen_) launch_build(d_x);
     const size_t ns = size_t(nsc_cap_) * kScAtoms;

@@ -56,13 +56,27 @@ void Engine::pme_setup(PmePath<R>& P) {
   // y, z: `la` consecutive a per block so that each row read is 128 bytes.
   const int cap = int(40 * 1024 / (2 * sizeof(T)));
   const int nlx = pk_[1] * pk_[2];
-  lines_x_ = std::max(1, std::min({cap / pk_[0], 16, (nlx + 4 * dev_sms_ - 1) / (4 * dev_sms_)}));
+  P.lines[0] = std::max(1, std::min({cap / pk_[0], 16, (nlx + 4 * dev_sms_ - 1) / (4 * dev_sms_)}));
   const int la = int(128 / sizeof(T));
-  lines_y_ = std::max(1, std::min({la, cap / pk_[1], ph1_}));
-  lines_z_ = std::max(1, std::min({la, cap / pk_[2], ph1_}));
+  P.lines[1] = std::max(1, std::min({la, cap / pk_[1], ph1_}));
+  P.lines[2] = std::max(1, std::min({la, cap / pk_[2], ph1_}));
   pme_tune(P);
+  for (int d = 0; d < 3; ++d) P.k[d] = pk_[d];
   green_valid_ = false;
   CK(cudaStreamSynchronize(stream_));
+}
+
+// The mixed path transforms in FP32 (pf_), the FP64 path in FP64 (pd_); each path is set up for the current grid on
+// first use.
+void Engine::ensure_pme() {
+  if (!pme_ || pk_[0] == 0) return;
+  auto same = [&](const int* k) { return k[0] == pk_[0] && k[1] == pk_[1] && k[2] == pk_[2]; };
+  if (mixed_) {
+    if (!same(pf_.k)) pme_setup(pf_);
+    d_gridq_.alloc(size_t(pk_[0]) * pk_[1] * pk_[2]);
+  } else if (!same(pd_.k)) {
+    pme_setup(pd_);
+  }
 }
 
 // The five line-transform passes of one PME evaluation (forward x, y; z with the solve; inverse y, x).
@@ -71,19 +85,22 @@ void Engine::fft_passes(PmePath<R>& P, bool ener, bool vir) {
   using T = typename Cpx<R>::T;
   PmeArgs A{pk_[0], pk_[1], pk_[2], ph1_, dcell_, nullptr, d_q_.p, n_};
   // shared memory: twiddle table(s) + two line buffers
-  const size_t sx = (size_t(lines_x_) * 2 + 1) * pk_[0] * sizeof(T), sy = (size_t(lines_y_) * 2 + 1) * pk_[1] * sizeof(T),
-               sz = (size_t(lines_z_) + 1) * 2 * pk_[2] * sizeof(T);
+  const size_t sx = (size_t(P.lines[0]) * 2 + 1) * pk_[0] * sizeof(T), sy = (size_t(P.lines[1]) * 2 + 1) * pk_[1] * sizeof(T),
+               sz = (size_t(P.lines[2]) + 1) * 2 * pk_[2] * sizeof(T);
   const int nlx = pk_[1] * pk_[2];
-  launch_k(k_fft_x_fwd<R>, blocks_for(size_t(nlx), lines_x_), 128, sx, stream_, A, mixed_ ? nullptr : d_grid_.p, mixed_ ? d_gridq_.p : nullptr, P.h.p,
-                                                                        P.plan[0][0], lines_x_);
-  const int gy = ((ph1_ + lines_y_ - 1) / lines_y_) * pk_[2];
-  launch_k(k_fft_y<R>, gy, 128, sy, stream_, A, P.h.p, P.plan[1][0], lines_y_);
-  const int gz = ((ph1_ + lines_z_ - 1) / lines_z_) * pk_[1];
+  // the kernels stride over their line groups: a grid cap (the tuner's pme_cap_, 0 for none) leaves SM slots to the
+  // pair kernel that runs beside them
+  auto capped = [&](int g) { return pme_cap_ > 0 ? std::min(g, pme_cap_) : g; };
+  launch_k(k_fft_x_fwd<R>, capped(blocks_for(size_t(nlx), P.lines[0])), 128, sx, stream_, A, mixed_ ? nullptr : d_grid_.p, mixed_ ? d_gridq_.p : nullptr, P.h.p,
+                                                                        P.plan[0][0], P.lines[0]);
+  const int gy = capped(((ph1_ + P.lines[1] - 1) / P.lines[1]) * pk_[2]);
+  launch_k(k_fft_y<R>, gy, 128, sy, stream_, A, P.h.p, P.plan[1][0], P.lines[1]);
+  const int gz = capped(((ph1_ + P.lines[2] - 1) / P.lines[2]) * pk_[1]);
   EnergySink en{d_efix_.p, d_edbl_.p};
-  if (ener) { if (vir) launch_k(k_fft_z_solve<R, true, true>, gz, 128, sz, stream_, A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); else launch_k(k_fft_z_solve<R, true, false>, gz, 128, sz, stream_, A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); }
-  else { if (vir) launch_k(k_fft_z_solve<R, false, true>, gz, 128, sz, stream_, A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); else launch_k(k_fft_z_solve<R, false, false>, gz, 128, sz, stream_, A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], lines_z_, en, mixed_); }
-  launch_k(k_fft_y<R>, gy, 128, sy, stream_, A, P.h.p, P.plan[1][1], lines_y_);
-  launch_k(k_fft_x_inv<R>, blocks_for(size_t(nlx), lines_x_), 128, sx, stream_, A, P.h.p, P.gr.p, P.plan[0][1], lines_x_);
+  if (ener) { if (vir) launch_k(k_fft_z_solve<R, true, true>, gz, 128, sz, stream_, A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], P.lines[2], en, mixed_); else launch_k(k_fft_z_solve<R, true, false>, gz, 128, sz, stream_, A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], P.lines[2], en, mixed_); }
+  else { if (vir) launch_k(k_fft_z_solve<R, false, true>, gz, 128, sz, stream_, A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], P.lines[2], en, mixed_); else launch_k(k_fft_z_solve<R, false, false>, gz, 128, sz, stream_, A, P.h.p, P.gt.p, P.wt.p, P.plan[2][0], P.plan[2][1], P.lines[2], en, mixed_); }
+  launch_k(k_fft_y<R>, gy, 128, sy, stream_, A, P.h.p, P.plan[1][1], P.lines[1]);
+  launch_k(k_fft_x_inv<R>, capped(blocks_for(size_t(nlx), P.lines[0])), 128, sx, stream_, A, P.h.p, P.gr.p, P.plan[0][1], P.lines[0]);
 }
 
 // Autotuner for the line transforms: every block shape that fits (x: 1-16 lines per block; y, z: 1-8 consecutive a per
@@ -99,7 +116,7 @@ void Engine::pme_tune(PmePath<R>& P) {
     std::lock_guard<std::mutex> lock(mu);
     auto it = cache.find(key);
     if (it != cache.end()) {
-      lines_x_ = it->second[0], lines_y_ = it->second[1], lines_z_ = it->second[2];
+      P.lines[0] = it->second[0], P.lines[1] = it->second[1], P.lines[2] = it->second[2];
       return;
     }
   }
@@ -114,13 +131,13 @@ void Engine::pme_tune(PmePath<R>& P) {
   CK(cudaEventCreate(&e1));
   const size_t smax = 48 * 1024;
   float best = 1e30f;
-  std::array<int, 3> pick{lines_x_, lines_y_, lines_z_};
+  std::array<int, 3> pick{P.lines[0], P.lines[1], P.lines[2]};
   for (int lx : {1, 2, 4, 8, 16})
     for (int la : {1, 2, 4, 8}) {
       if ((size_t(lx) * 2 + 1) * pk_[0] * sizeof(T) > smax) continue;
       const int ly = std::min(la, ph1_), lz = std::min(la, ph1_);
       if ((size_t(ly) * 2 + 1) * pk_[1] * sizeof(T) > smax || (size_t(lz) + 1) * 2 * pk_[2] * sizeof(T) > smax) continue;
-      lines_x_ = lx, lines_y_ = ly, lines_z_ = lz;
+      P.lines[0] = lx, P.lines[1] = ly, P.lines[2] = lz;
       fft_passes(P, false, false);   // warm
       CK(cudaEventRecord(e0, stream_));
       for (int rep = 0; rep < 3; ++rep) fft_passes(P, false, false);
@@ -132,7 +149,7 @@ void Engine::pme_tune(PmePath<R>& P) {
     }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  lines_x_ = pick[0], lines_y_ = pick[1], lines_z_ = pick[2];
+  P.lines[0] = pick[0], P.lines[1] = pick[1], P.lines[2] = pick[2];
   std::lock_guard<std::mutex> lock(mu);
   cache[key] = pick;
 }
@@ -184,12 +201,19 @@ void Engine::pme_run(PmePath<R>& P, const double* d_x, bool ener, bool vir) {
   CK(cudaGetLastError());
 }
 
-void Engine::pme_forces(const double* d_x, bool ener, bool vir) { pme_run(pd_, d_x, ener, vir); }
+void Engine::pme_forces(const double* d_x, bool ener, bool vir) {
+  if (mixed_) pme_run(pf_, d_x, ener, vir);
+  else pme_run(pd_, d_x, ener, vir);
+}
 
 
 template void Engine::pme_setup<double>(PmePath<double>&);
 template void Engine::pme_run<double>(PmePath<double>&, const double*, bool, bool);
 template void Engine::fft_passes<double>(PmePath<double>&, bool, bool);
 template void Engine::pme_tune<double>(PmePath<double>&);
+template void Engine::pme_setup<float>(PmePath<float>&);
+template void Engine::pme_run<float>(PmePath<float>&, const double*, bool, bool);
+template void Engine::fft_passes<float>(PmePath<float>&, bool, bool);
+template void Engine::pme_tune<float>(PmePath<float>&);
 
 }  // namespace capsb

@@ -191,19 +191,22 @@ static __global__ void __launch_bounds__(128) k_fft_x_fwd(PmeArgs A, const doubl
   T* s0 = tw + A.k1;
   T* s1 = s0 + lines_per_block * A.k1;
   const int nlines = A.k2 * A.k3;
-  const int l0 = blockIdx.x * lines_per_block;
-  const int nl = min(lines_per_block, nlines - l0);
   stage_twiddles(tw, P.tw, A.k1);
-  for (int t = threadIdx.x; t < nl * A.k1; t += blockDim.x) {
-    const size_t gidx = size_t(l0) * A.k1 + t;   // lines are contiguous in the real grid
-    const R v = gq ? R(double(gq[gidx]) * kInvFixQ) : R(g[gidx]);
-    s0[t] = {v, R(0)};
-  }
-  __syncthreads();
-  const T* res = fft_lines_smem<R>(s0, s1, tw, nl, P);
-  for (int t = threadIdx.x; t < nl * A.h1; t += blockDim.x) {
-    const int l = t / A.h1, a = t - l * A.h1;
-    h[size_t(l0 + l) * A.h1 + a] = res[l * A.k1 + a];
+  // groups of lines_per_block lines, strided over the grid (the grid may be smaller than the group count)
+  for (int l0 = blockIdx.x * lines_per_block; l0 < nlines; l0 += gridDim.x * lines_per_block) {
+    const int nl = min(lines_per_block, nlines - l0);
+    for (int t = threadIdx.x; t < nl * A.k1; t += blockDim.x) {
+      const size_t gidx = size_t(l0) * A.k1 + t;   // lines are contiguous in the real grid
+      const R v = gq ? R(double(gq[gidx]) * kInvFixQ) : R(g[gidx]);
+      s0[t] = {v, R(0)};
+    }
+    __syncthreads();
+    const T* res = fft_lines_smem<R>(s0, s1, tw, nl, P);
+    for (int t = threadIdx.x; t < nl * A.h1; t += blockDim.x) {
+      const int l = t / A.h1, a = t - l * A.h1;
+      h[size_t(l0 + l) * A.h1 + a] = res[l * A.k1 + a];
+    }
+    __syncthreads();
   }
 }
 
@@ -217,23 +220,25 @@ static __global__ void __launch_bounds__(128) k_fft_x_inv(PmeArgs A, const typen
   T* s0 = tw + A.k1;
   T* s1 = s0 + lines_per_block * A.k1;
   const int nlines = A.k2 * A.k3;
-  const int l0 = blockIdx.x * lines_per_block;
-  const int nl = min(lines_per_block, nlines - l0);
   stage_twiddles(tw, P.tw, A.k1);
-  for (int t = threadIdx.x; t < nl * A.k1; t += blockDim.x) {
-    const int l = t / A.k1, m = t - l * A.k1;
-    const size_t lb = size_t(l0 + l) * A.h1;
-    T v;
-    if (m <= A.k1 / 2) v = h[lb + m];
-    else {
-      const T c = h[lb + (A.k1 - m)];
-      v = {c.x, -c.y};
+  for (int l0 = blockIdx.x * lines_per_block; l0 < nlines; l0 += gridDim.x * lines_per_block) {
+    const int nl = min(lines_per_block, nlines - l0);
+    for (int t = threadIdx.x; t < nl * A.k1; t += blockDim.x) {
+      const int l = t / A.k1, m = t - l * A.k1;
+      const size_t lb = size_t(l0 + l) * A.h1;
+      T v;
+      if (m <= A.k1 / 2) v = h[lb + m];
+      else {
+        const T c = h[lb + (A.k1 - m)];
+        v = {c.x, -c.y};
+      }
+      s0[t] = v;
     }
-    s0[t] = v;
+    __syncthreads();
+    const T* res = fft_lines_smem<R>(s0, s1, tw, nl, P);
+    for (int t = threadIdx.x; t < nl * A.k1; t += blockDim.x) gr[size_t(l0) * A.k1 + t] = res[t].x;
+    __syncthreads();
   }
-  __syncthreads();
-  const T* res = fft_lines_smem<R>(s0, s1, tw, nl, P);
-  for (int t = threadIdx.x; t < nl * A.k1; t += blockDim.x) gr[size_t(l0) * A.k1 + t] = res[t].x;
 }
 
 // K-FFT-Y: lines along b for fixed (a, c); a block takes `la` consecutive a (coalesced rows) of one c.
@@ -245,18 +250,21 @@ static __global__ void __launch_bounds__(128) k_fft_y(PmeArgs A, typename Cpx<R>
   T* s0 = tw + A.k2;
   T* s1 = s0 + la * A.k2;
   const int ngrp = (A.h1 + la - 1) / la;
-  const int c = blockIdx.x / ngrp, a0 = (blockIdx.x % ngrp) * la;
-  const int nl = min(la, A.h1 - a0);
   stage_twiddles(tw, P.tw, A.k2);
-  for (int t = threadIdx.x; t < nl * A.k2; t += blockDim.x) {
-    const int b = t / nl, al = t - b * nl;
-    s0[al * A.k2 + b] = h[size_t(a0 + al) + size_t(A.h1) * (size_t(b) + size_t(A.k2) * c)];
-  }
-  __syncthreads();
-  const T* res = fft_lines_smem<R>(s0, s1, tw, nl, P);
-  for (int t = threadIdx.x; t < nl * A.k2; t += blockDim.x) {
-    const int b = t / nl, al = t - b * nl;
-    h[size_t(a0 + al) + size_t(A.h1) * (size_t(b) + size_t(A.k2) * c)] = res[al * A.k2 + b];
+  for (int grp = blockIdx.x; grp < ngrp * A.k3; grp += gridDim.x) {
+    const int c = grp / ngrp, a0 = (grp % ngrp) * la;
+    const int nl = min(la, A.h1 - a0);
+    for (int t = threadIdx.x; t < nl * A.k2; t += blockDim.x) {
+      const int b = t / nl, al = t - b * nl;
+      s0[al * A.k2 + b] = h[size_t(a0 + al) + size_t(A.h1) * (size_t(b) + size_t(A.k2) * c)];
+    }
+    __syncthreads();
+    const T* res = fft_lines_smem<R>(s0, s1, tw, nl, P);
+    for (int t = threadIdx.x; t < nl * A.k2; t += blockDim.x) {
+      const int b = t / nl, al = t - b * nl;
+      h[size_t(a0 + al) + size_t(A.h1) * (size_t(b) + size_t(A.k2) * c)] = res[al * A.k2 + b];
+    }
+    __syncthreads();
   }
 }
 
@@ -273,53 +281,76 @@ static __global__ void __launch_bounds__(128) k_fft_z_solve(PmeArgs A, typename 
   T* s0 = twi + A.k3;
   T* s1 = s0 + la * A.k3;
   const int ngrp = (A.h1 + la - 1) / la;
-  const int b = blockIdx.x / ngrp, a0 = (blockIdx.x % ngrp) * la;
-  const int nl = min(la, A.h1 - a0);
   const size_t plane = size_t(A.h1) * A.k2;
   stage_twiddles(twf, Pf.tw, A.k3);
   stage_twiddles(twi, Pi.tw, A.k3);
-  for (int t = threadIdx.x; t < nl * A.k3; t += blockDim.x) {
-    const int c = t / nl, al = t - c * nl;
-    s0[al * A.k3 + c] = h[size_t(a0 + al) + size_t(A.h1) * b + plane * c];
-  }
-  __syncthreads();
-  T* res = fft_lines_smem<R>(s0, s1, twf, nl, Pf);
-  T* other = res == s0 ? s1 : s0;
   double e = 0, w[6] = {0, 0, 0, 0, 0, 0};
-  for (int t = threadIdx.x; t < nl * A.k3; t += blockDim.x) {
-    const int al = t / A.k3, c = t - al * A.k3;
-    const int a = a0 + al;
-    const size_t gi = size_t(a) + size_t(A.h1) * b + plane * c;
-    T v = res[t];
-    const R G = gt[gi];
-    if (ENER || VIR) {
-      double em = 0.5 * (double(v.x) * v.x + double(v.y) * v.y);
-      if (a > 0 && 2 * a != A.k1) em *= 2;
-      if (ENER) e += em * double(G);
-      if (VIR)
-        for (int k = 0; k < 6; ++k) w[k] += em * double(wt[6 * gi + k]);
+  long long ef = 0, wf[6] = {0, 0, 0, 0, 0, 0};
+  for (int grp = blockIdx.x; grp < ngrp * A.k2; grp += gridDim.x) {
+    const int b = grp / ngrp, a0 = (grp % ngrp) * la;
+    const int nl = min(la, A.h1 - a0);
+    for (int t = threadIdx.x; t < nl * A.k3; t += blockDim.x) {
+      const int c = t / nl, al = t - c * nl;
+      s0[al * A.k3 + c] = h[size_t(a0 + al) + size_t(A.h1) * b + plane * c];
     }
-    v.x *= G;
-    v.y *= G;
-    res[t] = v;
+    __syncthreads();
+    T* res = fft_lines_smem<R>(s0, s1, twf, nl, Pf);
+    T* other = res == s0 ? s1 : s0;
+    for (int t = threadIdx.x; t < nl * A.k3; t += blockDim.x) {
+      const int al = t / A.k3, c = t - al * A.k3;
+      const int a = a0 + al;
+      const size_t gi = size_t(a) + size_t(A.h1) * b + plane * c;
+      T v = res[t];
+      const R G = gt[gi];
+      if (ENER || VIR) {
+        double em = 0.5 * (double(v.x) * v.x + double(v.y) * v.y);
+        if (a > 0 && 2 * a != A.k1) em *= 2;
+        // mixed path: every term rounded to fixed point on its own, so the sum does not depend on which block took
+        // which line group
+        if (ENER) {
+          if (fixed) ef += to_fix(em * double(G), kFixE);
+          else e += em * double(G);
+        }
+        if (VIR)
+          for (int k = 0; k < 6; ++k) {
+            if (fixed) wf[k] += to_fix(em * double(wt[6 * gi + k]), kFixE);
+            else w[k] += em * double(wt[6 * gi + k]);
+          }
+      }
+      v.x *= G;
+      v.y *= G;
+      res[t] = v;
+    }
+    __syncthreads();
+    const T* back = fft_lines_smem<R>(res, other, twi, nl, Pi);
+    for (int t = threadIdx.x; t < nl * A.k3; t += blockDim.x) {
+      const int c = t / nl, al = t - c * nl;
+      h[size_t(a0 + al) + size_t(A.h1) * b + plane * c] = back[al * A.k3 + c];
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  const T* back = fft_lines_smem<R>(res, other, twi, nl, Pi);
-  for (int t = threadIdx.x; t < nl * A.k3; t += blockDim.x) {
-    const int c = t / nl, al = t - c * nl;
-    h[size_t(a0 + al) + size_t(A.h1) * b + plane * c] = back[al * A.k3 + c];
-  }
-  if (ENER || VIR) {
+  if ((ENER || VIR) && fixed) {
+    __shared__ long long scratch_q[32];
+    if (ENER) {
+      const long long s = block_sum(ef, scratch_q);
+      if (threadIdx.x == 0) atomic_add_fix(en.fix + kECoul, s), atomic_add_fix(en.fix + kEPmeRecip, s);
+    }
+    if (VIR)
+      for (int k = 0; k < 6; ++k) {
+        const long long s = block_sum(wf[k], scratch_q);
+        if (threadIdx.x == 0) atomic_add_fix(en.fix + kEW0 + k, s);
+      }
+  } else if (ENER || VIR) {
     __shared__ double scratch[32];
     if (ENER) {
       const double s = block_sum(e, scratch);
-      if (threadIdx.x == 0) en.add(kECoul, s, fixed);
-      if (threadIdx.x == 0) en.add(kEPmeRecip, s, fixed);
+      if (threadIdx.x == 0) en.add(kECoul, s, false);
+      if (threadIdx.x == 0) en.add(kEPmeRecip, s, false);
     }
     if (VIR)
       for (int k = 0; k < 6; ++k) {
         const double s = block_sum(w[k], scratch);
-        if (threadIdx.x == 0) en.add(kEW0 + k, s, fixed);
+        if (threadIdx.x == 0) en.add(kEW0 + k, s, false);
       }
   }
 }
