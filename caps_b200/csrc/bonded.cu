@@ -22,7 +22,7 @@ void Engine::bonded_forces(const double* d_x, bool ener, bool vir, int parts) {
     if (cnt <= 0) return;
     W.kind[W.nseg] = kind;
     W.first[W.nseg] = blocks;
-    blocks += std::min(blocks_for(size_t(cnt), T), dev_sms_ * 4);
+    blocks += std::min(blocks_for(size_t(cnt), T), bonded_cap_ > 0 ? bonded_cap_ : dev_sms_ * 4);
     ++W.nseg;
   };
   if (bonded) {

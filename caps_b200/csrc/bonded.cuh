@@ -18,31 +18,57 @@ struct BondedArgs {
   int fixed;   // 1: mixed path (fixed-point sinks)
 };
 
-// Per-thread energy and virial, summed over the block and added once.
+// Per-thread energy and virial, summed over the block and added once. On the mixed path (fixed) every term is rounded
+// to fixed point on its own, so that the sums do not depend on how the terms are spread over threads and blocks.
 template <bool VIR>
 struct Tally {
+  bool fixed;
   double e = 0;
   double w[6] = {0, 0, 0, 0, 0, 0};
+  long long eq = 0;
+  long long wq[6] = {0, 0, 0, 0, 0, 0};
+  __device__ explicit Tally(bool f) : fixed(f) {}
+  __device__ __forceinline__ void energy(double v) {
+    if (fixed) eq += to_fix(v, kFixE);
+    else e += v;
+  }
+  __device__ __forceinline__ void wadd(int k, double v) {
+    if (fixed) wq[k] += to_fix(v, kFixE);
+    else w[k] += v;
+  }
   template <class R>
   __device__ __forceinline__ void vir(R dx, R dy, R dz, R fx, R fy, R fz) {
     if (!VIR) return;
-    w[0] += double(dx * fx);
-    w[1] += double(dy * fy);
-    w[2] += double(dz * fz);
-    w[3] += 0.5 * double(dx * fy + dy * fx);
-    w[4] += 0.5 * double(dx * fz + dz * fx);
-    w[5] += 0.5 * double(dy * fz + dz * fy);
+    wadd(0, double(dx * fx));
+    wadd(1, double(dy * fy));
+    wadd(2, double(dz * fz));
+    wadd(3, 0.5 * double(dx * fy + dy * fx));
+    wadd(4, 0.5 * double(dx * fz + dz * fx));
+    wadd(5, 0.5 * double(dy * fz + dz * fy));
   }
   __device__ void flush(const BondedArgs& A, int slot, bool ener) {
+    if (fixed) {
+      __shared__ long long scratch_q[32];
+      if (ener) {
+        const long long s = block_sum(eq, scratch_q);
+        if (threadIdx.x == 0 && s != 0) atomic_add_fix(A.en.fix + slot, s);
+      }
+      if (VIR)
+        for (int k = 0; k < 6; ++k) {
+          const long long s = block_sum(wq[k], scratch_q);
+          if (threadIdx.x == 0 && s != 0) atomic_add_fix(A.en.fix + kEW0 + k, s);
+        }
+      return;
+    }
     __shared__ double scratch[32];
     if (ener) {
       const double s = block_sum(e, scratch);
-      if (threadIdx.x == 0 && s != 0) A.en.add(slot, s, A.fixed);
+      if (threadIdx.x == 0 && s != 0) A.en.add(slot, s, false);
     }
     if (VIR)
       for (int k = 0; k < 6; ++k) {
         const double s = block_sum(w[k], scratch);
-        if (threadIdx.x == 0 && s != 0) A.en.add(kEW0 + k, s, A.fixed);
+        if (threadIdx.x == 0 && s != 0) A.en.add(kEW0 + k, s, false);
       }
   }
 };
@@ -60,14 +86,14 @@ template <> __device__ __forceinline__ float rsq<float>(float v) { return sqrtf(
 // harmonic bonds: k (r - r0)^2
 template <class R, class S, bool ENER, bool VIR>
 __device__ __forceinline__ void bonds_body(int blk, int nblk, int nb, const uint32_t* __restrict__ ij, const double* __restrict__ kr, BondedArgs A, S F) {
-  Tally<VIR> T;
+  Tally<VIR> T(A.fixed != 0);
   for (int t = blk * blockDim.x + threadIdx.x; t < nb; t += nblk * blockDim.x) {
     const int i = int(ij[2 * t]), j = int(ij[2 * t + 1]);
     R dx, dy, dz;
     sep(A, i, j, dx, dy, dz);
     const R k = R(kr[2 * t]), r0 = R(kr[2 * t + 1]);
     const R r = rsq(dx * dx + dy * dy + dz * dz), dr = r - r0;
-    if (ENER) T.e += double(k * dr * dr);
+    if (ENER) T.energy(double(k * dr * dr));
     const R s = r > R(1e-12) ? -2 * k * dr / r : R(0);
     const R fx = dx * s, fy = dy * s, fz = dz * s;
     F.add(j, fx, fy, fz);
@@ -80,7 +106,7 @@ __device__ __forceinline__ void bonds_body(int blk, int nblk, int nb, const uint
 // harmonic angles: kt (theta - theta0)^2, j the vertex
 template <class R, class S, bool ENER, bool VIR>
 __device__ __forceinline__ void angles_body(int blk, int nblk, int na, const uint32_t* __restrict__ ijk, const double* __restrict__ kt0, BondedArgs A, S F) {
-  Tally<VIR> T;
+  Tally<VIR> T(A.fixed != 0);
   for (int t = blk * blockDim.x + threadIdx.x; t < na; t += nblk * blockDim.x) {
     const int i = int(ijk[3 * t]), j = int(ijk[3 * t + 1]), k = int(ijk[3 * t + 2]);
     R ux, uy, uz, vx, vy, vz;
@@ -94,7 +120,7 @@ __device__ __forceinline__ void angles_body(int blk, int nblk, int na, const uin
     sn = sn > R(1e-8) ? sn : R(1e-8);
     const R dth = th - R(kt0[2 * t + 1]);
     const R kk = R(kt0[2 * t]);
-    if (ENER) T.e += double(kk * dth * dth);
+    if (ENER) T.energy(double(kk * dth * dth));
     const R g = 2 * kk * dth / sn;
     const R iuv = R(1) / (lu * lv), cu = c / (lu * lu), cv = c / (lv * lv);
     const R fix = (vx * iuv - ux * cu) * g, fiy = (vy * iuv - uy * cu) * g, fiz = (vz * iuv - uz * cu) * g;
@@ -113,7 +139,7 @@ __device__ __forceinline__ void angles_body(int blk, int nblk, int na, const uin
 template <class R, class S, bool ENER, bool VIR>
 __device__ __forceinline__ void torsions_body(int blk, int nblk, int ngroups, const int* __restrict__ gs, const uint32_t* __restrict__ ijkl, const double* __restrict__ vd,
                            const int* __restrict__ nn, BondedArgs A, S F, int slot) {
-  Tally<VIR> T;
+  Tally<VIR> T(A.fixed != 0);
   for (int g = blk * blockDim.x + threadIdx.x; g < ngroups; g += nblk * blockDim.x) {
     const int t0 = gs[g], t1 = gs[g + 1];
     const int i = int(ijkl[4 * t0]), j = int(ijkl[4 * t0 + 1]), k = int(ijkl[4 * t0 + 2]), l = int(ijkl[4 * t0 + 3]);
@@ -153,7 +179,7 @@ __device__ __forceinline__ void torsions_body(int blk, int nblk, int ngroups, co
       e += v * (1 + cn * cd + sn * sd);
       dEdphi -= v * R(n) * (sn * cd - cn * sd);
     }
-    if (ENER) T.e += double(e);
+    if (ENER) T.energy(double(e));
     const R g1x = mx * (-lb2 / m2), g1y = my * (-lb2 / m2), g1z = mz * (-lb2 / m2);
     const R g4x = nx * (lb2 / n2), g4y = ny * (lb2 / n2), g4z = nz * (lb2 / n2);
     const R p = (b1x * b2x + b1y * b2y + b1z * b2z) / (lb2 * lb2), qd = (b3x * b2x + b3y * b2y + b3z * b2z) / (lb2 * lb2);
@@ -177,7 +203,7 @@ __device__ __forceinline__ void torsions_body(int blk, int nblk, int ngroups, co
 template <class R, class S, bool ENER, bool VIR>
 __device__ __forceinline__ void pairs14_body(int blk, int nblk, int np, const uint32_t* __restrict__ ij, const double* __restrict__ scale, double lj14, const int* __restrict__ type, int nt,
                           const double4* __restrict__ lj, const double4* __restrict__ cap, BondedArgs A, S F, int lj96) {
-  Tally<VIR> T;
+  Tally<VIR> T(A.fixed != 0);
   for (int t = blk * blockDim.x + threadIdx.x; t < np; t += nblk * blockDim.x) {
     const int i = int(ij[2 * t]), j = int(ij[2 * t + 1]);
     R dx, dy, dz;
@@ -203,7 +229,7 @@ __device__ __forceinline__ void pairs14_body(int blk, int nblk, int np, const ui
         fr = sc * 24 * R(c.x) * (2 * q * q - q) / r2;
       }
     }
-    if (ENER) T.e += double(ev - sc * R(c.z));
+    if (ENER) T.energy(double(ev - sc * R(c.z)));
     const R fx = dx * fr, fy = dy * fr, fz = dz * fr;
     F.add(j, fx, fy, fz);
     F.add(i, -fx, -fy, -fz);
@@ -234,7 +260,7 @@ __device__ __forceinline__ double erfc_as(double x, double& ex2) {   // Abramowi
 
 template <class S, bool ENER, bool VIR>
 __device__ __forceinline__ void excl_body(int blk, int nblk, int nx, ExclArgs E, BondedArgs A, S F) {
-  Tally<VIR> T;
+  Tally<VIR> T(A.fixed != 0);
   const double sp = 2 / sqrt(kPi), kap = E.kappa;
   for (int t = blk * blockDim.x + threadIdx.x; t < nx; t += nblk * blockDim.x) {
     const int i = int(E.ij[2 * t]), j = int(E.ij[2 * t + 1]);
@@ -274,7 +300,7 @@ __device__ __forceinline__ void excl_body(int blk, int nblk, int nx, ExclArgs E,
       e = qq * er / r - (1 - f) * qq / r;
       fr = qq * ((er / r2 + sp * kap * ex2 / r) - (1 - f) / r2) / r;
     }
-    if (ENER) T.e += e;
+    if (ENER) T.energy(e);
     const double fx = dx * fr, fy = dy * fr, fz = dz * fr;
     F.add(j, fx, fy, fz);
     F.add(i, -fx, -fy, -fz);
@@ -288,7 +314,7 @@ __device__ __forceinline__ void excl_body(int blk, int nblk, int nx, ExclArgs E,
 template <class R, class S, bool ENER, bool VIR>
 __device__ __forceinline__ void fene_body(int blk, int nblk, int nf, const uint32_t* __restrict__ ij, const double* __restrict__ p, BondedArgs A, S F, int* counters,
                                           double* info) {
-  Tally<VIR> T;
+  Tally<VIR> T(A.fixed != 0);
   for (int t = blk * blockDim.x + threadIdx.x; t < nf; t += nblk * blockDim.x) {
     const int i = int(ij[2 * t]), j = int(ij[2 * t + 1]);
     R dx, dy, dz;
@@ -313,7 +339,7 @@ __device__ __forceinline__ void fene_body(int blk, int nblk, int nf, const uint3
       e += 4 * eps * (s6 * s6 - s6) + eps;
       dEdr += -24 * eps * (2 * s6 * s6 - s6) / r;
     }
-    if (ENER) T.e += double(e);
+    if (ENER) T.energy(double(e));
     const R s = r > R(1e-12) ? -dEdr / r : R(0);
     const R fx = dx * s, fy = dy * s, fz = dz * s;
     F.add(j, fx, fy, fz);

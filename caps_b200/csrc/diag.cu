@@ -21,6 +21,9 @@ void Engine::time_pair_kernel(const double* x, const double* cell, int launches,
   for (auto& e : ev) {
     if (cudaEventCreate(&e) != cudaSuccess) throw CudaError("cudaEventCreate");
   }
+  // the kernel alone: its full persistent grid, whatever share of the SMs the tuner leaves it inside a step
+  const int cut = pair_cut_;
+  pair_cut_ = 0;
   for (int k = 0; k < launches; ++k) {
     if (flush_bytes > 0) cudaMemsetAsync(d_flush_.p, k & 255, size_t(flush_bytes), stream_);
     if (mixed_) cudaMemsetAsync(d_Fs_.p, 0, d_Fs_.n * sizeof(long long), stream_);
@@ -30,6 +33,7 @@ void Engine::time_pair_kernel(const double* x, const double* cell, int launches,
     pair_forces(false, false);
     cudaEventRecord(ev[size_t(2 * k + 1)], stream_);
   }
+  pair_cut_ = cut;
   if (cudaStreamSynchronize(stream_) != cudaSuccess) throw CudaError("pair timing: stream failed");
   double sum = 0;
   for (int k = 0; k < launches; ++k) {

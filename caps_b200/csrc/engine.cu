@@ -354,6 +354,21 @@ void Engine::setup_options() {
       l14[size_t(a0) * nt_ + b0] = make_double4(eps, s6, sh, 0.0);
     }
   d_tab_.upload(tab, stream_);
+  // geometric mixing (c6_ab = sqrt(c6_aa c6_bb) and the same for c12, as OPLS-style force fields give): the FP32 pair
+  // kernel takes per-type factors instead of the per-pair table (12-6 only)
+  comb_ = !lj96_;
+  std::vector<float2> ljf(size_t(ntab), make_float2(0.f, 0.f));
+  for (int a0 = 0; a0 < nt_ && comb_; ++a0) {
+    const double c6a = tabd[size_t(a0) * ntab + a0].x, c12a = tabd[size_t(a0) * ntab + a0].y;
+    ljf[size_t(a0)] = make_float2(float(std::sqrt(c6a)), float(std::sqrt(c12a)));
+    for (int b0 = 0; b0 < nt_; ++b0) {
+      const double c6b = tabd[size_t(b0) * ntab + b0].x, c12b = tabd[size_t(b0) * ntab + b0].y;
+      const double c6 = tabd[size_t(a0) * ntab + b0].x, c12 = tabd[size_t(a0) * ntab + b0].y;
+      if (std::fabs(c6 - std::sqrt(c6a * c6b)) > 1e-12 * std::max(c6, 1e-300) || std::fabs(c12 - std::sqrt(c12a * c12b)) > 1e-12 * std::max(c12, 1e-300))
+        comb_ = false;
+    }
+  }
+  d_ljf_.upload(ljf, stream_);
   d_tabd_.upload(tabd, stream_);
   d_lj14_.upload(l14, stream_);
   // force-cap radii (field.cpp:557-581): where |F_LJ| reaches the cap, by bisection; beyond it nothing changes
@@ -412,7 +427,7 @@ std::string Engine::capture_state() const {
   put(&epoch, sizeof epoch);
   put(&opt_, sizeof opt_);
   const int flags[] = {mixed_ ? 1 : 0, energies_ ? 1 : 0, list_valid_ ? 1 : 0, green_valid_ ? 1 : 0, frozen_ ? 1 : 0, batch_tuned_ ? 1 : 0,
-                       batch_, pme_lines()[0], pme_lines()[1], pme_lines()[2], nsc_cap_, pk_[0], pk_[1], pk_[2], n_, pair_cut_, pme_cap_};
+                       batch_, pme_lines()[0], pme_lines()[1], pme_lines()[2], nsc_cap_, pk_[0], pk_[1], pk_[2], n_, pair_cut_, pme_cap_, bonded_cap_};
   put(flags, sizeof flags);
   put(cell_h_, sizeof cell_h_);
   put(&dcell_, sizeof dcell_);

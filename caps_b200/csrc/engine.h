@@ -195,6 +195,7 @@ class Engine {
   int batch_ = kBatch;
   int pair_cut_ = 0;   // the pair kernel's persistent grid leaves this many block slots per SM to the other branches
   int pme_cap_ = 0;    // at most this many blocks per PME line-transform launch (0: one per line group)
+  int bonded_cap_ = 0; // at most this many blocks per bonded term kind (0: four per SM)
   bool sums_cleared_ = false;   // the atom-order force sums were cleared by the integrator's kick (the next forces() skips it)
   bool batch_tuned_ = false;
   void tune_batch(const double* d_x);
@@ -224,6 +225,8 @@ class Engine {
   std::vector<std::array<uint32_t, 3>> ha_;   // angles and theta0, for rigid waters
   std::vector<double> hth0_;
   DevBuf<float4> d_tab_;
+  DevBuf<float2> d_ljf_;   // per type (sqrt c6, sqrt c12), the padding type last
+  bool comb_ = false;      // the pair coefficients factor per type (geometric mixing, 12-6)
   DevBuf<double4> d_tabd_, d_lj14_, d_tabcap_, d_cap14_;
   DevBuf<double> d_gtab_;
   int gnodes_ = 0;

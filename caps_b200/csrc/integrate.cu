@@ -1842,9 +1842,9 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
     const double setup = std::chrono::duration<double>(w0 - t_enter).count();
     std::snprintf(b, sizeof b,
                   "%lld steps of %.2f fs in %.3f s (device %.3f s, set-up %.3f s) · %.2f ns/day · %d constraints · %.0f degrees of freedom · %s"
-                  " · tuned: %d entries per work item, pair grid %d block(s) per SM short of full, PME line blocks %d/%d/%d, PME grid cap %d",
+                  " · tuned: %d entries per work item, pair grid %d block(s) per SM short of full, PME line blocks %d/%d/%d, PME grid cap %d, bonded cap %d",
                   (long long)done, o.dt, wall, ms * 1e-3, setup, nsday, S.ncons, S.ndof, mixed_ ? "mixed FP32/fixed-point" : "FP64", batch_,
-                  pair_cut_, pme_lines()[0], pme_lines()[1], pme_lines()[2], pme_cap_);
+                  pair_cut_, pme_lines()[0], pme_lines()[1], pme_lines()[2], pme_cap_, bonded_cap_);
     *report = b;
   }
   R.completed = true;

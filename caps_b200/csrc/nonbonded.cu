@@ -100,31 +100,39 @@ void Engine::tune_batch(const double* d_x) {
   // evaluation wait for it to end unless it leaves room; PME's line transforms, on the other hand, run in fewer waves
   // on the slots left when their grid is capped. Time whole force-only evaluations for each pair (pair grid full or one
   // block per SM fewer; PME grid uncapped, one or two blocks per SM), in alternating rounds, and keep the fastest.
+  // The bonded kernel's blocks, launched at the same time on a side stream, are capped likewise (four per SM, or half
+  // a block per SM per term kind), so that they do not take every slot ahead of the list and pair kernels.
   const int caps[3] = {0, dev_sms_, 2 * dev_sms_};
-  float bestc[2][3];
+  const int bcaps[2] = {0, std::max(1, dev_sms_ / 2)};
+  float bestc[2][3][2];
   for (auto& r : bestc)
-    for (float& v : r) v = 1e30f;
+    for (auto& q : r)
+      for (float& v : q) v = 1e30f;
   for (int round = 0; round < 3; ++round)
     for (int cut = 0; cut < 2; ++cut)
-      for (int ci = 0; ci < (pme_ ? 3 : 1); ++ci) {
-        pair_cut_ = cut;
-        pme_cap_ = caps[ci];
-        for (int rep = 0; rep < 4; ++rep) {
-          if (rep == 1) CK(cudaEventRecord(e0, stream_));
-          forces(d_x, false, false, false);
+      for (int ci = 0; ci < (pme_ ? 3 : 1); ++ci)
+        for (int bi = 0; bi < 2; ++bi) {
+          pair_cut_ = cut;
+          pme_cap_ = caps[ci];
+          bonded_cap_ = bcaps[bi];
+          for (int rep = 0; rep < 4; ++rep) {
+            if (rep == 1) CK(cudaEventRecord(e0, stream_));
+            forces(d_x, false, false, false);
+          }
+          CK(cudaEventRecord(e1, stream_));
+          CK(cudaEventSynchronize(e1));
+          float ms = 0;
+          CK(cudaEventElapsedTime(&ms, e0, e1));
+          bestc[cut][ci][bi] = std::min(bestc[cut][ci][bi], ms);
         }
-        CK(cudaEventRecord(e1, stream_));
-        CK(cudaEventSynchronize(e1));
-        float ms = 0;
-        CK(cudaEventElapsedTime(&ms, e0, e1));
-        bestc[cut][ci] = std::min(bestc[cut][ci], ms);
-      }
-  int bc = 0, bi = 0;
+  int bc = 0, pc = 0, bb = 0;
   for (int cut = 0; cut < 2; ++cut)
     for (int ci = 0; ci < 3; ++ci)
-      if (bestc[cut][ci] < bestc[bc][bi]) bc = cut, bi = ci;
+      for (int bi = 0; bi < 2; ++bi)
+        if (bestc[cut][ci][bi] < bestc[bc][pc][bb]) bc = cut, pc = ci, bb = bi;
   pair_cut_ = bc;
-  pme_cap_ = caps[bi];
+  pme_cap_ = caps[pc];
+  bonded_cap_ = bcaps[bb];
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
 }
@@ -165,6 +173,8 @@ PairArgs Engine::pair_args() {
   A.xq = d_xq_.p;
   A.xqd = d_xqd_.p;
   A.tab = d_tab_.p;
+  A.ljf = d_ljf_.p;
+  A.batch = std::max(1, std::min(geom_.batch, kBatch));
   A.tabd = d_tabd_.p;
   A.tabcap = d_tabcap_.p;
   A.gtab = d_gtab_.p;
@@ -211,22 +221,24 @@ void Engine::pair_forces(bool ener, bool vir) {
   // fetch work items until none are left
   const int ntab = nt_ + 1;
   if (mixed_) {
-    // LJ table, the 4 warps' i atoms, and their staged entries with the entries' j atoms and exclusion masks
-    const size_t smem = sizeof(float4) * (size_t(ntab) * ntab + 4 * 64) + sizeof(int) * 4 * 64 +
-                        4 * kBatch * (sizeof(uint4) + sizeof(float4) + 8 * sizeof(float4) + 8 * sizeof(int) + 8 * sizeof(unsigned long long));
+    // LJ table, the 4 warps' i atoms (three float4 each) and types, and their staged entries with the entries' j atoms
+    // and exclusion masks
+    const size_t smem = sizeof(float4) * (size_t(ntab) * ntab + 4 * 64 * 3) + sizeof(int) * 4 * 64 +
+                        4 * size_t(A.batch) * (sizeof(uint4) + sizeof(float4) + 8 * sizeof(float4) + 8 * sizeof(int) + 8 * sizeof(unsigned long long));
     // the rational fits hold for (kappa r_c)^2 <= 16; past that the library erfc form
     const int c32 = coul == 0 ? 0 : (kappa_ * kappa_ * rc_ * rc_ <= double(kEwUMax) ? coul : coul + 2);
-#define PAIR32L(C, E, V, L)                                                                                          \
+#define PAIR32L(C, E, V, L, M)                                                                                       \
   do {                                                                                                               \
-    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_pair_f32<C, E, V, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
+    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_pair_f32<C, E, V, L, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
     int per_sm = 0;                                                                                                  \
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_f32<C, E, V, L>, 128, smem));                   \
-    launch_k(k_pair_f32<C, E, V, L>, dev_sms_ * std::max(1, per_sm - pair_cut_), 128, smem, stream_, A);                               \
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_f32<C, E, V, L, M>, 128, smem));                \
+    launch_k(k_pair_f32<C, E, V, L, M>, dev_sms_ * std::max(1, per_sm - pair_cut_), 128, smem, stream_, A);          \
   } while (0)
 #define PAIR32(C, E, V)                                                                                              \
   do {                                                                                                               \
-    if (lj96_) PAIR32L(C, E, V, true);                                                                               \
-    else PAIR32L(C, E, V, false);                                                                                    \
+    if (lj96_) PAIR32L(C, E, V, true, false);                                                                        \
+    else if (comb_ && !(E)) PAIR32L(C, E, V, false, !(E));                                                           \
+    else PAIR32L(C, E, V, false, false);                                                                             \
   } while (0)
 #define PAIR32C(C) { if (ener) { if (vir) PAIR32(C, true, true); else PAIR32(C, true, false); } else { if (vir) PAIR32(C, false, true); else PAIR32(C, false, false); } }
     switch (c32) {

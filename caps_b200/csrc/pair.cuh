@@ -98,6 +98,8 @@ struct PairArgs {
   const float4* xq;      // FP32 path
   const double4* xqd;    // FP64 path
   const float4* tab;     // FP32: per type pair (c6, c12, energy shift, 0)
+  const float2* ljf;     // FP32 with geometric mixing: per type (sqrt c6, sqrt c12)
+  int batch;             // entries per work item of the list (<= kBatch): the FP32 kernel's staging per warp
   const double4* tabd;   // FP64: per type pair (c6, c12, energy shift, 0)
   const double4* tabcap; // FP64 with a force cap: per type pair (r_cap^2, E at r_cap, |F| at r_cap, 0)
   const double* gtab;    // FP64 Ewald table: 2 per node (G, h dG/ds)
@@ -175,50 +177,77 @@ __device__ __forceinline__ void reduce_i(int jq, const T fx[8], const T fy[8], c
 }
 
 // --- FP32 path ---------------------------------------------------------------------------------------------------
+// Packed FP32 arithmetic (sm_100 f32x2): a lane's two j atoms of an entry (quarters jq and jq + 4) are the two lanes of
+// every add, multiply and multiply-add, so one instruction evaluates both of its pairs with an i atom.
+__device__ __forceinline__ float2 p_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 p_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 p_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 p_dup(float v) { return make_float2(v, v); }
+
 // COUL: 0 none; 1 Ewald real space (PME) and 2 damped shifted force through the rational fits of ewald_fit.cuh
-// (kappa r_c <= 4); 3 and 4 the same through erfcf and expf (any kappa).
-template <int COUL, bool ENER, bool VIR, bool LJ96 = false>
-static __global__ void __launch_bounds__(128, 5) k_pair_f32(PairArgs A) {
+// (kappa r_c <= 4); 3 and 4 the same through erfcf and expf (any kappa). COMB: the LJ coefficients of a type pair are
+// products of per-type factors (geometric mixing: c6_ab = sqrt(c6_aa c6_bb), the same for c12), taken from a
+// per-type table instead of the per-pair one. Force-only evaluations only: the products of rounded factors carry a
+// bias of a few 1e-7 per type pair, which the cancelling sums of LJ energies would magnify, so energy steps take the
+// per-pair table.
+template <int COUL, bool ENER, bool VIR, bool LJ96 = false, bool COMB = false>
+static __global__ void __launch_bounds__(128, (ENER || VIR) ? 4 : 5) k_pair_f32(PairArgs A) {
+  static_assert(!(COMB && ENER), "energy evaluations use the per-pair table");
   extern __shared__ float4 smem_f4[];
-  float4* tab = smem_f4;                                  // ntab * ntab
-  float4* s_xi = smem_f4 + A.ntab * A.ntab;               // 4 warps x 64
-  int* s_ti = reinterpret_cast<int*>(s_xi + 4 * 64);      // 4 warps x 64
+  float4* tab = smem_f4;                                  // ntab * ntab (per-pair table; COMB: ntab float2 factors)
+  float2* ljf = reinterpret_cast<float2*>(smem_f4);
+  // per warp and i atom: (-x, -x, -y, -y), (-z, -z, q, q) and, COMB, (-6 f6, -6 f6, 12 f12, 12 f12); else the type
+  float4* s_xi = smem_f4 + A.ntab * A.ntab;               // 4 warps x 64 x 3
+  int* s_ti = reinterpret_cast<int*>(s_xi + 4 * 64 * 3);  // 4 warps x 64
   // a work item's entries, their j atoms and their exclusion masks, staged per warp in one batch of independent loads
-  uint4* s_en_all = reinterpret_cast<uint4*>(s_ti + 4 * 64);   // 4 warps x 32 entries
-  float4* s_sh_all = reinterpret_cast<float4*>(s_en_all + 4 * kBatch);
-  float4* s_xj_all = s_sh_all + 4 * kBatch;                     // 4 warps x 32 entries x 8 j atoms
-  int* s_tj_all = reinterpret_cast<int*>(s_xj_all + 4 * kBatch * 8);
-  unsigned long long* s_mk_all = reinterpret_cast<unsigned long long*>(s_tj_all + 4 * kBatch * 8);
-  for (int t = threadIdx.x; t < A.ntab * A.ntab; t += blockDim.x) tab[t] = A.tab[t];
+  // (sized for the list's entries per work item, A.batch <= kBatch)
+  const int nb = A.batch;
+  uint4* s_en_all = reinterpret_cast<uint4*>(s_ti + 4 * 64);   // 4 warps x nb entries
+  float4* s_sh_all = reinterpret_cast<float4*>(s_en_all + 4 * nb);
+  float4* s_xj_all = s_sh_all + 4 * nb;                         // 4 warps x nb entries x 8 j atoms
+  int* s_tj_all = reinterpret_cast<int*>(s_xj_all + 4 * nb * 8);
+  unsigned long long* s_mk_all = reinterpret_cast<unsigned long long*>(s_tj_all + 4 * nb * 8);
+  if (COMB) {
+    for (int t = threadIdx.x; t < A.ntab; t += blockDim.x) ljf[t] = A.ljf[t];
+  } else {
+    for (int t = threadIdx.x; t < A.ntab * A.ntab; t += blockDim.x) tab[t] = A.tab[t];
+  }
   __syncthreads();
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i8 = lane & 7, jq = lane >> 3;
-  float4* xi_s = s_xi + 64 * wib;
+  float4* xi_s = s_xi + 3 * 64 * wib;
   int* ti_s = s_ti + 64 * wib;
-  // a list build that ran out of room leaves stale work items: skip the pass, the host reports the error
   if (blockIdx.x == 0 && threadIdx.x == 0) {   // the step's list work is done: lower the rebuild and prune flags
     int* c = const_cast<int*>(A.counters);
     c[kCntRebuild] = 0;
     c[kCntPrune] = 0;
   }
+  // a list build that ran out of room leaves stale work items: skip the pass, the host reports the error
   if (A.counters[kCntErr] & (kErrListOverflow | kErrMaskOverflow | kErrScOverflow | kErrColumnTooBig | kErrExclOverflow)) return;
   const int nwork = min(A.counters[kCntWork], A.work_cap);
   const int pad = A.ntab - 1;
   const float rc2 = float(A.rc2), beta = float(A.beta), kc = float(A.kc), kcoul = float(A.kcoul);
-  const float ku = float(A.beta * A.beta / kEwUMax), kap3 = float(A.beta * A.beta * A.beta);
+  const float2 ku = p_dup(float(A.beta * A.beta / kEwUMax)), nkap3 = p_dup(-float(A.beta * A.beta * A.beta));
   const float e0 = float(A.dsf_e0), f0 = float(A.dsf_f0), rcf = float(A.rc);
-  // energy and virial: each work item's sums rounded to fixed point on their own, so that the totals do not depend on
-  // which warp took which item
+  // energy and virial: every pair's terms rounded to fixed point on their own (2^24 per kcal/mol), so that the totals do
+  // not depend on the list's grouping of pairs into entries and work items
   long long acc_v = 0, acc_c = 0, acc_w[6] = {0, 0, 0, 0, 0, 0};
   double acc_np = 0, acc_nl = 0;
+  constexpr float kq = 16777216.f;
   for (int w = next_work_item(A.counters, lane); w < nwork; w = next_work_item(A.counters, lane)) {
     const int4 wk = A.work[w];
     const int sc = wk.x;
     for (int t = lane; t < 64; t += 32) {
-      float4 v = A.xq[64 * sc + t];
-      v.w *= kcoul;
-      xi_s[t] = v;
-      ti_s[t] = A.tslot[64 * sc + t];
+      const float4 v = A.xq[64 * sc + t];
+      const int ty = A.tslot[64 * sc + t];
+      const float q = v.w * kcoul;
+      xi_s[3 * t] = make_float4(-v.x, -v.x, -v.y, -v.y);
+      xi_s[3 * t + 1] = make_float4(-v.z, -v.z, q, q);
+      if (COMB) {
+        const float2 g = ljf[ty];
+        xi_s[3 * t + 2] = make_float4(-6.f * g.x, -6.f * g.x, 12.f * g.y, 12.f * g.y);
+      }
+      ti_s[t] = ty;
     }
     __syncwarp();
     unsigned ireal = 0;
@@ -227,13 +256,13 @@ static __global__ void __launch_bounds__(128, 5) k_pair_f32(PairArgs A) {
     float fix[8], fiy[8], fiz[8];
 #pragma unroll
     for (int c = 0; c < 8; ++c) fix[c] = fiy[c] = fiz[c] = 0.f;
-    float ev = 0.f, ec = 0.f, vw[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, npair = 0.f, nlist = 0.f;
-    uint4* s_en = s_en_all + kBatch * wib;
-    float4* s_sh = s_sh_all + kBatch * wib;
-    float4* s_xj = s_xj_all + kBatch * 8 * wib;
-    int* s_tj = s_tj_all + kBatch * 8 * wib;
-    unsigned long long* s_mk = s_mk_all + kBatch * 8 * wib;
-    const int ne = min(wk.z, kBatch);
+    float npair = 0.f, nlist = 0.f;
+    uint4* s_en = s_en_all + nb * wib;
+    float4* s_sh = s_sh_all + nb * wib;
+    float4* s_xj = s_xj_all + nb * 8 * wib;
+    int* s_tj = s_tj_all + nb * 8 * wib;
+    unsigned long long* s_mk = s_mk_all + nb * 8 * wib;
+    const int ne = min(wk.z, nb);
     if (lane < ne) {
       s_en[lane] = A.ent[wk.y + lane];
       s_sh[lane] = A.ent_shift[wk.y + lane];
@@ -253,97 +282,107 @@ static __global__ void __launch_bounds__(128, 5) k_pair_f32(PairArgs A) {
     __syncwarp();
     for (int el = 0; el < ne; ++el) {
       const uint4 en = s_en[el];
-      const float4 sh = s_sh[el];
-      const int cj = int(en.x);
       const unsigned hmask = en.w & 0xffffu;
       if (!hmask) continue;
+      const float4 sh = s_sh[el];
+      const int cj = int(en.x);
       const unsigned imask = (hmask | (hmask >> 8)) & 255u;
       const int j0 = 8 * cj + jq, j1 = j0 + 4;
       const float4 a0 = s_xj[8 * el + jq], a1 = s_xj[8 * el + jq + 4];
       const int t0 = s_tj[8 * el + jq], t1 = s_tj[8 * el + jq + 4];
-      const float xj0 = a0.x + sh.x, yj0 = a0.y + sh.y, zj0 = a0.z + sh.z;
-      const float xj1 = a1.x + sh.x, yj1 = a1.y + sh.y, zj1 = a1.z + sh.z;
-      float f0x = 0.f, f0y = 0.f, f0z = 0.f, f1x = 0.f, f1y = 0.f, f1z = 0.f;
+      const float2 xj = make_float2(a0.x + sh.x, a1.x + sh.x), yj = make_float2(a0.y + sh.y, a1.y + sh.y),
+                   zj = make_float2(a0.z + sh.z, a1.z + sh.z), qj = make_float2(a0.w, a1.w);
+      float2 g6j = p_dup(0.f), g12j = p_dup(0.f);
+      if (COMB) {
+        const float2 g0 = ljf[t0], g1 = ljf[t1];
+        g6j = make_float2(g0.x, g1.x);
+        g12j = make_float2(g0.y, g1.y);
+      }
+      float2 fjx = p_dup(0.f), fjy = p_dup(0.f), fjz = p_dup(0.f);
 #pragma unroll
       for (int c = 0; c < 8; ++c) {
         if (!((imask >> c) & 1u)) continue;
         const unsigned long long mm = s_mk[8 * el + c];
-        const float4 xi = xi_s[8 * c + i8];
-        const int ti = ti_s[8 * c + i8];
-        // this lane's two pairs of the i cluster (j atoms jq and jq + 4): bits 0 and 4, real i atom and not excluded
+        const float4 pa = xi_s[3 * (8 * c + i8)], pb = xi_s[3 * (8 * c + i8) + 1];
+        // this lane's two pairs of the i cluster (j atoms jq and jq + 4): bits 0 and 4 of the exclusion mask, a real i
+        // atom, and the j half within the prune radius
         const unsigned lb = ((ireal >> c) & 1u) ? unsigned(mm >> (8 * i8 + jq)) & 0x11u : 0u;
-#pragma unroll
-        for (int jj = 0; jj < 2; ++jj) {
-          if (!((hmask >> (c + 8 * jj)) & 1u)) continue;   // this half of the j cluster is beyond the prune radius
-          const float xj = jj ? xj1 : xj0, yj = jj ? yj1 : yj0, zj = jj ? zj1 : zj0;
-          const float qj = jj ? a1.w : a0.w;
-          const int tj = jj ? t1 : t0;
-          const bool listed = (lb >> (4 * jj)) & 1u;
-          const float dx = xj - xi.x, dy = yj - xi.y, dz = zj - xi.z;
-          const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-          const bool ok = listed && (r2 < rc2);
+        const bool l0 = (lb & 1u) && ((hmask >> c) & 1u), l1 = (lb & 0x10u) && ((hmask >> (c + 8)) & 1u);
+        const float2 dx = p_add(xj, make_float2(pa.x, pa.y)), dy = p_add(yj, make_float2(pa.z, pa.w)), dz = p_add(zj, make_float2(pb.x, pb.y));
+        const float2 r2 = p_fma(dx, dx, p_fma(dy, dy, p_mul(dz, dz)));
+        const bool ok0 = l0 && (r2.x < rc2), ok1 = l1 && (r2.y < rc2);
+        if (ENER) {
+          npair += float(ok0) + float(ok1);
+          nlist += float(l0) + float(l1);
+        }
+        const float2 r2s = make_float2(ok0 ? r2.x : 1.f, ok1 ? r2.y : 1.f);
+        const float2 rinv = make_float2(rsqrtf(r2s.x), rsqrtf(r2s.y));
+        const float2 r2i = p_mul(rinv, rinv);
+        const float2 r6i = p_mul(p_mul(r2i, r2i), r2i);
+        float2 fr, elj;
+        if (COMB) {
+          const float4 pl = xi_s[3 * (8 * c + i8) + 2];
+          const float2 nC6 = p_mul(make_float2(pl.x, pl.y), g6j), C12 = p_mul(make_float2(pl.z, pl.w), g12j);
+          fr = p_mul(p_mul(r6i, p_fma(C12, r6i, nC6)), r2i);   // (12 c12 r^-12 - 6 c6 r^-6) / r^2
+        } else {
+          const int ti = ti_s[8 * c + i8];
+          const float4 cc0 = tab[ti * A.ntab + t0], cc1 = tab[ti * A.ntab + t1];
+          const float2 c6 = make_float2(cc0.x, cc1.x), c12 = make_float2(cc0.y, cc1.y);
+          // 12-6: a = c12 r^-6; 9-6: a = c9 r^-3 (the table's second slot holds c12 or c9): E = r^-6 (a - c6) - shift
+          const float2 a12 = p_mul(c12, LJ96 ? p_mul(r2i, rinv) : r6i);
+          fr = p_mul(p_mul(r6i, p_fma(p_dup(LJ96 ? 9.f : 12.f), a12, p_mul(p_dup(-6.f), c6))), r2i);
+          if (ENER) elj = p_fma(r6i, p_add(a12, p_mul(p_dup(-1.f), c6)), make_float2(-cc0.z, -cc1.z));
+        }
+        if (ENER) acc_v += (ok0 ? __float2ll_rn(elj.x * kq) : 0ll) + (ok1 ? __float2ll_rn(elj.y * kq) : 0ll);
+        if (COUL == 1 || COUL == 2) {
+          // E = qq (1/r - kappa g(u)), F = qq (1/r^3 - kappa^3 h(u)), u = (kappa r)^2: FMAs and one division per pair
+          const float2 qq = p_mul(make_float2(pb.z, pb.w), qj);
+          const float2 t = p_mul(r2s, ku);
+          float2 fc = p_mul(qq, p_fma(nkap3, ew_h2(t), p_mul(rinv, r2i)));
+          if (COUL == 2) fc = p_fma(p_mul(qq, p_dup(-f0)), rinv, fc);
+          fr = p_add(fr, fc);
           if (ENER) {
-            npair += ok ? 1.f : 0.f;
-            nlist += listed ? 1.f : 0.f;
+            float2 ecp = p_mul(qq, p_fma(p_dup(-beta), ew_g2(t), rinv));
+            if (COUL == 2) ecp = p_fma(qq, p_fma(p_dup(f0), p_add(p_mul(r2s, rinv), p_dup(-rcf)), p_dup(-e0)), ecp);
+            acc_c += (ok0 ? __float2ll_rn(ecp.x * kq) : 0ll) + (ok1 ? __float2ll_rn(ecp.y * kq) : 0ll);
           }
-          const float r2s = ok ? r2 : 1.f;
-          const float rinv = rsqrtf(r2s);
-          const float r2i = rinv * rinv;
-          const float r6i = r2i * r2i * r2i;
-          const float4 cc = tab[ti * A.ntab + tj];
-          // 12-6: a = c12 r^-6; 9-6: a = c9 r^-3 (cc.y holds c12 or c9): E = r^-6 (a - c6) - shift
-          const float a12 = cc.y * (LJ96 ? r2i * rinv : r6i);
-          float fr = r6i * fmaf(LJ96 ? 9.f : 12.f, a12, -6.f * cc.x) * r2i;
-          if (ENER) ev += ok ? fmaf(r6i, a12 - cc.x, -cc.z) : 0.f;
-          if (COUL == 1 || COUL == 2) {
-            // E = qq (1/r - kappa g(u)), F = qq (1/r^3 - kappa^3 h(u)), u = (kappa r)^2: FMAs and one division
-            const float qq = xi.w * qj;
-            const float t = r2s * ku;
-            float fc = qq * fmaf(-kap3, ew_h(t), rinv * r2i);
-            if (COUL == 2) fc -= qq * f0 * rinv;
-            fr += fc;
-            if (ENER) {
-              float ecp = qq * fmaf(-beta, ew_g(t), rinv);
-              if (COUL == 2) ecp += qq * (f0 * (r2s * rinv - rcf) - e0);
-              ec += ok ? ecp : 0.f;
-            }
-          }
-          if (COUL == 3 || COUL == 4) {
-            const float qq = xi.w * qj;
-            const float r = r2s * rinv;
-            const float br = beta * r;
+        }
+        if (COUL == 3 || COUL == 4) {
+          const float2 qq = p_mul(make_float2(pb.z, pb.w), qj);
+          const float2 r = p_mul(r2s, rinv);
+          float fcs[2], ecs[2];
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const float rh = h ? r.y : r.x, ih = h ? rinv.y : rinv.x, qh = h ? qq.y : qq.x;
+            const float br = beta * rh;
             const float erfcv = erfcf(br);
             const float ex = __expf(-br * br);
-            float fc = qq * fmaf(erfcv, rinv, kc * ex) * r2i;
-            if (COUL == 4) fc -= qq * f0 * rinv;
-            fr += fc;
-            if (ENER) {
-              float ecp = qq * erfcv * rinv;
-              if (COUL == 4) ecp += qq * (f0 * (r - rcf) - e0);
-              ec += ok ? ecp : 0.f;
-            }
+            fcs[h] = qh * fmaf(erfcv, ih, kc * ex) * (ih * ih);
+            if (COUL == 4) fcs[h] -= qh * f0 * ih;
+            ecs[h] = qh * erfcv * ih;
+            if (COUL == 4) ecs[h] += qh * (f0 * (rh - rcf) - e0);
           }
-          fr = ok ? fr : 0.f;
-          const float fx = fr * dx, fy = fr * dy, fz = fr * dz;
-          if (jj) f1x += fx, f1y += fy, f1z += fz;
-          else f0x += fx, f0y += fy, f0z += fz;
-          fix[c] -= fx;
-          fiy[c] -= fy;
-          fiz[c] -= fz;
-          if (VIR) {
-            vw[0] = fmaf(fx, dx, vw[0]);
-            vw[1] = fmaf(fy, dy, vw[1]);
-            vw[2] = fmaf(fz, dz, vw[2]);
-            vw[3] = fmaf(fx, dy, vw[3]);
-            vw[4] = fmaf(fx, dz, vw[4]);
-            vw[5] = fmaf(fy, dz, vw[5]);
-          }
+          fr = p_add(fr, make_float2(fcs[0], fcs[1]));
+          if (ENER) acc_c += (ok0 ? __float2ll_rn(ecs[0] * kq) : 0ll) + (ok1 ? __float2ll_rn(ecs[1] * kq) : 0ll);
+        }
+        fr = make_float2(ok0 ? fr.x : 0.f, ok1 ? fr.y : 0.f);
+        const float2 fx = p_mul(fr, dx), fy = p_mul(fr, dy), fz = p_mul(fr, dz);
+        fjx = p_add(fjx, fx);
+        fjy = p_add(fjy, fy);
+        fjz = p_add(fjz, fz);
+        fix[c] -= fx.x + fx.y;
+        fiy[c] -= fy.x + fy.y;
+        fiz[c] -= fz.x + fz.y;
+        if (VIR) {   // fr is 0 for the pairs left out
+          const float2 w6[6] = {p_mul(fx, dx), p_mul(fy, dy), p_mul(fz, dz), p_mul(fx, dy), p_mul(fx, dz), p_mul(fy, dz)};
+#pragma unroll
+          for (int k = 0; k < 6; ++k) acc_w[k] += __float2ll_rn(w6[k].x * kq) + __float2ll_rn(w6[k].y * kq);
         }
       }
       // j forces: summed over the 8 lanes holding the same j atoms, then one fixed-point add per component
       {
         float kx, ky, kz;
-        reduce_j(i8, f0x, f0y, f0z, f1x, f1y, f1z, kx, ky, kz);
+        reduce_j(i8, fjx.x, fjy.x, fjz.x, fjx.y, fjy.y, fjz.y, kx, ky, kz);
         const int comp = i8 & 3;
         if (comp < 3) {
           const float v = comp == 0 ? kx : comp == 1 ? ky : kz;
@@ -367,15 +406,17 @@ static __global__ void __launch_bounds__(128, 5) k_pair_f32(PairArgs A) {
       }
     }
     if (ENER) {
-      acc_v += to_fix(double(warp_sum(ev)), kFixE);
-      acc_c += to_fix(double(warp_sum(ec)), kFixE);
       acc_np += double(warp_sum(npair));   // whole numbers: exact in any order
       acc_nl += double(warp_sum(nlist));
     }
-    if (VIR)
-      for (int k = 0; k < 6; ++k) acc_w[k] += to_fix(double(warp_sum(vw[k])), kFixE);
     __syncwarp();
   }
+  if (ENER) {
+    acc_v = warp_sum(acc_v);
+    acc_c = warp_sum(acc_c);
+  }
+  if (VIR)
+    for (int k = 0; k < 6; ++k) acc_w[k] = warp_sum(acc_w[k]);
   if (lane == 0) {
     if (ENER) {
       atomic_add_fix(A.en.fix + kEVdw, acc_v);

@@ -73,6 +73,12 @@ def main():
             e = f"fmaf({e}, t, {float(c):.9e}f)"
         return e
 
+    def horner2(v) -> str:   # the same on both lanes of an f32x2 pair (sm_100 packed FP32 arithmetic)
+        e = f"make_float2({float(v[-1]):.9e}f, {float(v[-1]):.9e}f)"
+        for c in v[-2::-1]:
+            e = f"__ffma2_rn({e}, t, make_float2({float(c):.9e}f, {float(c):.9e}f))"
+        return e
+
     text = f"""// Generated by caps_b200/fits/make_ewald_fit.py: rational fits on u = (kappa r)^2 in [0, {U:g}], t = u / {U:g}.
 //   g(u) = erf(sqrt u) / sqrt u                       fit max relative error {ge:.1e}, float evaluation {f32_error(g, gp, gq):.1e}
 //   h(u) = (g(u) - 2 exp(-u) / sqrt(pi)) / u          fit max relative error {he:.1e}, float evaluation {f32_error(h, hp, hq):.1e}
@@ -81,6 +87,17 @@ namespace capsb {{
 constexpr float kEwUMax = {U:.1f}f;
 __device__ __forceinline__ float ew_h(float t) {{ return __fdividef({horner(hp)}, {horner(hq)}); }}
 __device__ __forceinline__ float ew_g(float t) {{ return __fdividef({horner(gp)}, {horner(gq)}); }}
+// both fits on a pair of arguments at once (packed FP32 multiply-adds; the two quotients are taken separately)
+__device__ __forceinline__ float2 ew_h2(float2 t) {{
+  const float2 n = {horner2(hp)};
+  const float2 d = {horner2(hq)};
+  return make_float2(__fdividef(n.x, d.x), __fdividef(n.y, d.y));
+}}
+__device__ __forceinline__ float2 ew_g2(float2 t) {{
+  const float2 n = {horner2(gp)};
+  const float2 d = {horner2(gq)};
+  return make_float2(__fdividef(n.x, d.x), __fdividef(n.y, d.y));
+}}
 }}  // namespace capsb
 """
     OUT.write_text(text)

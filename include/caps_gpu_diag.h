@@ -23,7 +23,8 @@ int32_t caps_gpu_diag_step_kernels(const caps_gpu_engine* e);
  * the kinetic-energy kernel of each thermo row; a barostat step (run outside a graph) counts as one thermo step. */
 int64_t caps_gpu_diag_kernels_run(const caps_gpu_engine* e);
 /* Times the non-bonded pair kernel alone: one force evaluation at x (host, 3N) builds the list, then `launches`
- * launches of the pair kernel (forces only), each bracketed by CUDA events, an L2 flush of flush_bytes before each.
+ * launches of the pair kernel (forces only, its full persistent grid), each bracketed by CUDA events, an L2 flush of
+ * flush_bytes before each.
  * avg_ms: mean launch time; pairs_in: atom pairs inside the cut-off per launch; pairs_listed: atom pairs the kernel
  * evaluates (list pairs, masked lanes excluded); entries: cluster-pair entries (FP32 path only; 0 on FP64). */
 int32_t caps_gpu_diag_pair_timing(caps_gpu_engine* e, const double* x, const double* cell, int32_t launches, int64_t flush_bytes, double* avg_ms,
