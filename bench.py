@@ -334,6 +334,53 @@ def run_replicas(args) -> dict:
             "timing": "device time over the step loop (CUDA events), L2 not flushed", "data": "synthetic"}
 
 
+def step_timeline(args) -> dict:
+    """Where a mixed MD step's time goes, kernel by kernel, with the concurrency of its graph: the kernel records of
+    args.profile_timeline steps (after args.warmup), each kernel's start taken from the step's first kernel (the
+    integrator's head). Measurement only: torch.profiler reads the CUDA profiling interface's kernel records, which
+    include the kernels of replayed CUDA graphs; no L2 flush between the steps."""
+    import bisect
+    import re
+    import statistics
+    import tempfile
+
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+
+    from caps_b200 import Evaluator
+    torch.zeros(1, device="cuda")
+    ff, x, v, cell = workload()
+    o = options("mixed", max(args.warmup, 50), 7)
+    ev = Evaluator(ff, o.energy)
+    if args.tuning:
+        ev.pin_tuning([int(t) for t in args.tuning.split(",")])
+    out = ev.run(x, cell, o, v=v)
+    ev.run(out["x"], cell, options("mixed", 50, 7), v=out["v"])
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        ev.run(out["x"], cell, options("mixed", args.profile_timeline, 7), v=out["v"])
+        torch.cuda.synchronize()
+    tuning = ev.tuning()
+    ev.close()
+    with tempfile.NamedTemporaryFile(suffix=".json") as tf:
+        prof.export_chrome_trace(tf.name)
+        trace = json.load(open(tf.name))
+    ks = sorted((e for e in trace["traceEvents"] if e.get("cat") == "kernel"), key=lambda e: e["ts"])
+    short = lambda n: re.sub(r"capsb::(\(anonymous namespace\)::)?", "", re.sub(r"^void ", "", n)).split("(")[0]
+    starts = [e["ts"] for e in ks if "k_nhc_begin" in e["name"]]
+    rows: dict = {}
+    for e in ks:
+        i = bisect.bisect_right(starts, e["ts"]) - 1
+        if 0 <= i < len(starts) - 1:
+            r = rows.setdefault(short(e["name"]), {"start": [], "dur": []})
+            r["start"].append(e["ts"] - starts[i])
+            r["dur"].append(e["dur"])
+    period = [b - a for a, b in zip(starts, starts[1:])]
+    kern = sorted(({"kernel": k, "start_us": statistics.median(r["start"]), "us": statistics.median(r["dur"]), "count": len(r["dur"])}
+                   for k, r in rows.items()), key=lambda d: d["start_us"])
+    return {"timeline_steps": len(period), "step_period_us": statistics.median(period) if period else None,
+            "tuning": ",".join(map(str, tuning)), "kernels": kern}
+
+
 def run_reference(args, rank: int) -> dict:
     """The reference's own CPU implementation (oracle/_ref: the reference core built from its sources) on this
     workload: run_dynamics in its fastest form (EnergyOptions::mixed = true), all host threads."""
@@ -384,6 +431,13 @@ def main():
                     help="only time the force evaluation's branches alone and together, and the MD step, in both precisions")
     ap.add_argument("--profile-md", type=int, default=0, metavar="STEPS",
                     help="only run the mixed MD: --warmup steps, then STEPS steps (the command for ncu launch lists)")
+    ap.add_argument("--profile-timeline", type=int, default=0, metavar="STEPS",
+                    help="only run the mixed MD and print the concurrent kernel timeline of STEPS steps after --warmup steps (kernel "
+                         "records of the CUDA profiling interface through torch.profiler): per kernel its median start within the "
+                         "step, median duration and count")
+    ap.add_argument("--tuning", default=None, metavar="V1,...,V7",
+                    help="with --profile-md or --profile-timeline: pin these launch shapes (as a plain run prints them) instead of "
+                         "tuning, so that a run under a profiler, which misleads the tuners, uses the shapes of a plain run")
     args = ap.parse_args()
     rank, world, local = int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
     if args.warmup < 3:
@@ -419,10 +473,17 @@ def main():
         ff, x, v, cell = workload()
         o = options("mixed", args.warmup, 7)
         ev = Evaluator(ff, o.energy)
+        if args.tuning:
+            ev.pin_tuning([int(t) for t in args.tuning.split(",")])
         out = ev.run(x, cell, o, v=v)
         out = ev.run(out["x"], cell, options("mixed", args.profile_md, 7), v=out["v"])
-        print(json.dumps({"profile_md": args.profile_md, "report": out["report"], "kernels_run": ev.kernels_run()}), flush=True)
+        print(json.dumps({"profile_md": args.profile_md, "report": out["report"], "kernels_run": ev.kernels_run(),
+                          "tuning": ",".join(map(str, ev.tuning()))}), flush=True)
         ev.close()
+        return
+
+    if args.profile_timeline:
+        print(json.dumps(step_timeline(args)), flush=True)
         return
 
     if args.config:

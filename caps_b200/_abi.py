@@ -61,6 +61,8 @@ class MdOpts(C.Structure):
         ("frame_every", C.c_int32), ("step_offset", C.c_int64), ("respa", C.c_int32),
         ("is_hydrogen", P), ("is_oxygen", P), ("respa_split", C.c_int32),
         ("checkpoint_every", C.c_int64), ("checkpoint", C.c_void_p), ("checkpoint_user", C.c_void_p),
+        ("hmr", C.c_double), ("anisotropic", C.c_int32), ("couple_axes", C.c_int32), ("axis_pressure_set", C.c_int32),
+        ("axis_pressure", C.c_double * 3),
     ]
 
 
@@ -88,7 +90,7 @@ FRAME_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_i
 CHECKPOINT_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int64, C.c_void_p)
 
 DIAG_EXPORTS = ["caps_gpu_diag_set_timing", "caps_gpu_diag_last_step_ms", "caps_gpu_diag_pair_timing", "caps_gpu_diag_step_kernels",
-                "caps_gpu_diag_kernels_run", "caps_gpu_diag_phase_timing"]
+                "caps_gpu_diag_kernels_run", "caps_gpu_diag_phase_timing", "caps_gpu_diag_get_tuning", "caps_gpu_diag_set_tuning"]
 
 EXPORTS = [
     "caps_gpu_abi_version", "caps_gpu_device_count", "caps_gpu_create", "caps_gpu_set_options", "caps_gpu_energies",
@@ -154,6 +156,8 @@ def load(path: Path | None = None) -> C.CDLL:
     lib.caps_gpu_diag_pair_timing.argtypes = [C.c_void_p, P, P, C.c_int32, C.c_int64, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                               C.POINTER(C.c_double), C.POINTER(C.c_double)]
     lib.caps_gpu_diag_phase_timing.argtypes = [C.c_void_p, P, P, C.c_int32, C.c_int64, P]
+    lib.caps_gpu_diag_get_tuning.argtypes = [C.c_void_p, P]
+    lib.caps_gpu_diag_set_tuning.argtypes = [C.c_void_p, P]
     if path is None:
         _lib = lib
     return lib

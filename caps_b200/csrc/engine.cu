@@ -893,6 +893,17 @@ int32_t caps_gpu_diag_set_timing(caps_gpu_engine* e, int64_t flush_bytes) {
   return CAPS_GPU_OK;
 }
 
+int32_t caps_gpu_diag_get_tuning(const caps_gpu_engine* e, int32_t* v) {
+  if (!e || !v) return CAPS_GPU_EINVAL;
+  e->e->tuning(v);
+  return CAPS_GPU_OK;
+}
+
+int32_t caps_gpu_diag_set_tuning(caps_gpu_engine* e, const int32_t* v) {
+  if (!e || !v) return CAPS_GPU_EINVAL;
+  return guard(e, [&] { e->e->pin_tuning(v); });
+}
+
 double caps_gpu_diag_last_step_ms(const caps_gpu_engine* e) { return e ? e->e->last_step_ms_device() : 0.0; }
 
 int32_t caps_gpu_diag_step_kernels(const caps_gpu_engine* e) { return e ? e->e->graph_kernels() : 0; }

@@ -155,6 +155,9 @@ class Engine {
   void time_phases(const double* x, const double* cell, int launches, int64_t flush_bytes, double* ms);
   double last_step_ms_device() const { return last_step_ms_; }
   int graph_kernels() const { return graph_kernels_; }
+  // the tuned launch shapes: j-tile depth, pair-grid cut, PME grid cap, bonded cap, PME line blocks x, y, z
+  void tuning(int32_t v[7]) const;
+  void pin_tuning(const int32_t v[7]);   // these shapes from now on, no tuning (profiling runs)
   long long kernels_run() const { return kernels_run_; }
   std::string err;
   // Host state that shapes a captured step graph besides the run's own options: the buffer epoch, the options, the
@@ -196,6 +199,8 @@ class Engine {
   int pair_cut_ = 0;   // the pair kernel's persistent grid leaves this many block slots per SM to the other branches
   int pme_cap_ = 0;    // at most this many blocks per PME line-transform launch (0: one per line group)
   int bonded_cap_ = 0; // at most this many blocks per bonded term kind (0: four per SM)
+  bool tuning_pinned_ = false;
+  int pinned_lines_[3] = {1, 1, 1};
   bool sums_cleared_ = false;   // the atom-order force sums were cleared by the integrator's kick (the next forces() skips it)
   bool batch_tuned_ = false;
   void tune_batch(const double* d_x);

@@ -861,6 +861,12 @@ struct Stepper {
   std::vector<double> hv;
   DevBuf<double> xs, vs;
   bool masses_ready = false;
+  // the run's masses: the force field's, or with hydrogen mass repartitioning (what they were made with: hmr, flags)
+  std::vector<double> hm;
+  double hm_hmr = -1;
+  std::vector<int8_t> hm_h;
+  long long hmr_moved = 0;
+  bool hmr_kept = false;
   bool cons_built = false, cons_from_positions = false;
   int cons_flag = -1;
   std::vector<int8_t> cons_h, cons_o;
@@ -1361,8 +1367,11 @@ void Engine::validate_md(const caps_gpu_md_opts& o) const {
   if (o.respa > 1 && o.constraints) throw ModelError(CAPS_GPU_EINVAL, "r-RESPA and bond constraints are alternatives: choose one");
   if (o.respa_split != 0 && o.respa_split != 1) throw ModelError(CAPS_GPU_EINVAL, "unknown r-RESPA split");
   if (o.thermostat < 0 || o.thermostat > 3) throw ModelError(CAPS_GPU_EINVAL, "unknown thermostat");
-  if (o.barostat != 0 && o.barostat != 1) throw ModelError(CAPS_GPU_EINVAL, "the device path takes stochastic cell rescaling or no barostat");
+  if (o.barostat < 0 || o.barostat > 2)
+    throw ModelError(CAPS_GPU_EINVAL, "the device path takes stochastic cell rescaling, the Berendsen barostat or no barostat");
   if (o.barostat == 1 && o.thermostat == 0) throw ModelError(CAPS_GPU_EINVAL, "stochastic cell rescaling needs a thermostat");
+  if (o.anisotropic && o.barostat == 1) throw ModelError(CAPS_GPU_EINVAL, "per-axis pressure coupling is available with the Berendsen barostat");
+  if (o.hmr < 0 || !std::isfinite(o.hmr)) throw ModelError(CAPS_GPU_EINVAL, "the repartitioned hydrogen mass must be 0 (off) or positive");
 }
 
 // A stop asked for from outside (caps_gpu_request_stop): read once per step by the run loops.
@@ -1467,7 +1476,7 @@ struct MdRun {
   double host_ke(const std::vector<double>& vv) const {
     double k = 0;
     for (int i = 0; i < E.n_; ++i)
-      k += E.h_mass_[size_t(i)] * (vv[3 * i] * vv[3 * i] + vv[3 * i + 1] * vv[3 * i + 1] + vv[3 * i + 2] * vv[3 * i + 2]);
+      k += S.hm[size_t(i)] * (vv[3 * i] * vv[3 * i] + vv[3 * i + 1] * vv[3 * i + 1] + vv[3 * i + 2] * vv[3 * i + 2]);
     return 0.5 * k / kAcc;
   }
 
@@ -1588,13 +1597,43 @@ void MdRun::start() {
   S.x.upload(st->x, n3, stream_);
   S.x0.alloc(n3);
   S.v.alloc(n3);
-  if (!S.masses_ready) {   // the masses are the force field's: set once per engine
-    S.m.upload(E.h_mass_, stream_);
-    std::vector<double> im(static_cast<size_t>(n_));
-    for (int i = 0; i < n_; ++i) im[size_t(i)] = E.h_mass_[size_t(i)] > 0 ? 1.0 / E.h_mass_[size_t(i)] : 0.0;
-    S.invm.upload(im, stream_);
-    CK(cudaStreamSynchronize(stream_));
-    S.masses_ready = true;
+  {
+    std::vector<int8_t> hflags;
+    if (o.hmr > 0 && o.is_hydrogen) hflags.assign(o.is_hydrogen, o.is_hydrogen + n_);
+    if (!S.masses_ready || S.hm_hmr != o.hmr || S.hm_h != hflags) {   // set again only when what they depend on changed
+      S.hm = E.h_mass_;
+      S.hmr_moved = 0;
+      S.hmr_kept = false;
+      if (o.hmr > 0) {
+        // hydrogen mass repartitioning (dynamics.cpp:125-147): a hydrogen with exactly one bonded neighbour heavier
+        // than itself takes mass from that neighbour up to o.hmr; a neighbour that would be left lighter than 1 u keeps
+        // its mass. Hydrogens: the element flags, or a mass below 1.6 u without them.
+        std::vector<std::vector<int>> nb(static_cast<size_t>(n_));
+        for (const auto& b : E.hb_) nb[b[0]].push_back(int(b[1])), nb[b[1]].push_back(int(b[0]));
+        auto hydrogen = [&](int i) { return o.is_hydrogen ? o.is_hydrogen[i] != 0 : E.h_mass_[size_t(i)] < 1.6; };
+        for (int i = 0; i < n_; ++i) {
+          if (!hydrogen(i) || nb[size_t(i)].size() != 1 || S.hm[size_t(i)] >= o.hmr) continue;
+          const int h = nb[size_t(i)][0];
+          const double dm = o.hmr - S.hm[size_t(i)];
+          if (hydrogen(h) || S.hm[size_t(h)] - dm < 1.0) {
+            S.hmr_kept = true;
+            continue;
+          }
+          S.hm[size_t(h)] -= dm;
+          S.hm[size_t(i)] = o.hmr;
+          ++S.hmr_moved;
+        }
+      }
+      S.m.upload(S.hm, stream_);
+      std::vector<double> im(static_cast<size_t>(n_));
+      for (int i = 0; i < n_; ++i) im[size_t(i)] = S.hm[size_t(i)] > 0 ? 1.0 / S.hm[size_t(i)] : 0.0;
+      S.invm.upload(im, stream_);
+      CK(cudaStreamSynchronize(stream_));
+      S.masses_ready = true;
+      S.hm_hmr = o.hmr;
+      S.hm_h = hflags;
+      S.cons_built = false;   // the constraint clusters are set up again with the masses
+    }
   }
   S.sc.alloc(kScNum);
   S.sc.zero(stream_);
@@ -1640,13 +1679,13 @@ void MdRun::start() {
   } else {
     std::fill(hv.begin(), hv.end(), 0.0);
     for (int i = 0; i < n_; ++i) {
-      const double sd = std::sqrt(kB * o.temperature * kAcc / E.h_mass_[size_t(i)]);
+      const double sd = std::sqrt(kB * o.temperature * kAcc / S.hm[size_t(i)]);
       for (int k = 0; k < 3; ++k) hv[3 * size_t(i) + k] = sd * S.rng->gauss();
     }
     double p[3] = {0, 0, 0}, mf = 0;
     for (int i = 0; i < n_; ++i) {
-      mf += E.h_mass_[size_t(i)];
-      for (int k = 0; k < 3; ++k) p[k] += E.h_mass_[size_t(i)] * hv[3 * size_t(i) + k];
+      mf += S.hm[size_t(i)];
+      for (int k = 0; k < 3; ++k) p[k] += S.hm[size_t(i)] * hv[3 * size_t(i) + k];
     }
     for (int i = 0; i < n_; ++i)
       for (int k = 0; k < 3; ++k) hv[3 * size_t(i) + k] -= p[k] / mf;
@@ -1734,24 +1773,50 @@ void MdRun::baro_step(long long s) {
   const double p = (2 * k + t.virial) / (3 * vol) * kAtm;
   const double hp = o.dt * baro_every;
   const double tnow = S.h_sc[kScTnow];
-  double deps = -o.compressibility / o.tau_p * (o.pressure - p) * hp;
-  const double ktv = kB * tnow / vol * kAtm;
-  deps += o.compressibility / o.tau_p * ktv * hp + std::sqrt(2 * ktv * o.compressibility * hp / o.tau_p) * S.rng->gauss();
-  deps = std::max(-0.01, std::min(0.01, deps));
-  const double mu = std::exp(deps / 3);
+  // per-axis factors (the isotropic update scales all three by the same mu)
+  double mu[3] = {1, 1, 1};
+  if (o.barostat == 2 && o.anisotropic) {
+    // Berendsen per axis (dynamics.cpp:668-687): mu_k = exp(-beta hp (P0 - P_kk) / (3 tau)), the step at most 0.33 %
+    const int axes = o.couple_axes ? o.couple_axes : 7;
+    for (int ax = 0; ax < 3; ++ax) {
+      if (!((axes >> ax) & 1)) continue;
+      const double target = ((o.axis_pressure_set >> ax) & 1) ? o.axis_pressure[ax] : o.pressure;
+      const double pk = (S.h_sc[kScKin0 + ax] + t.w[ax]) / vol * kAtm;
+      const double deps = std::max(-0.0033, std::min(0.0033, -o.compressibility / o.tau_p * (target - pk) * hp / 3));
+      mu[ax] = std::exp(deps);
+    }
+  } else {
+    double deps = -o.compressibility / o.tau_p * (o.pressure - p) * hp;
+    if (o.barostat == 1) {
+      // stochastic cell rescaling (Bernetti & Bussi 2020, eq. 5): the drift's k_B T / V term and the noise
+      const double ktv = kB * tnow / vol * kAtm;
+      deps += o.compressibility / o.tau_p * ktv * hp + std::sqrt(2 * ktv * o.compressibility * hp / o.tau_p) * S.rng->gauss();
+    }
+    deps = std::max(-0.01, std::min(0.01, deps));   // at most 1 % in volume per update
+    mu[0] = mu[1] = mu[2] = std::exp(deps / 3);
+  }
   std::vector<double> hx(n3);
   CK(cudaMemcpyAsync(hx.data(), S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
   CK(cudaMemcpyAsync(hv.data(), S.v.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
   CK(cudaStreamSynchronize(stream_));
   double cell[12];
   std::memcpy(cell, E.cell_h_, sizeof cell);
+  // positions about the cell origin, and every cell vector's component c, by mu[c]
   for (int i = 0; i < E.n_; ++i)
-    for (int c = 0; c < 3; ++c) hx[3 * size_t(i) + c] = cell[c] + mu * (hx[3 * size_t(i) + c] - cell[c]);
-  for (int q = 3; q < 12; ++q) cell[q] *= mu;
-  for (auto& q : hv) q /= mu;
-  const double k2 = host_ke(hv);
-  S.h_sc[kScBath] -= k2 - k;
-  CK(cudaMemcpyAsync(S.sc.p + kScBath, S.h_sc + kScBath, sizeof(double), cudaMemcpyHostToDevice, stream_));
+    for (int c = 0; c < 3; ++c) hx[3 * size_t(i) + c] = cell[c] + mu[c] * (hx[3 * size_t(i) + c] - cell[c]);
+  for (int q = 3; q < 12; ++q) cell[q] *= mu[q % 3];
+  if (o.barostat == 1) {   // the velocities follow the cell, and the bath takes the kinetic energy's change
+    for (auto& q : hv) q /= mu[0];
+    const double k2 = host_ke(hv);
+    S.h_sc[kScBath] -= k2 - k;
+    CK(cudaMemcpyAsync(S.sc.p + kScBath, S.h_sc + kScBath, sizeof(double), cudaMemcpyHostToDevice, stream_));
+  }
+  // the step's constraint virial, each component r_a F_b scaled with the cell (dynamics.cpp:448-456)
+  {
+    static const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
+    for (int c = 0; c < 6; ++c) S.h_sc[kScCW0 + c] *= std::sqrt(mu[ia[c]] * mu[ib[c]]);
+    CK(cudaMemcpyAsync(S.sc.p + kScCW0, S.h_sc + kScCW0, 6 * sizeof(double), cudaMemcpyHostToDevice, stream_));
+  }
   S.x.upload(hx, stream_);
   S.v.upload(hv, stream_);
   E.set_cell(cell);
@@ -1846,6 +1911,11 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
                   (long long)done, o.dt, wall, ms * 1e-3, setup, nsday, S.ncons, S.ndof, mixed_ ? "mixed FP32/fixed-point" : "FP64", batch_,
                   pair_cut_, pme_lines()[0], pme_lines()[1], pme_lines()[2], pme_cap_, bonded_cap_);
     *report = b;
+    if (o.hmr > 0) {   // the reference's note (dynamics.cpp:143-145)
+      std::snprintf(b, sizeof b, " · hydrogen mass repartitioning: %lld hydrogens at %.3f u, the difference taken from their bonded atoms%s",
+                    S.hmr_moved, o.hmr, S.hmr_kept ? " (some left as they were: their neighbour would have been too light)" : "");
+      *report += b;
+    }
   }
   R.completed = true;
   if (R.stopped_at >= 0) throw ModelError(CAPS_GPU_ESTOPPED, "stopped at step " + std::to_string(R.stopped_at + o.step_offset) + " (a stop was asked for)");

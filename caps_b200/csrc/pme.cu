@@ -60,10 +60,35 @@ void Engine::pme_setup(PmePath<R>& P) {
   const int la = int(128 / sizeof(T));
   P.lines[1] = std::max(1, std::min({la, cap / pk_[1], ph1_}));
   P.lines[2] = std::max(1, std::min({la, cap / pk_[2], ph1_}));
-  pme_tune(P);
+  if (tuning_pinned_)
+    for (int d = 0; d < 3; ++d) P.lines[d] = pinned_lines_[d];
+  else
+    pme_tune(P);
   for (int d = 0; d < 3; ++d) P.k[d] = pk_[d];
   green_valid_ = false;
   CK(cudaStreamSynchronize(stream_));
+}
+
+void Engine::tuning(int32_t v[7]) const {
+  const int* l = pme_lines();
+  const int32_t t[7] = {batch_, pair_cut_, pme_cap_, bonded_cap_, l[0], l[1], l[2]};
+  std::memcpy(v, t, sizeof t);
+}
+
+void Engine::pin_tuning(const int32_t v[7]) {
+  if (v[0] < 1 || v[0] > kBatch || v[1] < 0 || v[2] < 0 || v[3] < 0 || v[4] < 1 || v[5] < 1 || v[6] < 1)
+    throw ModelError(CAPS_GPU_EINVAL, "tuning values out of range");
+  batch_ = geom_.batch = v[0];
+  pair_cut_ = v[1];
+  pme_cap_ = v[2];
+  bonded_cap_ = v[3];
+  for (int d = 0; d < 3; ++d) pinned_lines_[d] = v[4 + d];
+  auto& lines = mixed_ ? pf_.lines : pd_.lines;
+  for (int d = 0; d < 3; ++d) lines[d] = v[4 + d];
+  tuning_pinned_ = true;
+  batch_tuned_ = true;
+  list_valid_ = false;
+  drop_run_state();
 }
 
 // The mixed path transforms in FP32 (pf_), the FP64 path in FP64 (pd_); each path is set up for the current grid on

@@ -62,7 +62,7 @@ struct LmpFrame {
     cell.a = {{norm3(c.a), 0, 0}};
     cell.b = {{dot3(c.b, ex), dot3(c.b, ey), 0}};
     cell.c = {{dot3(c.c, ex), dot3(c.c, ey), dot3(c.c, ez)}};
-    if (cell.c[2] < 0) {   // left-handed: the same box spanned by -c from the far face
+    if (cell.c[2] < 0) {   // c points below the ab plane: move the origin by c and flip c, which spans the same cell
       cell.o = add3(cell.o, cell.c);
       cell.c = scale3(cell.c, -1.0);
     }
@@ -135,7 +135,7 @@ struct caps_gpu_traj {
     std::memcpy(h, "CORD", 4);
     int32_t ic[20] = {};
     ic[2] = 1;
-    const float delta = float(dt_fs / 48.88821);   // AKMA time units
+    const float delta = float(dt_fs / 48.88821);   // the time step in units of 48.88821 fs (the CHARMM convention DCD readers expect)
     std::memcpy(&ic[9], &delta, 4);
     ic[19] = 24;
     std::memcpy(h + 4, ic, 80);

@@ -8,6 +8,7 @@ DynamicsCancelled).
 from __future__ import annotations
 
 import ctypes as C
+import math
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -116,7 +117,7 @@ class EnergyOptions:
 
 
 THERMOSTATS = {"none": 0, "nve": 0, "bussi": 1, "csvr": 1, "langevin": 2, "baoab": 2, "nose-hoover": 3, "nhc": 3}
-BAROSTATS = {"none": 0, "crescale": 1, "c-rescale": 1}
+BAROSTATS = {"none": 0, "crescale": 1, "c-rescale": 1, "berendsen": 2}
 
 
 @dataclass
@@ -142,6 +143,10 @@ class DynamicsOptions:
     step_offset: int = 0
     respa: int = 1
     respa_split: str = "bonded"        # "bonded": bonded terms inner (the reference's split); "pme": PME outer
+    hmr: float = 0.0                   # > 0: hydrogen mass repartitioning to this mass (u)
+    anisotropic: bool = False          # Berendsen barostat per Cartesian axis
+    couple_axis: tuple = (True, True, True)
+    axis_pressure: tuple = (float("nan"), float("nan"), float("nan"))   # atm per axis; NaN: `pressure`
     energy: EnergyOptions = field(default_factory=EnergyOptions)
 
     def to_struct(self, ff: ForceField, keep: list) -> _abi.MdOpts:
@@ -156,6 +161,14 @@ class DynamicsOptions:
         m.seed, m.thermo_every, m.frame_every, m.step_offset, m.respa = self.seed, self.thermo_every, self.frame_every, self.step_offset, self.respa
         m.respa_split = {"bonded": 0, "pme": 1}[self.respa_split]
         m.checkpoint_every = int(self.checkpoint_every)
+        m.hmr = float(self.hmr)
+        m.anisotropic = int(bool(self.anisotropic))
+        m.couple_axes = sum(1 << k for k in range(3) if self.couple_axis[k])
+        if self.anisotropic and m.couple_axes == 0:
+            raise ValueError("anisotropic pressure coupling needs at least one coupled axis")
+        m.axis_pressure_set = sum(1 << k for k in range(3) if not math.isnan(self.axis_pressure[k]))
+        for k in range(3):
+            m.axis_pressure[k] = 0.0 if math.isnan(self.axis_pressure[k]) else float(self.axis_pressure[k])
         if ff.element is not None:
             h = np.ascontiguousarray((ff.element == 1).astype(np.int8))
             o = np.ascontiguousarray((ff.element == 8).astype(np.int8))
@@ -257,6 +270,18 @@ class Evaluator:
     def set_timing(self, flush_bytes: int):
         """Measurement mode for run(): per-step CUDA events, an L2 flush of flush_bytes between steps (< 0: off)."""
         self._check(self.lib.caps_gpu_diag_set_timing(self.h, int(flush_bytes)))
+
+    def tuning(self) -> list[int]:
+        """The tuned launch shapes (include/caps_gpu_diag.h): entries per work item, pair-grid cut, PME grid cap, bonded
+        cap, PME line blocks x, y, z."""
+        v = (C.c_int32 * 7)()
+        self._check(self.lib.caps_gpu_diag_get_tuning(self.h, C.cast(v, C.c_void_p)))
+        return list(v)
+
+    def pin_tuning(self, v):
+        """Pins these launch shapes (the seven values tuning() returns); the engine tunes nothing afterwards."""
+        a = (C.c_int32 * 7)(*[int(x) for x in v])
+        self._check(self.lib.caps_gpu_diag_set_tuning(self.h, C.cast(a, C.c_void_p)))
 
     def last_step_ms(self) -> float:
         return float(self.lib.caps_gpu_diag_last_step_ms(self.h))

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define CAPS_GPU_ABI_VERSION 3
+#define CAPS_GPU_ABI_VERSION 4
 
 /* Status codes (negative). The text is in caps_gpu_error(). */
 #define CAPS_GPU_OK 0
@@ -122,7 +122,7 @@ typedef struct {
   double temperature_end;   /* K; >= 0 ramps the target linearly over the run */
   int32_t thermostat;       /* 0 none (NVE), 1 Bussi, 2 Langevin (BAOAB), 3 Nose-Hoover chain of 3 */
   double tau_t;             /* fs */
-  int32_t barostat;         /* 0 none, 1 stochastic cell rescaling */
+  int32_t barostat;         /* 0 none, 1 stochastic cell rescaling, 2 Berendsen (the reference's CRescale and Berendsen) */
   double pressure;          /* atm */
   double tau_p;             /* fs */
   double compressibility;   /* 1/atm */
@@ -142,6 +142,12 @@ typedef struct {
                                (dynamics.cpp:758-763) */
   caps_gpu_checkpoint_fn checkpoint;   /* NULL none */
   void* checkpoint_user;
+  /* ABI 4 */
+  double hmr;               /* > 0: hydrogen mass repartitioning to this mass in u (DynamicsOptions::hmr, dynamics.cpp:125-147) */
+  int32_t anisotropic;      /* with the Berendsen barostat: each Cartesian axis scaled on its own (dynamics.cpp:668-687) */
+  int32_t couple_axes;      /* with anisotropic: bit k couples axis k (DynamicsOptions::couple_axis); 0 means all three */
+  int32_t axis_pressure_set; /* with anisotropic: bit k set: axis k's target is axis_pressure[k], otherwise pressure */
+  double axis_pressure[3];  /* atm */
 } caps_gpu_md_opts;
 
 /* caps::ThermoRow (dynamics.hpp:28-43), the fields the device step fills. */

@@ -14,6 +14,12 @@ extern "C" {
  * stream and, when > 0, writes flush_bytes (larger than the 126 MB L2) between steps, outside the events; < 0 turns it
  * off. caps_gpu_last_steps_per_second then reports K / (sum of the per-step event times). */
 int32_t caps_gpu_diag_set_timing(caps_gpu_engine* e, int64_t flush_bytes);
+/* The launch shapes the engine's tuners chose (v[7]: entries per work item, pair-grid blocks per SM left free, PME
+ * line-transform grid cap, bonded blocks per term kind, PME line blocks along x, y, z; a cap of 0 means none), and
+ * the same shapes pinned on an engine, which then tunes nothing: a profiler, which slows the kernels it replays and
+ * so misleads the tuners, can see the shapes of a plain run. */
+int32_t caps_gpu_diag_get_tuning(const caps_gpu_engine* e, int32_t* v);
+int32_t caps_gpu_diag_set_tuning(caps_gpu_engine* e, const int32_t* v);
 /* Device milliseconds per MD step of the last run (the per-step events in measurement mode). */
 double caps_gpu_diag_last_step_ms(const caps_gpu_engine* e);
 /* Kernel launches in one plain MD step of the last run (the kernel nodes of its captured CUDA graph; the list-build and

@@ -362,11 +362,17 @@ int ref_run(const caps_gpu_ff* p, const caps_gpu_opts* eo, caps_gpu_state* st, c
     const Thermostat th[4] = {Thermostat::None, Thermostat::Bussi, Thermostat::Langevin, Thermostat::NoseHoover};
     o.thermostat = th[md->thermostat & 3];
     o.tau_t = md->tau_t;
-    o.barostat = md->barostat == 1 ? Barostat::CRescale : Barostat::None;
+    o.barostat = md->barostat == 1 ? Barostat::CRescale : md->barostat == 2 ? Barostat::Berendsen : Barostat::None;
     o.pressure = md->pressure;
     o.tau_p = md->tau_p;
     o.compressibility = md->compressibility;
     o.barostat_every = md->barostat_every;
+    o.hmr = md->hmr;
+    o.anisotropic = md->anisotropic != 0;
+    for (int a = 0; a < 3; ++a) {
+      o.couple_axis[a] = md->couple_axes == 0 || ((md->couple_axes >> a) & 1);
+      if ((md->axis_pressure_set >> a) & 1) o.axis_pressure[a] = md->axis_pressure[a];
+    }
     o.constraints = md->constraints ? ConstraintMode::HBonds : ConstraintMode::None;
     o.new_velocities = md->new_velocities != 0;
     o.seed = md->seed;
