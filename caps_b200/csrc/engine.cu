@@ -679,6 +679,46 @@ void Engine::read_terms(caps_gpu_terms* out, bool ener, bool vir) {
   if (out) *out = t;
 }
 
+// The pair list's entry, shift, work-item and exclusion-mask buffers made large enough for `ent` entries and `mk` mask
+// words; the next evaluation builds the list again.
+void Engine::grow_list(size_t ent, size_t mk) {
+  if (ent > d_ent_.n) {
+    d_ent_.release();
+    d_ent_shift_.release();
+    d_ent_.alloc(ent);
+    d_ent_shift_.alloc(ent);
+    d_work_.release();
+    d_work_.alloc(ent / 4 + size_t(nsc_cap_) * 2 + 64);
+  }
+  if (mk > d_masks_.n) {
+    d_masks_.release();
+    d_masks_.alloc(mk);
+  }
+  ensure_list_capacity();
+  list_valid_ = false;
+}
+
+// After the first evaluation of a run (synchronises): a list that overflowed its buffers, or filled more than two
+// thirds of them, is given room for 1.5 times what it holds (twice its capacity after an overflow), since a run's
+// list grows with the density it reaches and an overflow within a run ends the run. True: the list must be built again.
+bool Engine::grow_list_for_run() {
+  CK(cudaMemcpyAsync(h_counters_, d_counters_.p, sizeof(int) * kCntNum, cudaMemcpyDeviceToHost, stream_));
+  CK(cudaStreamSynchronize(stream_));
+  const unsigned e = unsigned(h_counters_[kCntErr]);
+  const bool over = (e & (kErrListOverflow | kErrMaskOverflow)) != 0;
+  const size_t used_e = size_t(std::max(0, h_counters_[kCntEnt])), used_m = size_t(std::max(0, h_counters_[kCntMask])) * 8;
+  size_t ent = d_ent_.n, mk = d_masks_.n;
+  if (over || 3 * used_e > 2 * d_ent_.n) ent = std::max(over ? 2 * d_ent_.n : d_ent_.n, used_e + used_e / 2);
+  if (over || 3 * used_m > 2 * d_masks_.n) mk = std::max(over ? 2 * d_masks_.n : d_masks_.n, used_m + used_m / 2);
+  if (ent == d_ent_.n && mk == d_masks_.n) return false;
+  if (over) {   // the overflow is answered here: clear it for the evaluation that follows
+    CK(cudaMemsetAsync(d_counters_.p + kCntErr, 0, sizeof(int), stream_));
+    h_counters_[kCntErr] = 0;
+  }
+  grow_list(ent, mk);
+  return true;
+}
+
 void Engine::compute_dev(const double* d_x, const double* cell, double* d_f, caps_gpu_terms* out) {
   set_cell(cell);
   for (int attempt = 0;; ++attempt) {
@@ -691,19 +731,7 @@ void Engine::compute_dev(const double* d_x, const double* cell, double* d_f, cap
       check_errors();
     } catch (const ModelError& m) {
       if (m.code != -100 || attempt >= 3) throw;
-      // grow the list and build again
-      const size_t ent = d_ent_.n * 2;
-      d_ent_.release();
-      d_ent_shift_.release();
-      d_ent_.alloc(ent);
-      d_ent_shift_.alloc(ent);
-      d_work_.release();
-      d_work_.alloc(ent / 4 + size_t(nsc_cap_) * 2 + 64);
-      const size_t mk = d_masks_.n * 2;
-      d_masks_.release();
-      d_masks_.alloc(mk);
-      ensure_list_capacity();
-      list_valid_ = false;
+      grow_list(d_ent_.n * 2, d_masks_.n * 2);   // and build again
       continue;
     }
     break;

@@ -181,6 +181,8 @@ class Engine {
   void setup_options();
   void set_cell(const double* cell);
   void ensure_list_capacity();
+  void grow_list(size_t ent, size_t mk);
+  bool grow_list_for_run();
   // One force evaluation up to the AoS doubles d_out (d_f_ by default), async. parts: a mask of 1 bonded, 2 short-range
   // non-bonded, 4 long-range (PME) terms (-1: the options' parts); clear_energies = false adds this evaluation's
   // energies and virial to the previous one's.

@@ -1703,8 +1703,11 @@ void MdRun::start() {
   if (S.ncons) S.rattle(0);
   if (S.bussi) S.make_draws(1, draw_chunk(1));
 
-  // the first force, energies and virial
-  S.forces(true, true);
+  // the first force, energies and virial; a list without room enough for the run is grown and built again
+  for (int attempt = 0;; ++attempt) {
+    S.forces(true, true);
+    if (attempt >= 3 || !E.grow_list_for_run()) break;
+  }
   if (S.ncons) {
     // step 0's constraint virial from one trial step on copies (dynamics.cpp:582-600)
     DevBuf<double>& xs = S.xs;
