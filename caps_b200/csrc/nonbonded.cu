@@ -224,7 +224,7 @@ void Engine::pair_forces(bool ener, bool vir) {
     // LJ table, the 4 warps' i atoms (three float4 each) and types, and their staged entries with the entries' j atoms
     // and exclusion masks
     const size_t smem = sizeof(float4) * (size_t(ntab) * ntab + 4 * 64 * 3) + sizeof(int) * 4 * 64 +
-                        4 * size_t(A.batch) * (sizeof(uint4) + sizeof(float4) + 8 * sizeof(float4) + 8 * sizeof(int) + 8 * sizeof(unsigned long long));
+                        4 * size_t(A.batch) * (sizeof(uint4) + sizeof(float4) + 8 * sizeof(float4) + 4 * sizeof(float4) + 8 * sizeof(unsigned long long));
     // the rational fits hold for (kappa r_c)^2 <= 16; past that the library erfc form
     const int c32 = coul == 0 ? 0 : (kappa_ * kappa_ * rc_ * rc_ <= double(kEwUMax) ? coul : coul + 2);
 #define PAIR32L(C, E, V, L, M)                                                                                       \

@@ -204,9 +204,12 @@ static __global__ void __launch_bounds__(128, (ENER || VIR) ? 4 : 5) k_pair_f32(
   const int nb = A.batch;
   uint4* s_en_all = reinterpret_cast<uint4*>(s_ti + 4 * 64);   // 4 warps x nb entries
   float4* s_sh_all = reinterpret_cast<float4*>(s_en_all + 4 * nb);
-  float4* s_xj_all = s_sh_all + 4 * nb;                         // 4 warps x nb entries x 8 j atoms
-  int* s_tj_all = reinterpret_cast<int*>(s_xj_all + 4 * nb * 8);
-  unsigned long long* s_mk_all = reinterpret_cast<unsigned long long*>(s_tj_all + 4 * nb * 8);
+  // the j atoms of an entry, shifted by its image and packed per lane quarter jq as the lane's operands:
+  // (x_jq, x_jq+4, y_jq, y_jq+4), (z_jq, z_jq+4, q_jq, q_jq+4)
+  float4* s_xj_all = s_sh_all + 4 * nb;                         // 4 warps x nb entries x 8 float4
+  // COMB: the j atoms' LJ factors per quarter, (f6_jq, f6_jq+4, f12_jq, f12_jq+4); else the j atoms' types
+  float4* s_gj_all = s_xj_all + 4 * nb * 8;                     // 4 warps x nb entries x 4 float4 (or 8 int)
+  unsigned long long* s_mk_all = reinterpret_cast<unsigned long long*>(s_gj_all + 4 * nb * 4);
   if (COMB) {
     for (int t = threadIdx.x; t < A.ntab; t += blockDim.x) ljf[t] = A.ljf[t];
   } else {
@@ -250,9 +253,12 @@ static __global__ void __launch_bounds__(128, (ENER || VIR) ? 4 : 5) k_pair_f32(
       ti_s[t] = ty;
     }
     __syncwarp();
+    // real i atoms of the lane, per i cluster c, in the layout of an entry's prune mask (bit c: the pair with j atom
+    // jq, bit c + 8: with jq + 4)
     unsigned ireal = 0;
 #pragma unroll
     for (int c = 0; c < 8; ++c) ireal |= unsigned(ti_s[8 * c + i8] != pad) << c;
+    ireal |= ireal << 8;
     float fix[8], fiy[8], fiz[8];
 #pragma unroll
     for (int c = 0; c < 8; ++c) fix[c] = fiy[c] = fiz[c] = 0.f;
@@ -260,7 +266,8 @@ static __global__ void __launch_bounds__(128, (ENER || VIR) ? 4 : 5) k_pair_f32(
     uint4* s_en = s_en_all + nb * wib;
     float4* s_sh = s_sh_all + nb * wib;
     float4* s_xj = s_xj_all + nb * 8 * wib;
-    int* s_tj = s_tj_all + nb * 8 * wib;
+    float4* s_gj = s_gj_all + nb * 4 * wib;
+    int* s_tj = reinterpret_cast<int*>(s_gj);
     unsigned long long* s_mk = s_mk_all + nb * 8 * wib;
     const int ne = min(wk.z, nb);
     if (lane < ne) {
@@ -272,11 +279,26 @@ static __global__ void __launch_bounds__(128, (ENER || VIR) ? 4 : 5) k_pair_f32(
     for (int k = 0; k < 8; ++k) {
       const int t = lane + 32 * k;   // entry t / 8, j atom t % 8
       if (t < 8 * ne) {
-        const uint4 e4 = s_en[t >> 3];
-        const int ja = 8 * int(e4.x) + (t & 7);
-        s_xj[t] = A.xq[ja];
-        s_tj[t] = A.tslot[ja];
-        s_mk[t] = e4.z ? A.masks[8 * size_t(e4.z - 1) + (t & 7)] : ~0ull;   // entry t / 8, i cluster t % 8
+        const int e = t >> 3, j = t & 7, q4 = j & 3, h = j >> 2;
+        const uint4 e4 = s_en[e];
+        const float4 sh = s_sh[e];
+        const int ja = 8 * int(e4.x) + j;
+        const float4 v = A.xq[ja];
+        float* px = reinterpret_cast<float*>(s_xj + 8 * e + 2 * q4);
+        px[h] = v.x + sh.x;
+        px[2 + h] = v.y + sh.y;
+        px[4 + h] = v.z + sh.z;
+        px[6 + h] = v.w;
+        const int ty = A.tslot[ja];
+        if (COMB) {
+          const float2 g = ljf[ty];
+          float* pg = reinterpret_cast<float*>(s_gj + 4 * e + q4);
+          pg[h] = g.x;
+          pg[2 + h] = g.y;
+        } else {
+          s_tj[t] = ty;
+        }
+        s_mk[t] = e4.z ? A.masks[8 * size_t(e4.z - 1) + j] : ~0ull;   // entry t / 8, i cluster t % 8
       }
     }
     __syncwarp();
@@ -284,30 +306,39 @@ static __global__ void __launch_bounds__(128, (ENER || VIR) ? 4 : 5) k_pair_f32(
       const uint4 en = s_en[el];
       const unsigned hmask = en.w & 0xffffu;
       if (!hmask) continue;
-      const float4 sh = s_sh[el];
       const int cj = int(en.x);
       const unsigned imask = (hmask | (hmask >> 8)) & 255u;
+      // the lane's listed pairs of the entry: a j half within the prune radius, a real i atom and, where the entry
+      // has exclusion masks, bits jq and jq + 4 of the i atom's row of its cluster's mask
+      unsigned lv = hmask & ireal;
+      if (en.z) {
+        unsigned xm = 0;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          const unsigned b = unsigned(s_mk[8 * el + c] >> (8 * i8 + jq));
+          xm |= ((b & 1u) << c) | (((b >> 4) & 1u) << (c + 8));
+        }
+        lv &= xm;
+      }
       const int j0 = 8 * cj + jq, j1 = j0 + 4;
-      const float4 a0 = s_xj[8 * el + jq], a1 = s_xj[8 * el + jq + 4];
-      const int t0 = s_tj[8 * el + jq], t1 = s_tj[8 * el + jq + 4];
-      const float2 xj = make_float2(a0.x + sh.x, a1.x + sh.x), yj = make_float2(a0.y + sh.y, a1.y + sh.y),
-                   zj = make_float2(a0.z + sh.z, a1.z + sh.z), qj = make_float2(a0.w, a1.w);
+      const float4 xa = s_xj[8 * el + 2 * jq], xb = s_xj[8 * el + 2 * jq + 1];
+      const float2 xj = make_float2(xa.x, xa.y), yj = make_float2(xa.z, xa.w), zj = make_float2(xb.x, xb.y), qj = make_float2(xb.z, xb.w);
       float2 g6j = p_dup(0.f), g12j = p_dup(0.f);
+      int t0 = 0, t1 = 0;
       if (COMB) {
-        const float2 g0 = ljf[t0], g1 = ljf[t1];
-        g6j = make_float2(g0.x, g1.x);
-        g12j = make_float2(g0.y, g1.y);
+        const float4 gg = s_gj[4 * el + jq];
+        g6j = make_float2(gg.x, gg.y);
+        g12j = make_float2(gg.z, gg.w);
+      } else {
+        t0 = s_tj[8 * el + jq];
+        t1 = s_tj[8 * el + jq + 4];
       }
       float2 fjx = p_dup(0.f), fjy = p_dup(0.f), fjz = p_dup(0.f);
 #pragma unroll
       for (int c = 0; c < 8; ++c) {
         if (!((imask >> c) & 1u)) continue;
-        const unsigned long long mm = s_mk[8 * el + c];
         const float4 pa = xi_s[3 * (8 * c + i8)], pb = xi_s[3 * (8 * c + i8) + 1];
-        // this lane's two pairs of the i cluster (j atoms jq and jq + 4): bits 0 and 4 of the exclusion mask, a real i
-        // atom, and the j half within the prune radius
-        const unsigned lb = ((ireal >> c) & 1u) ? unsigned(mm >> (8 * i8 + jq)) & 0x11u : 0u;
-        const bool l0 = (lb & 1u) && ((hmask >> c) & 1u), l1 = (lb & 0x10u) && ((hmask >> (c + 8)) & 1u);
+        const bool l0 = (lv >> c) & 1u, l1 = (lv >> (c + 8)) & 1u;
         const float2 dx = p_add(xj, make_float2(pa.x, pa.y)), dy = p_add(yj, make_float2(pa.z, pa.w)), dz = p_add(zj, make_float2(pb.x, pb.y));
         const float2 r2 = p_fma(dx, dx, p_fma(dy, dy, p_mul(dz, dz)));
         const bool ok0 = l0 && (r2.x < rc2), ok1 = l1 && (r2.y < rc2);
