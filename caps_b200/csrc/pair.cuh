@@ -183,6 +183,13 @@ __device__ __forceinline__ float2 p_add(float2 a, float2 b) { return __fadd2_rn(
 __device__ __forceinline__ float2 p_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 p_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 __device__ __forceinline__ float2 p_dup(float v) { return make_float2(v, v); }
+// the SFU's approximate 1/sqrt with denormals flushed (squared distances of listed pairs are > 0.01, or 1 for a pair
+// left out)
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
 
 // COUL: 0 none; 1 Ewald real space (PME) and 2 damped shifted force through the rational fits of ewald_fit.cuh
 // (kappa r_c <= 4); 3 and 4 the same through erfcf and expf (any kappa). COMB: the LJ coefficients of a type pair are
@@ -347,7 +354,7 @@ static __global__ void __launch_bounds__(128, (ENER || VIR) ? 4 : 5) k_pair_f32(
           nlist += float(l0) + float(l1);
         }
         const float2 r2s = make_float2(ok0 ? r2.x : 1.f, ok1 ? r2.y : 1.f);
-        const float2 rinv = make_float2(rsqrtf(r2s.x), rsqrtf(r2s.y));
+        const float2 rinv = make_float2(rsqrt_ftz(r2s.x), rsqrt_ftz(r2s.y));
         const float2 r2i = p_mul(rinv, rinv);
         const float2 r6i = p_mul(p_mul(r2i, r2i), r2i);
         float2 fr, elj;

@@ -87,16 +87,22 @@ namespace capsb {{
 constexpr float kEwUMax = {U:.1f}f;
 __device__ __forceinline__ float ew_h(float t) {{ return __fdividef({horner(hp)}, {horner(hq)}); }}
 __device__ __forceinline__ float ew_g(float t) {{ return __fdividef({horner(gp)}, {horner(gq)}); }}
-// both fits on a pair of arguments at once (packed FP32 multiply-adds; the two quotients are taken separately)
+// the SFU's approximate reciprocal with denormals flushed (the denominators lie in [1, 300])
+__device__ __forceinline__ float rcp_ftz(float x) {{
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}}
+// both fits on a pair of arguments at once (packed FP32 multiply-adds; the two reciprocals are taken separately)
 __device__ __forceinline__ float2 ew_h2(float2 t) {{
   const float2 n = {horner2(hp)};
   const float2 d = {horner2(hq)};
-  return make_float2(__fdividef(n.x, d.x), __fdividef(n.y, d.y));
+  return __fmul2_rn(n, make_float2(rcp_ftz(d.x), rcp_ftz(d.y)));
 }}
 __device__ __forceinline__ float2 ew_g2(float2 t) {{
   const float2 n = {horner2(gp)};
   const float2 d = {horner2(gq)};
-  return make_float2(__fdividef(n.x, d.x), __fdividef(n.y, d.y));
+  return __fmul2_rn(n, make_float2(rcp_ftz(d.x), rcp_ftz(d.y)));
 }}
 }}  // namespace capsb
 """
