@@ -212,6 +212,10 @@ class Engine {
   void read_terms(caps_gpu_terms* out, bool ener, bool vir);
   void check_errors();
   void launch_build(const double* d_x);
+  // the displacement check's arguments (SHAKE's launch: with the atoms in no constraint cluster), and whether a step may
+  // fold the check into its own kernels: a non-bonded evaluation with a valid list that is not frozen
+  ListCheck list_check(int nfree, const int* free_atoms) const;
+  bool list_check_fusable() const;
   void pme_forces(const double* d_x, bool ener, bool vir);
   template <class R> void pme_setup(PmePath<R>& P);
   template <class R> void pme_run(PmePath<R>& P, const double* d_x, bool ener, bool vir);

@@ -146,11 +146,16 @@ __device__ __forceinline__ void kick_drift_atom(const KickArgs& K, int i, double
     if (K.info && atomicCAS(K.counters + kCntNanClaim, 0, 1) == 0) K.info[kInfoNonFiniteStep] = K.sc[kScStep] + K.step_ahead;
   }
 }
-__global__ void k_kick_drift(KickArgs K) {
+// With L.xb set (a run without constraints), the displacement check of the drifted positions.
+__global__ void k_kick_drift(KickArgs K, ListCheck L) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (K.zero_cw && i < 6) K.sc[kScCW0 + i] = 0;
-  if (i >= K.n) return;
-  kick_drift_atom(K, i, K.scale ? K.sc[kScFactor] : 1.0);
+  bool mb = false, mp = false;
+  if (i < K.n) {
+    kick_drift_atom(K, i, K.scale ? K.sc[kScFactor] : 1.0);
+    if (L.xb) list_check_atom(L, i, K.x, mb, mp);
+  }
+  if (L.xb) list_check_flags(L, mb, mp);
 }
 
 // Constraint clusters. Star clusters (one centre bonded to 1-3 atoms, every constraint through the centre: CH, CH2, CH3)
@@ -319,9 +324,8 @@ __device__ void settle_water(const ConsArgs& C, int w, double* __restrict__ x, c
 
 // SHAKE on each cluster (Gauss-Seidel along the reference vectors, tol 1e-8 relative; core/src/constraints.cpp:196-230),
 // then v += (x - x_before) / h when h > 0.
-__global__ void k_shake(ConsArgs C, double* __restrict__ x, const double* __restrict__ x0, double* __restrict__ v, double h, int* counters) {
-  const int cc = blockIdx.x * blockDim.x + threadIdx.x;
-  if (cc >= C.ncl) return;
+__device__ void shake_cluster(const ConsArgs& C, int cc, double* __restrict__ x, const double* __restrict__ x0, double* __restrict__ v, double h,
+                              int* counters) {
   if (cc < C.e1) return shake_star<1>(C, cc, x, x0, v, h, counters);
   if (cc < C.e2) return shake_star<2>(C, cc, x, x0, v, h, counters);
   if (cc < C.e3) return shake_star<3>(C, cc, x, x0, v, h, counters);
@@ -376,6 +380,39 @@ __global__ void k_shake(ConsArgs C, double* __restrict__ x, const double* __rest
       if (h > 0) v[3 * g + r] += (px[a][r] - bx[a][r]) / h;
     }
   }
+}
+
+// The atoms of cluster cc through the displacement check.
+__device__ void check_cluster(const ConsArgs& C, const ListCheck& L, int cc, const double* x, bool& mb, bool& mp) {
+  if (cc < C.e3) {
+    const int4 at = C.star[cc];
+    const int ids[4] = {at.x, at.y, at.z, at.w};
+    for (int a = 0; a < 4; ++a)
+      if (ids[a] >= 0) list_check_atom(L, ids[a], x, mb, mp);
+  } else if (cc < C.e4) {
+    const int4 w = C.water[cc - C.e3];
+    list_check_atom(L, w.x, x, mb, mp);
+    list_check_atom(L, w.y, x, mb, mp);
+    list_check_atom(L, w.z, x, mb, mp);
+  } else {
+    const int c = cc - C.e4;
+    for (int a = C.cl_atom0[c]; a < C.cl_atom0[c + 1]; ++a) list_check_atom(L, C.cl_atoms[a], x, mb, mp);
+  }
+}
+
+// SHAKE, a thread per cluster; with L.xb set, the displacement check of the step's final positions on the clusters'
+// atoms and, after the clusters, on the L.nfree atoms in none.
+__global__ void k_shake(ConsArgs C, double* __restrict__ x, const double* __restrict__ x0, double* __restrict__ v, double h, int* counters,
+                        ListCheck L) {
+  const int cc = blockIdx.x * blockDim.x + threadIdx.x;
+  bool mb = false, mp = false;
+  if (cc < C.ncl) {
+    shake_cluster(C, cc, x, x0, v, h, counters);
+    if (L.xb) check_cluster(C, L, cc, x, mb, mp);
+  } else if (L.xb && cc < C.ncl + L.nfree) {
+    list_check_atom(L, L.free_atoms[cc - C.ncl], x, mb, mp);
+  }
+  if (L.xb) list_check_flags(L, mb, mp);
 }
 
 // The velocity update of one atom before RATTLE: a kick (v += hk kAcc f / m) or the Langevin O step
@@ -1208,14 +1245,19 @@ struct Stepper {
   // half kick, then drift with SHAKE; `scale` applies the thermostat's pending factor first
   // kick + drift, then SHAKE; the kick also clears the force evaluation's atom-order sums for the evaluation that
   // follows (Engine::forces then skips its own clearing)
+  // check: the list's displacement check runs in the drift (no constraints) or in SHAKE, and the force evaluation that
+  // follows skips its own
   void kick_drift(double hk, double hd, bool scale, bool zero_cw, const double* f = nullptr, const double* f2 = nullptr, double hk2 = 0,
-                  int step_ahead = 0) {
+                  int step_ahead = 0, bool check = false) {
     KickArgs K{n, x.p, v.p, x0.p, f ? f : E.d_f_.p, invm.p, hk, f2, hk2, hd, sc.p, scale ? 1 : 0, zero_cw ? 1 : 0, E.d_counters_.p,
                E.mixed_ ? E.d_F_.p : nullptr, E.mixed_ ? nullptr : E.d_Fd_.p, E.d_errinfo_.p, step_ahead};
-    launch_k(k_kick_drift, blocks(size_t(n), 256), 256, 0, E.stream_, K);
-    if (ncons) launch_k(k_shake, blocks(size_t(C.ncl), 128), 128, 0, E.stream_, C, x.p, x0.p, v.p, hd, E.d_counters_.p);
+    const ListCheck L = check ? E.list_check(nfree, free_atoms.p) : ListCheck{};
+    launch_k(k_kick_drift, blocks(size_t(n), 256), 256, 0, E.stream_, K, ncons ? ListCheck{} : L);
+    if (ncons) launch_k(k_shake, blocks(size_t(C.ncl) + (check ? size_t(nfree) : 0), 128), 128, 0, E.stream_, C, x.p, x0.p, v.p, hd, E.d_counters_.p, L);
     E.sums_cleared_ = true;
   }
+  // whether this step's drift may take the list's displacement check (a plain step: not r-RESPA)
+  bool fuse_check() const { return respa <= 1 && E.list_check_fusable(); }
   // a velocity update, then RATTLE (constraint virial summed when h > 0); with ke, also the kinetic energy and ke's
   // thermostat update (constraints only: the caller launches k_ke otherwise)
   void vel_rattle(const VelOp& op, double h, const KeArgs* ke = nullptr) {
@@ -1253,13 +1295,14 @@ struct Stepper {
   // fast one. Part masks as Engine::forces takes them.
   DevBuf<double> f_slow, f_fast;
   int respa = 1, slow_parts = 6, fast_parts = 1;
-  void forces(bool ener, bool vir, bool reduce = true) {
+  // checked: the drift before ran the list's displacement check
+  void forces(bool ener, bool vir, bool reduce = true, bool checked = false) {
     if (respa > 1) {
       E.forces(x.p, ener, vir, true, slow_parts, f_slow.p, true);
       E.forces(x.p, ener, vir, true, fast_parts, f_fast.p, false);
       return;
     }
-    E.forces(x.p, ener, vir, true, -1, nullptr, true, reduce);
+    E.forces(x.p, ener, vir, !checked, -1, nullptr, true, reduce);
   }
   void fast_forces() { E.forces(x.p, false, false, true, fast_parts, f_fast.p, true); }
 
@@ -1301,33 +1344,36 @@ struct Stepper {
       A = ke_args(kScKE, false);
       A.then = kThenBath;
       ke_launch(A);
-      kick_drift(0, 0.5 * dt, false, false);
-      forces(ener, vir);
+      const bool chk = fuse_check();
+      kick_drift(0, 0.5 * dt, false, false, nullptr, nullptr, 0, 0, chk);
+      forces(ener, vir, true, chk);
       vel_rattle(kick_op(0.5 * dt), hw);
     } else if (nhc) {
       launch_k(k_nhc_begin, 1, 1, 0, E.stream_, chain.p, sc.p, o.temperature, o.temperature_end, (long long)o.steps, ndof, t_freq, dt);
-      kick_drift(0.5 * dt, dt, true, true);
+      const bool chk = fuse_check();
+      kick_drift(0.5 * dt, dt, true, true, nullptr, nullptr, 0, 0, chk);
       KeArgs A = ke_args(kScKE, false);
       A.then = kThenNhc;
       if (fused_tail()) {
-        forces(ener, vir, false);
+        forces(ener, vir, false, chk);
         vel_rattle(kick_op_sums(0.5 * dt), hw, &A);
       } else {
-        forces(ener, vir);
+        forces(ener, vir, true, chk);
         vel_rattle(kick_op(0.5 * dt), hw);
         ke_launch(A);
       }
       scale_v();
     } else {
       launch_k(k_step_begin, 1, 1, 0, E.stream_, sc.p, o.temperature, o.temperature_end, (long long)o.steps, ndof);
-      kick_drift(0.5 * dt, dt, false, true);
+      const bool chk = fuse_check();
+      kick_drift(0.5 * dt, dt, false, true, nullptr, nullptr, 0, 0, chk);
       KeArgs A = ke_args(kScKE, false);
       A.then = kThenBussi;
       if (fused_tail()) {
-        forces(ener, vir, false);
+        forces(ener, vir, false, chk);
         vel_rattle(kick_op_sums(0.5 * dt), hw, bussi ? &A : nullptr);
       } else {
-        forces(ener, vir);
+        forces(ener, vir, true, chk);
         vel_rattle(kick_op(0.5 * dt), hw);
         if (bussi) ke_launch(A);
       }
@@ -1668,7 +1714,7 @@ void MdRun::start() {
   S.rng = std::make_unique<HostRng>(o.seed);
   if (S.ncons) {   // the constrained lengths hold from the start (dynamics.cpp:198-203)
     CK(cudaMemcpyAsync(S.x0.p, S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
-    launch_k(k_shake, blocks(size_t(S.C.ncl), 128), 128, 0, stream_, S.C, S.x.p, S.x0.p, S.v.p, 0.0, E.d_counters_.p);
+    launch_k(k_shake, blocks(size_t(S.C.ncl), 128), 128, 0, stream_, S.C, S.x.p, S.x0.p, S.v.p, 0.0, E.d_counters_.p, ListCheck{});
   }
 
   // velocities: given, or Maxwell-Boltzmann from the reference's stream, no centre-of-mass motion, rescaled to T
@@ -1826,7 +1872,7 @@ void MdRun::baro_step(long long s) {
   S.C.cell = E.dcell_;
   if (S.ncons) {
     CK(cudaMemcpyAsync(S.x0.p, S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
-    launch_k(k_shake, blocks(size_t(S.C.ncl), 128), 128, 0, stream_, S.C, S.x.p, S.x0.p, S.v.p, 0.0, E.d_counters_.p);
+    launch_k(k_shake, blocks(size_t(S.C.ncl), 128), 128, 0, stream_, S.C, S.x.p, S.x0.p, S.v.p, 0.0, E.d_counters_.p, ListCheck{});
     S.rattle(0);
   }
   S.forces(true, true);

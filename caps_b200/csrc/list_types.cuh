@@ -56,7 +56,7 @@ struct ListBufs {
 
 // Device counters: list sizes, the error word, the rebuild and prune flags, and running counts of builds and prunes.
 enum Counter { kCntEnt = 0, kCntWork, kCntMask, kCntErr, kCntRebuild, kCntNsc, kCntMaxCol, kCntPrune, kCntBuilds, kCntPrunes, kCntPairNext,
-               kCntFeneClaim, kCntNanClaim, kCntNum = 13 };   // *Claim: 1 once the first failure of that kind left its details
+               kCntFeneClaim, kCntNanClaim, kCntBinDone, kCntNum = 14 };   // *Claim: 1 once the first failure of that kind left its details
 
 __device__ __forceinline__ void raise_error(int* counters, unsigned bit) { atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), bit); }
 
@@ -72,5 +72,31 @@ __host__ __device__ __forceinline__ void unpack_image(unsigned p, int& qa, int& 
 
 // Gate for the build kernels in a captured step: they all return at once unless the rebuild flag is set.
 __device__ __forceinline__ bool build_off(const int* counters) { return *(volatile const int*)(counters + kCntRebuild) == 0; }
+
+// The displacement check (core/src/field.cpp:800-838, the constant-cell branch): has an atom moved more than half the
+// skin since the last build (x against xb, lim_b2), or half the prune margin since the last prune (x against xp,
+// lim_p2)? Sets the rebuild and prune flags. It runs in the kernel that writes a step's final positions (the drift, or
+// SHAKE and the atoms in no constraint cluster), or as a kernel of its own; xb null: no check.
+struct ListCheck {
+  const double* xb;
+  const double* xp;
+  double lim_b2, lim_p2;
+  int* counters;
+  int nfree;              // SHAKE's launch: the atoms in no cluster, after the clusters
+  const int* free_atoms;
+};
+__device__ __forceinline__ void list_check_atom(const ListCheck& L, int g, const double* x, bool& mb, bool& mp) {
+  const double x_ = x[3 * g], y_ = x[3 * g + 1], z_ = x[3 * g + 2];
+  const double bx = x_ - L.xb[3 * g], by = y_ - L.xb[3 * g + 1], bz = z_ - L.xb[3 * g + 2];
+  const double px = x_ - L.xp[3 * g], py = y_ - L.xp[3 * g + 1], pz = z_ - L.xp[3 * g + 2];
+  mb |= !(bx * bx + by * by + bz * bz <= L.lim_b2);   // NaN counts as moved
+  mp |= !(px * px + py * py + pz * pz <= L.lim_p2);
+}
+// Raises the flags a warp's atoms call for (every lane of the warp calls it).
+__device__ __forceinline__ void list_check_flags(const ListCheck& L, bool mb, bool mp) {
+  const bool lane0 = (threadIdx.x & 31) == 0;
+  if (__any_sync(0xffffffffu, mb) && lane0) atomicOr(L.counters + kCntRebuild, 1);
+  if (__any_sync(0xffffffffu, mp) && lane0) atomicOr(L.counters + kCntPrune, 1);
+}
 
 }  // namespace capsb

@@ -16,66 +16,32 @@
 namespace capsb {
 
 // ---------------------------------------------------------------------------------------------------------------
-// K-CHECK: has any atom moved more than half the skin since the last build (x against x0, lim_b2; core/src/field.cpp:
-// 800-838, the constant-cell branch), or half the prune margin since the last prune (x against xp, lim_p2)? Sets the
-// rebuild and prune flags; the pair kernel lowers both once the step's list work is done.
-static __global__ void k_check_step(int n, const double* __restrict__ x, const double* __restrict__ x0, double lim_b2, const double* __restrict__ xp,
-                                    double lim_p2, int* counters) {
+// K-CHECK: the displacement check as a kernel of its own, for force evaluations outside a step that folds it in.
+static __global__ void k_check_step(int n, const double* __restrict__ x, ListCheck L) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   bool mb = false, mp = false;
-  if (i < n) {
-    const double x_ = x[3 * i], y_ = x[3 * i + 1], z_ = x[3 * i + 2];
-    const double bx = x_ - x0[3 * i], by = y_ - x0[3 * i + 1], bz = z_ - x0[3 * i + 2];
-    const double px = x_ - xp[3 * i], py = y_ - xp[3 * i + 1], pz = z_ - xp[3 * i + 2];
-    mb = !(bx * bx + by * by + bz * bz <= lim_b2);   // NaN counts as moved
-    mp = !(px * px + py * py + pz * pz <= lim_p2);
-  }
-  const bool lane0 = (threadIdx.x & 31) == 0;
-  if (__any_sync(0xffffffffu, mb) && lane0) atomicOr(counters + kCntRebuild, 1);
-  if (__any_sync(0xffffffffu, mp) && lane0) atomicOr(counters + kCntPrune, 1);
+  if (i < n) list_check_atom(L, i, x, mb, mp);
+  list_check_flags(L, mb, mp);
 }
 
-// K-BIN: wrapped fractional coordinates, lattice offsets and the column of every atom; column counts.
-static __global__ void k_bin(int n, const double* __restrict__ x, DevCell cell, ListGeom g, ListBufs b) {
-  if (build_off(b.counters)) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double xi[3] = {x[3 * i], x[3 * i + 1], x[3 * i + 2]};
-  double f[3];
-  frac_of(cell, xi, f);
-  for (int k = 0; k < 3; ++k) {
-    const double fl = floor(f[k]);
-    double w = f[k] - fl;
-    w = fmin(fmax(w, 0.0), 1.0 - 1e-12);
-    b.frac[3 * i + k] = w;
-    b.ioff[3 * i + k] = -int(fl);
-  }
-  const int cu = min(g.nu - 1, int(b.frac[3 * i] * g.nu)), cv = min(g.nv - 1, int(b.frac[3 * i + 1] * g.nv));
-  const int c = cu * g.nv + cv;
-  b.col[i] = c;
-  // one atomic per distinct column in the warp (a column holds hundreds of atoms: the adds would contend)
-  const unsigned act = __activemask();
-  const unsigned same = __match_any_sync(act, c);
-  if ((threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(b.col_count + c, __popc(same));
-}
-
-// K-SCAN (one block): column starts, super-cluster starts (64 atoms each, the last one of a column partial), and the
-// column of every super-cluster. Also resets the list counters for the search.
-static __global__ void k_scan_columns(ListGeom g, ListBufs b) {
-  if (build_off(b.counters)) return;
-  __shared__ int s_a[1024], s_s[1024];
+// K-SCAN (one block, NT threads): column starts, super-cluster starts (64 atoms each, the last one of a column
+// partial), and the column of every super-cluster. Also resets the list counters for the search. The column counts are
+// read through L2 (the other blocks of the binning made them with atomics).
+template <int NT>
+__device__ void scan_columns(const ListGeom& g, const ListBufs& b) {
+  __shared__ int s_a[NT], s_s[NT];
   __shared__ int carry_a, carry_s, s_max;
   if (threadIdx.x == 0) carry_a = carry_s = s_max = 0;
   __syncthreads();
-  for (int base = 0; base < g.ncol; base += blockDim.x) {
+  for (int base = 0; base < g.ncol; base += NT) {
     const int c = base + threadIdx.x;
-    const int cnt = c < g.ncol ? b.col_count[c] : 0;
+    const int cnt = c < g.ncol ? __ldcg(b.col_count + c) : 0;
     if (c < g.ncol) b.col_count[c] = 0;   // cleared for the next build's binning
     if (c < g.ncol) atomicMax(&s_max, cnt);
     s_a[threadIdx.x] = cnt;
     s_s[threadIdx.x] = (cnt + kScAtoms - 1) / kScAtoms;
     __syncthreads();
-    for (int off = 1; off < int(blockDim.x); off <<= 1) {   // inclusive Hillis-Steele scan
+    for (int off = 1; off < NT; off <<= 1) {   // inclusive Hillis-Steele scan
       const int ta = threadIdx.x >= unsigned(off) ? s_a[threadIdx.x - off] : 0;
       const int ts = threadIdx.x >= unsigned(off) ? s_s[threadIdx.x - off] : 0;
       __syncthreads();
@@ -89,7 +55,7 @@ static __global__ void k_scan_columns(ListGeom g, ListBufs b) {
       b.col_fill[c] = 0;
     }
     __syncthreads();
-    if (threadIdx.x == blockDim.x - 1) {
+    if (threadIdx.x == NT - 1) {
       carry_a += s_a[threadIdx.x];
       carry_s += s_s[threadIdx.x];
     }
@@ -108,8 +74,44 @@ static __global__ void k_scan_columns(ListGeom g, ListBufs b) {
   }
   __syncthreads();
   const int nsc = min(carry_s, b.nsc_cap);
-  for (int c = threadIdx.x; c < g.ncol; c += blockDim.x)
+  for (int c = threadIdx.x; c < g.ncol; c += NT)
     for (int s = b.col_sc[c]; s < b.col_sc[c + 1] && s < nsc; ++s) b.sc_col[s] = c;
+}
+
+// K-BIN: wrapped fractional coordinates, lattice offsets and the column of every atom; column counts. The last block
+// to finish (a ticket taken after a fence) runs the column scan, so the build has no launch of its own for it.
+constexpr int kBinThreads = 256;
+static __global__ void __launch_bounds__(kBinThreads) k_bin(int n, const double* __restrict__ x, DevCell cell, ListGeom g, ListBufs b) {
+  if (build_off(b.counters)) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    const double xi[3] = {x[3 * i], x[3 * i + 1], x[3 * i + 2]};
+    double f[3];
+    frac_of(cell, xi, f);
+    for (int k = 0; k < 3; ++k) {
+      const double fl = floor(f[k]);
+      double w = f[k] - fl;
+      w = fmin(fmax(w, 0.0), 1.0 - 1e-12);
+      b.frac[3 * i + k] = w;
+      b.ioff[3 * i + k] = -int(fl);
+    }
+    const int cu = min(g.nu - 1, int(b.frac[3 * i] * g.nu)), cv = min(g.nv - 1, int(b.frac[3 * i + 1] * g.nv));
+    const int c = cu * g.nv + cv;
+    b.col[i] = c;
+    // one atomic per distinct column in the warp (a column holds hundreds of atoms: the adds would contend)
+    const unsigned act = __activemask();
+    const unsigned same = __match_any_sync(act, c);
+    if ((threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(b.col_count + c, __popc(same));
+  }
+  __shared__ bool s_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(b.counters + kCntBinDone, 1) == int(gridDim.x) - 1;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  scan_columns<kBinThreads>(g, b);
+  if (threadIdx.x == 0) b.counters[kCntBinDone] = 0;
 }
 
 // K-SCATTER: atoms into their column's range (unordered; the sort that follows fixes the order).
@@ -128,11 +130,121 @@ static __global__ void k_scatter(int n, ListBufs b) {
   b.order[b.col_start[c] + base + __popc(same & ((1u << lane) - 1))] = i;
 }
 
-// K-SORT (block per column): atoms by fractional c, ties by index. A bitonic sorting network in shared memory over the
-// column padded to a power of two (pad keys sort last): log2(n)(log2(n)+1)/2 compare-exchange rounds, one barrier each.
-static __global__ void k_sort_columns(ListGeom g, ListBufs b) {
+// K-SUPER (a warp per super-cluster, inside the sort of its column): the 2 x 2 x 2 split into clusters, perm / iperm,
+// cluster boxes and real-atom masks, the super-cluster's origin and its c range. Lane l holds atoms l (lower c half) and
+// l + 32 (upper c half): the ranks along y and x come from shuffles, the boxes from butterfly reductions over the 8 lanes
+// of a cluster. s_w and s_a: the warp's world positions and atoms by local slot (-1 padding).
+__device__ void form_supercluster(const DevCell& cell, const ListBufs& b, int sc, int c, int lane, double (*s_w)[3], int* s_a) {
+  const unsigned full = 0xffffffffu;
+  {
+    const int k = sc - b.col_sc[c];
+    const int s0 = b.col_start[c] + kScAtoms * k;
+    const int m = min(kScAtoms, b.col_start[c + 1] - s0);
+    if (m <= 0) {   // not made by the scan (every super-cluster holds at least one atom); kept empty
+      b.perm[64 * sc + lane] = b.perm[64 * sc + lane + 32] = -1;
+      return;
+    }
+    int id[2];
+    double fx[2], fy[2], w[2][3];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int t = lane + 32 * h;
+      id[h] = -1;
+      fx[h] = fy[h] = 0;
+      w[h][0] = w[h][1] = w[h][2] = 0;
+      if (t < m) {
+        const int a = b.order[s0 + t];
+        id[h] = a;
+        const double f0 = b.frac[3 * a], f1 = b.frac[3 * a + 1], f2 = b.frac[3 * a + 2];
+        fx[h] = f0, fy[h] = f1;
+        for (int r = 0; r < 3; ++r) w[h][r] = cell.o[r] + cell.h[r][0] * f0 + cell.h[r][1] * f1 + cell.h[r][2] * f2;
+      }
+      s_a[t] = -1;
+    }
+    // rank along y within the c half, then along x within the y half of the c half (ties by atom index)
+    int ry[2] = {0, 0}, rx[2] = {0, 0};
+    for (int u = 0; u < 32; ++u) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const double yu = __shfl_sync(full, fy[h], u);
+        const int iu = __shfl_sync(full, id[h], u);
+        ry[h] += (u + 32 * h < m) && (yu < fy[h] || (yu == fy[h] && iu < id[h]));
+      }
+    }
+    for (int u = 0; u < 32; ++u) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const double xu = __shfl_sync(full, fx[h], u);
+        const int iu = __shfl_sync(full, id[h], u);
+        const int qu = __shfl_sync(full, ry[h] >> 4, u);
+        rx[h] += (u + 32 * h < m) && qu == (ry[h] >> 4) && (xu < fx[h] || (xu == fx[h] && iu < id[h]));
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (lane + 32 * h >= m) continue;
+      const int slot = 8 * (4 * h + 2 * (ry[h] >> 4) + (rx[h] >> 3)) + (rx[h] & 7);
+      s_a[slot] = id[h];
+      for (int r = 0; r < 3; ++r) s_w[slot][r] = w[h][r];
+      b.iperm[id[h]] = 64 * sc + slot;
+    }
+    __syncwarp();
+    // cluster boxes and real masks: slot lane + 32 h belongs to cluster (lane >> 3) + 4 h
+    double slo[3] = {1e300, 1e300, 1e300}, shi[3] = {-1e300, -1e300, -1e300};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int t = lane + 32 * h;
+      const int a = s_a[t];
+      b.perm[64 * sc + t] = a;
+      double lo[3], hi[3];
+      for (int r = 0; r < 3; ++r) {
+        lo[r] = a >= 0 ? s_w[t][r] : 1e300;
+        hi[r] = a >= 0 ? s_w[t][r] : -1e300;
+      }
+#pragma unroll
+      for (int o = 1; o < 8; o <<= 1)
+        for (int r = 0; r < 3; ++r) {
+          lo[r] = fmin(lo[r], __shfl_xor_sync(full, lo[r], o));
+          hi[r] = fmax(hi[r], __shfl_xor_sync(full, hi[r], o));
+        }
+      const unsigned real = __ballot_sync(full, a >= 0);
+      if ((lane & 7) == 0) {
+        const int cg = 8 * sc + (lane >> 3) + 4 * h;
+        for (int r = 0; r < 3; ++r) b.cl_box[6 * cg + r] = lo[r], b.cl_box[6 * cg + 3 + r] = hi[r];
+        b.cl_real[cg] = (unsigned char)((real >> (lane & 24)) & 255u);
+      }
+      for (int r = 0; r < 3; ++r) slo[r] = fmin(slo[r], lo[r]), shi[r] = fmax(shi[r], hi[r]);
+    }
+#pragma unroll
+    for (int o = 8; o < 32; o <<= 1)
+      for (int r = 0; r < 3; ++r) {
+        slo[r] = fmin(slo[r], __shfl_xor_sync(full, slo[r], o));
+        shi[r] = fmax(shi[r], __shfl_xor_sync(full, shi[r], o));
+      }
+    const int last = m - 1;
+    const int id_first = __shfl_sync(full, id[0], 0);
+    const int id_last = __shfl_sync(full, (last >> 5) ? id[1] : id[0], last & 31);
+    if (lane == 0) {
+      for (int r = 0; r < 3; ++r) b.sc_org[3 * sc + r] = 0.5 * (slo[r] + shi[r]);
+      b.sc_z[2 * sc] = b.frac[3 * id_first + 2];
+      b.sc_z[2 * sc + 1] = b.frac[3 * id_last + 2];
+    }
+    __syncwarp();
+  }
+}
+
+// K-SORT (block per column): atoms by fractional c, ties by index, then the column's super-clusters (K-SUPER). A
+// bitonic sorting network in shared memory over the column padded to a power of two (pad keys sort last):
+// log2(n)(log2(n)+1)/2 compare-exchange rounds, one barrier each.
+constexpr int kSortThreads = 1024;
+constexpr int kScWarps = 16;   // warps of the sort block that form the column's super-clusters
+static_assert(sizeof(double) * 3 * 64 * kScWarps + sizeof(int) * 64 * kScWarps <= size_t(kSortMax) * (sizeof(double) + sizeof(int)),
+              "the super-cluster stage fits the sort's shared memory");
+static __global__ void __launch_bounds__(kSortThreads) k_sort_columns(DevCell cell, ListGeom g, ListBufs b) {
   if (build_off(b.counters)) return;
   extern __shared__ unsigned char smem_raw[];
+  const int nsc = min(b.counters[kCntNsc], b.nsc_cap);
   double* key = reinterpret_cast<double*>(smem_raw);
   int* id = reinterpret_cast<int*>(key + kSortMax);
   for (int c = blockIdx.x; c < g.ncol; c += gridDim.x) {
@@ -166,117 +278,18 @@ static __global__ void k_sort_columns(ListGeom g, ListBufs b) {
       }
     for (int k = threadIdx.x; k < n; k += blockDim.x) b.order[s0 + k] = id[k];
     __syncthreads();
+    // the column's super-clusters, a warp each, in the shared memory the sort is done with
+    const int w = threadIdx.x >> 5;
+    if (w < kScWarps) {
+      double(*s_w)[3] = reinterpret_cast<double(*)[3]>(smem_raw) + 64 * w;
+      int* s_a = reinterpret_cast<int*>(smem_raw + sizeof(double) * 3 * 64 * kScWarps) + 64 * w;
+      const int sc1 = min(b.col_sc[c + 1], nsc);
+      for (int sc = b.col_sc[c] + w; sc < sc1; sc += kScWarps) form_supercluster(cell, b, sc, c, threadIdx.x & 31, s_w, s_a);
+    }
+    __syncthreads();
   }
 }
 
-// K-SUPER (warp per super-cluster): the 2 x 2 x 2 split into clusters, perm / iperm, cluster boxes and real-atom
-// masks, the super-cluster's origin and its c range. Lane l holds atoms l (lower c half) and l + 32 (upper c half):
-// the ranks along y and x come from shuffles, the boxes from butterfly reductions over the 8 lanes of a cluster.
-static __global__ void k_superclusters(DevCell cell, ListBufs b) {
-  if (build_off(b.counters)) return;
-  __shared__ double s_w[4][64][3];   // world position by local slot
-  __shared__ int s_a[4][64];         // atom by local slot, -1 padding
-  const unsigned full = 0xffffffffu;
-  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nsc = min(b.counters[kCntNsc], b.nsc_cap);
-  for (int sc = blockIdx.x * 4 + wib; sc < nsc; sc += gridDim.x * 4) {
-    const int c = b.sc_col[sc];
-    const int k = sc - b.col_sc[c];
-    const int s0 = b.col_start[c] + kScAtoms * k;
-    const int m = min(kScAtoms, b.col_start[c + 1] - s0);
-    if (m <= 0) {   // not made by the scan (every super-cluster holds at least one atom); kept empty
-      b.perm[64 * sc + lane] = b.perm[64 * sc + lane + 32] = -1;
-      continue;
-    }
-    int id[2];
-    double fx[2], fy[2], w[2][3];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int t = lane + 32 * h;
-      id[h] = -1;
-      fx[h] = fy[h] = 0;
-      w[h][0] = w[h][1] = w[h][2] = 0;
-      if (t < m) {
-        const int a = b.order[s0 + t];
-        id[h] = a;
-        const double f0 = b.frac[3 * a], f1 = b.frac[3 * a + 1], f2 = b.frac[3 * a + 2];
-        fx[h] = f0, fy[h] = f1;
-        for (int r = 0; r < 3; ++r) w[h][r] = cell.o[r] + cell.h[r][0] * f0 + cell.h[r][1] * f1 + cell.h[r][2] * f2;
-      }
-      s_a[wib][t] = -1;
-    }
-    // rank along y within the c half, then along x within the y half of the c half (ties by atom index)
-    int ry[2] = {0, 0}, rx[2] = {0, 0};
-    for (int u = 0; u < 32; ++u) {
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const double yu = __shfl_sync(full, fy[h], u);
-        const int iu = __shfl_sync(full, id[h], u);
-        ry[h] += (u + 32 * h < m) && (yu < fy[h] || (yu == fy[h] && iu < id[h]));
-      }
-    }
-    for (int u = 0; u < 32; ++u) {
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const double xu = __shfl_sync(full, fx[h], u);
-        const int iu = __shfl_sync(full, id[h], u);
-        const int qu = __shfl_sync(full, ry[h] >> 4, u);
-        rx[h] += (u + 32 * h < m) && qu == (ry[h] >> 4) && (xu < fx[h] || (xu == fx[h] && iu < id[h]));
-      }
-    }
-    __syncwarp();
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      if (lane + 32 * h >= m) continue;
-      const int slot = 8 * (4 * h + 2 * (ry[h] >> 4) + (rx[h] >> 3)) + (rx[h] & 7);
-      s_a[wib][slot] = id[h];
-      for (int r = 0; r < 3; ++r) s_w[wib][slot][r] = w[h][r];
-      b.iperm[id[h]] = 64 * sc + slot;
-    }
-    __syncwarp();
-    // cluster boxes and real masks: slot lane + 32 h belongs to cluster (lane >> 3) + 4 h
-    double slo[3] = {1e300, 1e300, 1e300}, shi[3] = {-1e300, -1e300, -1e300};
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int t = lane + 32 * h;
-      const int a = s_a[wib][t];
-      b.perm[64 * sc + t] = a;
-      double lo[3], hi[3];
-      for (int r = 0; r < 3; ++r) {
-        lo[r] = a >= 0 ? s_w[wib][t][r] : 1e300;
-        hi[r] = a >= 0 ? s_w[wib][t][r] : -1e300;
-      }
-#pragma unroll
-      for (int o = 1; o < 8; o <<= 1)
-        for (int r = 0; r < 3; ++r) {
-          lo[r] = fmin(lo[r], __shfl_xor_sync(full, lo[r], o));
-          hi[r] = fmax(hi[r], __shfl_xor_sync(full, hi[r], o));
-        }
-      const unsigned real = __ballot_sync(full, a >= 0);
-      if ((lane & 7) == 0) {
-        const int cg = 8 * sc + (lane >> 3) + 4 * h;
-        for (int r = 0; r < 3; ++r) b.cl_box[6 * cg + r] = lo[r], b.cl_box[6 * cg + 3 + r] = hi[r];
-        b.cl_real[cg] = (unsigned char)((real >> (lane & 24)) & 255u);
-      }
-      for (int r = 0; r < 3; ++r) slo[r] = fmin(slo[r], lo[r]), shi[r] = fmax(shi[r], hi[r]);
-    }
-#pragma unroll
-    for (int o = 8; o < 32; o <<= 1)
-      for (int r = 0; r < 3; ++r) {
-        slo[r] = fmin(slo[r], __shfl_xor_sync(full, slo[r], o));
-        shi[r] = fmax(shi[r], __shfl_xor_sync(full, shi[r], o));
-      }
-    const int last = m - 1;
-    const int id_first = __shfl_sync(full, id[0], 0);
-    const int id_last = __shfl_sync(full, (last >> 5) ? id[1] : id[0], last & 31);
-    if (lane == 0) {
-      for (int r = 0; r < 3; ++r) b.sc_org[3 * sc + r] = 0.5 * (slo[r] + shi[r]);
-      b.sc_z[2 * sc] = b.frac[3 * id_first + 2];
-      b.sc_z[2 * sc + 1] = b.frac[3 * id_last + 2];
-    }
-    __syncwarp();
-  }
-}
 
 // ---------------------------------------------------------------------------------------------------------------
 constexpr int kSearchWarps = 8;       // warps per super-cluster in the search

@@ -149,12 +149,12 @@ int Engine::counter(int slot) {
 // ---------------------------------------------------------------------------------------------------------------
 void Engine::launch_build(const double* d_x) {
   const ListGeom& g = geom_;
-  launch_k(k_bin, blocks_for(size_t(n_), 256), 256, 0, stream_, n_, d_x, dcell_, g, lb_);
-  launch_k(k_scan_columns, 1, 1024, 0, stream_, g, lb_);
+  // binning (its last block scans the columns), the scatter into columns, and the sort of each column (its block then
+  // forms the column's super-clusters): three launches before the search
+  launch_k(k_bin, blocks_for(size_t(n_), kBinThreads), kBinThreads, 0, stream_, n_, d_x, dcell_, g, lb_);
   launch_k(k_scatter, blocks_for(size_t(n_), 256), 256, 0, stream_, n_, lb_);
   const size_t sort_smem = size_t(kSortMax) * (sizeof(double) + sizeof(int));
-  launch_k(k_sort_columns, std::min(g.ncol, dev_sms_ * 8), 1024, sort_smem, stream_, g, lb_);
-  launch_k(k_superclusters, std::max(1, std::min(blocks_for(size_t(nsc_cap_), 4), dev_sms_ * 16)), 128, 0, stream_, dcell_, lb_);
+  launch_k(k_sort_columns, std::min(g.ncol, dev_sms_ * 8), kSortThreads, sort_smem, stream_, dcell_, g, lb_);
   if (sizeof(SearchShared) > 48 * 1024) CK(cudaFuncSetAttribute(k_search, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(SearchShared))));
   launch_k(k_search, std::max(1, std::min(nsc_cap_, dev_sms_ * 8)), 32 * kSearchWarps, sizeof(SearchShared), stream_, dcell_, g, d_excl_off_.p,
                                                                                                           d_excl_list_.p, lb_);
@@ -203,6 +203,13 @@ PairArgs Engine::pair_args() {
   A.err = d_counters_.p + kCntErr;
   return A;
 }
+
+ListCheck Engine::list_check(int nfree, const int* free_atoms) const {
+  const double b = std::min(0.8, skin_);   // the prune margin (see prune())
+  return ListCheck{d_x0_.p, d_xp_.p, 0.25 * skin_ * skin_, 0.25 * b * b, d_counters_.p, nfree, free_atoms};
+}
+
+bool Engine::list_check_fusable() const { return (opt_.parts & 2) != 0 && list_valid_ && !frozen_; }
 
 // Dynamic pruning: when an atom has moved b/2 since the last prune (b = min(0.8 Å, skin), as field.cpp:1306-1312; the
 // step's check kernel tests it), or a build set the flag, every entry's masks are rewritten for r_c + b.
@@ -375,9 +382,7 @@ void Engine::forces(const double* d_x, bool ener, bool vir, bool check_rebuild, 
       launch_k(k_set_flag, 1, 1, 0, stream_, d_counters_.p, kCntRebuild, 1);
       list_valid_ = true;
     } else if (check_rebuild) {
-      const double b = std::min(0.8, skin_);   // the prune margin (see prune())
-      launch_k(k_check_step, blocks_for(size_t(n_), 256), 256, 0, stream_, n_, d_x, d_x0_.p, 0.25 * skin_ * skin_, d_xp_.p, 0.25 * b * b,
-               d_counters_.p);
+      launch_k(k_check_step, blocks_for(size_t(n_), 256), 256, 0, stream_, n_, d_x, list_check(0, nullptr));
     }
     if (!frozen_) launch_build(d_x);
     const size_t ns = size_t(nsc_cap_) * kScAtoms;
