@@ -123,14 +123,15 @@ Engine::Engine(const caps_gpu_ff* ff, const caps_gpu_opts* o) {
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&dev_sms_, cudaDevAttrMultiProcessorCount, dev));
   CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-  // the main stream (integrator, displacement check, list, pack, prune, pair kernel) runs at the highest priority and
-  // the side streams (bonded terms, PME) at the lowest: the chain that leads to the pair kernel takes SM slots first,
-  // the side branches fill what it leaves
+  // the main stream (integrator, list, pack, prune, pair kernel) runs at the highest priority, PME's chain of dependent
+  // launches one level below and the bonded terms at the lowest: the chain that leads to the pair kernel takes SM
+  // slots first, then PME's, and the bonded blocks fill what they leave
   int prio_lo = 0, prio_hi = 0;
   CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
   CK(cudaStreamDestroy(stream_));
   CK(cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, prio_hi));
-  for (auto& st : side_) CK(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio_lo));
+  CK(cudaStreamCreateWithPriority(&side_[0], cudaStreamNonBlocking, prio_lo));
+  CK(cudaStreamCreateWithPriority(&side_[1], cudaStreamNonBlocking, prio_hi < prio_lo ? prio_hi + 1 : prio_lo));
   CK(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
   for (auto& ev : ev_join_) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   CK(cudaMallocHost(&h_counters_, sizeof(int) * kCntNum));

@@ -888,10 +888,12 @@ struct Stepper {
   std::unique_ptr<HostRng> rng;
   double* h_sc = nullptr;
   Chain* h_chain = nullptr;
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};   // the captured plain step and thermo step (energies and virial on)
-  std::string graph_key[2];                          // what each was captured with (capture_key)
-  bool graph_valid[2] = {false, false};
-  int graph_kernels[2] = {0, 0};
+  // the captured plain step, thermo step (energies and virial on) and a block of kBlockSteps plain steps
+  static constexpr int kBlockSteps = 8;
+  cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
+  std::string graph_key[3];                          // what each was captured with (capture_key)
+  bool graph_valid[3] = {false, false, false};
+  int graph_kernels[3] = {0, 0, 0};
   int nparts = 0;
   // kept between runs: host velocities, the copies for step 0's trial step, the masses, the constraint set and what it
   // was built from, the run's timing events
@@ -1147,7 +1149,7 @@ struct Stepper {
 
   // The captured steps no longer match the run (new thermostat draws, a rescaled cell): the next launch captures again
   // and updates the instantiated graph in place.
-  void drop_graphs() { graph_valid[0] = graph_valid[1] = false; }
+  void drop_graphs() { graph_valid[0] = graph_valid[1] = graph_valid[2] = false; }
 
   // Everything a capture of step() records besides the kernels themselves: the engine's capture state and this run's
   // scalars and buffers. Equal keys give equal graphs.
@@ -1175,15 +1177,22 @@ struct Stepper {
     CK(cudaGraphLaunch(graph[k], E.stream_));
     return graph_kernels[k];
   }
-  // Captures (or updates) the plain or thermo step graph when the run's key differs from the one it was made with.
-  void ensure_graph(bool thermo) {
-    const int k = thermo ? 1 : 0;
-    std::string key = capture_key(thermo);
+  // Replays kBlockSteps plain steps as one graph (no launch gap between them); returns its kernel count.
+  int launch_block() {
+    ensure_graph(false, true);
+    CK(cudaGraphLaunch(graph[2], E.stream_));
+    return graph_kernels[2];
+  }
+  // Captures (or updates) the plain or thermo step graph, or the block of plain steps, when the run's key differs from
+  // the one it was made with.
+  void ensure_graph(bool thermo, bool block = false) {
+    const int k = block ? 2 : thermo ? 1 : 0;
+    std::string key = capture_key(thermo) + (block ? "B" : "");
     if (!graph[k] || !graph_valid[k] || key != graph_key[k]) {
       cudaGraph_t g;
       CK(cudaStreamBeginCapture(E.stream_, cudaStreamCaptureModeThreadLocal));
       try {
-        step(thermo, thermo);
+        for (int i = 0; i < (block ? kBlockSteps : 1); ++i) step(thermo, thermo);
       } catch (...) {   // leave no capture open behind an error
         cudaGraph_t junk = nullptr;
         (void)cudaStreamEndCapture(E.stream_, &junk);
@@ -1212,7 +1221,7 @@ struct Stepper {
       if (!updated) CK(cudaGraphInstantiate(&graph[k], g, cudaGraphInstantiateFlagUseNodePriority));
       CK(cudaGraphDestroy(g));
       // the capture state is read after the capture: step() may have changed host flags it holds
-      graph_key[k] = capture_key(thermo);
+      graph_key[k] = capture_key(thermo) + (block ? "B" : "");
       graph_valid[k] = graph_key[k] == key;
     }
   }
@@ -1632,6 +1641,13 @@ struct MdRun {
   void start();
   // step s; stop: a stop was asked for before it (and s < steps), so the run ends after it
   void advance(long long s, bool stop = false);
+  // steps s .. s + kBlockSteps - 1 are plain steps (no row, frame, checkpoint, cell rescaling or thermostat refill)
+  bool block_due(long long s) const {
+    if (s + Stepper::kBlockSteps - 1 >= o.steps) return false;
+    for (long long t = s; t < s + Stepper::kBlockSteps; ++t)
+      if (special(t)) return false;
+    return true;
+  }
   void baro_step(long long s);
 };
 
@@ -1905,10 +1921,18 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
   if (o.steps > 0 && !R.baro_due(1) && !R.refill_due(1)) {
     S.ensure_graph(false);
     S.ensure_graph(true);
+    if (!timed && o.steps > Stepper::kBlockSteps) S.ensure_graph(false, true);
   }
   const auto w0 = std::chrono::steady_clock::now();
   CK(cudaEventRecord(ev0, stream_));
   for (long long s = 1; s <= o.steps; ++s) {
+    // outside measurement mode, runs of plain steps go as blocks of kBlockSteps (a stop asked for from another thread
+    // takes effect at the end of a block)
+    if (!timed && g_stop.load(std::memory_order_relaxed) == 0 && R.block_due(s)) {
+      R.kernels += S.launch_block();
+      s += Stepper::kBlockSteps - 1;
+      continue;
+    }
     if (timed) {
       if (timing_flush_ > 0) CK(cudaMemsetAsync(d_flush_.p, int(s & 255), size_t(timing_flush_), stream_));
       CK(cudaEventRecord(tev[size_t(2 * (s - 1))], stream_));
