@@ -356,9 +356,11 @@ def step_timeline(args) -> dict:
         ev.pin_tuning([int(t) for t in args.tuning.split(",")])
     out = ev.run(x, cell, o, v=v)
     ev.run(out["x"], cell, options("mixed", 50, 7), v=out["v"])
+    b0, p0 = ev.list_counts()
     with profile(activities=[ProfilerActivity.CUDA]) as prof:
         ev.run(out["x"], cell, options("mixed", args.profile_timeline, 7), v=out["v"])
         torch.cuda.synchronize()
+    b1, p1 = ev.list_counts()
     tuning = ev.tuning()
     ev.close()
     with tempfile.NamedTemporaryFile(suffix=".json") as tf:
@@ -375,10 +377,12 @@ def step_timeline(args) -> dict:
             r["start"].append(e["ts"] - starts[i])
             r["dur"].append(e["dur"])
     period = [b - a for a, b in zip(starts, starts[1:])]
-    kern = sorted(({"kernel": k, "start_us": statistics.median(r["start"]), "us": statistics.median(r["dur"]), "count": len(r["dur"])}
-                   for k, r in rows.items()), key=lambda d: d["start_us"])
+    # median start and duration, and the mean duration (gated kernels that did their work on some steps: the list
+    # build, the prune)
+    kern = sorted(({"kernel": k, "start_us": statistics.median(r["start"]), "us": statistics.median(r["dur"]),
+                    "mean_us": statistics.fmean(r["dur"]), "count": len(r["dur"])} for k, r in rows.items()), key=lambda d: d["start_us"])
     return {"timeline_steps": len(period), "step_period_us": statistics.median(period) if period else None,
-            "tuning": ",".join(map(str, tuning)), "kernels": kern}
+            "tuning": ",".join(map(str, tuning)), "list_builds": b1 - b0, "prunes": p1 - p0, "kernels": kern}
 
 
 def run_reference(args, rank: int) -> dict:

@@ -90,7 +90,7 @@ FRAME_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_i
 CHECKPOINT_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int64, C.c_void_p)
 
 DIAG_EXPORTS = ["caps_gpu_diag_set_timing", "caps_gpu_diag_last_step_ms", "caps_gpu_diag_pair_timing", "caps_gpu_diag_step_kernels",
-                "caps_gpu_diag_kernels_run", "caps_gpu_diag_phase_timing", "caps_gpu_diag_get_tuning", "caps_gpu_diag_set_tuning"]
+                "caps_gpu_diag_kernels_run", "caps_gpu_diag_list_counts", "caps_gpu_diag_phase_timing", "caps_gpu_diag_get_tuning", "caps_gpu_diag_set_tuning"]
 
 EXPORTS = [
     "caps_gpu_abi_version", "caps_gpu_device_count", "caps_gpu_create", "caps_gpu_set_options", "caps_gpu_energies",
@@ -153,6 +153,8 @@ def load(path: Path | None = None) -> C.CDLL:
     lib.caps_gpu_diag_step_kernels.argtypes = [C.c_void_p]
     lib.caps_gpu_diag_kernels_run.restype = C.c_int64
     lib.caps_gpu_diag_kernels_run.argtypes = [C.c_void_p]
+    lib.caps_gpu_diag_list_counts.restype = C.c_int32
+    lib.caps_gpu_diag_list_counts.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
     lib.caps_gpu_diag_pair_timing.argtypes = [C.c_void_p, P, P, C.c_int32, C.c_int64, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                               C.POINTER(C.c_double), C.POINTER(C.c_double)]
     lib.caps_gpu_diag_phase_timing.argtypes = [C.c_void_p, P, P, C.c_int32, C.c_int64, P]

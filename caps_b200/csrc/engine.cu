@@ -937,6 +937,12 @@ double caps_gpu_diag_last_step_ms(const caps_gpu_engine* e) { return e ? e->e->l
 
 int32_t caps_gpu_diag_step_kernels(const caps_gpu_engine* e) { return e ? e->e->graph_kernels() : 0; }
 int64_t caps_gpu_diag_kernels_run(const caps_gpu_engine* e) { return e ? e->e->kernels_run() : 0; }
+int32_t caps_gpu_diag_list_counts(caps_gpu_engine* e, int64_t* v) {
+  if (!e || !v) return CAPS_GPU_EINVAL;
+  return guard(e, [&] {
+    e->e->list_counts(v);
+  });
+}
 
 int32_t caps_gpu_diag_pair_timing(caps_gpu_engine* e, const double* x, const double* cell, int32_t launches, int64_t flush_bytes, double* avg_ms,
                                   double* pairs_in, double* pairs_listed, double* entries) {

@@ -135,6 +135,7 @@ class Engine {
   void compute_host(const double* x, const double* cell, double* f, caps_gpu_terms* out);
   void compute_dev(const double* d_x, const double* cell, double* d_f, caps_gpu_terms* out);
   int list_builds();   // list builds so far (counted on the device)
+  void list_counts(int64_t* v);   // v[0] list builds, v[1] dynamic prunes so far
   // Evaluator::freeze_pairs / unfreeze (field.hpp:341-347): later evaluations take exactly the pairs inside the cut-off
   // at (x, cell), on the FP64 path, and never rebuild the list
   void freeze_pairs(const double* x, const double* cell);

@@ -138,6 +138,10 @@ void Engine::tune_batch(const double* d_x) {
 }
 
 int Engine::list_builds() { return counter(kCntBuilds); }
+void Engine::list_counts(int64_t* v) {
+  v[0] = counter(kCntBuilds);
+  v[1] = counter(kCntPrunes);
+}
 
 int Engine::counter(int slot) {
   int v = 0;
@@ -212,7 +216,7 @@ ListCheck Engine::list_check(int nfree, const int* free_atoms) const {
 bool Engine::list_check_fusable() const { return (opt_.parts & 2) != 0 && list_valid_ && !frozen_; }
 
 // Dynamic pruning: when an atom has moved b/2 since the last prune (b = min(0.8 Å, skin), as field.cpp:1306-1312; the
-// step's check kernel tests it), or a build set the flag, every entry's masks are rewritten for r_c + b.
+// step's displacement check tests it), or a build set the flag, every entry's masks are rewritten for r_c + b.
 void Engine::prune(const double* d_x) {
   const double b = std::min(0.8, skin_);
   const PairArgs A = pair_args();

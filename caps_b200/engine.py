@@ -294,6 +294,12 @@ class Evaluator:
         """Kernels the last run launched in its step loop (graph kernel nodes replayed, thermo-row kernels)."""
         return int(self.lib.caps_gpu_diag_kernels_run(self.h))
 
+    def list_counts(self) -> tuple[int, int]:
+        """List builds and dynamic prunes so far (counted on the device)."""
+        v = (C.c_int64 * 2)()
+        self._check(self.lib.caps_gpu_diag_list_counts(self.h, v))
+        return int(v[0]), int(v[1])
+
     def pair_timing(self, x, cell, launches: int = 50, flush_bytes: int = 0) -> dict:
         """The pair kernel alone: mean launch time and the pairs it evaluates (include/caps_gpu_diag.h)."""
         x = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1))

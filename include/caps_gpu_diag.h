@@ -28,6 +28,8 @@ int32_t caps_gpu_diag_step_kernels(const caps_gpu_engine* e);
 /* Kernels the last caps_gpu_run launched in its step loop: per step the kernel nodes of the step graph it replayed, plus
  * the kinetic-energy kernel of each thermo row; a barostat step (run outside a graph) counts as one thermo step. */
 int64_t caps_gpu_diag_kernels_run(const caps_gpu_engine* e);
+/* List builds and dynamic prunes the engine has run so far (counted on the device; v[0] builds, v[1] prunes). */
+int32_t caps_gpu_diag_list_counts(caps_gpu_engine* e, int64_t* v);
 /* Times the non-bonded pair kernel alone: one force evaluation at x (host, 3N) builds the list, then `launches`
  * launches of the pair kernel (forces only, its full persistent grid), each bracketed by CUDA events, an L2 flush of
  * flush_bytes before each.
