@@ -131,7 +131,7 @@ def options(precision: str, steps: int, seed: int, thermostat: str = "nose-hoove
                            thermo_every=thermo_every or max(steps, 1), energy=eo)
 
 
-E2E_CALLS = 3
+E2E_CALLS = 5
 
 
 def force_errors(f, f_ref, e, e_ref) -> dict:

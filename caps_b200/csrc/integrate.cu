@@ -888,6 +888,17 @@ struct Stepper {
   std::unique_ptr<HostRng> rng;
   double* h_sc = nullptr;
   Chain* h_chain = nullptr;
+  double* h_xv = nullptr;   // pinned staging for a run's positions and velocities in and out (2 x 3N)
+  size_t h_xv_n = 0;
+  double* pinned_xv(size_t n3) {
+    if (h_xv_n < n3) {
+      if (h_xv) CK(cudaFreeHost(h_xv));
+      h_xv = nullptr;
+      CK(cudaMallocHost(&h_xv, 2 * n3 * sizeof(double)));
+      h_xv_n = n3;
+    }
+    return h_xv;
+  }
   // the captured plain step, thermo step (energies and virial on) and a block of kBlockSteps plain steps
   static constexpr int kBlockSteps = 8;
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
@@ -916,6 +927,7 @@ struct Stepper {
     for (auto& g : graph)
       if (g) cudaGraphExecDestroy(g);
     if (h_sc) cudaFreeHost(h_sc);
+    if (h_xv) cudaFreeHost(h_xv);
     if (h_chain) cudaFreeHost(h_chain);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -1656,7 +1668,12 @@ void MdRun::start() {
   Engine& e = E;
   const int n_ = E.n_;
   e.set_cell(st->cell);
-  S.x.upload(st->x, n3, stream_);
+  {   // through pinned staging: the copy runs at the link's rate and returns at once
+    double* px = S.pinned_xv(n3);
+    std::memcpy(px, st->x, n3 * sizeof(double));
+    S.x.alloc(n3);
+    CK(cudaMemcpyAsync(S.x.p, px, n3 * sizeof(double), cudaMemcpyHostToDevice, stream_));
+  }
   S.x0.alloc(n3);
   S.v.alloc(n3);
   {
@@ -1752,7 +1769,13 @@ void MdRun::start() {
     for (int i = 0; i < n_; ++i)
       for (int k = 0; k < 3; ++k) hv[3 * size_t(i) + k] -= p[k] / mf;
   }
-  S.v.upload(hv, stream_);
+  auto upload_v = [&] {   // through the pinned staging (the copy before it has completed: the stream was synchronised)
+    double* pv = S.pinned_xv(n3) + n3;
+    std::memcpy(pv, hv.data(), n3 * sizeof(double));
+    S.v.alloc(n3);
+    CK(cudaMemcpyAsync(S.v.p, pv, n3 * sizeof(double), cudaMemcpyHostToDevice, stream_));
+  };
+  upload_v();
   if (drawn) {
     if (S.ncons) S.rattle(0);
     CK(cudaMemcpyAsync(hv.data(), S.v.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
@@ -1760,7 +1783,7 @@ void MdRun::start() {
     const double t0 = 2 * host_ke(hv) / (S.ndof * kB);
     if (t0 > 0)
       for (auto& q : hv) q *= std::sqrt(o.temperature / t0);
-    S.v.upload(hv, stream_);
+    upload_v();
   }
   if (S.ncons) S.rattle(0);
   if (S.bussi) S.make_draws(1, draw_chunk(1));
@@ -1969,10 +1992,13 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
   const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
   R.sync_scalars();
   last_sps_ = done > 0 && ms > 0 ? double(done) / (ms * 1e-3) : 0.0;
-  // state back to the caller
-  CK(cudaMemcpyAsync(st->x, S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
-  if (st->v) CK(cudaMemcpyAsync(st->v, S.v.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  // state back to the caller, through the pinned staging
+  double* px = S.pinned_xv(n3);
+  CK(cudaMemcpyAsync(px, S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  if (st->v) CK(cudaMemcpyAsync(px + n3, S.v.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
   CK(cudaStreamSynchronize(stream_));
+  std::memcpy(st->x, px, n3 * sizeof(double));
+  if (st->v) std::memcpy(st->v, px + n3, n3 * sizeof(double));
   std::memcpy(st->cell, cell_h_, sizeof cell_h_);
   if (report) {
     char b[512];
