@@ -33,7 +33,7 @@ sys.path.insert(0, str(ROOT))
 REF_SECONDS = 60.0           # bound on the reference arm's timed sample (CPU)
 CPU_SAMPLE_SECONDS = 15.0    # bound on the cpu_baseline sample beside the GPU run
 # DRAM bytes (read + write) of one k_pair_f32 launch on this workload, from an ncu capture of that kernel (cold L2)
-PAIR_DRAM_BYTES = 10.83e6
+PAIR_DRAM_BYTES = 10.94e6
 # FP32 flops of one interacting pair on a force-only step, FMA as 2: separation, r^2 and its inverse powers 11 (the
 # reciprocal square root not counted), LJ 12-6 6, the Ewald real-space term through its rational fit 33, force
 # components and their sums 9
