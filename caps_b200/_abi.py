@@ -63,6 +63,8 @@ class MdOpts(C.Structure):
         ("checkpoint_every", C.c_int64), ("checkpoint", C.c_void_p), ("checkpoint_user", C.c_void_p),
         ("hmr", C.c_double), ("anisotropic", C.c_int32), ("couple_axes", C.c_int32), ("axis_pressure_set", C.c_int32),
         ("axis_pressure", C.c_double * 3),
+        # ABI 5
+        ("constraint_algorithm", C.c_int32),
     ]
 
 

@@ -34,6 +34,8 @@ enum ErrorBits : unsigned {
   kErrImageRange = 1u << 9,       // an image shift outside +-63 cells
   kErrFixRange = 1u << 10,        // a force or energy outside the fixed-point range (overlapping atoms: push off first)
   kErrRattle = 1u << 11,          // RATTLE (the velocity constraints) did not converge
+  kErrLincs = 1u << 12,           // LINCS's rotational corrections did not converge
+  kErrConsOverlap = 1u << 13,     // two constrained atoms on each other (LINCS takes their direction)
 };
 
 // What the first failure of a kind leaves for the host's message (the engine's error-detail array, doubles): the

@@ -607,10 +607,14 @@ void Engine::check_errors() {
   if (e & kErrExclOverflow) throw ModelError(CAPS_GPU_EINVAL, "too many excluded partners in one super-cluster for the device list");
   if (e & kErrImageRange) throw ModelError(CAPS_GPU_EFIELD, "an excluded pair is more than 63 cells apart: unwrap the molecules first");
   // the reference's texts (constraints.cpp:219, 227, 259)
+  if (e & kErrConsOverlap) throw ModelError(CAPS_GPU_ECONSTRAINT, "two constrained atoms sit on each other");
   if (e & (kErrShake | kErrShakeTurn))
     throw ModelError(CAPS_GPU_ECONSTRAINT, (e & kErrShakeTurn) ? "a constrained bond turned by more than 90° in one step; lower the time step or relax first"
                                                                  : "the bond constraints did not converge (SHAKE); lower the time step or relax first");
   if (e & kErrRattle) throw ModelError(CAPS_GPU_ECONSTRAINT, "the bond constraints did not converge (RATTLE); lower the time step");
+  // constraints.cpp:131, 182
+  if (e & kErrConsOverlap) throw ModelError(CAPS_GPU_ECONSTRAINT, "two constrained atoms sit on each other");
+  if (e & kErrLincs) throw ModelError(CAPS_GPU_ECONSTRAINT, "the bond constraints did not converge (LINCS); lower the time step or relax first");
   if (e & kErrFixRange)
     throw ModelError(CAPS_GPU_EFIELD, "a force beyond the fixed-point range (2e9 kcal/mol/Å): overlapping atoms; push the structure off first (FP64 with a force cap)");
   if (e & kErrNonFinite)   // the reference's text (dynamics.cpp:757), with the step whose positions were not finite

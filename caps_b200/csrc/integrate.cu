@@ -176,7 +176,16 @@ struct ConsArgs {
   const double* d2;        // squared lengths
   const double* invm;      // per atom
   DevCell cell;
+  // LINCS (every cluster in the general layout): the constraints' lengths, and per cluster its couplings, pairs of its
+  // constraints (local indices) that share an atom with the coefficient -S_k S_l s_ka s_la / m_a, in the reference's
+  // order (atoms ascending, then the constraints on each)
+  int lincs;
+  const double* dlen;
+  const int* cp_start;     // general clusters + 1
+  const int2* cp;
+  const double* cpc;
 };
+constexpr int kMaxCouple = 56;   // couplings of a cluster of 8 constraints
 
 // SHAKE on a star cluster with NK constraints, in registers. The same Gauss-Seidel sweep as the general kernel, with each
 // constraint taken as (centre, partner).
@@ -322,6 +331,99 @@ __device__ void settle_water(const ConsArgs& C, int w, double* __restrict__ x, c
   }
 }
 
+// LINCS on general cluster c (core/src/constraints.cpp:125-185, Hess 1997, order 4): from the old directions B_k, one
+// projection of the separations onto the constraint lengths through the expansion (I - A)^-1 = sum_{n<=4} A^n, then the
+// rotational corrections (the projection along B_k aimed at sqrt(d^2 - perp^2)) until every length holds to tol; then
+// v += (x - x_before) / h when h > 0. The reference couples all constraints that share an atom; those of different
+// clusters share none, so each cluster is solved alone (its iterations stop when its own lengths hold).
+__device__ void lincs_cluster(const ConsArgs& C, int c, double* __restrict__ x, const double* __restrict__ x0, double* __restrict__ v, double h,
+                              int* counters) {
+  const int k0 = C.cl_start[c], k1 = C.cl_start[c + 1], a0 = C.cl_atom0[c], a1 = C.cl_atom0[c + 1];
+  const int q0 = C.cp_start[c], nq = C.cp_start[c + 1] - q0;
+  const int na = a1 - a0, nk = k1 - k0;
+  double px[kMaxClAtoms][3], ox[kMaxClAtoms][3], bx[kMaxClAtoms][3], im[kMaxClAtoms];
+  for (int a = 0; a < na; ++a) {
+    const int g = C.cl_atoms[a0 + a];
+    for (int r = 0; r < 3; ++r) px[a][r] = x[3 * g + r], ox[a][r] = x0[3 * g + r], bx[a][r] = px[a][r];
+    im[a] = C.invm[g];
+  }
+  double ref[kMaxClCons][3], B[kMaxClCons][3], S[kMaxClCons], dl[kMaxClCons];
+  int li[kMaxClCons], lj[kMaxClCons];
+  for (int k = 0; k < nk; ++k) {
+    const int4 q = C.cons[k0 + k];
+    li[k] = q.x, lj[k] = q.y;
+    dl[k] = C.dlen[k0 + k];
+    double d0 = ox[q.x][0] - ox[q.y][0], d1 = ox[q.x][1] - ox[q.y][1], d2v = ox[q.x][2] - ox[q.y][2];
+    min_image(C.cell, d0, d1, d2v);
+    ref[k][0] = d0, ref[k][1] = d1, ref[k][2] = d2v;
+    const double l = sqrt(d0 * d0 + d1 * d1 + d2v * d2v);
+    if (l < 1e-12) {
+      atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), kErrConsOverlap);
+      return;
+    }
+    const double il = 1 / l;
+    for (int r = 0; r < 3; ++r) B[k][r] = ref[k][r] * il;
+    S[k] = 1.0 / sqrt(im[q.x] + im[q.y]);
+  }
+  double akl[kMaxCouple];
+  int ck[kMaxCouple], cl[kMaxCouple];
+  for (int q = 0; q < nq; ++q) {
+    const int2 p = C.cp[q0 + q];
+    ck[q] = p.x, cl[q] = p.y;
+    akl[q] = C.cpc[q0 + q] * (B[p.x][0] * B[p.y][0] + B[p.x][1] * B[p.y][1] + B[p.x][2] * B[p.y][2]);
+  }
+  auto sep = [&](int k, double s[3]) {
+    for (int r = 0; r < 3; ++r) s[r] = ref[k][r] + (px[li[k]][r] - ox[li[k]][r]) - (px[lj[k]][r] - ox[lj[k]][r]);
+  };
+  double rhs[kMaxClCons], sol[kMaxClCons], t[kMaxClCons], t2[kMaxClCons];
+  auto solve_apply = [&]() {
+    for (int k = 0; k < nk; ++k) sol[k] = rhs[k], t[k] = rhs[k];
+    for (int order = 0; order < 4; ++order) {
+      for (int k = 0; k < nk; ++k) t2[k] = 0.0;
+      for (int q = 0; q < nq; ++q) t2[ck[q]] += akl[q] * t[cl[q]];
+      for (int k = 0; k < nk; ++k) sol[k] += t2[k], t[k] = t2[k];
+    }
+    for (int k = 0; k < nk; ++k) {
+      const double g = S[k] * sol[k];
+      for (int r = 0; r < 3; ++r) {
+        px[li[k]][r] -= im[li[k]] * g * B[k][r];
+        px[lj[k]][r] += im[lj[k]] * g * B[k][r];
+      }
+    }
+  };
+  for (int k = 0; k < nk; ++k) {
+    double s[3];
+    sep(k, s);
+    rhs[k] = S[k] * ((B[k][0] * s[0] + B[k][1] * s[1] + B[k][2] * s[2]) - dl[k]);
+  }
+  solve_apply();
+  bool done = false;
+  for (int it = 0; it < kShakeIter && !done; ++it) {
+    done = true;
+    for (int k = 0; k < nk; ++k) {
+      double s[3];
+      sep(k, s);
+      const double d = dl[k], l2 = s[0] * s[0] + s[1] * s[1] + s[2] * s[2], along = B[k][0] * s[0] + B[k][1] * s[1] + B[k][2] * s[2];
+      if (fabs(d * d - l2) > 2 * kShakeTol * d * d) done = false;
+      if (along < 0) {
+        atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), kErrShakeTurn);
+        return;
+      }
+      const double perp2 = fmax(0.0, l2 - along * along);
+      rhs[k] = S[k] * (along - sqrt(fmax(0.0, d * d - perp2)));
+    }
+    if (!done) solve_apply();
+  }
+  if (!done) atomicOr(reinterpret_cast<unsigned*>(counters + kCntErr), kErrLincs);
+  for (int a = 0; a < na; ++a) {
+    const int g = C.cl_atoms[a0 + a];
+    for (int r = 0; r < 3; ++r) {
+      x[3 * g + r] = px[a][r];
+      if (h > 0) v[3 * g + r] += (px[a][r] - bx[a][r]) / h;
+    }
+  }
+}
+
 // SHAKE on each cluster (Gauss-Seidel along the reference vectors, tol 1e-8 relative; core/src/constraints.cpp:196-230),
 // then v += (x - x_before) / h when h > 0.
 __device__ void shake_cluster(const ConsArgs& C, int cc, double* __restrict__ x, const double* __restrict__ x0, double* __restrict__ v, double h,
@@ -398,6 +500,20 @@ __device__ void check_cluster(const ConsArgs& C, const ListCheck& L, int cc, con
     const int c = cc - C.e4;
     for (int a = C.cl_atom0[c]; a < C.cl_atom0[c + 1]; ++a) list_check_atom(L, C.cl_atoms[a], x, mb, mp);
   }
+}
+
+// LINCS, a thread per cluster (every cluster in the general layout), with the displacement check as k_shake has it.
+__global__ void k_lincs(ConsArgs C, double* __restrict__ x, const double* __restrict__ x0, double* __restrict__ v, double h, int* counters,
+                        ListCheck L) {
+  const int cc = blockIdx.x * blockDim.x + threadIdx.x;
+  bool mb = false, mp = false;
+  if (cc < C.ncl) {
+    lincs_cluster(C, cc, x, x0, v, h, counters);
+    if (L.xb) check_cluster(C, L, cc, x, mb, mp);
+  } else if (L.xb && cc < C.ncl + L.nfree) {
+    list_check_atom(L, L.free_atoms[cc - C.ncl], x, mb, mp);
+  }
+  if (L.xb) list_check_flags(L, mb, mp);
 }
 
 // SHAKE, a thread per cluster; with L.xb set, the displacement check of the step's final positions on the clusters'
@@ -877,7 +993,10 @@ struct Stepper {
   DevBuf<int4> cons, star, water;
   DevBuf<double4> star_d2;
   DevBuf<double2> water_g;
-  DevBuf<double> d2;
+  DevBuf<double> d2, dlen, cpc;   // LINCS: lengths, coupling coefficients
+  DevBuf<int> cp_start;
+  DevBuf<int2> cp;
+  int cons_alg = -1;
   DevBuf<double2> draws;
   long long draws_first = 0, draws_count = 0;
   ConsArgs C{};
@@ -942,8 +1061,12 @@ struct Stepper {
     if (o.constraints && o.is_oxygen) oflags.assign(o.is_oxygen, o.is_oxygen + n);
     // the set depends on the options, the element flags and the force field; on the positions only where a bond has no
     // usable r0 or a water no angle
-    if (cons_built && !cons_from_positions && cons_flag == o.constraints && hflags == cons_h && oflags == cons_o) return;
+    if (cons_built && !cons_from_positions && cons_flag == o.constraints && cons_alg == o.constraint_algorithm && hflags == cons_h &&
+        oflags == cons_o)
+      return;
     cons_built = false;
+    cons_alg = o.constraint_algorithm;
+    const bool lincs = o.constraint_algorithm == 1;   // every cluster in the general layout, solved by LINCS
     cons_from_positions = false;
     ncons = 0;
     nfree = 0;
@@ -1019,15 +1142,18 @@ struct Stepper {
     for (int k = 0; k < ncons; ++k) comp_cons[find(cs[size_t(k)].i)].push_back(k);
     std::vector<int> st{0}, a0{0}, atoms, gen_atoms;   // atoms: every constrained atom; gen_atoms: the general clusters
     std::vector<int4> cv;
-    std::vector<double> dv;
+    std::vector<double> dv, dlv, cpcv;
+    std::vector<int> cps{0};
+    std::vector<int2> cpv;
     std::vector<int4> star_at[3], water_at;
     std::vector<double4> star_dd[3];
     std::vector<double2> water_geo;
-    for (auto& [r, ks] : comp_cons) {
+    for (auto& comp : comp_cons) {
+      const std::vector<int>& ks = comp.second;
       if (int(ks.size()) > kMaxClCons) throw ModelError(CAPS_GPU_EINVAL, "a constraint cluster has more than 8 atoms or constraints (the device SHAKE takes bonds to hydrogen and rigid waters)");
       // a star: 1-3 constraints that all share one atom, each with a distinct partner
       int centre = -1;
-      if (ks.size() <= 3) {
+      if (!lincs && ks.size() <= 3) {
         const Cn& c0 = cs[size_t(ks[0])];
         for (int cand : {c0.i, c0.j}) {
           bool all = true;
@@ -1061,7 +1187,7 @@ struct Stepper {
         star_dd[ks.size() - 1].push_back(make_double4(dd[0], dd[1], dd[2], 0.0));
         continue;
       }
-      if (ks.size() == 3) {
+      if (!lincs && ks.size() == 3) {
         // a rigid water: the atom shared by two equal constraints (O) and two partners of equal mass joined by the third
         const Cn& k0 = cs[size_t(ks[0])];
         const Cn& k1 = cs[size_t(ks[1])];
@@ -1094,6 +1220,34 @@ struct Stepper {
         const int li = local(c.i), lj = local(c.j);
         cv.push_back(make_int4(li, lj, c.i, c.j));
         dv.push_back(c.d * c.d);
+        dlv.push_back(c.d);
+      }
+      if (lincs) {
+        // the couplings in the reference's order (constraints.cpp:110-119): atoms ascending, then each pair (k, l), k != l,
+        // of the constraints on the atom in constraint order; S_k = 1 / sqrt(1/m_i + 1/m_j)
+        auto inv = [&](int a) { return hm[size_t(a)] > 0 ? 1.0 / hm[size_t(a)] : 0.0; };
+        auto S = [&](int k) {
+          const Cn& c = cs[size_t(ks[size_t(k)])];
+          return 1.0 / std::sqrt(inv(c.i) + inv(c.j));
+        };
+        std::vector<int> sorted = loc;
+        std::sort(sorted.begin(), sorted.end());
+        for (int a : sorted) {
+          std::vector<int> on;
+          for (int k = 0; k < int(ks.size()); ++k) {
+            const Cn& c = cs[size_t(ks[size_t(k)])];
+            if (c.i == a || c.j == a) on.push_back(k);
+          }
+          for (int k : on)
+            for (int l : on) {
+              if (k == l) continue;
+              const double sk = cs[size_t(ks[size_t(k)])].i == a ? 1.0 : -1.0, sl = cs[size_t(ks[size_t(l)])].i == a ? 1.0 : -1.0;
+              cpv.push_back(make_int2(k, l));
+              cpcv.push_back(-S(k) * S(l) * sk * sl * inv(a));
+            }
+        }
+        if (int(cpv.size()) - cps.back() > kMaxCouple) throw ModelError(CAPS_GPU_EINVAL, "a constraint cluster couples more than 56 constraint pairs (LINCS)");
+        cps.push_back(int(cpv.size()));
       }
       if (int(loc.size()) > kMaxClAtoms)
         throw ModelError(CAPS_GPU_EINVAL, "a constraint cluster has more than 8 atoms or constraints (the device SHAKE takes bonds to hydrogen and rigid waters)");
@@ -1137,6 +1291,19 @@ struct Stepper {
       cl_atoms.upload(gen_atoms, E.stream_);
       cons.upload(cv, E.stream_);
       d2.upload(dv, E.stream_);
+    }
+    C.lincs = lincs ? 1 : 0;
+    if (lincs) {
+      dlen.upload(dlv, E.stream_);
+      cp_start.upload(cps, E.stream_);
+      if (!cpv.empty()) {
+        cp.upload(cpv, E.stream_);
+        cpc.upload(cpcv, E.stream_);
+      }
+      C.dlen = dlen.p;
+      C.cp_start = cp_start.p;
+      C.cp = cp.p;
+      C.cpc = cpc.p;
     }
     C.ncl = C.e4 + int(st.size()) - 1;
     C.cl_start = cl_start.p;
@@ -1274,7 +1441,7 @@ struct Stepper {
                E.mixed_ ? E.d_F_.p : nullptr, E.mixed_ ? nullptr : E.d_Fd_.p, E.d_errinfo_.p, step_ahead};
     const ListCheck L = check ? E.list_check(nfree, free_atoms.p) : ListCheck{};
     launch_k(k_kick_drift, blocks(size_t(n), 256), 256, 0, E.stream_, K, ncons ? ListCheck{} : L);
-    if (ncons) launch_k(k_shake, blocks(size_t(C.ncl) + (check ? size_t(nfree) : 0), 128), 128, 0, E.stream_, C, x.p, x0.p, v.p, hd, E.d_counters_.p, L);
+    if (ncons) launch_k(C.lincs ? k_lincs : k_shake, blocks(size_t(C.ncl) + (check ? size_t(nfree) : 0), 128), 128, 0, E.stream_, C, x.p, x0.p, v.p, hd, E.d_counters_.p, L);
     E.sums_cleared_ = true;
   }
   // whether this step's drift may take the list's displacement check (a plain step: not r-RESPA)
@@ -1439,6 +1606,7 @@ void Engine::validate_md(const caps_gpu_md_opts& o) const {
   if (o.barostat == 1 && o.thermostat == 0) throw ModelError(CAPS_GPU_EINVAL, "stochastic cell rescaling needs a thermostat");
   if (o.anisotropic && o.barostat == 1) throw ModelError(CAPS_GPU_EINVAL, "per-axis pressure coupling is available with the Berendsen barostat");
   if (o.hmr < 0 || !std::isfinite(o.hmr)) throw ModelError(CAPS_GPU_EINVAL, "the repartitioned hydrogen mass must be 0 (off) or positive");
+  if (o.constraint_algorithm != 0 && o.constraint_algorithm != 1) throw ModelError(CAPS_GPU_EINVAL, "unknown constraint algorithm (shake | lincs)");
 }
 
 // A stop asked for from outside (caps_gpu_request_stop): read once per step by the run loops.
@@ -1747,7 +1915,7 @@ void MdRun::start() {
   S.rng = std::make_unique<HostRng>(o.seed);
   if (S.ncons) {   // the constrained lengths hold from the start (dynamics.cpp:198-203)
     CK(cudaMemcpyAsync(S.x0.p, S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
-    launch_k(k_shake, blocks(size_t(S.C.ncl), 128), 128, 0, stream_, S.C, S.x.p, S.x0.p, S.v.p, 0.0, E.d_counters_.p, ListCheck{});
+    launch_k(S.C.lincs ? k_lincs : k_shake, blocks(size_t(S.C.ncl), 128), 128, 0, stream_, S.C, S.x.p, S.x0.p, S.v.p, 0.0, E.d_counters_.p, ListCheck{});
   }
 
   // velocities: given, or Maxwell-Boltzmann from the reference's stream, no centre-of-mass motion, rescaled to T
@@ -1911,7 +2079,7 @@ void MdRun::baro_step(long long s) {
   S.C.cell = E.dcell_;
   if (S.ncons) {
     CK(cudaMemcpyAsync(S.x0.p, S.x.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
-    launch_k(k_shake, blocks(size_t(S.C.ncl), 128), 128, 0, stream_, S.C, S.x.p, S.x0.p, S.v.p, 0.0, E.d_counters_.p, ListCheck{});
+    launch_k(S.C.lincs ? k_lincs : k_shake, blocks(size_t(S.C.ncl), 128), 128, 0, stream_, S.C, S.x.p, S.x0.p, S.v.p, 0.0, E.d_counters_.p, ListCheck{});
     S.rattle(0);
   }
   S.forces(true, true);
@@ -2015,6 +2183,8 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
                     S.hmr_moved, o.hmr, S.hmr_kept ? " (some left as they were: their neighbour would have been too light)" : "");
       *report += b;
     }
+    if (S.ncons && o.constraint_algorithm == 1)   // the reference's note (dynamics.cpp:176)
+      *report += " · constraint solver: LINCS (order 4) for positions, RATTLE for velocities";
   }
   R.completed = true;
   if (R.stopped_at >= 0) throw ModelError(CAPS_GPU_ESTOPPED, "stopped at step " + std::to_string(R.stopped_at + o.step_offset) + " (a stop was asked for)");

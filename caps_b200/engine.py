@@ -118,6 +118,8 @@ class EnergyOptions:
 
 THERMOSTATS = {"none": 0, "nve": 0, "bussi": 1, "csvr": 1, "langevin": 2, "baoab": 2, "nose-hoover": 3, "nhc": 3}
 BAROSTATS = {"none": 0, "crescale": 1, "c-rescale": 1, "berendsen": 2}
+# constraint_algorithm_from_string (constraints.hpp:22)
+CONSTRAINT_ALGORITHMS = {"shake": 0, "lincs": 1}
 
 
 @dataclass
@@ -147,6 +149,7 @@ class DynamicsOptions:
     anisotropic: bool = False          # Berendsen barostat per Cartesian axis
     couple_axis: tuple = (True, True, True)
     axis_pressure: tuple = (float("nan"), float("nan"), float("nan"))   # atm per axis; NaN: `pressure`
+    constraint_algorithm: str = "shake"   # "shake" | "lincs" (positions; RATTLE for the velocities either way)
     energy: EnergyOptions = field(default_factory=EnergyOptions)
 
     def to_struct(self, ff: ForceField, keep: list) -> _abi.MdOpts:
@@ -154,6 +157,9 @@ class DynamicsOptions:
         m.dt, m.steps, m.temperature, m.temperature_end = self.dt, self.steps, self.temperature, self.temperature_end
         m.thermostat = THERMOSTATS[self.thermostat.lower()]
         m.tau_t = self.tau_t
+        if self.barostat.lower() not in BAROSTATS:
+            raise ValueError(f"barostat {self.barostat!r}: the device path takes none, c-rescale or berendsen (the reference's "
+                             "Barostat::MTK is not built)")
         m.barostat = BAROSTATS[self.barostat.lower()]
         m.pressure, m.tau_p, m.compressibility, m.barostat_every = self.pressure, self.tau_p, self.compressibility, self.barostat_every
         m.constraints = 0 if self.constraints in ("none", "", None) else 1
@@ -161,6 +167,10 @@ class DynamicsOptions:
         m.seed, m.thermo_every, m.frame_every, m.step_offset, m.respa = self.seed, self.thermo_every, self.frame_every, self.step_offset, self.respa
         m.respa_split = {"bonded": 0, "pme": 1}[self.respa_split]
         m.checkpoint_every = int(self.checkpoint_every)
+        alg = (self.constraint_algorithm or "shake").lower()
+        if alg not in CONSTRAINT_ALGORITHMS:
+            raise ValueError(f"unknown constraint algorithm {self.constraint_algorithm!r} (shake | lincs)")
+        m.constraint_algorithm = CONSTRAINT_ALGORITHMS[alg]
         m.hmr = float(self.hmr)
         m.anisotropic = int(bool(self.anisotropic))
         m.couple_axes = sum(1 << k for k in range(3) if self.couple_axis[k])

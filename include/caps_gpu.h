@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define CAPS_GPU_ABI_VERSION 4
+#define CAPS_GPU_ABI_VERSION 5
 
 /* Status codes (negative). The text is in caps_gpu_error(). */
 #define CAPS_GPU_OK 0
@@ -148,6 +148,9 @@ typedef struct {
   int32_t couple_axes;      /* with anisotropic: bit k couples axis k (DynamicsOptions::couple_axis); 0 means all three */
   int32_t axis_pressure_set; /* with anisotropic: bit k set: axis k's target is axis_pressure[k], otherwise pressure */
   double axis_pressure[3];  /* atm */
+  /* ABI 5 */
+  int32_t constraint_algorithm; /* 0 SHAKE, 1 LINCS (order 4) for the positions; RATTLE for the velocities either way
+                                   (DynamicsOptions::constraint_algorithm, constraints.cpp:125-185) */
 } caps_gpu_md_opts;
 
 /* caps::ThermoRow (dynamics.hpp:28-43), the fields the device step fills. */

@@ -374,6 +374,7 @@ int ref_run(const caps_gpu_ff* p, const caps_gpu_opts* eo, caps_gpu_state* st, c
       if ((md->axis_pressure_set >> a) & 1) o.axis_pressure[a] = md->axis_pressure[a];
     }
     o.constraints = md->constraints ? ConstraintMode::HBonds : ConstraintMode::None;
+    o.constraint_algorithm = md->constraint_algorithm == 1 ? ConstraintAlgorithm::Lincs : ConstraintAlgorithm::Shake;
     o.new_velocities = md->new_velocities != 0;
     o.seed = md->seed;
     o.thermo_every = md->thermo_every;

@@ -36,7 +36,7 @@ def test_library_exports_every_declared_symbol(lib):
     for name in declared_functions():
         assert hasattr(lib, name), name
     assert set(_abi.EXPORTS) | set(_abi.DIAG_EXPORTS) <= set(declared_functions())
-    assert lib.caps_gpu_abi_version() == 4
+    assert lib.caps_gpu_abi_version() == 5
 
 
 def test_no_torch_in_the_boundary():

@@ -44,3 +44,17 @@ def test_options_map_to_the_c_struct():
 def test_cell_array_forms():
     assert cell_array(np.eye(3) * 10).tolist() == [0, 0, 0, 10, 0, 0, 0, 10, 0, 0, 0, 10]
     assert cell_array(list(range(12))).size == 12
+
+
+def test_constraint_algorithm_and_barostat_names():
+    """constraint_algorithm maps shake / lincs onto the C struct (constraint_algorithm_from_string, constraints.hpp:22);
+    an unknown name, and the reference's MTK barostat (not built on the device path), are refused before any call."""
+    import pytest
+    fx = load("ps_small")
+    keep: list = []
+    assert DynamicsOptions(constraints="h-bonds", constraint_algorithm="LINCS").to_struct(fx.ff, keep).constraint_algorithm == 1
+    assert DynamicsOptions(constraints="h-bonds").to_struct(fx.ff, keep).constraint_algorithm == 0
+    with pytest.raises(ValueError, match="unknown constraint algorithm"):
+        DynamicsOptions(constraint_algorithm="p-lincs").to_struct(fx.ff, keep)
+    with pytest.raises(ValueError, match="MTK is not built"):
+        DynamicsOptions(barostat="mtk").to_struct(fx.ff, keep)
