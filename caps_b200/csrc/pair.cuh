@@ -776,13 +776,9 @@ static __global__ void __launch_bounds__(128) k_prune(PairArgs A, double rprune2
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * n; i += gridDim.x * blockDim.x) xp[i] = x[i];
   if (blockIdx.x == 0 && threadIdx.x == 0) const_cast<int*>(A.counters)[kCntPrunes] += 1;
   if (A.counters[kCntErr] & (kErrListOverflow | kErrMaskOverflow | kErrScOverflow | kErrColumnTooBig | kErrExclOverflow)) return;
-  // per warp: the work item's i atoms as (-x, -y, -z, real); its entries' j atoms shifted by the entry's image,
-  // packed per lane quarter jq as the pair kernel stages them: (x_jq, x_jq+4, y_jq, y_jq+4), (z_jq, z_jq+4, 0, 0); and
-  // the new half masks. A lane holds its i atom of each cluster in registers and tests its two pairs of an i cluster
-  // with one packed evaluation (the staged loads are the kernel's bound: one pair of them per entry); padding j atoms
-  // lie far from every real i atom.
+  // per warp: the work item's i atoms, its entries' j atoms (w: 1 real, 0 padding) and the new half masks
   __shared__ float4 s_xi[4][64];
-  __shared__ float4 s_xj[4][kBatch][4][2];
+  __shared__ float4 s_xj[4][kBatch * 8];
   __shared__ unsigned s_keep[4][kBatch];
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i8 = lane & 7, jq = lane >> 3;
@@ -817,17 +813,18 @@ static __global__ void __launch_bounds__(128) k_prune(PairArgs A, double rprune2
       } else {
         v = A.xq[64 * sc + t];
       }
-      s_xi[wib][t] = make_float4(-v.x, -v.y, -v.z, A.tslot[64 * sc + t] != pad ? 1.f : 0.f);
+      v.w = A.tslot[64 * sc + t] != pad ? 1.f : 0.f;
+      s_xi[wib][t] = v;
     }
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       const int t = lane + 32 * k;   // entry t / 8, j atom t % 8
-      const int e = t >> 3, j = t & 7;
+      const int e = t >> 3;
       const unsigned cj = __shfl_sync(0xffffffffu, en.x, e & 31);
       const float ex = __shfl_sync(0xffffffffu, sx, e & 31), ey = __shfl_sync(0xffffffffu, sy, e & 31),
                   ez = __shfl_sync(0xffffffffu, sz, e & 31);
       if (e < ne) {
-        const int ja = 8 * int(cj) + j;
+        const int ja = 8 * int(cj) + (t & 7);
         float4 v;
         // FP64 path: absolute positions rounded to float (1e-5 Å at 100 Å), far inside the 0.8 Å prune margin
         if (DBL) {
@@ -836,37 +833,28 @@ static __global__ void __launch_bounds__(128) k_prune(PairArgs A, double rprune2
         } else {
           v = A.xq[ja];
         }
-        float* px = reinterpret_cast<float*>(&s_xj[wib][e][j & 3][0]);
-        const int h = j >> 2;
-        px[h] = v.x + ex;
-        px[2 + h] = v.y + ey;
-        px[4 + h] = v.z + ez;
-        px[6 + h] = 0.f;
+        v.x += ex, v.y += ey, v.z += ez;
+        v.w = A.tslot[ja] != pad ? 1.f : 0.f;
+        s_xj[wib][t] = v;
       }
     }
     __syncwarp();
-    unsigned ireal = 0;
-    float xi[8], yi[8], zi[8];
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      const float4 p = s_xi[wib][8 * c + i8];
-      xi[c] = p.x, yi[c] = p.y, zi[c] = p.z;
-      ireal |= unsigned(p.w != 0.f) << c;
-    }
     for (int el = 0; el < ne; ++el) {
       const unsigned built = __shfl_sync(0xffffffffu, en.y, el) & 255u;
-      const float4 xa = s_xj[wib][el][jq][0], xb = s_xj[wib][el][jq][1];
-      const float2 xj = make_float2(xa.x, xa.y), yj = make_float2(xa.z, xa.w), zj = make_float2(xb.x, xb.y);
+      const float4 a0 = s_xj[wib][8 * el + jq], a1 = s_xj[wib][8 * el + jq + 4];
       unsigned keep = 0;
 #pragma unroll
       for (int c = 0; c < 8; ++c) {
         if (!((built >> c) & 1u)) continue;
-        const float2 dx = p_add(xj, p_dup(xi[c])), dy = p_add(yj, p_dup(yi[c])), dz = p_add(zj, p_dup(zi[c]));
-        const float2 r2 = p_fma(dx, dx, p_fma(dy, dy, p_mul(dz, dz)));
-        const bool ri = (ireal >> c) & 1u;
-        const unsigned in = ((ri && r2.x < rp2) ? 1u : 0u) | ((ri && r2.y < rp2) ? 2u : 0u);
-        const unsigned any = __reduce_or_sync(0xffffffffu, in);
-        keep |= ((any & 1u) << c) | ((any >> 1) << (c + 8));
+        const float4 xi = s_xi[wib][8 * c + i8];
+#pragma unroll
+        for (int jj = 0; jj < 2; ++jj) {
+          const float4 xj = jj ? a1 : a0;
+          const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+          const float r2 = dx * dx + dy * dy + dz * dz;
+          const bool in = xi.w != 0.f && xj.w != 0.f && r2 < rp2;
+          if (__any_sync(0xffffffffu, in)) keep |= 1u << (c + 8 * jj);
+        }
       }
       if (lane == 0) s_keep[wib][el] = keep;
     }
