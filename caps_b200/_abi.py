@@ -27,6 +27,8 @@ class FF(C.Structure):
         ("excl_offset", P), ("excl_list", P),
         ("nfene", C.c_int32), ("fene_ij", P), ("fene_k_r0_eps_sigma", P),
         ("lj_shift", C.c_int32), ("model_cutoff", C.c_double), ("lj_form", C.c_int32),
+        # ABI 5
+        ("npair_func", C.c_int32), ("pair_func_ab", C.c_void_p), ("pair_func_p", C.c_void_p),
     ]
 
 

@@ -202,7 +202,7 @@ __device__ __forceinline__ void torsions_body(int blk, int nblk, int ngroups, co
 // form eps (2 q^(3/2) - 3 q), q = (s/r)^6 (field.cpp:1471-1475), else 4 eps (q^2 - q).
 template <class R, class S, bool ENER, bool VIR>
 __device__ __forceinline__ void pairs14_body(int blk, int nblk, int np, const uint32_t* __restrict__ ij, const double* __restrict__ scale, double lj14, const int* __restrict__ type, int nt,
-                          const double4* __restrict__ lj, const double4* __restrict__ cap, BondedArgs A, S F, int lj96) {
+                          const double4* __restrict__ lj, const double4* __restrict__ cap, const double4* __restrict__ gen, BondedArgs A, S F, int lj96) {
   Tally<VIR> T(A.fixed != 0);
   for (int t = blk * blockDim.x + threadIdx.x; t < np; t += nblk * blockDim.x) {
     const int i = int(ij[2 * t]), j = int(ij[2 * t + 1]);
@@ -213,7 +213,16 @@ __device__ __forceinline__ void pairs14_body(int blk, int nblk, int np, const ui
     const R sc = R(scale ? scale[t] : lj14);
     const R r2 = dx * dx + dy * dy + dz * dz;
     R fr, ev;
-    if (cap && r2 < R(cap[type[i] * nt + type[j]].x)) {
+    if (c.w != 0) {
+      // a generic form (field.cpp:2033-2034, FP64 only): nothing beyond the pair's own cut-off
+      const double4 g = gen[type[i] * nt + type[j]];
+      const double r2d = double(r2);
+      if (g.w > 0 && r2d > g.w) continue;
+      double e = 0;
+      const double f = generic_pair(int(c.w), g.x, g.y, g.z, r2d, e);
+      ev = R(double(sc) * e);
+      fr = R(double(sc) * f);
+    } else if (cap && r2 < R(cap[type[i] * nt + type[j]].x)) {
       const double4 cp = cap[type[i] * nt + type[j]];
       const R r = rsq(r2), rcp = rsq(R(cp.x));
       ev = sc * (R(cp.y) + R(cp.z) * (rcp - r));
@@ -367,7 +376,7 @@ struct BondedWork {
   double lj14;
   const int* type;
   int nt, lj96;
-  const double4 *lj14_tab, *cap14_tab;
+  const double4 *lj14_tab, *cap14_tab, *lj14g_tab;
   ExclArgs X;
 };
 
@@ -387,7 +396,7 @@ static __global__ void __launch_bounds__(256) k_bonded(BondedWork W, BondedArgs 
       break;
     case kBkFene: fene_body<R, S, ENER, VIR>(blk, nblk, W.nf, W.fene_ij, W.fene_p, A, F, W.counters, W.info); break;
     case kBkPairs14:
-      pairs14_body<R, S, ENER, VIR>(blk, nblk, W.np14, W.p14_ij, W.p14_scale, W.lj14, W.type, W.nt, W.lj14_tab, W.cap14_tab, A, F, W.lj96);
+      pairs14_body<R, S, ENER, VIR>(blk, nblk, W.np14, W.p14_ij, W.p14_scale, W.lj14, W.type, W.nt, W.lj14_tab, W.cap14_tab, W.lj14g_tab, A, F, W.lj96);
       break;
     default: excl_body<S, ENER, VIR>(blk, nblk, W.nx, W.X, A, F); break;
   }

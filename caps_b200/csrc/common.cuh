@@ -42,6 +42,26 @@ enum ErrorBits : unsigned {
 // stretched FENE bond and its length, and the step whose positions stopped being finite.
 enum ErrInfo { kInfoFeneBond = 0, kInfoFeneR, kInfoNonFiniteStep, kInfoNum = 4 };
 
+// The generic pair forms (field.cpp:1382-1396): -(dE/dr)/r, and E in e. 1 Buckingham A e^(-r/rho) - C/r^6 (a A, b rho,
+// c C); 3 Rydberg (A + C r) e^(-r/rho) (a A, b rho, c C); 2 Morse D (e^(-2 alpha (r - r0)) - 2 e^(-alpha (r - r0))) (a D,
+// b alpha, c r0).
+__device__ __forceinline__ double generic_pair(int form, double pa, double pb, double pc, double r2, double& e) {
+  const double r = sqrt(r2);
+  if (form == 1) {
+    const double ex = pa * exp(-r / pb), c6 = pc / (r2 * r2 * r2);
+    e = ex - c6;
+    return (ex / pb - 6 * c6 / r) / r;
+  }
+  if (form == 3) {
+    const double ex = exp(-r / pb), u = pa + pc * r;
+    e = u * ex;
+    return (u / pb - pc) * ex / r;
+  }
+  const double e1 = exp(-pb * (r - pc));
+  e = pa * (e1 * e1 - 2 * e1);
+  return 2 * pa * pb * (e1 * e1 - e1) / r;
+}
+
 // Periodic cell: origin o, edge vectors a, b, c (columns of h) and h^-1 (rows: reciprocal vectors without 2 pi).
 struct DevCell {
   double o[3];

@@ -168,6 +168,26 @@ void Engine::setup_ff(const caps_gpu_ff* ff) {
   h_mass_.assign(ff->mass, ff->mass + n_);
   h_eps_.assign(ff->pair_eps, ff->pair_eps + size_t(nt_) * nt_);
   h_sig_.assign(ff->pair_sigma, ff->pair_sigma + size_t(nt_) * nt_);
+  // generic pair forms (field.cpp:478-487): both orders of each type pair; the pair is evaluated whatever its LJ eps
+  const size_t nt2 = size_t(nt_) * nt_;
+  h_form_.assign(nt2, 0);
+  h_pa_.assign(nt2, 0.0), h_pb_.assign(nt2, 0.0), h_pc_.assign(nt2, 0.0), h_prc2_.assign(nt2, 0.0);
+  generic_ = false;
+  for (int k = 0; k < ff->npair_func; ++k) {
+    const int a = ff->pair_func_ab[2 * k], b = ff->pair_func_ab[2 * k + 1];
+    const double* q = ff->pair_func_p + 5 * k;
+    const int form = int(q[0]);
+    if (a < 0 || b < 0 || a >= nt_ || b >= nt_) throw ModelError(CAPS_GPU_EINVAL, "a pair form refers to a type out of range");
+    if (form != 1 && form != 2 && form != 3)
+      throw ModelError(CAPS_GPU_EFIELD, "the device path takes the Buckingham, Morse and Rydberg pair forms (tabulated, cosine-squared, lj/gromacs and SDK "
+                                        "pairs stay on the reference's CPU path)");
+    for (const size_t tp : {size_t(a) * nt_ + b, size_t(b) * nt_ + a}) {
+      h_form_[tp] = form;
+      h_pa_[tp] = q[1], h_pb_[tp] = q[2], h_pc_[tp] = q[3];
+      h_prc2_[tp] = q[4] * q[4];
+    }
+    generic_ = true;
+  }
   type_count_.assign(size_t(nt_), 0.0);
   for (int t : h_type_) type_count_[size_t(t)] += 1;
   d_type_.upload(h_type_, stream_);
@@ -285,11 +305,22 @@ void Engine::setup_ff(const caps_gpu_ff* ff) {
   CK(cudaStreamSynchronize(stream_));
 }
 
+// The energy of a generic pair form at r^2 (field.cpp:1382-1396), for the cut-off shift.
+static double generic_pair_energy(int form, double pa, double pb, double pc, double r2) {
+  const double r = std::sqrt(r2);
+  if (form == 1) return pa * std::exp(-r / pb) - pc / (r2 * r2 * r2);
+  if (form == 3) return (pa + pc * r) * std::exp(-r / pb);
+  const double e1 = std::exp(-pb * (r - pc));
+  return pa * (e1 * e1 - 2 * e1);
+}
+
 void Engine::setup_options() {
   rc_ = model_cutoff_ > 0 ? model_cutoff_ : opt_.cutoff;
   skin_ = opt_.skin;
   if (!(rc_ > 0) || skin_ < 0) throw ModelError(CAPS_GPU_EINVAL, "cut-off must be positive and skin non-negative");
-  mixed_ = opt_.precision == 0;
+  // a force field with generic pair forms runs the FP64 path, as the reference's mixed path falls back to its FP64
+  // pair loop for them (field.cpp:848)
+  mixed_ = opt_.precision == 0 && !generic_;
   tail_ = opt_.tail != 0 && !lj_shift_model_;
   shifted_ = !tail_;
   coul_ = opt_.coulomb != 0;
@@ -354,6 +385,26 @@ void Engine::setup_options() {
       tabd[size_t(a0) * ntab + b0] = make_double4(c6, c12, sh, 0.0);
       l14[size_t(a0) * nt_ + b0] = make_double4(eps, s6, sh, 0.0);
     }
+  // generic forms: no LJ part; the shift is the form's energy at the pair's own cut-off, or at r_c, unless the tail
+  // correction is on (field.cpp:1482-1492)
+  std::vector<double4> tabg(size_t(ntab) * ntab, make_double4(0, 0, 0, 0)), l14g(size_t(nt_) * nt_, make_double4(0, 0, 0, 0));
+  for (int a0 = 0; a0 < nt_ && generic_; ++a0)
+    for (int b0 = 0; b0 < nt_; ++b0) {
+      const size_t tp = size_t(a0) * nt_ + b0;
+      const int form = h_form_[tp];
+      if (!form) continue;
+      double sh = 0;
+      if (shifted_) {
+        const double r2 = h_prc2_[tp] > 0 ? std::min(h_prc2_[tp], rc2) : rc2;
+        sh = generic_pair_energy(form, h_pa_[tp], h_pb_[tp], h_pc_[tp], r2);
+      }
+      tabd[size_t(a0) * ntab + b0] = make_double4(0.0, 0.0, sh, double(form));
+      tabg[size_t(a0) * ntab + b0] = make_double4(h_pa_[tp], h_pb_[tp], h_pc_[tp], h_prc2_[tp]);
+      l14[tp] = make_double4(1.0, 0.0, sh, double(form));
+      l14g[tp] = tabg[size_t(a0) * ntab + b0];
+    }
+  d_tabg_.upload(tabg, stream_);
+  d_lj14g_.upload(l14g, stream_);
   d_tab_.upload(tab, stream_);
   // geometric mixing (c6_ab = sqrt(c6_aa c6_bb) and the same for c12, as OPLS-style force fields give): the FP32 pair
   // kernel takes per-type factors instead of the per-pair table (12-6 only)
@@ -378,7 +429,7 @@ void Engine::setup_options() {
     for (int a0 = 0; a0 < nt_; ++a0)
       for (int b0 = 0; b0 < nt_; ++b0) {
         const double e = h_eps_[size_t(a0) * nt_ + b0], s6 = std::pow(h_sig_[size_t(a0) * nt_ + b0], 6);
-        if (e <= 0) continue;
+        if (e <= 0 || h_form_[size_t(a0) * nt_ + b0] != 0) continue;   // the cap is for Lennard-Jones only
         const double sg = std::pow(s6, 1.0 / 6);
         auto force = [&](double r) {
           if (lj96_) {
@@ -651,6 +702,14 @@ void Engine::host_constants(caps_gpu_terms* t, bool ener, bool vir) const {
       for (int b0 = 0; b0 < nt_; ++b0) {
         const double eps = h_eps_[size_t(a0) * nt_ + b0], s6 = std::pow(h_sig_[size_t(a0) * nt_ + b0], 6), s12 = s6 * s6;
         const double nn = type_count_[size_t(a0)] * type_count_[size_t(b0)];
+        const size_t tp = size_t(a0) * nt_ + b0;
+        if (h_form_[tp] == 1) {   // Buckingham, as LAMMPS pair buck (field.cpp:2508-2514)
+          const double A = h_pa_[tp], rho = h_pb_[tp], Cc = h_pc_[tp], ex = std::exp(-rc_ / rho);
+          et += nn * 2 * kPi * (A * rho * ex * (rc2 + 2 * rho * rc_ + 2 * rho * rho) - Cc / (3 * rc3));
+          wt += nn * 2 * kPi * (A * ex * (rc3 + 3 * rho * rc2 + 6 * rho * rho * rc_ + 6 * rho * rho * rho) - 2 * Cc / rc3);
+          continue;
+        }
+        if (h_form_[tp] == 2 || h_form_[tp] == 3) continue;   // Morse, Rydberg: no tail term
         if (lj96_) {   // lj/class2 (field.cpp:2523-2529)
           const double s3 = std::sqrt(s6), rc6 = rc3 * rc3;
           et += nn * 2 * kPi * eps * s6 * (s3 - 3 * rc3) / (3 * rc6);

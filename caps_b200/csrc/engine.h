@@ -240,6 +240,12 @@ class Engine {
   DevBuf<float2> d_ljf_;   // per type (sqrt c6, sqrt c12), the padding type last
   bool comb_ = false;      // the pair coefficients factor per type (geometric mixing, 12-6)
   DevBuf<double4> d_tabd_, d_lj14_, d_tabcap_, d_cap14_;
+  // ForceField::pair_func on the FP64 path: per type pair the form (0 LJ) and its parameters, the pair's own cut-off
+  // squared; tables of (a, b, c, rc^2) beside the LJ tables (their .w holds the form)
+  std::vector<int> h_form_;
+  std::vector<double> h_pa_, h_pb_, h_pc_, h_prc2_;
+  bool generic_ = false;
+  DevBuf<double4> d_tabg_, d_lj14g_;
   DevBuf<double> d_gtab_;
   int gnodes_ = 0;
   double ghi_ = 0;

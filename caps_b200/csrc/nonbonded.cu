@@ -181,6 +181,7 @@ PairArgs Engine::pair_args() {
   A.batch = std::max(1, std::min(geom_.batch, kBatch));
   A.tabd = d_tabd_.p;
   A.tabcap = d_tabcap_.p;
+  A.tabg = d_tabg_.p;
   A.gtab = d_gtab_.p;
   A.ntab = nt_ + 1;
   A.gnodes = coul_ ? gnodes_ : 0;   // a table only with Coulomb: the FP64 kernel's shared memory holds it then

@@ -102,6 +102,7 @@ struct PairArgs {
   int batch;             // entries per work item of the list (<= kBatch): the FP32 kernel's staging per warp
   const double4* tabd;   // FP64: per type pair (c6, c12, energy shift, 0)
   const double4* tabcap; // FP64 with a force cap: per type pair (r_cap^2, E at r_cap, |F| at r_cap, 0)
+  const double4* tabg;   // FP64 generic forms (tabd.w the form): per type pair (a, b, c, the pair's own cut-off^2)
   const double* gtab;    // FP64 Ewald table: 2 per node (G, h dG/ds)
   int ntab;              // types incl. the padding type
   int gnodes;            // table nodes
@@ -468,6 +469,7 @@ static __global__ void __launch_bounds__(128, (ENER || VIR) ? 4 : 5) k_pair_f32(
 }
 
 // --- FP64 path ---------------------------------------------------------------------------------------------------
+
 // The reference's ewald_ef (field.cpp:1593-1602): E = 1/r - G(s), F = 1/r^3 + 2 dG/ds by cubic Hermite interpolation.
 __device__ __forceinline__ void ewald_ef(const double* __restrict__ gt, double ghi, double s, double rinv, double& E, double& F) {
   const double u = s * ghi;
@@ -575,6 +577,12 @@ static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
             const double r = r2 * rinv, rcp = sqrt(cp.x);
             fr = cp.z * rinv;   // F / r with |F| = the cap
             if (ENER) ev += cp.y + cp.z * (rcp - r) - cc.z;
+          } else if (cc.w != 0) {
+            // a generic form (field.cpp:1381-1396), nothing beyond the pair's own cut-off (and no shift there)
+            const double4 g = A.tabg[ti * A.ntab + tj];
+            double e = 0;
+            fr = (g.w > 0 && r2 > g.w) ? 0.0 : generic_pair(int(cc.w), g.x, g.y, g.z, r2, e);
+            if (ENER && !(g.w > 0 && r2 > g.w)) ev += e - cc.z;
           } else {
             if (LJ96) {   // field.cpp:1658-1661
               const double r9i = r6i * r2i * rinv;

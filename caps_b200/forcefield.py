@@ -56,6 +56,9 @@ class ForceField:
     model_cutoff: float = 0.0
     pair_form: str = "lj12-6"        # "lj12-6" | "lj9-6" (class II)
     element: np.ndarray | None = None      # [n] atomic numbers (constraints: hydrogens, rigid waters)
+    # ForceField::pair_func (field.hpp:68, 174): {(a, b): (form, a, b, c, rc)} with form "buckingham" (A, rho, C),
+    # "morse" (D, alpha, r0) or "rydberg" (A, rho, C), or their codes 1, 2, 3; rc > 0 the pair's own cut-off
+    pair_func: dict | None = None
 
     def __post_init__(self):
         self.type_index = np.ascontiguousarray(np.asarray(self.type_index, dtype=np.int32))
@@ -126,6 +129,20 @@ class ForceField:
         if self.pair_form not in ("lj12-6", "lj9-6"):
             raise ValueError(f"unknown pair form '{self.pair_form}' (lj12-6, lj9-6)")
         s.lj_form = 1 if self.pair_form == "lj9-6" else 0
+        if self.pair_func:
+            forms = {"buckingham": 1, "buck": 1, "morse": 2, "rydberg": 3}
+            ab, par = [], []
+            for (a, b), spec in sorted(self.pair_func.items()):
+                form, pa, pb, pc = spec[:4]
+                rc = spec[4] if len(spec) > 4 else 0.0
+                code = forms.get(form.lower()) if isinstance(form, str) else int(form)
+                if code is None:
+                    raise ValueError(f"pair form {form!r} for types ({a}, {b}): the device path takes buckingham, morse and rydberg")
+                ab += [min(a, b), max(a, b)]
+                par += [float(code), float(pa), float(pb), float(pc), float(rc)]
+            s.npair_func = len(self.pair_func)
+            s.pair_func_ab = ptr(np.asarray(ab, dtype=np.int32))
+            s.pair_func_p = ptr(np.asarray(par, dtype=np.float64))
         return s, keep
 
     def arrays(self) -> dict:

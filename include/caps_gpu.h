@@ -84,6 +84,14 @@ typedef struct {
   double model_cutoff;            /* ForceField::cutoff: > 0 replaces the options' cut-off */
   int32_t lj_form;                /* ForceField::pair_form (field.cpp:505-506): 0 "lj12-6" 4 eps ((s/r)^12 - (s/r)^6), 1 "lj9-6"
                                    * (class II) eps (2 (s/r)^9 - 3 (s/r)^6); pair_eps / pair_sigma are the mixed values either way */
+  /* ABI 5: ForceField::pair_func (field.hpp:68, 174), non-LJ forms for type pairs, on the FP64 path (a force field with any
+   * runs every evaluation in FP64, as the reference's mixed path falls back to its FP64 pair loop for them; field.cpp:848).
+   * Per entry: the type pair (a <= b) and (form, a, b, c, rc): 1 Buckingham A e^(-r/rho) - C/r^6 (A, rho, C); 2 Morse
+   * D (e^(-2 alpha (r - r0)) - 2 e^(-alpha (r - r0))) (D, alpha, r0); 3 Rydberg (A + C r) e^(-r/rho) (A, rho, C); rc > 0
+   * the pair's own cut-off. The tabulated, cosine-squared, lj/gromacs and SDK forms are refused. */
+  int32_t npair_func;
+  const int32_t* pair_func_ab;    /* [2*npair_func] */
+  const double* pair_func_p;      /* [5*npair_func] form, a, b, c, rc */
 } caps_gpu_ff;
 
 /* caps::EnergyOptions (field.hpp:274-308), the fields the device path takes. */

@@ -79,6 +79,13 @@ std::shared_ptr<ForceField> to_ff(const caps_gpu_ff* p) {
     for (int b = a; b < nt; ++b) ff->pair_override[{a, b}] = PairType{p->pair_eps[a * nt + b], p->pair_sigma[a * nt + b]};
   ff->mixing = "geometric";
   ff->pair_form = p->lj_form == 1 ? "lj9-6" : "lj12-6";
+  for (int k = 0; k < p->npair_func; ++k) {
+    const double* q = p->pair_func_p + 5 * k;
+    PairFunc f;
+    f.form = int(q[0]);
+    f.a = q[1], f.b = q[2], f.c = q[3], f.rc = q[4];
+    ff->pair_func[{p->pair_func_ab[2 * k], p->pair_func_ab[2 * k + 1]}] = f;
+  }
   ff->charge.assign(p->charge, p->charge + n);
   ff->mass.assign(p->mass, p->mass + n);
   for (int k = 0; k < p->nbonds; ++k) ff->bonds.push_back({p->bond_ij[2 * k], p->bond_ij[2 * k + 1], p->bond_k_r0[2 * k], p->bond_k_r0[2 * k + 1]});

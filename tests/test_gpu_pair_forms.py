@@ -1,0 +1,73 @@
+"""The generic FP64 pair forms (ForceField::pair_func: Buckingham, Morse, Rydberg, each with an optional cut-off of its
+own; field.cpp:478-487, 1381-1396, 1482-1492, 2508-2515) on the device against the reference core (oracle/_ref) on
+the same cells: energies, virial and forces at the FP64 bar (1e-12), with the cut-off shift or the tail correction,
+in the non-bonded pairs and the 1-4 pairs, under PME and damped shifted force. A force field with any of them runs the
+FP64 path whatever precision is asked for, as the reference's mixed path falls back to its FP64 pair loop."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from caps_b200 import EnergyOptions, Evaluator
+from tests.fixtures import load, rel_rms
+
+pytestmark = pytest.mark.gpu
+TERMS = ["bond", "angle", "dihedral", "improper", "vdw", "coulomb"]
+
+
+def _ref():
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("oracle/_ref is not built")
+    return ref
+
+
+# per fixture: Buckingham on a carbon pair (its 1-4 pairs included), Morse with a cut-off of its own, Rydberg
+FORMS = {
+    "ps_small": {(0, 1): ("buckingham", 30000.0, 0.28, 600.0), (1, 1): ("morse", 0.1, 1.2, 3.8, 6.5),
+                 (2, 3): ("rydberg", 50.0, 0.35, -10.0)},
+    "lj_triclinic": {(0, 0): ("buckingham", 25000.0, 0.27, 500.0), (1, 2): ("morse", 0.12, 1.1, 3.6, 6.0),
+                     (0, 2): ("rydberg", 40.0, 0.3, -5.0, 7.0)},
+}
+
+
+def _ff(name):
+    fx = load(name)
+    return fx, dataclasses.replace(fx.ff, pair_func=FORMS[name])
+
+
+@pytest.mark.parametrize("name,elec,tail", [("ps_small", "pme", False), ("ps_small", "pme", True), ("ps_small", "dsf", False),
+                                            ("lj_triclinic", "dsf", False), ("lj_triclinic", "dsf", True)])
+def test_fp64_pair_forms_match_reference(name, elec, tail):
+    ref = _ref()
+    fx, ff = _ff(name)
+    eo = EnergyOptions(cutoff=8.0, skin=2.0, electrostatics=elec, pme_order=5, tail=tail, precision="double")
+    t, f = Evaluator(ff, eo).compute(fx.x, fx.cell)
+    rt, rf = ref.compute(ff, eo, fx.x, fx.cell)
+    for k in TERMS:
+        assert abs(t[k] - rt[k]) <= 1e-12 * abs(rt[k]) + 1e-9, (k, t[k], rt[k])
+    assert abs(t["virial"] - rt["virial"]) <= 1e-11 * abs(rt["virial"]) + 1e-8
+    if tail:
+        assert abs(t["tail_energy"] - rt["tail_energy"]) <= 1e-12 * abs(rt["tail_energy"]) + 1e-12
+    assert rel_rms(f, rf) <= 1e-12
+    # the forms change the answer: the plain LJ force field gives another vdW energy
+    t0, _ = Evaluator(fx.ff, eo).compute(fx.x, fx.cell)
+    assert abs(t0["vdw"] - t["vdw"]) > 1e-6 * abs(t["vdw"])
+
+
+def test_pair_forms_run_fp64_when_mixed_is_asked():
+    fx, ff = _ff("ps_small")
+    eo = dict(cutoff=8.0, skin=2.0, electrostatics="pme", pme_order=5)
+    td, fd = Evaluator(ff, EnergyOptions(precision="double", **eo)).compute(fx.x, fx.cell)
+    tm, fm = Evaluator(ff, EnergyOptions(precision="mixed", **eo)).compute(fx.x, fx.cell)
+    assert abs(tm["vdw"] - td["vdw"]) <= 1e-12 * abs(td["vdw"])
+    assert rel_rms(fm, fd) <= 1e-13
+
+
+def test_unsupported_pair_form_is_refused():
+    fx = load("ps_small")
+    with pytest.raises(ValueError, match="buckingham, morse and rydberg"):
+        dataclasses.replace(fx.ff, pair_func={(0, 0): ("table", 0, 0, 0)}).to_struct()
+    ff = dataclasses.replace(fx.ff, pair_func={(0, 0): (20, 0.1, 3.4, 0.0)})   # lj/gromacs by its code
+    with pytest.raises(Exception, match="Buckingham, Morse and Rydberg"):
+        Evaluator(ff, EnergyOptions(precision="double"))
