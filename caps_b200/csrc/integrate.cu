@@ -722,6 +722,19 @@ __global__ void k_scale_v(int n, double* __restrict__ v, const double* __restric
   if (i >= 3 * n) return;
   v[i] *= sc[kScFactor];
 }
+// v *= f (the MTK step's factors, made on the host)
+__global__ void k_scale_by(int n, double* __restrict__ v, double f) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < 3 * n) v[i] *= f;
+}
+// The MTK remap (dynamics.cpp:560-570): x = c0 + mu (x - c0) about the cell's centre c0.
+__global__ void k_remap(int n, double* __restrict__ x, double c0x, double c0y, double c0z, double mu) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  x[3 * i] = c0x + mu * (x[3 * i] - c0x);
+  x[3 * i + 1] = c0y + mu * (x[3 * i + 1] - c0y);
+  x[3 * i + 2] = c0z + mu * (x[3 * i + 2] - c0z);
+}
 
 // The step counter and the thermostat target: T ramps linearly from t0 to t1 over `steps` when t1 >= 0.
 __device__ void step_begin_body(double* sc, double t0, double t1, long long steps, double ndof) {
@@ -1601,8 +1614,15 @@ void Engine::validate_md(const caps_gpu_md_opts& o) const {
   if (o.respa > 1 && o.constraints) throw ModelError(CAPS_GPU_EINVAL, "r-RESPA and bond constraints are alternatives: choose one");
   if (o.respa_split != 0 && o.respa_split != 1) throw ModelError(CAPS_GPU_EINVAL, "unknown r-RESPA split");
   if (o.thermostat < 0 || o.thermostat > 3) throw ModelError(CAPS_GPU_EINVAL, "unknown thermostat");
-  if (o.barostat < 0 || o.barostat > 2)
-    throw ModelError(CAPS_GPU_EINVAL, "the device path takes stochastic cell rescaling, the Berendsen barostat or no barostat");
+  if (o.barostat < 0 || o.barostat > 3) throw ModelError(CAPS_GPU_EINVAL, "unknown barostat (none, crescale, berendsen, mtk)");
+  // the reference's checks for MTK (dynamics.cpp:93-94, 103-106)
+  if (o.barostat == 3 && o.respa > 1) throw ModelError(CAPS_GPU_EINVAL, "r-RESPA runs with the Bussi thermostat or none");
+  if (o.barostat == 3 && o.anisotropic)
+    throw ModelError(CAPS_GPU_EINVAL, "the MTK barostat couples the volume isotropically; per-axis coupling and deformation use Berendsen");
+  if (o.barostat == 3 && o.constraints)
+    throw ModelError(CAPS_GPU_EINVAL, "the MTK barostat runs without bond constraints; use the stochastic cell rescaling barostat with constraints");
+  if (o.barostat == 3 && !(o.thermostat == 3 || o.thermostat == 0))
+    throw ModelError(CAPS_GPU_EINVAL, "the MTK barostat pairs with the Nosé–Hoover thermostat (NPT) or none (NPH)");
   if (o.barostat == 1 && o.thermostat == 0) throw ModelError(CAPS_GPU_EINVAL, "stochastic cell rescaling needs a thermostat");
   if (o.anisotropic && o.barostat == 1) throw ModelError(CAPS_GPU_EINVAL, "per-axis pressure coupling is available with the Berendsen barostat");
   if (o.hmr < 0 || !std::isfinite(o.hmr)) throw ModelError(CAPS_GPU_EINVAL, "the repartitioned hydrogen mass must be 0 (off) or positive");
@@ -1736,11 +1756,20 @@ struct MdRun {
     r.density = mtot / kNA / (r.volume * 1e-24);
     r.pressure = (2 * r.kinetic + t.virial) / (3 * r.volume) * kAtm;
     for (int c = 0; c < 6; ++c) r.p[c] = (sc[kScKin0 + c] + t.w[c]) / r.volume * kAtm;
-    if (S.nhc) {
-      const Chain& ch = *S.h_chain;
+    if (S.nhc || mtk()) {
+      // the extended system's energy (LAMMPS fix nh compute_scalar, dynamics.cpp:369-381)
       const double kt = kB * r.target_temperature;
-      double e = S.ndof * kt * ch.eta[0] + 0.5 * ch.eta_mass[0] * ch.eta_dot[0] * ch.eta_dot[0];
-      for (int c = 1; c < 3; ++c) e += kt * ch.eta[c] + 0.5 * ch.eta_mass[c] * ch.eta_dot[c] * ch.eta_dot[c];
+      double e = 0;
+      if (S.nhc) {
+        const Chain& ch = *S.h_chain;
+        e += S.ndof * kt * ch.eta[0] + 0.5 * ch.eta_mass[0] * ch.eta_dot[0] * ch.eta_dot[0];
+        for (int c = 1; c < 3; ++c) e += kt * ch.eta[c] + 0.5 * ch.eta_mass[c] * ch.eta_dot[c] * ch.eta_dot[c];
+      }
+      if (mtk()) {
+        e += 3 * 0.5 * omega_mass * omega_dot * omega_dot + o.pressure * (r.volume - vol0) / kAtm;
+        e += 3 * kt * etap[0] + 0.5 * etap_mass[0] * etap_dot[0] * etap_dot[0];
+        for (int c = 1; c < 3; ++c) e += kt * etap[c] + 0.5 * etap_mass[c] * etap_dot[c] * etap_dot[c];
+      }
       r.conserved = r.total + e;
     } else {
       r.conserved = r.total + sc[kScBath] + (o.barostat ? o.pressure * r.volume / kAtm : 0.0);
@@ -1812,7 +1841,35 @@ struct MdRun {
     }
     return c;
   }
-  bool baro_due(long long s) const { return o.barostat && s % baro_every == 0; }
+  bool baro_due(long long s) const { return (o.barostat == 1 || o.barostat == 2) && s % baro_every == 0; }
+  // The MTK barostat (Barostat::MTK, LAMMPS fix npt / nph as dynamics.cpp:479-570, 628-642): every step on the host's
+  // schedule, outside the graphs (the cell moves twice a step); the barostat's chain, the volume's momentum and, with the
+  // Nose-Hoover thermostat, the particles' chain as the reference orders them.
+  bool mtk() const { return o.barostat == 3; }
+  double etap[3] = {0, 0, 0}, etap_dot[4] = {0, 0, 0, 0}, etap_dotdot[3] = {0, 0, 0}, etap_mass[3] = {0, 0, 0};
+  double omega_dot = 0, omega_mass = 0, mtk_term2 = 0, vol0 = 0, mtk_virial = 0;
+  double target_t(long long step) const {
+    return (o.temperature_end >= 0 && o.steps > 0) ? o.temperature + (o.temperature_end - o.temperature) * double(step) / double(o.steps) : o.temperature;
+  }
+  double ke_now() {
+    S.ke(kScKE, false);
+    CK(cudaMemcpyAsync(S.h_sc + kScKE, S.sc.p + kScKE, sizeof(double), cudaMemcpyDeviceToHost, E.stream_));
+    CK(cudaStreamSynchronize(E.stream_));
+    return S.h_sc[kScKE];
+  }
+  void scale_by(double f) { launch_k(k_scale_by, blocks(size_t(3) * S.n, 256), 256, 0, E.stream_, S.n, S.v.p, f); }
+  // the virial of the last force evaluation (energies and virial on), as the rows take it
+  void read_virial() {
+    sync_scalars();
+    caps_gpu_terms t{};
+    E.read_terms(&t, true, true);
+    mtk_virial = t.w[0] + t.w[1] + t.w[2];
+  }
+  void mtk_nhc_temp(double tt);
+  void mtk_nhc_press(double tt);
+  void mtk_omega_step(double tt);
+  void mtk_remap();
+  void mtk_step(long long s);
   // a step that reports, records, rescales the cell or refills the thermostat's draws
   bool special(long long s) const {
     return s % thermo_every == 0 || s == o.steps || frame_due(s) || checkpoint_due(s) || baro_due(s) || refill_due(s);
@@ -1823,7 +1880,7 @@ struct MdRun {
   void advance(long long s, bool stop = false);
   // steps s .. s + kBlockSteps - 1 are plain steps (no row, frame, checkpoint, cell rescaling or thermostat refill)
   bool block_due(long long s) const {
-    if (s + Stepper::kBlockSteps - 1 >= o.steps) return false;
+    if (mtk() || s + Stepper::kBlockSteps - 1 >= o.steps) return false;
     for (long long t = s; t < s + Stepper::kBlockSteps; ++t)
       if (special(t)) return false;
     return true;
@@ -1975,8 +2032,15 @@ void MdRun::start() {
     CK(cudaMemcpyAsync(S.v.p, vs.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     CK(cudaStreamSynchronize(stream_));
   }
+  if (mtk()) {   // the MTK state starts at rest (dynamics.cpp:331-337)
+    for (int c = 0; c < 3; ++c) etap[c] = etap_dotdot[c] = etap_mass[c] = 0;
+    for (int c = 0; c < 4; ++c) etap_dot[c] = 0;
+    omega_dot = omega_mass = mtk_term2 = 0;
+    vol0 = E.dcell_.vol;
+  }
   emit(0);
   take(0, frame_due(0), 0);
+  if (mtk()) read_virial();   // the first evaluation's virial, for the first step's volume momentum
 
   thermo_every = std::max(1, o.thermo_every);
   baro_every = std::max(1, o.barostat_every);
@@ -1990,7 +2054,10 @@ void MdRun::advance(long long s, bool stop) {
     S.drop_graphs();   // the draw table's first step is a parameter of the captured thermostat kernel
     ++generation;
   }
-  if (baro_due(s)) {
+  if (mtk()) {
+    mtk_step(s);
+    ++baro_steps;
+  } else if (baro_due(s)) {
     baro_step(s);
   } else {
     // energies and virial only for a thermo row: a step that only records, refills or stops runs the plain graph
@@ -2011,6 +2078,120 @@ void MdRun::advance(long long s, bool stop) {
   } else if (s < o.steps && g_stop.load(std::memory_order_relaxed) != 0) {
     stop_here(s);   // asked for during this step's callbacks: the reference's check comes after them (dynamics.cpp:765)
   }
+}
+
+// The particles' chain over half a step (dynamics.cpp:479-504) on the host copy of the chain, the velocities scaled on
+// the device; the chain goes back to the device for the rows.
+void MdRun::mtk_nhc_temp(double tt) {
+  const double dt = o.dt, dthalf = 0.5 * dt, dt4 = 0.25 * dt, dt8 = 0.125 * dt, t_freq = S.t_freq, ndof = S.ndof;
+  Chain& c = *S.h_chain;
+  const double kt = kB * tt, ke_target = ndof * kt;
+  c.eta_mass[0] = ndof * kt / (t_freq * t_freq);
+  for (int q = 1; q < 3; ++q) c.eta_mass[q] = kt / (t_freq * t_freq);
+  double kecur = 2 * ke_now();
+  c.eta_dotdot[0] = (kecur - ke_target) / c.eta_mass[0];
+  for (int q = 2; q > 0; --q) {
+    const double ex = std::exp(-dt8 * c.eta_dot[q + 1]);
+    c.eta_dot[q] = (c.eta_dot[q] * ex + c.eta_dotdot[q] * dt4) * ex;
+  }
+  double ex = std::exp(-dt8 * c.eta_dot[1]);
+  c.eta_dot[0] = (c.eta_dot[0] * ex + c.eta_dotdot[0] * dt4) * ex;
+  const double factor = std::exp(-dthalf * c.eta_dot[0]);
+  scale_by(factor);
+  kecur *= factor * factor;
+  c.eta_dotdot[0] = (kecur - ke_target) / c.eta_mass[0];
+  for (int q = 0; q < 3; ++q) c.eta[q] += dthalf * c.eta_dot[q];
+  c.eta_dot[0] = (c.eta_dot[0] * ex + c.eta_dotdot[0] * dt4) * ex;
+  for (int q = 1; q < 3; ++q) {
+    ex = std::exp(-dt8 * c.eta_dot[q + 1]);
+    c.eta_dot[q] *= ex;
+    c.eta_dotdot[q] = (c.eta_mass[q - 1] * c.eta_dot[q - 1] * c.eta_dot[q - 1] - kt) / c.eta_mass[q];
+    c.eta_dot[q] = (c.eta_dot[q] + c.eta_dotdot[q] * dt4) * ex;
+  }
+  CK(cudaMemcpy(S.chain.p, S.h_chain, sizeof(Chain), cudaMemcpyHostToDevice));
+}
+
+// The barostat's chain over half a step (FixNH::nhc_press_integrate, iso; dynamics.cpp:506-531).
+void MdRun::mtk_nhc_press(double tt) {
+  const double dt = o.dt, dthalf = 0.5 * dt, dt4 = 0.25 * dt, dt8 = 0.125 * dt;
+  const double p_freq = 1.0 / std::max(o.tau_p, 1e-9), natoms = double(S.n);
+  const double kt = kB * tt;
+  omega_mass = (natoms + 1) * kt / (p_freq * p_freq);
+  for (int c = 0; c < 3; ++c) etap_mass[c] = kt / (p_freq * p_freq);
+  for (int c = 1; c < 3; ++c) etap_dotdot[c] = (etap_mass[c - 1] * etap_dot[c - 1] * etap_dot[c - 1] - kt) / etap_mass[c];
+  double kecur = 3 * omega_mass * omega_dot * omega_dot;
+  etap_dotdot[0] = (kecur - kt) / etap_mass[0];
+  for (int c = 2; c > 0; --c) {
+    const double ex = std::exp(-dt8 * etap_dot[c + 1]);
+    etap_dot[c] = (etap_dot[c] * ex + etap_dotdot[c] * dt4) * ex;
+  }
+  double ex = std::exp(-dt8 * etap_dot[1]);
+  etap_dot[0] = (etap_dot[0] * ex + etap_dotdot[0] * dt4) * ex;
+  for (int c = 0; c < 3; ++c) etap[c] += dthalf * etap_dot[c];
+  omega_dot *= std::exp(-dthalf * etap_dot[0]);
+  kecur = 3 * omega_mass * omega_dot * omega_dot;
+  etap_dotdot[0] = (kecur - kt) / etap_mass[0];
+  etap_dot[0] = (etap_dot[0] * ex + etap_dotdot[0] * dt4) * ex;
+  for (int c = 1; c < 3; ++c) {
+    ex = std::exp(-dt8 * etap_dot[c + 1]);
+    etap_dot[c] *= ex;
+    etap_dotdot[c] = (etap_mass[c - 1] * etap_dot[c - 1] * etap_dot[c - 1] - kt) / etap_mass[c];
+    etap_dot[c] = (etap_dot[c] + etap_dotdot[c] * dt4) * ex;
+  }
+}
+
+// The volume's momentum over half a step (FixNH::nh_omega_dot, iso, with the MTK terms; dynamics.cpp:533-541), from the
+// kinetic energy now and the virial of the last force evaluation.
+void MdRun::mtk_omega_step(double tt) {
+  const double dthalf = 0.5 * o.dt, p_freq = 1.0 / std::max(o.tau_p, 1e-9), natoms = double(S.n);
+  const double kt = kB * tt;
+  omega_mass = (natoms + 1) * kt / (p_freq * p_freq);
+  const double vol = E.dcell_.vol;
+  const double ke2 = 2 * ke_now();
+  const double p = (ke2 + mtk_virial) / (3 * vol) * kAtm;
+  const double mtk_term1 = ke2 / (3 * natoms);
+  omega_dot += ((p - o.pressure) * vol / (omega_mass * kAtm) + mtk_term1 / omega_mass) * dthalf;
+  mtk_term2 = 3 * omega_dot / (3 * natoms);
+}
+
+// The cell and the positions scaled by exp(dt/2 omega_dot) about the cell's centre (dynamics.cpp:560-570).
+void MdRun::mtk_remap() {
+  const double mu = std::exp(0.5 * o.dt * omega_dot);
+  double c[12];
+  std::memcpy(c, E.cell_h_, sizeof c);
+  double c0[3];
+  for (int k = 0; k < 3; ++k) c0[k] = c[k] + (c[3 + k] + c[6 + k] + c[9 + k]) * 0.5;
+  launch_k(k_remap, blocks(size_t(S.n), 256), 256, 0, E.stream_, S.n, S.x.p, c0[0], c0[1], c0[2], mu);
+  for (int k = 3; k < 12; ++k) c[k] = c[k] * mu;
+  for (int k = 0; k < 3; ++k) c[k] = c0[k] - (c[3 + k] + c[6 + k] + c[9 + k]) * 0.5;
+  E.set_cell(c);
+  S.C.cell = E.dcell_;
+  S.drop_graphs();
+}
+
+// One MTK step in the reference's order (dynamics.cpp:628-642): the barostat's chain, the particles' chain, the volume's
+// momentum and its velocity factor, half kick, remap, drift, remap, forces (energies and virial), half kick, velocity
+// factor, the volume's momentum, the particles' chain, the barostat's chain.
+void MdRun::mtk_step(long long s) {
+  cudaStream_t stream_ = E.stream_;
+  const double dt = o.dt, dthalf = 0.5 * dt;
+  launch_k(k_step_begin, 1, 1, 0, stream_, S.sc.p, o.temperature, o.temperature_end, (long long)o.steps, S.ndof);
+  const double tt = target_t(s);
+  mtk_nhc_press(tt);
+  if (S.nhc) mtk_nhc_temp(tt);
+  mtk_omega_step(tt);
+  scale_by(std::exp(-dthalf * (omega_dot + mtk_term2)));
+  S.vel_rattle(S.kick_op(0.5 * dt), 0);
+  mtk_remap();
+  S.kick_drift(0.0, dt, false, true);
+  mtk_remap();
+  S.forces(true, true);
+  read_virial();
+  S.vel_rattle(S.kick_op(0.5 * dt), 0);
+  scale_by(std::exp(-dthalf * (omega_dot + mtk_term2)));
+  mtk_omega_step(tt);
+  if (S.nhc) mtk_nhc_temp(tt);
+  mtk_nhc_press(tt);
 }
 
 // A step with stochastic cell rescaling (Bernetti & Bussi 2020, dynamics.cpp:684-723), isotropic.
@@ -2109,7 +2290,7 @@ void Engine::run(caps_gpu_state* st, const caps_gpu_md_opts* md, caps_gpu_progre
   }
   // the step graphs are captured before the step loop, as set-up (like the first force evaluation), so that no step's
   // time holds a capture
-  if (o.steps > 0 && !R.baro_due(1) && !R.refill_due(1)) {
+  if (o.steps > 0 && !R.mtk() && !R.baro_due(1) && !R.refill_due(1)) {
     S.ensure_graph(false);
     S.ensure_graph(true);
     if (!timed && o.steps > Stepper::kBlockSteps) S.ensure_graph(false, true);

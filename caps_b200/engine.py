@@ -117,7 +117,8 @@ class EnergyOptions:
 
 
 THERMOSTATS = {"none": 0, "nve": 0, "bussi": 1, "csvr": 1, "langevin": 2, "baoab": 2, "nose-hoover": 3, "nhc": 3}
-BAROSTATS = {"none": 0, "crescale": 1, "c-rescale": 1, "berendsen": 2}
+# barostat_from_string (dynamics.cpp:36-42)
+BAROSTATS = {"none": 0, "crescale": 1, "c-rescale": 1, "berendsen": 2, "mtk": 3, "mttk": 3, "nose-hoover": 3, "parrinello-rahman-mtk": 3}
 # constraint_algorithm_from_string (constraints.hpp:22)
 CONSTRAINT_ALGORITHMS = {"shake": 0, "lincs": 1}
 
@@ -158,8 +159,7 @@ class DynamicsOptions:
         m.thermostat = THERMOSTATS[self.thermostat.lower()]
         m.tau_t = self.tau_t
         if self.barostat.lower() not in BAROSTATS:
-            raise ValueError(f"barostat {self.barostat!r}: the device path takes none, c-rescale or berendsen (the reference's "
-                             "Barostat::MTK is not built)")
+            raise ValueError(f"unknown barostat '{self.barostat}' (none, crescale, berendsen, mtk)")
         m.barostat = BAROSTATS[self.barostat.lower()]
         m.pressure, m.tau_p, m.compressibility, m.barostat_every = self.pressure, self.tau_p, self.compressibility, self.barostat_every
         m.constraints = 0 if self.constraints in ("none", "", None) else 1

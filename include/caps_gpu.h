@@ -130,7 +130,8 @@ typedef struct {
   double temperature_end;   /* K; >= 0 ramps the target linearly over the run */
   int32_t thermostat;       /* 0 none (NVE), 1 Bussi, 2 Langevin (BAOAB), 3 Nose-Hoover chain of 3 */
   double tau_t;             /* fs */
-  int32_t barostat;         /* 0 none, 1 stochastic cell rescaling, 2 Berendsen (the reference's CRescale and Berendsen) */
+  int32_t barostat;         /* 0 none, 1 stochastic cell rescaling, 2 Berendsen, 3 MTK (the reference's CRescale, Berendsen
+                               and MTK; MTK every step, isotropic, without constraints, with Nose-Hoover or no thermostat) */
   double pressure;          /* atm */
   double tau_p;             /* fs */
   double compressibility;   /* 1/atm */

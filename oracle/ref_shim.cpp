@@ -369,7 +369,7 @@ int ref_run(const caps_gpu_ff* p, const caps_gpu_opts* eo, caps_gpu_state* st, c
     const Thermostat th[4] = {Thermostat::None, Thermostat::Bussi, Thermostat::Langevin, Thermostat::NoseHoover};
     o.thermostat = th[md->thermostat & 3];
     o.tau_t = md->tau_t;
-    o.barostat = md->barostat == 1 ? Barostat::CRescale : md->barostat == 2 ? Barostat::Berendsen : Barostat::None;
+    o.barostat = md->barostat == 1 ? Barostat::CRescale : md->barostat == 2 ? Barostat::Berendsen : md->barostat == 3 ? Barostat::MTK : Barostat::None;
     o.pressure = md->pressure;
     o.tau_p = md->tau_p;
     o.compressibility = md->compressibility;

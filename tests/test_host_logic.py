@@ -47,8 +47,8 @@ def test_cell_array_forms():
 
 
 def test_constraint_algorithm_and_barostat_names():
-    """constraint_algorithm maps shake / lincs onto the C struct (constraint_algorithm_from_string, constraints.hpp:22);
-    an unknown name, and the reference's MTK barostat (not built on the device path), are refused before any call."""
+    """constraint_algorithm maps shake / lincs onto the C struct (constraint_algorithm_from_string, constraints.hpp:22),
+    the barostat names as barostat_from_string does (dynamics.cpp:36-42); unknown names are refused before any call."""
     import pytest
     fx = load("ps_small")
     keep: list = []
@@ -56,5 +56,6 @@ def test_constraint_algorithm_and_barostat_names():
     assert DynamicsOptions(constraints="h-bonds").to_struct(fx.ff, keep).constraint_algorithm == 0
     with pytest.raises(ValueError, match="unknown constraint algorithm"):
         DynamicsOptions(constraint_algorithm="p-lincs").to_struct(fx.ff, keep)
-    with pytest.raises(ValueError, match="MTK is not built"):
-        DynamicsOptions(barostat="mtk").to_struct(fx.ff, keep)
+    assert DynamicsOptions(barostat="mtk").to_struct(fx.ff, keep).barostat == 3
+    with pytest.raises(ValueError, match="unknown barostat"):
+        DynamicsOptions(barostat="andersen").to_struct(fx.ff, keep)
