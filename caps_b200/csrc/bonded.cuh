@@ -202,7 +202,8 @@ __device__ __forceinline__ void torsions_body(int blk, int nblk, int ngroups, co
 // form eps (2 q^(3/2) - 3 q), q = (s/r)^6 (field.cpp:1471-1475), else 4 eps (q^2 - q).
 template <class R, class S, bool ENER, bool VIR>
 __device__ __forceinline__ void pairs14_body(int blk, int nblk, int np, const uint32_t* __restrict__ ij, const double* __restrict__ scale, double lj14, const int* __restrict__ type, int nt,
-                          const double4* __restrict__ lj, const double4* __restrict__ cap, const double4* __restrict__ gen, BondedArgs A, S F, int lj96) {
+                          const double4* __restrict__ lj, const double4* __restrict__ cap, const double4* __restrict__ gen, const double4* __restrict__ gen2,
+                          double r1, PairTables tabs, BondedArgs A, S F, int lj96) {
   Tally<VIR> T(A.fixed != 0);
   for (int t = blk * blockDim.x + threadIdx.x; t < np; t += nblk * blockDim.x) {
     const int i = int(ij[2 * t]), j = int(ij[2 * t + 1]);
@@ -219,7 +220,7 @@ __device__ __forceinline__ void pairs14_body(int blk, int nblk, int np, const ui
       const double r2d = double(r2);
       if (g.w > 0 && r2d > g.w) continue;
       double e = 0;
-      const double f = generic_pair(int(c.w), g.x, g.y, g.z, r2d, e);
+      const double f = generic_pair(int(c.w), g, gen2[type[i] * nt + type[j]], r1, tabs, r2d, e);
       ev = R(double(sc) * e);
       fr = R(double(sc) * f);
     } else if (cap && r2 < R(cap[type[i] * nt + type[j]].x)) {
@@ -376,7 +377,9 @@ struct BondedWork {
   double lj14;
   const int* type;
   int nt, lj96;
-  const double4 *lj14_tab, *cap14_tab, *lj14g_tab;
+  const double4 *lj14_tab, *cap14_tab, *lj14g_tab, *lj14g2_tab;
+  double lj_inner;
+  PairTables tables;
   ExclArgs X;
 };
 
@@ -396,7 +399,7 @@ static __global__ void __launch_bounds__(256) k_bonded(BondedWork W, BondedArgs 
       break;
     case kBkFene: fene_body<R, S, ENER, VIR>(blk, nblk, W.nf, W.fene_ij, W.fene_p, A, F, W.counters, W.info); break;
     case kBkPairs14:
-      pairs14_body<R, S, ENER, VIR>(blk, nblk, W.np14, W.p14_ij, W.p14_scale, W.lj14, W.type, W.nt, W.lj14_tab, W.cap14_tab, W.lj14g_tab, A, F, W.lj96);
+      pairs14_body<R, S, ENER, VIR>(blk, nblk, W.np14, W.p14_ij, W.p14_scale, W.lj14, W.type, W.nt, W.lj14_tab, W.cap14_tab, W.lj14g_tab, W.lj14g2_tab, W.lj_inner, W.tables, A, F, W.lj96);
       break;
     default: excl_body<S, ENER, VIR>(blk, nblk, W.nx, W.X, A, F); break;
   }

@@ -42,24 +42,85 @@ enum ErrorBits : unsigned {
 // stretched FENE bond and its length, and the step whose positions stopped being finite.
 enum ErrInfo { kInfoFeneBond = 0, kInfoFeneR, kInfoNonFiniteStep, kInfoNum = 4 };
 
-// The generic pair forms (field.cpp:1382-1396): -(dE/dr)/r, and E in e. 1 Buckingham A e^(-r/rho) - C/r^6 (a A, b rho,
-// c C); 3 Rydberg (A + C r) e^(-r/rho) (a A, b rho, c C); 2 Morse D (e^(-2 alpha (r - r0)) - 2 e^(-alpha (r - r0))) (a D,
-// b alpha, c r0).
-__device__ __forceinline__ double generic_pair(int form, double pa, double pb, double pc, double r2, double& e) {
-  const double r = sqrt(r2);
+// The generic pair forms (field.cpp:1381-1455): returns -(dE/dr)/r, E in e. p = (a, b, c, the pair's cut-off^2), g the
+// lj/gromacs switch coefficients (its constant is the caller's shift), r1 = lj_inner, T the tabulated pairs.
+// 1 Buckingham A e^(-r/rho) - C/r^6 (a A, b rho, c C); 2 Morse D (e^(-2 alpha (r - r0)) - 2 e^(-alpha (r - r0))) (a D,
+// b alpha, c r0); 3 Rydberg (A + C r) e^(-r/rho) (a A, b rho, c C); 11-14 SDK C eps ((s/r)^m - (s/r)^n) (a eps, b
+// sigma); 20 lj/gromacs (a eps, b sigma); 31 / 32 cosine-squared, 32 with WCA (a eps, b sigma, c cut-off); 40 a table.
+struct PairTables {
+  const int* off;        // [ntables + 1] first point of each table
+  const double* r0dr;    // [2 ntables]
+  const double* e;
+  const double* f;
+};
+__device__ __forceinline__ double generic_pair(int form, const double4& p, const double4& g, double r1, const PairTables& T, double r2, double& e) {
+  const double pa = p.x, pb = p.y, pc = p.z;
+  e = 0;
   if (form == 1) {
-    const double ex = pa * exp(-r / pb), c6 = pc / (r2 * r2 * r2);
+    const double r = sqrt(r2), ex = pa * exp(-r / pb), c6 = pc / (r2 * r2 * r2);
     e = ex - c6;
     return (ex / pb - 6 * c6 / r) / r;
   }
   if (form == 3) {
-    const double ex = exp(-r / pb), u = pa + pc * r;
+    const double r = sqrt(r2), ex = exp(-r / pb), u = pa + pc * r;
     e = u * ex;
     return (u / pb - pc) * ex / r;
   }
-  const double e1 = exp(-pb * (r - pc));
-  e = pa * (e1 * e1 - 2 * e1);
-  return 2 * pa * pb * (e1 * e1 - e1) / r;
+  if (form == 2) {
+    const double r = sqrt(r2), e1 = exp(-pb * (r - pc));
+    e = pa * (e1 * e1 - 2 * e1);
+    return 2 * pa * pb * (e1 * e1 - e1) / r;
+  }
+  if (form == 31 || form == 32) {
+    const double r = sqrt(r2), ep = pa, sg = pb, rcp = pc;
+    if (r >= rcp && !(form == 32 && r < sg)) return 0.0;
+    double ev = 0, dEdr = 0;
+    if (r < sg) {
+      if (rcp > sg) ev = -ep;
+      if (form == 32) {
+        const double s6 = pow(sg / r, 6.0);
+        ev += ep * (s6 * s6 - 2 * s6 + 1);
+        dEdr += -12 * ep * (s6 * s6 - s6) / r;
+      }
+    } else {
+      const double w = 3.14159265358979323846 * (r - sg) / (2 * (rcp - sg)), c = cos(w);
+      ev = -ep * c * c;
+      dEdr = ep * 2 * c * sin(w) * 3.14159265358979323846 / (2 * (rcp - sg));
+    }
+    e = ev;
+    return -dEdr / r;
+  }
+  if (form == 40) {
+    const int t = int(pa), k0 = T.off[t], m = T.off[t + 1] - k0;
+    const double r = sqrt(r2), t0 = T.r0dr[2 * t], dr = T.r0dr[2 * t + 1];
+    if (m < 2 || r >= t0 + dr * double(m - 1)) return 0.0;
+    if (r < t0) {   // below the table: a straight wall at the first force
+      e = T.e[k0] + T.f[k0] * (t0 - r);
+      return T.f[k0] / r;
+    }
+    const double u = (r - t0) / dr;
+    const int k = min(m - 2, int(u));
+    const double w = u - double(k);
+    e = T.e[k0 + k] * (1 - w) + T.e[k0 + k + 1] * w;
+    return (T.f[k0 + k] * (1 - w) + T.f[k0 + k + 1] * w) / r;
+  }
+  if (form == 20) {
+    const double s6 = pow(pb, 6.0), r2i = 1 / r2, r6i = r2i * r2i * r2i;
+    double ev = r6i * (4 * pa * s6 * s6 * r6i - 4 * pa * s6), fr = r6i * (48 * pa * s6 * s6 * r6i - 24 * pa * s6);
+    if (r2 > r1 * r1) {
+      const double r = sqrt(r2), tl = r - r1;
+      ev += tl * tl * tl * (g.z + g.w * tl);
+      fr += r * tl * tl * (g.x + g.y * tl);
+    }
+    e = ev;
+    return fr * r2i;
+  }
+  // SDK (11-14)
+  const double pw1 = form == 11 ? 9.0 : 12.0, pw2 = form == 11 ? 6.0 : form == 12 ? 4.0 : form == 13 ? 6.0 : 5.0;
+  const double pre = form == 11 ? 6.75 : form == 12 ? 2.59807621135332 : form == 13 ? 4.0 : 3.20377984125109;
+  const double sr2 = pb * pb / r2, sm = pow(sr2, pw1 / 2), sn = pow(sr2, pw2 / 2), c = pre * pa;
+  e = c * (sm - sn);
+  return c * (pw1 * sm - pw2 * sn) / r2;
 }
 
 // Periodic cell: origin o, edge vectors a, b, c (columns of h) and h^-1 (rows: reciprocal vectors without 2 pi).

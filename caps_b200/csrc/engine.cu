@@ -178,15 +178,33 @@ void Engine::setup_ff(const caps_gpu_ff* ff) {
     const double* q = ff->pair_func_p + 5 * k;
     const int form = int(q[0]);
     if (a < 0 || b < 0 || a >= nt_ || b >= nt_) throw ModelError(CAPS_GPU_EINVAL, "a pair form refers to a type out of range");
-    if (form != 1 && form != 2 && form != 3)
-      throw ModelError(CAPS_GPU_EFIELD, "the device path takes the Buckingham, Morse and Rydberg pair forms (tabulated, cosine-squared, lj/gromacs and SDK "
-                                        "pairs stay on the reference's CPU path)");
+    if (!(form == 1 || form == 2 || form == 3 || (form >= 11 && form <= 14) || form == 20 || form == 31 || form == 32 || form == 40))
+      throw ModelError(CAPS_GPU_EFIELD, "unknown pair form " + std::to_string(form));
+    if (form == 40 && (q[1] < 0 || int(q[1]) >= ff->ntables)) throw ModelError(CAPS_GPU_EFIELD, "a tabulated pair refers to a table that is not there");
     for (const size_t tp : {size_t(a) * nt_ + b, size_t(b) * nt_ + a}) {
       h_form_[tp] = form;
       h_pa_[tp] = q[1], h_pb_[tp] = q[2], h_pc_[tp] = q[3];
       h_prc2_[tp] = q[4] * q[4];
     }
     generic_ = true;
+  }
+  lj_inner_ = ff->lj_inner;
+  // the tabulated pairs (ForceField::tables), one after another
+  h_toff_.assign(1, 0);
+  h_tr0dr_.clear(), h_te_.clear(), h_tf_.clear();
+  for (int k = 0; k < ff->ntables; ++k) {
+    const int m = ff->table_n[k];
+    h_tr0dr_.push_back(ff->table_r0_dr[2 * k]);
+    h_tr0dr_.push_back(ff->table_r0_dr[2 * k + 1]);
+    h_te_.insert(h_te_.end(), ff->table_e + h_toff_.back(), ff->table_e + h_toff_.back() + m);
+    h_tf_.insert(h_tf_.end(), ff->table_f + h_toff_.back(), ff->table_f + h_toff_.back() + m);
+    h_toff_.push_back(h_toff_.back() + m);
+  }
+  d_toff_.upload(h_toff_, stream_);
+  if (!h_tr0dr_.empty()) d_tr0dr_.upload(h_tr0dr_, stream_);
+  if (!h_te_.empty()) {
+    d_te_.upload(h_te_, stream_);
+    d_tf_.upload(h_tf_, stream_);
   }
   type_count_.assign(size_t(nt_), 0.0);
   for (int t : h_type_) type_count_[size_t(t)] += 1;
@@ -310,6 +328,12 @@ static double generic_pair_energy(int form, double pa, double pb, double pc, dou
   const double r = std::sqrt(r2);
   if (form == 1) return pa * std::exp(-r / pb) - pc / (r2 * r2 * r2);
   if (form == 3) return (pa + pc * r) * std::exp(-r / pb);
+  if (form >= 11 && form <= 14) {   // SDK (field.cpp:1443-1448)
+    static const double pw1[] = {9, 12, 12, 12}, pw2[] = {6, 4, 6, 5}, pre[] = {6.75, 2.59807621135332, 4.0, 3.20377984125109};
+    const int k = form - 11;
+    const double sr2 = pb * pb / r2, sm = std::pow(sr2, pw1[k] / 2), sn = std::pow(sr2, pw2[k] / 2), c = pre[k] * pa;
+    return c * (sm - sn);
+  }
   const double e1 = std::exp(-pb * (r - pc));
   return pa * (e1 * e1 - 2 * e1);
 }
@@ -387,24 +411,43 @@ void Engine::setup_options() {
     }
   // generic forms: no LJ part; the shift is the form's energy at the pair's own cut-off, or at r_c, unless the tail
   // correction is on (field.cpp:1482-1492)
+  // lj/gromacs: the switch coefficients for the cut-off in use (field.cpp:528-547); their constant g4 is the pair's
+  // (negative) shift, and the cut-off shift is none by construction, as for the cosine-squared and tabulated forms
   std::vector<double4> tabg(size_t(ntab) * ntab, make_double4(0, 0, 0, 0)), l14g(size_t(nt_) * nt_, make_double4(0, 0, 0, 0));
+  std::vector<double4> tabg2(size_t(ntab) * ntab, make_double4(0, 0, 0, 0)), l14g2(size_t(nt_) * nt_, make_double4(0, 0, 0, 0));
   for (int a0 = 0; a0 < nt_ && generic_; ++a0)
     for (int b0 = 0; b0 < nt_; ++b0) {
       const size_t tp = size_t(a0) * nt_ + b0;
       const int form = h_form_[tp];
       if (!form) continue;
       double sh = 0;
-      if (shifted_) {
+      double4 g2 = make_double4(0, 0, 0, 0);
+      if (form == 20) {
+        const double rc = rc_, r1 = lj_inner_;
+        if (r1 <= 0 || r1 >= rc) throw ModelError(CAPS_GPU_EFIELD, "lj/gromacs needs an inner radius below the cut-off");
+        const double e = h_pa_[tp], sg = h_pb_[tp], s6 = std::pow(sg, 6), s12 = s6 * s6;
+        const double l1 = 48 * e * s12, l2 = 24 * e * s6, l3 = 4 * e * s12, l4 = 4 * e * s6;
+        const double r6i = 1 / std::pow(rc, 6), r8i = 1 / std::pow(rc, 8), tt = rc - r1, t2i = 1 / (tt * tt), t3i = t2i / tt, t3 = tt * tt * tt;
+        const double a6 = (7 * r1 - 10 * rc) * r8i * t2i, b6 = (9 * rc - 7 * r1) * r8i * t3i;
+        const double a12 = (13 * r1 - 16 * rc) * r6i * r8i * t2i, b12 = (15 * rc - 13 * r1) * r6i * r8i * t3i;
+        const double c6 = r6i - t3 * (6 * a6 / 3 + 6 * b6 * tt / 4), c12 = r6i * r6i - t3 * (12 * a12 / 3 + 12 * b12 * tt / 4);
+        g2 = make_double4(l1 * a12 - l2 * a6, l1 * b12 - l2 * b6, -l3 * 12 * a12 / 3 + l4 * 6 * a6 / 3, -l3 * 12 * b12 / 4 + l4 * 6 * b6 / 4);
+        sh = -(-l3 * c12 + l4 * c6);
+      } else if (shifted_ && form != 31 && form != 32 && form != 40) {
         const double r2 = h_prc2_[tp] > 0 ? std::min(h_prc2_[tp], rc2) : rc2;
         sh = generic_pair_energy(form, h_pa_[tp], h_pb_[tp], h_pc_[tp], r2);
       }
       tabd[size_t(a0) * ntab + b0] = make_double4(0.0, 0.0, sh, double(form));
       tabg[size_t(a0) * ntab + b0] = make_double4(h_pa_[tp], h_pb_[tp], h_pc_[tp], h_prc2_[tp]);
+      tabg2[size_t(a0) * ntab + b0] = g2;
       l14[tp] = make_double4(1.0, 0.0, sh, double(form));
       l14g[tp] = tabg[size_t(a0) * ntab + b0];
+      l14g2[tp] = g2;
     }
   d_tabg_.upload(tabg, stream_);
   d_lj14g_.upload(l14g, stream_);
+  d_tabg2_.upload(tabg2, stream_);
+  d_lj14g2_.upload(l14g2, stream_);
   d_tab_.upload(tab, stream_);
   // geometric mixing (c6_ab = sqrt(c6_aa c6_bb) and the same for c12, as OPLS-style force fields give): the FP32 pair
   // kernel takes per-type factors instead of the per-pair table (12-6 only)
@@ -710,6 +753,13 @@ void Engine::host_constants(caps_gpu_terms* t, bool ener, bool vir) const {
           continue;
         }
         if (h_form_[tp] == 2 || h_form_[tp] == 3) continue;   // Morse, Rydberg: no tail term
+        if (h_form_[tp] == 13) {   // a 12-6 SDK pair: its own 12-6 tail (field.cpp:2516-2521)
+          const double e6 = h_pa_[tp], sg6 = std::pow(h_pb_[tp], 6), sg12 = sg6 * sg6;
+          et += nn * 2 * kPi * 4 * e6 * (sg12 / (9 * rc9) - sg6 / (3 * rc3));
+          wt += nn * 2 * kPi * 4 * e6 * (4 * sg12 / (3 * rc9) - 2 * sg6 / rc3);
+          continue;
+        }
+        if (h_form_[tp] >= 11) continue;   // the other SDK forms, lj/gromacs, cosine-squared, tables: none
         if (lj96_) {   // lj/class2 (field.cpp:2523-2529)
           const double s3 = std::sqrt(s6), rc6 = rc3 * rc3;
           et += nn * 2 * kPi * eps * s6 * (s3 - 3 * rc3) / (3 * rc6);

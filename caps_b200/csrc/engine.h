@@ -245,7 +245,13 @@ class Engine {
   std::vector<int> h_form_;
   std::vector<double> h_pa_, h_pb_, h_pc_, h_prc2_;
   bool generic_ = false;
-  DevBuf<double4> d_tabg_, d_lj14g_;
+  DevBuf<double4> d_tabg_, d_lj14g_, d_tabg2_, d_lj14g2_;
+  double lj_inner_ = 0;
+  DevBuf<int> d_toff_;
+  DevBuf<double> d_tr0dr_, d_te_, d_tf_;
+  std::vector<int> h_toff_;   // the tabulated pairs on the host (shift and bounds)
+  std::vector<double> h_tr0dr_, h_te_, h_tf_;
+  PairTables pair_tables() const { return PairTables{d_toff_.p, d_tr0dr_.p, d_te_.p, d_tf_.p}; }
   DevBuf<double> d_gtab_;
   int gnodes_ = 0;
   double ghi_ = 0;

@@ -182,6 +182,9 @@ PairArgs Engine::pair_args() {
   A.tabd = d_tabd_.p;
   A.tabcap = d_tabcap_.p;
   A.tabg = d_tabg_.p;
+  A.tabg2 = d_tabg2_.p;
+  A.lj_inner = lj_inner_;
+  A.tables = pair_tables();
   A.gtab = d_gtab_.p;
   A.ntab = nt_ + 1;
   A.gnodes = coul_ ? gnodes_ : 0;   // a table only with Coulomb: the FP64 kernel's shared memory holds it then

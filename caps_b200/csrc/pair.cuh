@@ -103,6 +103,9 @@ struct PairArgs {
   const double4* tabd;   // FP64: per type pair (c6, c12, energy shift, 0)
   const double4* tabcap; // FP64 with a force cap: per type pair (r_cap^2, E at r_cap, |F| at r_cap, 0)
   const double4* tabg;   // FP64 generic forms (tabd.w the form): per type pair (a, b, c, the pair's own cut-off^2)
+  const double4* tabg2;  // and the lj/gromacs switch coefficients
+  double lj_inner;
+  PairTables tables;
   const double* gtab;    // FP64 Ewald table: 2 per node (G, h dG/ds)
   int ntab;              // types incl. the padding type
   int gnodes;            // table nodes
@@ -581,7 +584,7 @@ static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
             // a generic form (field.cpp:1381-1396), nothing beyond the pair's own cut-off (and no shift there)
             const double4 g = A.tabg[ti * A.ntab + tj];
             double e = 0;
-            fr = (g.w > 0 && r2 > g.w) ? 0.0 : generic_pair(int(cc.w), g.x, g.y, g.z, r2, e);
+            fr = (g.w > 0 && r2 > g.w) ? 0.0 : generic_pair(int(cc.w), g, A.tabg2[ti * A.ntab + tj], A.lj_inner, A.tables, r2, e);
             if (ENER && !(g.w > 0 && r2 > g.w)) ev += e - cc.z;
           } else {
             if (LJ96) {   // field.cpp:1658-1661

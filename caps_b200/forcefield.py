@@ -59,6 +59,8 @@ class ForceField:
     # ForceField::pair_func (field.hpp:68, 174): {(a, b): (form, a, b, c, rc)} with form "buckingham" (A, rho, C),
     # "morse" (D, alpha, r0) or "rydberg" (A, rho, C), or their codes 1, 2, 3; rc > 0 the pair's own cut-off
     pair_func: dict | None = None
+    lj_inner: float = 0.0                  # ForceField::lj_inner: where the lj/gromacs switch starts (Å)
+    tables: list | None = None             # ForceField::tables: [(r0, dr, e[], f[])], pair_func form "table" (a = index)
 
     def __post_init__(self):
         self.type_index = np.ascontiguousarray(np.asarray(self.type_index, dtype=np.int32))
@@ -130,19 +132,27 @@ class ForceField:
             raise ValueError(f"unknown pair form '{self.pair_form}' (lj12-6, lj9-6)")
         s.lj_form = 1 if self.pair_form == "lj9-6" else 0
         if self.pair_func:
-            forms = {"buckingham": 1, "buck": 1, "morse": 2, "rydberg": 3}
+            forms = {"buckingham": 1, "buck": 1, "morse": 2, "rydberg": 3, "sdk9-6": 11, "sdk12-4": 12, "sdk12-6": 13, "sdk12-5": 14,
+                     "lj/gromacs": 20, "cos2": 31, "cos2-wca": 32, "table": 40}
             ab, par = [], []
             for (a, b), spec in sorted(self.pair_func.items()):
                 form, pa, pb, pc = spec[:4]
                 rc = spec[4] if len(spec) > 4 else 0.0
                 code = forms.get(form.lower()) if isinstance(form, str) else int(form)
                 if code is None:
-                    raise ValueError(f"pair form {form!r} for types ({a}, {b}): the device path takes buckingham, morse and rydberg")
+                    raise ValueError(f"unknown pair form {form!r} for types ({a}, {b}) ({', '.join(forms)})")
                 ab += [min(a, b), max(a, b)]
                 par += [float(code), float(pa), float(pb), float(pc), float(rc)]
             s.npair_func = len(self.pair_func)
             s.pair_func_ab = ptr(np.asarray(ab, dtype=np.int32))
             s.pair_func_p = ptr(np.asarray(par, dtype=np.float64))
+        s.lj_inner = float(self.lj_inner)
+        if self.tables:
+            s.ntables = len(self.tables)
+            s.table_n = ptr(np.asarray([len(t[2]) for t in self.tables], dtype=np.int32))
+            s.table_r0_dr = ptr(np.asarray([[float(t[0]), float(t[1])] for t in self.tables], dtype=np.float64))
+            s.table_e = ptr(np.concatenate([np.asarray(t[2], dtype=np.float64) for t in self.tables]))
+            s.table_f = ptr(np.concatenate([np.asarray(t[3], dtype=np.float64) for t in self.tables]))
         return s, keep
 
     def arrays(self) -> dict:

@@ -92,6 +92,15 @@ typedef struct {
   int32_t npair_func;
   const int32_t* pair_func_ab;    /* [2*npair_func] */
   const double* pair_func_p;      /* [5*npair_func] form, a, b, c, rc */
+  /* forms 11-14 SDK C eps ((s/r)^m - (s/r)^n) (a eps, b sigma; 9-6, 12-4, 12-6, 12-5), 20 LJ 12-6 with GROMACS's force
+   * switch from lj_inner to the cut-off (a eps, b sigma), 31 / 32 cosine-squared attraction, 32 with WCA below sigma
+   * (a eps, b sigma, c its cut-off), 40 tabulated (a the table's index): the reference's codes (field.hpp:61-75) */
+  double lj_inner;                /* ForceField::lj_inner (Å): where the lj/gromacs switch starts */
+  int32_t ntables;                /* ForceField::tables (field.hpp:75-76, 175) */
+  const int32_t* table_n;         /* [ntables] points of each table */
+  const double* table_r0_dr;      /* [2*ntables] first point and spacing (Å) */
+  const double* table_e;          /* the tables' energies, one after another (kcal/mol) */
+  const double* table_f;          /* the tables' forces -dE/dr (kcal/mol/Å), the same layout */
 } caps_gpu_ff;
 
 /* caps::EnergyOptions (field.hpp:274-308), the fields the device path takes. */

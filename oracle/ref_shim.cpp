@@ -86,6 +86,16 @@ std::shared_ptr<ForceField> to_ff(const caps_gpu_ff* p) {
     f.a = q[1], f.b = q[2], f.c = q[3], f.rc = q[4];
     ff->pair_func[{p->pair_func_ab[2 * k], p->pair_func_ab[2 * k + 1]}] = f;
   }
+  ff->lj_inner = p->lj_inner;
+  for (int k = 0, off = 0; k < p->ntables; ++k) {
+    TabulatedPair tb;
+    tb.r0 = p->table_r0_dr[2 * k];
+    tb.dr = p->table_r0_dr[2 * k + 1];
+    tb.e.assign(p->table_e + off, p->table_e + off + p->table_n[k]);
+    tb.f.assign(p->table_f + off, p->table_f + off + p->table_n[k]);
+    off += p->table_n[k];
+    ff->tables.push_back(std::move(tb));
+  }
   ff->charge.assign(p->charge, p->charge + n);
   ff->mass.assign(p->mass, p->mass + n);
   for (int k = 0; k < p->nbonds; ++k) ff->bonds.push_back({p->bond_ij[2 * k], p->bond_ij[2 * k + 1], p->bond_k_r0[2 * k], p->bond_k_r0[2 * k + 1]});

@@ -1,5 +1,6 @@
-"""The generic FP64 pair forms (ForceField::pair_func: Buckingham, Morse, Rydberg, each with an optional cut-off of its
-own; field.cpp:478-487, 1381-1396, 1482-1492, 2508-2515) on the device against the reference core (oracle/_ref) on
+"""The generic FP64 pair forms (ForceField::pair_func: Buckingham, Morse, Rydberg, SDK, lj/gromacs, cosine-squared with
+and without WCA, tabulated; each with an optional cut-off of its own; field.cpp:478-487, 528-555, 1381-1455, 1482-1492,
+2508-2522) on the device against the reference core (oracle/_ref) on
 the same cells: energies, virial and forces at the FP64 bar (1e-12), with the cut-off shift or the tail correction,
 in the non-bonded pairs and the 1-4 pairs, under PME and damped shifted force. A force field with any of them runs the
 FP64 path whatever precision is asked for, as the reference's mixed path falls back to its FP64 pair loop."""
@@ -31,13 +32,31 @@ FORMS = {
 }
 
 
+def _table():
+    """A tabulated H-H pair from 1.5 Å by 0.01 Å (700 points): a 12-6 well at 2.5 Å and its force -dE/dr."""
+    r = 1.5 + 0.01 * np.arange(700)
+    e = 0.02 * ((2.5 / r) ** 12 - 2 * (2.5 / r) ** 6)
+    f = 0.02 * (12 * 2.5 ** 12 / r ** 13 - 12 * 2.5 ** 6 / r ** 7)
+    return (1.5, 0.01, e, f)
+
+
+# the coarse-grained forms on the polystyrene cell: SDK, lj/gromacs, cosine-squared (with and without WCA), a table
+CG = {(0, 0): ("sdk12-4", 0.1, 3.2), (0, 2): ("sdk9-6", 0.05, 2.9), (0, 3): ("sdk12-6", 0.04, 2.9), (1, 2): ("sdk12-5", 0.05, 3.0),
+      (1, 3): ("lj/gromacs", 0.03, 2.6), (2, 2): ("cos2", 0.05, 2.5, 5.0), (2, 3): ("cos2-wca", 0.04, 2.6, 4.5),
+      (3, 3): ("table", 0, 0, 0)}
+
+
 def _ff(name):
+    if name == "ps_cg":   # every spec as (form, a, b, c)
+        fx = load("ps_small")
+        return fx, dataclasses.replace(fx.ff, pair_func={k: v + (0.0,) * (4 - len(v)) for k, v in CG.items()}, lj_inner=6.0, tables=[_table()])
     fx = load(name)
     return fx, dataclasses.replace(fx.ff, pair_func=FORMS[name])
 
 
 @pytest.mark.parametrize("name,elec,tail", [("ps_small", "pme", False), ("ps_small", "pme", True), ("ps_small", "dsf", False),
-                                            ("lj_triclinic", "dsf", False), ("lj_triclinic", "dsf", True)])
+                                            ("lj_triclinic", "dsf", False), ("lj_triclinic", "dsf", True),
+                                            ("ps_cg", "pme", False), ("ps_cg", "dsf", True)])
 def test_fp64_pair_forms_match_reference(name, elec, tail):
     ref = _ref()
     fx, ff = _ff(name)
@@ -66,8 +85,11 @@ def test_pair_forms_run_fp64_when_mixed_is_asked():
 
 def test_unsupported_pair_form_is_refused():
     fx = load("ps_small")
-    with pytest.raises(ValueError, match="buckingham, morse and rydberg"):
-        dataclasses.replace(fx.ff, pair_func={(0, 0): ("table", 0, 0, 0)}).to_struct()
-    ff = dataclasses.replace(fx.ff, pair_func={(0, 0): (20, 0.1, 3.4, 0.0)})   # lj/gromacs by its code
-    with pytest.raises(Exception, match="Buckingham, Morse and Rydberg"):
-        Evaluator(ff, EnergyOptions(precision="double"))
+    with pytest.raises(ValueError, match="unknown pair form"):
+        dataclasses.replace(fx.ff, pair_func={(0, 0): ("soft", 0, 0, 0)}).to_struct()
+    with pytest.raises(Exception, match="unknown pair form 99"):
+        Evaluator(dataclasses.replace(fx.ff, pair_func={(0, 0): (99, 0.1, 3.4, 0.0)}), EnergyOptions(precision="double"))
+    with pytest.raises(Exception, match="a table that is not there"):
+        Evaluator(dataclasses.replace(fx.ff, pair_func={(0, 0): ("table", 2, 0, 0)}), EnergyOptions(precision="double"))
+    with pytest.raises(Exception, match="inner radius below the cut-off"):
+        Evaluator(dataclasses.replace(fx.ff, pair_func={(0, 0): ("lj/gromacs", 0.1, 3.4, 0.0)}), EnergyOptions(precision="double"))
