@@ -29,7 +29,7 @@ class FF(C.Structure):
         ("lj_shift", C.c_int32), ("model_cutoff", C.c_double), ("lj_form", C.c_int32),
         # ABI 5
         ("npair_func", C.c_int32), ("pair_func_ab", C.c_void_p), ("pair_func_p", C.c_void_p),
-        ("lj_inner", C.c_double), ("ntables", C.c_int32), ("table_n", C.c_void_p), ("table_r0_dr", C.c_void_p),
+        ("lj_inner", C.c_double), ("lj_fsw", C.c_int32), ("ntables", C.c_int32), ("table_n", C.c_void_p), ("table_r0_dr", C.c_void_p),
         ("table_e", C.c_void_p), ("table_f", C.c_void_p),
     ]
 

@@ -44,6 +44,7 @@ void Engine::bonded_forces(const double* d_x, bool ener, bool vir, int parts) {
   W.fene_ij = d_fene_ij_.p, W.fene_p = d_fene_p_.p, W.counters = d_counters_.p, W.info = d_errinfo_.p;
   W.p14_ij = d_p14_ij_.p, W.p14_scale = p14_scaled_ ? d_p14_scale_.p : nullptr, W.lj14 = lj14_, W.type = d_type_.p, W.nt = nt_;
   W.lj14g_tab = d_lj14g_.p, W.lj14g2_tab = d_lj14g2_.p, W.lj_inner = lj_inner_, W.tables = pair_tables();
+  W.lj_fsw = lj_fsw_ && !lj96_ ? 1 : 0, W.rc = rc_;
   W.lj14_tab = d_lj14_.p, W.cap14_tab = opt_.force_cap > 0 ? (const double4*)d_cap14_.p : (const double4*)nullptr, W.lj96 = lj96_ ? 1 : 0;
   W.X = ExclArgs{d_excl_ij_.p, d_excl_f_.p, d_q_.p, d_gtab_.p, ghi_, rc_, rc_ * rc_, kappa_, dsf_e0_, dsf_f0_, pme_ ? 1 : 0};
   auto run = [&](auto sink) {

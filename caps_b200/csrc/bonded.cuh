@@ -203,7 +203,7 @@ __device__ __forceinline__ void torsions_body(int blk, int nblk, int ngroups, co
 template <class R, class S, bool ENER, bool VIR>
 __device__ __forceinline__ void pairs14_body(int blk, int nblk, int np, const uint32_t* __restrict__ ij, const double* __restrict__ scale, double lj14, const int* __restrict__ type, int nt,
                           const double4* __restrict__ lj, const double4* __restrict__ cap, const double4* __restrict__ gen, const double4* __restrict__ gen2,
-                          double r1, PairTables tabs, BondedArgs A, S F, int lj96) {
+                          double r1, PairTables tabs, BondedArgs A, S F, int lj96, int fsw, double rc) {
   Tally<VIR> T(A.fixed != 0);
   for (int t = blk * blockDim.x + threadIdx.x; t < np; t += nblk * blockDim.x) {
     const int i = int(ij[2 * t]), j = int(ij[2 * t + 1]);
@@ -228,6 +228,11 @@ __device__ __forceinline__ void pairs14_body(int blk, int nblk, int np, const ui
       const R r = rsq(r2), rcp = rsq(R(cp.x));
       ev = sc * (R(cp.y) + R(cp.z) * (rcp - r));
       fr = sc * R(cp.z) / r;
+    } else if (fsw) {   // CHARMM's force switch (the 1-4 pairs take it as the others, field.cpp:2033)
+      double e = 0;
+      const double f = charmm_fsw(4 * c.x * c.y * c.y, 4 * c.x * c.y, r1, rc, double(r2), e, true);
+      ev = R(double(sc) * e);
+      fr = R(double(sc) * f);
     } else {
       const R q = R(c.y) / (r2 * r2 * r2);
       if (lj96) {
@@ -378,7 +383,8 @@ struct BondedWork {
   const int* type;
   int nt, lj96;
   const double4 *lj14_tab, *cap14_tab, *lj14g_tab, *lj14g2_tab;
-  double lj_inner;
+  double lj_inner, rc;
+  int lj_fsw;
   PairTables tables;
   ExclArgs X;
 };
@@ -399,7 +405,7 @@ static __global__ void __launch_bounds__(256) k_bonded(BondedWork W, BondedArgs 
       break;
     case kBkFene: fene_body<R, S, ENER, VIR>(blk, nblk, W.nf, W.fene_ij, W.fene_p, A, F, W.counters, W.info); break;
     case kBkPairs14:
-      pairs14_body<R, S, ENER, VIR>(blk, nblk, W.np14, W.p14_ij, W.p14_scale, W.lj14, W.type, W.nt, W.lj14_tab, W.cap14_tab, W.lj14g_tab, W.lj14g2_tab, W.lj_inner, W.tables, A, F, W.lj96);
+      pairs14_body<R, S, ENER, VIR>(blk, nblk, W.np14, W.p14_ij, W.p14_scale, W.lj14, W.type, W.nt, W.lj14_tab, W.cap14_tab, W.lj14g_tab, W.lj14g2_tab, W.lj_inner, W.tables, A, F, W.lj96, W.lj_fsw, W.rc);
       break;
     default: excl_body<S, ENER, VIR>(blk, nblk, W.nx, W.X, A, F); break;
   }

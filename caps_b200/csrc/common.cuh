@@ -47,6 +47,21 @@ enum ErrInfo { kInfoFeneBond = 0, kInfoFeneR, kInfoNonFiniteStep, kInfoNum = 4 }
 // 1 Buckingham A e^(-r/rho) - C/r^6 (a A, b rho, c C); 2 Morse D (e^(-2 alpha (r - r0)) - 2 e^(-alpha (r - r0))) (a D,
 // b alpha, c r0); 3 Rydberg (A + C r) e^(-r/rho) (a A, b rho, c C); 11-14 SDK C eps ((s/r)^m - (s/r)^n) (a eps, b
 // sigma); 20 lj/gromacs (a eps, b sigma); 31 / 32 cosine-squared, 32 with WCA (a eps, b sigma, c cut-off); 40 a table.
+// CHARMM's force switch on a 12-6 pair (field.cpp:1455-1469; A = 4 eps s^12, B = 4 eps s^6): below r_in the plain 12-6
+// plus a constant, between r_in and r_c E = A k12 (r^-6 - r_c^-6)^2 - B k6 (r^-3 - r_c^-3)^2; returns -(dE/dr)/r, adds
+// E to e when ener.
+__device__ __forceinline__ double charmm_fsw(double A, double B, double ri, double rc, double r2, double& e, bool ener) {
+  const double ri3 = ri * ri * ri, rc2 = rc * rc, rc3 = rc2 * rc, ri6 = ri3 * ri3, rc6 = rc3 * rc3, r6i = 1 / (r2 * r2 * r2);
+  if (r2 <= ri * ri) {
+    if (ener) e += A * (r6i * r6i - 1 / (ri6 * rc6)) - B * (r6i - 1 / (ri3 * rc3));
+    return (12 * A * r6i * r6i - 6 * B * r6i) / r2;
+  }
+  const double r3i = 1 / (r2 * sqrt(r2)), k12 = rc6 / (rc6 - ri6), k6 = rc3 / (rc3 - ri3);
+  const double u = r6i - 1 / rc6, w = r3i - 1 / rc3;
+  if (ener) e += A * k12 * u * u - B * k6 * w * w;
+  return (12 * A * k12 * u * r6i - 6 * B * k6 * w * r3i) / r2;
+}
+
 struct PairTables {
   const int* off;        // [ntables + 1] first point of each table
   const double* r0dr;    // [2 ntables]

@@ -189,6 +189,7 @@ void Engine::setup_ff(const caps_gpu_ff* ff) {
     generic_ = true;
   }
   lj_inner_ = ff->lj_inner;
+  lj_fsw_ = ff->lj_fsw != 0;
   // the tabulated pairs (ForceField::tables), one after another
   h_toff_.assign(1, 0);
   h_tr0dr_.clear(), h_te_.clear(), h_tf_.clear();
@@ -344,13 +345,14 @@ void Engine::setup_options() {
   if (!(rc_ > 0) || skin_ < 0) throw ModelError(CAPS_GPU_EINVAL, "cut-off must be positive and skin non-negative");
   // a force field with generic pair forms runs the FP64 path, as the reference's mixed path falls back to its FP64
   // pair loop for them (field.cpp:848)
-  mixed_ = opt_.precision == 0 && !generic_;
-  tail_ = opt_.tail != 0 && !lj_shift_model_;
+  mixed_ = opt_.precision == 0 && !generic_ && !lj_fsw_;
+  tail_ = opt_.tail != 0 && !lj_shift_model_ && !lj_fsw_;   // CHARMM: switched to zero at the cut-off, no tail (field.cpp:440-443)
   shifted_ = !tail_;
   coul_ = opt_.coulomb != 0;
   pme_ = coul_ && opt_.electrostatics == 1;
   order_ = opt_.pme_order;
   if (pme_ && (order_ < 3 || order_ > kMaxOrder)) throw ModelError(CAPS_GPU_EINVAL, "PME order must be 3..8");
+  if (lj_fsw_ && (lj_inner_ <= 0 || lj_inner_ >= rc_)) throw ModelError(CAPS_GPU_EFIELD, "the CHARMM force switch needs an inner radius below the cut-off");
   if (opt_.force_cap > 0 && mixed_) throw ModelError(CAPS_GPU_EINVAL, "a force cap runs on the FP64 path (as the reference's push-off)");
   beta_ = pme_ ? ewald_beta(rc_, opt_.ewald_rtol) : 0.0;
   const double a = opt_.dsf_alpha;
@@ -404,7 +406,7 @@ void Engine::setup_options() {
       const double c6 = eps > 0 ? (lj96_ ? 3 : 4) * eps * s6 : 0.0;
       const double c12 = eps > 0 ? (lj96_ ? 2 * eps * s6 * std::sqrt(s6) : 4 * eps * s6 * s6) : 0.0;
       const double qc = s6 / (rc2 * rc2 * rc2);
-      const double sh = shifted_ && eps > 0 ? (lj96_ ? eps * (2 * qc * std::sqrt(qc) - 3 * qc) : 4 * eps * (qc * qc - qc)) : 0.0;
+      const double sh = shifted_ && eps > 0 && !(lj_fsw_ && !lj96_) ? (lj96_ ? eps * (2 * qc * std::sqrt(qc) - 3 * qc) : 4 * eps * (qc * qc - qc)) : 0.0;
       tab[size_t(a0) * ntab + b0] = make_float4(float(c6), float(c12), float(sh), 0.f);
       tabd[size_t(a0) * ntab + b0] = make_double4(c6, c12, sh, 0.0);
       l14[size_t(a0) * nt_ + b0] = make_double4(eps, s6, sh, 0.0);

@@ -247,6 +247,7 @@ class Engine {
   bool generic_ = false;
   DevBuf<double4> d_tabg_, d_lj14g_, d_tabg2_, d_lj14g2_;
   double lj_inner_ = 0;
+  bool lj_fsw_ = false;   // CHARMM's force switch on every 12-6 pair (FP64 path)
   DevBuf<int> d_toff_;
   DevBuf<double> d_tr0dr_, d_te_, d_tf_;
   std::vector<int> h_toff_;   // the tabulated pairs on the host (shift and bounds)

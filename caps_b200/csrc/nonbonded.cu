@@ -184,6 +184,7 @@ PairArgs Engine::pair_args() {
   A.tabg = d_tabg_.p;
   A.tabg2 = d_tabg2_.p;
   A.lj_inner = lj_inner_;
+  A.lj_fsw = lj_fsw_ && !lj96_ ? 1 : 0;
   A.tables = pair_tables();
   A.gtab = d_gtab_.p;
   A.ntab = nt_ + 1;

@@ -105,6 +105,7 @@ struct PairArgs {
   const double4* tabg;   // FP64 generic forms (tabd.w the form): per type pair (a, b, c, the pair's own cut-off^2)
   const double4* tabg2;  // and the lj/gromacs switch coefficients
   double lj_inner;
+  int lj_fsw;            // FP64: CHARMM's force switch on the 12-6 pairs
   PairTables tables;
   const double* gtab;    // FP64 Ewald table: 2 per node (G, h dG/ds)
   int ntab;              // types incl. the padding type
@@ -591,6 +592,8 @@ static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
               const double r9i = r6i * r2i * rinv;
               fr = (9 * cc.y * r9i - 6 * cc.x * r6i) * r2i;
               if (ENER) ev += cc.y * r9i - cc.x * r6i - cc.z;
+            } else if (A.lj_fsw) {
+              fr = charmm_fsw(cc.y, cc.x, A.lj_inner, A.rc, r2, ev, ENER);
             } else {
               fr = r6i * (12 * cc.y * r6i - 6 * cc.x) * r2i;
               if (ENER) ev += r6i * (cc.y * r6i - cc.x) - cc.z;

@@ -59,7 +59,8 @@ class ForceField:
     # ForceField::pair_func (field.hpp:68, 174): {(a, b): (form, a, b, c, rc)} with form "buckingham" (A, rho, C),
     # "morse" (D, alpha, r0) or "rydberg" (A, rho, C), or their codes 1, 2, 3; rc > 0 the pair's own cut-off
     pair_func: dict | None = None
-    lj_inner: float = 0.0                  # ForceField::lj_inner: where the lj/gromacs switch starts (Å)
+    lj_inner: float = 0.0                  # ForceField::lj_inner: where the lj/gromacs and CHARMM switches start (Å)
+    lj_fsw: bool = False                   # ForceField::lj_fsw: CHARMM's force switch on every 12-6 pair
     tables: list | None = None             # ForceField::tables: [(r0, dr, e[], f[])], pair_func form "table" (a = index)
 
     def __post_init__(self):
@@ -147,6 +148,7 @@ class ForceField:
             s.pair_func_ab = ptr(np.asarray(ab, dtype=np.int32))
             s.pair_func_p = ptr(np.asarray(par, dtype=np.float64))
         s.lj_inner = float(self.lj_inner)
+        s.lj_fsw = int(bool(self.lj_fsw))
         if self.tables:
             s.ntables = len(self.tables)
             s.table_n = ptr(np.asarray([len(t[2]) for t in self.tables], dtype=np.int32))

@@ -95,7 +95,9 @@ typedef struct {
   /* forms 11-14 SDK C eps ((s/r)^m - (s/r)^n) (a eps, b sigma; 9-6, 12-4, 12-6, 12-5), 20 LJ 12-6 with GROMACS's force
    * switch from lj_inner to the cut-off (a eps, b sigma), 31 / 32 cosine-squared attraction, 32 with WCA below sigma
    * (a eps, b sigma, c its cut-off), 40 tabulated (a the table's index): the reference's codes (field.hpp:61-75) */
-  double lj_inner;                /* ForceField::lj_inner (Å): where the lj/gromacs switch starts */
+  double lj_inner;                /* ForceField::lj_inner (Å): where the lj/gromacs and CHARMM switches start */
+  int32_t lj_fsw;                 /* ForceField::lj_fsw: every 12-6 pair with CHARMM's force switch from lj_inner to the cut-off
+                                   * (field.cpp:1455-1469), no shift and no tail; runs the FP64 path */
   int32_t ntables;                /* ForceField::tables (field.hpp:75-76, 175) */
   const int32_t* table_n;         /* [ntables] points of each table */
   const double* table_r0_dr;      /* [2*ntables] first point and spacing (Å) */

@@ -87,6 +87,7 @@ std::shared_ptr<ForceField> to_ff(const caps_gpu_ff* p) {
     ff->pair_func[{p->pair_func_ab[2 * k], p->pair_func_ab[2 * k + 1]}] = f;
   }
   ff->lj_inner = p->lj_inner;
+  ff->lj_fsw = p->lj_fsw != 0;
   for (int k = 0, off = 0; k < p->ntables; ++k) {
     TabulatedPair tb;
     tb.r0 = p->table_r0_dr[2 * k];

@@ -93,3 +93,23 @@ def test_unsupported_pair_form_is_refused():
         Evaluator(dataclasses.replace(fx.ff, pair_func={(0, 0): ("table", 2, 0, 0)}), EnergyOptions(precision="double"))
     with pytest.raises(Exception, match="inner radius below the cut-off"):
         Evaluator(dataclasses.replace(fx.ff, pair_func={(0, 0): ("lj/gromacs", 0.1, 3.4, 0.0)}), EnergyOptions(precision="double"))
+
+
+@pytest.mark.parametrize("name,elec", [("ps_small", "pme"), ("ps_small", "dsf"), ("lj_triclinic", "dsf")])
+def test_fp64_charmm_force_switch_matches_reference(name, elec):
+    """ForceField::lj_fsw: every 12-6 pair (the 1-4 pairs too) switched from lj_inner to the cut-off, no shift and no
+    tail (field.cpp:440-443, 1455-1469, 2033); the FP64 path whatever precision is asked for."""
+    ref = _ref()
+    fx = load(name)
+    ff = dataclasses.replace(fx.ff, lj_fsw=True, lj_inner=6.5)
+    for prec in ("double", "mixed"):
+        eo = EnergyOptions(cutoff=8.0, skin=2.0, electrostatics=elec, pme_order=5, tail=True, precision=prec)
+        t, f = Evaluator(ff, eo).compute(fx.x, fx.cell)
+        rt, rf = ref.compute(ff, eo, fx.x, fx.cell)
+        for k in TERMS:
+            assert abs(t[k] - rt[k]) <= 1e-12 * abs(rt[k]) + 1e-9, (prec, k, t[k], rt[k])
+        assert abs(t["virial"] - rt["virial"]) <= 1e-11 * abs(rt["virial"]) + 1e-8
+        assert t["tail_energy"] == 0.0
+        assert rel_rms(f, rf) <= 1e-12
+    with pytest.raises(Exception, match="inner radius below the cut-off"):
+        Evaluator(dataclasses.replace(fx.ff, lj_fsw=True, lj_inner=9.0), EnergyOptions(cutoff=8.0, precision="double"))
