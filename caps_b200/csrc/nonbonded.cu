@@ -292,8 +292,9 @@ void Engine::pair_forces(bool ener, bool vir) {
       if (coul == 1) PAIR64FROZEN(1);
       else if (coul == 2) PAIR64FROZEN(2);
       else PAIR64FROZEN(0);
-    } else if (opt_.force_cap > 0) {
-      // push-off: energies and virial always on (a rare path, kept to one instantiation per Coulomb form)
+    } else if (opt_.force_cap > 0 || generic_ || lj_fsw_) {
+      // the push-off cap, the generic pair forms and CHARMM's force switch: energies and virial always on (rare paths,
+      // kept to one instantiation per Coulomb form, so the plain kernels carry none of their branches)
       if (coul == 1) PAIR64(1, true, true, true);
       else if (coul == 2) PAIR64(2, true, true, true);
       else PAIR64(0, true, true, true);

@@ -497,6 +497,8 @@ __device__ __forceinline__ double erfc_exp_as(double x, double& ex2) {
 
 // FROZEN: the pairs are those of the frozen set (A.frozen), whatever their distance now (field.cpp:1700); one beyond
 // the cut-off takes the closed-form Coulomb term (field.cpp:1759-1768).
+// CAP: the rare forms' variant (the push-off force cap, the generic pair forms, CHARMM's force switch), taken with energies
+// and virial on; the plain variants carry none of their branches.
 template <int COUL, bool ENER, bool VIR, bool CAP = false, bool LJ96 = false, bool FROZEN = false>
 static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
   extern __shared__ double4 smem_d4[];
@@ -581,7 +583,7 @@ static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
             const double r = r2 * rinv, rcp = sqrt(cp.x);
             fr = cp.z * rinv;   // F / r with |F| = the cap
             if (ENER) ev += cp.y + cp.z * (rcp - r) - cc.z;
-          } else if (cc.w != 0) {
+          } else if ((CAP || FROZEN) && cc.w != 0) {
             // a generic form (field.cpp:1381-1396), nothing beyond the pair's own cut-off (and no shift there)
             const double4 g = A.tabg[ti * A.ntab + tj];
             double e = 0;
@@ -592,7 +594,7 @@ static __global__ void __launch_bounds__(128, 2) k_pair_f64(PairArgs A) {
               const double r9i = r6i * r2i * rinv;
               fr = (9 * cc.y * r9i - 6 * cc.x * r6i) * r2i;
               if (ENER) ev += cc.y * r9i - cc.x * r6i - cc.z;
-            } else if (A.lj_fsw) {
+            } else if ((CAP || FROZEN) && A.lj_fsw) {
               fr = charmm_fsw(cc.y, cc.x, A.lj_inner, A.rc, r2, ev, ENER);
             } else {
               fr = r6i * (12 * cc.y * r6i - 6 * cc.x) * r2i;
