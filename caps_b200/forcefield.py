@@ -136,7 +136,7 @@ class ForceField:
             forms = {"buckingham": 1, "buck": 1, "morse": 2, "rydberg": 3, "sdk9-6": 11, "sdk12-4": 12, "sdk12-6": 13, "sdk12-5": 14,
                      "lj/gromacs": 20, "cos2": 31, "cos2-wca": 32, "table": 40}
             ab, par = [], []
-            for (a, b), spec in sorted(self.pair_func.items()):
+            for (a, b), spec in sorted(self.pair_func.items(), key=lambda kv: (min(kv[0]), max(kv[0]))):
                 form, pa, pb, pc = spec[:4]
                 rc = spec[4] if len(spec) > 4 else 0.0
                 code = forms.get(form.lower()) if isinstance(form, str) else int(form)

@@ -59,3 +59,25 @@ def test_constraint_algorithm_and_barostat_names():
     assert DynamicsOptions(barostat="mtk").to_struct(fx.ff, keep).barostat == 3
     with pytest.raises(ValueError, match="unknown barostat"):
         DynamicsOptions(barostat="andersen").to_struct(fx.ff, keep)
+
+
+def test_pair_forms_and_tables_map_to_the_c_struct():
+    """ForceField.pair_func and tables flatten into the ABI 5 fields: type pairs as (a <= b), the reference's form codes
+    (field.hpp:61-75), (form, a, b, c, rc) per entry, and the tables one after another."""
+    import ctypes as C
+    import dataclasses
+    import numpy as np
+    fx = load("ps_small")
+    tab = (1.5, 0.01, np.linspace(1.0, 0.0, 5), np.linspace(2.0, 0.0, 5))
+    ff = dataclasses.replace(fx.ff, pair_func={(1, 0): ("buckingham", 1.0, 0.3, 2.0), (2, 2): ("morse", 0.1, 1.2, 3.8, 6.5),
+                                               (3, 3): ("table", 0, 0, 0), (0, 3): (20, 0.03, 2.6, 0.0)},
+                             lj_inner=6.0, lj_fsw=True, tables=[tab, tab])
+    s, keep = ff.to_struct()
+    assert s.npair_func == 4 and s.ntables == 2 and s.lj_fsw == 1 and s.lj_inner == 6.0
+    ab = np.ctypeslib.as_array(C.cast(s.pair_func_ab, C.POINTER(C.c_int32)), shape=(8,)).reshape(4, 2)
+    p = np.ctypeslib.as_array(C.cast(s.pair_func_p, C.POINTER(C.c_double)), shape=(20,)).reshape(4, 5)
+    assert ab.tolist() == [[0, 1], [0, 3], [2, 2], [3, 3]]
+    assert p[:, 0].tolist() == [1.0, 20.0, 2.0, 40.0] and p[2, 4] == 6.5 and p[0, 4] == 0.0
+    n = np.ctypeslib.as_array(C.cast(s.table_n, C.POINTER(C.c_int32)), shape=(2,))
+    e = np.ctypeslib.as_array(C.cast(s.table_e, C.POINTER(C.c_double)), shape=(10,))
+    assert n.tolist() == [5, 5] and np.allclose(e[:5], tab[2]) and np.allclose(e[5:], tab[2])
