@@ -1871,8 +1871,9 @@ struct MdRun {
   void mtk_remap();
   void mtk_step(long long s);
   // a step that reports, records, rescales the cell or refills the thermostat's draws
+  // (every MTK step is one: it runs on the host's schedule, in a batch too)
   bool special(long long s) const {
-    return s % thermo_every == 0 || s == o.steps || frame_due(s) || checkpoint_due(s) || baro_due(s) || refill_due(s);
+    return mtk() || s % thermo_every == 0 || s == o.steps || frame_due(s) || checkpoint_due(s) || baro_due(s) || refill_due(s);
   }
 
   void start();
